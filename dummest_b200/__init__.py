@@ -1,0 +1,22 @@
+"""B200-native implementation of DUMMEST's search hot path.
+
+The frameshift-aware DNA x protein-profile Forward/Backward DP (mid-anchored
+score), the lean backward-only filter, and the random-sequence scoring of
+Gumbel calibration, as hand-written sm_100a CUDA behind the C ABI in
+include/dummest_b200.h.  This package is the host-side mirror of the
+reference interface over that ABI (see engine.py).
+"""
+from ._ffi import MODE_FILTER, MODE_FORCE_EXACT, MODE_MID, MODE_PLAIN, load  # noqa: F401
+from .engine import (  # noqa: F401
+    Context,
+    DmstError,
+    Score,
+    Similarity,
+    calibration_sequence,
+    decode_dna,
+    decode_letters,
+    encode_dna,
+    estimate_gumbel,
+    finalize_hmm,
+    pack_dna,
+)

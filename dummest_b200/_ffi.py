@@ -1,0 +1,134 @@
+"""ctypes binding of libdummest_b200.so (the C ABI in include/dummest_b200.h).
+
+The shared library is the product: there is no CPU fallback.  Loading fails
+loudly when the library is missing or cannot be loaded.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdummest_b200.so")
+
+DMST_OK = 0
+DMST_EINVAL = -1
+DMST_ENOMEM = -2
+DMST_EDEVICE = -3
+DMST_ETIMEOUT = -4
+DMST_EPARSE = -5
+DMST_ERANGE = -6
+
+MODE_MID = 0
+MODE_FILTER = 1
+MODE_PLAIN = 0x100
+MODE_FORCE_EXACT = 0x200
+RES_EXACT_PATH = 1
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("alpha_prime", C.c_float * 3),
+        ("beta_prime", C.c_float * 3),
+        ("delta_prime", C.c_float * 3),
+        ("epsilon_prime", C.c_float),
+        ("enter_match_probability", C.c_float),
+    ]
+
+
+class Score(C.Structure):
+    _fields_ = [("m", C.c_float), ("e", C.c_int32)]
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("insert1", C.c_double),
+        ("insert2", C.c_double),
+        ("delete1", C.c_double),
+        ("delete2", C.c_double),
+        ("stop_codon_prob", C.c_double),
+        ("bg_stop_codon_prob", C.c_double),
+        ("device", C.c_int),
+        ("rows_per_lane", C.c_int),
+        ("device_budget_bytes", C.c_size_t),
+    ]
+
+
+class Pair(C.Structure):
+    _fields_ = [("seq", C.c_int32), ("profile", C.c_int32), ("min_prob_ratio", C.c_float)]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("mid", Score),
+        ("filter", Score),
+        ("mid_ln", C.c_double),
+        ("filter_ln", C.c_double),
+        ("filter_f", C.c_float),
+        ("flags", C.c_int32),
+    ]
+
+
+# (name, restype, argtypes) of every entry point declared in include/dummest_b200.h.
+SIGNATURES = [
+    ("dmst_opts_default", None, [C.POINTER(Opts)]),
+    ("dmst_ctx_create", C.c_int, [C.POINTER(Opts), C.POINTER(C.c_void_p)]),
+    ("dmst_ctx_destroy", None, [C.c_void_p]),
+    ("dmst_strerror", C.c_char_p, [C.c_int]),
+    ("dmst_last_error", C.c_char_p, [C.c_void_p]),
+    ("dmst_profile_add", C.c_int,
+     [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(Params), C.POINTER(C.c_float),
+      C.POINTER(C.c_int)]),
+    ("dmst_profile_load_hmm", C.c_int,
+     [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("dmst_hmm_finalize", C.c_int,
+     [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(Opts), C.POINTER(C.c_int), C.POINTER(C.c_float),
+      C.POINTER(Params), C.POINTER(C.c_float), C.c_char_p, C.c_size_t]),
+    ("dmst_profile_count", C.c_int, [C.c_void_p]),
+    ("dmst_profile_length", C.c_int, [C.c_void_p, C.c_int]),
+    ("dmst_seqs_add_decoded", C.c_int,
+     [C.c_void_p, C.POINTER(C.c_uint8), C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]),
+    ("dmst_seqs_add_dna", C.c_int,
+     [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]),
+    ("dmst_seqs_add_packed", C.c_int,
+     [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int64), C.c_int,
+      C.POINTER(C.c_int)]),
+    ("dmst_seqs_clear", C.c_int, [C.c_void_p]),
+    ("dmst_seq_count", C.c_int, [C.c_void_p]),
+    ("dmst_decode_letters", C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_uint8)]),
+    ("dmst_encode_dna", C.c_int, [C.c_char_p, C.c_int, C.c_char_p]),
+    ("dmst_score_pairs", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.c_int, C.POINTER(Result)]),
+    ("dmst_last_timing", C.c_int,
+     [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("dmst_null_model", C.c_int,
+     [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("dmst_estimate_gumbel", C.c_int, [C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double)]),
+    ("dmst_calibration_sequence", C.c_int,
+     [C.POINTER(C.c_float), C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+      C.c_int, C.c_char_p]),
+    ("dmst_calibrate", C.c_int,
+     [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load (once) and bind the library.  Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m dummest_b200.build` (there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return [s[0] for s in SIGNATURES]

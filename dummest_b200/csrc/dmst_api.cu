@@ -1,0 +1,993 @@
+// C ABI of the B200 search path (include/dummest_b200.h): context, device
+// memory, profile and sequence upload, pair scheduling and kernel launches.
+#include "dummest_b200.h"
+
+#include "dp_common.cuh"
+#include "dp_exact.cuh"
+#include "dp_wavefront.cuh"
+#include "host_model.h"
+#include "null_model.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+using namespace dmst;
+
+namespace {
+
+__constant__ uint8_t cCodonTable[64];
+
+// ---------------------------------------------------------------------------
+// Device decode: DNA -> codon codes (decodeSequence, dummest-sequence.hh:181-204)
+// One CTA per sequence.  Bases are 0..3 (ACGT) or 4 (anything else / masked).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int asciiBase(unsigned char ch) {
+    switch (ch | 0x20) {
+    case 'a': return 0;
+    case 'c': return 1;
+    case 'g': return 2;
+    case 't': return 3;
+    default: return 4;
+    }
+}
+
+__global__ void decodeAsciiKernel(const char *ascii, const long long *inOff, const long long *outOff, const int *lens,
+                                  uint8_t *codes) {
+    const int s = blockIdx.x;
+    const int L = lens[s];
+    const char *in = ascii + inOff[s];
+    uint8_t *out = codes + outOff[s];
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        uint8_t c = 0;
+        if (i + 2 < L) {
+            int b0 = asciiBase(in[i]), b1 = asciiBase(in[i + 1]), b2 = asciiBase(in[i + 2]);
+            c = (b0 > 3 || b1 > 3 || b2 > 3) ? (uint8_t)kMaskCode : cCodonTable[16 * b0 + 4 * b1 + b2];
+        }
+        out[i] = c;
+    }
+}
+
+// 2-bit packed input: 16 bases per 32-bit word, optional masked-base bitmap.
+__global__ void decodePackedKernel(const uint32_t *words, const uint32_t *mask, const long long *wordOff,
+                                   const long long *maskOff, const long long *outOff, const int *lens,
+                                   uint8_t *codes) {
+    const int s = blockIdx.x;
+    const int L = lens[s];
+    const uint32_t *w = words + wordOff[s];
+    const uint32_t *mk = mask ? mask + maskOff[s] : nullptr;
+    uint8_t *out = codes + outOff[s];
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        uint8_t c = 0;
+        if (i + 2 < L) {
+            int b[3];
+            bool masked = false;
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const int k = i + t;
+                b[t] = (int)((__ldg(w + (k >> 4)) >> (2 * (k & 15))) & 3u);
+                if (mk && ((__ldg(mk + (k >> 5)) >> (k & 31)) & 1u)) masked = true;
+            }
+            c = masked ? (uint8_t)kMaskCode : cCodonTable[16 * b[0] + 4 * b[1] + b[2]];
+        }
+        out[i] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small device buffer helper
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;  // elements
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(n, 1);
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    // Grow keeping the first `keep` elements.
+    cudaError_t grow(size_t n, size_t keep, cudaStream_t st) {
+        if (n <= cap && p) return cudaSuccess;
+        size_t want = std::max(n, cap * 2);
+        T *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, want * sizeof(T));
+        if (e != cudaSuccess) return e;
+        if (p && keep) {
+            e = cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) {
+                cudaFree(q);
+                return e;
+            }
+            cudaStreamSynchronize(st);
+        }
+        if (p) cudaFree(p);
+        p = q;
+        cap = want;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct HostProfile {
+    int M;
+    int rowPad;
+    std::vector<float> emit;    // [25][rowPad]
+    std::vector<float> params;  // (M+2) x 11
+    float bg[26];
+    std::vector<float> values;  // (M+1) x 29 (kept for calibration letter freqs)
+};
+
+const char *statusText(int s) {
+    switch (s) {
+    case DMST_OK: return "ok";
+    case DMST_EINVAL: return "invalid argument";
+    case DMST_ENOMEM: return "out of memory";
+    case DMST_EDEVICE: return "CUDA device error";
+    case DMST_ETIMEOUT: return "kernel iteration budget exceeded";
+    case DMST_EPARSE: return "parse error";
+    case DMST_ERANGE: return "size beyond a documented limit";
+    default: return "unknown status";
+    }
+}
+
+int rowsPerLane(int M, int forced) {
+    if (forced == 1 || forced == 2 || forced == 4) return forced;
+    const int rows = M + 1;
+    // Waste of padding rows in the last stripe against wavefront depth: tall
+    // profiles use 4 rows per lane, short ones fewer.
+    if (rows > 192) return 4;
+    if (rows > 80) return 2;
+    return 1;
+}
+
+}  // namespace
+
+struct dmst_ctx {
+    dmst_opts opts;
+    Rates rates;
+    int device = 0;
+    int smCount = 0;
+    int maxSmemOptin = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    std::string err;
+
+    std::vector<HostProfile> profiles;
+    bool profilesDirty = false;
+    DevBuf<float> dEmit, dParams;
+    DevBuf<DevProfile> dProfiles;
+    int maxRowPad = 0;
+
+    std::vector<long long> seqOff;  // code offsets (device buffer)
+    std::vector<int> seqLen;
+    long long codeBytes = 0;
+    DevBuf<uint8_t> dCodes;
+    DevBuf<char> dStage;
+    DevBuf<long long> dStageOff;
+    DevBuf<int> dStageLen;
+
+    // per call
+    DevBuf<DevPair> dPairs;
+    DevBuf<float> dSeeds;
+    DevBuf<XS> dNullTmp;
+    DevBuf<long long> dNullTmpOff;
+    DevBuf<PairScales> dScales;
+    DevBuf<PairOut> dOut;
+    DevBuf<Chunk> dChunks;
+    DevBuf<int> dCounter;
+    DevBuf<float> dW1, dRing;
+    DevBuf<ExactJob> dJobs;
+    DevBuf<float> dExactScratch;
+    DevBuf<ExactOut> dExactOut;
+
+    double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0;
+    int lastLaunches = 0;
+
+    int fail(int status, const char *fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return status;
+    }
+    int cudaFail(cudaError_t e, const char *what) {
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return fail(DMST_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+        }
+        return fail(DMST_EDEVICE, "%s: %s", what, cudaGetErrorString(e));
+    }
+};
+
+#define CK(call, what)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return ctx->cudaFail(e_, what); \
+    } while (0)
+
+extern "C" {
+
+void dmst_opts_default(dmst_opts *o) {
+    if (!o) return;
+    o->insert1 = 0.0171;  // OPT_insert1 (dummest-core.hh:66-71)
+    o->insert2 = 0.0018;
+    o->delete1 = 0.0328;
+    o->delete2 = 0.0083;
+    o->stop_codon_prob = 0.0005;
+    o->bg_stop_codon_prob = 0.046875;
+    o->device = 0;
+    o->rows_per_lane = 0;
+    o->device_budget_bytes = 0;
+}
+
+const char *dmst_strerror(int status) { return statusText(status); }
+
+const char *dmst_last_error(const dmst_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out) {
+    if (!out) return DMST_EINVAL;
+    *out = nullptr;
+    dmst_opts o;
+    dmst_opts_default(&o);
+    if (opts) o = *opts;
+    if (!(o.insert1 >= 0 && o.insert1 < 1 && o.insert2 >= 0 && o.insert2 < 1 && o.delete1 >= 0 && o.delete1 < 1 &&
+          o.delete2 >= 0 && o.delete2 < 1 && o.insert1 + o.insert2 + o.delete1 + o.delete2 < 1 &&
+          o.stop_codon_prob >= 0 && o.stop_codon_prob < 1 && o.bg_stop_codon_prob >= 0 &&
+          o.bg_stop_codon_prob < 1))
+        return DMST_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= o.device || o.device < 0) {
+        cudaGetLastError();
+        return DMST_EDEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, o.device) != cudaSuccess) return DMST_EDEVICE;
+    if (prop.major < 10) return DMST_EDEVICE;  // built for sm_100a only
+    dmst_ctx *ctx = new (std::nothrow) dmst_ctx();
+    if (!ctx) return DMST_ENOMEM;
+    ctx->opts = o;
+    ctx->rates.insert1 = (float)o.insert1;
+    ctx->rates.insert2 = (float)o.insert2;
+    ctx->rates.delete1 = (float)o.delete1;
+    ctx->rates.delete2 = (float)o.delete2;
+    ctx->rates.stop = (float)o.stop_codon_prob;
+    ctx->rates.bgStop = (float)o.bg_stop_codon_prob;
+    ctx->device = o.device;
+    ctx->smCount = prop.multiProcessorCount;
+    ctx->maxSmemOptin = (int)prop.sharedMemPerBlockOptin;
+    if (cudaSetDevice(o.device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return DMST_EDEVICE;
+    }
+    for (auto &e : ctx->ev) cudaEventCreate(&e);
+    uint8_t table[64];
+    standardCodeTable(table);
+    if (cudaMemcpyToSymbol(cCodonTable, table, 64) != cudaSuccess) {
+        delete ctx;
+        return DMST_EDEVICE;
+    }
+    *out = ctx;
+    return DMST_OK;
+}
+
+void dmst_ctx_destroy(dmst_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->dEmit.release();
+    ctx->dParams.release();
+    ctx->dProfiles.release();
+    ctx->dCodes.release();
+    ctx->dStage.release();
+    ctx->dStageOff.release();
+    ctx->dStageLen.release();
+    ctx->dPairs.release();
+    ctx->dSeeds.release();
+    ctx->dNullTmp.release();
+    ctx->dNullTmpOff.release();
+    ctx->dScales.release();
+    ctx->dOut.release();
+    ctx->dChunks.release();
+    ctx->dCounter.release();
+    ctx->dW1.release();
+    ctx->dRing.release();
+    ctx->dJobs.release();
+    ctx->dExactScratch.release();
+    ctx->dExactOut.release();
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// ---------------------------------------------------------------------------
+// Profiles
+// ---------------------------------------------------------------------------
+int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const dmst_params *params,
+                     const float *bg, int *id) {
+    if (!ctx || !values || !params || !bg || width != kWidth || M < 2) return DMST_EINVAL;
+    HostProfile hp;
+    hp.M = M;
+    hp.rowPad = (M + 1 + kRowAlign - 1) / kRowAlign * kRowAlign;
+    hp.emit.assign((size_t)kNumCodes * hp.rowPad, 0.0f);
+    for (int i = 0; i <= M; ++i)
+        for (int c = 0; c < kNumCodes; ++c) hp.emit[(size_t)c * hp.rowPad + i] = values[(size_t)i * width + 4 + c];
+    hp.params.resize((size_t)(M + 2) * kParamFloats);
+    std::memcpy(hp.params.data(), params, hp.params.size() * sizeof(float));
+    for (int c = 0; c < 26; ++c) hp.bg[c] = (c < kNumCodes) ? bg[4 + c] : 0.0f;
+    hp.bg[kPad] = 0.0f;  // zero_idx pad reads as 0
+    hp.values.assign(values, values + (size_t)(M + 1) * width);
+    ctx->profiles.push_back(std::move(hp));
+    ctx->profilesDirty = true;
+    if (id) *id = (int)ctx->profiles.size() - 1;
+    return DMST_OK;
+}
+
+int dmst_hmm_finalize(const char *text, size_t len, int index, int background_type, const dmst_opts *opts, int *M,
+                      float *values, dmst_params *params, float *bg, char *name, size_t name_cap) {
+    if (!text || !M) return DMST_EINVAL;
+    dmst_opts o;
+    dmst_opts_default(&o);
+    if (opts) o = *opts;
+    std::vector<RawProfile> raws;
+    if (parseHmmText(text, len, raws, nullptr) < 0) return DMST_EPARSE;
+    if (index < 0 || index >= (int)raws.size()) return DMST_EINVAL;
+    *M = raws[index].M;
+    if (!values) return DMST_OK;
+    Rates r{(float)o.insert1, (float)o.insert2, (float)o.delete1, (float)o.delete2, (float)o.stop_codon_prob,
+            (float)o.bg_stop_codon_prob};
+    FinalProfile f;
+    if (finalizeProfile(raws[index], r, background_type ? background_type : 'G', f, nullptr) < 0) return DMST_EPARSE;
+    std::memcpy(values, f.values.data(), f.values.size() * sizeof(float));
+    if (params) std::memcpy(params, f.params.data(), f.params.size() * sizeof(Params));
+    if (bg) std::memcpy(bg, f.bg.data(), f.bg.size() * sizeof(float));
+    if (name && name_cap) {
+        std::snprintf(name, name_cap, "%s", f.name.c_str());
+    }
+    return DMST_OK;
+}
+
+int dmst_profile_load_hmm(dmst_ctx *ctx, const char *text, size_t len, int background_type, int *first_id,
+                          int *count) {
+    if (!ctx || !text) return DMST_EINVAL;
+    std::vector<RawProfile> raws;
+    std::string e;
+    if (parseHmmText(text, len, raws, &e) < 0) return ctx->fail(DMST_EPARSE, "HMMER3: %s", e.c_str());
+    int first = (int)ctx->profiles.size();
+    for (auto &raw : raws) {
+        FinalProfile f;
+        if (finalizeProfile(raw, ctx->rates, background_type ? background_type : 'G', f, &e) < 0)
+            return ctx->fail(DMST_EPARSE, "profile %s: %s", raw.name.c_str(), e.c_str());
+        int st = dmst_profile_add(ctx, f.values.data(), f.width, f.M,
+                                  reinterpret_cast<const dmst_params *>(f.params.data()), f.bg.data(), nullptr);
+        if (st) return st;
+    }
+    if (first_id) *first_id = first;
+    if (count) *count = (int)raws.size();
+    return DMST_OK;
+}
+
+int dmst_profile_count(const dmst_ctx *ctx) { return ctx ? (int)ctx->profiles.size() : 0; }
+int dmst_profile_length(const dmst_ctx *ctx, int id) {
+    if (!ctx || id < 0 || id >= (int)ctx->profiles.size()) return DMST_EINVAL;
+    return ctx->profiles[id].M;
+}
+
+static int uploadProfiles(dmst_ctx *ctx) {
+    if (!ctx->profilesDirty) return DMST_OK;
+    size_t nE = 0, nP = 0;
+    for (auto &p : ctx->profiles) {
+        nE += p.emit.size();
+        nP += p.params.size();
+    }
+    std::vector<float> emit(nE), par(nP);
+    std::vector<DevProfile> desc(ctx->profiles.size());
+    size_t oE = 0, oP = 0;
+    ctx->maxRowPad = 0;
+    for (size_t i = 0; i < ctx->profiles.size(); ++i) {
+        auto &p = ctx->profiles[i];
+        std::copy(p.emit.begin(), p.emit.end(), emit.begin() + oE);
+        std::copy(p.params.begin(), p.params.end(), par.begin() + oP);
+        DevProfile &d = desc[i];
+        d.M = p.M;
+        d.rowPad = p.rowPad;
+        d.emitOff = (long long)oE;
+        d.paramOff = (long long)oP;
+        std::memcpy(d.bg, p.bg, sizeof d.bg);
+        oE += p.emit.size();
+        oP += p.params.size();
+        ctx->maxRowPad = std::max(ctx->maxRowPad, p.rowPad);
+    }
+    CK(ctx->dEmit.ensure(nE), "alloc emission tables");
+    CK(ctx->dParams.ensure(nP), "alloc params");
+    CK(ctx->dProfiles.ensure(desc.size()), "alloc profiles");
+    CK(cudaMemcpy(ctx->dEmit.p, emit.data(), nE * sizeof(float), cudaMemcpyHostToDevice), "upload emission");
+    CK(cudaMemcpy(ctx->dParams.p, par.data(), nP * sizeof(float), cudaMemcpyHostToDevice), "upload params");
+    CK(cudaMemcpy(ctx->dProfiles.p, desc.data(), desc.size() * sizeof(DevProfile), cudaMemcpyHostToDevice),
+       "upload profiles");
+    ctx->profilesDirty = false;
+    return DMST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Sequences
+// ---------------------------------------------------------------------------
+static int checkOffsets(const int64_t *offsets, int nseq) {
+    if (!offsets || nseq < 0) return DMST_EINVAL;
+    for (int i = 0; i < nseq; ++i) {
+        int64_t L = offsets[i + 1] - offsets[i];
+        if (L < 3 || L > (1 << 30)) return DMST_EINVAL;
+    }
+    return DMST_OK;
+}
+
+// Reserve device code space for nseq new sequences; fills the new offsets.
+static int reserveSeqs(dmst_ctx *ctx, const int64_t *offsets, int nseq, std::vector<long long> &outOff,
+                       std::vector<int> &lens) {
+    long long total = 0;
+    outOff.resize(nseq);
+    lens.resize(nseq);
+    for (int i = 0; i < nseq; ++i) {
+        lens[i] = (int)(offsets[i + 1] - offsets[i]);
+        outOff[i] = ctx->codeBytes + total;
+        total += (lens[i] + 15) / 16 * 16;  // 16-byte aligned starts
+    }
+    CK(ctx->dCodes.grow((size_t)(ctx->codeBytes + total), (size_t)ctx->codeBytes, ctx->stream), "alloc codes");
+    return DMST_OK;
+}
+
+static void commitSeqs(dmst_ctx *ctx, const std::vector<long long> &off, const std::vector<int> &lens, int *first) {
+    if (first) *first = (int)ctx->seqLen.size();
+    for (size_t i = 0; i < lens.size(); ++i) {
+        ctx->seqOff.push_back(off[i]);
+        ctx->seqLen.push_back(lens[i]);
+        ctx->codeBytes = off[i] + (lens[i] + 15) / 16 * 16;
+    }
+}
+
+int dmst_seqs_add_decoded(dmst_ctx *ctx, const uint8_t *codes, const int64_t *offsets, int nseq, int *first_id) {
+    if (!ctx || (!codes && nseq > 0)) return DMST_EINVAL;
+    int st = checkOffsets(offsets, nseq);
+    if (st) return ctx->fail(st, "every sequence needs length >= 3");
+    for (int64_t k = offsets[0]; k < offsets[nseq]; ++k)
+        if (codes[k] >= kNumCodes) return ctx->fail(DMST_EINVAL, "codon code out of range at %lld", (long long)k);
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<long long> off;
+    std::vector<int> lens;
+    if ((st = reserveSeqs(ctx, offsets, nseq, off, lens))) return st;
+    for (int i = 0; i < nseq; ++i)
+        CK(cudaMemcpyAsync(ctx->dCodes.p + off[i], codes + offsets[i], lens[i], cudaMemcpyHostToDevice, ctx->stream),
+           "upload codes");
+    CK(cudaStreamSynchronize(ctx->stream), "upload codes");
+    commitSeqs(ctx, off, lens, first_id);
+    return DMST_OK;
+}
+
+int dmst_seqs_add_dna(dmst_ctx *ctx, const char *ascii, const int64_t *offsets, int nseq, int *first_id) {
+    if (!ctx || (!ascii && nseq > 0)) return DMST_EINVAL;
+    int st = checkOffsets(offsets, nseq);
+    if (st) return ctx->fail(st, "every sequence needs length >= 3");
+    if (nseq == 0) {
+        if (first_id) *first_id = (int)ctx->seqLen.size();
+        return DMST_OK;
+    }
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<long long> off;
+    std::vector<int> lens;
+    if ((st = reserveSeqs(ctx, offsets, nseq, off, lens))) return st;
+    const size_t nbytes = (size_t)(offsets[nseq] - offsets[0]);
+    std::vector<long long> inOff(nseq);
+    for (int i = 0; i < nseq; ++i) inOff[i] = offsets[i] - offsets[0];
+    CK(ctx->dStage.ensure(nbytes), "alloc staging");
+    CK(ctx->dStageOff.ensure(2 * (size_t)nseq), "alloc staging");
+    CK(ctx->dStageLen.ensure(nseq), "alloc staging");
+    CK(cudaMemcpyAsync(ctx->dStage.p, ascii + offsets[0], nbytes, cudaMemcpyHostToDevice, ctx->stream), "upload dna");
+    CK(cudaMemcpyAsync(ctx->dStageOff.p, inOff.data(), nseq * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream),
+       "upload offsets");
+    CK(cudaMemcpyAsync(ctx->dStageOff.p + nseq, off.data(), nseq * sizeof(long long), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "upload offsets");
+    CK(cudaMemcpyAsync(ctx->dStageLen.p, lens.data(), nseq * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+       "upload lengths");
+    decodeAsciiKernel<<<nseq, 256, 0, ctx->stream>>>(ctx->dStage.p, ctx->dStageOff.p, ctx->dStageOff.p + nseq,
+                                                       ctx->dStageLen.p, ctx->dCodes.p);
+    CK(cudaGetLastError(), "decode kernel");
+    CK(cudaStreamSynchronize(ctx->stream), "decode kernel");
+    commitSeqs(ctx, off, lens, first_id);
+    return DMST_OK;
+}
+
+int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *mask_bits, const int64_t *offsets,
+                         int nseq, int *first_id) {
+    if (!ctx || (!words && nseq > 0)) return DMST_EINVAL;
+    int st = checkOffsets(offsets, nseq);
+    if (st) return ctx->fail(st, "every sequence needs length >= 3");
+    if (nseq == 0) {
+        if (first_id) *first_id = (int)ctx->seqLen.size();
+        return DMST_OK;
+    }
+    CK(cudaSetDevice(ctx->device), "set device");
+    std::vector<long long> off;
+    std::vector<int> lens;
+    if ((st = reserveSeqs(ctx, offsets, nseq, off, lens))) return st;
+    // word / mask-word offsets per sequence: each sequence starts on a fresh word.
+    std::vector<long long> wOff(nseq), mOff(nseq);
+    long long nw = 0, nm = 0;
+    for (int i = 0; i < nseq; ++i) {
+        wOff[i] = nw;
+        mOff[i] = nm;
+        nw += (lens[i] + 15) / 16;
+        nm += (lens[i] + 31) / 32;
+    }
+    const size_t bytes = (size_t)nw * 4 + (mask_bits ? (size_t)nm * 4 : 0);
+    CK(ctx->dStage.ensure(bytes), "alloc staging");
+    CK(ctx->dStageOff.ensure(3 * (size_t)nseq), "alloc staging");
+    CK(ctx->dStageLen.ensure(nseq), "alloc staging");
+    uint32_t *dw = reinterpret_cast<uint32_t *>(ctx->dStage.p);
+    uint32_t *dm = mask_bits ? dw + nw : nullptr;
+    CK(cudaMemcpyAsync(dw, words, (size_t)nw * 4, cudaMemcpyHostToDevice, ctx->stream), "upload packed");
+    if (mask_bits) CK(cudaMemcpyAsync(dm, mask_bits, (size_t)nm * 4, cudaMemcpyHostToDevice, ctx->stream), "upload mask");
+    CK(cudaMemcpyAsync(ctx->dStageOff.p, wOff.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream), "upload offsets");
+    CK(cudaMemcpyAsync(ctx->dStageOff.p + nseq, mOff.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream),
+       "upload offsets");
+    CK(cudaMemcpyAsync(ctx->dStageOff.p + 2 * nseq, off.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream),
+       "upload offsets");
+    CK(cudaMemcpyAsync(ctx->dStageLen.p, lens.data(), nseq * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+       "upload lengths");
+    decodePackedKernel<<<nseq, 256, 0, ctx->stream>>>(dw, dm, ctx->dStageOff.p, ctx->dStageOff.p + nseq,
+                                                        ctx->dStageOff.p + 2 * nseq, ctx->dStageLen.p, ctx->dCodes.p);
+    CK(cudaGetLastError(), "decode kernel");
+    CK(cudaStreamSynchronize(ctx->stream), "decode kernel");
+    commitSeqs(ctx, off, lens, first_id);
+    return DMST_OK;
+}
+
+int dmst_seqs_clear(dmst_ctx *ctx) {
+    if (!ctx) return DMST_EINVAL;
+    ctx->seqOff.clear();
+    ctx->seqLen.clear();
+    ctx->codeBytes = 0;
+    return DMST_OK;
+}
+
+int dmst_seq_count(const dmst_ctx *ctx) { return ctx ? (int)ctx->seqLen.size() : 0; }
+
+int dmst_decode_letters(const char *letters, int L, uint8_t *codes) {
+    if (!letters || !codes || L < 0) return DMST_EINVAL;
+    decodeLetters(letters, L, codes);
+    return DMST_OK;
+}
+
+int dmst_encode_dna(const char *ascii, int L, char *letters) {
+    if (!ascii || !letters || L < 0) return DMST_EINVAL;
+    return encodeDna(ascii, L, letters) < 0 ? DMST_EPARSE : DMST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scoring
+// ---------------------------------------------------------------------------
+static void fillResult(dmst_result &r, float v, bool isFilterF, dmst_score *dst, double *ln) {
+    (void)isFilterF;
+    (void)r;
+    if (!(v > 0.0f)) {
+        dst->m = 0.0f;
+        dst->e = 0;
+        *ln = -INFINITY;
+        return;
+    }
+    int e = 0;
+    float m = std::frexp(v, &e);
+    if (std::isinf(v)) {
+        m = 0.0f;
+        e = 0;
+    }
+    dst->m = m;
+    dst->e = e;
+    *ln = (m == 0.0f) ? (std::isinf(v) ? INFINITY : -INFINITY) : std::log((double)m) + (double)e * 0.6931471805599453;
+}
+
+static void scoreToResult(XS s, dmst_score *dst, double *ln) {
+    dst->m = s.m;
+    dst->e = s.e;
+    *ln = (s.m == 0.0f) ? -INFINITY : std::log((double)s.m) + (double)s.e * 0.6931471805599453;
+}
+
+int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
+    if (!ctx || (n && (!pairs || !out))) return DMST_EINVAL;
+    const int base = mode & 0xff;
+    const bool plain = (mode & DMST_MODE_PLAIN) != 0;
+    const bool forceExact = (mode & DMST_MODE_FORCE_EXACT) != 0;
+    if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
+    const bool mid = base == DMST_MODE_MID;
+    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = 0;
+    ctx->lastLaunches = 0;
+    if (n == 0) return DMST_OK;
+    if (n > (size_t)INT32_MAX / 2) return ctx->fail(DMST_ERANGE, "too many pairs");
+    CK(cudaSetDevice(ctx->device), "set device");
+    int st = uploadProfiles(ctx);
+    if (st) return st;
+
+    // Pair descriptors, ordered by profile then by cost (costliest first).
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    for (size_t i = 0; i < n; ++i) {
+        const dmst_pair &q = pairs[i];
+        if (q.seq < 0 || q.seq >= (int)ctx->seqLen.size() || q.profile < 0 || q.profile >= (int)ctx->profiles.size())
+            return ctx->fail(DMST_EINVAL, "pair %zu: unknown sequence or profile id", i);
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const dmst_pair &x = pairs[a], &y = pairs[b];
+        if (x.profile != y.profile) return x.profile < y.profile;
+        return ctx->seqLen[x.seq] > ctx->seqLen[y.seq];
+    });
+    std::vector<DevPair> dp(n);
+    std::vector<long long> tmpOff(n);
+    long long seedFloats = 0, tmpEntries = 0;
+    size_t w1Max = 0, ringMax = 0;
+    for (size_t k = 0; k < n; ++k) {
+        const dmst_pair &q = pairs[order[k]];
+        DevPair &d = dp[k];
+        d.codeOff = ctx->seqOff[q.seq];
+        d.L = ctx->seqLen[q.seq];
+        d.M = ctx->profiles[q.profile].M;
+        d.prof = q.profile;
+        d.R = rowsPerLane(d.M, ctx->opts.rows_per_lane);
+        d.seedOff = seedFloats;
+        seedFloats += 2LL * d.L;
+        tmpOff[k] = tmpEntries;
+        tmpEntries += d.L + 4;
+        const int S = kLanes * d.R;
+        const size_t nS = (size_t)(d.M + 1 + S - 1) / S;
+        const size_t P = (size_t)std::max(d.L, kLanes);
+        const size_t D = P + kLanes - 1;
+        if (mid) w1Max = std::max(w1Max, nS * D * (size_t)S);
+        ringMax = std::max(ringMax, 2 * P);
+    }
+    // Chunks: runs of up to 2 * warps pairs of one profile; costliest first.
+    const int chunkPairs = 2 * kWarpsPerCta;
+    std::vector<Chunk> chunks;
+    std::vector<double> chunkCost;
+    for (size_t k = 0; k < n;) {
+        size_t e = k;
+        double cost = 0;
+        while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
+            cost += (double)(dp[e].M + 1) * dp[e].L;
+            ++e;
+        }
+        chunks.push_back(Chunk{(int)k, (int)(e - k), dp[k].prof, ctx->profiles[dp[k].prof].rowPad});
+        chunkCost.push_back(cost);
+        k = e;
+    }
+    {
+        std::vector<int> co(chunks.size());
+        std::iota(co.begin(), co.end(), 0);
+        std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return chunkCost[a] > chunkCost[b]; });
+        std::vector<Chunk> sorted(chunks.size());
+        for (size_t i = 0; i < co.size(); ++i) sorted[i] = chunks[co[i]];
+        chunks.swap(sorted);
+    }
+
+    CK(ctx->dPairs.ensure(n), "alloc pairs");
+    CK(ctx->dSeeds.ensure((size_t)seedFloats), "alloc seeds");
+    CK(ctx->dNullTmp.ensure((size_t)tmpEntries), "alloc null tmp");
+    CK(ctx->dNullTmpOff.ensure(n), "alloc null tmp");
+    CK(ctx->dScales.ensure(n), "alloc scales");
+    CK(ctx->dOut.ensure(n), "alloc out");
+    CK(ctx->dChunks.ensure(chunks.size()), "alloc chunks");
+    CK(cudaMemcpyAsync(ctx->dPairs.p, dp.data(), n * sizeof(DevPair), cudaMemcpyHostToDevice, ctx->stream),
+       "upload pairs");
+    CK(cudaMemcpyAsync(ctx->dNullTmpOff.p, tmpOff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream),
+       "upload pairs");
+    CK(cudaMemcpyAsync(ctx->dChunks.p, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "upload chunks");
+
+    // Launch geometry of the persistent kernel.
+    const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
+    if ((int)smem > ctx->maxSmemOptin - 1024)
+        return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
+                         (ctx->maxSmemOptin - 1024) / (kNumCodes * 4) - 1);
+    auto kern = mid ? dpKernel<true> : dpKernel<false>;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    int perSm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kWarpsPerCta * kLanes, smem), "occupancy");
+    if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
+    int grid = plain ? 1 : std::min<long long>((long long)perSm * ctx->smCount, (long long)chunks.size());
+    if (grid < 1) grid = 1;
+    const size_t slots = (size_t)grid * kWarpsPerCta;
+    const size_t w1Slot = (w1Max + 63) / 64 * 64;
+    const size_t ringSlot = (ringMax + 63) / 64 * 64;
+    CK(ctx->dW1.ensure(std::max<size_t>(slots * w1Slot, 1)), "alloc W1 slots");
+    CK(ctx->dRing.ensure(slots * ringSlot), "alloc ring slots");
+    const size_t nCounters = plain ? n : 1;
+    CK(ctx->dCounter.ensure(nCounters), "alloc counters");
+    CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
+
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
+    NullRates nr;
+    nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
+    nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
+    {
+        const int tpb = 128;
+        nullModelKernel<<<(int)((n + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
+            ctx->dPairs.p, (int)n, ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p, ctx->dNullTmp.p,
+            ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+        CK(cudaGetLastError(), "null-model kernel");
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+    DpArgs g;
+    g.chunks = ctx->dChunks.p;
+    g.nChunks = (int)chunks.size();
+    g.chunkCounter = ctx->dCounter.p;
+    g.pairs = ctx->dPairs.p;
+    g.profiles = ctx->dProfiles.p;
+    g.emit = ctx->dEmit.p;
+    g.params = ctx->dParams.p;
+    g.codes = ctx->dCodes.p;
+    g.seeds = ctx->dSeeds.p;
+    g.scales = ctx->dScales.p;
+    g.w1 = ctx->dW1.p;
+    g.w1SlotFloats = w1Slot;
+    g.ring = ctx->dRing.p;
+    g.ringSlotFloats = ringSlot;
+    g.out = ctx->dOut.p;
+    int launches = 1;  // null-model kernel
+    if (!forceExact) {
+        if (plain) {
+            // One pair per launch: a one-warp grid over a one-pair chunk list.
+            std::vector<Chunk> single(n);
+            for (size_t k = 0; k < n; ++k)
+                single[k] = Chunk{(int)k, 1, dp[k].prof, ctx->profiles[dp[k].prof].rowPad};
+            CK(ctx->dChunks.ensure(n), "alloc chunks");
+            CK(cudaMemcpyAsync(ctx->dChunks.p, single.data(), n * sizeof(Chunk), cudaMemcpyHostToDevice,
+                               ctx->stream),
+               "upload chunks");
+            for (size_t k = 0; k < n; ++k) {
+                DpArgs gk = g;
+                gk.chunks = ctx->dChunks.p + k;
+                gk.nChunks = 1;
+                gk.chunkCounter = ctx->dCounter.p + k;
+                kern<<<1, kWarpsPerCta * kLanes, smem, ctx->stream>>>(gk);
+                ++launches;
+            }
+        } else {
+            kern<<<grid, kWarpsPerCta * kLanes, smem, ctx->stream>>>(g);
+            ++launches;
+        }
+        CK(cudaGetLastError(), "DP kernel");
+    }
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+    std::vector<PairOut> po(n);
+    if (!forceExact)
+        CK(cudaMemcpyAsync(po.data(), ctx->dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
+           "download results");
+    CK(cudaStreamSynchronize(ctx->stream), "DP kernel");
+
+    // Pairs outside the fast path's exact range go to the row-rescaled kernel.
+    std::vector<int> flagged;
+    for (size_t k = 0; k < n; ++k) {
+        if (!mid) continue;
+        const PairOut &o = po[k];
+        const bool ok = !forceExact && o.maxYb <= kRescaleThresh && o.maxFw <= kRescaleThresh &&
+                        o.mid < INFINITY && o.filt < INFINITY && o.mid >= 0x1p-100f;
+        if (!ok) flagged.push_back((int)k);
+    }
+    std::vector<ExactOut> eo;
+    float exactMs = 0;
+    if (!flagged.empty()) {
+        // Batch the flagged pairs under a scratch budget.
+        size_t free = 0, total = 0;
+        cudaMemGetInfo(&free, &total);
+        const size_t budget = std::max<size_t>(free / 2, (size_t)256 << 20);
+        eo.resize(flagged.size());
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        size_t i0 = 0;
+        while (i0 < flagged.size()) {
+            std::vector<ExactJob> jobs;
+            long long used = 0;
+            size_t i1 = i0;
+            while (i1 < flagged.size()) {
+                const DevPair &d = dp[flagged[i1]];
+                long long need = exactScratchFloats(d.M, d.L);
+                if (!jobs.empty() && (size_t)(used + need) * 4 > budget) break;
+                jobs.push_back(ExactJob{flagged[i1], used});
+                used += need;
+                ++i1;
+            }
+            CK(ctx->dJobs.ensure(jobs.size()), "alloc exact jobs");
+            CK(ctx->dExactScratch.ensure((size_t)used), "alloc exact scratch");
+            CK(ctx->dExactOut.ensure(jobs.size()), "alloc exact out");
+            CK(cudaMemcpyAsync(ctx->dJobs.p, jobs.data(), jobs.size() * sizeof(ExactJob), cudaMemcpyHostToDevice,
+                               ctx->stream),
+               "upload jobs");
+            const int tpb = 32;
+            exactKernel<<<(int)((jobs.size() + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
+                ctx->dJobs.p, (int)jobs.size(), ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+                ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
+            CK(cudaGetLastError(), "exact kernel");
+            ++launches;
+            CK(cudaMemcpyAsync(eo.data() + i0, ctx->dExactOut.p, jobs.size() * sizeof(ExactOut),
+                               cudaMemcpyDeviceToHost, ctx->stream),
+               "download exact");
+            CK(cudaStreamSynchronize(ctx->stream), "exact kernel");
+            i0 = i1;
+        }
+        CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
+        CK(cudaEventSynchronize(ctx->ev[4]), "event");
+        cudaEventElapsedTime(&exactMs, ctx->ev[3], ctx->ev[4]);
+    }
+
+    float nullMs = 0, dpMs = 0;
+    cudaEventElapsedTime(&nullMs, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&dpMs, ctx->ev[1], ctx->ev[2]);
+    ctx->lastNullMs = nullMs;
+    ctx->lastDpMs = dpMs;
+    ctx->lastTotalMs = nullMs + dpMs + exactMs;
+    ctx->lastLaunches = launches;
+
+    std::vector<int> flagAt(n, -1);
+    for (size_t f = 0; f < flagged.size(); ++f) flagAt[flagged[f]] = (int)f;
+    for (size_t k = 0; k < n; ++k) {
+        dmst_result &r = out[order[k]];
+        std::memset(&r, 0, sizeof r);
+        if (mid) {
+            if (flagAt[k] >= 0) {
+                scoreToResult(eo[flagAt[k]].mid, &r.mid, &r.mid_ln);
+                scoreToResult(eo[flagAt[k]].filt, &r.filter, &r.filter_ln);
+                r.flags |= DMST_RES_EXACT_PATH;
+            } else {
+                fillResult(r, po[k].mid, false, &r.mid, &r.mid_ln);
+                fillResult(r, po[k].filt, false, &r.filter, &r.filter_ln);
+            }
+            r.filter_f = po[k].filt;
+        } else {
+            const float f = po[k].filt;
+            r.filter_f = f;
+            r.filter_ln = std::log((double)f);
+            r.mid_ln = -INFINITY;
+        }
+    }
+    return DMST_OK;
+}
+
+int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, double *null_ms, int *launches) {
+    if (!ctx) return DMST_EINVAL;
+    if (total_ms) *total_ms = ctx->lastTotalMs;
+    if (dp_ms) *dp_ms = ctx->lastDpMs;
+    if (null_ms) *null_ms = ctx->lastNullMs;
+    if (launches) *launches = ctx->lastLaunches;
+    return DMST_OK;
+}
+
+int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, float *suffix_seed, float *scales3) {
+    if (!ctx || seq < 0 || seq >= (int)ctx->seqLen.size() || profile < 0 || profile >= (int)ctx->profiles.size())
+        return DMST_EINVAL;
+    CK(cudaSetDevice(ctx->device), "set device");
+    int st = uploadProfiles(ctx);
+    if (st) return st;
+    DevPair d;
+    d.codeOff = ctx->seqOff[seq];
+    d.L = ctx->seqLen[seq];
+    d.M = ctx->profiles[profile].M;
+    d.prof = profile;
+    d.R = 1;
+    d.seedOff = 0;
+    long long zero = 0;
+    CK(ctx->dPairs.ensure(1), "alloc");
+    CK(ctx->dSeeds.ensure(2 * (size_t)d.L), "alloc");
+    CK(ctx->dNullTmp.ensure((size_t)d.L + 4), "alloc");
+    CK(ctx->dNullTmpOff.ensure(1), "alloc");
+    CK(ctx->dScales.ensure(1), "alloc");
+    CK(cudaMemcpy(ctx->dPairs.p, &d, sizeof d, cudaMemcpyHostToDevice), "upload");
+    CK(cudaMemcpy(ctx->dNullTmpOff.p, &zero, sizeof zero, cudaMemcpyHostToDevice), "upload");
+    NullRates nr;
+    nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
+    nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
+    nullModelKernel<<<1, 32, 0, ctx->stream>>>(ctx->dPairs.p, 1, ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p,
+                                               ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+    CK(cudaGetLastError(), "null-model kernel");
+    CK(cudaStreamSynchronize(ctx->stream), "null-model kernel");
+    std::vector<float> s(2 * (size_t)d.L);
+    PairScales sc;
+    CK(cudaMemcpy(s.data(), ctx->dSeeds.p, s.size() * 4, cudaMemcpyDeviceToHost), "download");
+    CK(cudaMemcpy(&sc, ctx->dScales.p, sizeof sc, cudaMemcpyDeviceToHost), "download");
+    if (prefix_seed) std::memcpy(prefix_seed, s.data(), (size_t)d.L * 4);
+    if (suffix_seed) std::memcpy(suffix_seed, s.data() + d.L, (size_t)d.L * 4);
+    if (scales3) {
+        scales3[0] = sc.s1;
+        scales3[1] = sc.s2;
+        scales3[2] = sc.sC;
+    }
+    return DMST_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Calibration
+// ---------------------------------------------------------------------------
+int dmst_estimate_gumbel(double *scores, int n, double seq_length, double *out8) {
+    if (!scores || !out8 || n < 2) return DMST_EINVAL;
+    estimateGumbel(scores, n, seq_length, out8);
+    return DMST_OK;
+}
+
+int dmst_calibration_sequence(const float *letter_freqs, double bg_stop, double insert1, double insert2,
+                              double delete1, double delete2, int trial, int sequence_length, int border,
+                              char *letters) {
+    if (!letter_freqs || !letters || sequence_length < 1 || border < 0 || trial < 0) return DMST_EINVAL;
+    Rates r{(float)insert1, (float)insert2, (float)delete1, (float)delete2, 0.0f, (float)bg_stop};
+    calibrationSequence(letter_freqs, (float)bg_stop, r, trial, sequence_length, border, letters);
+    return DMST_OK;
+}
+
+int dmst_calibrate(dmst_ctx *ctx, int profile, int sequence_length, int border, int num_sequences, double *out4,
+                   double *scores) {
+    if (!ctx || profile < 0 || profile >= (int)ctx->profiles.size() || sequence_length < 1 || border < 0 ||
+        num_sequences < 2 || !out4)
+        return DMST_EINVAL;
+    if (sequence_length + border < 3) return DMST_EINVAL;
+    const HostProfile &hp = ctx->profiles[profile];
+    // Letter frequencies = the background row the reference reads
+    // (p.values + width * length + 4, dummest.cc:376 -> estimateK).
+    const float *freqs = hp.values.data() + (size_t)kWidth * hp.M + 4;
+    const int Ltot = sequence_length + border;
+    std::vector<char> letters(Ltot);
+    std::vector<uint8_t> codes((size_t)Ltot * num_sequences);
+    std::vector<int64_t> off(num_sequences + 1);
+    for (int t = 0; t < num_sequences; ++t) {
+        calibrationSequence(freqs, ctx->rates.bgStop, ctx->rates, t, sequence_length, border, letters.data());
+        decodeLetters(letters.data(), Ltot, codes.data() + (size_t)t * Ltot);
+        off[t] = (int64_t)t * Ltot;
+    }
+    off[num_sequences] = (int64_t)num_sequences * Ltot;
+    // Keep the caller's sequences: append, score, then drop ours.
+    const size_t keepSeqs = ctx->seqLen.size();
+    const long long keepBytes = ctx->codeBytes;
+    int first = 0;
+    int st = dmst_seqs_add_decoded(ctx, codes.data(), off.data(), num_sequences, &first);
+    if (st) return st;
+    std::vector<dmst_pair> pairs(num_sequences);
+    for (int t = 0; t < num_sequences; ++t) pairs[t] = dmst_pair{first + t, profile, -2.0f};
+    std::vector<dmst_result> res(num_sequences);
+    st = dmst_score_pairs(ctx, pairs.data(), pairs.size(), DMST_MODE_MID, res.data());
+    ctx->seqLen.resize(keepSeqs);
+    ctx->seqOff.resize(keepSeqs);
+    ctx->codeBytes = keepBytes;
+    if (st) return st;
+    std::vector<double> mids(num_sequences), flts(num_sequences);
+    for (int t = 0; t < num_sequences; ++t) {
+        mids[t] = res[t].mid_ln;
+        flts[t] = res[t].filter_ln;
+    }
+    if (scores) {
+        std::copy(mids.begin(), mids.end(), scores);
+        std::copy(flts.begin(), flts.end(), scores + num_sequences);
+    }
+    double g[8];
+    estimateGumbel(mids.data(), num_sequences, sequence_length, g);
+    out4[0] = g[0];
+    out4[1] = g[1];
+    estimateGumbel(flts.data(), num_sequences, sequence_length, g);
+    out4[2] = g[0];
+    out4[3] = g[1];
+    return DMST_OK;
+}
+
+}  // extern "C"

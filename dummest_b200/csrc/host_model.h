@@ -1,0 +1,60 @@
+// Host-side model types and preparation routines (see host_model.cpp).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace dmst {
+
+constexpr int kNonLetterWidth = 9;  // dummest-core.hh:231
+constexpr int kWidth = 29;          // 20 letters + 9 (protein profiles)
+constexpr int kCodes = 25;          // codon codes 0..24; 24 is the zero pad (dummest-dp.hh:93)
+constexpr int kPadCode = 24;
+constexpr int kMaskCode = 22;       // '?' masked / ambiguous triplet
+extern const char kAlphabet[];
+
+// FP32 engine rates (dummest-core.hh:115-124); Float = float.
+struct Rates {
+    float insert1, insert2, delete1, delete2;
+    float stop, bgStop;
+};
+
+// Reference Params (dummest-core.hh:233-239).
+struct Params {
+    float alpha[3];
+    float beta[3];
+    float delta[3];
+    float epsilon;
+    float enter;
+};
+static_assert(sizeof(Params) == 11 * sizeof(float), "Params must be 11 floats");
+
+struct RawProfile {
+    std::string name;
+    int M = 0;
+    int width = 0;
+    std::vector<float> values;  // (M+1) * width, the reader's layout
+};
+
+struct FinalProfile {
+    std::string name;
+    int M = 0;
+    int width = 0;
+    std::vector<float> values;  // (M+1) * width after finalize
+    std::vector<Params> params; // M + 2
+    std::vector<float> bg;      // width
+};
+
+int codonCount(char aa);
+void standardCodeTable(uint8_t out[64]);
+int parseHmmText(const char *text, size_t len, std::vector<RawProfile> &out, std::string *err);
+int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err);
+int encodeDna(const char *ascii, int L, char *letters);
+int decodeLetters(const char *letters, int L, uint8_t *codes);
+int calibrationSequence(const float *letterFreqs, float bgStop, const Rates &r, int trial, int seqLen, int border,
+                        char *out);
+void estimateGumbel(double *scores, int n, double len, double out[8]);
+
+}  // namespace dmst

@@ -1,0 +1,229 @@
+// Per-pair null model on the device: the codon/frameshift background prefix
+// and suffix probabilities, the whole-sequence null total, the per-base
+// scales and the seed vectors that the DP consumes.
+//
+// Restates, for one sequence (single-lane semantics), the reference's
+//   buildNullSuffix            dummest-dp-backward.hh:6-55
+//   buildNullPrefixFirstCodon  dummest-dp-backward.hh:58-100
+//   buildNullTotalAndScales    dummest-dp-backward.hh:103-129
+//   buildNullSeedModels        dummest-dp-backward.hh:133-165
+// with the exact score algebra of dummest-score.hh / dummest-batch.hh: each
+// step rounds a double to a float mantissa exactly where the reference does,
+// so the seeds are bit-identical to the reference's (up to the last-ulp
+// behaviour of log2/exp2 in double, which feeds one float rounding).
+// A sequence's per-lane result in the reference does not depend on the batch
+// it was scored in (lanes past their length are forced to 0 or 1), so the
+// single-sequence form is the reference's result for that lane.
+#pragma once
+
+#include "dp_common.cuh"
+
+namespace dmst {
+
+struct XS {  // ExpScore (dummest-score.hh:28-33)
+    float m;
+    int e;
+};
+
+__device__ __forceinline__ XS xsZero() { return XS{0.0f, 0}; }
+__device__ __forceinline__ XS pow2Score(int e2) { return XS{0.5f, e2 + 1}; }  // dummest-score.hh:197-199
+
+// splitNormalizedDouble (dummest-batch.hh:42-53); also normalizeScore's frexp
+// for every non-subnormal double (products here never reach double
+// subnormals).
+__device__ __forceinline__ XS splitNorm(double x, int eAdd) {
+    if (x == 0.0) return xsZero();
+    unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    int ef = (int)((u >> 52) & 0x7FFULL);
+    if (ef == 0x7FF) return XS{__double2float_rn(x), eAdd};
+    if (ef == 0) return xsZero();
+    double m = __longlong_as_double((long long)((u & 0xFFFFFFFFFFFFFULL) | (1022ULL << 52)));
+    return XS{__double2float_rn(m), eAdd + ef - 1022};
+}
+
+// scaleScore / batchScaleScores (dummest-score.hh:155-160, dummest-batch.hh:114-130).
+__device__ __forceinline__ XS scaleScore(XS a, double f) {
+    if (a.m == 0.0f) return xsZero();
+    if (!(f > 0.0) || !isfinite(f)) return xsZero();
+    return splitNorm(__dmul_rn((double)a.m, f), a.e);
+}
+
+// batchAddScores (dummest-batch.hh:78-108).
+__device__ __forceinline__ XS batchAdd(XS a, XS b) {
+    if (a.m == 0.0f) return b;
+    if (b.m == 0.0f) return a;
+    const bool agebe = a.e >= b.e;
+    const float mh = agebe ? a.m : b.m, ml = agebe ? b.m : a.m;
+    const int eh = agebe ? a.e : b.e, el = agebe ? b.e : a.e;
+    int d = eh - el;
+    d = d > 60 ? 60 : d;
+    // ml * 2^-d is exact, so an fma here rounds exactly like mul-then-add.
+    double s = __dadd_rn((double)mh, __dmul_rn((double)ml, 1.0 / (double)(1ULL << (unsigned)d)));
+    int e = eh;
+    if (s >= 1.0) {
+        s *= 0.5;
+        e += 1;
+    }
+    return XS{__double2float_rn(s), e};
+}
+
+// addScores, the scalar form (dummest-score.hh:169-181).
+__device__ __forceinline__ XS scalarAdd(XS a, XS b) {
+    if (a.m == 0.0f) return b;
+    if (b.m == 0.0f) return a;
+    if (a.e >= b.e) {
+        int d = a.e - b.e;
+        if (d > 60) return a;
+        return splitNorm(__dadd_rn((double)a.m, ldexp((double)b.m, -d)), a.e);
+    }
+    int d = b.e - a.e;
+    if (d > 60) return b;
+    return splitNorm(__dadd_rn((double)b.m, ldexp((double)a.m, -d)), b.e);
+}
+
+// batchMulScores with eFold = 0 (dummest-batch.hh:58-72).
+__device__ __forceinline__ XS batchMul(XS a, XS b) {
+    if (a.m == 0.0f || b.m == 0.0f) return xsZero();
+    double p = __dmul_rn((double)a.m, (double)b.m);
+    int e = a.e + b.e;
+    if (p < 0.5) {
+        p *= 2.0;
+        e -= 1;
+    }
+    return XS{__double2float_rn(p), e};
+}
+
+// mulScores, the scalar form (dummest-score.hh:184-188).
+__device__ __forceinline__ XS scalarMul(XS a, XS b) {
+    if (a.m == 0.0f || b.m == 0.0f) return xsZero();
+    return splitNorm(__dmul_rn((double)a.m, (double)b.m), a.e + b.e);
+}
+
+// scoreToFloatClamped (dummest-score.hh:224-230), FP32 engine: exponent capped at 120.
+__device__ __forceinline__ float packScore(XS a) {
+    if (a.m == 0.0f) return 0.0f;
+    int e = a.e > 120 ? 120 : a.e;
+    return ldexpf(a.m, e);
+}
+
+struct NullRates {
+    double single;      // BACKGROUND_FRAMESHIFT_RATE (a float value)
+    double dbl;         // BACKGROUND_FRAMESHIFT_RATE_2 (a float value)
+};
+
+__device__ __forceinline__ float bgAt(const float *bg, const uint8_t *codes, int L, int j) {
+    return (j >= 0 && j < L) ? bg[codes[j]] : 0.0f;  // beyond the sequence: zero_idx, bg 0
+}
+
+// Prefix recurrence (dummest-dp-backward.hh:66-99) step i, given the three
+// previous prefix values.
+__device__ __forceinline__ XS prefixStep(int i, const float *bg, const uint8_t *codes, int L, XS p1, XS p2, XS p3,
+                                         double keep, double sNE, double dNE) {
+    const float bgc = bgAt(bg, codes, L, i - 2);
+    const double codonScale = __dmul_rn((double)bgc, keep);
+    const double frame = 1.0 / 3.0;
+    XS codon;
+    if (i >= 3)
+        codon = scaleScore(p3, codonScale);
+    else if (i == 2)
+        codon = scaleScore(splitNorm((double)bgc, 0), frame);
+    else if (i == 1)
+        codon = scaleScore(pow2Score(-4), frame);
+    else
+        codon = scaleScore(pow2Score(-2), frame);
+    XS single = scaleScore(i > 0 ? p1 : xsZero(), sNE);
+    XS dbl = scaleScore(i >= 2 ? p2 : xsZero(), dNE);
+    return batchAdd(codon, batchAdd(single, dbl));
+}
+
+// One thread per pair.  Outputs prefixSeed[0..L) and suffixSeedFromNext[0..L)
+// at seeds + seedOff, the three scales, and uses tmp (L+4 ExpScores per pair)
+// for the suffix probabilities.
+__device__ void nullModelPair(const uint8_t *codes, int L, const float *bg, NullRates r, float *prefixSeed,
+                              float *suffixSeed, XS *suffix, PairScales *scalesOut) {
+    const double keep = 1.0 - r.single - r.dbl;   // codonKeepProbability
+    const double sNE = r.single * 0.25;           // singleNucleotideEmission
+    const double dNE = r.dbl * 0.0625;            // doubleNucleotideEmission
+
+    // Pass 1: prefix probabilities; keep the last three for the total.
+    XS p1 = xsZero(), p2 = xsZero(), p3 = xsZero();
+    for (int i = 0; i < L; ++i) {
+        XS p = prefixStep(i, bg, codes, L, p1, p2, p3, keep, sNE, dNE);
+        p3 = p2;
+        p2 = p1;
+        p1 = p;
+    }
+    // Total and scales (dummest-dp-backward.hh:103-129); p1 = prefix[L-1],
+    // p2 = prefix[L-2], p3 = prefix[L-3].
+    const double keepSingle = 1.0 - r.single;
+    const double keepBoth = keepSingle - r.dbl;
+    XS trailingSingle = scaleScore(p2, keepSingle * 0.25);
+    XS trailingDouble = scaleScore(p3, keepBoth * 0.0625);
+    XS total = scalarAdd(scalarAdd(p1, trailingSingle), trailingDouble);
+    const float nullLog = (total.m == 0.0f) ? -INFINITY : (float)(log2((double)total.m) + (double)total.e);
+    double perBaseLog = -(double)nullLog / (double)L;
+    if (!(perBaseLog < 120.0)) perBaseLog = 120.0;
+    const double perBaseRaw = exp2(perBaseLog);
+    const XS perBase = splitNorm(perBaseRaw, 0);
+    const XS perBaseInv = splitNorm(1.0 / perBaseRaw, 0);
+    const XS quarter = splitNorm(0.25, 0), sixteenth = splitNorm(0.0625, 0);
+    const XS s1 = scalarMul(perBase, quarter);
+    const XS s2 = scalarMul(scalarMul(perBase, perBase), sixteenth);
+    const XS sC = scalarMul(scalarMul(perBase, perBase), perBase);
+    scalesOut->s1 = packScore(s1);
+    scalesOut->s2 = packScore(s2);
+    scalesOut->sC = packScore(sC);
+    scalesOut->pad = 0.0f;
+
+    // Pass 2: suffix probabilities (dummest-dp-backward.hh:6-55), j = L-1..0,
+    // suffix[L] = 1, suffix[L+1..L+3] = 0.
+    {
+        const XS trailing = splitNorm(0.5 * keep, 0);
+        suffix[L] = pow2Score(0);
+        suffix[L + 1] = xsZero();
+        suffix[L + 2] = xsZero();
+        suffix[L + 3] = xsZero();
+        for (int i = L - 1; i >= 0; --i) {
+            const double codonScale = __dmul_rn((double)bgAt(bg, codes, L, i), keep);
+            XS single = scaleScore(suffix[i + 1], sNE);
+            XS dIn = (i + 1 < L) ? suffix[i + 2] : pow2Score(2);
+            XS dbl = scaleScore(dIn, dNE);
+            XS codon = (i + 2 < L) ? scaleScore(suffix[i + 3], codonScale)
+                                   : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
+            suffix[i] = batchAdd(codon, batchAdd(single, dbl));
+        }
+    }
+
+    // Pass 3: suffix seeds (dummest-dp-backward.hh:137-154).
+    XS running = pow2Score(0);
+    for (int t = 0; t < L - 1; ++t) running = batchMul(running, perBase);
+    for (int j = 0; j < L; ++j) {
+        suffixSeed[j] = packScore(batchMul(suffix[j + 1], running));
+        running = batchMul(running, perBaseInv);
+    }
+
+    // Pass 4: prefix seeds (dummest-dp-backward.hh:155-164), recomputing the
+    // prefix recurrence.
+    running = perBase;
+    p1 = p2 = p3 = xsZero();
+    for (int i = 0; i < L; ++i) {
+        XS p = prefixStep(i, bg, codes, L, p1, p2, p3, keep, sNE, dNE);
+        p3 = p2;
+        p2 = p1;
+        p1 = p;
+        prefixSeed[i] = packScore(batchMul(p, running));
+        running = batchMul(running, perBase);
+    }
+}
+
+__global__ void nullModelKernel(const DevPair *pairs, int n, const DevProfile *profiles, const uint8_t *codes,
+                                float *seeds, XS *tmp, const long long *tmpOff, PairScales *scales, NullRates r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DevPair p = pairs[i];
+    const float *bg = profiles[p.prof].bg;
+    float *pre = seeds + p.seedOff;
+    nullModelPair(codes + p.codeOff, p.L, bg, r, pre, pre + p.L, tmp + tmpOff[i], &scales[i]);
+}
+
+}  // namespace dmst

@@ -1,0 +1,351 @@
+"""Host-side mirror of the reference's hot-path interface, over the C ABI.
+
+Names and argument meaning follow the reference engine:
+
+  find_similarities(profile, decoded, min_prob_ratio=-2, need_align=False)
+      dummest-search.hh:9-17 as the calibration calls it (needAlign=false):
+      backward then forward; per sequence the mid-anchored score (ExpScore and
+      its natural log, dummest-dp-forward.hh:536-544) and the exact filter
+      best (the bestOut of dummest-dp-backward.hh:579-609).
+  find_similarities_backward_only(profile, decoded)
+      dummest-dp-backward.hh:300-438, the lean float filter.
+  estimate_k(profile, sequence_length, border, trials)
+      dummest-calibration.hh:338-649 without the cache: random sequences,
+      mid and filter scores, method-of-moments Gumbel lambda and K.
+
+Errors: the reference asserts on L < 3 (dummest-dp.hh:84) and on empty
+batches (dummest-dp-backward.hh:195); here they raise ValueError.  Device and
+allocation failures raise RuntimeError with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _ffi as F
+
+
+class DmstError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+@dataclass
+class Score:
+    """ExpScore: value = m * 2**e (dummest-score.hh:28-33)."""
+    m: float
+    e: int
+
+    @property
+    def ln(self) -> float:
+        return -math.inf if self.m == 0 else math.log(self.m) + self.e * 0.6931471805599453
+
+    @property
+    def bits(self) -> float:
+        return self.ln / 0.6931471805599453
+
+
+@dataclass
+class Similarity:
+    mid: Score
+    mid_ln: float
+    filter: Score
+    filter_ln: float
+    filter_f: float
+    exact_path: bool
+
+
+def default_opts() -> F.Opts:
+    lib = F.load()
+    o = F.Opts()
+    lib.dmst_opts_default(C.byref(o))
+    return o
+
+
+class Context:
+    """One device context (one per host thread)."""
+
+    def __init__(self, device: int = 0, rates: dict | None = None, rows_per_lane: int = 0):
+        self.lib = F.load()
+        o = default_opts()
+        o.device = device
+        o.rows_per_lane = rows_per_lane
+        for k, v in (rates or {}).items():
+            setattr(o, k, float(v))
+        self.opts = o
+        h = C.c_void_p()
+        st = self.lib.dmst_ctx_create(C.byref(o), C.byref(h))
+        if st != F.DMST_OK:
+            raise DmstError(st, "dmst_ctx_create: " + self.lib.dmst_strerror(st).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dmst_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != F.DMST_OK:
+            msg = self.lib.dmst_last_error(self.h).decode() or self.lib.dmst_strerror(st).decode()
+            if st == F.DMST_EINVAL:
+                raise ValueError(f"{what}: {msg}")
+            raise DmstError(st, f"{what}: {msg}")
+
+    # ---- profiles -------------------------------------------------------
+    def add_profile(self, values: np.ndarray, params: np.ndarray, bg: np.ndarray) -> int:
+        """values: (M+1, 29) float32; params: (M+2, 11) float32; bg: (29,) float32."""
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        bg = np.ascontiguousarray(bg, dtype=np.float32)
+        M = values.shape[0] - 1
+        if values.shape[1] != 29 or params.shape != (M + 2, 11) or bg.shape != (29,):
+            raise ValueError("profile arrays have the wrong shape")
+        pid = C.c_int()
+        st = self.lib.dmst_profile_add(self.h, values.ctypes.data_as(C.POINTER(C.c_float)), 29, M,
+                                       params.ctypes.data_as(C.POINTER(F.Params)),
+                                       bg.ctypes.data_as(C.POINTER(C.c_float)), C.byref(pid))
+        self._check(st, "dmst_profile_add")
+        return pid.value
+
+    def load_hmm(self, text: str | bytes, background_type: str = "G") -> list[int]:
+        b = text.encode() if isinstance(text, str) else text
+        first, count = C.c_int(), C.c_int()
+        st = self.lib.dmst_profile_load_hmm(self.h, b, len(b), ord(background_type), C.byref(first),
+                                            C.byref(count))
+        self._check(st, "dmst_profile_load_hmm")
+        return list(range(first.value, first.value + count.value))
+
+    def profile_length(self, pid: int) -> int:
+        return self.lib.dmst_profile_length(self.h, pid)
+
+    # ---- sequences ------------------------------------------------------
+    @staticmethod
+    def _offsets(lengths: Sequence[int]) -> np.ndarray:
+        off = np.zeros(len(lengths) + 1, dtype=np.int64)
+        np.cumsum(np.asarray(lengths, dtype=np.int64), out=off[1:])
+        return off
+
+    def add_decoded(self, seqs: Sequence[np.ndarray]) -> list[int]:
+        """Sequences given as codon codes (decodeSequence output)."""
+        if len(seqs) == 0:
+            return []
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.uint8) for s in seqs]))
+        off = self._offsets([len(s) for s in seqs])
+        first = C.c_int()
+        st = self.lib.dmst_seqs_add_decoded(self.h, flat.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                            off.ctypes.data_as(C.POINTER(C.c_int64)), len(seqs), C.byref(first))
+        self._check(st, "dmst_seqs_add_decoded")
+        return list(range(first.value, first.value + len(seqs)))
+
+    def add_dna(self, seqs: Sequence[str | bytes]) -> list[int]:
+        if len(seqs) == 0:
+            return []
+        bs = [s.encode() if isinstance(s, str) else bytes(s) for s in seqs]
+        flat = b"".join(bs)
+        off = self._offsets([len(s) for s in bs])
+        first = C.c_int()
+        st = self.lib.dmst_seqs_add_dna(self.h, flat, off.ctypes.data_as(C.POINTER(C.c_int64)), len(bs),
+                                        C.byref(first))
+        self._check(st, "dmst_seqs_add_dna")
+        return list(range(first.value, first.value + len(bs)))
+
+    def add_packed(self, words: np.ndarray, lengths: Sequence[int], mask: np.ndarray | None = None) -> list[int]:
+        """2-bit packed DNA (pack_dna output) with per-sequence lengths."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        off = self._offsets(lengths)
+        first = C.c_int()
+        mp = None
+        if mask is not None:
+            mask = np.ascontiguousarray(mask, dtype=np.uint32)
+            mp = mask.ctypes.data_as(C.POINTER(C.c_uint32))
+        st = self.lib.dmst_seqs_add_packed(self.h, words.ctypes.data_as(C.POINTER(C.c_uint32)), mp,
+                                           off.ctypes.data_as(C.POINTER(C.c_int64)), len(lengths), C.byref(first))
+        self._check(st, "dmst_seqs_add_packed")
+        return list(range(first.value, first.value + len(lengths)))
+
+    def clear_sequences(self):
+        self._check(self.lib.dmst_seqs_clear(self.h), "dmst_seqs_clear")
+
+    # ---- scoring --------------------------------------------------------
+    def score_pairs(self, seq_ids: Sequence[int], profile_ids: Sequence[int] | int, mode: int = F.MODE_MID,
+                    min_prob_ratio: float = -2.0) -> list[Similarity]:
+        n = len(seq_ids)
+        if isinstance(profile_ids, int):
+            profile_ids = [profile_ids] * n
+        pairs = (F.Pair * n)()
+        for k, (s, p) in enumerate(zip(seq_ids, profile_ids)):
+            pairs[k].seq = s
+            pairs[k].profile = p
+            pairs[k].min_prob_ratio = min_prob_ratio
+        res = (F.Result * n)()
+        st = self.lib.dmst_score_pairs(self.h, pairs, n, mode, res)
+        self._check(st, "dmst_score_pairs")
+        out = []
+        for r in res:
+            out.append(Similarity(Score(r.mid.m, r.mid.e), r.mid_ln, Score(r.filter.m, r.filter.e), r.filter_ln,
+                                  r.filter_f, bool(r.flags & F.RES_EXACT_PATH)))
+        return out
+
+    def score_pairs_raw(self, pairs, mode: int) -> "C.Array":
+        """Score a ctypes Pair array; returns the ctypes Result array (no Python objects per pair)."""
+        n = len(pairs)
+        res = (F.Result * n)()
+        st = self.lib.dmst_score_pairs(self.h, pairs, n, mode, res)
+        self._check(st, "dmst_score_pairs")
+        return res
+
+    def last_timing(self) -> dict:
+        t, d, nm, la = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        self.lib.dmst_last_timing(self.h, C.byref(t), C.byref(d), C.byref(nm), C.byref(la))
+        return {"total_ms": t.value, "dp_ms": d.value, "null_ms": nm.value, "launches": la.value}
+
+    def find_similarities(self, profile: int, decoded: Sequence[np.ndarray]) -> list[Similarity]:
+        if len(decoded) == 0:
+            raise ValueError("empty batch (the reference asserts activeCount > 0)")
+        ids = self.add_decoded(decoded)
+        return self.score_pairs(ids, profile, F.MODE_MID)
+
+    def find_similarities_backward_only(self, profile: int, decoded: Sequence[np.ndarray]) -> list[float]:
+        if len(decoded) == 0:
+            raise ValueError("empty batch (the reference asserts activeCount > 0)")
+        ids = self.add_decoded(decoded)
+        return [r.filter_f for r in self.score_pairs(ids, profile, F.MODE_FILTER)]
+
+    def null_model(self, seq: int, profile: int, L: int):
+        pre = np.zeros(L, np.float32)
+        suf = np.zeros(L, np.float32)
+        sc = np.zeros(3, np.float32)
+        st = self.lib.dmst_null_model(self.h, seq, profile, pre.ctypes.data_as(C.POINTER(C.c_float)),
+                                      suf.ctypes.data_as(C.POINTER(C.c_float)),
+                                      sc.ctypes.data_as(C.POINTER(C.c_float)))
+        self._check(st, "dmst_null_model")
+        return pre, suf, sc
+
+    def estimate_k(self, profile: int, sequence_length: int = 5000, border: int = 100, trials: int = 1000,
+                   return_scores: bool = False):
+        out = (C.c_double * 4)()
+        scores = (C.c_double * (2 * trials))()
+        st = self.lib.dmst_calibrate(self.h, profile, sequence_length, border, trials, out, scores)
+        self._check(st, "dmst_calibrate")
+        fit = {"lambda": out[0], "K": out[1], "lambda_filter": out[2], "K_filter": out[3]}
+        if return_scores:
+            s = np.frombuffer(scores, dtype=np.float64).copy()
+            return fit, s[:trials], s[trials:]
+        return fit
+
+
+# ---- host helpers without a context ---------------------------------------
+def decode_letters(letters: np.ndarray) -> np.ndarray:
+    lib = F.load()
+    letters = np.ascontiguousarray(letters, dtype=np.int8)
+    out = np.zeros(len(letters), np.uint8)
+    st = lib.dmst_decode_letters(letters.ctypes.data_as(C.c_char_p), len(letters),
+                                 out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    if st != F.DMST_OK:
+        raise ValueError("dmst_decode_letters failed")
+    return out
+
+
+def encode_dna(ascii: str | bytes) -> np.ndarray:
+    lib = F.load()
+    b = ascii.encode() if isinstance(ascii, str) else bytes(ascii)
+    out = C.create_string_buffer(len(b))
+    st = lib.dmst_encode_dna(b, len(b), out)
+    if st != F.DMST_OK:
+        raise ValueError("dmst_encode_dna: not DNA")
+    return np.frombuffer(out.raw, dtype=np.int8).copy()
+
+
+def decode_dna(ascii: str | bytes) -> np.ndarray:
+    return decode_letters(encode_dna(ascii))
+
+
+def finalize_hmm(text: str | bytes, index: int = 0, background_type: str = "G", rates: dict | None = None):
+    """(name, values (M+1,29), params (M+2,11), bg (29,)) of profile `index`."""
+    lib = F.load()
+    b = text.encode() if isinstance(text, str) else text
+    o = default_opts()
+    for k, v in (rates or {}).items():
+        setattr(o, k, float(v))
+    M = C.c_int()
+    st = lib.dmst_hmm_finalize(b, len(b), index, ord(background_type), C.byref(o), C.byref(M), None, None, None,
+                               None, 0)
+    if st != F.DMST_OK:
+        raise ValueError(f"dmst_hmm_finalize: status {st}")
+    M = M.value
+    values = np.zeros((M + 1, 29), np.float32)
+    params = np.zeros((M + 2, 11), np.float32)
+    bg = np.zeros(29, np.float32)
+    name = C.create_string_buffer(256)
+    st = lib.dmst_hmm_finalize(b, len(b), index, ord(background_type), C.byref(o), C.byref(C.c_int()),
+                               values.ctypes.data_as(C.POINTER(C.c_float)),
+                               params.ctypes.data_as(C.POINTER(F.Params)), bg.ctypes.data_as(C.POINTER(C.c_float)),
+                               name, 256)
+    if st != F.DMST_OK:
+        raise ValueError(f"dmst_hmm_finalize: status {st}")
+    return name.value.decode(), values, params, bg
+
+
+def estimate_gumbel(scores: np.ndarray, seq_length: float) -> np.ndarray:
+    lib = F.load()
+    s = np.ascontiguousarray(scores, dtype=np.float64).copy()
+    out = (C.c_double * 8)()
+    st = lib.dmst_estimate_gumbel(s.ctypes.data_as(C.POINTER(C.c_double)), len(s), seq_length, out)
+    if st != F.DMST_OK:
+        raise ValueError("dmst_estimate_gumbel failed")
+    return np.array(out[:])
+
+
+def calibration_sequence(letter_freqs: np.ndarray, trial: int, sequence_length: int, border: int,
+                         rates: dict | None = None) -> np.ndarray:
+    lib = F.load()
+    o = default_opts()
+    for k, v in (rates or {}).items():
+        setattr(o, k, float(v))
+    lf = np.ascontiguousarray(letter_freqs, dtype=np.float32)
+    out = C.create_string_buffer(sequence_length + border)
+    st = lib.dmst_calibration_sequence(lf.ctypes.data_as(C.POINTER(C.c_float)), o.bg_stop_codon_prob, o.insert1,
+                                       o.insert2, o.delete1, o.delete2, trial, sequence_length, border, out)
+    if st != F.DMST_OK:
+        raise ValueError("dmst_calibration_sequence failed")
+    return np.frombuffer(out.raw, dtype=np.int8).copy()
+
+
+def pack_dna(seqs: Sequence[str | bytes]) -> tuple[np.ndarray, np.ndarray, list[int]]:
+    """2-bit pack DNA: A=0 C=1 G=2 T=3, 16 bases per uint32 word, each sequence
+    starting on a fresh word; other letters set the masked-base bitmap."""
+    lut = np.full(256, 255, np.uint8)
+    for ch, v in zip(b"ACGTacgt", (0, 1, 2, 3, 0, 1, 2, 3)):
+        lut[ch] = v
+    words, masks, lens = [], [], []
+    for s in seqs:
+        b = np.frombuffer(s.encode() if isinstance(s, str) else bytes(s), dtype=np.uint8)
+        v = lut[b]
+        m = v == 255
+        v = np.where(m, 0, v).astype(np.uint32)
+        L = len(v)
+        nw = (L + 15) // 16
+        vv = np.zeros(nw * 16, np.uint32)
+        vv[:L] = v
+        w = (vv.reshape(nw, 16) << (2 * np.arange(16, dtype=np.uint32))).sum(axis=1, dtype=np.uint64)
+        words.append(w.astype(np.uint32))
+        nm = (L + 31) // 32
+        mm = np.zeros(nm * 32, np.uint64)
+        mm[:L] = m
+        masks.append((mm.reshape(nm, 32) << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32))
+        lens.append(L)
+    return np.concatenate(words), np.concatenate(masks), lens

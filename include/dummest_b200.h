@@ -1,0 +1,209 @@
+/*
+ * dummest_b200.h -- C ABI of the B200 (sm_100a) implementation of DUMMEST's
+ * search hot path: the frameshift-aware DNA x protein-profile Forward/Backward
+ * dynamic program, its mid-anchored score, the lean backward-only filter, and
+ * the random-sequence scoring behind Gumbel E-value calibration.
+ *
+ * Plain C types only.  Every call returns a status (0 or a negative DMST_E*
+ * code); nothing aborts and no exception crosses the ABI.  One context per
+ * host thread (contexts are not internally locked).  All host buffers are
+ * caller-owned; device memory is owned by the context.
+ *
+ * Reference interfaces this ABI replaces (paths relative to the reference
+ * repository root):
+ *   Params / Profile            dummest-core.hh:233-254
+ *   ExpScore                    dummest-score.hh:28-33
+ *   readProfiles/finalizeProfile dummest-profile.hh:235-329, :105-233
+ *   decodeSequence              dummest-sequence.hh:181-204
+ *   findSimilarities            dummest-search.hh:9-17   (needAlign=false)
+ *   findSimilaritiesBackwardOnly dummest-dp-backward.hh:300-438
+ *   backwardPass bestOut        dummest-dp-backward.hh:579-609
+ *   estimateK / estimateGumbel  dummest-calibration.hh:338-649, :97-104
+ *   rate globals                dummest-core.hh:115-131
+ */
+#ifndef DUMMEST_B200_H
+#define DUMMEST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define DMST_OK 0
+#define DMST_EINVAL (-1)   /* bad argument (null pointer, L < 3, unknown id, ...) */
+#define DMST_ENOMEM (-2)   /* host or device allocation failed */
+#define DMST_EDEVICE (-3)  /* CUDA error, or no usable sm_100 device */
+#define DMST_ETIMEOUT (-4) /* a kernel exceeded its iteration budget */
+#define DMST_EPARSE (-5)   /* malformed HMMER3 / sequence text */
+#define DMST_ERANGE (-6)   /* size beyond a documented limit */
+
+/* ---- score modes for dmst_score_pairs --------------------------------- */
+/* Backward then forward; mid-anchored score and the exact filter best.  The
+ * GPU counterpart of findSimilarities(needAlign=false) as estimateK calls it
+ * (dummest-calibration.hh:489-505, dummest-dp-forward.hh:536-544). */
+#define DMST_MODE_MID 0
+/* The lean float backward-only filter (findSimilaritiesBackwardOnly): plain
+ * float W1 with no row rescaling, score = max W1[i][j]*prefixSeed[j], which
+ * may be +inf ("inf always survives", dummest-search.hh:163-168). */
+#define DMST_MODE_FILTER 1
+/* Flag for either mode: run the plain schedule, one pair per kernel launch
+ * (same per-pair code), the baseline the batched persistent kernel is
+ * measured against. */
+#define DMST_MODE_PLAIN 0x100
+/* Flag: route every pair through the exact row-rescaled path (for tests). */
+#define DMST_MODE_FORCE_EXACT 0x200
+
+/* ---- per-result flags -------------------------------------------------- */
+#define DMST_RES_EXACT_PATH 1 /* pair was scored by the exact row-rescaled kernel */
+
+/* Reference Params (dummest-core.hh:233-239), FP32 engine layout. */
+typedef struct dmst_params {
+    float alpha_prime[3];
+    float beta_prime[3];
+    float delta_prime[3];
+    float epsilon_prime;
+    float enter_match_probability;
+} dmst_params;
+
+/* Reference ExpScore (dummest-score.hh:28-33): value = m * 2^e, m in [0.5,1)
+ * (the float rounding of a [0.5,1) double may give exactly 1.0, as in the
+ * reference), m == 0 for zero. */
+typedef struct dmst_score {
+    float m;
+    int32_t e;
+} dmst_score;
+
+/* Rates and limits (dummest-core.hh:60-80, :115-131). */
+typedef struct dmst_opts {
+    double insert1, insert2, delete1, delete2; /* frameshift rates per base */
+    double stop_codon_prob;                    /* STOP_CODON_PROB */
+    double bg_stop_codon_prob;                 /* BG_STOP_CODON_PROB */
+    int device;                                /* CUDA device ordinal */
+    int rows_per_lane;                         /* 0 = autotuned, else 1, 2 or 4 */
+    size_t device_budget_bytes;                /* 0 = 60% of free device memory */
+} dmst_opts;
+
+/* One (sequence, profile) pair; min_prob_ratio < 0 means "report" as in the
+ * calibration call (minProbRatio = -2, dummest-calibration.hh:490). */
+typedef struct dmst_pair {
+    int32_t seq;
+    int32_t profile;
+    float min_prob_ratio;
+} dmst_pair;
+
+typedef struct dmst_result {
+    dmst_score mid;    /* max_{i,j} W0*W1 (exact pair)                        */
+    dmst_score filter; /* max_{i,j} W1*prefixSeed (exact pair, MODE_MID)     */
+    double mid_ln;     /* ln(mid) = scoreToLog(mid); -inf for zero            */
+    double filter_ln;  /* ln(filter) (MODE_MID) or ln of the float filter     */
+    float filter_f;    /* MODE_FILTER: the float filter score as the reference returns it */
+    int32_t flags;     /* DMST_RES_*                                          */
+} dmst_result;
+
+typedef struct dmst_ctx dmst_ctx;
+
+/* Default options: the reference's compile-time defaults. */
+void dmst_opts_default(dmst_opts *opts);
+
+int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out);
+void dmst_ctx_destroy(dmst_ctx *ctx);
+const char *dmst_strerror(int status);
+/* Text of the last error on this context ("" if none). */
+const char *dmst_last_error(const dmst_ctx *ctx);
+
+/* ---- profiles ----------------------------------------------------------
+ * dmst_profile_add takes an already-finalized profile exactly as the
+ * reference holds it: values is (M+1) x width floats (row i = transitions of
+ * node i followed by the match emissions of node i+1, width = 29 for protein,
+ * dummest-profile.hh:264-313), params is M+2 Params, bg is width floats
+ * (bg_probs, dummest-profile.hh:135-148).  Replaces: Profile construction. */
+int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const dmst_params *params,
+                     const float *bg, int *id);
+
+/* Parse HMMER3 text and finalize each profile with the reference's semantics
+ * (readProfiles + finalizeProfile without tantan masking or filtering;
+ * background type 'G', 'A' or 'M').  Replaces: readProfiles
+ * (dummest-profile.hh:235-329).  first_id/count receive the new ids. */
+int dmst_profile_load_hmm(dmst_ctx *ctx, const char *text, size_t len, int background_type, int *first_id,
+                          int *count);
+
+/* Host-side finalize without a context (for tests and tools): fills values
+ * ((M+1)*29), params (M+2) and bg (29) of profile number `index` in the text.
+ * Returns its M via *M.  Call with values == NULL first to learn M. */
+int dmst_hmm_finalize(const char *text, size_t len, int index, int background_type, const dmst_opts *opts,
+                      int *M, float *values, dmst_params *params, float *bg, char *name, size_t name_cap);
+
+int dmst_profile_count(const dmst_ctx *ctx);
+int dmst_profile_length(const dmst_ctx *ctx, int id);
+
+/* ---- sequences ----------------------------------------------------------
+ * Sequences are kept on the device as per-base codon codes (0..24, the
+ * output of decodeSequence, dummest-sequence.hh:181-204).
+ *   _decoded: codes given by the caller.
+ *   _dna:     ASCII DNA (ACGT any case; IUPAC ambiguity and other letters of
+ *             RYSWKMBDHVN map to the masked code), decoded on the device.
+ *   _packed:  2-bit packed DNA (A=0 C=1 G=2 T=3, base k of a sequence at bits
+ *             2*(k%16) of 32-bit word k/16 counted from that sequence's first
+ *             word), plus an optional bitmap of masked bases (bit k%32 of
+ *             word k/32; NULL = none); decoded on the device.
+ * offsets has nseq+1 entries (base offsets; packed: word offsets follow from
+ * the base offsets rounded up to 16 per sequence).  Every sequence needs
+ * L >= 3 (dummest-dp.hh:84).  first_id receives the id of the first one. */
+int dmst_seqs_add_decoded(dmst_ctx *ctx, const uint8_t *codes, const int64_t *offsets, int nseq, int *first_id);
+int dmst_seqs_add_dna(dmst_ctx *ctx, const char *ascii, const int64_t *offsets, int nseq, int *first_id);
+int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *mask_bits, const int64_t *offsets,
+                         int nseq, int *first_id);
+/* Drop all sequences (device memory is kept for reuse). */
+int dmst_seqs_clear(dmst_ctx *ctx);
+int dmst_seq_count(const dmst_ctx *ctx);
+
+/* Host decode of letter codes (A=0 C=1 G=5 T=16, masked=22, the engine's
+ * protein-alphabet coding of DNA) into codon codes; replaces decodeSequence. */
+int dmst_decode_letters(const char *letters, int L, uint8_t *codes);
+/* Host ASCII DNA -> letter codes as the engine reads FASTA (dummest.cc:437-449). */
+int dmst_encode_dna(const char *ascii, int L, char *letters);
+
+/* ---- scoring ------------------------------------------------------------
+ * Score n pairs.  mode = DMST_MODE_MID or DMST_MODE_FILTER, optionally or-ed
+ * with DMST_MODE_PLAIN / DMST_MODE_FORCE_EXACT.  Synchronous. */
+int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out);
+
+/* Timing of the last dmst_score_pairs call, from CUDA events on the context's
+ * stream: total device ms and the ms of the main DP kernel(s). */
+int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, double *null_ms, int *launches);
+
+/* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
+ * and the three per-base scales (one-nt, two-nt, codon) for one pair, computed
+ * by the device prologue kernel.  Replaces the null half of setupBatch
+ * (dummest-dp-backward.hh:6-188). */
+int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, float *suffix_seed, float *scales3);
+
+/* ---- calibration --------------------------------------------------------
+ * Gumbel fits of the reference (estimateGumbel, dummest-calibration.hh:97-104),
+ * FP64 on the host.  Sorts scores in place.  out8 = MM lambda, MM K,
+ * MM K(lambda=1), ML lambda, ML K, ML K(lambda=1), L-moments lambda, L-moments K. */
+int dmst_estimate_gumbel(double *scores, int n, double seq_length, double *out8);
+
+/* The reference's random calibration sequences (estimateK's generator,
+ * dummest-calibration.hh:436-483): trial t of a profile, as letter codes
+ * (sequence_length + border of them).  letter_freqs = the profile's
+ * background letter probabilities (bg_probs + 4). */
+int dmst_calibration_sequence(const float *letter_freqs, double bg_stop_codon_prob, double insert1,
+                              double insert2, double delete1, double delete2, int trial, int sequence_length,
+                              int border, char *letters);
+
+/* Calibrate a profile on the device: generate num_sequences random sequences
+ * as estimateK does, score them (mode MID), and fit.  out receives
+ * lambda (MM mid), K (MM mid), lambda_filter, K_filter; scores (may be NULL)
+ * receives num_sequences mid ln-scores then num_sequences filter ln-scores. */
+int dmst_calibrate(dmst_ctx *ctx, int profile, int sequence_length, int border, int num_sequences, double *out4,
+                   double *scores);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DUMMEST_B200_H */

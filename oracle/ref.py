@@ -1,0 +1,194 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the reference engine built by
+oracle/Makefile (oracle/_ref/libdmst_ref32.so = FP32 engine "dummestl",
+oracle/_ref/libdmst_ref64.so = FP64 engine "dummest").  See ref_harness.cc
+for the reference functions each entry point calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+LIBS = {32: os.path.join(REF_DIR, "libdmst_ref32.so"), 64: os.path.join(REF_DIR, "libdmst_ref64.so")}
+CLI = {32: os.path.join(REF_DIR, "dummestl_core"), 64: os.path.join(REF_DIR, "dummest_core")}
+
+_libs: dict[int, C.CDLL] = {}
+
+
+def available(bits: int = 32) -> bool:
+    return os.path.exists(LIBS[bits])
+
+
+def build(reference: str = "/root/reference") -> None:
+    """Compile the oracle (needs the reference sources; not available on the GPU box)."""
+    subprocess.run(["make", "-C", HERE, f"REF={reference}", "-j4", "all"], check=True, capture_output=True)
+
+
+def lib(bits: int = 32) -> C.CDLL:
+    if bits in _libs:
+        return _libs[bits]
+    path = LIBS[bits]
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing: run `make -C oracle` where the reference sources are present")
+    L = C.CDLL(path)
+    P = C.POINTER
+    sig = {
+        "dmstref_float_bytes": (C.c_int, []),
+        "dmstref_simd_width": (C.c_int, []),
+        "dmstref_set_rates": (None, [C.c_double] * 6),
+        "dmstref_get_rates": (None, [P(C.c_double)]),
+        "dmstref_load_profiles": (C.c_int, [C.c_char_p, C.c_int, C.c_int]),
+        "dmstref_profile_dims": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int)]),
+        "dmstref_profile_name": (C.c_char_p, [C.c_int]),
+        "dmstref_profile_export": (C.c_int, [C.c_int, P(C.c_float), P(C.c_float), P(C.c_float)]),
+        "dmstref_encode_dna": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p]),
+        "dmstref_decode": (C.c_int, [C.c_char_p, C.c_int, P(C.c_uint8)]),
+        "dmstref_mask_sequence": (C.c_int, [C.c_char_p, C.c_int]),
+        "dmstref_find_similarities": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float),
+                                                P(C.c_int), P(C.c_double), P(C.c_float), P(C.c_int)]),
+        "dmstref_backward_only": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float)]),
+        "dmstref_score_many": (C.c_int, [C.c_int, P(C.c_uint8), P(C.c_int64), C.c_int, C.c_int, C.c_int,
+                                         P(C.c_double), P(C.c_double)]),
+        "dmstref_null_model": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_float),
+                                         P(C.c_float)]),
+        "dmstref_backward_matrix": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_int)]),
+        "dmstref_estimate_gumbel": (None, [P(C.c_double), C.c_int, C.c_double, P(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _libs[bits] = L
+    return L
+
+
+class RefEngine:
+    """The reference engine (FP32 or FP64 build) on explicit inputs."""
+
+    def __init__(self, bits: int = 32):
+        self.bits = bits
+        self.L = lib(bits)
+        self.width = self.L.dmstref_simd_width()
+
+    def set_rates(self, insert1=0.0171, insert2=0.0018, delete1=0.0328, delete2=0.0083, stop=0.0005,
+                  bg_stop=0.046875):
+        self.L.dmstref_set_rates(insert1, insert2, delete1, delete2, stop, bg_stop)
+
+    def load_profiles(self, path: str, mask: bool = False, background_type: str = "G") -> int:
+        n = self.L.dmstref_load_profiles(path.encode(), ord(background_type), int(mask))
+        if n < 0:
+            raise ValueError(f"reference could not read {path}")
+        return n
+
+    def profile(self, p: int):
+        M, W = C.c_int(), C.c_int()
+        if self.L.dmstref_profile_dims(p, C.byref(M), C.byref(W)) != 0:
+            raise IndexError(p)
+        M, W = M.value, W.value
+        values = np.zeros((M + 1, W), np.float32)
+        params = np.zeros((M + 2, 11), np.float32)
+        bg = np.zeros(W, np.float32)
+        P = C.POINTER(C.c_float)
+        self.L.dmstref_profile_export(p, values.ctypes.data_as(P), params.ctypes.data_as(P), bg.ctypes.data_as(P))
+        return self.L.dmstref_profile_name(p).decode(), values, params, bg
+
+    def encode(self, dna: str | bytes) -> np.ndarray:
+        b = dna.encode() if isinstance(dna, str) else dna
+        out = C.create_string_buffer(len(b))
+        if self.L.dmstref_encode_dna(b, len(b), out) < 0:
+            raise ValueError("not DNA")
+        return np.frombuffer(out.raw, dtype=np.int8).copy()
+
+    def decode(self, letters: np.ndarray) -> np.ndarray:
+        letters = np.ascontiguousarray(letters, dtype=np.int8)
+        out = np.zeros(len(letters), np.uint8)
+        self.L.dmstref_decode(letters.ctypes.data_as(C.c_char_p), len(letters),
+                              out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return out
+
+    def mask(self, letters: np.ndarray) -> np.ndarray:
+        """tantan-masked copy of a DNA strand (letter codes), as -m 2 does."""
+        n = len(letters)
+        buf = C.create_string_buffer(2 * n + 16)
+        C.memmove(buf, np.ascontiguousarray(letters, dtype=np.int8).ctypes.data, n)
+        self.L.dmstref_mask_sequence(buf, n)
+        return np.frombuffer(buf.raw[n:2 * n], dtype=np.int8).copy()
+
+    def _ptrs(self, seqs):
+        arrs = [np.ascontiguousarray(s, dtype=np.uint8) for s in seqs]
+        ptrs = (C.POINTER(C.c_uint8) * len(arrs))(*[a.ctypes.data_as(C.POINTER(C.c_uint8)) for a in arrs])
+        lens = (C.c_int * len(arrs))(*[len(a) for a in arrs])
+        return arrs, ptrs, lens
+
+    def find_similarities(self, p: int, seqs):
+        """Per sequence: (mid_m, mid_e, mid_ln, filter_m, filter_e)."""
+        out = []
+        for b in range(0, len(seqs), self.width):
+            chunk = seqs[b:b + self.width]
+            n = len(chunk)
+            arrs, ptrs, lens = self._ptrs(chunk)
+            mm, me, ml = (C.c_float * n)(), (C.c_int * n)(), (C.c_double * n)()
+            fm, fe = (C.c_float * n)(), (C.c_int * n)()
+            if self.L.dmstref_find_similarities(p, ptrs, lens, n, mm, me, ml, fm, fe) != 0:
+                raise ValueError("reference findSimilarities rejected the batch")
+            out += [(mm[k], me[k], ml[k], fm[k], fe[k]) for k in range(n)]
+        return out
+
+    def backward_only(self, p: int, seqs) -> list[float]:
+        out = []
+        for b in range(0, len(seqs), self.width):
+            chunk = seqs[b:b + self.width]
+            n = len(chunk)
+            arrs, ptrs, lens = self._ptrs(chunk)
+            best = (C.c_float * n)()
+            if self.L.dmstref_backward_only(p, ptrs, lens, n, best) != 0:
+                raise ValueError("reference findSimilaritiesBackwardOnly rejected the batch")
+            out += list(best)
+        return out
+
+    def score_many(self, p: int, seqs, threads: int = 1, mode: int = 0):
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint8) for s in seqs]))
+        off = np.zeros(len(seqs) + 1, np.int64)
+        np.cumsum([len(s) for s in seqs], out=off[1:])
+        mid = np.zeros(len(seqs), np.float64)
+        flt = np.zeros(len(seqs), np.float64)
+        P = C.POINTER
+        st = self.L.dmstref_score_many(p, flat.ctypes.data_as(P(C.c_uint8)), off.ctypes.data_as(P(C.c_int64)),
+                                       len(seqs), threads, mode, mid.ctypes.data_as(P(C.c_double)),
+                                       flt.ctypes.data_as(P(C.c_double)))
+        if st != 0:
+            raise ValueError("reference score_many failed")
+        return mid, flt
+
+    def null_model(self, p: int, seq: np.ndarray):
+        seq = np.ascontiguousarray(seq, np.uint8)
+        L = len(seq)
+        pre, suf, sc = np.zeros(L, np.float32), np.zeros(L, np.float32), np.zeros(3, np.float32)
+        P = C.POINTER(C.c_float)
+        if self.L.dmstref_null_model(p, seq.ctypes.data_as(C.POINTER(C.c_uint8)), L, pre.ctypes.data_as(P),
+                                     suf.ctypes.data_as(P), sc.ctypes.data_as(P)) != 0:
+            raise ValueError("null model failed")
+        return pre, suf, sc
+
+    def backward_matrix(self, p: int, seq: np.ndarray):
+        seq = np.ascontiguousarray(seq, np.uint8)
+        L = len(seq)
+        M = C.c_int()
+        self.L.dmstref_profile_dims(p, C.byref(M), C.byref(C.c_int()))
+        M = M.value
+        W1 = np.zeros((M + 1, L), np.float32)
+        cnt = np.zeros(M + 1, np.int32)
+        self.L.dmstref_backward_matrix(p, seq.ctypes.data_as(C.POINTER(C.c_uint8)), L,
+                                       W1.ctypes.data_as(C.POINTER(C.c_float)),
+                                       cnt.ctypes.data_as(C.POINTER(C.c_int)))
+        return W1, cnt
+
+    def estimate_gumbel(self, scores, seq_length: float) -> np.ndarray:
+        s = np.ascontiguousarray(scores, np.float64).copy()
+        out = (C.c_double * 8)()
+        self.L.dmstref_estimate_gumbel(s.ctypes.data_as(C.POINTER(C.c_double)), len(s), seq_length, out)
+        return np.array(out[:])

@@ -1,0 +1,394 @@
+// TEST INFRASTRUCTURE ONLY -- the CPU oracle built from the reference sources.
+//
+// This single translation unit includes the DUMMEST reference engine headers
+// (they define non-inline globals, so the engine must live in exactly one TU,
+// in the include order of dummest.cc:8-17) and exposes a flat C interface to
+// the reference's own hot-path routines, so that tests and the CPU-baseline leg
+// of bench.py can call the unmodified reference code on explicit inputs:
+//
+//   readProfiles / finalizeProfile        dummest-profile.hh:235-329, :105-233
+//   decodeSequence                        dummest-sequence.hh:181-204
+//   findSimilarities (needAlign=false)    dummest-search.hh:9-17
+//     = backwardPass + forwardPass        dummest-dp-backward.hh:444-615,
+//                                         dummest-dp-forward.hh:9-547
+//   findSimilaritiesBackwardOnly          dummest-dp-backward.hh:300-438
+//   setupBatch (null model + seeds)       dummest-dp-backward.hh:191-297
+//   estimateGumbel                        dummest-calibration.hh:97-104
+//
+// Built by oracle/Makefile into oracle/_ref/ (git-ignored) twice: with
+// Float=float (the FP32 engine, "dummestl") and with -DDOUBLE (the FP64
+// engine, "dummest").  It is never linked into, or called by, the product.
+#include "dummest-core.hh"
+#include "dummest-sequence.hh"
+#include "dummest-output.hh"
+#include "dummest-dp.hh"
+#include "dummest-traceback.hh"
+#include "dummest-dp-backward.hh"
+#include "dummest-dp-forward.hh"
+#include "dummest-search.hh"
+#include "dummest-calibration.hh"
+#include "dummest-profile.hh"
+
+#include <atomic>
+#include <thread>
+#include <unistd.h>
+
+namespace {
+
+std::vector<Profile> g_profiles;
+std::vector<Float> g_values;
+std::vector<char> g_charVec;
+std::mutex g_lock;
+
+// The reference keeps a calibration cache that it writes at exit
+// (dummest-calibration.hh:163-336); point it at a scratch directory so the
+// oracle never touches a user's cache.
+struct CacheDirGuard {
+    CacheDirGuard() {
+        std::string dir = "/tmp/dmst-oracle-cache-" + std::to_string((long)getuid());
+        setenv("DUMMEST_CACHE_DIR", dir.c_str(), 0);
+    }
+} g_cacheDirGuard;
+
+// Flush-to-zero for the duration of one oracle call (the reference sets it on
+// every engine thread, dummest-core.hh:143-154); the caller's floating-point
+// mode is restored afterwards.
+struct FtzScope {
+    unsigned saved;
+    FtzScope() : saved(_mm_getcsr()) { enableFlushToZero(); }
+    ~FtzScope() { _mm_setcsr(saved); }
+};
+
+void ensureInit() {
+    static bool done = [] {
+        build_standard_genetic_code();
+        return true;
+    }();
+    (void)done;
+}
+
+const Profile *getProfile(int p) {
+    if (p < 0 || p >= (int)g_profiles.size()) return nullptr;
+    return &g_profiles[p];
+}
+
+// Mid and filter results of one findSimilarities(needAlign=false) batch, exactly
+// as estimateK consumes them (dummest-calibration.hh:489-505).
+void runBatch(const Profile &prof, std::vector<std::vector<uint8_t>> &seqs, int n, DPScratch &scratch,
+              ExpScore *mid, double *midLn, ExpScore *flt) {
+    std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+    for (int k = 0; k < n; ++k) ptrs[k] = &seqs[k];
+    std::array<Float, simdWidth> minProbRatio;
+    minProbRatio.fill((Float)-2.0);
+    std::array<std::vector<AlignedSimilarity>, simdWidth> sims;
+    std::array<ExpScore, simdWidth> filterBest{};
+    findSimilarities(sims, prof, ptrs, minProbRatio, scratch, n, &filterBest, false);
+    for (int k = 0; k < n; ++k) {
+        if (sims[k].size() < 3) {
+            mid[k] = ExpScore{0.0f, 0};
+            midLn[k] = -INFINITY;
+        } else {
+            mid[k] = sims[k][2].pair;
+            midLn[k] = sims[k][2].logProbRatio;
+        }
+        flt[k] = filterBest[k];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmstref_float_bytes(void) { return (int)sizeof(Float); }
+int dmstref_simd_width(void) { return (int)simdWidth; }
+
+// Rates are mutable globals in the reference (dummest-core.hh:115-131).
+void dmstref_set_rates(double insert1, double insert2, double delete1, double delete2, double stop,
+                       double bgStop) {
+    std::lock_guard<std::mutex> g(g_lock);
+    INSERT1 = (Float)insert1;
+    INSERT2 = (Float)insert2;
+    DELETE1 = (Float)delete1;
+    DELETE2 = (Float)delete2;
+    STOP_CODON_PROB = (Float)stop;
+    BG_STOP_CODON_PROB = (Float)bgStop;
+    updateBackgroundFrameshiftRates();
+}
+
+void dmstref_get_rates(double *out6) {
+    out6[0] = INSERT1;
+    out6[1] = INSERT2;
+    out6[2] = DELETE1;
+    out6[3] = DELETE2;
+    out6[4] = STOP_CODON_PROB;
+    out6[5] = BG_STOP_CODON_PROB;
+}
+
+// Parse an HMMER3 text file with the reference reader.  Replaces any profiles
+// loaded before.  Returns the number of profiles, or -1.
+int dmstref_load_profiles(const char *path, int backgroundType, int maskProfiles) {
+    std::lock_guard<std::mutex> g(g_lock);
+    ensureInit();
+    FtzScope ftz;
+    g_profiles.clear();
+    g_values.clear();
+    g_charVec.clear();
+    std::ifstream in(path);
+    if (!in) return -1;
+    if (!readProfiles(in, g_profiles, g_values, g_charVec, backgroundType, maskProfiles != 0, 0.0, false))
+        return -1;
+    // names live in g_charVec; keep Profile::name (a std::string) as is.
+    return (int)g_profiles.size();
+}
+
+int dmstref_profile_dims(int p, int *M, int *width) {
+    const Profile *pr = getProfile(p);
+    if (!pr) return -1;
+    *M = pr->length;
+    *width = pr->width;
+    return 0;
+}
+
+const char *dmstref_profile_name(int p) {
+    const Profile *pr = getProfile(p);
+    return pr ? pr->name.c_str() : "";
+}
+
+// values: (M+1)*width, params: (M+2)*11 (alpha'[3] beta'[3] delta'[3] eps' enter),
+// bg: width.  Converted to float (the FP64 build rounds here).
+int dmstref_profile_export(int p, float *values, float *params, float *bg) {
+    const Profile *pr = getProfile(p);
+    if (!pr) return -1;
+    const int M = pr->length, W = pr->width;
+    for (int i = 0; i < (M + 1) * W; ++i) values[i] = (float)pr->values[i];
+    for (int i = 0; i < M + 2; ++i) {
+        const Params &q = pr->values_v2[i];
+        float *o = params + 11 * i;
+        for (int t = 0; t < 3; ++t) {
+            o[t] = (float)q.alpha_prime[t];
+            o[3 + t] = (float)q.beta_prime[t];
+            o[6 + t] = (float)q.delta_prime[t];
+        }
+        o[9] = (float)q.epsilon_prime;
+        o[10] = (float)q.enter_match_probability;
+    }
+    for (int k = 0; k < W; ++k) bg[k] = (float)pr->bg_probs[k];
+    return 0;
+}
+
+// ASCII DNA -> the engine's letter codes, as main() reads FASTA with IUPAC
+// ambiguity mapped to the masked letter (dummest.cc:437-449).  Returns L or -1.
+int dmstref_encode_dna(const char *ascii, int L, char *out) {
+    ensureInit();
+    FtzScope ftz;
+    char charToNumber[256];
+    memset(charToNumber, 127, 256);
+    setCharToNumber(charToNumber, getAlphabet(20));
+    for (auto c : "RYSWKMBDHVN")
+        if (c != '\0') charToNumber[(unsigned char)c] = charToNumber[tolower(c)] = 22;
+    for (int i = 0; i < L; ++i) {
+        char v = charToNumber[(unsigned char)ascii[i]];
+        if (v == 127) return -1;
+        out[i] = v;
+    }
+    return L;
+}
+
+// Letter codes (length L) -> per-base codon codes (dummest-sequence.hh:181-204).
+int dmstref_decode(const char *codes, int L, uint8_t *out) {
+    ensureInit();
+    FtzScope ftz;
+    char charToNumber[256];
+    memset(charToNumber, 0, 256);
+    const char *alphabet = getAlphabet(20);
+    setCharToNumber(charToNumber, alphabet);
+    std::vector<uint8_t> d = decodeSequence(codes, L, alphabet, charToNumber);
+    std::copy(d.begin(), d.end(), out);
+    return L;
+}
+
+// tantan masking of a DNA strand (dummest-sequence.hh:206-236).  buf holds the
+// L letter codes followed by room for L more; the masked copy lands there.
+int dmstref_mask_sequence(char *buf, int L) {
+    ensureInit();
+    FtzScope ftz;
+    makeMaskedSequence(buf, L, 20);
+    return L;
+}
+
+// One findSimilarities(needAlign=false) call on n <= simdWidth decoded
+// sequences: the calibration mid score (pair and ln) and the exact filter best.
+int dmstref_find_similarities(int p, const uint8_t *const *decoded, const int *lens, int n, float *midM,
+                              int *midE, double *midLn, float *fltM, int *fltE) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || n < 1 || n > (int)simdWidth) return -1;
+    std::vector<std::vector<uint8_t>> seqs(n);
+    for (int k = 0; k < n; ++k) {
+        if (lens[k] < 3) return -1;
+        seqs[k].assign(decoded[k], decoded[k] + lens[k]);
+    }
+    thread_local DPScratch scratch;
+    ExpScore mid[simdWidth], flt[simdWidth];
+    double ln[simdWidth];
+    runBatch(*pr, seqs, n, scratch, mid, ln, flt);
+    for (int k = 0; k < n; ++k) {
+        midM[k] = mid[k].m;
+        midE[k] = mid[k].e;
+        midLn[k] = ln[k];
+        fltM[k] = flt[k].m;
+        fltE[k] = flt[k].e;
+    }
+    return 0;
+}
+
+// The lean float filter (findSimilaritiesBackwardOnly) on n <= simdWidth lanes.
+int dmstref_backward_only(int p, const uint8_t *const *decoded, const int *lens, int n, float *best) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || n < 1 || n > (int)simdWidth) return -1;
+    std::vector<std::vector<uint8_t>> seqs(n);
+    std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+    for (int k = 0; k < n; ++k) {
+        if (lens[k] < 3) return -1;
+        seqs[k].assign(decoded[k], decoded[k] + lens[k]);
+        ptrs[k] = &seqs[k];
+    }
+    thread_local DPScratch scratch;
+    std::array<Float, simdWidth> b;
+    findSimilaritiesBackwardOnly(b, *pr, ptrs, scratch, n);
+    for (int k = 0; k < n; ++k) best[k] = (float)b[k];
+    return 0;
+}
+
+// Many sequences against one profile, the way the reference schedules them
+// (dummest-search.hh:111-117, :201-208): sorted by length (descending), cut
+// into <= simdWidth-lane batches, batches pulled by nthreads workers, each
+// worker with its own DPScratch and flush-to-zero set.  mode 0: backward +
+// forward mid score (needAlign=false) plus the exact filter best; mode 1: the
+// lean float filter only.  Outputs are per input sequence (input order).
+int dmstref_score_many(int p, const uint8_t *codes, const int64_t *offsets, int nseq, int nthreads, int mode,
+                       double *midLn, double *fltLn) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || nseq < 0 || nthreads < 1) return -1;
+    std::vector<int> order(nseq);
+    for (int i = 0; i < nseq; ++i) {
+        order[i] = i;
+        if (offsets[i + 1] - offsets[i] < 3) return -1;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return offsets[a + 1] - offsets[a] > offsets[b + 1] - offsets[b];
+    });
+    const int nb = (nseq + (int)simdWidth - 1) / (int)simdWidth;
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        enableFlushToZero();
+        DPScratch scratch;
+        std::vector<std::vector<uint8_t>> seqs(simdWidth);
+        for (;;) {
+            int b = next.fetch_add(1);
+            if (b >= nb) break;
+            int start = b * (int)simdWidth;
+            int n = std::min((int)simdWidth, nseq - start);
+            for (int k = 0; k < n; ++k) {
+                int s = order[start + k];
+                seqs[k].assign(codes + offsets[s], codes + offsets[s + 1]);
+            }
+            if (mode == 0) {
+                ExpScore mid[simdWidth], flt[simdWidth];
+                double ln[simdWidth];
+                runBatch(*pr, seqs, n, scratch, mid, ln, flt);
+                for (int k = 0; k < n; ++k) {
+                    int s = order[start + k];
+                    midLn[s] = ln[k];
+                    fltLn[s] = scoreToLog(flt[k]);
+                }
+            } else {
+                std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+                for (int k = 0; k < n; ++k) ptrs[k] = &seqs[k];
+                std::array<Float, simdWidth> best;
+                findSimilaritiesBackwardOnly(best, *pr, ptrs, scratch, n);
+                for (int k = 0; k < n; ++k) {
+                    int s = order[start + k];
+                    fltLn[s] = std::log((double)best[k]);
+                    if (midLn) midLn[s] = NAN;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    return 0;
+}
+
+// Null model of one sequence (setupBatch, dummest-dp-backward.hh:191-297):
+// prefixSeed[0..L), suffixSeedFromNext[0..L) as stored Float lanes, and the
+// three per-base scales (one-nt, two-nt, codon) as packed Float lanes.
+int dmstref_null_model(int p, const uint8_t *decoded, int L, float *prefixSeed, float *sufSeed, float *scales) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || L < 3) return -1;
+    std::vector<uint8_t> seq(decoded, decoded + L);
+    std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+    ptrs[0] = &seq;
+    thread_local DPScratch scratch;
+    BackwardCtx ctx;
+    setupBatch(*pr, ptrs, scratch, 1, ctx, false);
+    alignas(64) Float buf[simdWidth];
+    for (int j = 0; j < L; ++j) {
+        Kokkos::Experimental::simd_unchecked_store(scratch.nullPrefixSeed[j], buf,
+                                                   Kokkos::Experimental::simd_flag_default);
+        prefixSeed[j] = (float)buf[0];
+        Kokkos::Experimental::simd_unchecked_store(scratch.nullSuffixSeedFromNext[j], buf,
+                                                   Kokkos::Experimental::simd_flag_default);
+        sufSeed[j] = (float)buf[0];
+    }
+    Kokkos::Experimental::simd_unchecked_store(ctx.nullScaleOneNucleotide, buf, Kokkos::Experimental::simd_flag_default);
+    scales[0] = (float)buf[0];
+    Kokkos::Experimental::simd_unchecked_store(ctx.nullScaleTwoNucleotide, buf, Kokkos::Experimental::simd_flag_default);
+    scales[1] = (float)buf[0];
+    Kokkos::Experimental::simd_unchecked_store(ctx.nullScaleCodon, buf, Kokkos::Experimental::simd_flag_default);
+    scales[2] = (float)buf[0];
+    return 0;
+}
+
+// Full backward W1 matrix of one sequence (rows 0..M, columns 0..L) and the
+// per-row rescale counts, for cell-by-cell comparisons on small cases.
+int dmstref_backward_matrix(int p, const uint8_t *decoded, int L, float *W1, int *counts) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || L < 3) return -1;
+    std::vector<uint8_t> seq(decoded, decoded + L);
+    std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+    ptrs[0] = &seq;
+    thread_local DPScratch scratch;
+    BackwardCtx ctx;
+    backwardPass(*pr, ptrs, scratch, 1, nullptr, ctx, false);
+    alignas(64) Float buf[simdWidth];
+    for (int i = 0; i <= pr->length; ++i) {
+        for (int j = 0; j < L; ++j) {
+            Kokkos::Experimental::simd_unchecked_store(scratch.W1.get(i, j), buf,
+                                                       Kokkos::Experimental::simd_flag_default);
+            W1[(size_t)i * L + j] = (float)buf[0];
+        }
+        counts[i] = scratch.backwardRescaleCount[i][0];
+    }
+    return 0;
+}
+
+// Gumbel fits of the reference (dummest-calibration.hh:97-104).  Sorts scores
+// in place.  out8: MM lambda, MM K, MM K(lambda=1), ML lambda, ML K,
+// ML K(lambda=1), L-moments lambda, L-moments K.
+void dmstref_estimate_gumbel(double *scores, int n, double seqLength, double *out8) {
+    estimateGumbel(out8[0], out8[1], out8[2], out8[3], out8[4], out8[5], out8[6], out8[7], scores, n, seqLength);
+}
+
+}  // extern "C"
