@@ -23,6 +23,7 @@ MODE_MID = 0
 MODE_FILTER = 1
 MODE_PLAIN = 0x100
 MODE_FORCE_EXACT = 0x200
+MODE_EXACT_SEQUENTIAL = 0x400
 RES_EXACT_PATH = 1
 
 

@@ -4,6 +4,7 @@
 
 #include "dp_common.cuh"
 #include "dp_exact.cuh"
+#include "dp_exact_wave.cuh"
 #include "dp_wavefront.cuh"
 #include "host_model.h"
 #include "null_model.cuh"
@@ -193,10 +194,12 @@ struct dmst_ctx {
     DevBuf<int> dCounter;
     DevBuf<float> dW1, dRing;
     DevBuf<ExactJob> dJobs;
+    DevBuf<ExactWaveJob> dWaveJobs;
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
 
-    double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0;
+    double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0;
+    int lastExactPairs = 0;
     int lastLaunches = 0;
 
     int fail(int status, const char *fmt, ...) {
@@ -310,6 +313,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dW1.release();
     ctx->dRing.release();
     ctx->dJobs.release();
+    ctx->dWaveJobs.release();
     ctx->dExactScratch.release();
     ctx->dExactOut.release();
     for (auto &e : ctx->ev)
@@ -614,7 +618,8 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     if (!ctx || (n && (!pairs || !out))) return DMST_EINVAL;
     const int base = mode & 0xff;
     const bool plain = (mode & DMST_MODE_PLAIN) != 0;
-    const bool forceExact = (mode & DMST_MODE_FORCE_EXACT) != 0;
+    const bool forceExact = (mode & (DMST_MODE_FORCE_EXACT | DMST_MODE_EXACT_SEQUENTIAL)) != 0;
+    const bool sequentialExact = (mode & DMST_MODE_EXACT_SEQUENTIAL) != 0;
     if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
     const bool mid = base == DMST_MODE_MID;
     ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = 0;
@@ -661,28 +666,64 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         if (mid) w1Max = std::max(w1Max, nS * D * (size_t)S);
         ringMax = std::max(ringMax, 2 * P);
     }
-    // Chunks: runs of up to 2 * warps pairs of one profile; costliest first.
-    const int chunkPairs = 2 * kWarpsPerCta;
-    std::vector<Chunk> chunks;
-    std::vector<double> chunkCost;
+    // Kernel groups by rows per lane (fixed per profile).  Chunks: runs of up to
+    // 2 x warps pairs of one profile, costliest first within each group.
+    struct Group {
+        int R, warps;
+        void (*kern)(DpArgs);
+        std::vector<Chunk> chunks;
+        std::vector<double> cost;
+        int maxRowPad = 0;
+        size_t smem = 0;
+        int grid = 0;
+        size_t chunkBase = 0;
+    };
+    Group groups[3] = {
+        {4, KernelShape<4>::warps, mid ? dpKernel<4, true> : dpKernel<4, false>},
+        {2, KernelShape<2>::warps, mid ? dpKernel<2, true> : dpKernel<2, false>},
+        {1, KernelShape<1>::warps, mid ? dpKernel<1, true> : dpKernel<1, false>},
+    };
+    auto groupOf = [](int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); };
     for (size_t k = 0; k < n;) {
+        Group &G = groups[groupOf(dp[k].R)];
         size_t e = k;
         double cost = 0;
+        const int chunkPairs = plain ? 1 : 2 * G.warps;
         while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
             cost += (double)(dp[e].M + 1) * dp[e].L;
             ++e;
         }
-        chunks.push_back(Chunk{(int)k, (int)(e - k), dp[k].prof, ctx->profiles[dp[k].prof].rowPad});
-        chunkCost.push_back(cost);
+        const int rowPad = ctx->profiles[dp[k].prof].rowPad;
+        G.chunks.push_back(Chunk{(int)k, (int)(e - k), dp[k].prof, rowPad});
+        G.cost.push_back(cost);
+        G.maxRowPad = std::max(G.maxRowPad, rowPad);
         k = e;
     }
-    {
-        std::vector<int> co(chunks.size());
-        std::iota(co.begin(), co.end(), 0);
-        std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return chunkCost[a] > chunkCost[b]; });
-        std::vector<Chunk> sorted(chunks.size());
-        for (size_t i = 0; i < co.size(); ++i) sorted[i] = chunks[co[i]];
-        chunks.swap(sorted);
+    std::vector<Chunk> allChunks;
+    size_t slotsMax = 0;
+    for (Group &G : groups) {
+        if (G.chunks.empty()) continue;
+        if (!plain) {
+            std::vector<int> co(G.chunks.size());
+            std::iota(co.begin(), co.end(), 0);
+            std::stable_sort(co.begin(), co.end(), [&](int a, int b) { return G.cost[a] > G.cost[b]; });
+            std::vector<Chunk> sorted(co.size());
+            for (size_t i = 0; i < co.size(); ++i) sorted[i] = G.chunks[co[i]];
+            G.chunks.swap(sorted);
+        }
+        G.chunkBase = allChunks.size();
+        allChunks.insert(allChunks.end(), G.chunks.begin(), G.chunks.end());
+        G.smem = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
+        if ((int)G.smem > ctx->maxSmemOptin - 1024)
+            return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
+                             (ctx->maxSmemOptin - 1024) / (kNumCodes * 4) - 1);
+        CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
+           "smem attribute");
+        int perSm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
+        if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
+        G.grid = plain ? 1 : (int)std::min<long long>((long long)perSm * ctx->smCount, (long long)G.chunks.size());
+        slotsMax = std::max(slotsMax, (size_t)G.grid * G.warps);
     }
 
     CK(ctx->dPairs.ensure(n), "alloc pairs");
@@ -691,35 +732,23 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(ctx->dNullTmpOff.ensure(n), "alloc null tmp");
     CK(ctx->dScales.ensure(n), "alloc scales");
     CK(ctx->dOut.ensure(n), "alloc out");
-    CK(ctx->dChunks.ensure(chunks.size()), "alloc chunks");
+    CK(ctx->dChunks.ensure(allChunks.size()), "alloc chunks");
     CK(cudaMemcpyAsync(ctx->dPairs.p, dp.data(), n * sizeof(DevPair), cudaMemcpyHostToDevice, ctx->stream),
        "upload pairs");
     CK(cudaMemcpyAsync(ctx->dNullTmpOff.p, tmpOff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream),
        "upload pairs");
-    CK(cudaMemcpyAsync(ctx->dChunks.p, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
                        ctx->stream),
        "upload chunks");
-
-    // Launch geometry of the persistent kernel.
-    const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
-    if ((int)smem > ctx->maxSmemOptin - 1024)
-        return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
-                         (ctx->maxSmemOptin - 1024) / (kNumCodes * 4) - 1);
-    auto kern = mid ? dpKernel<true> : dpKernel<false>;
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
-    int perSm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kWarpsPerCta * kLanes, smem), "occupancy");
-    if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
-    int grid = plain ? 1 : std::min<long long>((long long)perSm * ctx->smCount, (long long)chunks.size());
-    if (grid < 1) grid = 1;
-    const size_t slots = (size_t)grid * kWarpsPerCta;
     const size_t w1Slot = (w1Max + 63) / 64 * 64;
     const size_t ringSlot = (ringMax + 63) / 64 * 64;
-    CK(ctx->dW1.ensure(std::max<size_t>(slots * w1Slot, 1)), "alloc W1 slots");
-    CK(ctx->dRing.ensure(slots * ringSlot), "alloc ring slots");
-    const size_t nCounters = plain ? n : 1;
+    // The groups run one after another on the stream, so they share the slots.
+    CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
+    CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
+    const size_t nCounters = allChunks.size() + 3;
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
     CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
+    const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
 
     CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
     NullRates nr;
@@ -734,9 +763,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
     DpArgs g;
-    g.chunks = ctx->dChunks.p;
-    g.nChunks = (int)chunks.size();
-    g.chunkCounter = ctx->dCounter.p;
     g.pairs = ctx->dPairs.p;
     g.profiles = ctx->dProfiles.p;
     g.emit = ctx->dEmit.p;
@@ -751,28 +777,29 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     g.out = ctx->dOut.p;
     int launches = 1;  // null-model kernel
     if (!forceExact) {
-        if (plain) {
-            // One pair per launch: a one-warp grid over a one-pair chunk list.
-            std::vector<Chunk> single(n);
-            for (size_t k = 0; k < n; ++k)
-                single[k] = Chunk{(int)k, 1, dp[k].prof, ctx->profiles[dp[k].prof].rowPad};
-            CK(ctx->dChunks.ensure(n), "alloc chunks");
-            CK(cudaMemcpyAsync(ctx->dChunks.p, single.data(), n * sizeof(Chunk), cudaMemcpyHostToDevice,
-                               ctx->stream),
-               "upload chunks");
-            for (size_t k = 0; k < n; ++k) {
+        for (int gi = 0; gi < 3; ++gi) {
+            Group &G = groups[gi];
+            if (G.chunks.empty()) continue;
+            if (plain) {
+                // One pair per launch: a one-CTA grid over a one-pair chunk.
+                for (size_t k = 0; k < G.chunks.size(); ++k) {
+                    DpArgs gk = g;
+                    gk.chunks = ctx->dChunks.p + G.chunkBase + k;
+                    gk.nChunks = 1;
+                    gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
+                    G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk);
+                    ++launches;
+                }
+            } else {
                 DpArgs gk = g;
-                gk.chunks = ctx->dChunks.p + k;
-                gk.nChunks = 1;
-                gk.chunkCounter = ctx->dCounter.p + k;
-                kern<<<1, kWarpsPerCta * kLanes, smem, ctx->stream>>>(gk);
+                gk.chunks = ctx->dChunks.p + G.chunkBase;
+                gk.nChunks = (int)G.chunks.size();
+                gk.chunkCounter = ctx->dCounter.p + gi;
+                G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk);
                 ++launches;
             }
-        } else {
-            kern<<<grid, kWarpsPerCta * kLanes, smem, ctx->stream>>>(g);
-            ++launches;
+            CK(cudaGetLastError(), "DP kernel");
         }
-        CK(cudaGetLastError(), "DP kernel");
     }
     CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
     std::vector<PairOut> po(n);
@@ -799,33 +826,53 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const size_t budget = std::max<size_t>(free / 2, (size_t)256 << 20);
         eo.resize(flagged.size());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        if (!sequentialExact)
+            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+               "smem attribute");
         size_t i0 = 0;
         while (i0 < flagged.size()) {
             std::vector<ExactJob> jobs;
+            std::vector<ExactWaveJob> wjobs;
             long long used = 0;
             size_t i1 = i0;
             while (i1 < flagged.size()) {
                 const DevPair &d = dp[flagged[i1]];
-                long long need = exactScratchFloats(d.M, d.L);
-                if (!jobs.empty() && (size_t)(used + need) * 4 > budget) break;
-                jobs.push_back(ExactJob{flagged[i1], used});
+                long long need = sequentialExact ? exactScratchFloats(d.M, d.L) : exactWaveScratch(d.M, d.L);
+                need = (need + 63) / 64 * 64;
+                if (i1 > i0 && (size_t)(used + need) * 4 > budget) break;
+                if (sequentialExact)
+                    jobs.push_back(ExactJob{flagged[i1], used});
+                else
+                    wjobs.push_back(ExactWaveJob{flagged[i1], 0, used});
                 used += need;
                 ++i1;
             }
-            CK(ctx->dJobs.ensure(jobs.size()), "alloc exact jobs");
+            const size_t nj = i1 - i0;
             CK(ctx->dExactScratch.ensure((size_t)used), "alloc exact scratch");
-            CK(ctx->dExactOut.ensure(jobs.size()), "alloc exact out");
-            CK(cudaMemcpyAsync(ctx->dJobs.p, jobs.data(), jobs.size() * sizeof(ExactJob), cudaMemcpyHostToDevice,
-                               ctx->stream),
-               "upload jobs");
-            const int tpb = 32;
-            exactKernel<<<(int)((jobs.size() + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
-                ctx->dJobs.p, (int)jobs.size(), ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
+            CK(ctx->dExactOut.ensure(nj), "alloc exact out");
+            if (sequentialExact) {
+                CK(ctx->dJobs.ensure(nj), "alloc exact jobs");
+                CK(cudaMemcpyAsync(ctx->dJobs.p, jobs.data(), nj * sizeof(ExactJob), cudaMemcpyHostToDevice,
+                                   ctx->stream),
+                   "upload jobs");
+                const int tpb = 32;
+                exactKernel<<<(int)((nj + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
+                    ctx->dJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
+            } else {
+                CK(ctx->dWaveJobs.ensure(nj), "alloc exact jobs");
+                CK(cudaMemcpyAsync(ctx->dWaveJobs.p, wjobs.data(), nj * sizeof(ExactWaveJob),
+                                   cudaMemcpyHostToDevice, ctx->stream),
+                   "upload jobs");
+                const int blocks = (int)std::min<size_t>(nj, (size_t)ctx->smCount * 16);
+                exactWaveKernel<<<blocks, kLanes, smem, ctx->stream>>>(
+                    ctx->dWaveJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
+            }
             CK(cudaGetLastError(), "exact kernel");
             ++launches;
-            CK(cudaMemcpyAsync(eo.data() + i0, ctx->dExactOut.p, jobs.size() * sizeof(ExactOut),
-                               cudaMemcpyDeviceToHost, ctx->stream),
+            CK(cudaMemcpyAsync(eo.data() + i0, ctx->dExactOut.p, nj * sizeof(ExactOut), cudaMemcpyDeviceToHost,
+                               ctx->stream),
                "download exact");
             CK(cudaStreamSynchronize(ctx->stream), "exact kernel");
             i0 = i1;
@@ -834,6 +881,8 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaEventSynchronize(ctx->ev[4]), "event");
         cudaEventElapsedTime(&exactMs, ctx->ev[3], ctx->ev[4]);
     }
+    ctx->lastExactMs = exactMs;
+    ctx->lastExactPairs = (int)flagged.size();
 
     float nullMs = 0, dpMs = 0;
     cudaEventElapsedTime(&nullMs, ctx->ev[0], ctx->ev[1]);

@@ -132,15 +132,33 @@ __device__ __forceinline__ void storeW1(float *p, const float (&w)[R]) {
 template <int R>
 __device__ __forceinline__ void loadW1(float (&w)[R], const float *p) {
     if constexpr (R == 4) {
-        float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+        float4 v = __ldcg(reinterpret_cast<const float4 *>(p));
         w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
     } else if constexpr (R == 2) {
-        float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
+        float2 v = __ldcg(reinterpret_cast<const float2 *>(p));
         w[0] = v.x; w[1] = v.y;
     } else {
-        w[0] = __ldcs(p);
+        w[0] = __ldcg(p);
     }
 }
+
+// Steps of look-ahead for the per-step global operands (codon code, seeds,
+// W1, ring): each step issues the loads of step t + kPF into a register FIFO,
+// so their latency overlaps kPF steps of arithmetic.
+constexpr int kPF = 4;
+
+// Per-lane position in the wavefront: local time u and (stripe, column).
+struct Cursor {
+    int u, sp, jj;
+    __device__ __forceinline__ void advance(int P) {
+        if (u >= 0 && ++jj == P) {
+            jj = 0;
+            ++sp;
+        }
+        ++u;
+    }
+    __device__ __forceinline__ bool active(int nS, int L) const { return u >= 0 && sp < nS && jj < L; }
+};
 
 // Backward sweep.  STORE: keep W1 for the forward sweep (mid mode); without
 // it this is the lean float filter (findSimilaritiesBackwardOnly), whose
@@ -157,15 +175,39 @@ __device__ void backwardSweep(const SweepArgs &a, int lane, float &filtOut, floa
     float filt = 0.0f, maxY = 0.0f;
     const int L = a.L, P = a.P, nS = a.nS;
     const int T = nS * P + (kLanes - 1);
-    int u = -(kLanes - 1 - lane);  // local time of this lane
-    int sp = 0, jj = 0;            // stripe counted from the bottom, column counted from the right
-    for (int t = 0; t < T; ++t, ++u) {
+    const bool ringAhead = P > kLanes + kPF;  // ring entries are written > kPF steps before use
+    Cursor cur{-(kLanes - 1 - lane), 0, 0}, ahead = cur;
+    int qc[kPF];
+    float qs[kPF], qp[kPF], qw[kPF], qy[kPF];
+    auto fetch = [&](const Cursor &x, int &code, float &suf, float &pre, float &rw, float &ry) {
+        code = kPad;
+        suf = pre = rw = ry = 0.0f;
+        if (x.active(nS, L)) {
+            const int j = L - 1 - x.jj;
+            code = (j + 1 < L) ? (int)__ldg(a.codes + j + 1) : kPad;
+            suf = __ldg(a.suf + j);
+            pre = __ldg(a.pre + j);
+            if (ringAhead && lane == kLanes - 1 && x.sp > 0) {
+                rw = __ldcg(a.ring + 2 * x.jj);
+                ry = __ldcg(a.ring + 2 * x.jj + 1);
+            }
+        }
+    };
+#pragma unroll
+    for (int k = 0; k < kPF; ++k) {
+        fetch(ahead, qc[k], qs[k], qp[k], qw[k], qy[k]);
+        ahead.advance(P);
+    }
+    for (int t = 0; t < T; ++t) {
+        int nc;
+        float ns, np, nw, ny;
+        fetch(ahead, nc, ns, np, nw, ny);
+        ahead.advance(P);
         float inW = __shfl_down_sync(kFull, sendW, 1);
         float inY = __shfl_down_sync(kFull, sendY, 1);
-        const bool act = (u >= 0) && (sp < nS) && (jj < L);
-        if (act) {
+        if (cur.active(nS, L)) {
+            const int sp = cur.sp, jj = cur.jj;
             const int s = nS - 1 - sp;
-            const int j = L - 1 - jj;
             const int rowBase = s * S + lane * R;
             if (jj == 0) {
                 loadBackwardCoef<R>(c, a, rowBase);
@@ -174,20 +216,22 @@ __device__ void backwardSweep(const SweepArgs &a, int lane, float &filtOut, floa
                 rb1 = rb2 = rb3 = 0.0f;
             }
             if (lane == kLanes - 1) {
-                if (sp > 0) {
+                if (sp == 0) {
+                    inW = inY = 0.0f;
+                } else if (ringAhead) {
+                    inW = qw[0];
+                    inY = qy[0];
+                } else {
                     inW = __ldcg(a.ring + 2 * jj);
                     inY = __ldcg(a.ring + 2 * jj + 1);
-                } else {
-                    inW = 0.0f;
-                    inY = 0.0f;
                 }
             }
-            const int code = (j + 1 < L) ? (int)__ldg(a.codes + j + 1) : kPad;
+            const int code = qc[0];
             const float bgv = a.smBg[code];
             float e[R];
             loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
-            const float sufv = __ldg(a.suf + j);
-            const float prev = __ldg(a.pre + j);
+            const float sufv = qs[0];
+            const float prev = qp[0];
             float bW1 = rb1, bW2 = rb2, bW3 = rb3, bY = inY;
             float wv[R];
 #pragma unroll
@@ -234,12 +278,20 @@ __device__ void backwardSweep(const SweepArgs &a, int lane, float &filtOut, floa
             sendW = 0.0f;
             sendY = 0.0f;
         }
-        if (u >= 0) {
-            if (++jj == P) {
-                jj = 0;
-                ++sp;
-            }
+#pragma unroll
+        for (int k = 0; k < kPF - 1; ++k) {
+            qc[k] = qc[k + 1];
+            qs[k] = qs[k + 1];
+            qp[k] = qp[k + 1];
+            qw[k] = qw[k + 1];
+            qy[k] = qy[k + 1];
         }
+        qc[kPF - 1] = nc;
+        qs[kPF - 1] = ns;
+        qp[kPF - 1] = np;
+        qw[kPF - 1] = nw;
+        qy[kPF - 1] = ny;
+        cur.advance(P);
         __syncwarp();
     }
     filtOut = filt;
@@ -258,13 +310,41 @@ __device__ void forwardSweep(const SweepArgs &a, int lane, float &bestOut, float
     float best = 0.0f, mx = 0.0f;
     const int L = a.L, P = a.P, nS = a.nS;
     const int T = nS * P + (kLanes - 1);
-    int u = -lane;
-    int s = 0, j = 0;
-    for (int t = 0; t < T; ++t, ++u) {
+    const bool ringAhead = P > kLanes + kPF;
+    Cursor cur{-lane, 0, 0}, ahead = cur;
+    int qc[kPF];
+    float qp[kPF], qw[kPF], qy[kPF], qb[kPF][R];
+    auto fetch = [&](const Cursor &x, int &code, float &pre, float &rw, float &ry, float (&wb)[R]) {
+        code = kPad;
+        pre = rw = ry = 0.0f;
+#pragma unroll
+        for (int k = 0; k < R; ++k) wb[k] = 0.0f;
+        if (x.active(nS, L)) {
+            const int s = x.sp, j = x.jj;
+            code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
+            pre = __ldg(a.pre + j);
+            const int db = (L - 1 - j) + (kLanes - 1 - lane);
+            loadW1<R>(wb, a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
+            if (ringAhead && lane == 0 && s > 0) {
+                rw = __ldcg(a.ring + 2 * j);
+                ry = __ldcg(a.ring + 2 * j + 1);
+            }
+        }
+    };
+#pragma unroll
+    for (int k = 0; k < kPF; ++k) {
+        fetch(ahead, qc[k], qp[k], qw[k], qy[k], qb[k]);
+        ahead.advance(P);
+    }
+    for (int t = 0; t < T; ++t) {
+        int nc;
+        float np, nw, ny, nb[R];
+        fetch(ahead, nc, np, nw, ny, nb);
+        ahead.advance(P);
         float inW = __shfl_up_sync(kFull, sendIn, 1);
         float inY = __shfl_up_sync(kFull, sendY, 1);
-        const bool act = (u >= 0) && (s < nS) && (j < L);
-        if (act) {
+        if (cur.active(nS, L)) {
+            const int s = cur.sp, j = cur.jj;
             const int rowBase = s * S + lane * R;
             if (j == 0) {
                 loadForwardCoef<R>(c, a, rowBase);
@@ -272,22 +352,21 @@ __device__ void forwardSweep(const SweepArgs &a, int lane, float &bestOut, float
                 for (int k = 0; k < R; ++k) w1[k] = w2[k] = w3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
             }
             if (lane == 0) {
-                if (s > 0) {
+                if (s == 0) {
+                    inW = inY = 0.0f;
+                } else if (ringAhead) {
+                    inW = qw[0];
+                    inY = qy[0];
+                } else {
                     inW = __ldcg(a.ring + 2 * j);
                     inY = __ldcg(a.ring + 2 * j + 1);
-                } else {
-                    inW = 0.0f;
-                    inY = 0.0f;
                 }
             }
-            const int code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
+            const int code = qc[0];
             const float bgsC = a.smBg[code] * a.sc.sC;
             float e[R];
             loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
-            const float prev = __ldg(a.pre + j);
-            float wb[R];
-            const int db = (L - 1 - j) + (kLanes - 1 - lane);
-            loadW1<R>(wb, a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
+            const float prev = qp[0];
             float win = inW, yab = inY;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
@@ -297,7 +376,7 @@ __device__ void forwardSweep(const SweepArgs &a, int lane, float &bestOut, float
                 const float Z2 = c.a2[k] * w2[k];
                 const float W0 = win + __fmaf_rn(prev, c.rs[k], (Z0 + Z1) + Z2);
                 mx = fmaxf(mx, W0);
-                best = fmaxf(best, W0 * wb[k]);
+                best = fmaxf(best, W0 * qb[0][k]);
                 const float Y0 = __fmaf_rn(c.d0[k], W0, c.eps[k] * yab);
                 mx = fmaxf(mx, Y0);
                 const float nin = __fmaf_rn(c.d2[k], w1[k], __fmaf_rn(c.d1[k], w2[k], X + Y0));
@@ -320,12 +399,22 @@ __device__ void forwardSweep(const SweepArgs &a, int lane, float &bestOut, float
             sendIn = 0.0f;
             sendY = 0.0f;
         }
-        if (u >= 0) {
-            if (++j == P) {
-                j = 0;
-                ++s;
-            }
+#pragma unroll
+        for (int k = 0; k < kPF - 1; ++k) {
+            qc[k] = qc[k + 1];
+            qp[k] = qp[k + 1];
+            qw[k] = qw[k + 1];
+            qy[k] = qy[k + 1];
+#pragma unroll
+            for (int r = 0; r < R; ++r) qb[k][r] = qb[k + 1][r];
         }
+        qc[kPF - 1] = nc;
+        qp[kPF - 1] = np;
+        qw[kPF - 1] = nw;
+        qy[kPF - 1] = ny;
+#pragma unroll
+        for (int r = 0; r < R; ++r) qb[kPF - 1][r] = nb[r];
+        cur.advance(P);
         __syncwarp();
     }
     bestOut = best;
@@ -393,19 +482,27 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     }
 }
 
-constexpr int kWarpsPerCta = 4;
+// Warps per CTA by rows per lane: tall profiles (R = 4) carry the largest
+// shared emission tables, so more warps share one copy.
+template <int R>
+struct KernelShape {
+    static constexpr int warps = R == 4 ? 6 : 4;
+    static constexpr int minBlocks = R == 4 ? 2 : 3;
+};
 
-// Persistent kernel: CTAs pull chunks (same-profile runs of pairs, costliest
-// first) from a global counter, stage the chunk's profile emission table in
-// shared memory, and their warps pull pairs from the chunk.
-template <bool MID>
-__global__ void __launch_bounds__(kWarpsPerCta * kLanes) dpKernel(DpArgs g) {
+// Persistent kernel for one rows-per-lane value: CTAs pull chunks
+// (same-profile runs of pairs, costliest first) from a global counter, stage
+// the chunk's profile emission table in shared memory, and their warps pull
+// pairs from the chunk.
+template <int R, bool MID>
+__global__ void __launch_bounds__(KernelShape<R>::warps * kLanes, KernelShape<R>::minBlocks) dpKernel(DpArgs g) {
+    constexpr int NW = KernelShape<R>::warps;
     extern __shared__ float4 smRaw[];
     float *smE = reinterpret_cast<float *>(smRaw);
     __shared__ float smBg[32];
     __shared__ int smChunk, smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t slot = (size_t)blockIdx.x * kWarpsPerCta + warp;
+    const size_t slot = (size_t)blockIdx.x * NW + warp;
     float *w1 = g.w1 + slot * g.w1SlotFloats;
     float *ring = g.ring + slot * g.ringSlotFloats;
     int loaded = -1;
@@ -433,14 +530,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * kLanes) dpKernel(DpArgs g) {
             if (lane == 0) k = atomicAdd(&smNext, 1);
             k = __shfl_sync(kFull, k, 0);
             if (k >= ch.count) break;
-            const int pi = ch.first + k;
-            const int R = g.pairs[pi].R;
-            if (R == 4)
-                scorePair<4, MID>(g, pi, smE, rowPad, smBg, w1, ring, lane);
-            else if (R == 2)
-                scorePair<2, MID>(g, pi, smE, rowPad, smBg, w1, ring, lane);
-            else
-                scorePair<1, MID>(g, pi, smE, rowPad, smBg, w1, ring, lane);
+            scorePair<R, MID>(g, ch.first + k, smE, rowPad, smBg, w1, ring, lane);
         }
         __syncthreads();
     }

@@ -53,8 +53,13 @@ extern "C" {
  * (same per-pair code), the baseline the batched persistent kernel is
  * measured against. */
 #define DMST_MODE_PLAIN 0x100
-/* Flag: route every pair through the exact row-rescaled path (for tests). */
+/* Flag: route every pair through the exact row-rescaled wavefront path
+ * (the path taken by pairs whose rows the reference would rescale). */
 #define DMST_MODE_FORCE_EXACT 0x200
+/* Flag: route every pair through the one-thread-per-pair exact kernel, a
+ * direct restatement of the reference's row-at-a-time loops (a slow
+ * cross-check of the wavefront paths). */
+#define DMST_MODE_EXACT_SEQUENTIAL 0x400
 
 /* ---- per-result flags -------------------------------------------------- */
 #define DMST_RES_EXACT_PATH 1 /* pair was scored by the exact row-rescaled kernel */

@@ -119,6 +119,7 @@ def test_regression_fixtures(gpu_ctx, regression):
 
 
 def test_force_exact_path_matches(gpu_ctx, ref32, tmp_path):
+    """Every pair through the warp-parallel exact path."""
     rng, profs, txt = _setup_profiles(tmp_path, ref32, [20, 150], seed=23)
     pids = gpu_ctx.load_hmm(txt)
     reads = _mk_reads(rng, profs, [5, 50, 400, 900])
@@ -165,3 +166,42 @@ def test_input_paths_agree(gpu_ctx, ref32, tmp_path):
 def test_rejects_short_sequences(gpu_ctx):
     with pytest.raises(ValueError):
         gpu_ctx.add_decoded([np.zeros(2, np.uint8)])
+
+
+def test_exact_paths_agree_on_rescaled_fixture(gpu_ctx, regression):
+    """herpes rescales rows ~35 times (scores ~e^1554): the warp-parallel
+    exact path (count discovery + replay) and the one-thread restatement of
+    the reference loops must give the same ExpScores, within 1e-3 bits of the
+    FP32 reference."""
+    g = regression
+    pid = gpu_ctx.add_profile(g["profile_values"], g["profile_params"], g["profile_bg"])
+    lens = g["record_lengths"]
+    off = np.concatenate([[0], np.cumsum(lens)])
+    codes = [g["record_codes"][off[k]:off[k + 1]] for k in range(len(lens))]
+    sids = gpu_ctx.add_decoded(codes)
+    wave = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | d.MODE_FORCE_EXACT)
+    seq = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | d.MODE_EXACT_SEQUENTIAL)
+    for k, (a, b) in enumerate(zip(wave, seq)):
+        want = _bits(g["mid_ln_f32"][k])
+        print(g["record_names"][k], "wave %.6f seq %.6f ref %.6f" % (_bits(a.mid_ln), _bits(b.mid_ln), want),
+              "bit-identical to ref:", (a.mid.m, a.mid.e) == (float(g["mid_m_f32"][k]), int(g["mid_e_f32"][k])))
+        assert abs(_bits(a.mid_ln) - want) <= BITS_TOL
+        assert abs(_bits(b.mid_ln) - want) <= BITS_TOL
+        assert abs(_bits(a.mid_ln) - _bits(b.mid_ln)) <= 1e-5
+        wf = math.log(g["filter_m_f32"][k]) + int(g["filter_e_f32"][k]) * LN2
+        assert abs(_bits(a.filter_ln) - _bits(wf)) <= BITS_TOL
+
+
+def test_exact_wave_matches_sequential_on_synthetic(gpu_ctx, ref32, tmp_path):
+    rng, profs, txt = _setup_profiles(tmp_path, ref32, [7, 64, 300], seed=51)
+    pids = gpu_ctx.load_hmm(txt)
+    reads = _mk_reads(rng, profs, [3, 33, 200, 1100], implant=1.0)
+    codes = [ref32.decode(ref32.encode(s)) for s in reads]
+    sids = gpu_ctx.add_decoded(codes)
+    for p, pid in enumerate(pids):
+        a = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | d.MODE_FORCE_EXACT)
+        b = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | d.MODE_EXACT_SEQUENTIAL)
+        want = ref32.find_similarities(p, codes)
+        for x, y, w in zip(a, b, want):
+            assert abs(_bits(x.mid_ln) - _bits(y.mid_ln)) <= 1e-5
+            assert abs(_bits(x.mid_ln) - _bits(w[2])) <= BITS_TOL
