@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdummest_b200.so")
+# DMST_LIB selects another build of the same library (A/B comparisons of build options).
+LIB_PATH = os.environ.get("DMST_LIB") or os.path.join(HERE, "libdummest_b200.so")
 
 DMST_OK = 0
 DMST_EINVAL = -1

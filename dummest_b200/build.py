@@ -51,10 +51,10 @@ def needs_build() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
+def build(force: bool = False, verbose: bool = False, out: str = LIB, defines: tuple = ()) -> str:
+    if not force and out == LIB and not needs_build():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", LIB]
+    cmd = [nvcc(), *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-o", out]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -64,7 +64,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libdummest_b200.so")
     if verbose and (res.stdout or res.stderr):
         sys.stderr.write(res.stdout + res.stderr)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

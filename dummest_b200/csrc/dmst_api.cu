@@ -661,7 +661,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         tmpEntries += d.L + 4;
         const int S = kLanes * d.R;
         const size_t nS = (size_t)(d.M + 1 + S - 1) / S;
-        const size_t P = (size_t)std::max(d.L, kLanes);
+        const size_t P = (size_t)wavePeriod(d.L);
         const size_t D = P + kLanes - 1;
         if (mid) w1Max = std::max(w1Max, nS * D * (size_t)S);
         ringMax = std::max(ringMax, 2 * P);
@@ -670,7 +670,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     // 2 x warps pairs of one profile, costliest first within each group.
     struct Group {
         int R, warps;
-        void (*kern)(DpArgs);
+        void (*kern)(DpArgs, int);
         std::vector<Chunk> chunks;
         std::vector<double> cost;
         int maxRowPad = 0;
@@ -679,16 +679,16 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         size_t chunkBase = 0;
     };
     Group groups[3] = {
-        {4, KernelShape<4>::warps, mid ? dpKernel<4, true> : dpKernel<4, false>},
-        {2, KernelShape<2>::warps, mid ? dpKernel<2, true> : dpKernel<2, false>},
-        {1, KernelShape<1>::warps, mid ? dpKernel<1, true> : dpKernel<1, false>},
+        {4, kCtaWarps, mid ? dpKernel<4, true> : dpKernel<4, false>},
+        {2, kCtaWarps, mid ? dpKernel<2, true> : dpKernel<2, false>},
+        {1, kCtaWarps, mid ? dpKernel<1, true> : dpKernel<1, false>},
     };
     auto groupOf = [](int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); };
     for (size_t k = 0; k < n;) {
         Group &G = groups[groupOf(dp[k].R)];
         size_t e = k;
         double cost = 0;
-        const int chunkPairs = plain ? 1 : 2 * G.warps;
+        const int chunkPairs = plain ? 1 : 4 * kCtaWarps;
         while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
             cost += (double)(dp[e].M + 1) * dp[e].L;
             ++e;
@@ -713,17 +713,22 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         }
         G.chunkBase = allChunks.size();
         allChunks.insert(allChunks.end(), G.chunks.begin(), G.chunks.end());
-        G.smem = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
-        if ((int)G.smem > ctx->maxSmemOptin - 1024)
+        // Shared memory: the emission table, then one staging window per warp;
+        // tall profiles get fewer warps so that both fit.
+        const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
+        const size_t limit = (size_t)ctx->maxSmemOptin - 1024;
+        if (table + sizeof(Window) > limit)
             return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
-                             (ctx->maxSmemOptin - 1024) / (kNumCodes * 4) - 1);
+                             (int)((limit - sizeof(Window)) / (kNumCodes * 4)) - 1);
+        G.warps = (int)std::min<size_t>(kCtaWarps, (limit - table) / sizeof(Window));
+        G.smem = table + (size_t)G.warps * sizeof(Window);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
         int perSm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
         if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
         G.grid = plain ? 1 : (int)std::min<long long>((long long)perSm * ctx->smCount, (long long)G.chunks.size());
-        slotsMax = std::max(slotsMax, (size_t)G.grid * G.warps);
+        slotsMax = std::max(slotsMax, (size_t)G.grid * kCtaWarps);
     }
 
     CK(ctx->dPairs.ensure(n), "alloc pairs");
@@ -787,7 +792,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                     gk.chunks = ctx->dChunks.p + G.chunkBase + k;
                     gk.nChunks = 1;
                     gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
-                    G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk);
+                    G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
                     ++launches;
                 }
             } else {
@@ -795,7 +800,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                 gk.chunks = ctx->dChunks.p + G.chunkBase;
                 gk.nChunks = (int)G.chunks.size();
                 gk.chunkCounter = ctx->dCounter.p + gi;
-                G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk);
+                G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
                 ++launches;
             }
             CK(cudaGetLastError(), "DP kernel");

@@ -10,6 +10,12 @@
 // crossing from one stripe to the next go through a small per-warp ring in
 // global memory.  Per pair there is one fill and one drain of 31 steps.
 //
+// Per-column operands (codon code, background, seeds, and the ring values of
+// the stripe boundary) are staged in a per-warp shared-memory window indexed
+// by lane-local time, refilled once every 32 steps by one coalesced load per
+// lane; a step reads its column with one 16-byte shared load.  The forward
+// reads W1 two steps ahead into registers.
+//
 // The recurrences are the reference's, term for term and in the same
 // association order (so that the float rounding matches):
 //   backward  dummest-dp-backward.hh:473-574 (and the float filter :367-430)
@@ -23,13 +29,13 @@
 // exceed RESCALE_THRESH.  It reports the largest backward Y (Y >= W1 at every
 // cell) and the largest forward W0/Y0, so the host can tell whether the
 // reference would have rescaled; such pairs are re-scored by the exact
-// row-rescaled kernel (dp_exact.cuh).
+// row-rescaled path (dp_exact_wave.cuh).
 //
 // Mid score.  The reference forms promote(W0)*promote(W1) in double and
 // rounds the mantissa to float (dummest-batch.hh:216-235); with both counts
 // zero that is the float product W0*W1 whenever it is a normal float, so the
 // per-cell product is one FMUL.  Overflow (a score above 2^128) is reported
-// as +inf and routed to the exact kernel.
+// as +inf and routed to the exact path.
 #pragma once
 
 #include "dp_common.cuh"
@@ -129,6 +135,8 @@ __device__ __forceinline__ void storeW1(float *p, const float (&w)[R]) {
     }
 }
 
+// W1 values are read once, by the warp that wrote them: bypass L1 (the slot is
+// rewritten by the warp's next pair).
 template <int R>
 __device__ __forceinline__ void loadW1(float (&w)[R], const float *p) {
     if constexpr (R == 4) {
@@ -142,29 +150,65 @@ __device__ __forceinline__ void loadW1(float (&w)[R], const float *p) {
     }
 }
 
-// Steps of look-ahead for the per-step global operands (codon code, seeds,
-// W1, ring): each step issues the loads of step t + kPF into a register FIFO,
-// so their latency overlaps kPF steps of arithmetic.
-constexpr int kPF = 4;
+// ---------------------------------------------------------------------------
+// Wavefront geometry.  The period P of a lane (steps per stripe) is at least
+// kMinPeriod, so that a stripe-boundary value is written by one lane at least
+// 64 steps before the window refill that hands it to the other lane.
+// ---------------------------------------------------------------------------
+constexpr int kMinPeriod = 96;
+constexpr int kWin = 128;  // window entries (lane-local times), a power of two
 
-// Per-lane position in the wavefront: local time u and (stripe, column).
-struct Cursor {
-    int u, sp, jj;
-    __device__ __forceinline__ void advance(int P) {
-        if (u >= 0 && ++jj == P) {
-            jj = 0;
-            ++sp;
-        }
-        ++u;
-    }
-    __device__ __forceinline__ bool active(int nS, int L) const { return u >= 0 && sp < nS && jj < L; }
+__host__ __device__ inline int wavePeriod(int L) { return L > kMinPeriod ? L : kMinPeriod; }
+
+// Per-warp staging window: entry t & (kWin-1) holds the column operands of
+// lane-local time t.
+struct Window {
+    float4 col[kWin];   // backward: {code, bg, suf, pre}; forward: {code, bg*sC, pre, unused}
+    float2 ring[kWin];  // stripe-boundary (W, Y) for the lane that reads the ring
 };
 
+// Backward window entry for local time u (the column of u is L-1 - u mod P).
+__device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int u) {
+    const int e = u & (kWin - 1);
+    float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
+    float2 r = make_float2(0.0f, 0.0f);
+    if (u >= 0 && u < a.nS * a.P) {
+        const int sp = u / a.P, jj = u - sp * a.P;
+        if (jj < a.L) {
+            const int j = a.L - 1 - jj;
+            const int code = (j + 1 < a.L) ? (int)__ldg(a.codes + j + 1) : kPad;
+            c = make_float4(__int_as_float(code), a.smBg[code], __ldg(a.suf + j), __ldg(a.pre + j));
+            if (sp > 0) r = __ldcg(reinterpret_cast<const float2 *>(a.ring) + jj);
+        }
+    }
+    w.col[e] = c;
+    w.ring[e] = r;
+}
+
+// Forward window entry for local time u (the column of u is u mod P).
+__device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u) {
+    const int e = u & (kWin - 1);
+    float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
+    float2 r = make_float2(0.0f, 0.0f);
+    if (u >= 0 && u < a.nS * a.P) {
+        const int s = u / a.P, j = u - s * a.P;
+        if (j < a.L) {
+            const int code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
+            c = make_float4(__int_as_float(code), a.smBg[code] * a.sc.sC, __ldg(a.pre + j), 0.0f);
+            if (s > 0) r = __ldcg(reinterpret_cast<const float2 *>(a.ring) + j);
+        }
+    }
+    w.col[e] = c;
+    w.ring[e] = r;
+}
+
+// ---------------------------------------------------------------------------
 // Backward sweep.  STORE: keep W1 for the forward sweep (mid mode); without
 // it this is the lean float filter (findSimilaritiesBackwardOnly), whose
 // arithmetic is the same with every rescale count at zero.
+// ---------------------------------------------------------------------------
 template <int R, bool STORE>
-__device__ void backwardSweep(const SweepArgs &a, int lane, float &filtOut, float &maxYOut) {
+__device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &filtOut, float &maxYOut) {
     constexpr int S = kLanes * R;
     Coef<R> c;
     float h1[R], h2[R], h3[R], z1[R], z2[R], z3[R];
@@ -174,251 +218,233 @@ __device__ void backwardSweep(const SweepArgs &a, int lane, float &filtOut, floa
     float sendW = 0.0f, sendY = 0.0f;
     float filt = 0.0f, maxY = 0.0f;
     const int L = a.L, P = a.P, nS = a.nS;
-    const int T = nS * P + (kLanes - 1);
-    const bool ringAhead = P > kLanes + kPF;  // ring entries are written > kPF steps before use
-    Cursor cur{-(kLanes - 1 - lane), 0, 0}, ahead = cur;
-    int qc[kPF];
-    float qs[kPF], qp[kPF], qw[kPF], qy[kPF];
-    auto fetch = [&](const Cursor &x, int &code, float &suf, float &pre, float &rw, float &ry) {
-        code = kPad;
-        suf = pre = rw = ry = 0.0f;
-        if (x.active(nS, L)) {
-            const int j = L - 1 - x.jj;
-            code = (j + 1 < L) ? (int)__ldg(a.codes + j + 1) : kPad;
-            suf = __ldg(a.suf + j);
-            pre = __ldg(a.pre + j);
-            if (ringAhead && lane == kLanes - 1 && x.sp > 0) {
-                rw = __ldcg(a.ring + 2 * x.jj);
-                ry = __ldcg(a.ring + 2 * x.jj + 1);
-            }
-        }
-    };
-#pragma unroll
-    for (int k = 0; k < kPF; ++k) {
-        fetch(ahead, qc[k], qs[k], qp[k], qw[k], qy[k]);
-        ahead.advance(P);
-    }
-    for (int t = 0; t < T; ++t) {
-        int nc;
-        float ns, np, nw, ny;
-        fetch(ahead, nc, ns, np, nw, ny);
-        ahead.advance(P);
-        float inW = __shfl_down_sync(kFull, sendW, 1);
-        float inY = __shfl_down_sync(kFull, sendY, 1);
-        if (cur.active(nS, L)) {
-            const int sp = cur.sp, jj = cur.jj;
-            const int s = nS - 1 - sp;
-            const int rowBase = s * S + lane * R;
-            if (jj == 0) {
-                loadBackwardCoef<R>(c, a, rowBase);
-#pragma unroll
-                for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
-                rb1 = rb2 = rb3 = 0.0f;
-            }
-            if (lane == kLanes - 1) {
-                if (sp == 0) {
-                    inW = inY = 0.0f;
-                } else if (ringAhead) {
-                    inW = qw[0];
-                    inY = qy[0];
-                } else {
-                    inW = __ldcg(a.ring + 2 * jj);
-                    inY = __ldcg(a.ring + 2 * jj + 1);
-                }
-            }
-            const int code = qc[0];
-            const float bgv = a.smBg[code];
-            float e[R];
-            loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
-            const float sufv = qs[0];
-            const float prev = qp[0];
-            float bW1 = rb1, bW2 = rb2, bW3 = rb3, bY = inY;
-            float wv[R];
-#pragma unroll
-            for (int k = R - 1; k >= 0; --k) {
-                float acc = (bW3 * e[k]) * c.enter[k];
-                acc = __fmaf_rn(bY, c.d0[k], acc);
-                acc = __fmaf_rn(bW2, c.d1[k], acc);
-                acc = __fmaf_rn(bW1, c.d2[k], acc);
-                const float zbg = z3[k] * bgv;
-                acc = __fmaf_rn(zbg, c.a0[k], acc);
-                acc = __fmaf_rn(h2[k], c.a2[k], acc);
-                acc = __fmaf_rn(h1[k], c.a1[k], acc);
-                const float W = __fmaf_rn(sufv, c.rs[k], acc);
-                const float Y = __fmaf_rn(c.eps[k], bY, W);
-                const float Z = __fmaf_rn(c.b0[k], zbg, W);
-                maxY = fmaxf(maxY, Y);
-                filt = fmaxf(filt, W * prev);
-                bW1 = h1[k];
-                bW2 = h2[k];
-                bW3 = h3[k];
-                bY = Y;
-                h3[k] = h2[k];
-                h2[k] = h1[k];
-                h1[k] = W;
-                z3[k] = z2[k];
-                z2[k] = z1[k];
-                z1[k] = Z;
-                wv[k] = W;
-            }
-            rb3 = rb2;
-            rb2 = rb1;
-            rb1 = inW;
-            sendW = wv[0];
-            sendY = bY;
-            if (STORE) {
-                const int d = jj + (kLanes - 1 - lane);
-                storeW1<R>(a.w1 + (((size_t)s * a.D + d) * kLanes + lane) * R, wv);
-            }
-            if (lane == 0 && sp < nS - 1) {
-                __stcg(a.ring + 2 * jj, sendW);
-                __stcg(a.ring + 2 * jj + 1, sendY);
-            }
-        } else {
-            sendW = 0.0f;
-            sendY = 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < kPF - 1; ++k) {
-            qc[k] = qc[k + 1];
-            qs[k] = qs[k + 1];
-            qp[k] = qp[k + 1];
-            qw[k] = qw[k + 1];
-            qy[k] = qy[k + 1];
-        }
-        qc[kPF - 1] = nc;
-        qs[kPF - 1] = ns;
-        qp[kPF - 1] = np;
-        qw[kPF - 1] = nw;
-        qy[kPF - 1] = ny;
-        cur.advance(P);
+    const int total = nS * P;
+    const int T = total + (kLanes - 1);
+    const int lag = kLanes - 1 - lane;  // lane 31 leads
+    int u = -lag;                       // local time
+    int sp = 0, jj = 0;                 // stripe from the bottom, column from the right
+    float *wp = a.w1;                   // W1 store pointer of the current step
+    // Window: local times [0, 64) now, then 32 ahead at every block start.
+    __syncwarp();
+    fillBackward(win, a, lane);
+    fillBackward(win, a, lane + 32);
+    for (int t0 = 0; t0 < T; t0 += 32) {
         __syncwarp();
+        if (t0 > 0) fillBackward(win, a, t0 + 32 + lane);
+        const int tEnd = t0 + 32 < T ? t0 + 32 : T;
+        for (int t = t0; t < tEnd; ++t) {
+            float inW = __shfl_down_sync(kFull, sendW, 1);
+            float inY = __shfl_down_sync(kFull, sendY, 1);
+            if (u >= 0 && u < total && jj < L) {
+                const int s = nS - 1 - sp;
+                const int rowBase = s * S + lane * R;
+                if (jj == 0) {
+                    loadBackwardCoef<R>(c, a, rowBase);
+#pragma unroll
+                    for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
+                    rb1 = rb2 = rb3 = 0.0f;
+                    wp = a.w1 + (((size_t)s * a.D + lag) * kLanes + lane) * R;
+                }
+                const int slot = u & (kWin - 1);
+                const float4 col = win.col[slot];
+                if (lane == kLanes - 1) {
+                    const float2 r = win.ring[slot];
+                    inW = r.x;
+                    inY = r.y;
+                }
+                const int code = __float_as_int(col.x);
+                const float bgv = col.y, sufv = col.z, prev = col.w;
+                float e[R];
+                loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
+                float bW1 = rb1, bW2 = rb2, bW3 = rb3, bY = inY;
+                float wv[R];
+#pragma unroll
+                for (int k = R - 1; k >= 0; --k) {
+                    float acc = (bW3 * e[k]) * c.enter[k];
+                    acc = __fmaf_rn(bY, c.d0[k], acc);
+                    acc = __fmaf_rn(bW2, c.d1[k], acc);
+                    acc = __fmaf_rn(bW1, c.d2[k], acc);
+                    const float zbg = z3[k] * bgv;
+                    acc = __fmaf_rn(zbg, c.a0[k], acc);
+                    acc = __fmaf_rn(h2[k], c.a2[k], acc);
+                    acc = __fmaf_rn(h1[k], c.a1[k], acc);
+                    const float W = __fmaf_rn(sufv, c.rs[k], acc);
+                    const float Y = __fmaf_rn(c.eps[k], bY, W);
+                    const float Z = __fmaf_rn(c.b0[k], zbg, W);
+                    maxY = fmaxf(maxY, Y);
+                    filt = fmaxf(filt, W * prev);
+                    bW1 = h1[k];
+                    bW2 = h2[k];
+                    bW3 = h3[k];
+                    bY = Y;
+                    h3[k] = h2[k];
+                    h2[k] = h1[k];
+                    h1[k] = W;
+                    z3[k] = z2[k];
+                    z2[k] = z1[k];
+                    z1[k] = Z;
+                    wv[k] = W;
+                }
+                rb3 = rb2;
+                rb2 = rb1;
+                rb1 = inW;
+                sendW = wv[0];
+                sendY = bY;
+                if (STORE) {
+                    storeW1<R>(wp, wv);
+                    wp += kLanes * R;
+                }
+                if (lane == 0 && sp < nS - 1) __stcg(reinterpret_cast<float2 *>(a.ring) + jj, make_float2(sendW, sendY));
+            } else {
+                sendW = 0.0f;
+                sendY = 0.0f;
+            }
+            if (u >= 0 && ++jj == P) {
+                jj = 0;
+                ++sp;
+            }
+            ++u;
+        }
     }
     filtOut = filt;
     maxYOut = maxY;
 }
 
-// Forward sweep with the mid-anchored product (reads W1 written above).
+// W1 read-ahead for the forward sweep: a cursor two steps ahead of the lane.
 template <int R>
-__device__ void forwardSweep(const SweepArgs &a, int lane, float &bestOut, float &maxOut) {
-    constexpr int S = kLanes * R;
+struct W1Ahead {
+    int u, s, j;
+    __device__ __forceinline__ void next(const SweepArgs &a, int lane, int total, float (&q)[R]) {
+        if (u >= 0 && u < total && j < a.L) {
+            const int db = (a.L - 1 - j) + (kLanes - 1 - lane);
+            loadW1<R>(q, a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
+        }
+        if (u >= 0 && ++j == a.P) {
+            j = 0;
+            ++s;
+        }
+        ++u;
+    }
+};
+
+// One forward step of a lane; q holds the W1 values of this step.
+template <int R>
+struct FwdState {
     Coef<R> c;
     float w1[R], w2[R], w3[R], z1[R], z2[R], z3[R];
+    float sendIn, sendY, best, mx;
+    int u, s, j;
+};
+
+template <int R>
+__device__ __forceinline__ void forwardStep(FwdState<R> &f, const SweepArgs &a, Window &win, int lane, int total,
+                                            const float (&q)[R]) {
+    constexpr int S = kLanes * R;
+    float inW = __shfl_up_sync(kFull, f.sendIn, 1);
+    float inY = __shfl_up_sync(kFull, f.sendY, 1);
+    if (f.u >= 0 && f.u < total && f.j < a.L) {
+        const int rowBase = f.s * S + lane * R;
+        if (f.j == 0) {
+            loadForwardCoef<R>(f.c, a, rowBase);
 #pragma unroll
-    for (int k = 0; k < R; ++k) w1[k] = w2[k] = w3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
-    float sendIn = 0.0f, sendY = 0.0f;
-    float best = 0.0f, mx = 0.0f;
-    const int L = a.L, P = a.P, nS = a.nS;
-    const int T = nS * P + (kLanes - 1);
-    const bool ringAhead = P > kLanes + kPF;
-    Cursor cur{-lane, 0, 0}, ahead = cur;
-    int qc[kPF];
-    float qp[kPF], qw[kPF], qy[kPF], qb[kPF][R];
-    auto fetch = [&](const Cursor &x, int &code, float &pre, float &rw, float &ry, float (&wb)[R]) {
-        code = kPad;
-        pre = rw = ry = 0.0f;
-#pragma unroll
-        for (int k = 0; k < R; ++k) wb[k] = 0.0f;
-        if (x.active(nS, L)) {
-            const int s = x.sp, j = x.jj;
-            code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
-            pre = __ldg(a.pre + j);
-            const int db = (L - 1 - j) + (kLanes - 1 - lane);
-            loadW1<R>(wb, a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
-            if (ringAhead && lane == 0 && s > 0) {
-                rw = __ldcg(a.ring + 2 * j);
-                ry = __ldcg(a.ring + 2 * j + 1);
-            }
+            for (int k = 0; k < R; ++k) f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
         }
-    };
+        const int slot = f.u & (kWin - 1);
+        const float4 col = win.col[slot];
+        if (lane == 0) {
+            const float2 r = win.ring[slot];
+            inW = r.x;
+            inY = r.y;
+        }
+        const int code = __float_as_int(col.x);
+        const float bgsC = col.y, prev = col.z;
+        float e[R];
+        loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
+        float win0 = inW, yab = inY;
 #pragma unroll
-    for (int k = 0; k < kPF; ++k) {
-        fetch(ahead, qc[k], qp[k], qw[k], qy[k], qb[k]);
-        ahead.advance(P);
+        for (int k = 0; k < R; ++k) {
+            const float X = (f.c.enter[k] * e[k]) * f.w3[k];
+            const float Z0 = bgsC * __fmaf_rn(f.c.a0[k], f.w3[k], f.c.b0[k] * f.z3[k]);
+            const float Z1 = f.c.a1[k] * f.w1[k];
+            const float Z2 = f.c.a2[k] * f.w2[k];
+            const float W0 = win0 + __fmaf_rn(prev, f.c.rs[k], (Z0 + Z1) + Z2);
+            f.best = fmaxf(f.best, W0 * q[k]);
+            const float Y0 = __fmaf_rn(f.c.d0[k], W0, f.c.eps[k] * yab);
+            f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
+            const float nin = __fmaf_rn(f.c.d2[k], f.w1[k], __fmaf_rn(f.c.d1[k], f.w2[k], X + Y0));
+            f.w3[k] = f.w2[k];
+            f.w2[k] = f.w1[k];
+            f.w1[k] = W0;
+            f.z3[k] = f.z2[k];
+            f.z2[k] = f.z1[k];
+            f.z1[k] = Z0;
+            win0 = nin;
+            yab = Y0;
+        }
+        f.sendIn = win0;
+        f.sendY = yab;
+        if (lane == kLanes - 1 && f.s < a.nS - 1)
+            __stcg(reinterpret_cast<float2 *>(a.ring) + f.j, make_float2(f.sendIn, f.sendY));
+    } else {
+        f.sendIn = 0.0f;
+        f.sendY = 0.0f;
     }
-    for (int t = 0; t < T; ++t) {
-        int nc;
-        float np, nw, ny, nb[R];
-        fetch(ahead, nc, np, nw, ny, nb);
-        ahead.advance(P);
-        float inW = __shfl_up_sync(kFull, sendIn, 1);
-        float inY = __shfl_up_sync(kFull, sendY, 1);
-        if (cur.active(nS, L)) {
-            const int s = cur.sp, j = cur.jj;
-            const int rowBase = s * S + lane * R;
-            if (j == 0) {
-                loadForwardCoef<R>(c, a, rowBase);
+    if (f.u >= 0 && ++f.j == a.P) {
+        f.j = 0;
+        ++f.s;
+    }
+    ++f.u;
+}
+
+// ---------------------------------------------------------------------------
+// Forward sweep with the mid-anchored product (reads W1 written above).
+// ---------------------------------------------------------------------------
+template <int R>
+__device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &bestOut, float &maxOut) {
+    FwdState<R> f;
 #pragma unroll
-                for (int k = 0; k < R; ++k) w1[k] = w2[k] = w3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
-            }
-            if (lane == 0) {
-                if (s == 0) {
-                    inW = inY = 0.0f;
-                } else if (ringAhead) {
-                    inW = qw[0];
-                    inY = qy[0];
-                } else {
-                    inW = __ldcg(a.ring + 2 * j);
-                    inY = __ldcg(a.ring + 2 * j + 1);
-                }
-            }
-            const int code = qc[0];
-            const float bgsC = a.smBg[code] * a.sc.sC;
-            float e[R];
-            loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
-            const float prev = qp[0];
-            float win = inW, yab = inY;
+    for (int k = 0; k < R; ++k) f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
+    f.sendIn = f.sendY = f.best = f.mx = 0.0f;
+    f.u = -lane;  // lane 0 leads
+    f.s = f.j = 0;
+    const int total = a.nS * a.P;
+    const int T = total + (kLanes - 1);
+    W1Ahead<R> ah{-lane, 0, 0};
+    float qa[R], qb[R];
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                const float X = (c.enter[k] * e[k]) * w3[k];
-                const float Z0 = bgsC * __fmaf_rn(c.a0[k], w3[k], c.b0[k] * z3[k]);
-                const float Z1 = c.a1[k] * w1[k];
-                const float Z2 = c.a2[k] * w2[k];
-                const float W0 = win + __fmaf_rn(prev, c.rs[k], (Z0 + Z1) + Z2);
-                mx = fmaxf(mx, W0);
-                best = fmaxf(best, W0 * qb[0][k]);
-                const float Y0 = __fmaf_rn(c.d0[k], W0, c.eps[k] * yab);
-                mx = fmaxf(mx, Y0);
-                const float nin = __fmaf_rn(c.d2[k], w1[k], __fmaf_rn(c.d1[k], w2[k], X + Y0));
-                w3[k] = w2[k];
-                w2[k] = w1[k];
-                w1[k] = W0;
-                z3[k] = z2[k];
-                z2[k] = z1[k];
-                z1[k] = Z0;
-                win = nin;
-                yab = Y0;
-            }
-            sendIn = win;
-            sendY = yab;
-            if (lane == kLanes - 1 && s < nS - 1) {
-                __stcg(a.ring + 2 * j, sendIn);
-                __stcg(a.ring + 2 * j + 1, sendY);
-            }
-        } else {
-            sendIn = 0.0f;
-            sendY = 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < kPF - 1; ++k) {
-            qc[k] = qc[k + 1];
-            qp[k] = qp[k + 1];
-            qw[k] = qw[k + 1];
-            qy[k] = qy[k + 1];
-#pragma unroll
-            for (int r = 0; r < R; ++r) qb[k][r] = qb[k + 1][r];
-        }
-        qc[kPF - 1] = nc;
-        qp[kPF - 1] = np;
-        qw[kPF - 1] = nw;
-        qy[kPF - 1] = ny;
-#pragma unroll
-        for (int r = 0; r < R; ++r) qb[kPF - 1][r] = nb[r];
-        cur.advance(P);
+    for (int k = 0; k < R; ++k) qa[k] = qb[k] = 0.0f;
+    ah.next(a, lane, total, qa);
+    ah.next(a, lane, total, qb);
+    __syncwarp();
+    fillForward(win, a, lane);
+    fillForward(win, a, lane + 32);
+    for (int t0 = 0; t0 < T; t0 += 32) {
         __syncwarp();
+        if (t0 > 0) fillForward(win, a, t0 + 32 + lane);
+        // T counts whole blocks of 32 steps except the last; an odd tail
+        // step is handled after the pairwise loop.
+        const int n = (t0 + 32 < T ? 32 : T - t0);
+        int k = 0;
+        for (; k + 1 < n; k += 2) {
+            forwardStep<R>(f, a, win, lane, total, qa);
+            ah.next(a, lane, total, qa);
+            forwardStep<R>(f, a, win, lane, total, qb);
+            ah.next(a, lane, total, qb);
+        }
+        if (k < n) {
+            forwardStep<R>(f, a, win, lane, total, qa);
+            ah.next(a, lane, total, qa);
+            // the next step reads qb, then qa: swap roles to keep the order
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float x = qa[r];
+                qa[r] = qb[r];
+                qb[r] = x;
+            }
+        }
     }
-    bestOut = best;
-    maxOut = mx;
+    bestOut = f.best;
+    maxOut = f.mx;
 }
 
 __device__ __forceinline__ float warpMax(float v) {
@@ -446,8 +472,8 @@ struct DpArgs {
 };
 
 template <int R, bool MID>
-__device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad, const float *smBg, float *w1,
-                          float *ring, int lane) {
+__device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad, const float *smBg, Window &win,
+                          float *w1, float *ring, int lane) {
     const DevPair p = g.pairs[pi];
     SweepArgs a;
     a.codes = g.codes + p.codeOff;
@@ -463,11 +489,11 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     a.M = p.M;
     a.rowPad = rowPad;
     a.nS = (p.M + 1 + kLanes * R - 1) / (kLanes * R);
-    a.P = p.L > kLanes ? p.L : kLanes;
+    a.P = wavePeriod(p.L);
     a.D = a.P + kLanes - 1;
     float filt, maxYb, mid = 0.0f, maxFw = 0.0f;
-    backwardSweep<R, MID>(a, lane, filt, maxYb);
-    if (MID) forwardSweep<R>(a, lane, mid, maxFw);
+    backwardSweep<R, MID>(a, win, lane, filt, maxYb);
+    if (MID) forwardSweep<R>(a, win, lane, mid, maxFw);
     filt = warpMax(filt);
     maxYb = warpMax(maxYb);
     mid = warpMax(mid);
@@ -482,29 +508,30 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     }
 }
 
-// Warps per CTA by rows per lane: tall profiles (R = 4) carry the largest
-// shared emission tables, so more warps share one copy.
-template <int R>
-struct KernelShape {
-    static constexpr int warps = R == 4 ? 6 : 4;
-    static constexpr int minBlocks = R == 4 ? 2 : 3;
-};
+// CTA shape: kCtaWarps warps share one shared-memory copy of the profile's
+// emission table; at most 128 registers per thread.
+#ifndef DMST_CTA_WARPS
+#define DMST_CTA_WARPS 16
+#endif
+constexpr int kCtaWarps = DMST_CTA_WARPS;
 
 // Persistent kernel for one rows-per-lane value: CTAs pull chunks
 // (same-profile runs of pairs, costliest first) from a global counter, stage
 // the chunk's profile emission table in shared memory, and their warps pull
-// pairs from the chunk.
+// pairs from the chunk.  Dynamic shared memory: the table (tableFloats), then
+// one Window per warp.
 template <int R, bool MID>
-__global__ void __launch_bounds__(KernelShape<R>::warps * kLanes, KernelShape<R>::minBlocks) dpKernel(DpArgs g) {
-    constexpr int NW = KernelShape<R>::warps;
+__global__ void __launch_bounds__(kCtaWarps * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
     extern __shared__ float4 smRaw[];
     float *smE = reinterpret_cast<float *>(smRaw);
+    Window *wins = reinterpret_cast<Window *>(smE + tableFloats);
     __shared__ float smBg[32];
     __shared__ int smChunk, smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t slot = (size_t)blockIdx.x * NW + warp;
+    const size_t slot = (size_t)blockIdx.x * kCtaWarps + warp;
     float *w1 = g.w1 + slot * g.w1SlotFloats;
     float *ring = g.ring + slot * g.ringSlotFloats;
+    Window &win = wins[warp];
     int loaded = -1;
     for (;;) {
         if (threadIdx.x == 0) {
@@ -530,7 +557,7 @@ __global__ void __launch_bounds__(KernelShape<R>::warps * kLanes, KernelShape<R>
             if (lane == 0) k = atomicAdd(&smNext, 1);
             k = __shfl_sync(kFull, k, 0);
             if (k >= ch.count) break;
-            scorePair<R, MID>(g, ch.first + k, smE, rowPad, smBg, w1, ring, lane);
+            scorePair<R, MID>(g, ch.first + k, smE, rowPad, smBg, win, w1, ring, lane);
         }
         __syncthreads();
     }
