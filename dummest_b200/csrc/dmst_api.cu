@@ -664,7 +664,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const size_t P = (size_t)wavePeriod(d.L);
         const size_t D = P + kLanes - 1;
         if (mid) w1Max = std::max(w1Max, nS * D * (size_t)S);
-        ringMax = std::max(ringMax, 2 * P);
+        ringMax = std::max(ringMax, 4 * P);
     }
     // Kernel groups by rows per lane (fixed per profile).  Chunks: runs of up to
     // 2 x warps pairs of one profile, costliest first within each group.
@@ -832,7 +832,8 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         eo.resize(flagged.size());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         if (!sequentialExact)
-            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(smem + sizeof(Window))),
                "smem attribute");
         size_t i0 = 0;
         while (i0 < flagged.size()) {
@@ -870,9 +871,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                                    cudaMemcpyHostToDevice, ctx->stream),
                    "upload jobs");
                 const int blocks = (int)std::min<size_t>(nj, (size_t)ctx->smCount * 16);
-                exactWaveKernel<<<blocks, kLanes, smem, ctx->stream>>>(
+                exactWaveKernel<<<blocks, kLanes, smem + sizeof(Window), ctx->stream>>>(
                     ctx->dWaveJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
+                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p,
+                    kNumCodes * ctx->maxRowPad);
             }
             CK(cudaGetLastError(), "exact kernel");
             ++launches;

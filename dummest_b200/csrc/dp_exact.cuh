@@ -13,11 +13,10 @@
 #pragma once
 
 #include "dp_common.cuh"
+#include "dp_wavefront.cuh"
 #include "null_model.cuh"
 
 namespace dmst {
-
-constexpr int kRescaleBits = 64;  // RESCALE_BITS (dummest-score.hh:83)
 
 __device__ __forceinline__ int clampCount(int c) {
     return c > 1000000 ? 1000000 : (c < -1000000 ? -1000000 : c);

@@ -50,7 +50,7 @@ struct SweepArgs {
     const float *smE;       // emission table in shared memory, [25][rowPad]
     const float *smBg;      // bg_probs[4 + c] in shared memory
     float *w1;              // this warp's W1 slot
-    float *ring;            // this warp's stripe-boundary ring (2 floats per column)
+    float *ring;            // this warp's stripe-boundary ring (4 floats per column)
     PairScales sc;
     int L, M, rowPad, nS, P, D;
 };
@@ -164,21 +164,32 @@ __host__ __device__ inline int wavePeriod(int L) { return L > kMinPeriod ? L : k
 // lane-local time t.
 struct Window {
     float4 col[kWin];   // backward: {code, bg, suf, pre}; forward: {code, bg*sC, pre, unused}
-    float2 ring[kWin];  // stripe-boundary (W, Y) for the lane that reads the ring
+    float4 ring[kWin];  // stripe-boundary (W, Y, scale count) for the lane that reads the ring
 };
+
+// The stripe-boundary ring in global memory: 4 floats per column.
+__device__ __forceinline__ float4 ringLoad(const float *ring, int col) {
+    return __ldcg(reinterpret_cast<const float4 *>(ring) + col);
+}
+__device__ __forceinline__ void ringStore(float *ring, int col, float w, float y, int cnt) {
+    __stcg(reinterpret_cast<float4 *>(ring) + col, make_float4(w, y, __int_as_float(cnt), 0.0f));
+}
+__device__ __forceinline__ void ringStore(float *ring, int col, float w, float y) {
+    __stcg(reinterpret_cast<float2 *>(ring) + 2 * col, make_float2(w, y));
+}
 
 // Backward window entry for local time u (the column of u is L-1 - u mod P).
 __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
     float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
-    float2 r = make_float2(0.0f, 0.0f);
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (u >= 0 && u < a.nS * a.P) {
         const int sp = u / a.P, jj = u - sp * a.P;
         if (jj < a.L) {
             const int j = a.L - 1 - jj;
             const int code = (j + 1 < a.L) ? (int)__ldg(a.codes + j + 1) : kPad;
             c = make_float4(__int_as_float(code), a.smBg[code], __ldg(a.suf + j), __ldg(a.pre + j));
-            if (sp > 0) r = __ldcg(reinterpret_cast<const float2 *>(a.ring) + jj);
+            if (sp > 0) r = ringLoad(a.ring, jj);
         }
     }
     w.col[e] = c;
@@ -189,13 +200,13 @@ __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int 
 __device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
     float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
-    float2 r = make_float2(0.0f, 0.0f);
+    float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (u >= 0 && u < a.nS * a.P) {
         const int s = u / a.P, j = u - s * a.P;
         if (j < a.L) {
             const int code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
             c = make_float4(__int_as_float(code), a.smBg[code] * a.sc.sC, __ldg(a.pre + j), 0.0f);
-            if (s > 0) r = __ldcg(reinterpret_cast<const float2 *>(a.ring) + j);
+            if (s > 0) r = ringLoad(a.ring, j);
         }
     }
     w.col[e] = c;
@@ -203,20 +214,86 @@ __device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u
 }
 
 // ---------------------------------------------------------------------------
-// Backward sweep.  STORE: keep W1 for the forward sweep (mid mode); without
-// it this is the lean float filter (findSimilaritiesBackwardOnly), whose
-// arithmetic is the same with every rescale count at zero.
+// Sweep modes.
+//   kFilter    fast backward, no W1 kept: findSimilaritiesBackwardOnly
+//   kMid       fast backward keeping W1 / fast forward with the float mid
+//   kDiscover  exact path, pass 1: per-lane scale counts, row maxima
+//   kReplay    exact path, pass 2: the reference's counts, exact maxima
+// The fast modes compute with every rescale count at zero.
 // ---------------------------------------------------------------------------
-template <int R, bool STORE>
-__device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &filtOut, float &maxYOut) {
+enum SweepMode { kFilter = 0, kMid = 1, kDiscover = 2, kReplay = 3 };
+
+constexpr float kBump = 0x1p100f;  // discovery: rescale a lane above this
+constexpr float kStep = 0x1p-64f;  // one rescale step, RESCALE_STEP (dummest-score.hh:87)
+constexpr int kRescaleBits = 64;   // RESCALE_BITS (dummest-score.hh:83)
+
+__device__ __forceinline__ float stepsDown(int d) {  // 2^(-64 d), d >= 0; 0 past float range
+    return d == 0 ? 1.0f : (d == 1 ? kStep : 0.0f);
+}
+
+// Seed coefficient at scale count c: scale * 2^(-64 c) as the float the
+// reference builds (rowRescaleVector, dummest-score.hh:145-152; FTZ makes it 0
+// from c = 2 on).
+__device__ __forceinline__ float seedCoef(bool realRow, int c) {
+    return realRow ? (c == 0 ? 1.0f : (c == 1 ? kStep : 0.0f)) : 0.0f;
+}
+
+// Exact (double mantissa, binary exponent) maximum of the exact path.
+struct ExactBest {
+    double m;
+    int e;
+};
+
+__device__ __forceinline__ void foldBest(ExactBest &b, double v, int countSum) {
+    if (!(v > 0.0)) return;
+    int e;
+    const double m = frexp(v, &e);
+    e += kRescaleBits * countSum;
+    if (b.m == 0.0 || e > b.e || (e == b.e && m > b.m)) {
+        b.m = m;
+        b.e = e;
+    }
+}
+
+// Per-pair rows of the exact path (global scratch).
+struct ExactRows {
+    float *rowMax;  // M+1: discovery row maxima
+    int *rowCnt;    // M+1: discovery counts at the row ends
+    int *cntB;      // M+2: reference backward counts, cntB[M+1] = 0
+    int *cntF;      // M+2: reference forward counts, cntF[i+1] = row i, cntF[0] = 0
+};
+
+// ---------------------------------------------------------------------------
+// Backward sweep (dummest-dp-backward.hh:473-574; the float filter :367-430).
+// ---------------------------------------------------------------------------
+template <int R, int MODE>
+__device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &filtOut, float &maxYOut,
+                              const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
     constexpr int S = kLanes * R;
+    constexpr bool kStore = MODE == kMid || MODE == kReplay;
     Coef<R> c;
     float h1[R], h2[R], h3[R], z1[R], z2[R], z3[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
     float rb1 = 0.0f, rb2 = 0.0f, rb3 = 0.0f;  // row below (other lane) at j+1..j+3
     float sendW = 0.0f, sendY = 0.0f;
+    int sendC = 0;
     float filt = 0.0f, maxY = 0.0f;
+    // exact-path state
+    int cnt = 0;                  // discovery: this lane's scale count
+    float rmax[R];                // discovery: per-row maxima at count cnt
+    int cOut[R];                  // replay: count of each row after its decision
+    float fOut[R];                // replay: 1 or 2^-64, the row's own rescale
+    double rowBest[R];            // replay: per-row max of W1 * prefixSeed
+    if constexpr (MODE == kDiscover || MODE == kReplay) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            rmax[k] = 0.0f;
+            cOut[k] = 0;
+            fOut[k] = 1.0f;
+            rowBest[k] = 0.0;
+        }
+    }
     const int L = a.L, P = a.P, nS = a.nS;
     const int total = nS * P;
     const int T = total + (kLanes - 1);
@@ -235,6 +312,8 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
         for (int t = t0; t < tEnd; ++t) {
             float inW = __shfl_down_sync(kFull, sendW, 1);
             float inY = __shfl_down_sync(kFull, sendY, 1);
+            int inC = 0;
+            if (MODE == kDiscover) inC = __shfl_down_sync(kFull, sendC, 1);
             if (u >= 0 && u < total && jj < L) {
                 const int s = nS - 1 - sp;
                 const int rowBase = s * S + lane * R;
@@ -244,13 +323,50 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
                     for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
                     rb1 = rb2 = rb3 = 0.0f;
                     wp = a.w1 + (((size_t)s * a.D + lag) * kLanes + lane) * R;
+                    if (MODE == kDiscover) {
+                        cnt = 0;
+#pragma unroll
+                        for (int k = 0; k < R; ++k) rmax[k] = 0.0f;
+                    }
+                    if (MODE == kReplay) {
+#pragma unroll
+                        for (int k = 0; k < R; ++k) {
+                            const int i = rowBase + k;
+                            const int ci = i <= a.M ? i : a.M + 1;
+                            const int cIn = x->cntB[ci + 1 <= a.M + 1 ? ci + 1 : a.M + 1];
+                            cOut[k] = x->cntB[ci];
+                            fOut[k] = stepsDown(cOut[k] - cIn);
+                            c.rs[k] = seedCoef(i <= a.M, cIn);
+                            rowBest[k] = 0.0;
+                        }
+                    }
                 }
                 const int slot = u & (kWin - 1);
                 const float4 col = win.col[slot];
                 if (lane == kLanes - 1) {
-                    const float2 r = win.ring[slot];
+                    const float4 r = win.ring[slot];
                     inW = r.x;
                     inY = r.y;
+                    if (MODE == kDiscover) inC = __float_as_int(r.z);
+                }
+                if (MODE == kDiscover) {
+                    // Align the incoming values and this lane to one scale.
+                    if (inC > cnt) {
+                        const float f = stepsDown(inC - cnt);
+#pragma unroll
+                        for (int k = 0; k < R; ++k) {
+                            h1[k] *= f; h2[k] *= f; h3[k] *= f;
+                            z1[k] *= f; z2[k] *= f; z3[k] *= f;
+                            rmax[k] *= f;
+                            c.rs[k] = seedCoef(rowBase + k <= a.M, inC);
+                        }
+                        rb1 *= f; rb2 *= f; rb3 *= f;
+                        cnt = inC;
+                    } else if (inC < cnt) {
+                        const float f = stepsDown(cnt - inC);
+                        inW *= f;
+                        inY *= f;
+                    }
                 }
                 const int code = __float_as_int(col.x);
                 const float bgv = col.y, sufv = col.z, prev = col.w;
@@ -258,6 +374,7 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
                 loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
                 float bW1 = rb1, bW2 = rb2, bW3 = rb3, bY = inY;
                 float wv[R];
+                float stepMax = 0.0f;
 #pragma unroll
                 for (int k = R - 1; k >= 0; --k) {
                     float acc = (bW3 * e[k]) * c.enter[k];
@@ -271,33 +388,85 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
                     const float W = __fmaf_rn(sufv, c.rs[k], acc);
                     const float Y = __fmaf_rn(c.eps[k], bY, W);
                     const float Z = __fmaf_rn(c.b0[k], zbg, W);
-                    maxY = fmaxf(maxY, Y);
-                    filt = fmaxf(filt, W * prev);
-                    bW1 = h1[k];
-                    bW2 = h2[k];
-                    bW3 = h3[k];
-                    bY = Y;
+                    if (MODE == kFilter || MODE == kMid) {
+                        maxY = fmaxf(maxY, Y);
+                        filt = fmaxf(filt, W * prev);
+                    }
+                    if (MODE == kDiscover) {
+                        rmax[k] = fmaxf(rmax[k], Y);  // Y >= W1 at every cell
+                        stepMax = fmaxf(stepMax, Y);
+                    }
+                    if (MODE == kReplay) {
+                        // What leaves the row is scaled by the row's own decision.
+                        const float Wo = W * fOut[k];
+                        rowBest[k] = fmax(rowBest[k], (double)Wo * (double)prev);
+                        bW1 = h1[k] * fOut[k];
+                        bW2 = h2[k] * fOut[k];
+                        bW3 = h3[k] * fOut[k];
+                        bY = Y * fOut[k];
+                        wv[k] = Wo;
+                    } else {
+                        bW1 = h1[k];
+                        bW2 = h2[k];
+                        bW3 = h3[k];
+                        bY = Y;
+                        wv[k] = W;
+                    }
                     h3[k] = h2[k];
                     h2[k] = h1[k];
                     h1[k] = W;
                     z3[k] = z2[k];
                     z2[k] = z1[k];
                     z1[k] = Z;
-                    wv[k] = W;
                 }
                 rb3 = rb2;
                 rb2 = rb1;
                 rb1 = inW;
                 sendW = wv[0];
                 sendY = bY;
-                if (STORE) {
+                if (MODE == kDiscover) {
+                    if (stepMax > kBump) {
+#pragma unroll
+                        for (int k = 0; k < R; ++k) {
+                            h1[k] *= kStep; h2[k] *= kStep; h3[k] *= kStep;
+                            z1[k] *= kStep; z2[k] *= kStep; z3[k] *= kStep;
+                            rmax[k] *= kStep;
+                            c.rs[k] = seedCoef(rowBase + k <= a.M, cnt + 1);
+                        }
+                        rb1 *= kStep; rb2 *= kStep; rb3 *= kStep;
+                        sendW *= kStep;
+                        sendY *= kStep;
+                        ++cnt;
+                    }
+                    sendC = cnt;
+                }
+                if (kStore) {
                     storeW1<R>(wp, wv);
                     wp += kLanes * R;
                 }
-                if (lane == 0 && sp < nS - 1) __stcg(reinterpret_cast<float2 *>(a.ring) + jj, make_float2(sendW, sendY));
+                if (lane == 0 && sp < nS - 1) {
+                    if (MODE == kDiscover)
+                        ringStore(a.ring, jj, sendW, sendY, sendC);
+                    else
+                        ringStore(a.ring, jj, sendW, sendY);
+                }
+                if (jj == L - 1) {
+                    // the last column of these rows
+#pragma unroll
+                    for (int k = 0; k < R; ++k) {
+                        const int i = rowBase + k;
+                        if (i > a.M) continue;
+                        if (MODE == kDiscover) {
+                            x->rowMax[i] = rmax[k];
+                            x->rowCnt[i] = cnt;
+                        }
+                        if (MODE == kReplay) foldBest(*exact, rowBest[k], cOut[k]);
+                    }
+                }
             } else {
                 sendW = 0.0f;
                 sendY = 0.0f;
+                sendC = 0;
             }
             if (u >= 0 && ++jj == P) {
                 jj = 0;
@@ -327,40 +496,86 @@ struct W1Ahead {
     }
 };
 
-// One forward step of a lane; q holds the W1 values of this step.
-template <int R>
+template <int R, int MODE>
 struct FwdState {
     Coef<R> c;
     float w1[R], w2[R], w3[R], z1[R], z2[R], z3[R];
     float sendIn, sendY, best, mx;
+    int sendC;
     int u, s, j;
+    // exact-path state (see backwardSweep)
+    int cnt;
+    float rmax[R];
+    int cIn[R], cB[R];
+    float fOut[R];
+    double rowBest[R];
 };
 
-template <int R>
-__device__ __forceinline__ void forwardStep(FwdState<R> &f, const SweepArgs &a, Window &win, int lane, int total,
-                                            const float (&q)[R]) {
+// One forward step of a lane (dummest-dp-forward.hh:112-223); q holds the W1
+// values of this step.
+template <int R, int MODE>
+__device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
+                                            int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
     float inW = __shfl_up_sync(kFull, f.sendIn, 1);
     float inY = __shfl_up_sync(kFull, f.sendY, 1);
+    int inC = 0;
+    if (MODE == kDiscover) inC = __shfl_up_sync(kFull, f.sendC, 1);
     if (f.u >= 0 && f.u < total && f.j < a.L) {
         const int rowBase = f.s * S + lane * R;
         if (f.j == 0) {
             loadForwardCoef<R>(f.c, a, rowBase);
 #pragma unroll
             for (int k = 0; k < R; ++k) f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
+            if (MODE == kDiscover) {
+                f.cnt = 0;
+#pragma unroll
+                for (int k = 0; k < R; ++k) f.rmax[k] = 0.0f;
+            }
+            if (MODE == kReplay) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    const int i = rowBase + k;
+                    const int ci = i <= a.M ? i : a.M;
+                    f.cIn[k] = x->cntF[ci];
+                    f.fOut[k] = stepsDown(x->cntF[ci + 1] - f.cIn[k]);
+                    f.cB[k] = x->cntB[ci];
+                    f.c.rs[k] = seedCoef(i <= a.M, f.cIn[k]);
+                    f.rowBest[k] = 0.0;
+                }
+            }
         }
         const int slot = f.u & (kWin - 1);
         const float4 col = win.col[slot];
         if (lane == 0) {
-            const float2 r = win.ring[slot];
+            const float4 r = win.ring[slot];
             inW = r.x;
             inY = r.y;
+            if (MODE == kDiscover) inC = __float_as_int(r.z);
+        }
+        if (MODE == kDiscover) {
+            if (inC > f.cnt) {
+                const float g = stepsDown(inC - f.cnt);
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    f.w1[k] *= g; f.w2[k] *= g; f.w3[k] *= g;
+                    f.z1[k] *= g; f.z2[k] *= g; f.z3[k] *= g;
+                    f.rmax[k] *= g;
+                    f.c.rs[k] = seedCoef(rowBase + k <= a.M, inC);
+                }
+                f.cnt = inC;
+            } else if (inC < f.cnt) {
+                const float g = stepsDown(f.cnt - inC);
+                inW *= g;
+                inY *= g;
+            }
         }
         const int code = __float_as_int(col.x);
         const float bgsC = col.y, prev = col.z;
         float e[R];
         loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
         float win0 = inW, yab = inY;
+        float stepMax = 0.0f;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const float X = (f.c.enter[k] * e[k]) * f.w3[k];
@@ -368,26 +583,68 @@ __device__ __forceinline__ void forwardStep(FwdState<R> &f, const SweepArgs &a, 
             const float Z1 = f.c.a1[k] * f.w1[k];
             const float Z2 = f.c.a2[k] * f.w2[k];
             const float W0 = win0 + __fmaf_rn(prev, f.c.rs[k], (Z0 + Z1) + Z2);
-            f.best = fmaxf(f.best, W0 * q[k]);
+            if (MODE == kMid) f.best = fmaxf(f.best, W0 * q[k]);
+            if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
             const float Y0 = __fmaf_rn(f.c.d0[k], W0, f.c.eps[k] * yab);
-            f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
+            if (MODE == kMid) f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
             const float nin = __fmaf_rn(f.c.d2[k], f.w1[k], __fmaf_rn(f.c.d1[k], f.w2[k], X + Y0));
+            if (MODE == kDiscover) {
+                f.rmax[k] = fmaxf(f.rmax[k], fmaxf(W0, Y0));
+                stepMax = fmaxf(stepMax, fmaxf(fmaxf(W0, Y0), nin));
+            }
             f.w3[k] = f.w2[k];
             f.w2[k] = f.w1[k];
             f.w1[k] = W0;
             f.z3[k] = f.z2[k];
             f.z2[k] = f.z1[k];
             f.z1[k] = Z0;
-            win0 = nin;
-            yab = Y0;
+            if (MODE == kReplay) {
+                win0 = nin * f.fOut[k];
+                yab = Y0 * f.fOut[k];
+            } else {
+                win0 = nin;
+                yab = Y0;
+            }
+        }
+        if (MODE == kDiscover) {
+            if (stepMax > kBump) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    f.w1[k] *= kStep; f.w2[k] *= kStep; f.w3[k] *= kStep;
+                    f.z1[k] *= kStep; f.z2[k] *= kStep; f.z3[k] *= kStep;
+                    f.rmax[k] *= kStep;
+                    f.c.rs[k] = seedCoef(rowBase + k <= a.M, f.cnt + 1);
+                }
+                win0 *= kStep;
+                yab *= kStep;
+                ++f.cnt;
+            }
+            f.sendC = f.cnt;
         }
         f.sendIn = win0;
         f.sendY = yab;
-        if (lane == kLanes - 1 && f.s < a.nS - 1)
-            __stcg(reinterpret_cast<float2 *>(a.ring) + f.j, make_float2(f.sendIn, f.sendY));
+        if (lane == kLanes - 1 && f.s < a.nS - 1) {
+            if (MODE == kDiscover)
+                ringStore(a.ring, f.j, f.sendIn, f.sendY, f.sendC);
+            else
+                ringStore(a.ring, f.j, f.sendIn, f.sendY);
+        }
+        if (f.j == a.L - 1) {
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int i = rowBase + k;
+                if (i > a.M) continue;
+                if (MODE == kDiscover) {
+                    x->rowMax[i] = f.rmax[k];
+                    x->rowCnt[i] = f.cnt;
+                }
+                if (MODE == kReplay) foldBest(*exact, f.rowBest[k], f.cIn[k] + f.cB[k]);
+            }
+        }
     } else {
         f.sendIn = 0.0f;
         f.sendY = 0.0f;
+        f.sendC = 0;
     }
     if (f.u >= 0 && ++f.j == a.P) {
         f.j = 0;
@@ -397,50 +654,56 @@ __device__ __forceinline__ void forwardStep(FwdState<R> &f, const SweepArgs &a, 
 }
 
 // ---------------------------------------------------------------------------
-// Forward sweep with the mid-anchored product (reads W1 written above).
+// Forward sweep (reads W1 written by the backward sweep of the same mode).
 // ---------------------------------------------------------------------------
-template <int R>
-__device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &bestOut, float &maxOut) {
-    FwdState<R> f;
+template <int R, int MODE>
+__device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &bestOut, float &maxOut,
+                             const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
+    FwdState<R, MODE> f;
 #pragma unroll
-    for (int k = 0; k < R; ++k) f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
+    for (int k = 0; k < R; ++k) {
+        f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
+        if constexpr (MODE == kDiscover || MODE == kReplay) {
+            f.rmax[k] = 0.0f;
+            f.cIn[k] = f.cB[k] = 0;
+            f.fOut[k] = 1.0f;
+            f.rowBest[k] = 0.0;
+        }
+    }
     f.sendIn = f.sendY = f.best = f.mx = 0.0f;
+    f.sendC = f.cnt = 0;
     f.u = -lane;  // lane 0 leads
     f.s = f.j = 0;
     const int total = a.nS * a.P;
     const int T = total + (kLanes - 1);
+    constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
     W1Ahead<R> ah{-lane, 0, 0};
     float qa[R], qb[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) qa[k] = qb[k] = 0.0f;
-    ah.next(a, lane, total, qa);
-    ah.next(a, lane, total, qb);
+    if (kReadW1) {
+        ah.next(a, lane, total, qa);
+        ah.next(a, lane, total, qb);
+    }
     __syncwarp();
     fillForward(win, a, lane);
     fillForward(win, a, lane + 32);
     for (int t0 = 0; t0 < T; t0 += 32) {
         __syncwarp();
         if (t0 > 0) fillForward(win, a, t0 + 32 + lane);
-        // T counts whole blocks of 32 steps except the last; an odd tail
-        // step is handled after the pairwise loop.
+        // Blocks are 32 steps (even) except the last; its odd tail step is
+        // handled after the pairwise loop.
         const int n = (t0 + 32 < T ? 32 : T - t0);
         int k = 0;
         for (; k + 1 < n; k += 2) {
-            forwardStep<R>(f, a, win, lane, total, qa);
-            ah.next(a, lane, total, qa);
-            forwardStep<R>(f, a, win, lane, total, qb);
-            ah.next(a, lane, total, qb);
+            forwardStep<R, MODE>(f, a, win, lane, total, qa, x, exact);
+            if (kReadW1) ah.next(a, lane, total, qa);
+            forwardStep<R, MODE>(f, a, win, lane, total, qb, x, exact);
+            if (kReadW1) ah.next(a, lane, total, qb);
         }
         if (k < n) {
-            forwardStep<R>(f, a, win, lane, total, qa);
-            ah.next(a, lane, total, qa);
-            // the next step reads qb, then qa: swap roles to keep the order
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const float x = qa[r];
-                qa[r] = qb[r];
-                qb[r] = x;
-            }
+            forwardStep<R, MODE>(f, a, win, lane, total, qa, x, exact);
+            if (kReadW1) ah.next(a, lane, total, qa);
         }
     }
     bestOut = f.best;
@@ -492,8 +755,12 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     a.P = wavePeriod(p.L);
     a.D = a.P + kLanes - 1;
     float filt, maxYb, mid = 0.0f, maxFw = 0.0f;
-    backwardSweep<R, MID>(a, win, lane, filt, maxYb);
-    if (MID) forwardSweep<R>(a, win, lane, mid, maxFw);
+    if (MID) {
+        backwardSweep<R, kMid>(a, win, lane, filt, maxYb);
+        forwardSweep<R, kMid>(a, win, lane, mid, maxFw);
+    } else {
+        backwardSweep<R, kFilter>(a, win, lane, filt, maxYb);
+    }
     filt = warpMax(filt);
     maxYb = warpMax(maxYb);
     mid = warpMax(mid);
