@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark: batched forward+backward GCUPS of the B200 search path.
+
+Workload (one "step"): a batch of synthetic DNA reads, both strands, scored
+against 64 synthetic profile HMMs (M log-uniform in [50, 800]; reads L
+log-uniform in [150, 3000] nt, GC 0.4-0.6, 10% with implanted frameshifted
+homologs) -- every (record, profile) pair, backward + forward with the
+mid-anchored score, as one call of dmst_score_pairs (one persistent launch per
+rows-per-lane group).  A cell is one (i, j), i in [0, M], j in [0, L), of one
+pair; GCUPS = cells / s / 1e9.
+
+Printed: one JSON line (rank 0).
+  value      device-timed GCUPS with the reads resident in HBM (CUDA events on
+             the library's stream around exactly --steps calls, max over ranks)
+  e2e        the same metric through the public API with host buffers: each
+             step copies its 2-bit packed reads host->device, decodes them on
+             the device, scores, and copies the results back
+  roofline   the dominant kernel (the R=4 mid kernel) against the FP32 issue
+             peak: 52 algorithmic flops per cell (24 backward + 28 forward with
+             the mid product) over its CUDA-event-timed duration
+  plain      the same pairs (a sample) through the plain schedule, one pair per
+             launch, and the batched/plain ratio
+  cpu_baseline  the reference engine itself (oracle/_ref, compiled from the
+             reference sources) on a bounded sample of the same pairs, all host
+             threads
+With --impl reference the reference engine alone runs (rank 0 only) and prints
+the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from datetime import timedelta
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOPS_PER_CELL = 52  # 24 backward + 28 forward with the mid product
+METRIC = "fwd+bwd GCUPS (batched persistent kernel)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--reads-per-step", type=int, default=1024)
+    ap.add_argument("--profiles", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=20261205)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-pairs", type=int, default=48)
+    ap.add_argument("--rows-per-lane", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU, weak scaling: every rank scores
+# its own reads against all profiles; no data-path collective)
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_profiles(seed, n):
+    from dummest_b200 import synth
+    rng = np.random.default_rng(seed)
+    Ms = np.exp(rng.uniform(np.log(50), np.log(800), size=n)).round().astype(int)
+    profiles = [synth.make_profile(rng, int(M), f"synth{k:03d}") for k, M in enumerate(Ms)]
+    return profiles, synth.hmmer3_text(profiles)
+
+
+def make_steps(seed, profiles, n_steps, reads_per_step):
+    from dummest_b200 import synth
+    rng = np.random.default_rng(seed)
+    steps = []
+    for _ in range(n_steps):
+        reads = synth.make_reads(rng, reads_per_step, 150, 3000, profiles, 0.10, gc_range=(0.4, 0.6))
+        steps.append(synth.both_strands(reads))
+    return steps
+
+
+# ---------------------------------------------------------------------------
+# GPU clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        return {}
+
+
+def traffic_per_cell():
+    """DRAM bytes per cell of the mid kernel from the committed ncu summary."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "dp_mid_r4_traffic.json")))["dram_bytes_per_cell"]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference engine (oracle/_ref) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_baseline(hmm_text, records, n_profiles, seconds, seed):
+    from oracle.ref import RefEngine, available
+    if not available(32):
+        return None
+    e = RefEngine(32)
+    e.set_rates()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(hmm_text)
+        path = f.name
+    n = e.load_profiles(path)
+    os.unlink(path)
+    Ms = [e.profile(p)[1].shape[0] for p in range(n)]  # M+1 rows
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    codes = [e.decode(e.encode(r)) for r in records]
+    lens = np.array([len(c) for c in codes], dtype=np.float64)
+    # Every record of the step against profiles in random order until the time
+    # budget is spent: each call hands the reference >= 8 x threads lanes, so
+    # all threads have SIMD batches to run.
+    done_cells, done_s, used = 0.0, 0.0, 0
+    for p in rng.permutation(n):
+        t = time.perf_counter()
+        e.score_many(int(p), codes, threads=threads, mode=0)
+        done_s += time.perf_counter() - t
+        done_cells += Ms[p] * lens.sum()
+        used += 1
+        if done_s >= seconds:
+            break
+    k = len(records)
+    return {
+        "value": done_cells / done_s / 1e9,
+        "unit": "GCUPS",
+        "cores": threads,
+        "kind": "reference",
+        "sample": f"all {k} records of one step (both strands) x {used} of {n} profiles, "
+                  f"{done_cells:.3e} cells in {done_s:.1f} s, reference FP32 engine "
+                  "(findSimilarities needAlign=false, the calibration call) in <=8-lane SIMD batches",
+    }
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    profiles, txt = make_profiles(args.seed, args.profiles)
+    steps = make_steps(args.seed + 1, profiles, 1, args.reads_per_step)
+    vals = []
+    cb = None
+    per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+    for _ in range(args.warmup + args.steps):
+        cb = cpu_baseline(txt, steps[0], args.profiles, per_step, args.seed + len(vals))
+        vals.append(cb["value"])
+    v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else vals[-1]
+    cb["value"] = v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched fwd+bwd, 64 profiles M 50-800 x reads L 150-3000 both strands",
+                   "reads_per_step": args.reads_per_step, "profiles": args.profiles},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import dummest_b200 as d
+    from dummest_b200 import _ffi as F
+    import torch
+
+    profiles, txt = make_profiles(args.seed, args.profiles)
+    n_steps = args.warmup + args.steps
+    steps = make_steps(args.seed + 1 + 1000 * rank, profiles, n_steps, args.reads_per_step)
+    ctx = d.Context(device=local, rows_per_lane=args.rows_per_lane)
+    pids = ctx.load_hmm(txt)
+    Ms = np.array([ctx.profile_length(p) for p in pids])
+
+    def pairs_for(sids):
+        n = len(sids) * len(pids)
+        arr = (F.Pair * n)()
+        k = 0
+        for p in pids:
+            for s in sids:
+                arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
+                k += 1
+        return arr
+
+    # ---- value: reads resident in HBM ----
+    step_sids, step_pairs, step_cells = [], [], []
+    for recs in steps:
+        sids = ctx.add_dna(recs)
+        step_sids.append(sids)
+        step_pairs.append(pairs_for(sids))
+        step_cells.append(float(sum(len(r) for r in recs)) * float((Ms + 1).sum()))
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    for w in range(args.warmup):
+        ctx.score_pairs_raw(step_pairs[w], d.MODE_MID)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    launches, dp_ms, exact_pairs, cells = 0, 0.0, 0, 0.0
+    for k in range(args.warmup, n_steps):
+        res = ctx.score_pairs_raw(step_pairs[k], d.MODE_MID)
+        t = ctx.last_timing()
+        launches += t["launches"]
+        dp_ms += t["dp_ms"]
+        exact_pairs += sum(1 for r in res if r.flags & F.RES_EXACT_PATH)
+        cells += step_cells[k]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = allreduce_max(ms, world)
+    cells_all = allreduce_sum(cells, world)
+    value = cells_all / (ms_max / 1e3) / 1e9
+
+    # ---- roofline of the DP kernels (CUDA-event durations) ----
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = n_sm * 128 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s
+    achieved = cells * FLOPS_PER_CELL / (dp_ms / 1e3) / 1e12
+    tpc = traffic_per_cell()
+    launch_cells = cells / args.steps
+    roofline = {
+        "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+        "traffic": (tpc * launch_cells) if tpc else None,
+        "peak_source": f"derived: {n_sm} SMs x 128 FP32 lanes x 2 x sm_max_mhz {sm_max:g} (of measured clock; "
+                       "MEASURED_PEAKS.json has no FP32 figure)",
+        "kernel": "dpKernel (mid: backward + forward), CUDA events on the library stream, per step",
+        "algorithmic_flops_per_cell": FLOPS_PER_CELL,
+        "hbm_algorithmic_bytes_per_cell": 8,
+        "hbm_frac_of_measured": (8 * cells / (dp_ms / 1e3)) / (peaks.get("hbm_gbs", 6451.2) * 1e9),
+    }
+
+    # ---- e2e: host buffers through the C ABI every step ----
+    packed = [d.pack_dna(recs) for recs in steps]
+    h2d = d2h = 0
+    for w in range(args.warmup):
+        ctx.clear_sequences()
+        words, mask, lens = packed[w]
+        sids = ctx.add_packed(words, lens, mask)
+        ctx.score_pairs_raw(pairs_for(sids), d.MODE_MID)
+    e2e_pairs = [None] * n_steps
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.warmup, n_steps):
+        ctx.clear_sequences()
+        words, mask, lens = packed[k]
+        sids = ctx.add_packed(words, lens, mask)
+        pr = pairs_for(sids)
+        res = ctx.score_pairs_raw(pr, d.MODE_MID)
+        # packed reads + mask + offsets, then the per-pair descriptors the
+        # library uploads (32 B pair + 8 B scratch offset) and the 16-byte
+        # per-pair results it reads back
+        h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 40 * len(pr)
+        d2h += 16 * len(pr)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
+           "d2h_bytes_per_step": d2h // args.steps}
+
+    # ---- plain schedule on a sample of step pairs ----
+    plain = None
+    if rank == 0 and args.plain_pairs > 0:
+        ctx.clear_sequences()
+        recs = steps[args.warmup]
+        sids = ctx.add_dna(recs)
+        rng = np.random.default_rng(args.seed)
+        sel = rng.choice(len(sids) * len(pids), size=min(args.plain_pairs, len(sids) * len(pids)), replace=False)
+        arr = (F.Pair * len(sel))()
+        pc = 0.0
+        for k, idx in enumerate(sel):
+            p, s = pids[idx // len(sids)], sids[idx % len(sids)]
+            arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
+            pc += (Ms[p] + 1) * len(recs[idx % len(sids)])
+        ctx.score_pairs_raw(arr, d.MODE_MID | d.MODE_PLAIN)
+        ctx.score_pairs_raw(arr, d.MODE_MID | d.MODE_PLAIN)
+        tp = ctx.last_timing()
+        plain = {"gcups": pc / (tp["dp_ms"] / 1e3) / 1e9, "pairs": len(sel), "launches": tp["launches"]}
+        plain["batched_over_plain"] = value / world / plain["gcups"]
+
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(txt, steps[args.warmup], args.profiles, args.cpu_seconds, args.seed)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": "batched fwd+bwd (mid-anchored score): 64 profiles M log-uniform 50-800 x "
+                            "reads L log-uniform 150-3000 nt, GC 0.4-0.6, 10% implants, both strands",
+                "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
+                "profiles": args.profiles, "pairs_per_step": len(step_pairs[0]),
+                "cells_per_step": cells / args.steps, "l2": "inputs larger than L2 (W1 slots)",
+                "parallelism": f"replicas x{world} (pairs sharded per rank)",
+            },
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
+            "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

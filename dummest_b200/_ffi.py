@@ -78,6 +78,7 @@ SIGNATURES = [
     ("dmst_ctx_destroy", None, [C.c_void_p]),
     ("dmst_strerror", C.c_char_p, [C.c_int]),
     ("dmst_last_error", C.c_char_p, [C.c_void_p]),
+    ("dmst_ctx_stream", C.c_void_p, [C.c_void_p]),
     ("dmst_profile_add", C.c_int,
      [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(Params), C.POINTER(C.c_float),
       C.POINTER(C.c_int)]),

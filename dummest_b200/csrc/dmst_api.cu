@@ -245,6 +245,8 @@ const char *dmst_strerror(int status) { return statusText(status); }
 
 const char *dmst_last_error(const dmst_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
 
+void *dmst_ctx_stream(const dmst_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
 int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out) {
     if (!out) return DMST_EINVAL;
     *out = nullptr;

@@ -98,6 +98,11 @@ class Context:
     def __exit__(self, *a):
         self.close()
 
+    @property
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return self.lib.dmst_ctx_stream(self.h) or 0
+
     def _check(self, st: int, what: str):
         if st != F.DMST_OK:
             msg = self.lib.dmst_last_error(self.h).decode() or self.lib.dmst_strerror(st).decode()

@@ -118,6 +118,9 @@ void dmst_ctx_destroy(dmst_ctx *ctx);
 const char *dmst_strerror(int status);
 /* Text of the last error on this context ("" if none). */
 const char *dmst_last_error(const dmst_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), on which every kernel of the
+ * context runs; callers may record events on it to time a sequence of calls. */
+void *dmst_ctx_stream(const dmst_ctx *ctx);
 
 /* ---- profiles ----------------------------------------------------------
  * dmst_profile_add takes an already-finalized profile exactly as the
