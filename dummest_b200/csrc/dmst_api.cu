@@ -149,12 +149,12 @@ const char *statusText(int s) {
 
 int rowsPerLane(int M, int forced) {
     if (forced == 1 || forced == 2 || forced == 4) return forced;
-    const int rows = M + 1;
-    // Waste of padding rows in the last stripe against wavefront depth: tall
-    // profiles use 4 rows per lane, short ones fewer.
-    if (rows > 192) return 4;
-    if (rows > 80) return 2;
-    return 1;
+    (void)M;
+    // Measured on B200 (synthetic profiles, M 50-800): the per-step cost of a
+    // lane (shuffles, staging reads, W1 traffic) dominates, so four rows per
+    // lane is fastest per real cell even for the shortest profiles, where
+    // most of the 128-row stripe is padding.
+    return 4;
 }
 
 }  // namespace
@@ -187,6 +187,8 @@ struct dmst_ctx {
     DevBuf<DevPair> dPairs;
     DevBuf<float> dSeeds;
     DevBuf<XS> dNullTmp;
+    DevBuf<NullJob> dNullJobs;
+    DevBuf<int> dNullJobPairs;
     DevBuf<long long> dNullTmpOff;
     DevBuf<PairScales> dScales;
     DevBuf<PairOut> dOut;
@@ -307,6 +309,8 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dPairs.release();
     ctx->dSeeds.release();
     ctx->dNullTmp.release();
+    ctx->dNullJobs.release();
+    ctx->dNullJobPairs.release();
     ctx->dNullTmpOff.release();
     ctx->dScales.release();
     ctx->dOut.release();
@@ -646,8 +650,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         return ctx->seqLen[x.seq] > ctx->seqLen[y.seq];
     });
     std::vector<DevPair> dp(n);
-    std::vector<long long> tmpOff(n);
-    long long seedFloats = 0, tmpEntries = 0;
+    long long seedFloats = 0;
     size_t w1Max = 0, ringMax = 0;
     for (size_t k = 0; k < n; ++k) {
         const dmst_pair &q = pairs[order[k]];
@@ -659,8 +662,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         d.R = rowsPerLane(d.M, ctx->opts.rows_per_lane);
         d.seedOff = seedFloats;
         seedFloats += 2LL * d.L;
-        tmpOff[k] = tmpEntries;
-        tmpEntries += d.L + 4;
         const int S = kLanes * d.R;
         const size_t nS = (size_t)(d.M + 1 + S - 1) / S;
         const size_t P = (size_t)wavePeriod(d.L);
@@ -735,14 +736,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
 
     CK(ctx->dPairs.ensure(n), "alloc pairs");
     CK(ctx->dSeeds.ensure((size_t)seedFloats), "alloc seeds");
-    CK(ctx->dNullTmp.ensure((size_t)tmpEntries), "alloc null tmp");
-    CK(ctx->dNullTmpOff.ensure(n), "alloc null tmp");
     CK(ctx->dScales.ensure(n), "alloc scales");
     CK(ctx->dOut.ensure(n), "alloc out");
     CK(ctx->dChunks.ensure(allChunks.size()), "alloc chunks");
     CK(cudaMemcpyAsync(ctx->dPairs.p, dp.data(), n * sizeof(DevPair), cudaMemcpyHostToDevice, ctx->stream),
-       "upload pairs");
-    CK(cudaMemcpyAsync(ctx->dNullTmpOff.p, tmpOff.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream),
        "upload pairs");
     CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
                        ctx->stream),
@@ -757,15 +754,44 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
     const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
 
+    // Null-model jobs: up to 32 pairs of one read per warp.
+    std::vector<int> jobPairs(n);
+    std::iota(jobPairs.begin(), jobPairs.end(), 0);
+    std::stable_sort(jobPairs.begin(), jobPairs.end(), [&](int a, int b) { return dp[a].codeOff < dp[b].codeOff; });
+    std::vector<NullJob> nullJobs;
+    std::vector<long long> nullTmpOff;
+    long long nullTmpEntries = 0;
+    for (size_t k = 0; k < n;) {
+        size_t e = k;
+        while (e < n && e - k < 32 && dp[jobPairs[e]].codeOff == dp[jobPairs[k]].codeOff) ++e;
+        nullJobs.push_back(NullJob{(int)k, (int)(e - k)});
+        nullTmpOff.push_back(nullTmpEntries);
+        nullTmpEntries += 32LL * (dp[jobPairs[k]].L + 1);
+        k = e;
+    }
+    CK(ctx->dNullJobs.ensure(nullJobs.size()), "alloc null jobs");
+    CK(ctx->dNullJobPairs.ensure(n), "alloc null jobs");
+    CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries), "alloc null tmp");
+    CK(ctx->dNullTmpOff.ensure(nullJobs.size()), "alloc null tmp");
+    CK(cudaMemcpyAsync(ctx->dNullJobs.p, nullJobs.data(), nullJobs.size() * sizeof(NullJob), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "upload null jobs");
+    CK(cudaMemcpyAsync(ctx->dNullJobPairs.p, jobPairs.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+       "upload null jobs");
+    CK(cudaMemcpyAsync(ctx->dNullTmpOff.p, nullTmpOff.data(), nullTmpOff.size() * sizeof(long long),
+                       cudaMemcpyHostToDevice, ctx->stream),
+       "upload null jobs");
+
     CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
     {
-        const int tpb = 128;
-        nullModelKernel<<<(int)((n + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
-            ctx->dPairs.p, (int)n, ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p, ctx->dNullTmp.p,
-            ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+        const int nj = (int)nullJobs.size();
+        const int blocks = std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * 16));
+        nullModelKernel<<<blocks, kNullWarps * 32, 0, ctx->stream>>>(
+            ctx->dNullJobs.p, nj, ctx->dNullJobPairs.p, ctx->dPairs.p, ctx->dProfiles.p, ctx->dCodes.p,
+            ctx->dSeeds.p, ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
         CK(cudaGetLastError(), "null-model kernel");
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
@@ -949,18 +975,25 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
     d.R = 1;
     d.seedOff = 0;
     long long zero = 0;
+    const int pairIndex = 0;
+    const NullJob job{0, 1};
     CK(ctx->dPairs.ensure(1), "alloc");
     CK(ctx->dSeeds.ensure(2 * (size_t)d.L), "alloc");
-    CK(ctx->dNullTmp.ensure((size_t)d.L + 4), "alloc");
+    CK(ctx->dNullTmp.ensure(32 * ((size_t)d.L + 1)), "alloc");
     CK(ctx->dNullTmpOff.ensure(1), "alloc");
+    CK(ctx->dNullJobs.ensure(1), "alloc");
+    CK(ctx->dNullJobPairs.ensure(1), "alloc");
     CK(ctx->dScales.ensure(1), "alloc");
     CK(cudaMemcpy(ctx->dPairs.p, &d, sizeof d, cudaMemcpyHostToDevice), "upload");
     CK(cudaMemcpy(ctx->dNullTmpOff.p, &zero, sizeof zero, cudaMemcpyHostToDevice), "upload");
+    CK(cudaMemcpy(ctx->dNullJobs.p, &job, sizeof job, cudaMemcpyHostToDevice), "upload");
+    CK(cudaMemcpy(ctx->dNullJobPairs.p, &pairIndex, sizeof pairIndex, cudaMemcpyHostToDevice), "upload");
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
-    nullModelKernel<<<1, 32, 0, ctx->stream>>>(ctx->dPairs.p, 1, ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p,
-                                               ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+    nullModelKernel<<<1, kNullWarps * 32, 0, ctx->stream>>>(ctx->dNullJobs.p, 1, ctx->dNullJobPairs.p, ctx->dPairs.p,
+                                                           ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p,
+                                                           ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
     CK(cudaGetLastError(), "null-model kernel");
     CK(cudaStreamSynchronize(ctx->stream), "null-model kernel");
     std::vector<float> s(2 * (size_t)d.L);

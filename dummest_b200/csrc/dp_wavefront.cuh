@@ -582,7 +582,11 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             const float Z0 = bgsC * __fmaf_rn(f.c.a0[k], f.w3[k], f.c.b0[k] * f.z3[k]);
             const float Z1 = f.c.a1[k] * f.w1[k];
             const float Z2 = f.c.a2[k] * f.w2[k];
-            const float W0 = win0 + __fmaf_rn(prev, f.c.rs[k], (Z0 + Z1) + Z2);
+            // fma(prev, 1, x) is prev + x; in the fast mode every row takes the
+            // seed: padding rows (past M, zero coefficients) then hold only
+            // their seed, which reaches no real row and multiplies a zero W1.
+            const float W0 = (MODE == kMid) ? win0 + __fadd_rn((Z0 + Z1) + Z2, prev)
+                                            : win0 + __fmaf_rn(prev, f.c.rs[k], (Z0 + Z1) + Z2);
             if (MODE == kMid) f.best = fmaxf(f.best, W0 * q[k]);
             if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
             const float Y0 = __fmaf_rn(f.c.d0[k], W0, f.c.eps[k] * yab);

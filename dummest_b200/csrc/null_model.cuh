@@ -136,94 +136,137 @@ __device__ __forceinline__ XS prefixStep(int i, const float *bg, const uint8_t *
     return batchAdd(codon, batchAdd(single, dbl));
 }
 
-// One thread per pair.  Outputs prefixSeed[0..L) and suffixSeedFromNext[0..L)
-// at seeds + seedOff, the three scales, and uses tmp (L+4 ExpScores per pair)
-// for the suffix probabilities.
-__device__ void nullModelPair(const uint8_t *codes, int L, const float *bg, NullRates r, float *prefixSeed,
-                              float *suffixSeed, XS *suffix, PairScales *scalesOut) {
-    const double keep = 1.0 - r.single - r.dbl;   // codonKeepProbability
-    const double sNE = r.single * 0.25;           // singleNucleotideEmission
-    const double dNE = r.dbl * 0.0625;            // doubleNucleotideEmission
+// Pairs that share a read are scored by one warp, one lane per pair: the
+// lanes run in lock step over the same codon codes (one broadcast load per
+// column), keep the suffix recurrence in registers, store the temporary
+// suffix probabilities interleaved (one coalesced 256-byte store per column),
+// and write their seed vectors through a shared-memory transpose, so that each
+// store instruction writes 32 consecutive seeds of one pair.
+struct NullJob {
+    int first;  // index of the job's first pair in the pair-index array
+    int count;  // pairs in the job (<= 32), all with the same read
+};
 
-    // Pass 1: prefix probabilities; keep the last three for the total.
-    XS p1 = xsZero(), p2 = xsZero(), p3 = xsZero();
-    for (int i = 0; i < L; ++i) {
-        XS p = prefixStep(i, bg, codes, L, p1, p2, p3, keep, sNE, dNE);
-        p3 = p2;
-        p2 = p1;
-        p1 = p;
-    }
-    // Total and scales (dummest-dp-backward.hh:103-129); p1 = prefix[L-1],
-    // p2 = prefix[L-2], p3 = prefix[L-3].
-    const double keepSingle = 1.0 - r.single;
-    const double keepBoth = keepSingle - r.dbl;
-    XS trailingSingle = scaleScore(p2, keepSingle * 0.25);
-    XS trailingDouble = scaleScore(p3, keepBoth * 0.0625);
-    XS total = scalarAdd(scalarAdd(p1, trailingSingle), trailingDouble);
-    const float nullLog = (total.m == 0.0f) ? -INFINITY : (float)(log2((double)total.m) + (double)total.e);
-    double perBaseLog = -(double)nullLog / (double)L;
-    if (!(perBaseLog < 120.0)) perBaseLog = 120.0;
-    const double perBaseRaw = exp2(perBaseLog);
-    const XS perBase = splitNorm(perBaseRaw, 0);
-    const XS perBaseInv = splitNorm(1.0 / perBaseRaw, 0);
-    const XS quarter = splitNorm(0.25, 0), sixteenth = splitNorm(0.0625, 0);
-    const XS s1 = scalarMul(perBase, quarter);
-    const XS s2 = scalarMul(scalarMul(perBase, perBase), sixteenth);
-    const XS sC = scalarMul(scalarMul(perBase, perBase), perBase);
-    scalesOut->s1 = packScore(s1);
-    scalesOut->s2 = packScore(s2);
-    scalesOut->sC = packScore(sC);
-    scalesOut->pad = 0.0f;
+constexpr int kNullWarps = 4;
 
-    // Pass 2: suffix probabilities (dummest-dp-backward.hh:6-55), j = L-1..0,
-    // suffix[L] = 1, suffix[L+1..L+3] = 0.
-    {
-        const XS trailing = splitNorm(0.5 * keep, 0);
-        suffix[L] = pow2Score(0);
-        suffix[L + 1] = xsZero();
-        suffix[L + 2] = xsZero();
-        suffix[L + 3] = xsZero();
-        for (int i = L - 1; i >= 0; --i) {
-            const double codonScale = __dmul_rn((double)bgAt(bg, codes, L, i), keep);
-            XS single = scaleScore(suffix[i + 1], sNE);
-            XS dIn = (i + 1 < L) ? suffix[i + 2] : pow2Score(2);
-            XS dbl = scaleScore(dIn, dNE);
-            XS codon = (i + 2 < L) ? scaleScore(suffix[i + 3], codonScale)
-                                   : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
-            suffix[i] = batchAdd(codon, batchAdd(single, dbl));
-        }
-    }
-
-    // Pass 3: suffix seeds (dummest-dp-backward.hh:137-154).
-    XS running = pow2Score(0);
-    for (int t = 0; t < L - 1; ++t) running = batchMul(running, perBase);
-    for (int j = 0; j < L; ++j) {
-        suffixSeed[j] = packScore(batchMul(suffix[j + 1], running));
-        running = batchMul(running, perBaseInv);
-    }
-
-    // Pass 4: prefix seeds (dummest-dp-backward.hh:155-164), recomputing the
-    // prefix recurrence.
-    running = perBase;
-    p1 = p2 = p3 = xsZero();
-    for (int i = 0; i < L; ++i) {
-        XS p = prefixStep(i, bg, codes, L, p1, p2, p3, keep, sNE, dNE);
-        p3 = p2;
-        p2 = p1;
-        p1 = p;
-        prefixSeed[i] = packScore(batchMul(p, running));
-        running = batchMul(running, perBase);
-    }
+__device__ __forceinline__ void flushSeeds(float (*stage)[33], float *const *dst, int count, int j0, int ncol,
+                                           int lane) {
+    // stage[c][p] holds column j0 + c of pair p; write pair p's columns with
+    // lanes over columns.
+    __syncwarp();
+    for (int p = 0; p < count; ++p)
+        if (lane < ncol) dst[p][j0 + lane] = stage[lane][p];
+    __syncwarp();
 }
 
-__global__ void nullModelKernel(const DevPair *pairs, int n, const DevProfile *profiles, const uint8_t *codes,
-                                float *seeds, XS *tmp, const long long *tmpOff, PairScales *scales, NullRates r) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const DevPair p = pairs[i];
-    const float *bg = profiles[p.prof].bg;
-    float *pre = seeds + p.seedOff;
-    nullModelPair(codes + p.codeOff, p.L, bg, r, pre, pre + p.L, tmp + tmpOff[i], &scales[i]);
+__global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob *jobs, int nJobs, const int *jobPairs,
+                                                                   const DevPair *pairs, const DevProfile *profiles,
+                                                                   const uint8_t *codes, float *seeds, XS *tmp,
+                                                                   const long long *tmpOff, PairScales *scales,
+                                                                   NullRates r) {
+    __shared__ float stageAll[kNullWarps][32][33];
+    __shared__ float *dstAll[kNullWarps][2][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float (*stage)[33] = stageAll[warp];
+    const double keep = 1.0 - r.single - r.dbl;  // codonKeepProbability
+    const double sNE = r.single * 0.25;          // singleNucleotideEmission
+    const double dNE = r.dbl * 0.0625;           // doubleNucleotideEmission
+    for (int ji = blockIdx.x * kNullWarps + warp; ji < nJobs; ji += gridDim.x * kNullWarps) {
+        const NullJob job = jobs[ji];
+        const bool on = lane < job.count;
+        const int pi = jobPairs[job.first + (on ? lane : 0)];
+        const DevPair p = pairs[pi];
+        const int L = p.L;
+        const uint8_t *cd = codes + p.codeOff;
+        const float *bg = profiles[p.prof].bg;
+        float *pre = seeds + p.seedOff;
+        dstAll[warp][0][lane] = on ? pre : nullptr;
+        dstAll[warp][1][lane] = on ? pre + L : nullptr;
+        XS *sfx = tmp + tmpOff[ji];  // [(L+1) x 32] interleaved suffix probabilities
+
+        // Pass 1: prefix probabilities (dummest-dp-backward.hh:58-100); the
+        // last three give the total.
+        XS p1 = xsZero(), p2 = xsZero(), p3 = xsZero();
+        for (int i = 0; i < L; ++i) {
+            const XS q = prefixStep(i, bg, cd, L, p1, p2, p3, keep, sNE, dNE);
+            p3 = p2;
+            p2 = p1;
+            p1 = q;
+        }
+        // Total and scales (dummest-dp-backward.hh:103-129).
+        const double keepSingle = 1.0 - r.single;
+        const double keepBoth = keepSingle - r.dbl;
+        const XS trailingSingle = scaleScore(p2, keepSingle * 0.25);
+        const XS trailingDouble = scaleScore(p3, keepBoth * 0.0625);
+        const XS total = scalarAdd(scalarAdd(p1, trailingSingle), trailingDouble);
+        const float nullLog = (total.m == 0.0f) ? -INFINITY : (float)(log2((double)total.m) + (double)total.e);
+        double perBaseLog = -(double)nullLog / (double)L;
+        if (!(perBaseLog < 120.0)) perBaseLog = 120.0;
+        const double perBaseRaw = exp2(perBaseLog);
+        const XS perBase = splitNorm(perBaseRaw, 0);
+        const XS perBaseInv = splitNorm(1.0 / perBaseRaw, 0);
+        const XS quarter = splitNorm(0.25, 0), sixteenth = splitNorm(0.0625, 0);
+        if (on) {
+            PairScales sc;
+            sc.s1 = packScore(scalarMul(perBase, quarter));
+            sc.s2 = packScore(scalarMul(scalarMul(perBase, perBase), sixteenth));
+            sc.sC = packScore(scalarMul(scalarMul(perBase, perBase), perBase));
+            sc.pad = 0.0f;
+            scales[pi] = sc;
+        }
+
+        // Pass 2: suffix probabilities (dummest-dp-backward.hh:6-55), i = L-1..0,
+        // from suffix[L] = 1 and suffix[L+1..L+3] = 0.
+        {
+            const XS trailing = splitNorm(0.5 * keep, 0);
+            XS s1 = pow2Score(0), s2 = xsZero(), s3 = xsZero();  // suffix[i+1], [i+2], [i+3]
+            for (int i = L - 1; i >= 0; --i) {
+                const double codonScale = __dmul_rn((double)bgAt(bg, cd, L, i), keep);
+                const XS single = scaleScore(s1, sNE);
+                const XS dIn = (i + 1 < L) ? s2 : pow2Score(2);
+                const XS dbl = scaleScore(dIn, dNE);
+                const XS codon = (i + 2 < L) ? scaleScore(s3, codonScale) : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
+                const XS v = batchAdd(codon, batchAdd(single, dbl));
+                sfx[(size_t)i * 32 + lane] = v;
+                s3 = s2;
+                s2 = s1;
+                s1 = v;
+            }
+        }
+
+        // Pass 3: suffix seeds (dummest-dp-backward.hh:137-154).
+        XS running = pow2Score(0);
+        for (int t = 0; t < L - 1; ++t) running = batchMul(running, perBase);
+        for (int j0 = 0; j0 < L; j0 += 32) {
+            const int ncol = L - j0 < 32 ? L - j0 : 32;
+            for (int c = 0; c < ncol; ++c) {
+                const int j = j0 + c;
+                const XS nx = (j + 1 < L) ? sfx[(size_t)(j + 1) * 32 + lane] : pow2Score(0);
+                stage[c][lane] = packScore(batchMul(nx, running));
+                running = batchMul(running, perBaseInv);
+            }
+            flushSeeds(stage, dstAll[warp][1], job.count, j0, ncol, lane);
+        }
+
+        // Pass 4: prefix seeds (dummest-dp-backward.hh:155-164), recomputing
+        // the prefix recurrence.
+        running = perBase;
+        p1 = p2 = p3 = xsZero();
+        for (int j0 = 0; j0 < L; j0 += 32) {
+            const int ncol = L - j0 < 32 ? L - j0 : 32;
+            for (int c = 0; c < ncol; ++c) {
+                const int i = j0 + c;
+                const XS q = prefixStep(i, bg, cd, L, p1, p2, p3, keep, sNE, dNE);
+                p3 = p2;
+                p2 = p1;
+                p1 = q;
+                stage[c][lane] = packScore(batchMul(q, running));
+                running = batchMul(running, perBase);
+            }
+            flushSeeds(stage, dstAll[warp][0], job.count, j0, ncol, lane);
+        }
+        __syncwarp();
+    }
 }
 
 }  // namespace dmst
