@@ -306,11 +306,14 @@ def run_ours(args, rank, world, local):
     ev0.record(stream)
     launches, dp_ms, cells = 0, 0.0, 0.0
     results = []
+    parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0}
     for k in range(args.warmup, n_steps):
         results.append(ctx.score_pairs_raw(step_pairs[k], d.MODE_MID))
         t = ctx.last_timing()
         launches += t["launches"]
         dp_ms += t["dp_ms"]
+        for key in parts:
+            parts[key] += t[key]
         cells += step_cells[k]
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -411,6 +414,7 @@ def run_ours(args, rank, world, local):
             },
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
+            "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

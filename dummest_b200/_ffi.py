@@ -103,6 +103,7 @@ SIGNATURES = [
     ("dmst_score_pairs", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.c_int, C.POINTER(Result)]),
     ("dmst_last_timing", C.c_int,
      [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    ("dmst_last_timing_ex", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("dmst_null_model", C.c_int,
      [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     ("dmst_estimate_gumbel", C.c_int, [C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double)]),

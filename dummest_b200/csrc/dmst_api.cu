@@ -10,6 +10,7 @@
 #include "null_model.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -200,7 +201,7 @@ struct dmst_ctx {
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
 
-    double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0;
+    double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0, lastHostMs = 0;
     int lastExactPairs = 0;
     int lastLaunches = 0;
 
@@ -628,8 +629,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     const bool sequentialExact = (mode & DMST_MODE_EXACT_SEQUENTIAL) != 0;
     if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
     const bool mid = base == DMST_MODE_MID;
-    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = 0;
+    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = ctx->lastExactMs = ctx->lastHostMs = 0;
     ctx->lastLaunches = 0;
+    ctx->lastExactPairs = 0;
+    const auto hostT0 = std::chrono::steady_clock::now();
     if (n == 0) return DMST_OK;
     if (n > (size_t)INT32_MAX / 2) return ctx->fail(DMST_ERANGE, "too many pairs");
     CK(cudaSetDevice(ctx->device), "set device");
@@ -644,11 +647,16 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         if (q.seq < 0 || q.seq >= (int)ctx->seqLen.size() || q.profile < 0 || q.profile >= (int)ctx->profiles.size())
             return ctx->fail(DMST_EINVAL, "pair %zu: unknown sequence or profile id", i);
     }
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        const dmst_pair &x = pairs[a], &y = pairs[b];
-        if (x.profile != y.profile) return x.profile < y.profile;
-        return ctx->seqLen[x.seq] > ctx->seqLen[y.seq];
-    });
+    {
+        // Profile-major, longest read first: one key sort (the index breaks ties).
+        std::vector<std::pair<uint64_t, int>> keys(n);
+        for (size_t i = 0; i < n; ++i) {
+            const uint32_t inv = 0xFFFFFFFFu - (uint32_t)ctx->seqLen[pairs[i].seq];
+            keys[i] = {((uint64_t)(uint32_t)pairs[i].profile << 32) | inv, (int)i};
+        }
+        std::sort(keys.begin(), keys.end());
+        for (size_t i = 0; i < n; ++i) order[i] = keys[i].second;
+    }
     std::vector<DevPair> dp(n);
     long long seedFloats = 0;
     size_t w1Max = 0, ringMax = 0;
@@ -756,8 +764,14 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
 
     // Null-model jobs: up to 32 pairs of one read per warp.
     std::vector<int> jobPairs(n);
-    std::iota(jobPairs.begin(), jobPairs.end(), 0);
-    std::stable_sort(jobPairs.begin(), jobPairs.end(), [&](int a, int b) { return dp[a].codeOff < dp[b].codeOff; });
+    {
+        // Counting sort of the (profile-major) pair slots by sequence id.
+        const size_t nSeq = ctx->seqLen.size();
+        std::vector<int> start(nSeq + 1, 0);
+        for (size_t k = 0; k < n; ++k) ++start[pairs[order[k]].seq + 1];
+        for (size_t q = 0; q < nSeq; ++q) start[q + 1] += start[q];
+        for (size_t k = 0; k < n; ++k) jobPairs[start[pairs[order[k]].seq]++] = (int)k;
+    }
     std::vector<NullJob> nullJobs;
     std::vector<long long> nullTmpOff;
     long long nullTmpEntries = 0;
@@ -782,6 +796,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                        cudaMemcpyHostToDevice, ctx->stream),
        "upload null jobs");
 
+    ctx->lastHostMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostT0).count();
     CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
@@ -949,6 +964,14 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             r.mid_ln = -INFINITY;
         }
     }
+    return DMST_OK;
+}
+
+int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n) {
+    if (!ctx || !out || n < 0) return DMST_EINVAL;
+    const double v[7] = {ctx->lastTotalMs, ctx->lastNullMs, ctx->lastDpMs, ctx->lastExactMs,
+                         ctx->lastHostMs,  (double)ctx->lastLaunches, (double)ctx->lastExactPairs};
+    for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
     return DMST_OK;
 }
 

@@ -214,9 +214,10 @@ class Context:
         return res
 
     def last_timing(self) -> dict:
-        t, d, nm, la = C.c_double(), C.c_double(), C.c_double(), C.c_int()
-        self.lib.dmst_last_timing(self.h, C.byref(t), C.byref(d), C.byref(nm), C.byref(la))
-        return {"total_ms": t.value, "dp_ms": d.value, "null_ms": nm.value, "launches": la.value}
+        v = (C.c_double * 7)()
+        self.lib.dmst_last_timing_ex(self.h, v, 7)
+        return {"total_ms": v[0], "null_ms": v[1], "dp_ms": v[2], "exact_ms": v[3], "host_ms": v[4],
+                "launches": int(v[5]), "exact_pairs": int(v[6])}
 
     def find_similarities(self, profile: int, decoded: Sequence[np.ndarray]) -> list[Similarity]:
         if len(decoded) == 0:

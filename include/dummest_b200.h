@@ -182,6 +182,11 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
 /* Timing of the last dmst_score_pairs call, from CUDA events on the context's
  * stream: total device ms and the ms of the main DP kernel(s). */
 int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, double *null_ms, int *launches);
+/* The same breakdown as an array: out[0] device ms of the call, [1] null-model
+ * kernel ms, [2] DP kernel ms, [3] exact-path ms, [4] host preparation ms
+ * (wall clock), [5] kernel launches, [6] pairs on the exact path.  n = number
+ * of entries wanted (<= 7). */
+int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
 
 /* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
  * and the three per-base scales (one-nt, two-nt, codon) for one pair, computed
