@@ -13,8 +13,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <string>
@@ -1105,3 +1107,122 @@ int dmst_calibrate(dmst_ctx *ctx, int profile, int sequence_length, int border, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Null model without allocation.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// read's null-model seeds: a process whose device memory is already claimed
+// by another pool (a framework's caching allocator holding nearly all HBM
+// fails a fresh cudaMalloc), or a latency-bound caller whose other streams
+// must not stall on cudaFree's implicit device synchronisation.  For them
+// dmst_null_model_noalloc runs the same null-model kernel as dmst_null_model
+// with the caller's device buffers for input and output and a fixed,
+// file-scope device array for everything else.  It calls no cudaMalloc,
+// cudaFree or any other allocating function.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Layout of the static scratch: a 2 KiB header (the kernel's profile, pair,
+// job and offset records), then the interleaved suffix temporary of
+// 32 x (L+1) ExpScores.  The header is 2 KiB although its records take 192
+// bytes so that a background lookup with any 8-bit code (bg[0..255] starts
+// 24 bytes into the profile record) stays inside the array.
+constexpr size_t kNaHeaderBytes = 2048;
+constexpr size_t kNaTmpEntries = 32 * ((size_t)DMST_NOALLOC_MAX_LEN + 1);
+constexpr size_t kNaScratchBytes = kNaHeaderBytes + kNaTmpEntries * sizeof(XS);  // 4,196,608 bytes
+
+static __device__ __align__(256) unsigned char gNullScratch[kNaScratchBytes];
+
+struct NaHeader {
+    DevProfile profile;  // offset 0
+    DevPair pair;        // offset 128
+    NullJob job;         // offset 160
+    int jobPair;         // offset 168
+    int pad;
+    long long tmpOff;    // offset 176
+};
+static_assert(sizeof(NaHeader) <= 192, "no-alloc header layout");
+static_assert(offsetof(NaHeader, profile) + offsetof(DevProfile, bg) + 256 * sizeof(float) <= kNaHeaderBytes,
+              "an 8-bit code must index inside the header");
+
+// Writes one call's header records into the scratch from a kernel argument,
+// in stream order with the null-model launch that reads them.
+__global__ void naHeaderKernel(NaHeader h, NaHeader *dst) {
+    if (threadIdx.x == 0) *dst = h;
+}
+
+constexpr int kNaMaxDevices = 64;
+std::mutex gNaMutex;
+void *gNaScratch[kNaMaxDevices];  // per-device address of gNullScratch, set on first use
+
+}  // namespace
+
+extern "C" int dmst_null_model_noalloc(const uint8_t *codes, int length, const float *bg, const dmst_opts *opts,
+                                       float *seeds, float *scales4, void *stream) {
+    if (!codes || !bg || !seeds || !scales4 || length < 1) return DMST_EINVAL;
+    if (length > DMST_NOALLOC_MAX_LEN) return DMST_ERANGE;
+    dmst_opts o;
+    dmst_opts_default(&o);
+    if (opts) o = *opts;
+    if (!(o.insert1 >= 0 && o.insert1 < 1 && o.insert2 >= 0 && o.insert2 < 1 && o.delete1 >= 0 && o.delete1 < 1 &&
+          o.delete2 >= 0 && o.delete2 < 1 && o.insert1 + o.insert2 + o.delete1 + o.delete2 < 1))
+        return DMST_EINVAL;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
+        cudaGetLastError();
+        return DMST_EDEVICE;
+    }
+    void *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(gNaMutex);
+        if (!gNaScratch[dev]) {
+            // Set-up, once per device, with that device current.
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, gNullScratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return DMST_EDEVICE;
+            }
+            gNaScratch[dev] = p;
+        }
+        base = gNaScratch[dev];
+    }
+    NaHeader *hdr = reinterpret_cast<NaHeader *>(base);
+    XS *tmp = reinterpret_cast<XS *>(static_cast<unsigned char *>(base) + kNaHeaderBytes);
+
+    // The records dmst_null_model builds for one pair, with offsets 0 into the
+    // caller's buffers.  Every scratch word the kernel reads is written in the
+    // same call (the header here, the suffix temporary before its reads), so
+    // nothing has to start at zero.
+    NaHeader h;
+    std::memset(&h, 0, sizeof h);
+    h.profile.M = 0;
+    h.profile.rowPad = 0;
+    for (int c = 0; c < 26; ++c) h.profile.bg[c] = (c < kNumCodes) ? bg[4 + c] : 0.0f;
+    h.profile.bg[kPad] = 0.0f;  // zero_idx pad reads as 0
+    h.pair.codeOff = 0;
+    h.pair.seedOff = 0;
+    h.pair.L = length;
+    h.pair.M = 0;
+    h.pair.prof = 0;
+    h.pair.R = 1;
+    h.job = NullJob{0, 1};
+    h.jobPair = 0;
+    h.tmpOff = 0;
+    Rates r{};
+    r.insert1 = (float)o.insert1;
+    r.insert2 = (float)o.insert2;
+    r.delete1 = (float)o.delete1;
+    r.delete2 = (float)o.delete2;
+    NullRates nr;
+    nr.single = (double)(r.insert1 + r.delete2);
+    nr.dbl = (double)(r.insert2 + r.delete1);
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    naHeaderKernel<<<1, 32, 0, s>>>(h, hdr);
+    nullModelKernel<<<1, kNullWarps * 32, 0, s>>>(&hdr->job, 1, &hdr->jobPair, &hdr->pair, &hdr->profile, codes,
+                                                  seeds, tmp, &hdr->tmpOff, reinterpret_cast<PairScales *>(scales4),
+                                                  nr);
+    if (cudaGetLastError() != cudaSuccess) return DMST_EDEVICE;
+    return DMST_OK;
+}

@@ -194,6 +194,45 @@ int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
  * (dummest-dp-backward.hh:6-188). */
 int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, float *suffix_seed, float *scales3);
 
+/* ---- null model without allocation -------------------------------------
+ * This entry point has no counterpart in the reference.  It serves callers
+ * that cannot allocate device memory where they need a read's null model:
+ * a process whose device memory is already claimed by another pool (a
+ * framework's caching allocator holding nearly all HBM makes a fresh
+ * cudaMalloc fail), or a latency-bound caller whose other streams must not
+ * stall on cudaFree's implicit device synchronisation.
+ *
+ * It computes exactly what dmst_null_model computes (the same kernel), with
+ * no context and no allocation of any kind: inputs and outputs are the
+ * caller's DEVICE buffers, and the kernel's scratch is a fixed file-scope
+ * device array of 4,196,608 bytes (a 2 KiB header plus 32 x (L+1) 8-byte
+ * scores for L <= DMST_NOALLOC_MAX_LEN).
+ *
+ *   codes    device pointer, `length` codon codes 0..24 (dmst_decode_letters);
+ *            a larger code yields meaningless seeds but reads stay in bounds
+ *   length   1 .. DMST_NOALLOC_MAX_LEN; larger returns DMST_ERANGE
+ *   bg       HOST pointer, 29 floats (bg_probs, as for dmst_profile_add)
+ *   opts     HOST pointer to the rates (insert1..delete2 are used), or NULL
+ *            for the defaults
+ *   seeds    device pointer, 2*length floats: prefixSeed[0..L) then
+ *            suffixSeedFromNext[0..L)
+ *   scales4  device pointer, 4 floats: one-nt, two-nt and codon scales, 0
+ *   stream   cudaStream_t (NULL = the legacy default stream); the work is
+ *            queued there and the call returns without waiting
+ *
+ * The scratch is set up on the first call on each device (the current device
+ * when the call is made: cudaGetSymbolAddress, return code checked), so make
+ * that first call before any stream capture.  Nothing in the scratch has to
+ * start at zero: the call writes every word it later reads.  Calls on one
+ * device share the one scratch array, so calls whose work can overlap (two
+ * streams, or two host threads) race; order them on one stream or wait for
+ * the previous call's work.  Returns DMST_EINVAL for a null pointer, a length
+ * below 1 or invalid rates, DMST_ERANGE beyond the maximum, DMST_EDEVICE for
+ * a CUDA error (including set-up and launch). */
+#define DMST_NOALLOC_MAX_LEN 16384
+int dmst_null_model_noalloc(const uint8_t *codes, int length, const float *bg, const dmst_opts *opts,
+                            float *seeds, float *scales4, void *stream);
+
 /* ---- calibration --------------------------------------------------------
  * Gumbel fits of the reference (estimateGumbel, dummest-calibration.hh:97-104),
  * FP64 on the host.  Sorts scores in place.  out8 = MM lambda, MM K,
