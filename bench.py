@@ -192,7 +192,7 @@ def measured_peaks():
 def traffic_per_cell():
     """DRAM bytes per cell of the mid kernel from the committed ncu summary."""
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "dp_mid_r4_traffic.json")))["dram_bytes_per_cell"]
+        return json.load(open(os.path.join(ROOT, "profiles", "dpKernel_mid_8192pairs_traffic.json")))["dram_bytes_per_cell"]
     except (OSError, KeyError, ValueError):
         return None
 

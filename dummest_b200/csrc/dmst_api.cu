@@ -597,6 +597,11 @@ int dmst_encode_dna(const char *ascii, int L, char *letters) {
 // ---------------------------------------------------------------------------
 // Scoring
 // ---------------------------------------------------------------------------
+// scoreToLog (dummest-score.hh:202-207): std::log of the float mantissa is the
+// float overload, so the logarithm is taken in single precision and then
+// added to e * ln 2 in double, as the reference's logProbRatio is.
+static double scoreLn(float m, int e) { return (double)std::log(m) + (double)e * 0.6931471805599453; }
+
 static void fillResult(dmst_result &r, float v, bool isFilterF, dmst_score *dst, double *ln) {
     (void)isFilterF;
     (void)r;
@@ -614,13 +619,13 @@ static void fillResult(dmst_result &r, float v, bool isFilterF, dmst_score *dst,
     }
     dst->m = m;
     dst->e = e;
-    *ln = (m == 0.0f) ? (std::isinf(v) ? INFINITY : -INFINITY) : std::log((double)m) + (double)e * 0.6931471805599453;
+    *ln = (m == 0.0f) ? (std::isinf(v) ? INFINITY : -INFINITY) : scoreLn(m, e);
 }
 
 static void scoreToResult(XS s, dmst_score *dst, double *ln) {
     dst->m = s.m;
     dst->e = s.e;
-    *ln = (s.m == 0.0f) ? -INFINITY : std::log((double)s.m) + (double)s.e * 0.6931471805599453;
+    *ln = (s.m == 0.0f) ? -INFINITY : scoreLn(s.m, s.e);
 }
 
 int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {

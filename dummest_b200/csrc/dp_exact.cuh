@@ -191,10 +191,10 @@ __global__ void exactKernel(const ExactJob *jobs, int n, const DevPair *pairs, c
             const float e = E[(size_t)c * rowPad + i];
             const float bgv = bg[c];
             const float X = (enter * e) * w3;
-            const float Z0 = (bgv * sc.sC) * __fmaf_rn(a0, w3, b0 * z0[(j - 3) & 3]);
+            // GCC's contraction of dummest-dp-forward.hh:148-166 at -O3.
+            const float Z0 = (bgv * sc.sC) * __fmaf_rn(b0, z0[(j - 3) & 3], a0 * w3);
             z0[j & 3] = Z0;
-            const float Z1 = a1 * w1, Z2 = a2 * w2;
-            const float w0 = W0cur[j] + __fmaf_rn(pre[j], rs, (Z0 + Z1) + Z2);
+            const float w0 = W0cur[j] + __fmaf_rn(pre[j], rs, __fmaf_rn(a2, w2, __fmaf_rn(a1, w1, Z0)));
             rowMax = fmaxf(rowMax, w0);
             const XS f = promote(w0, cntF[i]);
             const XS b = promote(w1row[j], cntB[i]);
@@ -204,7 +204,7 @@ __global__ void exactKernel(const ExactJob *jobs, int n, const DevPair *pairs, c
             ws2 = ws1;
             ws1 = ws0;
             ws0 = w0;
-            Ycur[j] = __fmaf_rn(d0, w0, eps * Ynext[j]);
+            Ycur[j] = __fmaf_rn(eps, Ynext[j], d0 * w0);
             rowMax = fmaxf(rowMax, Ycur[j]);
             if (i < M) W0nxt[j] = W0nxt[j] + __fmaf_rn(d2, w1, __fmaf_rn(d1, w2, X + Ycur[j]));
         }

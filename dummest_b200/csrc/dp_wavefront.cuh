@@ -578,18 +578,20 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         float stepMax = 0.0f;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
+            // The reference's operations as GCC contracts them at -O3
+            // (dummest-dp-forward.hh:116-222): Z0 = (bg*sC)*fma(b0, Z0[j-3],
+            // a0*w3); the alpha1/alpha2 products fuse into the W0 sum, and
+            // Y0 = fma(eps, Y0[i-1], d0*W0).
             const float X = (f.c.enter[k] * e[k]) * f.w3[k];
-            const float Z0 = bgsC * __fmaf_rn(f.c.a0[k], f.w3[k], f.c.b0[k] * f.z3[k]);
-            const float Z1 = f.c.a1[k] * f.w1[k];
-            const float Z2 = f.c.a2[k] * f.w2[k];
+            const float Z0 = bgsC * __fmaf_rn(f.c.b0[k], f.z3[k], f.c.a0[k] * f.w3[k]);
+            const float zs = __fmaf_rn(f.c.a2[k], f.w2[k], __fmaf_rn(f.c.a1[k], f.w1[k], Z0));
             // fma(prev, 1, x) is prev + x; in the fast mode every row takes the
             // seed: padding rows (past M, zero coefficients) then hold only
             // their seed, which reaches no real row and multiplies a zero W1.
-            const float W0 = (MODE == kMid) ? win0 + __fadd_rn((Z0 + Z1) + Z2, prev)
-                                            : win0 + __fmaf_rn(prev, f.c.rs[k], (Z0 + Z1) + Z2);
+            const float W0 = (MODE == kMid) ? win0 + __fadd_rn(zs, prev) : win0 + __fmaf_rn(prev, f.c.rs[k], zs);
             if (MODE == kMid) f.best = fmaxf(f.best, W0 * q[k]);
             if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
-            const float Y0 = __fmaf_rn(f.c.d0[k], W0, f.c.eps[k] * yab);
+            const float Y0 = __fmaf_rn(f.c.eps[k], yab, f.c.d0[k] * W0);
             if (MODE == kMid) f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
             const float nin = __fmaf_rn(f.c.d2[k], f.w1[k], __fmaf_rn(f.c.d1[k], f.w2[k], X + Y0));
             if (MODE == kDiscover) {

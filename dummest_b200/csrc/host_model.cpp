@@ -396,15 +396,21 @@ static double meanOf(const double *x, int n) {
 
 // Method of moments (dummest-calibration.hh:7-20): lambda = pi / sqrt(6 var)
 // with the population variance; K = exp(lambda*mean - euler) / length.
+// The reference's build (-O3, x86-64-v3) sums the squares in order but forms
+// them as separate products, except the last one when n is odd, which its
+// scalar loop tail fuses into the sum; and it fuses lambda*mean - euler.
 static double mmLambda(const double *s, int n, double mean) {
     const double pi = 3.1415926535897932;
     double v = 0;
-    for (int i = 0; i < n; ++i) v += (s[i] - mean) * (s[i] - mean);
+    for (int i = 0; i < n; ++i) {
+        const double d = s[i] - mean;
+        v = ((n & 1) && i == n - 1) ? std::fma(d, d, v) : v + d * d;
+    }
     return pi / std::sqrt(6 * (v / n));
 }
 static double mmK(double mean, double lambda, double len) {
     const double euler = 0.57721566490153286;
-    return std::exp(lambda * mean - euler) / len;
+    return std::exp(std::fma(lambda, mean, -euler)) / len;
 }
 // L-moments lambda (dummest-calibration.hh:22-29), on sorted scores.
 static double lmLambda(const double *sorted, int n, double mean) {

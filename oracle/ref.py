@@ -57,6 +57,7 @@ def lib(bits: int = 32) -> C.CDLL:
                                          P(C.c_float)]),
         "dmstref_backward_matrix": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_int)]),
         "dmstref_estimate_gumbel": (None, [P(C.c_double), C.c_int, C.c_double, P(C.c_double)]),
+        "dmstref_estimate_k": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -191,4 +192,14 @@ class RefEngine:
         s = np.ascontiguousarray(scores, np.float64).copy()
         out = (C.c_double * 8)()
         self.L.dmstref_estimate_gumbel(s.ctypes.data_as(C.POINTER(C.c_double)), len(s), seq_length, out)
+        return np.array(out[:])
+
+    def estimate_k(self, p: int, sequence_length: int, border: int, num: int, threads: int = 1,
+                   scores_path: str | None = None) -> np.ndarray:
+        """The reference's estimateK on profile p: [lambda, K, lambda_filter, K_filter]."""
+        out = (C.c_double * 4)()
+        st = self.L.dmstref_estimate_k(p, sequence_length, border, num, threads,
+                                       scores_path.encode() if scores_path else None, out)
+        if st != 0:
+            raise ValueError("reference estimateK rejected the arguments")
         return np.array(out[:])

@@ -391,4 +391,34 @@ void dmstref_estimate_gumbel(double *scores, int n, double seqLength, double *ou
     estimateGumbel(out8[0], out8[1], out8[2], out8[3], out8[4], out8[5], out8[6], out8[7], scores, n, seqLength);
 }
 
+// The reference's own calibration of profile p, estimateK
+// (dummest-calibration.hh:338-649), called the way dummest.cc:395-408 calls
+// it: letter frequencies = the profile's background row, nthreads workers.
+// out4 = lambda (MM, mid), K (MM, mid), lambda_filter, K_filter.  With
+// scoresPath the per-trial scores go to that file (estimateK then bypasses
+// its cache), as the CLI's scores option does.
+int dmstref_estimate_k(int p, int seqLen, int border, int num, int nthreads, const char *scoresPath,
+                       double *out4) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || seqLen < 1 || border < 0 || num < 2 || nthreads < 1 || !out4) return -1;
+    Profile prof = *pr;  // estimateK stores lambda/K into the profile
+    const Float *bgProbs = prof.values + prof.width * prof.length + 4;
+    std::vector<char> buf(seqLen + border + 64);
+    std::ofstream scores;
+    if (scoresPath) scores.open(scoresPath);
+    {
+        ThreadPool pool(nthreads);
+        std::vector<DPScratch> scratches(nthreads);
+        estimateK(prof, bgProbs, buf.data(), seqLen, border, num, 0, pool, scratches,
+                  scoresPath ? &scores : nullptr, nullptr);
+    }
+    out4[0] = prof.lambda;
+    out4[1] = prof.gumbelKmidAnchored;
+    out4[2] = prof.lambda_filter;
+    out4[3] = prof.gumbel_k_filter;
+    return 0;
+}
+
 }  // extern "C"

@@ -99,6 +99,33 @@ def test_mid_and_filter_match_fp32_reference(ref32, ref64, tmp_path, rows_per_la
         print(f"R={rows_per_lane}: max |d bits| vs FP32 ref {worst:.3e}, vs FP64 ref {worst64:.3e}, exact-path pairs {n_exact}")
 
 
+def test_mid_and_filter_bit_identical_to_oracle(ref32, tmp_path):
+    """The batched kernel, the plain C oracle and the FP32 reference give the
+    same ExpScores, mantissa and exponent, for every pair: the float
+    recurrences use the reference's operations in its order (including the
+    multiply-adds its compiler forms) and the scores are exact products."""
+    from oracle import port
+    Ms = [2, 31, 33, 128, 257]
+    rng, profs, txt = _setup_profiles(tmp_path, ref32, Ms, seed=41)
+    reads = _mk_reads(rng, profs, [3, 4, 7, 33, 150, 640, 1000])
+    codes = [ref32.decode(ref32.encode(s)) for s in reads]
+    with d.Context(device=0) as ctx:
+        pids = ctx.load_hmm(txt)
+        sids = ctx.add_decoded(codes)
+        for p, pid in enumerate(pids):
+            _, values, params, bg = ref32.profile(p)
+            got = ctx.score_pairs(sids, pid, d.MODE_MID)
+            want = ref32.find_similarities(p, codes)
+            gf = ctx.score_pairs(sids, pid, d.MODE_FILTER)
+            wf = ref32.backward_only(p, codes)
+            for c, g, w, f, w_f in zip(codes, got, want, gf, wf):
+                mid, flt, _ = port.score_pair(values, params, bg, c)
+                assert mid == (w[0], w[1]) and flt == (w[3], w[4])  # oracle pinned to the reference
+                assert (g.mid.m, g.mid.e) == mid, (Ms[p], len(c), g, mid)
+                assert (g.filter.m, g.filter.e) == flt, (Ms[p], len(c), g, flt)
+                assert f.filter_f == w_f == port.filter_pair(values, params, bg, c), (Ms[p], len(c))
+
+
 def test_regression_fixtures(gpu_ctx, regression):
     """The reference's overflow regression inputs (herpes: scores ~e^1554,
     rescaled rows; medium: E ~ 1e-216): every record within 1e-3 bits of the
@@ -113,6 +140,9 @@ def test_regression_fixtures(gpu_ctx, regression):
     for k, r in enumerate(res):
         want = _bits(g["mid_ln_f32"][k])
         assert abs(_bits(r.mid_ln) - want) <= BITS_TOL, (g["record_names"][k], _bits(r.mid_ln), want)
+        # herpes0+ takes the row-rescaled exact path; every record is bit-identical.
+        assert (r.mid.m, r.mid.e) == (g["mid_m_f32"][k], g["mid_e_f32"][k]), (g["record_names"][k], r.mid)
+        assert (r.filter.m, r.filter.e) == (g["filter_m_f32"][k], g["filter_e_f32"][k]), (g["record_names"][k], r)
     names = list(g["record_names"])
     assert abs(_bits(res[names.index("herpes0+")].mid_ln) - 2242.35) <= 6  # test_overflow.sh:67,69
     assert abs(_bits(res[names.index("medium0+")].mid_ln) - 754.34) <= 1  # test_overflow.sh:68,70
