@@ -69,16 +69,34 @@ def parse():
 # distributed plumbing (one process per GPU, weak scaling: every rank scores
 # its own reads against all profiles; no data-path collective)
 # ---------------------------------------------------------------------------
-def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+def dist_env():
+    """(rank, world, local rank) from the launcher's environment (torchrun)."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU; a short process-group timeout so that ranks that
+    wait for a missing peer end with an error instead of hanging."""
+    rank, world, local = dist_env()
     if world > 1:
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
     return rank, world, local
+
+
+def _reduce(x: float, world: int, op: str) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
 
 
 def barrier(world):
@@ -88,28 +106,42 @@ def barrier(world):
 
 
 def allreduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _reduce(x, world, "max")
 
 
 def allreduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, "sum")
+
+
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank scores its own reads (weak scaling: pairs shard by rank)."""
+    return seed + 1 + 1000 * rank
+
+
+def aggregate(cells: float, ms: float, world: int) -> tuple[float, float, float]:
+    """Whole-job throughput: the cells of all ranks over the slowest rank's
+    device time.  Returns (GCUPS, max ms, total cells)."""
+    ms_max = allreduce_max(ms, world)
+    cells_all = allreduce_sum(cells, world)
+    return cells_all / (ms_max * 1e-3) / 1e9, ms_max, cells_all
 
 
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
+def workload_config(args, world: int) -> dict:
+    """The workload both arms report (cells_per_step is added by the GPU arm,
+    which counts them)."""
+    return {
+        "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform 50-800 x "
+                    "reads L log-uniform 150-3000 nt, GC 0.4-0.6, 10% implants, both strands",
+        "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
+        "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
+        "l2": "inputs larger than L2 (W1 slots)",
+        "parallelism": f"replicas x{world} (pairs sharded per rank)",
+    }
+
+
 def make_profiles(seed, n):
     from dummest_b200 import synth
     rng = np.random.default_rng(seed)
@@ -245,7 +277,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     profiles, txt = make_profiles(args.seed, args.profiles)
-    steps = make_steps(args.seed + 1, profiles, 1, args.reads_per_step)
+    steps = make_steps(rank_seed(args.seed, 0), profiles, 1, args.reads_per_step)
     vals = []
     cb = None
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
@@ -258,8 +290,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "GCUPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batched fwd+bwd, 64 profiles M 50-800 x reads L 150-3000 both strands",
-                   "reads_per_step": args.reads_per_step, "profiles": args.profiles},
+        "config": workload_config(args, world),
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -273,7 +304,7 @@ def run_ours(args, rank, world, local):
 
     profiles, txt = make_profiles(args.seed, args.profiles)
     n_steps = args.warmup + args.steps
-    steps = make_steps(args.seed + 1 + 1000 * rank, profiles, n_steps, args.reads_per_step)
+    steps = make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step)
     ctx = d.Context(device=local, rows_per_lane=args.rows_per_lane)
     pids = ctx.load_hmm(txt)
     Ms = np.array([ctx.profile_length(p) for p in pids])
@@ -321,9 +352,7 @@ def run_ours(args, rank, world, local):
     barrier(world)
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    ms_max = allreduce_max(ms, world)
-    cells_all = allreduce_sum(cells, world)
-    value = cells_all / (ms_max / 1e3) / 1e9
+    value, ms_max, cells_all = aggregate(cells, ms, world)
 
     # ---- roofline of the DP kernels (CUDA-event durations) ----
     peaks = measured_peaks()
@@ -404,14 +433,7 @@ def run_ours(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {
-                "workload": "batched fwd+bwd (mid-anchored score): 64 profiles M log-uniform 50-800 x "
-                            "reads L log-uniform 150-3000 nt, GC 0.4-0.6, 10% implants, both strands",
-                "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
-                "profiles": args.profiles, "pairs_per_step": len(step_pairs[0]),
-                "cells_per_step": cells / args.steps, "l2": "inputs larger than L2 (W1 slots)",
-                "parallelism": f"replicas x{world} (pairs sharded per rank)",
-            },
+            "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
             "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
@@ -422,6 +444,13 @@ def run_ours(args, rank, world, local):
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        # The reference's CPU engine runs on rank 0 alone; it needs no process
+        # group, and the other ranks exit without work.
+        rank, world, _ = dist_env()
+        if rank == 0:
+            run_reference(args, rank, world)
+        return
     rank, world, local = dist_setup()
     try:
         if args.impl == "reference":
