@@ -91,12 +91,15 @@ template <typename T>
 struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;  // elements
+    // Capacity for n elements, contents not kept.  Growth is geometric (x1.25)
+    // so that calls whose sizes vary a little do not reallocate (cudaFree and
+    // cudaMalloc synchronise the device).
     cudaError_t ensure(size_t n) {
         if (n <= cap && p) return cudaSuccess;
+        const size_t want = std::max<size_t>({n, cap + cap / 4, 1});
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
-        size_t want = std::max<size_t>(n, 1);
         cudaError_t e = cudaMalloc(&p, want * sizeof(T));
         if (e == cudaSuccess) cap = want;
         return e;

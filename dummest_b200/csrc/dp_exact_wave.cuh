@@ -108,16 +108,21 @@ __global__ void __launch_bounds__(kLanes) exactWaveKernel(const ExactWaveJob *jo
             smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
         }
         __syncwarp();
+        if (lane == 0) {
+            PairCold &c = win.cold;
+            c.codes = codes + p.codeOff;
+            c.pre = seeds + p.seedOff;
+            c.suf = c.pre + p.L;
+            c.params = params + pr.paramOff;
+            c.smBg = smBg;
+            c.sc = scales[job.pair];
+            c.M = p.M;
+        }
+        __syncwarp();
         SweepArgs a;
-        a.codes = codes + p.codeOff;
-        a.pre = seeds + p.seedOff;
-        a.suf = a.pre + p.L;
-        a.params = params + pr.paramOff;
+        a.cold = &win.cold;
         a.smE = smE;
-        a.smBg = smBg;
-        a.sc = scales[job.pair];
         a.L = p.L;
-        a.M = p.M;
         a.rowPad = rowPad;
         a.nS = (p.M + 1 + kLanes * kExactR - 1) / (kLanes * kExactR);
         a.P = wavePeriod(p.L);

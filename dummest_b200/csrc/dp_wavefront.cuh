@@ -12,9 +12,14 @@
 //
 // Per-column operands (codon code, background, seeds, and the ring values of
 // the stripe boundary) are staged in a per-warp shared-memory window indexed
-// by lane-local time, refilled once every 32 steps by one coalesced load per
-// lane; a step reads its column with one 16-byte shared load.  The forward
-// reads W1 two steps ahead into registers.
+// by lane-local time, refilled once every 48 steps by coalesced loads; a step
+// reads its column with one 16-byte shared load.  The forward copies W1 five
+// steps ahead into a shared-memory ring with cp.async, so that the DRAM
+// latency of the W1 round trip is hidden without holding registers.
+//
+// Steps run in groups of three (six in the forward): the three-column
+// histories of each row live in register slots whose roles rotate with the
+// step's phase, so the history shifts by renaming instead of copying.
 //
 // The recurrences are the reference's, term for term and in the same
 // association order (so that the float rounding matches):
@@ -42,17 +47,48 @@
 
 namespace dmst {
 
-struct SweepArgs {
+// Fields of the pair that the sweeps read only at window refills and stripe
+// starts.  They sit in the warp's shared memory and are read through volatile
+// loads, so that the compiler re-reads them instead of holding them in
+// registers across the sweeps.
+struct PairCold {
     const uint8_t *codes;   // codon codes of the read
     const float *pre;       // prefixSeed[L]
     const float *suf;       // suffixSeedFromNext[L]
     const float *params;    // the profile's (M+2) x 11 Params
-    const float *smE;       // emission table in shared memory, [25][rowPad]
     const float *smBg;      // bg_probs[4 + c] in shared memory
+    PairScales sc;
+    int M;
+    int pad[3];
+};
+
+struct SweepArgs {
+    PairCold *cold;         // in shared memory
+    const float *smE;       // emission table in shared memory, [25][rowPad]
     float *w1;              // this warp's W1 slot
     float *ring;            // this warp's stripe-boundary ring (4 floats per column)
-    PairScales sc;
-    int L, M, rowPad, nS, P, D;
+    int L, rowPad, nS, P, D;
+
+    __device__ __forceinline__ const uint8_t *codes() const {
+        return *reinterpret_cast<const uint8_t *const volatile *>(&cold->codes);
+    }
+    __device__ __forceinline__ const float *pre() const {
+        return *reinterpret_cast<const float *const volatile *>(&cold->pre);
+    }
+    __device__ __forceinline__ const float *suf() const {
+        return *reinterpret_cast<const float *const volatile *>(&cold->suf);
+    }
+    __device__ __forceinline__ const float *params() const {
+        return *reinterpret_cast<const float *const volatile *>(&cold->params);
+    }
+    __device__ __forceinline__ const float *smBg() const {
+        return *reinterpret_cast<const float *const volatile *>(&cold->smBg);
+    }
+    __device__ __forceinline__ PairScales sc() const {
+        const volatile PairScales *v = &cold->sc;
+        return PairScales{v->s1, v->s2, v->sC, 0.0f};
+    }
+    __device__ __forceinline__ int M() const { return *reinterpret_cast<const volatile int *>(&cold->M); }
 };
 
 template <int R>
@@ -63,19 +99,22 @@ struct Coef {
 // Backward coefficients of rows rowBase..rowBase+R-1 (dummest-dp-backward.hh:481-494).
 template <int R>
 __device__ __forceinline__ void loadBackwardCoef(Coef<R> &c, const SweepArgs &a, int rowBase) {
+    const int M = a.M();
+    const float *params = a.params();
+    const PairScales sc = a.sc();
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int i = rowBase + k;
-        if (i <= a.M) {
-            const float *q = a.params + (size_t)i * kParamFloats;
-            c.enter[k] = q[10] * a.sc.sC;
+        if (i <= M) {
+            const float *q = params + (size_t)i * kParamFloats;
+            c.enter[k] = q[10] * sc.sC;
             c.d0[k] = q[6];
-            c.d1[k] = q[7] * a.sc.s2;
-            c.d2[k] = q[8] * a.sc.s1;
-            c.a0[k] = q[0] * a.sc.sC;
-            c.a1[k] = q[1] * a.sc.s1;
-            c.a2[k] = q[2] * a.sc.s2;
-            c.b0[k] = q[3] * a.sc.sC;
+            c.d1[k] = q[7] * sc.s2;
+            c.d2[k] = q[8] * sc.s1;
+            c.a0[k] = q[0] * sc.sC;
+            c.a1[k] = q[1] * sc.s1;
+            c.a2[k] = q[2] * sc.s2;
+            c.b0[k] = q[3] * sc.sC;
             c.eps[k] = q[9];
             c.rs[k] = 1.0f;
         } else {
@@ -89,19 +128,22 @@ __device__ __forceinline__ void loadBackwardCoef(Coef<R> &c, const SweepArgs &a,
 // unscaled here, the codon scale multiplies the background term instead.
 template <int R>
 __device__ __forceinline__ void loadForwardCoef(Coef<R> &c, const SweepArgs &a, int rowBase) {
+    const int M = a.M();
+    const float *params = a.params();
+    const PairScales sc = a.sc();
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int i = rowBase + k;
-        if (i <= a.M) {
-            const float *q = a.params + (size_t)i * kParamFloats;
-            c.enter[k] = q[10] * a.sc.sC;
+        if (i <= M) {
+            const float *q = params + (size_t)i * kParamFloats;
+            c.enter[k] = q[10] * sc.sC;
             c.a0[k] = q[0];
-            c.a1[k] = q[1] * a.sc.s1;
-            c.a2[k] = q[2] * a.sc.s2;
+            c.a1[k] = q[1] * sc.s1;
+            c.a2[k] = q[2] * sc.s2;
             c.b0[k] = q[3];
             c.d0[k] = q[6];
-            c.d1[k] = q[7] * a.sc.s2;
-            c.d2[k] = q[8] * a.sc.s1;
+            c.d1[k] = q[7] * sc.s2;
+            c.d2[k] = q[8] * sc.s1;
             c.eps[k] = q[9];
             c.rs[k] = 1.0f;
         } else {
@@ -151,20 +193,35 @@ __device__ __forceinline__ void loadW1(float (&w)[R], const float *p) {
 }
 
 // ---------------------------------------------------------------------------
-// Wavefront geometry.  The period P of a lane (steps per stripe) is at least
-// kMinPeriod, so that a stripe-boundary value is written by one lane at least
-// 64 steps before the window refill that hands it to the other lane.
+// Wavefront geometry.  Steps run in blocks of kBlock (a multiple of three);
+// the window holds the column operands of local times [t0 - 31, t0 + 2 kBlock)
+// around a block starting at t0 (127 entries), and each block start refills
+// the kBlock entries of the next block.  The period P of a lane (steps per
+// stripe) is at least kMinPeriod, so that a stripe-boundary value is written
+// by one lane before the window refill that hands it to the other lane
+// (31 + s P + j < (s+1) P + j - 2 kBlock + 1 for every stripe s and column j).
 // ---------------------------------------------------------------------------
-constexpr int kMinPeriod = 96;
+constexpr int kBlock = 48;
+constexpr int kMinPeriod = 128;
 constexpr int kWin = 128;  // window entries (lane-local times), a power of two
+static_assert(kBlock % 6 == 0 && kBlock <= kWin - 31 - kBlock, "window geometry");
+static_assert(kMinPeriod >= 31 + 2 * kBlock, "stripe hand-off before the refill that reads it");
 
 __host__ __device__ inline int wavePeriod(int L) { return L > kMinPeriod ? L : kMinPeriod; }
 
 // Per-warp staging window: entry t & (kWin-1) holds the column operands of
 // lane-local time t.
+// W1 staging of the forward sweep: each lane copies its R values of W1 for
+// the step kW1Ahead steps ahead into a ring of kW1Slots slots (cp.async, one
+// commit group per step), so that a step waits on shared memory, not DRAM.
+constexpr int kW1Slots = 6;
+constexpr int kW1Ahead = kW1Slots - 1;
+
 struct Window {
     float4 col[kWin];   // backward: {code, bg, suf, pre}; forward: {code, bg*sC, pre, unused}
     float4 ring[kWin];  // stripe-boundary (W, Y, scale count) for the lane that reads the ring
+    float4 w1[kW1Slots][kLanes];  // forward W1 staging ring (lane l uses [slot][l], R floats)
+    PairCold cold;      // the pair in flight: fields read only at refills and stripe starts
 };
 
 // The stripe-boundary ring in global memory: 4 floats per column.
@@ -187,8 +244,8 @@ __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int 
         const int sp = u / a.P, jj = u - sp * a.P;
         if (jj < a.L) {
             const int j = a.L - 1 - jj;
-            const int code = (j + 1 < a.L) ? (int)__ldg(a.codes + j + 1) : kPad;
-            c = make_float4(__int_as_float(code), a.smBg[code], __ldg(a.suf + j), __ldg(a.pre + j));
+            const int code = (j + 1 < a.L) ? (int)__ldg(a.codes() + j + 1) : kPad;
+            c = make_float4(__int_as_float(code), a.smBg()[code], __ldg(a.suf() + j), __ldg(a.pre() + j));
             if (sp > 0) r = ringLoad(a.ring, jj);
         }
     }
@@ -204,8 +261,8 @@ __device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u
     if (u >= 0 && u < a.nS * a.P) {
         const int s = u / a.P, j = u - s * a.P;
         if (j < a.L) {
-            const int code = (j >= 2) ? (int)__ldg(a.codes + j - 2) : kPad;
-            c = make_float4(__int_as_float(code), a.smBg[code] * a.sc.sC, __ldg(a.pre + j), 0.0f);
+            const int code = (j >= 2) ? (int)__ldg(a.codes() + j - 2) : kPad;
+            c = make_float4(__int_as_float(code), a.smBg()[code] * a.sc().sC, __ldg(a.pre() + j), 0.0f);
             if (s > 0) r = ringLoad(a.ring, j);
         }
     }
@@ -265,229 +322,305 @@ struct ExactRows {
 
 // ---------------------------------------------------------------------------
 // Backward sweep (dummest-dp-backward.hh:473-574; the float filter :367-430).
+//
+// Steps run in groups of three.  A row's history (W1 and Z at columns j+1,
+// j+2, j+3) lives in three register slots whose roles rotate with the step's
+// phase PH = t mod 3: slot (3-PH)%3 holds column j+1, (4-PH)%3 column j+2 and
+// (5-PH)%3 column j+3, and the new value of column j replaces column j+3.  The
+// history then shifts by renaming, with no register copies.
 // ---------------------------------------------------------------------------
+template <int R, int MODE>
+struct BwdState {
+    Coef<R> c;
+    float h[3][R], z[3][R];  // this lane's rows: W1 and Z history slots
+    float rb[3];             // the row below (the next lane's top row): W1 history slots
+    float sendW, sendY, filt, maxY;
+    int sendC;
+    int realRows;            // rows of this lane at or above row M (the rest are padding)
+    int u, sp, jj;           // lane-local time, stripe from the bottom, column from the right
+    float *wp;               // W1 store pointer of the current step
+    // exact-path state
+    int cnt;                 // discovery: this lane's scale count
+    float rmax[R];           // discovery: per-row maxima at count cnt
+    int cOut[R];             // replay: count of each row after its decision
+    float fOut[R];           // replay: 1 or 2^-64, the row's own rescale
+    double rowBest[R];       // replay: per-row max of W1 * prefixSeed
+};
+
+template <int R, int MODE, int PH>
+__device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepArgs &a, Window &win, int lane,
+                                             int total, const ExactRows *x, ExactBest *exact) {
+    constexpr int S = kLanes * R;
+    constexpr bool kStore = MODE == kMid || MODE == kReplay;
+    constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
+    float inW = __shfl_down_sync(kFull, b.sendW, 1);
+    float inY = __shfl_down_sync(kFull, b.sendY, 1);
+    int inC = 0;
+    if (MODE == kDiscover) inC = __shfl_down_sync(kFull, b.sendC, 1);
+    const int lag = kLanes - 1 - lane;
+    if (b.u >= 0 && b.u < total && b.jj < a.L) {
+        const int s = a.nS - 1 - b.sp;
+        const int rowBase = s * S + lane * R;
+        if (b.jj == 0) {
+            loadBackwardCoef<R>(b.c, a, rowBase);
+            b.realRows = min(max(a.M() - rowBase + 1, 0), R);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) b.h[q][k] = b.z[q][k] = 0.0f;
+                b.rb[q] = 0.0f;
+            }
+            b.wp = a.w1 + (((size_t)s * a.D + lag) * kLanes + lane) * R;
+            if (MODE == kDiscover) {
+                b.cnt = 0;
+#pragma unroll
+                for (int k = 0; k < R; ++k) b.rmax[k] = 0.0f;
+            }
+            if (MODE == kReplay) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    const int i = rowBase + k;
+                    const int ci = i <= a.M() ? i : a.M() + 1;
+                    const int cIn = x->cntB[ci + 1 <= a.M() + 1 ? ci + 1 : a.M() + 1];
+                    b.cOut[k] = x->cntB[ci];
+                    b.fOut[k] = stepsDown(b.cOut[k] - cIn);
+                    b.c.rs[k] = seedCoef(i <= a.M(), cIn);
+                    b.rowBest[k] = 0.0;
+                }
+            }
+        }
+        const int slot = b.u & (kWin - 1);
+        const float4 col = win.col[slot];
+        if (lane == kLanes - 1) {
+            const float4 r = win.ring[slot];
+            inW = r.x;
+            inY = r.y;
+            if (MODE == kDiscover) inC = __float_as_int(r.z);
+        }
+        if (MODE == kDiscover) {
+            // Align the incoming values and this lane to one scale.
+            if (inC > b.cnt) {
+                const float f = stepsDown(inC - b.cnt);
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        b.h[q][k] *= f;
+                        b.z[q][k] *= f;
+                    }
+                    b.rmax[k] *= f;
+                    b.c.rs[k] = seedCoef(rowBase + k <= a.M(), inC);
+                }
+#pragma unroll
+                for (int q = 0; q < 3; ++q) b.rb[q] *= f;
+                b.cnt = inC;
+            } else if (inC < b.cnt) {
+                const float f = stepsDown(b.cnt - inC);
+                inW *= f;
+                inY *= f;
+            }
+        }
+        const int code = __float_as_int(col.x);
+        const float bgv = col.y, sufv = col.z, prev = col.w;
+        float e[R];
+        loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
+        // First products (W1[i+1][j+3] * e) * enter, taken before any row of
+        // this step overwrites its column-j+3 slot.
+        float p[R];
+        p[R - 1] = (b.rb[I3] * e[R - 1]) * b.c.enter[R - 1];
+#pragma unroll
+        for (int k = 0; k < R - 1; ++k) {
+            const float h3 = (MODE == kReplay) ? b.h[I3][k + 1] * b.fOut[k + 1] : b.h[I3][k + 1];
+            p[k] = (h3 * e[k]) * b.c.enter[k];
+        }
+        float bW1 = b.rb[I1], bW2 = b.rb[I2], bY = inY;
+        float wv[R];
+        float stepMax = 0.0f;
+#pragma unroll
+        for (int k = R - 1; k >= 0; --k) {
+            float acc = p[k];
+            acc = __fmaf_rn(bY, b.c.d0[k], acc);
+            acc = __fmaf_rn(bW2, b.c.d1[k], acc);
+            acc = __fmaf_rn(bW1, b.c.d2[k], acc);
+            const float zbg = b.z[I3][k] * bgv;
+            acc = __fmaf_rn(zbg, b.c.a0[k], acc);
+            acc = __fmaf_rn(b.h[I2][k], b.c.a2[k], acc);
+            acc = __fmaf_rn(b.h[I1][k], b.c.a1[k], acc);
+            // Seed term fma(suf, rs, acc): rs is 1 on real rows, so the fast
+            // modes add suf exactly; rows past M (zero coefficients and inputs)
+            // accumulate exactly 0 and must stay 0, so they take no seed.
+            const float W = (MODE == kFilter || MODE == kMid) ? __fadd_rn(acc, k < b.realRows ? sufv : 0.0f)
+                                                             : __fmaf_rn(sufv, b.c.rs[k], acc);
+            const float Y = __fmaf_rn(b.c.eps[k], bY, W);
+            const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
+            if (MODE == kFilter || MODE == kMid) {
+                b.maxY = fmaxf(b.maxY, Y);
+                b.filt = fmaxf(b.filt, W * prev);
+            }
+            if (MODE == kDiscover) {
+                b.rmax[k] = fmaxf(b.rmax[k], Y);  // Y >= W1 at every cell
+                stepMax = fmaxf(stepMax, Y);
+            }
+            if (MODE == kReplay) {
+                // What leaves the row is scaled by the row's own decision.
+                const float Wo = W * b.fOut[k];
+                b.rowBest[k] = fmax(b.rowBest[k], (double)Wo * (double)prev);
+                bW1 = b.h[I1][k] * b.fOut[k];
+                bW2 = b.h[I2][k] * b.fOut[k];
+                bY = Y * b.fOut[k];
+                wv[k] = Wo;
+            } else {
+                bW1 = b.h[I1][k];
+                bW2 = b.h[I2][k];
+                bY = Y;
+                wv[k] = W;
+            }
+            b.h[I3][k] = W;
+            b.z[I3][k] = Z;
+        }
+        b.rb[I3] = inW;
+        b.sendW = wv[0];
+        b.sendY = bY;
+        if (MODE == kDiscover) {
+            if (stepMax > kBump) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        b.h[q][k] *= kStep;
+                        b.z[q][k] *= kStep;
+                    }
+                    b.rmax[k] *= kStep;
+                    b.c.rs[k] = seedCoef(rowBase + k <= a.M(), b.cnt + 1);
+                }
+#pragma unroll
+                for (int q = 0; q < 3; ++q) b.rb[q] *= kStep;
+                b.sendW *= kStep;
+                b.sendY *= kStep;
+                ++b.cnt;
+            }
+            b.sendC = b.cnt;
+        }
+        if (kStore) {
+            storeW1<R>(b.wp, wv);
+            b.wp += kLanes * R;
+        }
+        if (lane == 0 && b.sp < a.nS - 1) {
+            if (MODE == kDiscover)
+                ringStore(a.ring, b.jj, b.sendW, b.sendY, b.sendC);
+            else
+                ringStore(a.ring, b.jj, b.sendW, b.sendY);
+        }
+        if (b.jj == a.L - 1) {
+            // the last column of these rows
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const int i = rowBase + k;
+                if (i > a.M()) continue;
+                if (MODE == kDiscover) {
+                    x->rowMax[i] = b.rmax[k];
+                    x->rowCnt[i] = b.cnt;
+                }
+                if (MODE == kReplay) foldBest(*exact, b.rowBest[k], b.cOut[k]);
+            }
+        }
+    } else {
+        b.sendW = 0.0f;
+        b.sendY = 0.0f;
+        b.sendC = 0;
+    }
+    if (b.u >= 0 && ++b.jj == a.P) {
+        b.jj = 0;
+        ++b.sp;
+    }
+    ++b.u;
+}
+
+// Window refills for a block of kBlock steps starting at t0: local times
+// [t0 + kBlock, t0 + 2 kBlock), one entry per lane and pass.
+template <bool BACKWARD>
+__device__ __forceinline__ void fillBlock(Window &win, const SweepArgs &a, int first, int lane) {
+#pragma unroll
+    for (int o = 0; o < kBlock; o += kLanes) {
+        if (o + lane < kBlock) {
+            if (BACKWARD)
+                fillBackward(win, a, first + o + lane);
+            else
+                fillForward(win, a, first + o + lane);
+        }
+    }
+}
+
 template <int R, int MODE>
 __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &filtOut, float &maxYOut,
                               const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
-    constexpr int S = kLanes * R;
-    constexpr bool kStore = MODE == kMid || MODE == kReplay;
-    Coef<R> c;
-    float h1[R], h2[R], h3[R], z1[R], z2[R], z3[R];
+    BwdState<R, MODE> b;
 #pragma unroll
-    for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
-    float rb1 = 0.0f, rb2 = 0.0f, rb3 = 0.0f;  // row below (other lane) at j+1..j+3
-    float sendW = 0.0f, sendY = 0.0f;
-    int sendC = 0;
-    float filt = 0.0f, maxY = 0.0f;
-    // exact-path state
-    int cnt = 0;                  // discovery: this lane's scale count
-    float rmax[R];                // discovery: per-row maxima at count cnt
-    int cOut[R];                  // replay: count of each row after its decision
-    float fOut[R];                // replay: 1 or 2^-64, the row's own rescale
-    double rowBest[R];            // replay: per-row max of W1 * prefixSeed
-    if constexpr (MODE == kDiscover || MODE == kReplay) {
+    for (int q = 0; q < 3; ++q) {
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            rmax[k] = 0.0f;
-            cOut[k] = 0;
-            fOut[k] = 1.0f;
-            rowBest[k] = 0.0;
-        }
+        for (int k = 0; k < R; ++k) b.h[q][k] = b.z[q][k] = 0.0f;
+        b.rb[q] = 0.0f;
     }
-    const int L = a.L, P = a.P, nS = a.nS;
-    const int total = nS * P;
-    const int T = total + (kLanes - 1);
-    const int lag = kLanes - 1 - lane;  // lane 31 leads
-    int u = -lag;                       // local time
-    int sp = 0, jj = 0;                 // stripe from the bottom, column from the right
-    float *wp = a.w1;                   // W1 store pointer of the current step
-    // Window: local times [0, 64) now, then 32 ahead at every block start.
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        b.rmax[k] = 0.0f;
+        b.cOut[k] = 0;
+        b.fOut[k] = 1.0f;
+        b.rowBest[k] = 0.0;
+    }
+    b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
+    b.sendC = b.cnt = 0;
+    b.realRows = 0;
+    b.u = -(kLanes - 1 - lane);  // lane 31 leads
+    b.sp = b.jj = 0;
+    b.wp = a.w1;
+    const int total = a.nS * a.P;
+    const int T = (total + (kLanes - 1) + 2) / 3 * 3;  // whole groups of three steps
     __syncwarp();
-    fillBackward(win, a, lane);
-    fillBackward(win, a, lane + 32);
-    for (int t0 = 0; t0 < T; t0 += 32) {
+    fillBlock<true>(win, a, 0, lane);
+    for (int t0 = 0; t0 < T; t0 += kBlock) {
         __syncwarp();
-        if (t0 > 0) fillBackward(win, a, t0 + 32 + lane);
-        const int tEnd = t0 + 32 < T ? t0 + 32 : T;
-        for (int t = t0; t < tEnd; ++t) {
-            float inW = __shfl_down_sync(kFull, sendW, 1);
-            float inY = __shfl_down_sync(kFull, sendY, 1);
-            int inC = 0;
-            if (MODE == kDiscover) inC = __shfl_down_sync(kFull, sendC, 1);
-            if (u >= 0 && u < total && jj < L) {
-                const int s = nS - 1 - sp;
-                const int rowBase = s * S + lane * R;
-                if (jj == 0) {
-                    loadBackwardCoef<R>(c, a, rowBase);
-#pragma unroll
-                    for (int k = 0; k < R; ++k) h1[k] = h2[k] = h3[k] = z1[k] = z2[k] = z3[k] = 0.0f;
-                    rb1 = rb2 = rb3 = 0.0f;
-                    wp = a.w1 + (((size_t)s * a.D + lag) * kLanes + lane) * R;
-                    if (MODE == kDiscover) {
-                        cnt = 0;
-#pragma unroll
-                        for (int k = 0; k < R; ++k) rmax[k] = 0.0f;
-                    }
-                    if (MODE == kReplay) {
-#pragma unroll
-                        for (int k = 0; k < R; ++k) {
-                            const int i = rowBase + k;
-                            const int ci = i <= a.M ? i : a.M + 1;
-                            const int cIn = x->cntB[ci + 1 <= a.M + 1 ? ci + 1 : a.M + 1];
-                            cOut[k] = x->cntB[ci];
-                            fOut[k] = stepsDown(cOut[k] - cIn);
-                            c.rs[k] = seedCoef(i <= a.M, cIn);
-                            rowBest[k] = 0.0;
-                        }
-                    }
-                }
-                const int slot = u & (kWin - 1);
-                const float4 col = win.col[slot];
-                if (lane == kLanes - 1) {
-                    const float4 r = win.ring[slot];
-                    inW = r.x;
-                    inY = r.y;
-                    if (MODE == kDiscover) inC = __float_as_int(r.z);
-                }
-                if (MODE == kDiscover) {
-                    // Align the incoming values and this lane to one scale.
-                    if (inC > cnt) {
-                        const float f = stepsDown(inC - cnt);
-#pragma unroll
-                        for (int k = 0; k < R; ++k) {
-                            h1[k] *= f; h2[k] *= f; h3[k] *= f;
-                            z1[k] *= f; z2[k] *= f; z3[k] *= f;
-                            rmax[k] *= f;
-                            c.rs[k] = seedCoef(rowBase + k <= a.M, inC);
-                        }
-                        rb1 *= f; rb2 *= f; rb3 *= f;
-                        cnt = inC;
-                    } else if (inC < cnt) {
-                        const float f = stepsDown(cnt - inC);
-                        inW *= f;
-                        inY *= f;
-                    }
-                }
-                const int code = __float_as_int(col.x);
-                const float bgv = col.y, sufv = col.z, prev = col.w;
-                float e[R];
-                loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
-                float bW1 = rb1, bW2 = rb2, bW3 = rb3, bY = inY;
-                float wv[R];
-                float stepMax = 0.0f;
-#pragma unroll
-                for (int k = R - 1; k >= 0; --k) {
-                    float acc = (bW3 * e[k]) * c.enter[k];
-                    acc = __fmaf_rn(bY, c.d0[k], acc);
-                    acc = __fmaf_rn(bW2, c.d1[k], acc);
-                    acc = __fmaf_rn(bW1, c.d2[k], acc);
-                    const float zbg = z3[k] * bgv;
-                    acc = __fmaf_rn(zbg, c.a0[k], acc);
-                    acc = __fmaf_rn(h2[k], c.a2[k], acc);
-                    acc = __fmaf_rn(h1[k], c.a1[k], acc);
-                    const float W = __fmaf_rn(sufv, c.rs[k], acc);
-                    const float Y = __fmaf_rn(c.eps[k], bY, W);
-                    const float Z = __fmaf_rn(c.b0[k], zbg, W);
-                    if (MODE == kFilter || MODE == kMid) {
-                        maxY = fmaxf(maxY, Y);
-                        filt = fmaxf(filt, W * prev);
-                    }
-                    if (MODE == kDiscover) {
-                        rmax[k] = fmaxf(rmax[k], Y);  // Y >= W1 at every cell
-                        stepMax = fmaxf(stepMax, Y);
-                    }
-                    if (MODE == kReplay) {
-                        // What leaves the row is scaled by the row's own decision.
-                        const float Wo = W * fOut[k];
-                        rowBest[k] = fmax(rowBest[k], (double)Wo * (double)prev);
-                        bW1 = h1[k] * fOut[k];
-                        bW2 = h2[k] * fOut[k];
-                        bW3 = h3[k] * fOut[k];
-                        bY = Y * fOut[k];
-                        wv[k] = Wo;
-                    } else {
-                        bW1 = h1[k];
-                        bW2 = h2[k];
-                        bW3 = h3[k];
-                        bY = Y;
-                        wv[k] = W;
-                    }
-                    h3[k] = h2[k];
-                    h2[k] = h1[k];
-                    h1[k] = W;
-                    z3[k] = z2[k];
-                    z2[k] = z1[k];
-                    z1[k] = Z;
-                }
-                rb3 = rb2;
-                rb2 = rb1;
-                rb1 = inW;
-                sendW = wv[0];
-                sendY = bY;
-                if (MODE == kDiscover) {
-                    if (stepMax > kBump) {
-#pragma unroll
-                        for (int k = 0; k < R; ++k) {
-                            h1[k] *= kStep; h2[k] *= kStep; h3[k] *= kStep;
-                            z1[k] *= kStep; z2[k] *= kStep; z3[k] *= kStep;
-                            rmax[k] *= kStep;
-                            c.rs[k] = seedCoef(rowBase + k <= a.M, cnt + 1);
-                        }
-                        rb1 *= kStep; rb2 *= kStep; rb3 *= kStep;
-                        sendW *= kStep;
-                        sendY *= kStep;
-                        ++cnt;
-                    }
-                    sendC = cnt;
-                }
-                if (kStore) {
-                    storeW1<R>(wp, wv);
-                    wp += kLanes * R;
-                }
-                if (lane == 0 && sp < nS - 1) {
-                    if (MODE == kDiscover)
-                        ringStore(a.ring, jj, sendW, sendY, sendC);
-                    else
-                        ringStore(a.ring, jj, sendW, sendY);
-                }
-                if (jj == L - 1) {
-                    // the last column of these rows
-#pragma unroll
-                    for (int k = 0; k < R; ++k) {
-                        const int i = rowBase + k;
-                        if (i > a.M) continue;
-                        if (MODE == kDiscover) {
-                            x->rowMax[i] = rmax[k];
-                            x->rowCnt[i] = cnt;
-                        }
-                        if (MODE == kReplay) foldBest(*exact, rowBest[k], cOut[k]);
-                    }
-                }
-            } else {
-                sendW = 0.0f;
-                sendY = 0.0f;
-                sendC = 0;
-            }
-            if (u >= 0 && ++jj == P) {
-                jj = 0;
-                ++sp;
-            }
-            ++u;
+        fillBlock<true>(win, a, t0 + kBlock, lane);
+        const int n = (t0 + kBlock < T ? kBlock : T - t0);
+#pragma unroll 1
+        for (int g = 0; g < n; g += 3) {
+            backwardStep<R, MODE, 0>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 1>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 2>(b, a, win, lane, total, x, exact);
         }
     }
-    filtOut = filt;
-    maxYOut = maxY;
+    filtOut = b.filt;
+    maxYOut = b.maxY;
 }
 
-// W1 read-ahead for the forward sweep: a cursor two steps ahead of the lane.
+// Asynchronous global-to-shared copies of W1 (cp.async: the copy bypasses the
+// registers; cp.async.wait_group orders it before the lane's own reads).
 template <int R>
-struct W1Ahead {
+__device__ __forceinline__ void cpAsyncW1(float4 *dst, const float *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (R == 4)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(4 * R) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// W1 staging cursor of the forward sweep: the lane-local time whose W1 is
+// copied next (kW1Ahead steps ahead of the lane).  Every call commits one
+// group, empty for steps the lane does not compute.
+template <int R>
+struct W1Stage {
     int u, s, j;
-    __device__ __forceinline__ void next(const SweepArgs &a, int lane, int total, float (&q)[R]) {
+    __device__ __forceinline__ void issue(const SweepArgs &a, Window &win, int slot, int lane, int total) {
         if (u >= 0 && u < total && j < a.L) {
             const int db = (a.L - 1 - j) + (kLanes - 1 - lane);
-            loadW1<R>(q, a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
+            cpAsyncW1<R>(&win.w1[slot][lane], a.w1 + (((size_t)s * a.D + db) * kLanes + lane) * R);
         }
+        cpAsyncCommit();
         if (u >= 0 && ++j == a.P) {
             j = 0;
             ++s;
@@ -499,11 +632,11 @@ struct W1Ahead {
 template <int R, int MODE>
 struct FwdState {
     Coef<R> c;
-    float w1[R], w2[R], w3[R], z1[R], z2[R], z3[R];
+    float w[3][R], z[3][R];  // W0 and Z0 history slots (rotating roles, see backwardStep)
     float sendIn, sendY, best, mx;
     int sendC;
     int u, s, j;
-    // exact-path state (see backwardSweep)
+    // exact-path state (see BwdState)
     int cnt;
     float rmax[R];
     int cIn[R], cB[R];
@@ -511,12 +644,14 @@ struct FwdState {
     double rowBest[R];
 };
 
-// One forward step of a lane (dummest-dp-forward.hh:112-223); q holds the W1
-// values of this step.
-template <int R, int MODE>
+// One forward step of a lane (dummest-dp-forward.hh:112-223) at phase PH;
+// q holds the W1 values of this step.  Slot (3-PH)%3 holds column j-1,
+// (4-PH)%3 column j-2, (5-PH)%3 column j-3, which the new column j replaces.
+template <int R, int MODE, int PH>
 __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                             int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
+    constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
     float inW = __shfl_up_sync(kFull, f.sendIn, 1);
     float inY = __shfl_up_sync(kFull, f.sendY, 1);
     int inC = 0;
@@ -526,7 +661,9 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         if (f.j == 0) {
             loadForwardCoef<R>(f.c, a, rowBase);
 #pragma unroll
-            for (int k = 0; k < R; ++k) f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
+            for (int h = 0; h < 3; ++h)
+#pragma unroll
+                for (int k = 0; k < R; ++k) f.w[h][k] = f.z[h][k] = 0.0f;
             if (MODE == kDiscover) {
                 f.cnt = 0;
 #pragma unroll
@@ -536,11 +673,11 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
                     const int i = rowBase + k;
-                    const int ci = i <= a.M ? i : a.M;
+                    const int ci = i <= a.M() ? i : a.M();
                     f.cIn[k] = x->cntF[ci];
                     f.fOut[k] = stepsDown(x->cntF[ci + 1] - f.cIn[k]);
                     f.cB[k] = x->cntB[ci];
-                    f.c.rs[k] = seedCoef(i <= a.M, f.cIn[k]);
+                    f.c.rs[k] = seedCoef(i <= a.M(), f.cIn[k]);
                     f.rowBest[k] = 0.0;
                 }
             }
@@ -558,10 +695,13 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
                 const float g = stepsDown(inC - f.cnt);
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
-                    f.w1[k] *= g; f.w2[k] *= g; f.w3[k] *= g;
-                    f.z1[k] *= g; f.z2[k] *= g; f.z3[k] *= g;
+#pragma unroll
+                    for (int h = 0; h < 3; ++h) {
+                        f.w[h][k] *= g;
+                        f.z[h][k] *= g;
+                    }
                     f.rmax[k] *= g;
-                    f.c.rs[k] = seedCoef(rowBase + k <= a.M, inC);
+                    f.c.rs[k] = seedCoef(rowBase + k <= a.M(), inC);
                 }
                 f.cnt = inC;
             } else if (inC < f.cnt) {
@@ -578,13 +718,14 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         float stepMax = 0.0f;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
+            const float w1 = f.w[I1][k], w2 = f.w[I2][k], w3 = f.w[I3][k];
             // The reference's operations as GCC contracts them at -O3
             // (dummest-dp-forward.hh:116-222): Z0 = (bg*sC)*fma(b0, Z0[j-3],
             // a0*w3); the alpha1/alpha2 products fuse into the W0 sum, and
             // Y0 = fma(eps, Y0[i-1], d0*W0).
-            const float X = (f.c.enter[k] * e[k]) * f.w3[k];
-            const float Z0 = bgsC * __fmaf_rn(f.c.b0[k], f.z3[k], f.c.a0[k] * f.w3[k]);
-            const float zs = __fmaf_rn(f.c.a2[k], f.w2[k], __fmaf_rn(f.c.a1[k], f.w1[k], Z0));
+            const float X = (f.c.enter[k] * e[k]) * w3;
+            const float Z0 = bgsC * __fmaf_rn(f.c.b0[k], f.z[I3][k], f.c.a0[k] * w3);
+            const float zs = __fmaf_rn(f.c.a2[k], w2, __fmaf_rn(f.c.a1[k], w1, Z0));
             // fma(prev, 1, x) is prev + x; in the fast mode every row takes the
             // seed: padding rows (past M, zero coefficients) then hold only
             // their seed, which reaches no real row and multiplies a zero W1.
@@ -593,17 +734,13 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
             const float Y0 = __fmaf_rn(f.c.eps[k], yab, f.c.d0[k] * W0);
             if (MODE == kMid) f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
-            const float nin = __fmaf_rn(f.c.d2[k], f.w1[k], __fmaf_rn(f.c.d1[k], f.w2[k], X + Y0));
+            const float nin = __fmaf_rn(f.c.d2[k], w1, __fmaf_rn(f.c.d1[k], w2, X + Y0));
             if (MODE == kDiscover) {
                 f.rmax[k] = fmaxf(f.rmax[k], fmaxf(W0, Y0));
                 stepMax = fmaxf(stepMax, fmaxf(fmaxf(W0, Y0), nin));
             }
-            f.w3[k] = f.w2[k];
-            f.w2[k] = f.w1[k];
-            f.w1[k] = W0;
-            f.z3[k] = f.z2[k];
-            f.z2[k] = f.z1[k];
-            f.z1[k] = Z0;
+            f.w[I3][k] = W0;
+            f.z[I3][k] = Z0;
             if (MODE == kReplay) {
                 win0 = nin * f.fOut[k];
                 yab = Y0 * f.fOut[k];
@@ -616,10 +753,13 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             if (stepMax > kBump) {
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
-                    f.w1[k] *= kStep; f.w2[k] *= kStep; f.w3[k] *= kStep;
-                    f.z1[k] *= kStep; f.z2[k] *= kStep; f.z3[k] *= kStep;
+#pragma unroll
+                    for (int h = 0; h < 3; ++h) {
+                        f.w[h][k] *= kStep;
+                        f.z[h][k] *= kStep;
+                    }
                     f.rmax[k] *= kStep;
-                    f.c.rs[k] = seedCoef(rowBase + k <= a.M, f.cnt + 1);
+                    f.c.rs[k] = seedCoef(rowBase + k <= a.M(), f.cnt + 1);
                 }
                 win0 *= kStep;
                 yab *= kStep;
@@ -639,7 +779,7 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 const int i = rowBase + k;
-                if (i > a.M) continue;
+                if (i > a.M()) continue;
                 if (MODE == kDiscover) {
                     x->rowMax[i] = f.rmax[k];
                     x->rowCnt[i] = f.cnt;
@@ -659,59 +799,81 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
     ++f.u;
 }
 
+// One forward step at position P6 of a six-step group: wait for this step's
+// W1 copy, read it from the staging ring, run the step, and stage the W1 of
+// the step kW1Ahead later into the slot this lane read one step ago.
+template <int R, int MODE, int P6>
+__device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
+                                              int total, W1Stage<R> &st, const ExactRows *x, ExactBest *exact) {
+    constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
+    float q[R];
+    if (kReadW1) {
+        cpAsyncWait<kW1Ahead - 1>();
+        const float4 v = win.w1[P6][lane];
+        q[0] = v.x;
+        if constexpr (R > 1) q[1] = v.y;
+        if constexpr (R > 2) {
+            q[2] = v.z;
+            q[3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < R; ++k) q[k] = 0.0f;
+    }
+    forwardStep<R, MODE, P6 % 3>(f, a, win, lane, total, q, x, exact);
+    if (kReadW1) st.issue(a, win, (P6 + kW1Ahead) % kW1Slots, lane, total);
+}
+
 // ---------------------------------------------------------------------------
 // Forward sweep (reads W1 written by the backward sweep of the same mode).
+// Steps run in groups of six, so that both the history phase (t mod 3) and
+// the W1 staging slot (t mod 6) are compile-time constants.
 // ---------------------------------------------------------------------------
 template <int R, int MODE>
 __device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &bestOut, float &maxOut,
                              const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
+    static_assert(kW1Slots == 6 && kBlock % 6 == 0, "six-step groups");
     FwdState<R, MODE> f;
 #pragma unroll
+    for (int h = 0; h < 3; ++h)
+#pragma unroll
+        for (int k = 0; k < R; ++k) f.w[h][k] = f.z[h][k] = 0.0f;
+#pragma unroll
     for (int k = 0; k < R; ++k) {
-        f.w1[k] = f.w2[k] = f.w3[k] = f.z1[k] = f.z2[k] = f.z3[k] = 0.0f;
-        if constexpr (MODE == kDiscover || MODE == kReplay) {
-            f.rmax[k] = 0.0f;
-            f.cIn[k] = f.cB[k] = 0;
-            f.fOut[k] = 1.0f;
-            f.rowBest[k] = 0.0;
-        }
+        f.rmax[k] = 0.0f;
+        f.cIn[k] = f.cB[k] = 0;
+        f.fOut[k] = 1.0f;
+        f.rowBest[k] = 0.0;
     }
     f.sendIn = f.sendY = f.best = f.mx = 0.0f;
     f.sendC = f.cnt = 0;
     f.u = -lane;  // lane 0 leads
     f.s = f.j = 0;
     const int total = a.nS * a.P;
-    const int T = total + (kLanes - 1);
+    const int T = (total + (kLanes - 1) + 5) / 6 * 6;  // whole groups of six steps
     constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
-    W1Ahead<R> ah{-lane, 0, 0};
-    float qa[R], qb[R];
-#pragma unroll
-    for (int k = 0; k < R; ++k) qa[k] = qb[k] = 0.0f;
+    W1Stage<R> st{-lane, 0, 0};
     if (kReadW1) {
-        ah.next(a, lane, total, qa);
-        ah.next(a, lane, total, qb);
+#pragma unroll
+        for (int k = 0; k < kW1Ahead; ++k) st.issue(a, win, k, lane, total);
     }
     __syncwarp();
-    fillForward(win, a, lane);
-    fillForward(win, a, lane + 32);
-    for (int t0 = 0; t0 < T; t0 += 32) {
+    fillBlock<false>(win, a, 0, lane);
+    for (int t0 = 0; t0 < T; t0 += kBlock) {
         __syncwarp();
-        if (t0 > 0) fillForward(win, a, t0 + 32 + lane);
-        // Blocks are 32 steps (even) except the last; its odd tail step is
-        // handled after the pairwise loop.
-        const int n = (t0 + 32 < T ? 32 : T - t0);
-        int k = 0;
-        for (; k + 1 < n; k += 2) {
-            forwardStep<R, MODE>(f, a, win, lane, total, qa, x, exact);
-            if (kReadW1) ah.next(a, lane, total, qa);
-            forwardStep<R, MODE>(f, a, win, lane, total, qb, x, exact);
-            if (kReadW1) ah.next(a, lane, total, qb);
-        }
-        if (k < n) {
-            forwardStep<R, MODE>(f, a, win, lane, total, qa, x, exact);
-            if (kReadW1) ah.next(a, lane, total, qa);
+        fillBlock<false>(win, a, t0 + kBlock, lane);
+        const int n = (t0 + kBlock < T ? kBlock : T - t0);
+#pragma unroll 1
+        for (int g = 0; g < n; g += 6) {
+            forwardStaged<R, MODE, 0>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 1>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 2>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 3>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 4>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 5>(f, a, win, lane, total, st, x, exact);
         }
     }
+    if (kReadW1) cpAsyncWait<0>();  // no copy outlives the sweep (the slot is reused)
     bestOut = f.best;
     maxOut = f.mx;
 }
@@ -744,18 +906,24 @@ template <int R, bool MID>
 __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad, const float *smBg, Window &win,
                           float *w1, float *ring, int lane) {
     const DevPair p = g.pairs[pi];
+    __syncwarp();
+    if (lane == 0) {
+        PairCold &c = win.cold;
+        c.codes = g.codes + p.codeOff;
+        c.pre = g.seeds + p.seedOff;
+        c.suf = c.pre + p.L;
+        c.params = g.params + g.profiles[p.prof].paramOff;
+        c.smBg = smBg;
+        c.sc = g.scales[pi];
+        c.M = p.M;
+    }
+    __syncwarp();
     SweepArgs a;
-    a.codes = g.codes + p.codeOff;
-    a.pre = g.seeds + p.seedOff;
-    a.suf = a.pre + p.L;
-    a.params = g.params + g.profiles[p.prof].paramOff;
+    a.cold = &win.cold;
     a.smE = smE;
-    a.smBg = smBg;
     a.w1 = w1;
     a.ring = ring;
-    a.sc = g.scales[pi];
     a.L = p.L;
-    a.M = p.M;
     a.rowPad = rowPad;
     a.nS = (p.M + 1 + kLanes * R - 1) / (kLanes * R);
     a.P = wavePeriod(p.L);
