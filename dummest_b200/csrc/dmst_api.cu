@@ -207,6 +207,7 @@ struct dmst_ctx {
     DevBuf<ExactOut> dExactOut;
 
     double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0, lastHostMs = 0;
+    double lastPostMs = 0, lastWallMs = 0;
     int lastExactPairs = 0;
     int lastLaunches = 0;
 
@@ -640,6 +641,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
     const bool mid = base == DMST_MODE_MID;
     ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = ctx->lastExactMs = ctx->lastHostMs = 0;
+    ctx->lastPostMs = ctx->lastWallMs = 0;
     ctx->lastLaunches = 0;
     ctx->lastExactPairs = 0;
     const auto hostT0 = std::chrono::steady_clock::now();
@@ -658,14 +660,30 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             return ctx->fail(DMST_EINVAL, "pair %zu: unknown sequence or profile id", i);
     }
     {
-        // Profile-major, longest read first: one key sort (the index breaks ties).
-        std::vector<std::pair<uint64_t, int>> keys(n);
-        for (size_t i = 0; i < n; ++i) {
-            const uint32_t inv = 0xFFFFFFFFu - (uint32_t)ctx->seqLen[pairs[i].seq];
-            keys[i] = {((uint64_t)(uint32_t)pairs[i].profile << 32) | inv, (int)i};
+        // Profile-major, longest read first, input order breaking ties.  Two
+        // stable counting sorts (by length, descending, then by profile) when
+        // the length range is small against n; one key sort otherwise.
+        int maxLen = 0;
+        for (size_t i = 0; i < n; ++i) maxLen = std::max(maxLen, ctx->seqLen[pairs[i].seq]);
+        const size_t nProf = ctx->profiles.size();
+        if ((size_t)maxLen <= 4 * n + 65536) {
+            std::vector<int> cnt((size_t)maxLen + 2, 0), byLen(n);
+            for (size_t i = 0; i < n; ++i) ++cnt[(size_t)(maxLen - ctx->seqLen[pairs[i].seq]) + 1];
+            for (size_t v = 1; v < cnt.size(); ++v) cnt[v] += cnt[v - 1];
+            for (size_t i = 0; i < n; ++i) byLen[cnt[(size_t)(maxLen - ctx->seqLen[pairs[i].seq])]++] = (int)i;
+            std::vector<int> start(nProf + 1, 0);
+            for (size_t i = 0; i < n; ++i) ++start[(size_t)pairs[i].profile + 1];
+            for (size_t q = 0; q < nProf; ++q) start[q + 1] += start[q];
+            for (size_t k = 0; k < n; ++k) order[start[pairs[byLen[k]].profile]++] = byLen[k];
+        } else {
+            std::vector<std::pair<uint64_t, int>> keys(n);
+            for (size_t i = 0; i < n; ++i) {
+                const uint32_t inv = 0xFFFFFFFFu - (uint32_t)ctx->seqLen[pairs[i].seq];
+                keys[i] = {((uint64_t)(uint32_t)pairs[i].profile << 32) | inv, (int)i};
+            }
+            std::sort(keys.begin(), keys.end());
+            for (size_t i = 0; i < n; ++i) order[i] = keys[i].second;
         }
-        std::sort(keys.begin(), keys.end());
-        for (size_t i = 0; i < n; ++i) order[i] = keys[i].second;
     }
     std::vector<DevPair> dp(n);
     long long seedFloats = 0;
@@ -952,6 +970,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     ctx->lastTotalMs = nullMs + dpMs + exactMs;
     ctx->lastLaunches = launches;
 
+    const auto postT0 = std::chrono::steady_clock::now();
     std::vector<int> flagAt(n, -1);
     for (size_t f = 0; f < flagged.size(); ++f) flagAt[flagged[f]] = (int)f;
     for (size_t k = 0; k < n; ++k) {
@@ -974,14 +993,18 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             r.mid_ln = -INFINITY;
         }
     }
+    const auto endT = std::chrono::steady_clock::now();
+    ctx->lastPostMs = std::chrono::duration<double, std::milli>(endT - postT0).count();
+    ctx->lastWallMs = std::chrono::duration<double, std::milli>(endT - hostT0).count();
     return DMST_OK;
 }
 
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n) {
     if (!ctx || !out || n < 0) return DMST_EINVAL;
-    const double v[7] = {ctx->lastTotalMs, ctx->lastNullMs, ctx->lastDpMs, ctx->lastExactMs,
-                         ctx->lastHostMs,  (double)ctx->lastLaunches, (double)ctx->lastExactPairs};
-    for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
+    const double v[9] = {ctx->lastTotalMs, ctx->lastNullMs,      ctx->lastDpMs,
+                         ctx->lastExactMs, ctx->lastHostMs,      (double)ctx->lastLaunches,
+                         (double)ctx->lastExactPairs, ctx->lastPostMs, ctx->lastWallMs};
+    for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
     return DMST_OK;
 }
 

@@ -57,8 +57,11 @@ __device__ __forceinline__ XS batchAdd(XS a, XS b) {
     const int eh = agebe ? a.e : b.e, el = agebe ? b.e : a.e;
     int d = eh - el;
     d = d > 60 ? 60 : d;
-    // ml * 2^-d is exact, so an fma here rounds exactly like mul-then-add.
-    double s = __dadd_rn((double)mh, __dmul_rn((double)ml, 1.0 / (double)(1ULL << (unsigned)d)));
+    // 1 / 2^d is the exact power 2^-d (0 <= d <= 60), built from its exponent
+    // bits instead of a double division; ml * 2^-d is exact, so the sum
+    // rounds once, as the reference's does.
+    const double inv = __longlong_as_double((long long)(1023 - d) << 52);
+    double s = __dadd_rn((double)mh, __dmul_rn((double)ml, inv));
     int e = eh;
     if (s >= 1.0) {
         s *= 0.5;

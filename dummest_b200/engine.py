@@ -214,10 +214,10 @@ class Context:
         return res
 
     def last_timing(self) -> dict:
-        v = (C.c_double * 7)()
-        self.lib.dmst_last_timing_ex(self.h, v, 7)
+        v = (C.c_double * 9)()
+        self.lib.dmst_last_timing_ex(self.h, v, 9)
         return {"total_ms": v[0], "null_ms": v[1], "dp_ms": v[2], "exact_ms": v[3], "host_ms": v[4],
-                "launches": int(v[5]), "exact_pairs": int(v[6])}
+                "launches": int(v[5]), "exact_pairs": int(v[6]), "post_ms": v[7], "wall_ms": v[8]}
 
     def find_similarities(self, profile: int, decoded: Sequence[np.ndarray]) -> list[Similarity]:
         if len(decoded) == 0:

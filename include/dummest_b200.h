@@ -184,8 +184,9 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
 int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, double *null_ms, int *launches);
 /* The same breakdown as an array: out[0] device ms of the call, [1] null-model
  * kernel ms, [2] DP kernel ms, [3] exact-path ms, [4] host preparation ms
- * (wall clock), [5] kernel launches, [6] pairs on the exact path.  n = number
- * of entries wanted (<= 7). */
+ * (wall clock), [5] kernel launches, [6] pairs on the exact path, [7] host ms
+ * after the device work (result assembly), [8] wall ms of the whole call.
+ * n = number of entries wanted (<= 9). */
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
 
 /* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
