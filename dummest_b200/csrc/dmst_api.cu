@@ -808,7 +808,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         while (e < n && e - k < 32 && dp[jobPairs[e]].codeOff == dp[jobPairs[k]].codeOff) ++e;
         nullJobs.push_back(NullJob{(int)k, (int)(e - k)});
         nullTmpOff.push_back(nullTmpEntries);
-        nullTmpEntries += 32LL * (dp[jobPairs[k]].L + 1);
+        nullTmpEntries += dmst::nullTmpEntries(dp[jobPairs[k]].L);
         k = e;
     }
     CK(ctx->dNullJobs.ensure(nullJobs.size()), "alloc null jobs");
@@ -1035,7 +1035,7 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
     const NullJob job{0, 1};
     CK(ctx->dPairs.ensure(1), "alloc");
     CK(ctx->dSeeds.ensure(2 * (size_t)d.L), "alloc");
-    CK(ctx->dNullTmp.ensure(32 * ((size_t)d.L + 1)), "alloc");
+    CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries(d.L)), "alloc");
     CK(ctx->dNullTmpOff.ensure(1), "alloc");
     CK(ctx->dNullJobs.ensure(1), "alloc");
     CK(ctx->dNullJobPairs.ensure(1), "alloc");
@@ -1155,13 +1155,14 @@ int dmst_calibrate(dmst_ctx *ctx, int profile, int sequence_length, int border, 
 namespace {
 
 // Layout of the static scratch: a 2 KiB header (the kernel's profile, pair,
-// job and offset records), then the interleaved suffix temporary of
-// 32 x (L+1) ExpScores.  The header is 2 KiB although its records take 192
+// job and offset records), then the interleaved prefix and suffix
+// temporaries, 2 x 32 x (L+1) ExpScores.  The header is 2 KiB although its records take 192
 // bytes so that a background lookup with any 8-bit code (bg[0..255] starts
 // 24 bytes into the profile record) stays inside the array.
 constexpr size_t kNaHeaderBytes = 2048;
-constexpr size_t kNaTmpEntries = 32 * ((size_t)DMST_NOALLOC_MAX_LEN + 1);
-constexpr size_t kNaScratchBytes = kNaHeaderBytes + kNaTmpEntries * sizeof(XS);  // 4,196,608 bytes
+constexpr size_t kNaTmpEntries = (size_t)nullTmpEntries(DMST_NOALLOC_MAX_LEN);
+constexpr size_t kNaScratchBytes = kNaHeaderBytes + kNaTmpEntries * sizeof(XS);  // 8,391,168 bytes
+static_assert(kNaScratchBytes == 8391168, "documented scratch size");
 
 static __device__ __align__(256) unsigned char gNullScratch[kNaScratchBytes];
 

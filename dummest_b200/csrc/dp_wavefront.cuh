@@ -218,7 +218,7 @@ constexpr int kW1Slots = 6;
 constexpr int kW1Ahead = kW1Slots - 1;
 
 struct Window {
-    float4 col[kWin];   // backward: {code, bg, suf, pre}; forward: {code, bg*sC, pre, unused}
+    float4 col[kWin];   // backward: {code*rowPad, bg, suf, pre}; forward: {code*rowPad, bg*sC, pre, unused}
     float4 ring[kWin];  // stripe-boundary (W, Y, scale count) for the lane that reads the ring
     float4 w1[kW1Slots][kLanes];  // forward W1 staging ring (lane l uses [slot][l], R floats)
     PairCold cold;      // the pair in flight: fields read only at refills and stripe starts
@@ -235,17 +235,24 @@ __device__ __forceinline__ void ringStore(float *ring, int col, float w, float y
     __stcg(reinterpret_cast<float2 *>(ring) + 2 * col, make_float2(w, y));
 }
 
+// max(a, b, c) in one instruction (the three-input max.f32 of sm_100).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Backward window entry for local time u (the column of u is L-1 - u mod P).
 __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
-    float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
+    float4 c = make_float4(__int_as_float(kPad * a.rowPad), 0.0f, 0.0f, 0.0f);
     float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (u >= 0 && u < a.nS * a.P) {
         const int sp = u / a.P, jj = u - sp * a.P;
         if (jj < a.L) {
             const int j = a.L - 1 - jj;
             const int code = (j + 1 < a.L) ? (int)__ldg(a.codes() + j + 1) : kPad;
-            c = make_float4(__int_as_float(code), a.smBg()[code], __ldg(a.suf() + j), __ldg(a.pre() + j));
+            c = make_float4(__int_as_float(code * a.rowPad), a.smBg()[code], __ldg(a.suf() + j), __ldg(a.pre() + j));
             if (sp > 0) r = ringLoad(a.ring, jj);
         }
     }
@@ -256,13 +263,13 @@ __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int 
 // Forward window entry for local time u (the column of u is u mod P).
 __device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
-    float4 c = make_float4(__int_as_float(kPad), 0.0f, 0.0f, 0.0f);
+    float4 c = make_float4(__int_as_float(kPad * a.rowPad), 0.0f, 0.0f, 0.0f);
     float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (u >= 0 && u < a.nS * a.P) {
         const int s = u / a.P, j = u - s * a.P;
         if (j < a.L) {
             const int code = (j >= 2) ? (int)__ldg(a.codes() + j - 2) : kPad;
-            c = make_float4(__int_as_float(code), a.smBg()[code] * a.sc().sC, __ldg(a.pre() + j), 0.0f);
+            c = make_float4(__int_as_float(code * a.rowPad), a.smBg()[code] * a.sc().sC, __ldg(a.pre() + j), 0.0f);
             if (s > 0) r = ringLoad(a.ring, j);
         }
     }
@@ -420,10 +427,10 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
                 inY *= f;
             }
         }
-        const int code = __float_as_int(col.x);
+        const int eOff = __float_as_int(col.x);  // code * rowPad
         const float bgv = col.y, sufv = col.z, prev = col.w;
         float e[R];
-        loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
+        loadEmit<R>(e, a.smE + eOff + rowBase);
         // First products (W1[i+1][j+3] * e) * enter, taken before any row of
         // this step overwrites its column-j+3 slot.
         float p[R];
@@ -434,7 +441,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             p[k] = (h3 * e[k]) * b.c.enter[k];
         }
         float bW1 = b.rb[I1], bW2 = b.rb[I2], bY = inY;
-        float wv[R];
+        float wv[R], yv[R], fv[R];
         float stepMax = 0.0f;
 #pragma unroll
         for (int k = R - 1; k >= 0; --k) {
@@ -454,8 +461,8 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             const float Y = __fmaf_rn(b.c.eps[k], bY, W);
             const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
             if (MODE == kFilter || MODE == kMid) {
-                b.maxY = fmaxf(b.maxY, Y);
-                b.filt = fmaxf(b.filt, W * prev);
+                yv[k] = Y;
+                fv[k] = W * prev;
             }
             if (MODE == kDiscover) {
                 b.rmax[k] = fmaxf(b.rmax[k], Y);  // Y >= W1 at every cell
@@ -477,6 +484,19 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             }
             b.h[I3][k] = W;
             b.z[I3][k] = Z;
+        }
+        if (MODE == kFilter || MODE == kMid) {
+            // running maxima, two rows per three-input max
+#pragma unroll
+            for (int k = 0; k < R; k += 2) {
+                if (k + 1 < R) {
+                    b.maxY = fmax3(b.maxY, yv[k], yv[k + 1]);
+                    b.filt = fmax3(b.filt, fv[k], fv[k + 1]);
+                } else {
+                    b.maxY = fmaxf(b.maxY, yv[k]);
+                    b.filt = fmaxf(b.filt, fv[k]);
+                }
+            }
         }
         b.rb[I3] = inW;
         b.sendW = wv[0];
@@ -710,12 +730,13 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
                 inY *= g;
             }
         }
-        const int code = __float_as_int(col.x);
+        const int eOff = __float_as_int(col.x);  // code * rowPad
         const float bgsC = col.y, prev = col.z;
         float e[R];
-        loadEmit<R>(e, a.smE + code * a.rowPad + rowBase);
+        loadEmit<R>(e, a.smE + eOff + rowBase);
         float win0 = inW, yab = inY;
         float stepMax = 0.0f;
+        float bv[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const float w1 = f.w[I1][k], w2 = f.w[I2][k], w3 = f.w[I3][k];
@@ -730,10 +751,10 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             // seed: padding rows (past M, zero coefficients) then hold only
             // their seed, which reaches no real row and multiplies a zero W1.
             const float W0 = (MODE == kMid) ? win0 + __fadd_rn(zs, prev) : win0 + __fmaf_rn(prev, f.c.rs[k], zs);
-            if (MODE == kMid) f.best = fmaxf(f.best, W0 * q[k]);
+            if (MODE == kMid) bv[k] = W0 * q[k];
             if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
             const float Y0 = __fmaf_rn(f.c.eps[k], yab, f.c.d0[k] * W0);
-            if (MODE == kMid) f.mx = fmaxf(f.mx, fmaxf(W0, Y0));
+            if (MODE == kMid) f.mx = fmax3(f.mx, W0, Y0);
             const float nin = __fmaf_rn(f.c.d2[k], w1, __fmaf_rn(f.c.d1[k], w2, X + Y0));
             if (MODE == kDiscover) {
                 f.rmax[k] = fmaxf(f.rmax[k], fmaxf(W0, Y0));
@@ -748,6 +769,10 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
                 win0 = nin;
                 yab = Y0;
             }
+        }
+        if (MODE == kMid) {
+#pragma unroll
+            for (int k = 0; k < R; k += 2) f.best = (k + 1 < R) ? fmax3(f.best, bv[k], bv[k + 1]) : fmaxf(f.best, bv[k]);
         }
         if (MODE == kDiscover) {
             if (stepMax > kBump) {

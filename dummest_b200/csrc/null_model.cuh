@@ -145,6 +145,10 @@ __device__ __forceinline__ XS prefixStep(int i, const float *bg, const uint8_t *
 // suffix probabilities interleaved (one coalesced 256-byte store per column),
 // and write their seed vectors through a shared-memory transpose, so that each
 // store instruction writes 32 consecutive seeds of one pair.
+// Temporary ExpScores of one null-model job: the prefix [L][32] and the
+// suffix [L+1][32] probabilities of its (up to) 32 pairs, interleaved.
+__host__ __device__ constexpr long long nullTmpEntries(long long L) { return 2 * 32 * (L + 1); }
+
 struct NullJob {
     int first;  // index of the job's first pair in the pair-index array
     int count;  // pairs in the job (<= 32), all with the same read
@@ -185,16 +189,33 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
         float *pre = seeds + p.seedOff;
         dstAll[warp][0][lane] = on ? pre : nullptr;
         dstAll[warp][1][lane] = on ? pre + L : nullptr;
-        XS *sfx = tmp + tmpOff[ji];  // [(L+1) x 32] interleaved suffix probabilities
+        XS *pfx = tmp + tmpOff[ji];           // [L x 32] interleaved prefix probabilities
+        XS *sfx = pfx + 32 * ((size_t)L + 1);  // [(L+1) x 32] interleaved suffix probabilities
 
-        // Pass 1: prefix probabilities (dummest-dp-backward.hh:58-100); the
-        // last three give the total.
+        // Pass 1: the prefix recurrence (dummest-dp-backward.hh:58-100, i = 0..L-1)
+        // and the suffix recurrence (:6-55, i = L-1..0, from suffix[L] = 1 and
+        // suffix[L+1..L+3] = 0), two independent chains run side by side; both
+        // sequences are kept for the seed passes.
         XS p1 = xsZero(), p2 = xsZero(), p3 = xsZero();
-        for (int i = 0; i < L; ++i) {
-            const XS q = prefixStep(i, bg, cd, L, p1, p2, p3, keep, sNE, dNE);
+        const XS trailing = splitNorm(0.5 * keep, 0);
+        XS s1 = pow2Score(0), s2 = xsZero(), s3 = xsZero();  // suffix[i+1], [i+2], [i+3]
+        for (int k = 0; k < L; ++k) {
+            const XS q = prefixStep(k, bg, cd, L, p1, p2, p3, keep, sNE, dNE);
+            pfx[(size_t)k * 32 + lane] = q;
             p3 = p2;
             p2 = p1;
             p1 = q;
+            const int i = L - 1 - k;
+            const double codonScale = __dmul_rn((double)bgAt(bg, cd, L, i), keep);
+            const XS single = scaleScore(s1, sNE);
+            const XS dIn = (i + 1 < L) ? s2 : pow2Score(2);
+            const XS dbl = scaleScore(dIn, dNE);
+            const XS codon = (i + 2 < L) ? scaleScore(s3, codonScale) : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
+            const XS v = batchAdd(codon, batchAdd(single, dbl));
+            sfx[(size_t)i * 32 + lane] = v;
+            s3 = s2;
+            s2 = s1;
+            s1 = v;
         }
         // Total and scales (dummest-dp-backward.hh:103-129).
         const double keepSingle = 1.0 - r.single;
@@ -218,28 +239,23 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
             scales[pi] = sc;
         }
 
-        // Pass 2: suffix probabilities (dummest-dp-backward.hh:6-55), i = L-1..0,
-        // from suffix[L] = 1 and suffix[L+1..L+3] = 0.
-        {
-            const XS trailing = splitNorm(0.5 * keep, 0);
-            XS s1 = pow2Score(0), s2 = xsZero(), s3 = xsZero();  // suffix[i+1], [i+2], [i+3]
-            for (int i = L - 1; i >= 0; --i) {
-                const double codonScale = __dmul_rn((double)bgAt(bg, cd, L, i), keep);
-                const XS single = scaleScore(s1, sNE);
-                const XS dIn = (i + 1 < L) ? s2 : pow2Score(2);
-                const XS dbl = scaleScore(dIn, dNE);
-                const XS codon = (i + 2 < L) ? scaleScore(s3, codonScale) : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
-                const XS v = batchAdd(codon, batchAdd(single, dbl));
-                sfx[(size_t)i * 32 + lane] = v;
-                s3 = s2;
-                s2 = s1;
-                s1 = v;
+        // Pass 2: prefix seeds (dummest-dp-backward.hh:155-164) from the kept
+        // prefix, beside the L-1 multiplications that start the suffix seeds'
+        // running scale (:137-145).
+        XS running = pow2Score(0);
+        XS runPre = perBase;
+        for (int j0 = 0; j0 < L; j0 += 32) {
+            const int ncol = L - j0 < 32 ? L - j0 : 32;
+            for (int c = 0; c < ncol; ++c) {
+                const int j = j0 + c;
+                stage[c][lane] = packScore(batchMul(pfx[(size_t)j * 32 + lane], runPre));
+                runPre = batchMul(runPre, perBase);
+                if (j < L - 1) running = batchMul(running, perBase);
             }
+            flushSeeds(stage, dstAll[warp][0], job.count, j0, ncol, lane);
         }
 
-        // Pass 3: suffix seeds (dummest-dp-backward.hh:137-154).
-        XS running = pow2Score(0);
-        for (int t = 0; t < L - 1; ++t) running = batchMul(running, perBase);
+        // Pass 3: suffix seeds (dummest-dp-backward.hh:146-154).
         for (int j0 = 0; j0 < L; j0 += 32) {
             const int ncol = L - j0 < 32 ? L - j0 : 32;
             for (int c = 0; c < ncol; ++c) {
@@ -249,24 +265,6 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
                 running = batchMul(running, perBaseInv);
             }
             flushSeeds(stage, dstAll[warp][1], job.count, j0, ncol, lane);
-        }
-
-        // Pass 4: prefix seeds (dummest-dp-backward.hh:155-164), recomputing
-        // the prefix recurrence.
-        running = perBase;
-        p1 = p2 = p3 = xsZero();
-        for (int j0 = 0; j0 < L; j0 += 32) {
-            const int ncol = L - j0 < 32 ? L - j0 : 32;
-            for (int c = 0; c < ncol; ++c) {
-                const int i = j0 + c;
-                const XS q = prefixStep(i, bg, cd, L, p1, p2, p3, keep, sNE, dNE);
-                p3 = p2;
-                p2 = p1;
-                p1 = q;
-                stage[c][lane] = packScore(batchMul(q, running));
-                running = batchMul(running, perBase);
-            }
-            flushSeeds(stage, dstAll[warp][0], job.count, j0, ncol, lane);
         }
         __syncwarp();
     }

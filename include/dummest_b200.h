@@ -206,7 +206,7 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
  * It computes exactly what dmst_null_model computes (the same kernel), with
  * no context and no allocation of any kind: inputs and outputs are the
  * caller's DEVICE buffers, and the kernel's scratch is a fixed file-scope
- * device array of 4,196,608 bytes (a 2 KiB header plus 32 x (L+1) 8-byte
+ * device array of 8,391,168 bytes (a 2 KiB header plus 2 x 32 x (L+1) 8-byte
  * scores for L <= DMST_NOALLOC_MAX_LEN).
  *
  *   codes    device pointer, `length` codon codes 0..24 (dmst_decode_letters);
