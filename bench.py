@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true", help="skip the kernel-shape autotuner")
+    ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
     return ap.parse_args()
 
 
@@ -327,8 +329,21 @@ def run_ours(args, rank, world, local):
         step_pairs.append(pairs_for(sids))
         step_cells.append(float(sum(len(r) for r in recs)) * float((Ms + 1).sum()))
     stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    # Kernel shapes from the autotuner (untimed): every shape on the first
+    # (warm-up) step's pairs, a sample large enough to fill the GPU.
+    tuning = None
+    if not args.no_autotune and args.rows_per_lane == 0:
+        samp = step_sids[0]
+        rates = ctx.autotune([s for _ in pids for s in samp], [p for p in pids for _ in samp])
+        shapes = {}
+        for M in Ms:
+            key = "R%d/W%d" % ctx.tuned_shape(int(M))
+            shapes[key] = shapes.get(key, 0) + 1
+        tuning = {"gcups_computed_cells": {f"R{r}/W{w}": round(v, 2) for (r, w), v in rates.items()},
+                  "profiles_per_shape": shapes}
+    MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
     for w in range(args.warmup):
-        ctx.score_pairs_raw(step_pairs[w], d.MODE_MID)
+        ctx.score_pairs_raw(step_pairs[w], MODE)
     barrier(world)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -339,7 +354,7 @@ def run_ours(args, rank, world, local):
     results = []
     parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0}
     for k in range(args.warmup, n_steps):
-        results.append(ctx.score_pairs_raw(step_pairs[k], d.MODE_MID))
+        results.append(ctx.score_pairs_raw(step_pairs[k], MODE))
         t = ctx.last_timing()
         launches += t["launches"]
         dp_ms += t["dp_ms"]
@@ -380,7 +395,7 @@ def run_ours(args, rank, world, local):
         ctx.clear_sequences()
         words, mask, lens = packed[w]
         sids = ctx.add_packed(words, lens, mask)
-        ctx.score_pairs_raw(pairs_for(sids), d.MODE_MID)
+        ctx.score_pairs_raw(pairs_for(sids), MODE)
     # After a clear, sequence ids restart at 0, so every step's pair list is
     # the same array (built once, outside the timed region).
     e2e_pairs = pairs_for(list(range(len(steps[0]))))
@@ -393,7 +408,7 @@ def run_ours(args, rank, world, local):
         sids = ctx.add_packed(words, lens, mask)
         assert sids[0] == 0 and len(sids) == len(lens)
         pr = e2e_pairs
-        res = ctx.score_pairs_raw(pr, d.MODE_MID)
+        res = ctx.score_pairs_raw(pr, MODE)
         # packed reads + mask + offsets, then the per-pair descriptors the
         # library uploads (32 B pair + 8 B scratch offset) and the 16-byte
         # per-pair results it reads back
@@ -437,6 +452,7 @@ def run_ours(args, rank, world, local):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
             "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
+            "launch": {"cuda_graph": not args.no_graph, "autotune": tuning},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

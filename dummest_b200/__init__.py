@@ -6,7 +6,15 @@ Gumbel calibration, as hand-written sm_100a CUDA behind the C ABI in
 include/dummest_b200.h.  This package is the host-side mirror of the
 reference interface over that ABI (see engine.py).
 """
-from ._ffi import MODE_EXACT_SEQUENTIAL, MODE_FILTER, MODE_FORCE_EXACT, MODE_MID, MODE_PLAIN, load  # noqa: F401
+from ._ffi import (  # noqa: F401
+    MODE_EXACT_SEQUENTIAL,
+    MODE_FILTER,
+    MODE_FORCE_EXACT,
+    MODE_GRAPH,
+    MODE_MID,
+    MODE_PLAIN,
+    load,
+)
 from .engine import (  # noqa: F401
     Context,
     DmstError,

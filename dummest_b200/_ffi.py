@@ -25,6 +25,7 @@ MODE_FILTER = 1
 MODE_PLAIN = 0x100
 MODE_FORCE_EXACT = 0x200
 MODE_EXACT_SEQUENTIAL = 0x400
+MODE_GRAPH = 0x800
 NOALLOC_MAX_LEN = 16384  # DMST_NOALLOC_MAX_LEN
 RES_EXACT_PATH = 1
 
@@ -107,6 +108,8 @@ SIGNATURES = [
     ("dmst_last_timing_ex", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("dmst_null_model", C.c_int,
      [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("dmst_autotune", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double)]),
+    ("dmst_tuned_shape", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("dmst_null_model_noalloc", C.c_int,
      [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(Opts), C.c_void_p, C.c_void_p, C.c_void_p]),
     ("dmst_estimate_gumbel", C.c_int, [C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double)]),

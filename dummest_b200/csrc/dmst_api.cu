@@ -153,14 +153,56 @@ const char *statusText(int s) {
     }
 }
 
-int rowsPerLane(int M, int forced) {
+// Kernel shapes the autotuner chooses among: rows per lane (the stripe is
+// 32 R rows) and warps per CTA.
+constexpr int kShapeR[3] = {4, 2, 1};
+constexpr int kShapeWarps[2] = {kCtaWarps, kCtaWarpsNarrow};
+inline int rIndex(int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); }
+
+using DpKern = void (*)(DpArgs, int);
+template <bool MID, int W>
+DpKern kernByR(int R) {
+    return R == 4 ? dpKernel<4, MID, W> : (R == 2 ? dpKernel<2, MID, W> : dpKernel<1, MID, W>);
+}
+DpKern dpKernelFor(int R, bool mid, int warps) {
+    if (warps == kCtaWarpsNarrow) return mid ? kernByR<true, kCtaWarpsNarrow>(R) : kernByR<false, kCtaWarpsNarrow>(R);
+    return mid ? kernByR<true, kCtaWarps>(R) : kernByR<false, kCtaWarps>(R);
+}
+
+// Rows of a profile as the kernel with R rows per lane computes them.
+inline long long paddedRows(int M, int R) {
+    const long long S = (long long)kLanes * R;
+    return (M + 1 + S - 1) / S * S;
+}
+
+// What the autotuner measured: per rows-per-lane value, the faster CTA shape
+// and its rate in computed (padded) cells per millisecond.
+struct Tuning {
+    bool tuned = false;
+    int warps[3] = {kCtaWarps, kCtaWarps, kCtaWarps};
+    double rate[3] = {0, 0, 0};
+    int forceR = 0, forceWarps = 0;  // set while the autotuner measures one shape
+};
+
+int rowsPerLane(int M, int forced, const Tuning &t) {
     if (forced == 1 || forced == 2 || forced == 4) return forced;
-    (void)M;
-    // Measured on B200 (synthetic profiles, M 50-800): the per-step cost of a
-    // lane (shuffles, staging reads, W1 traffic) dominates, so four rows per
-    // lane is fastest per real cell even for the shortest profiles, where
-    // most of the 128-row stripe is padding.
-    return 4;
+    if (t.forceR) return t.forceR;
+    // Untuned default, measured on B200 (synthetic profiles, M 50-800): the
+    // per-step cost of a lane dominates, so four rows per lane is fastest per
+    // real cell even where most of the 128-row stripe is padding.
+    if (!t.tuned) return 4;
+    // Tuned: the shape with the least expected time for this profile length.
+    int best = 4;
+    double bestT = 1e300;
+    for (int q = 0; q < 3; ++q) {
+        if (!(t.rate[q] > 0)) continue;
+        const double time = (double)paddedRows(M, kShapeR[q]) / t.rate[q];
+        if (time < bestT) {
+            bestT = time;
+            best = kShapeR[q];
+        }
+    }
+    return best;
 }
 
 }  // namespace
@@ -168,6 +210,11 @@ int rowsPerLane(int M, int forced) {
 struct dmst_ctx {
     dmst_opts opts;
     Rates rates;
+    Tuning tune;
+    cudaGraphExec_t graphExec = nullptr;  // DMST_MODE_GRAPH: the instantiated launch graph
+    std::vector<uintptr_t> graphKey;      // the launch shape and buffers it was captured with
+    int graphLaunches = 0;                // kernel launches in it
+    int graphCaptures = 0;                // captures so far (replays reuse the last)
     int device = 0;
     int smCount = 0;
     int maxSmemOptin = 0;
@@ -306,6 +353,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
     ctx->dEmit.release();
     ctx->dParams.release();
     ctx->dProfiles.release();
@@ -632,6 +680,20 @@ static void scoreToResult(XS s, dmst_score *dst, double *ln) {
     *ln = (s.m == 0.0f) ? -INFINITY : scoreLn(s.m, s.e);
 }
 
+// Milliseconds between two recorded events; a timing failure is noted in the
+// context's error text and cleared (it must not surface as the error of a
+// later launch check), and reads as -1.
+static float elapsedMs(dmst_ctx *ctx, cudaEvent_t a, cudaEvent_t b) {
+    float ms = -1.0f;
+    const cudaError_t e = cudaEventElapsedTime(&ms, a, b);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = std::string("event timing: ") + cudaGetErrorString(e);
+        return -1.0f;
+    }
+    return ms;
+}
+
 int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
     if (!ctx || (n && (!pairs || !out))) return DMST_EINVAL;
     const int base = mode & 0xff;
@@ -685,6 +747,29 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             for (size_t i = 0; i < n; ++i) order[i] = keys[i].second;
         }
     }
+    // Rows per lane per profile.  With tuned shapes, a rows-per-lane group too
+    // small to give every CTA two chunks would run as its own underfilled
+    // launch; its profiles join the largest group instead.
+    std::vector<int> profR(ctx->profiles.size(), 0);
+    {
+        long long groupPairs[3] = {0, 0, 0};
+        for (size_t i = 0; i < n; ++i) {
+            int &r = profR[pairs[i].profile];
+            if (!r) r = rowsPerLane(ctx->profiles[pairs[i].profile].M, ctx->opts.rows_per_lane, ctx->tune);
+            ++groupPairs[rIndex(r)];
+        }
+        if (ctx->tune.tuned && !ctx->tune.forceR && ctx->opts.rows_per_lane == 0 && !plain) {
+            int big = 0;
+            for (int q = 1; q < 3; ++q)
+                if (groupPairs[q] > groupPairs[big]) big = q;
+            for (int q = 0; q < 3; ++q) {
+                const long long fill = 2LL * ctx->smCount * 4 * ctx->tune.warps[q];
+                if (q != big && groupPairs[q] > 0 && groupPairs[q] < fill)
+                    for (int &r : profR)
+                        if (r == kShapeR[q]) r = kShapeR[big];
+            }
+        }
+    }
     std::vector<DevPair> dp(n);
     long long seedFloats = 0;
     size_t w1Max = 0, ringMax = 0;
@@ -695,7 +780,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         d.L = ctx->seqLen[q.seq];
         d.M = ctx->profiles[q.profile].M;
         d.prof = q.profile;
-        d.R = rowsPerLane(d.M, ctx->opts.rows_per_lane);
+        d.R = profR[q.profile];
         d.seedOff = seedFloats;
         seedFloats += 2LL * d.L;
         const int S = kLanes * d.R;
@@ -708,8 +793,9 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     // Kernel groups by rows per lane (fixed per profile).  Chunks: runs of up to
     // 2 x warps pairs of one profile, costliest first within each group.
     struct Group {
-        int R, warps;
-        void (*kern)(DpArgs, int);
+        int R, warps;     // warps launched per CTA (<= kernWarps when shared memory is short)
+        int kernWarps;    // the kernel's CTA shape (warp slots per CTA)
+        DpKern kern;
         std::vector<Chunk> chunks;
         std::vector<double> cost;
         int maxRowPad = 0;
@@ -717,17 +803,20 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         int grid = 0;
         size_t chunkBase = 0;
     };
-    Group groups[3] = {
-        {4, kCtaWarps, mid ? dpKernel<4, true> : dpKernel<4, false>},
-        {2, kCtaWarps, mid ? dpKernel<2, true> : dpKernel<2, false>},
-        {1, kCtaWarps, mid ? dpKernel<1, true> : dpKernel<1, false>},
-    };
-    auto groupOf = [](int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); };
+    Group groups[3];
+    for (int q = 0; q < 3; ++q) {
+        const int W = ctx->tune.forceWarps ? ctx->tune.forceWarps : ctx->tune.warps[q];
+        groups[q].R = kShapeR[q];
+        groups[q].kernWarps = W;
+        groups[q].warps = W;
+        groups[q].kern = dpKernelFor(kShapeR[q], mid, W);
+    }
+    auto groupOf = [](int R) { return rIndex(R); };
     for (size_t k = 0; k < n;) {
         Group &G = groups[groupOf(dp[k].R)];
         size_t e = k;
         double cost = 0;
-        const int chunkPairs = plain ? 1 : 4 * kCtaWarps;
+        const int chunkPairs = plain ? 1 : 4 * G.kernWarps;
         while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
             cost += (double)(dp[e].M + 1) * dp[e].L;
             ++e;
@@ -759,7 +848,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         if (table + sizeof(Window) > limit)
             return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
                              (int)((limit - sizeof(Window)) / (kNumCodes * 4)) - 1);
-        G.warps = (int)std::min<size_t>(kCtaWarps, (limit - table) / sizeof(Window));
+        G.warps = (int)std::min<size_t>(G.kernWarps, (limit - table) / sizeof(Window));
         G.smem = table + (size_t)G.warps * sizeof(Window);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
@@ -767,7 +856,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
         if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
         G.grid = plain ? 1 : (int)std::min<long long>((long long)perSm * ctx->smCount, (long long)G.chunks.size());
-        slotsMax = std::max(slotsMax, (size_t)G.grid * kCtaWarps);
+        slotsMax = std::max(slotsMax, (size_t)G.grid * G.kernWarps);
     }
 
     CK(ctx->dPairs.ensure(n), "alloc pairs");
@@ -780,14 +869,22 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
                        ctx->stream),
        "upload chunks");
-    const size_t w1Slot = (w1Max + 63) / 64 * 64;
-    const size_t ringSlot = (ringMax + 63) / 64 * 64;
+    // Slot sizes rounded up to one of eight levels per power of two (at most
+    // 12.5% larger), so that calls of similar shape keep the same slot layout
+    // (and replay the same launch graph under DMST_MODE_GRAPH).
+    auto slotLevel = [](size_t v) {
+        v = std::max<size_t>(v, 64);
+        const int hb = 63 - __builtin_clzll((unsigned long long)v);
+        const size_t q = std::max<size_t>((size_t)1 << std::max(hb - 3, 6), 64);
+        return (v + q - 1) / q * q;
+    };
+    const size_t w1Slot = slotLevel(w1Max);
+    const size_t ringSlot = slotLevel(ringMax);
     // The groups run one after another on the stream, so they share the slots.
     CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
     const size_t nCounters = allChunks.size() + 3;
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
-    CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
     const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
 
     // Null-model jobs: up to 32 pairs of one read per warp.
@@ -825,19 +922,11 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
        "upload null jobs");
 
     ctx->lastHostMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostT0).count();
-    CK(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
-    {
-        const int nj = (int)nullJobs.size();
-        const int blocks = std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * 16));
-        nullModelKernel<<<blocks, kNullWarps * 32, 0, ctx->stream>>>(
-            ctx->dNullJobs.p, nj, ctx->dNullJobPairs.p, ctx->dPairs.p, ctx->dProfiles.p, ctx->dCodes.p,
-            ctx->dSeeds.p, ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
-        CK(cudaGetLastError(), "null-model kernel");
-    }
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+    const int nj = (int)nullJobs.size();
+    const int nullBlocks = std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * 16));
     DpArgs g;
     g.pairs = ctx->dPairs.p;
     g.profiles = ctx->dProfiles.p;
@@ -851,33 +940,107 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     g.ring = ctx->dRing.p;
     g.ringSlotFloats = ringSlot;
     g.out = ctx->dOut.p;
-    int launches = 1;  // null-model kernel
-    if (!forceExact) {
-        for (int gi = 0; gi < 3; ++gi) {
-            Group &G = groups[gi];
-            if (G.chunks.empty()) continue;
-            if (plain) {
-                // One pair per launch: a one-CTA grid over a one-pair chunk.
-                for (size_t k = 0; k < G.chunks.size(); ++k) {
+    // The device work of the call up to the DP results: counter reset,
+    // null-model kernel, the DP kernels of each rows-per-lane group, and the
+    // timing events between them.
+    int launches = 0;
+    // Inside a stream capture the timing events become external event-record
+    // nodes, which (unlike internal ones) can be read with cudaEventElapsedTime.
+    bool capturing = false;
+    auto record = [&](cudaEvent_t ev) {
+        return capturing ? cudaEventRecordWithFlags(ev, ctx->stream, cudaEventRecordExternal)
+                         : cudaEventRecord(ev, ctx->stream);
+    };
+    auto enqueue = [&]() -> int {
+        launches = 0;
+        CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
+        CK(record(ctx->ev[0]), "event");
+        nullModelKernel<<<nullBlocks, kNullWarps * 32, 0, ctx->stream>>>(
+            ctx->dNullJobs.p, nj, ctx->dNullJobPairs.p, ctx->dPairs.p, ctx->dProfiles.p, ctx->dCodes.p,
+            ctx->dSeeds.p, ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+        CK(cudaGetLastError(), "null-model kernel");
+        ++launches;
+        CK(record(ctx->ev[1]), "event");
+        if (!forceExact) {
+            for (int gi = 0; gi < 3; ++gi) {
+                Group &G = groups[gi];
+                if (G.chunks.empty()) continue;
+                if (plain) {
+                    // One pair per launch: a one-CTA grid over a one-pair chunk.
+                    for (size_t k = 0; k < G.chunks.size(); ++k) {
+                        DpArgs gk = g;
+                        gk.chunks = ctx->dChunks.p + G.chunkBase + k;
+                        gk.nChunks = 1;
+                        gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
+                        G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
+                        ++launches;
+                    }
+                } else {
                     DpArgs gk = g;
-                    gk.chunks = ctx->dChunks.p + G.chunkBase + k;
-                    gk.nChunks = 1;
-                    gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
-                    G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
+                    gk.chunks = ctx->dChunks.p + G.chunkBase;
+                    gk.nChunks = (int)G.chunks.size();
+                    gk.chunkCounter = ctx->dCounter.p + gi;
+                    G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
                     ++launches;
                 }
-            } else {
-                DpArgs gk = g;
-                gk.chunks = ctx->dChunks.p + G.chunkBase;
-                gk.nChunks = (int)G.chunks.size();
-                gk.chunkCounter = ctx->dCounter.p + gi;
-                G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
-                ++launches;
+                CK(cudaGetLastError(), "DP kernel");
             }
-            CK(cudaGetLastError(), "DP kernel");
         }
+        CK(record(ctx->ev[2]), "event");
+        return DMST_OK;
+    };
+    if ((mode & DMST_MODE_GRAPH) && !plain) {
+        // Replay the captured graph when the launch shape and the buffers are
+        // those of the last capture; otherwise capture again and update the
+        // executable graph (or instantiate a new one).
+        std::vector<uintptr_t> key = {(uintptr_t)nCounters, (uintptr_t)nj, (uintptr_t)nullBlocks,
+                                      (uintptr_t)forceExact, (uintptr_t)ctx->dCounter.p, (uintptr_t)ctx->dNullJobs.p,
+                                      (uintptr_t)ctx->dNullJobPairs.p, (uintptr_t)ctx->dPairs.p,
+                                      (uintptr_t)ctx->dProfiles.p, (uintptr_t)ctx->dCodes.p, (uintptr_t)ctx->dSeeds.p,
+                                      (uintptr_t)ctx->dNullTmp.p, (uintptr_t)ctx->dNullTmpOff.p,
+                                      (uintptr_t)ctx->dScales.p, (uintptr_t)ctx->dEmit.p, (uintptr_t)ctx->dParams.p,
+                                      (uintptr_t)ctx->dW1.p, (uintptr_t)ctx->dRing.p, (uintptr_t)ctx->dOut.p,
+                                      (uintptr_t)ctx->dChunks.p, (uintptr_t)w1Slot, (uintptr_t)ringSlot};
+        for (const Group &G : groups) {
+            const uintptr_t v[8] = {(uintptr_t)G.kern, (uintptr_t)G.grid,         (uintptr_t)G.warps,
+                                    (uintptr_t)G.smem, (uintptr_t)G.chunks.size(), (uintptr_t)G.chunkBase,
+                                    (uintptr_t)G.maxRowPad, (uintptr_t)G.kernWarps};
+            key.insert(key.end(), v, v + 8);
+        }
+        if (!ctx->graphExec || key != ctx->graphKey) {
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            capturing = true;
+            const int st = enqueue();
+            capturing = false;
+            const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+            if (st) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            CK(ce, "end capture");
+            if (ctx->graphExec) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(ctx->graphExec, graph, &info) != cudaSuccess) {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(ctx->graphExec);
+                    ctx->graphExec = nullptr;
+                }
+            }
+            cudaError_t ie = cudaSuccess;
+            if (!ctx->graphExec) ie = cudaGraphInstantiate(&ctx->graphExec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(ie, "instantiate graph");
+            ctx->graphKey = key;
+            ctx->graphLaunches = launches;
+            ++ctx->graphCaptures;
+        }
+        CK(cudaGraphLaunch(ctx->graphExec, ctx->stream), "graph launch");
+        launches = ctx->graphLaunches;
+    } else {
+        const int st = enqueue();
+        if (st) return st;
     }
-    CK(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
     std::vector<PairOut> po(n);
     if (!forceExact)
         CK(cudaMemcpyAsync(po.data(), ctx->dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
@@ -957,14 +1120,14 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         }
         CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
         CK(cudaEventSynchronize(ctx->ev[4]), "event");
-        cudaEventElapsedTime(&exactMs, ctx->ev[3], ctx->ev[4]);
+        exactMs = elapsedMs(ctx, ctx->ev[3], ctx->ev[4]);
     }
     ctx->lastExactMs = exactMs;
     ctx->lastExactPairs = (int)flagged.size();
 
     float nullMs = 0, dpMs = 0;
-    cudaEventElapsedTime(&nullMs, ctx->ev[0], ctx->ev[1]);
-    cudaEventElapsedTime(&dpMs, ctx->ev[1], ctx->ev[2]);
+    nullMs = elapsedMs(ctx, ctx->ev[0], ctx->ev[1]);
+    dpMs = elapsedMs(ctx, ctx->ev[1], ctx->ev[2]);
     ctx->lastNullMs = nullMs;
     ctx->lastDpMs = dpMs;
     ctx->lastTotalMs = nullMs + dpMs + exactMs;
@@ -1001,10 +1164,11 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
 
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n) {
     if (!ctx || !out || n < 0) return DMST_EINVAL;
-    const double v[9] = {ctx->lastTotalMs, ctx->lastNullMs,      ctx->lastDpMs,
-                         ctx->lastExactMs, ctx->lastHostMs,      (double)ctx->lastLaunches,
-                         (double)ctx->lastExactPairs, ctx->lastPostMs, ctx->lastWallMs};
-    for (int i = 0; i < n && i < 9; ++i) out[i] = v[i];
+    const double v[10] = {ctx->lastTotalMs, ctx->lastNullMs,      ctx->lastDpMs,
+                          ctx->lastExactMs, ctx->lastHostMs,      (double)ctx->lastLaunches,
+                          (double)ctx->lastExactPairs, ctx->lastPostMs, ctx->lastWallMs,
+                          (double)ctx->graphCaptures};
+    for (int i = 0; i < n && i < 10; ++i) out[i] = v[i];
     return DMST_OK;
 }
 
@@ -1014,6 +1178,57 @@ int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, doubl
     if (dp_ms) *dp_ms = ctx->lastDpMs;
     if (null_ms) *null_ms = ctx->lastNullMs;
     if (launches) *launches = ctx->lastLaunches;
+    return DMST_OK;
+}
+
+int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcups6) {
+    if (!ctx || !sample || n == 0) return DMST_EINVAL;
+    for (size_t i = 0; i < n; ++i)
+        if (sample[i].seq < 0 || sample[i].seq >= (int)ctx->seqLen.size() || sample[i].profile < 0 ||
+            sample[i].profile >= (int)ctx->profiles.size())
+            return ctx->fail(DMST_EINVAL, "autotune sample pair %zu: unknown sequence or profile id", i);
+    std::vector<dmst_result> res(n);
+    Tuning t = ctx->tune;
+    for (int q = 0; q < 3; ++q) {
+        const int R = kShapeR[q];
+        double padded = 0;
+        for (size_t i = 0; i < n; ++i)
+            padded += (double)paddedRows(ctx->profiles[sample[i].profile].M, R) * ctx->seqLen[sample[i].seq];
+        double bestRate = 0;
+        for (int w = 0; w < 2; ++w) {
+            ctx->tune.forceR = R;
+            ctx->tune.forceWarps = kShapeWarps[w];
+            double ms = 0;
+            int st = DMST_OK;
+            for (int rep = 0; rep < 2 && st == DMST_OK; ++rep) {  // the first run warms up
+                st = dmst_score_pairs(ctx, sample, n, DMST_MODE_MID, res.data());
+                ms = ctx->lastDpMs;
+            }
+            ctx->tune.forceR = ctx->tune.forceWarps = 0;
+            if (st) {
+                ctx->tune = t;
+                return st;
+            }
+            const double rate = ms > 0 ? padded / ms : 0;  // padded cells per ms
+            if (gcups6) gcups6[q * 2 + w] = rate / 1e6;
+            if (rate > bestRate) {
+                bestRate = rate;
+                t.warps[q] = kShapeWarps[w];
+            }
+        }
+        t.rate[q] = bestRate;
+    }
+    t.tuned = true;
+    t.forceR = t.forceWarps = 0;
+    ctx->tune = t;
+    return DMST_OK;
+}
+
+int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta) {
+    if (!ctx || M < 1) return DMST_EINVAL;
+    const int R = rowsPerLane(M, ctx->opts.rows_per_lane, ctx->tune);
+    if (rows_per_lane) *rows_per_lane = R;
+    if (warps_per_cta) *warps_per_cta = ctx->tune.warps[rIndex(R)];
     return DMST_OK;
 }
 

@@ -974,27 +974,27 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     }
 }
 
-// CTA shape: kCtaWarps warps share one shared-memory copy of the profile's
-// emission table; at most 128 registers per thread.
-#ifndef DMST_CTA_WARPS
-#define DMST_CTA_WARPS 16
-#endif
-constexpr int kCtaWarps = DMST_CTA_WARPS;
+// CTA shapes: WARPS warps share one shared-memory copy of the profile's
+// emission table, one CTA per SM; 16 warps leave 128 registers per thread,
+// 8 warps 255.  The autotuner picks the shape per rows-per-lane value.
+constexpr int kCtaWarps = 16;       // the default (and widest) shape
+constexpr int kCtaWarpsNarrow = 8;
 
 // Persistent kernel for one rows-per-lane value: CTAs pull chunks
 // (same-profile runs of pairs, costliest first) from a global counter, stage
 // the chunk's profile emission table in shared memory, and their warps pull
 // pairs from the chunk.  Dynamic shared memory: the table (tableFloats), then
-// one Window per warp.
-template <int R, bool MID>
-__global__ void __launch_bounds__(kCtaWarps * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
+// one Window per warp (the launch may use fewer than WARPS warps when the
+// table leaves no room; warp slots are still indexed by WARPS).
+template <int R, bool MID, int WARPS>
+__global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
     extern __shared__ float4 smRaw[];
     float *smE = reinterpret_cast<float *>(smRaw);
     Window *wins = reinterpret_cast<Window *>(smE + tableFloats);
     __shared__ float smBg[32];
     __shared__ int smChunk, smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t slot = (size_t)blockIdx.x * kCtaWarps + warp;
+    const size_t slot = (size_t)blockIdx.x * WARPS + warp;
     float *w1 = g.w1 + slot * g.w1SlotFloats;
     float *ring = g.ring + slot * g.ringSlotFloats;
     Window &win = wins[warp];

@@ -213,11 +213,28 @@ class Context:
         self._check(st, "dmst_score_pairs")
         return res
 
+    def autotune(self, seq_ids: Sequence[int], profile_ids: Sequence[int]) -> dict:
+        """Time every kernel shape on these pairs (dmst_autotune); returns the
+        rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)."""
+        n = len(seq_ids)
+        pairs = (F.Pair * n)()
+        for k, (s, p) in enumerate(zip(seq_ids, profile_ids)):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, p, -2.0
+        out = (C.c_double * 6)()
+        self._check(self.lib.dmst_autotune(self.h, pairs, n, out), "dmst_autotune")
+        return {(r, w): out[i * 2 + j] for i, r in enumerate((4, 2, 1)) for j, w in enumerate((16, 8))}
+
+    def tuned_shape(self, M: int) -> tuple[int, int]:
+        r, w = C.c_int(), C.c_int()
+        self._check(self.lib.dmst_tuned_shape(self.h, M, C.byref(r), C.byref(w)), "dmst_tuned_shape")
+        return r.value, w.value
+
     def last_timing(self) -> dict:
-        v = (C.c_double * 9)()
-        self.lib.dmst_last_timing_ex(self.h, v, 9)
+        v = (C.c_double * 10)()
+        self.lib.dmst_last_timing_ex(self.h, v, 10)
         return {"total_ms": v[0], "null_ms": v[1], "dp_ms": v[2], "exact_ms": v[3], "host_ms": v[4],
-                "launches": int(v[5]), "exact_pairs": int(v[6]), "post_ms": v[7], "wall_ms": v[8]}
+                "launches": int(v[5]), "exact_pairs": int(v[6]), "post_ms": v[7], "wall_ms": v[8],
+                "graph_captures": int(v[9])}
 
     def find_similarities(self, profile: int, decoded: Sequence[np.ndarray]) -> list[Similarity]:
         if len(decoded) == 0:

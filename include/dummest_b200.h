@@ -61,6 +61,15 @@ extern "C" {
  * cross-check of the wavefront paths). */
 #define DMST_MODE_EXACT_SEQUENTIAL 0x400
 
+/* Flag: launch the call's device work up to the DP results (counter reset,
+ * null-model kernel, persistent DP kernels) through a captured CUDA graph.
+ * The graph is captured on the first such call and replayed by later calls
+ * with the same launch shape and buffers (their descriptors are uploaded into
+ * the same device buffers first); a changed shape captures again and updates
+ * the executable graph.  Results are those of the direct launches.  Ignored
+ * with DMST_MODE_PLAIN. */
+#define DMST_MODE_GRAPH 0x800
+
 /* ---- per-result flags -------------------------------------------------- */
 #define DMST_RES_EXACT_PATH 1 /* pair was scored by the exact row-rescaled kernel */
 
@@ -185,9 +194,24 @@ int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, doubl
 /* The same breakdown as an array: out[0] device ms of the call, [1] null-model
  * kernel ms, [2] DP kernel ms, [3] exact-path ms, [4] host preparation ms
  * (wall clock), [5] kernel launches, [6] pairs on the exact path, [7] host ms
- * after the device work (result assembly), [8] wall ms of the whole call.
- * n = number of entries wanted (<= 9). */
+ * after the device work (result assembly), [8] wall ms of the whole call,
+ * [9] CUDA-graph captures made by the context so far (DMST_MODE_GRAPH).
+ * n = number of entries wanted (<= 10). */
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
+
+/* ---- autotuning ------------------------------------------------------
+ * Kernel shapes: R rows of the profile per lane (a stripe of 32 R rows: 4, 2
+ * or 1) and 16 or 8 warps per CTA.  dmst_autotune times the DP kernel of
+ * every shape on the caller's sample of pairs (mode MID, each shape run twice,
+ * the second timed) and keeps, per R, the faster CTA shape and its rate in
+ * computed cells per second.  Later calls with rows_per_lane == 0 then pick,
+ * per profile, the R with the least expected time (computed rows / rate).
+ * gcups6 (may be NULL) receives the rates in GCUPS of computed cells, for
+ * R = 4, 2, 1 x 16, 8 warps.  No counterpart in the reference (its SIMD width
+ * is fixed at compile time). */
+int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcups6);
+/* The shape a call would use for a profile of length M. */
+int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta);
 
 /* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
  * and the three per-base scales (one-nt, two-nt, codon) for one pair, computed
