@@ -812,11 +812,33 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         groups[q].kern = dpKernelFor(kShapeR[q], mid, W);
     }
     auto groupOf = [](int R) { return rIndex(R); };
+    // Warps per CTA: tall profiles leave less shared memory for the windows.
+    // Chunks then hold four pairs per launched warp, fewer when the group has
+    // too few pairs to give each CTA four chunks.
+    const size_t smemLimit = (size_t)ctx->maxSmemOptin - 1024;
+    long long groupPairs[3] = {0, 0, 0};
+    for (size_t k = 0; k < n; ++k) {
+        Group &G = groups[groupOf(dp[k].R)];
+        G.maxRowPad = std::max(G.maxRowPad, ctx->profiles[dp[k].prof].rowPad);
+        ++groupPairs[groupOf(dp[k].R)];
+    }
+    int chunkPairsOf[3] = {1, 1, 1};
+    for (int q = 0; q < 3; ++q) {
+        Group &G = groups[q];
+        if (!groupPairs[q]) continue;
+        const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
+        if (table + sizeof(Window) > smemLimit)
+            return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
+                             (int)((smemLimit - sizeof(Window)) / (kNumCodes * 4)) - 1);
+        G.warps = (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / sizeof(Window));
+        const long long perCta = groupPairs[q] / (4LL * ctx->smCount);
+        chunkPairsOf[q] = plain ? 1 : (int)std::max<long long>(1, std::min<long long>(4LL * G.warps, perCta));
+    }
     for (size_t k = 0; k < n;) {
         Group &G = groups[groupOf(dp[k].R)];
         size_t e = k;
         double cost = 0;
-        const int chunkPairs = plain ? 1 : 4 * G.kernWarps;
+        const int chunkPairs = chunkPairsOf[groupOf(dp[k].R)];
         while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
             cost += (double)(dp[e].M + 1) * dp[e].L;
             ++e;
@@ -824,7 +846,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const int rowPad = ctx->profiles[dp[k].prof].rowPad;
         G.chunks.push_back(Chunk{(int)k, (int)(e - k), dp[k].prof, rowPad});
         G.cost.push_back(cost);
-        G.maxRowPad = std::max(G.maxRowPad, rowPad);
         k = e;
     }
     std::vector<Chunk> allChunks;
@@ -841,14 +862,8 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         }
         G.chunkBase = allChunks.size();
         allChunks.insert(allChunks.end(), G.chunks.begin(), G.chunks.end());
-        // Shared memory: the emission table, then one staging window per warp;
-        // tall profiles get fewer warps so that both fit.
+        // Shared memory: the emission table, then one staging window per warp.
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
-        const size_t limit = (size_t)ctx->maxSmemOptin - 1024;
-        if (table + sizeof(Window) > limit)
-            return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
-                             (int)((limit - sizeof(Window)) / (kNumCodes * 4)) - 1);
-        G.warps = (int)std::min<size_t>(G.kernWarps, (limit - table) / sizeof(Window));
         G.smem = table + (size_t)G.warps * sizeof(Window);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
@@ -856,7 +871,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
         if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
         G.grid = plain ? 1 : (int)std::min<long long>((long long)perSm * ctx->smCount, (long long)G.chunks.size());
-        slotsMax = std::max(slotsMax, (size_t)G.grid * G.kernWarps);
+        slotsMax = std::max(slotsMax, (size_t)G.grid * G.warps);
     }
 
     CK(ctx->dPairs.ensure(n), "alloc pairs");

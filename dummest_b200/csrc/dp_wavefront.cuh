@@ -985,7 +985,7 @@ constexpr int kCtaWarpsNarrow = 8;
 // the chunk's profile emission table in shared memory, and their warps pull
 // pairs from the chunk.  Dynamic shared memory: the table (tableFloats), then
 // one Window per warp (the launch may use fewer than WARPS warps when the
-// table leaves no room; warp slots are still indexed by WARPS).
+// table leaves no room; W1 slots are indexed by the launched warps).
 template <int R, bool MID, int WARPS>
 __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
     extern __shared__ float4 smRaw[];
@@ -994,7 +994,7 @@ __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tabl
     __shared__ float smBg[32];
     __shared__ int smChunk, smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t slot = (size_t)blockIdx.x * WARPS + warp;
+    const size_t slot = (size_t)blockIdx.x * (blockDim.x >> 5) + warp;  // launched warps, not WARPS
     float *w1 = g.w1 + slot * g.w1SlotFloats;
     float *ring = g.ring + slot * g.ringSlotFloats;
     Window &win = wins[warp];

@@ -178,3 +178,31 @@ def batched_config(seed: int = 20261205, n_profiles: int = 64, n_reads: int = 10
     profiles = [make_profile(rng, int(M), f"synth{k:03d}") for k, M in enumerate(Ms)]
     reads = make_reads(rng, n_reads, lmin, lmax, profiles, implant_frac, gc_range=(0.4, 0.6))
     return profiles, reads
+
+
+def genome_scan_config(seed: int = 20261207, M: int = 2000, genome_len: int = 10_000_000, gc: float = 0.45,
+                       window: int = 10_000, overlap: int = 1_000, n_implants: int = 200):
+    """The long-profile genome scan: one profile of length M, a uniform random
+    genome of genome_len nt at the given GC content carrying n_implants
+    frameshifted homologs of the profile (random strand and offset), cut into
+    windows of `window` nt overlapping by `overlap`.  Returns (profile,
+    windows), the windows as both-strand records (forward, reverse
+    complement, ...)."""
+    rng = np.random.default_rng(seed)
+    prof = make_profile(rng, M, f"scan{M}")
+    p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
+    g = np.frombuffer(b"ACGT", np.uint8)[rng.choice(4, size=genome_len, p=p)].copy()
+    for _ in range(n_implants):
+        h = sample_homolog(rng, prof, max_aa=int(rng.integers(M // 4, M + 1)))
+        if rng.random() < 0.5:
+            h = revcomp(h)
+        hb = np.frombuffer(h.encode(), np.uint8)
+        off = int(rng.integers(0, genome_len - len(hb)))
+        g[off:off + len(hb)] = hb
+    step = window - overlap
+    windows = []
+    for start in range(0, max(genome_len - overlap, 1), step):
+        w = g[start:start + window].tobytes().decode()
+        if len(w) >= 3:
+            windows.append(w)
+    return prof, both_strands(windows)
