@@ -108,6 +108,14 @@ SIGNATURES = [
     ("dmst_last_timing_ex", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("dmst_null_model", C.c_int,
      [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("dmst_profile_set", C.c_int,
+     [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(Params), C.POINTER(C.c_float)]),
+    ("dmst_loglik_grad", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double),
+      C.POINTER(C.c_double)]),
+    ("dmst_posteriors", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("dmst_seq_length", C.c_int, [C.c_void_p, C.c_int]),
     ("dmst_autotune", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double)]),
     ("dmst_tuned_shape", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("dmst_null_model_noalloc", C.c_int,

@@ -4,6 +4,7 @@
 
 #include "dp_common.cuh"
 #include "dp_exact.cuh"
+#include "dp_adjoint.cuh"
 #include "dp_exact_wave.cuh"
 #include "dp_wavefront.cuh"
 #include "host_model.h"
@@ -250,6 +251,10 @@ struct dmst_ctx {
     DevBuf<float> dW1, dRing;
     DevBuf<ExactJob> dJobs;
     DevBuf<ExactWaveJob> dWaveJobs;
+    DevBuf<AdjointJob> dAdjJobs;             // dmst_loglik_grad, dmst_posteriors
+    DevBuf<double> dPost;                    // dmst_posteriors: the batch's posterior tables
+    DevBuf<double> dAdjF, dAdjB, dGrad, dLogT;
+    std::vector<int> lastOrder;              // sorted position -> caller's pair index of the last call
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
 
@@ -375,6 +380,12 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dRing.release();
     ctx->dJobs.release();
     ctx->dWaveJobs.release();
+    ctx->dAdjJobs.release();
+    ctx->dAdjF.release();
+    ctx->dAdjB.release();
+    ctx->dGrad.release();
+    ctx->dLogT.release();
+    ctx->dPost.release();
     ctx->dExactScratch.release();
     ctx->dExactOut.release();
     for (auto &e : ctx->ev)
@@ -386,9 +397,8 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
 // ---------------------------------------------------------------------------
 // Profiles
 // ---------------------------------------------------------------------------
-int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const dmst_params *params,
-                     const float *bg, int *id) {
-    if (!ctx || !values || !params || !bg || width != kWidth || M < 2) return DMST_EINVAL;
+static HostProfile makeHostProfile(const float *values, int width, int M, const dmst_params *params,
+                                   const float *bg) {
     HostProfile hp;
     hp.M = M;
     hp.rowPad = (M + 1 + kRowAlign - 1) / kRowAlign * kRowAlign;
@@ -400,9 +410,25 @@ int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const
     for (int c = 0; c < 26; ++c) hp.bg[c] = (c < kNumCodes) ? bg[4 + c] : 0.0f;
     hp.bg[kPad] = 0.0f;  // zero_idx pad reads as 0
     hp.values.assign(values, values + (size_t)(M + 1) * width);
-    ctx->profiles.push_back(std::move(hp));
+    return hp;
+}
+
+int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const dmst_params *params,
+                     const float *bg, int *id) {
+    if (!ctx || !values || !params || !bg || width != kWidth || M < 2) return DMST_EINVAL;
+    ctx->profiles.push_back(makeHostProfile(values, width, M, params, bg));
     ctx->profilesDirty = true;
     if (id) *id = (int)ctx->profiles.size() - 1;
+    return DMST_OK;
+}
+
+int dmst_profile_set(dmst_ctx *ctx, int id, const float *values, int width, int M, const dmst_params *params,
+                     const float *bg) {
+    if (!ctx || !values || !params || !bg || width != kWidth || M < 2 || id < 0 ||
+        id >= (int)ctx->profiles.size())
+        return DMST_EINVAL;
+    ctx->profiles[id] = makeHostProfile(values, width, M, params, bg);
+    ctx->profilesDirty = true;
     return DMST_OK;
 }
 
@@ -635,6 +661,10 @@ int dmst_seqs_clear(dmst_ctx *ctx) {
 
 int dmst_seq_count(const dmst_ctx *ctx) { return ctx ? (int)ctx->seqLen.size() : 0; }
 
+int dmst_seq_length(const dmst_ctx *ctx, int id) {
+    return (ctx && id >= 0 && id < (int)ctx->seqLen.size()) ? ctx->seqLen[id] : -1;
+}
+
 int dmst_decode_letters(const char *letters, int L, uint8_t *codes) {
     if (!letters || !codes || L < 0) return DMST_EINVAL;
     decodeLetters(letters, L, codes);
@@ -694,8 +724,13 @@ static float elapsedMs(dmst_ctx *ctx, cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
+// Internal mode bit: set up the pairs and run the null model only (the
+// device pair descriptors, seeds and scales of the call stay in the context).
+constexpr int kModeNullOnly = 0x10000;
+
 int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
-    if (!ctx || (n && (!pairs || !out))) return DMST_EINVAL;
+    const bool nullOnly = (mode & kModeNullOnly) != 0;
+    if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
     const int base = mode & 0xff;
     const bool plain = (mode & DMST_MODE_PLAIN) != 0;
     const bool forceExact = (mode & (DMST_MODE_FORCE_EXACT | DMST_MODE_EXACT_SEQUENTIAL)) != 0;
@@ -770,6 +805,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             }
         }
     }
+    ctx->lastOrder = order;
     std::vector<DevPair> dp(n);
     long long seedFloats = 0;
     size_t w1Max = 0, ringMax = 0;
@@ -817,7 +853,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     // too few pairs to give each CTA four chunks.
     const size_t smemLimit = (size_t)ctx->maxSmemOptin - 1024;
     long long groupPairs[3] = {0, 0, 0};
-    for (size_t k = 0; k < n; ++k) {
+    for (size_t k = 0; k < n && !nullOnly; ++k) {
         Group &G = groups[groupOf(dp[k].R)];
         G.maxRowPad = std::max(G.maxRowPad, ctx->profiles[dp[k].prof].rowPad);
         ++groupPairs[groupOf(dp[k].R)];
@@ -834,7 +870,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const long long perCta = groupPairs[q] / (4LL * ctx->smCount);
         chunkPairsOf[q] = plain ? 1 : (int)std::max<long long>(1, std::min<long long>(4LL * G.warps, perCta));
     }
-    for (size_t k = 0; k < n;) {
+    for (size_t k = 0; k < n && !nullOnly;) {
         Group &G = groups[groupOf(dp[k].R)];
         size_t e = k;
         double cost = 0;
@@ -881,9 +917,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(ctx->dChunks.ensure(allChunks.size()), "alloc chunks");
     CK(cudaMemcpyAsync(ctx->dPairs.p, dp.data(), n * sizeof(DevPair), cudaMemcpyHostToDevice, ctx->stream),
        "upload pairs");
-    CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice,
-                       ctx->stream),
-       "upload chunks");
+    if (!allChunks.empty())
+        CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk),
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "upload chunks");
     // Slot sizes rounded up to one of eight levels per power of two (at most
     // 12.5% larger), so that calls of similar shape keep the same slot layout
     // (and replay the same launch graph under DMST_MODE_GRAPH).
@@ -976,7 +1013,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaGetLastError(), "null-model kernel");
         ++launches;
         CK(record(ctx->ev[1]), "event");
-        if (!forceExact) {
+        if (!forceExact && !nullOnly) {
             for (int gi = 0; gi < 3; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
@@ -1004,7 +1041,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(record(ctx->ev[2]), "event");
         return DMST_OK;
     };
-    if ((mode & DMST_MODE_GRAPH) && !plain) {
+    if ((mode & DMST_MODE_GRAPH) && !plain && !nullOnly) {
         // Replay the captured graph when the launch shape and the buffers are
         // those of the last capture; otherwise capture again and update the
         // executable graph (or instantiate a new one).
@@ -1056,11 +1093,12 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const int st = enqueue();
         if (st) return st;
     }
-    std::vector<PairOut> po(n);
-    if (!forceExact)
+    std::vector<PairOut> po(nullOnly ? 0 : n);
+    if (!forceExact && !nullOnly)
         CK(cudaMemcpyAsync(po.data(), ctx->dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
            "download results");
     CK(cudaStreamSynchronize(ctx->stream), "DP kernel");
+    if (nullOnly) return DMST_OK;
 
     // Pairs outside the fast path's exact range go to the row-rescaled kernel.
     std::vector<int> flagged;
@@ -1237,6 +1275,118 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
     t.forceR = t.forceWarps = 0;
     ctx->tune = t;
     return DMST_OK;
+}
+
+// The adjoint kernel over n pairs of one profile: log T per pair, the summed
+// gradient of log T (Params then emissions) and, if post is given, each
+// pair's posterior tables at the offsets of dmst_posteriors.
+static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *grad_params,
+                      double *grad_emit, double *post, const char *what) {
+    if (!ctx || !pairs || n == 0 || (n >> 31)) return DMST_EINVAL;
+    const int prof = pairs[0].profile;
+    for (size_t i = 0; i < n; ++i)
+        if (pairs[i].profile != prof)
+            return ctx->fail(DMST_EINVAL, "%s: pair %zu is for another profile (one profile per call)", what, i);
+    // Pair descriptors, null models and seeds on the device, sorted longest
+    // read first.
+    int st = dmst_score_pairs(ctx, pairs, n, DMST_MODE_MID | kModeNullOnly, nullptr);
+    if (st) return st;
+    const std::vector<int> order = ctx->lastOrder;
+    const int M = ctx->profiles[prof].M;
+    // Posterior offsets in the caller's order.
+    std::vector<long long> postOff(n, -1);
+    if (post) {
+        long long o = 0;
+        for (size_t i = 0; i < n; ++i) {
+            postOff[i] = o;
+            o += 2LL * (M + 1) * ctx->seqLen[pairs[i].seq];
+        }
+    }
+    std::vector<AdjointJob> jobs(n);
+    std::vector<long long> warpF, warpB, warpP;
+    for (size_t w0 = 0; w0 < n; w0 += 32) {
+        const int Lw = ctx->seqLen[pairs[order[w0]].seq];  // longest of the warp
+        long long pNeed = 0;
+        for (size_t k = w0; k < std::min(n, w0 + 32); ++k) {
+            const long long pk = post ? 2LL * (M + 1) * ctx->seqLen[pairs[order[k]].seq] : 0;
+            jobs[k] = AdjointJob{(int)k, Lw, 0, 0, post ? pNeed : -1};
+            pNeed += pk;
+        }
+        warpF.push_back(adjStoreDoubles(M, Lw));
+        warpB.push_back(adjRowDoubles(Lw));
+        warpP.push_back(pNeed);
+    }
+    const size_t gN = (size_t)(M + 2) * kParamFloats + (size_t)(M + 1) * kNumCodes;
+    CK(cudaSetDevice(ctx->device), "set device");
+    CK(ctx->dGrad.ensure(gN), "alloc gradient");
+    CK(ctx->dLogT.ensure(n), "alloc log T");
+    CK(ctx->dAdjJobs.ensure(n), "alloc adjoint jobs");
+    CK(cudaMemsetAsync(ctx->dGrad.p, 0, gN * sizeof(double), ctx->stream), "zero gradient");
+    // Batches of whole warps under the device budget (the forward store is
+    // 24 bytes per cell, the posterior tables 16).
+    size_t freeB = 0, totalB = 0;
+    CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+    const size_t budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : freeB / 2;
+    const size_t nWarps = warpF.size();
+    for (size_t w = 0; w < nWarps;) {
+        size_t w1 = w;
+        long long f = 0, b = 0, pp = 0;
+        while (w1 < nWarps &&
+               (w1 == w || (size_t)(f + warpF[w1] + b + warpB[w1] + pp + warpP[w1]) * 8 <= budget)) {
+            // offsets of this warp's buffers inside the batch
+            for (size_t k = w1 * 32; k < std::min(n, w1 * 32 + 32); ++k) {
+                jobs[k].fOff = f;
+                jobs[k].bOff = b;
+                if (post) jobs[k].pOff += pp;
+            }
+            f += warpF[w1];
+            b += warpB[w1];
+            pp += warpP[w1];
+            ++w1;
+        }
+        const size_t k0 = w * 32, k1 = std::min(n, w1 * 32);
+        const int nj = (int)(k1 - k0);
+        CK(ctx->dAdjF.ensure((size_t)f), "alloc adjoint store");
+        CK(ctx->dAdjB.ensure((size_t)b), "alloc adjoint rows");
+        if (post) CK(ctx->dPost.ensure((size_t)std::max<long long>(pp, 1)), "alloc posterior tables");
+        CK(cudaMemcpyAsync(ctx->dAdjJobs.p, jobs.data() + k0, nj * sizeof(AdjointJob), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload adjoint jobs");
+        const int blocks = (nj + 127) / 128;
+        adjointKernel<<<blocks, 128, 0, ctx->stream>>>(
+            ctx->dAdjJobs.p, nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
+            ctx->dSeeds.p, ctx->dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
+            post ? ctx->dPost.p : nullptr);
+        CK(cudaGetLastError(), "adjoint kernel");
+        if (post)
+            for (size_t k = k0; k < k1; ++k) {
+                const size_t cnt = 2 * (size_t)(M + 1) * ctx->seqLen[pairs[order[k]].seq];
+                CK(cudaMemcpyAsync(post + postOff[order[k]], ctx->dPost.p + jobs[k].pOff, cnt * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->stream),
+                   "download posterior tables");
+            }
+        CK(cudaStreamSynchronize(ctx->stream), "adjoint kernel");
+        w = w1;
+    }
+    std::vector<double> g(gN), lt(n);
+    CK(cudaMemcpy(g.data(), ctx->dGrad.p, gN * sizeof(double), cudaMemcpyDeviceToHost), "download gradient");
+    CK(cudaMemcpy(lt.data(), ctx->dLogT.p, n * sizeof(double), cudaMemcpyDeviceToHost), "download log T");
+    if (log_t)
+        for (size_t k = 0; k < n; ++k) log_t[order[k]] = lt[k];
+    if (grad_params) std::memcpy(grad_params, g.data(), (size_t)(M + 2) * kParamFloats * sizeof(double));
+    if (grad_emit)
+        std::memcpy(grad_emit, g.data() + (size_t)(M + 2) * kParamFloats, (size_t)(M + 1) * kNumCodes * sizeof(double));
+    return DMST_OK;
+}
+
+int dmst_loglik_grad(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *grad_params,
+                     double *grad_emit) {
+    return runAdjoint(ctx, pairs, n, log_t, grad_params, grad_emit, nullptr, "dmst_loglik_grad");
+}
+
+int dmst_posteriors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *post) {
+    if (!post) return DMST_EINVAL;
+    return runAdjoint(ctx, pairs, n, log_t, nullptr, nullptr, post, "dmst_posteriors");
 }
 
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta) {

@@ -213,6 +213,58 @@ class Context:
         self._check(st, "dmst_score_pairs")
         return res
 
+    def set_profile(self, pid: int, values: np.ndarray, params: np.ndarray, bg: np.ndarray) -> None:
+        """Replace profile pid (dmst_profile_set); shapes as for add_profile."""
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        bg = np.ascontiguousarray(bg, dtype=np.float32)
+        M = values.shape[0] - 1
+        st = self.lib.dmst_profile_set(self.h, pid, values.ctypes.data_as(C.POINTER(C.c_float)), 29, M,
+                                       params.ctypes.data_as(C.POINTER(F.Params)),
+                                       bg.ctypes.data_as(C.POINTER(C.c_float)))
+        self._check(st, "dmst_profile_set")
+
+    def loglik_grad(self, seq_ids: Sequence[int], pid: int):
+        """(log T per pair, d sum(log T)/d Params (M+2, 11), d sum(log T)/d emissions (M+1, 25))
+        for the reads seq_ids against profile pid (dmst_loglik_grad)."""
+        n = len(seq_ids)
+        M = self.profile_length(pid)
+        pairs = (F.Pair * n)()
+        for k, s in enumerate(seq_ids):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, pid, -2.0
+        logt = np.zeros(n, np.float64)
+        gp = np.zeros((M + 2, 11), np.float64)
+        ge = np.zeros((M + 1, 25), np.float64)
+        D = C.POINTER(C.c_double)
+        st = self.lib.dmst_loglik_grad(self.h, pairs, n, logt.ctypes.data_as(D), gp.ctypes.data_as(D),
+                                       ge.ctypes.data_as(D))
+        self._check(st, "dmst_loglik_grad")
+        return logt, gp, ge
+
+    def seq_length(self, sid: int) -> int:
+        return self.lib.dmst_seq_length(self.h, sid)
+
+    def posteriors(self, seq_ids: Sequence[int], pid: int):
+        """(log T per pair, [(cell (M+1, L), match (M+1, L)) per pair]) for the
+        reads seq_ids against profile pid (dmst_posteriors)."""
+        n = len(seq_ids)
+        M = self.profile_length(pid)
+        pairs = (F.Pair * n)()
+        lens = [self.seq_length(s) for s in seq_ids]
+        for k, s in enumerate(seq_ids):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, pid, -2.0
+        logt = np.zeros(n, np.float64)
+        post = np.zeros(2 * (M + 1) * sum(lens), np.float64)
+        D = C.POINTER(C.c_double)
+        st = self.lib.dmst_posteriors(self.h, pairs, n, logt.ctypes.data_as(D), post.ctypes.data_as(D))
+        self._check(st, "dmst_posteriors")
+        out, o = [], 0
+        for L in lens:
+            t = post[o:o + 2 * (M + 1) * L].reshape(2, M + 1, L)
+            out.append((t[0], t[1]))
+            o += 2 * (M + 1) * L
+        return logt, out
+
     def autotune(self, seq_ids: Sequence[int], profile_ids: Sequence[int]) -> dict:
         """Time every kernel shape on these pairs (dmst_autotune); returns the
         rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)."""

@@ -140,6 +140,11 @@ void *dmst_ctx_stream(const dmst_ctx *ctx);
 int dmst_profile_add(dmst_ctx *ctx, const float *values, int width, int M, const dmst_params *params,
                      const float *bg, int *id);
 
+/* Replace profile `id` by new values, Params and background (any length);
+ * later calls use the new profile.  For refining a profile in place. */
+int dmst_profile_set(dmst_ctx *ctx, int id, const float *values, int width, int M, const dmst_params *params,
+                     const float *bg);
+
 /* Parse HMMER3 text and finalize each profile with the reference's semantics
  * (readProfiles + finalizeProfile without tantan masking or filtering;
  * background type 'G', 'A' or 'M').  Replaces: readProfiles
@@ -176,6 +181,8 @@ int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *m
 /* Drop all sequences (device memory is kept for reuse). */
 int dmst_seqs_clear(dmst_ctx *ctx);
 int dmst_seq_count(const dmst_ctx *ctx);
+/* Length in nucleotides of sequence id, -1 for an unknown id. */
+int dmst_seq_length(const dmst_ctx *ctx, int id);
 
 /* Host decode of letter codes (A=0 C=1 G=5 T=16, masked=22, the engine's
  * protein-alphabet coding of DNA) into codon codes; replaces decodeSequence. */
@@ -212,6 +219,32 @@ int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
 int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcups6);
 /* The shape a call would use for a profile of length M. */
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta);
+
+/* ---- log-likelihood and its gradient --------------------------------------
+ * For pairs of one profile: log_t[k] = log T of pair k, T the total weight of
+ * all local alignments of the read under the profile, i.e. the sum over cells
+ * of prefixSeed[j] * W1[i][j] (equally, of W0[i][j] * suffixSeedFromNext[j]);
+ * and the gradient of sum_k log T_k with respect to the profile's Params
+ * (grad_params: (M+2) x 11 doubles, the dmst_params fields in order) and its
+ * emission table (grad_emit: (M+1) x 25 doubles, the entries values[i][4+c]).
+ * The null model (seeds, per-base scales, background) is held fixed.  Any of
+ * the outputs may be NULL.  FP64 throughout.  The reference computes no
+ * gradient: its forward recurrence (dummest-dp-forward.hh:63-250) is the
+ * adjoint of its backward one (dummest-dp-backward.hh:473-574), and this call
+ * evaluates both, with the gradient sums of each row. */
+int dmst_loglik_grad(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *grad_params,
+                     double *grad_emit);
+
+/* Posterior tables of pairs of one profile, FP64.  For pair k (the caller's
+ * order), at post + sum_{k'<k} 2 (M+1) L_k': (M+1) x L_k doubles of cell
+ * posteriors W0[i][j] W1[i][j] / T, then (M+1) x L_k doubles of match
+ * posteriors X(i,j) W1[i+1][j] / T, X(i,j) the match term of the forward
+ * (enter_i sC e_i(c_{j-2}) W0[i][j-3]; the combined table of
+ * dummest-dp-forward.hh:125-157, divided by T).  log_t (n, may be NULL) as in
+ * dmst_loglik_grad.  The reference's search never outputs posteriors; its
+ * mid score is the maximum over cells of W0 W1 (dummest-dp-forward.hh:174-206),
+ * so max_ij cell * T is that score. */
+int dmst_posteriors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *post);
 
 /* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
  * and the three per-base scales (one-nt, two-nt, codon) for one pair, computed

@@ -587,3 +587,239 @@ int dmsto_filter_pair(const float *values, const float *params, const float *bg,
     ftz_leave(csr);
     return st;
 }
+
+/* ---------------------------------------------------------------------------
+ * log T in FP64 (the finite-difference oracle of the library's gradient): T
+ * is the total weight of all local alignments of the read, the sum over cells
+ * of prefixSeed[j] * W1[i][j], W1 the backward recurrence
+ * (dummest-dp-backward.hh:473-574) evaluated in double on double-precision
+ * profile values (values: (M+1) x 29, params: (M+2) x 11).  The null model is
+ * the reference's, computed from the float background (it is held fixed).
+ * Rows are scaled by 2^-512 when their maximum passes 2^512 (exact powers of
+ * two), and T is summed as a mantissa with a binary exponent.
+ * ------------------------------------------------------------------------- */
+int dmsto_log_total(const double *values, const double *params, const float *bg, int M, const uint8_t *codes,
+                    int L, dmsto_rates r, double *logT) {
+    if (!values || !params || !bg || !codes || M < 1 || L < 3 || !logT) return -1;
+    const unsigned csr = ftz_enter();
+    float *seeds = (float *)calloc(2 * (size_t)L + 8, sizeof(float));
+    const size_t W = (size_t)L + 4;
+    double *rows = (double *)calloc(4 * W, sizeof(double));
+    int st = -1;
+    null_out o = {seeds, seeds + L + 4, 0, 0, 0};
+    if (seeds && rows && !null_model(bg, codes, L, r, &o)) {
+        const double s1 = o.s1, s2 = o.s2, sC = o.sC;
+        const float *bg4 = bg + 4;
+        double *below = rows, *row = rows + W, *ynext = rows + 2 * W, *ycur = rows + 3 * W;
+        int cnt = 0;
+        double tm = 0.0;  /* T = tm * 2^te */
+        int te = 0;
+        for (int i = M; i >= 0; --i) {
+            const double *q = params + (size_t)i * NPARAM;
+            const double *erow = values + (size_t)i * WIDTH + 4;
+            const double enter = q[10] * sC, d0 = q[6], d1 = q[7] * s2, d2 = q[8] * s1;
+            const double a0 = q[0] * sC, a1 = q[1] * s1, a2 = q[2] * s2, b0 = q[3] * sC, eps = q[9];
+            double z[4] = {0, 0, 0, 0};
+            double n3 = below[L + 2], n2 = below[L + 1], n1 = below[L], c2 = 0, c1 = 0;
+            double mx = 0, part = 0;
+            for (int j = L; j < L + 4; ++j) row[j] = 0;
+            for (int j = L - 1; j >= 0; --j) {
+                const int c = (j + 1 < L) ? codes[j + 1] : NCODE_PAD;
+                const double zbg = z[(j + 3) & 3] * (double)bg4[c];
+                const double w = n3 * erow[c] * enter + ynext[j] * d0 + n2 * d1 + n1 * d2 + zbg * a0 + c2 * a2 +
+                                 c1 * a1 + ldexp((double)o.suf[j], -512 * cnt);
+                row[j] = w;
+                ycur[j] = eps * ynext[j] + w;
+                z[j & 3] = b0 * zbg + w;
+                part += (double)o.pre[j] * w;
+                if (ycur[j] > mx) mx = ycur[j];
+                n3 = n2; n2 = n1; n1 = below[j];
+                c2 = c1; c1 = w;
+            }
+            /* add part * 2^(512 cnt) to T */
+            if (part > 0) {
+                int pe;
+                const double pm = frexp(part, &pe);
+                pe += 512 * cnt;
+                if (tm == 0 || pe > te + 60) {
+                    tm = pm;
+                    te = pe;
+                } else if (pe >= te - 60) {
+                    int e2;
+                    tm = frexp(tm + ldexp(pm, pe - te), &e2);  /* keep tm in [0.5, 1) */
+                    te += e2;
+                }
+            }
+            if (mx > 0x1p512) {  /* this row and the Y rows the next one reads */
+                ++cnt;
+                for (size_t k = 0; k < W; ++k) {
+                    row[k] = ldexp(row[k], -512);
+                    ycur[k] = ldexp(ycur[k], -512);
+                }
+            }
+            double *t = below;
+            below = row;
+            row = t;
+            t = ynext;
+            ynext = ycur;
+            ycur = t;
+        }
+        *logT = tm > 0 ? log(tm) + te * 0.6931471805599453 : -INFINITY;
+        st = 0;
+    }
+    free(seeds);
+    free(rows);
+    ftz_leave(csr);
+    return st;
+}
+
+/* ---------------------------------------------------------------------------
+ * Posterior tables in FP64.  The forward recurrence (dummest-dp-forward.hh:
+ * 63-250) and the backward one (dummest-dp-backward.hh:473-574) evaluated in
+ * double on double profile arrays, without anchoring:
+ *   forward, row i:  W0in[i][j] = X(i-1,j) + Y0[i-1][j] + d'1 s2 W0[i-1][j-2] + d'2 s1 W0[i-1][j-1],
+ *                    X(i,j) = enter_i sC e_i(c_{j-2}) W0[i][j-3],
+ *                    Z0[j] = bg[j-2] sC (a'0 W0[i][j-3] + b'0 Z0[j-3]),
+ *                    W0[i][j] = W0in + Z0 + a'1 s1 W0[i][j-1] + a'2 s2 W0[i][j-2] + pre[j],
+ *                    Y0[i][j] = d'0 W0[i][j] + eps' Y0[i-1][j];
+ *   backward:        as dmsto_log_total.
+ * Each row is held at its own power-of-two offset (the exponent of the
+ * maximum of the row it reads from), so values far below a row's maximum
+ * flush to zero as in the reference's per-row rescaling, in double range.
+ * Outputs (each (M+1) x L, row-major): cell[i][j] = W0[i][j] W1[i][j] / T and
+ * match[i][j] = X(i,j) W1[i+1][j] / T (the match-state posterior of the
+ * combined table, dummest-dp-forward.hh:125-157); log T from the forward
+ * total sum W0 suf and, as a self-check, from the backward total sum pre W1.
+ * ------------------------------------------------------------------------- */
+typedef struct { double m; int e; } dx;  /* m * 2^e, m in [0.5, 1) or 0 */
+
+static void dx_add(dx *a, double v, int ve) {
+    if (!(v > 0)) return;
+    int pe;
+    const double pm = frexp(v, &pe);
+    pe += ve;
+    if (a->m == 0 || pe > a->e + 60) {
+        a->m = pm;
+        a->e = pe;
+    } else if (pe >= a->e - 60) {
+        int e2;
+        a->m = frexp(a->m + ldexp(pm, pe - a->e), &e2);
+        a->e += e2;
+    }
+}
+
+static int row_exponent(const double *a, const double *b, int n) {
+    double mx = 0;
+    for (int k = 0; k < n; ++k) {
+        if (a[k] > mx) mx = a[k];
+        if (b && b[k] > mx) mx = b[k];
+    }
+    int e = 0;
+    if (mx > 0) frexp(mx, &e);
+    return e;
+}
+
+int dmsto_posteriors(const double *values, const double *params, const float *bg, int M, const uint8_t *codes,
+                     int L, dmsto_rates r, double *logT_fwd, double *logT_bwd, double *cell, double *match) {
+    if (!values || !params || !bg || !codes || M < 1 || L < 3) return -1;
+    const unsigned csr = ftz_enter();
+    const size_t R = (size_t)M + 1;
+    float *seeds = (float *)calloc(2 * (size_t)L + 8, sizeof(float));
+    double *W0 = (double *)calloc(R * (size_t)L, sizeof(double));
+    double *Y0 = (double *)calloc(R * (size_t)L, sizeof(double));
+    int *eF = (int *)calloc(R, sizeof(int));
+    const size_t W = (size_t)L + 4;
+    double *rows = (double *)calloc(4 * W, sizeof(double));
+    int st = -1;
+    null_out o = {seeds, seeds + L + 4, 0, 0, 0};
+    if (seeds && W0 && Y0 && eF && rows && !null_model(bg, codes, L, r, &o)) {
+        const double s1 = o.s1, s2 = o.s2, sC = o.sC;
+        const float *bg4 = bg + 4;
+#define CODE(j) (((j) >= 0 && (j) < L) ? codes[(j)] : NCODE_PAD)
+        dx Tf = {0, 0}, Tb = {0, 0};
+        /* forward */
+        for (int i = 0; i <= M; ++i) {
+            const double *q = params + (size_t)i * NPARAM;
+            const double *qp = params + (size_t)(i > 0 ? i - 1 : 0) * NPARAM;
+            const double *eprev = values + (size_t)(i > 0 ? i - 1 : 0) * WIDTH + 4;
+            double *w = W0 + (size_t)i * L, *y = Y0 + (size_t)i * L;
+            const double *wp = i > 0 ? W0 + (size_t)(i - 1) * L : NULL, *yp = i > 0 ? Y0 + (size_t)(i - 1) * L : NULL;
+            const int sh = i > 0 ? row_exponent(wp, yp, L) : 0;
+            eF[i] = i > 0 ? eF[i - 1] + sh : 0;
+            const double f = ldexp(1.0, -sh);
+            double z[3] = {0, 0, 0};
+            double part = 0;
+            for (int j = 0; j < L; ++j) {
+                double in = 0;
+                if (i > 0) {
+                    const double u3 = j >= 3 ? wp[j - 3] : 0, u2 = j >= 2 ? wp[j - 2] : 0, u1 = j >= 1 ? wp[j - 1] : 0;
+                    in = (qp[10] * sC * eprev[CODE(j - 2)] * u3 + yp[j] + qp[7] * s2 * u2 + qp[8] * s1 * u1) * f;
+                }
+                const double w3 = j >= 3 ? w[j - 3] : 0, w2 = j >= 2 ? w[j - 2] : 0, w1 = j >= 1 ? w[j - 1] : 0;
+                const double zz = (double)bg4[CODE(j - 2)] * sC * (q[0] * w3 + q[3] * z[j % 3]);
+                w[j] = in + zz + q[1] * s1 * w1 + q[2] * s2 * w2 + ldexp((double)o.pre[j], -eF[i]);
+                y[j] = q[6] * w[j] + q[9] * (i > 0 ? yp[j] * f : 0);
+                z[j % 3] = zz;
+                part += w[j] * (double)o.suf[j];
+            }
+            dx_add(&Tf, part, eF[i]);
+        }
+        /* backward */
+        const double invT = Tf.m > 0 ? 1.0 / Tf.m : 0.0;
+        double *below = rows, *row = rows + W, *ynext = rows + 2 * W, *ycur = rows + 3 * W;
+        int eBn = 0; /* offset of row i+1 */
+        for (int i = M; i >= 0; --i) {
+            const double *q = params + (size_t)i * NPARAM;
+            const double *erow = values + (size_t)i * WIDTH + 4;
+            const int sh = i < M ? row_exponent(below, ynext, L) : 0;
+            const int eB = eBn + sh;
+            const double f = ldexp(1.0, -sh);
+            const double enter = q[10] * sC, d0 = q[6], d1 = q[7] * s2, d2 = q[8] * s1;
+            const double a0 = q[0] * sC, a1 = q[1] * s1, a2 = q[2] * s2, b0 = q[3] * sC, eps = q[9];
+            double z[4] = {0, 0, 0, 0};
+            double n3 = below[L + 2] * f, n2 = below[L + 1] * f, n1 = below[L] * f, c2 = 0, c1 = 0, part = 0;
+            for (int j = L; j < L + 4; ++j) row[j] = ycur[j] = 0;
+            for (int j = L - 1; j >= 0; --j) {
+                const int c = CODE(j + 1);
+                const double zbg = z[(j + 3) & 3] * (double)bg4[c];
+                const double yn = ynext[j] * f;
+                const double wv = n3 * erow[c] * enter + yn * d0 + n2 * d1 + n1 * d2 + zbg * a0 + c2 * a2 +
+                                  c1 * a1 + ldexp((double)o.suf[j], -eB);
+                row[j] = wv;
+                ycur[j] = eps * yn + wv;
+                z[j & 3] = b0 * zbg + wv;
+                part += (double)o.pre[j] * wv;
+                if (cell) cell[(size_t)i * L + j] = ldexp(W0[(size_t)i * L + j] * wv * invT, eF[i] + eB - Tf.e);
+                if (match && j + 3 < L)  /* X(i, j+3) W1[i+1][j+3]; row i+1 unscaled, offset eBn */
+                    match[(size_t)i * L + j + 3] =
+                        ldexp(enter * erow[c] * W0[(size_t)i * L + j] * below[j + 3] * invT, eF[i] + eBn - Tf.e);
+                n3 = n2;
+                n2 = n1;
+                n1 = below[j] * f;
+                c2 = c1;
+                c1 = wv;
+            }
+            if (match)
+                for (int j = 0; j < 3 && j < L; ++j) match[(size_t)i * L + j] = 0;
+            dx_add(&Tb, part, eB);
+            eBn = eB;
+            double *t = below;
+            below = row;
+            row = t;
+            t = ynext;
+            ynext = ycur;
+            ycur = t;
+        }
+#undef CODE
+        if (logT_fwd) *logT_fwd = Tf.m > 0 ? log(Tf.m) + Tf.e * 0.6931471805599453 : -INFINITY;
+        if (logT_bwd) *logT_bwd = Tb.m > 0 ? log(Tb.m) + Tb.e * 0.6931471805599453 : -INFINITY;
+        st = 0;
+    }
+    free(seeds);
+    free(W0);
+    free(Y0);
+    free(eF);
+    free(rows);
+    ftz_leave(csr);
+    return st;
+}

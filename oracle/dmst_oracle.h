@@ -64,6 +64,20 @@ int dmsto_filter_pair(const float *values, const float *params, const float *bg,
 int dmsto_backward_matrix(const float *values, const float *params, const float *bg, int M, const uint8_t *codes,
                           int L, dmsto_rates r, float *w1, int *counts);
 
+/* log T in FP64: T = sum over cells of prefixSeed * W1 (the total weight of
+ * all local alignments), the backward recurrence in double on double profile
+ * arrays (values (M+1) x 29, params (M+2) x 11), the reference's null model
+ * from the float background.  The finite-difference oracle of the gradient. */
+int dmsto_log_total(const double *values, const double *params, const float *bg, int M, const uint8_t *codes,
+                    int L, dmsto_rates r, double *logT);
+
+/* Posterior tables in FP64 ((M+1) x L each, row-major; either may be NULL):
+ * cell[i][j] = W0[i][j] W1[i][j] / T, match[i][j] = X(i,j) W1[i+1][j] / T
+ * (X the match term of the forward, dummest-dp-forward.hh:125-157), with
+ * log T from the forward total and from the backward total. */
+int dmsto_posteriors(const double *values, const double *params, const float *bg, int M, const uint8_t *codes,
+                     int L, dmsto_rates r, double *logT_fwd, double *logT_bwd, double *cell, double *match);
+
 /* Rescale counts of the last dmsto_score_pair call on this thread: sum over
  * rows of the backward and forward counts (0 when no row was rescaled). */
 void dmsto_last_rescales(int *backward, int *forward);

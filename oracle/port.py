@@ -52,6 +52,11 @@ def lib() -> C.CDLL:
         L.dmsto_filter_pair.argtypes = [F, F, F, C.c_int, U8, C.c_int, Rates, F]
         L.dmsto_backward_matrix.restype = C.c_int
         L.dmsto_backward_matrix.argtypes = [F, F, F, C.c_int, U8, C.c_int, Rates, F, C.POINTER(C.c_int)]
+        D = C.POINTER(C.c_double)
+        L.dmsto_log_total.restype = C.c_int
+        L.dmsto_log_total.argtypes = [D, D, F, C.c_int, U8, C.c_int, Rates, D]
+        L.dmsto_posteriors.restype = C.c_int
+        L.dmsto_posteriors.argtypes = [D, D, F, C.c_int, U8, C.c_int, Rates, D, D, D, D]
         L.dmsto_last_rescales.restype = None
         L.dmsto_last_rescales.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib = L
@@ -126,6 +131,41 @@ def backward_matrix(values, params, bg, codes, r: Rates | None = None):
     if st:
         raise ValueError("oracle backward_matrix rejected the pair")
     return W1, cnt
+
+
+def log_total(values, params, bg, codes, r: Rates | None = None) -> float:
+    """log T in FP64 (values (M+1) x 29 and params (M+2) x 11 as float64)."""
+    values = np.ascontiguousarray(values, np.float64)
+    params = np.ascontiguousarray(params, np.float64)
+    bg = np.ascontiguousarray(bg, np.float32)
+    codes = np.ascontiguousarray(codes, np.uint8)
+    out = C.c_double()
+    D = C.POINTER(C.c_double)
+    st = lib().dmsto_log_total(values.ctypes.data_as(D), params.ctypes.data_as(D), _f(bg), values.shape[0] - 1,
+                               codes.ctypes.data_as(C.POINTER(C.c_uint8)), len(codes), r or rates(),
+                               C.byref(out))
+    if st:
+        raise ValueError("oracle log_total rejected the pair")
+    return out.value
+
+
+def posteriors(values, params, bg, codes, r: Rates | None = None):
+    """(log T forward, log T backward, cell (M+1, L), match (M+1, L)) in FP64."""
+    values = np.ascontiguousarray(values, np.float64)
+    params = np.ascontiguousarray(params, np.float64)
+    bg = np.ascontiguousarray(bg, np.float32)
+    codes = np.ascontiguousarray(codes, np.uint8)
+    M, L = values.shape[0] - 1, len(codes)
+    cell = np.zeros((M + 1, L))
+    match = np.zeros((M + 1, L))
+    lf, lb = C.c_double(), C.c_double()
+    D = C.POINTER(C.c_double)
+    st = lib().dmsto_posteriors(values.ctypes.data_as(D), params.ctypes.data_as(D), _f(bg), M,
+                                codes.ctypes.data_as(C.POINTER(C.c_uint8)), L, r or rates(), C.byref(lf),
+                                C.byref(lb), cell.ctypes.data_as(D), match.ctypes.data_as(D))
+    if st:
+        raise ValueError("oracle posteriors rejected the pair")
+    return lf.value, lb.value, cell, match
 
 
 def score_ln(s) -> float:
