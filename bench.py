@@ -46,6 +46,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FLOPS_PER_CELL = 52  # 24 backward + 28 forward with the mid product
+AG_M, AG_READS = 400, 4096          # the differentiation workload
+AG_BYTES_PER_CELL = 48              # adjoint: (W0, Y0, Z0) written, (W0, Z0, Y0 of the row below) read, FP64
 METRIC = "fwd+bwd GCUPS (batched persistent kernel)"
 
 
@@ -62,9 +64,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
-    ap.add_argument("--workload", choices=["batched", "genome"], default="batched",
+    ap.add_argument("--workload", choices=["batched", "genome", "autograd"], default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
-                         "10 Mbp genome in 10 kb windows")
+                         "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
+                         "profile over 4096 implant reads (L 600-2400), one SGD step per step")
     ap.add_argument("--no-autotune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
     return ap.parse_args()
@@ -137,6 +140,14 @@ def aggregate(cells: float, ms: float, world: int) -> tuple[float, float, float]
 def workload_config(args, world: int) -> dict:
     """The workload both arms report (cells_per_step is added by the GPU arm,
     which counts them)."""
+    if args.workload == "autograd":
+        return {
+            "workload": f"log-likelihood + gradient (adjoint, FP64): 1 profile M={AG_M} x {AG_READS} "
+                        "reads L uniform 600-2400 nt, each carrying a frameshifted homolog, one SGD step of the "
+                        "emission/transition/frameshift logits per step",
+            "profiles": 1, "pairs_per_step": AG_READS, "l2": "inputs larger than L2 (forward store)",
+            "parallelism": f"replicas x{world} (reads sharded per rank)",
+        }
     if args.workload == "genome":
         return {
             "workload": "long-profile genome scan: 1 profile M=2000 x a 10 Mbp synthetic genome (GC 0.45, "
@@ -488,8 +499,139 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
+def autograd_problem(seed, rank):
+    """The profile, its starting logits and one rank's reads."""
+    from dummest_b200 import synth
+    rng = np.random.default_rng(seed)
+    prof = synth.make_profile(rng, AG_M, "grad400")
+    rrng = np.random.default_rng(rank_seed(seed, rank))
+    reads = synth.make_reads(rrng, AG_READS, 600, 2400, [prof], 1.0, gc_range=(0.4, 0.6), log_uniform=False)
+    return prof, reads
+
+
+def run_autograd(args, rank, world, local):
+    import torch
+    import dummest_b200 as d
+    from dummest_b200 import autograd as ag
+    from dummest_b200 import synth
+
+    prof, reads = autograd_problem(args.seed, rank)
+    txt = synth.hmmer3_text([prof])
+    _, values, params, bg = d.finalize_hmm(txt)
+    M = AG_M
+    ctx = d.Context(device=local)
+    sids = ctx.add_dna(reads)
+    cells = float(sum(len(r) for r in reads)) * (M + 1)
+    slot = ag.ProfileSlot(ctx, values, params, bg, sids)
+    bg_row = torch.tensor(values[-1, 4:29], dtype=torch.float64)
+    MI, MD, II, DD = synth.T_MI, synth.T_MD, synth.T_II, synth.T_DD
+    em = torch.tensor(np.log(prof.match), requires_grad=True)
+    tr = torch.tensor(np.tile(np.log([1 - MI - MD, MI, MD, 1 - II, II, 1 - DD, DD]), (M + 1, 1)),
+                      requires_grad=True)
+    fs = torch.tensor(np.log([0.0171, 0.0018, 0.0328, 0.0083]), requires_grad=True)
+    opt = torch.optim.SGD([em, tr, fs], lr=1e-3)
+
+    def step():
+        opt.zero_grad()
+        emit, par = ag.profile_params(em, tr, fs, bg_row)
+        loss = -ag.log_likelihood(emit, par, slot) / len(reads)
+        loss.backward()
+        opt.step()
+        return float(loss)
+
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    adj_ms = null_ms = 0.0
+    launches = 0
+    losses = []
+    for _ in range(args.steps):
+        losses.append(step())
+        t = ctx.last_timing()
+        adj_ms += t["dp_ms"]
+        null_ms += t["null_ms"]
+        launches += t["launches"]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    total_cells = cells * args.steps
+    value, ms_max, cells_all = aggregate(total_cells, ms, world)
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6451.2)
+    achieved = AG_BYTES_PER_CELL * total_cells / (adj_ms / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+        "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+        "kernel": "adjointKernel (forward store + backward with gradient sums), CUDA events on the library "
+                  "stream, summed over the step's launches",
+        "algorithmic_bytes_per_cell": AG_BYTES_PER_CELL,
+        "adjoint_gcups": total_cells / (adj_ms / 1e3) / 1e9,
+    }
+    # e2e: the reads re-uploaded from host memory (2-bit packed) every step
+    words, mask, lens = d.pack_dna(reads)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        ctx.clear_sequences()
+        slot.seq_ids = ctx.add_packed(words, lens, mask)
+        step()
+        # packed reads + mask + offsets, the per-pair descriptors and jobs, the
+        # profile tables; back: log T per read and the gradient
+        h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 72 * len(lens) + 4 * (29 * (M + 1) + 11 * (M + 2))
+        d2h += 8 * len(lens) + 8 * (11 * (M + 2) + 25 * (M + 1))
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
+           "d2h_bytes_per_step": d2h // args.steps}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import port
+        v64, p64 = values.astype(np.float64), params.astype(np.float64)
+        done_c, done_s, n = 0.0, 0.0, 0
+        for r in reads:
+            c = d.decode_dna(r)
+            t = time.perf_counter()
+            port.log_total(v64, p64, bg, c)
+            done_s += time.perf_counter() - t
+            done_c += (M + 1) * len(c)
+            n += 1
+            if done_s >= args.cpu_seconds:
+                break
+        cb = {"value": done_c / done_s / 1e9, "unit": "GCUPS", "cores": 1, "kind": "port",
+              "sample": f"{n} reads of the step, {done_c:.3e} cells in {done_s:.1f} s: the oracle's FP64 log T "
+                        "(one backward sweep, no gradient: the reference computes none), one core"}
+    if rank == 0:
+        line = {
+            "metric": "log-likelihood + gradient GCUPS (adjoint, FP64)", "value": value, "unit": "GCUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_config(args, world), cells_per_step=cells), "e2e": e2e, "roofline": roofline,
+            "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk,
+            "breakdown_ms_per_step": {"null_ms": null_ms / args.steps, "adjoint_ms": adj_ms / args.steps},
+            "loss_first_last": [losses[0], losses[-1]],
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.impl == "reference" and args.workload == "autograd":
+        rank, _, _ = dist_env()
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference computes no gradient of its "
+                              "likelihood (its search path scores only)"}), flush=True)
+        return
     if args.impl == "reference":
         # The reference's CPU engine runs on rank 0 alone; it needs no process
         # group, and the other ranks exit without work.
@@ -501,6 +643,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "autograd":
+            run_autograd(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -1289,8 +1289,12 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
             return ctx->fail(DMST_EINVAL, "%s: pair %zu is for another profile (one profile per call)", what, i);
     // Pair descriptors, null models and seeds on the device, sorted longest
     // read first.
+    const auto wallT0 = std::chrono::steady_clock::now();
     int st = dmst_score_pairs(ctx, pairs, n, DMST_MODE_MID | kModeNullOnly, nullptr);
     if (st) return st;
+    const double nullMs = elapsedMs(ctx, ctx->ev[0], ctx->ev[1]);
+    double adjMs = 0.0;
+    int launches = 1;
     const std::vector<int> order = ctx->lastOrder;
     const int M = ctx->profiles[prof].M;
     // Posterior offsets in the caller's order.
@@ -1303,18 +1307,13 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
         }
     }
     std::vector<AdjointJob> jobs(n);
-    std::vector<long long> warpF, warpB, warpP;
-    for (size_t w0 = 0; w0 < n; w0 += 32) {
-        const int Lw = ctx->seqLen[pairs[order[w0]].seq];  // longest of the warp
-        long long pNeed = 0;
-        for (size_t k = w0; k < std::min(n, w0 + 32); ++k) {
-            const long long pk = post ? 2LL * (M + 1) * ctx->seqLen[pairs[order[k]].seq] : 0;
-            jobs[k] = AdjointJob{(int)k, Lw, 0, 0, post ? pNeed : -1};
-            pNeed += pk;
-        }
-        warpF.push_back(adjStoreDoubles(M, Lw));
-        warpB.push_back(adjRowDoubles(Lw));
-        warpP.push_back(pNeed);
+    std::vector<long long> needF(n), needB(n), needP(n);
+    for (size_t k = 0; k < n; ++k) {
+        const int L = ctx->seqLen[pairs[order[k]].seq];
+        jobs[k] = AdjointJob{(int)k, 0, 0, 0, post ? 0 : -1};
+        needF[k] = adjStoreDoubles(M, L);
+        needB[k] = adjBoundDoubles(L);
+        needP[k] = post ? 2LL * (M + 1) * L : 0;
     }
     const size_t gN = (size_t)(M + 2) * kParamFloats + (size_t)(M + 1) * kNumCodes;
     CK(cudaSetDevice(ctx->device), "set device");
@@ -1322,29 +1321,23 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     CK(ctx->dLogT.ensure(n), "alloc log T");
     CK(ctx->dAdjJobs.ensure(n), "alloc adjoint jobs");
     CK(cudaMemsetAsync(ctx->dGrad.p, 0, gN * sizeof(double), ctx->stream), "zero gradient");
-    // Batches of whole warps under the device budget (the forward store is
-    // 24 bytes per cell, the posterior tables 16).
+    // Batches of pairs under the device budget (the forward store is 24
+    // bytes per cell, the posterior tables 16).
     size_t freeB = 0, totalB = 0;
     CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
     const size_t budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : freeB / 2;
-    const size_t nWarps = warpF.size();
-    for (size_t w = 0; w < nWarps;) {
-        size_t w1 = w;
+    for (size_t k0 = 0; k0 < n;) {
+        size_t k1 = k0;
         long long f = 0, b = 0, pp = 0;
-        while (w1 < nWarps &&
-               (w1 == w || (size_t)(f + warpF[w1] + b + warpB[w1] + pp + warpP[w1]) * 8 <= budget)) {
-            // offsets of this warp's buffers inside the batch
-            for (size_t k = w1 * 32; k < std::min(n, w1 * 32 + 32); ++k) {
-                jobs[k].fOff = f;
-                jobs[k].bOff = b;
-                if (post) jobs[k].pOff += pp;
-            }
-            f += warpF[w1];
-            b += warpB[w1];
-            pp += warpP[w1];
-            ++w1;
+        while (k1 < n && (k1 == k0 || (size_t)(f + needF[k1] + b + needB[k1] + pp + needP[k1]) * 8 <= budget)) {
+            jobs[k1].fOff = f;
+            jobs[k1].bOff = b;
+            if (post) jobs[k1].pOff = pp;
+            f += needF[k1];
+            b += needB[k1];
+            pp += needP[k1];
+            ++k1;
         }
-        const size_t k0 = w * 32, k1 = std::min(n, w1 * 32);
         const int nj = (int)(k1 - k0);
         CK(ctx->dAdjF.ensure((size_t)f), "alloc adjoint store");
         CK(ctx->dAdjB.ensure((size_t)b), "alloc adjoint rows");
@@ -1352,22 +1345,31 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
         CK(cudaMemcpyAsync(ctx->dAdjJobs.p, jobs.data() + k0, nj * sizeof(AdjointJob), cudaMemcpyHostToDevice,
                            ctx->stream),
            "upload adjoint jobs");
-        const int blocks = (nj + 127) / 128;
-        adjointKernel<<<blocks, 128, 0, ctx->stream>>>(
+        const int blocks = (nj + kAdjWarps - 1) / kAdjWarps;
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        adjointKernel<<<blocks, kAdjWarps * 32, 0, ctx->stream>>>(
             ctx->dAdjJobs.p, nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
             ctx->dSeeds.p, ctx->dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
             post ? ctx->dPost.p : nullptr);
         CK(cudaGetLastError(), "adjoint kernel");
+        CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
+        ++launches;
         if (post)
-            for (size_t k = k0; k < k1; ++k) {
-                const size_t cnt = 2 * (size_t)(M + 1) * ctx->seqLen[pairs[order[k]].seq];
-                CK(cudaMemcpyAsync(post + postOff[order[k]], ctx->dPost.p + jobs[k].pOff, cnt * sizeof(double),
-                                   cudaMemcpyDeviceToHost, ctx->stream),
+            for (size_t k = k0; k < k1; ++k)
+                CK(cudaMemcpyAsync(post + postOff[order[k]], ctx->dPost.p + jobs[k].pOff,
+                                   (size_t)needP[k] * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
                    "download posterior tables");
-            }
         CK(cudaStreamSynchronize(ctx->stream), "adjoint kernel");
-        w = w1;
+        adjMs += elapsedMs(ctx, ctx->ev[3], ctx->ev[4]);
+        k0 = k1;
     }
+    // Timing of the call: [1] null model, [2] adjoint kernels, [0] both.
+    ctx->lastNullMs = nullMs;
+    ctx->lastDpMs = adjMs;
+    ctx->lastExactMs = 0;
+    ctx->lastTotalMs = nullMs + adjMs;
+    ctx->lastLaunches = launches;
+    ctx->lastWallMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wallT0).count();
     std::vector<double> g(gN), lt(n);
     CK(cudaMemcpy(g.data(), ctx->dGrad.p, gN * sizeof(double), cudaMemcpyDeviceToHost), "download gradient");
     CK(cudaMemcpy(lt.data(), ctx->dLogT.p, n * sizeof(double), cudaMemcpyDeviceToHost), "download log T");
