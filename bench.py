@@ -46,7 +46,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FLOPS_PER_CELL = 52  # 24 backward + 28 forward with the mid product
-AG_M, AG_READS = 400, 4096          # the differentiation workload
 AG_BYTES_PER_CELL = 48              # adjoint: (W0, Y0, Z0) written, (W0, Z0, Y0 of the row below) read, FP64
 METRIC = "fwd+bwd GCUPS (batched persistent kernel)"
 
@@ -68,6 +67,10 @@ def parse():
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
                          "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
                          "profile over 4096 implant reads (L 600-2400), one SGD step per step")
+    ap.add_argument("--ag-reads", type=int, default=4096, help="autograd workload: reads per rank")
+    ap.add_argument("--ag-m", type=int, default=400, help="autograd workload: profile length")
+    ap.add_argument("--ag-lmin", type=int, default=600, help="autograd workload: shortest read")
+    ap.add_argument("--ag-lmax", type=int, default=2400, help="autograd workload: longest read")
     ap.add_argument("--no-autotune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
     return ap.parse_args()
@@ -142,10 +145,10 @@ def workload_config(args, world: int) -> dict:
     which counts them)."""
     if args.workload == "autograd":
         return {
-            "workload": f"log-likelihood + gradient (adjoint, FP64): 1 profile M={AG_M} x {AG_READS} "
-                        "reads L uniform 600-2400 nt, each carrying a frameshifted homolog, one SGD step of the "
-                        "emission/transition/frameshift logits per step",
-            "profiles": 1, "pairs_per_step": AG_READS, "l2": "inputs larger than L2 (forward store)",
+            "workload": f"log-likelihood + gradient (adjoint, FP64): 1 profile M={args.ag_m} x {args.ag_reads} "
+                        f"reads L uniform {args.ag_lmin}-{args.ag_lmax} nt, each carrying a frameshifted homolog, "
+                        "one SGD step of the emission/transition/frameshift logits per step",
+            "profiles": 1, "pairs_per_step": args.ag_reads, "l2": "inputs larger than L2 (forward store)",
             "parallelism": f"replicas x{world} (reads sharded per rank)",
         }
     if args.workload == "genome":
@@ -499,13 +502,14 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
-def autograd_problem(seed, rank):
-    """The profile, its starting logits and one rank's reads."""
+def autograd_problem(args, rank):
+    """The profile and one rank's reads."""
     from dummest_b200 import synth
-    rng = np.random.default_rng(seed)
-    prof = synth.make_profile(rng, AG_M, "grad400")
-    rrng = np.random.default_rng(rank_seed(seed, rank))
-    reads = synth.make_reads(rrng, AG_READS, 600, 2400, [prof], 1.0, gc_range=(0.4, 0.6), log_uniform=False)
+    rng = np.random.default_rng(args.seed)
+    prof = synth.make_profile(rng, args.ag_m, f"grad{args.ag_m}")
+    rrng = np.random.default_rng(rank_seed(args.seed, rank))
+    reads = synth.make_reads(rrng, args.ag_reads, args.ag_lmin, args.ag_lmax, [prof], 1.0, gc_range=(0.4, 0.6),
+                             log_uniform=False)
     return prof, reads
 
 
@@ -515,10 +519,10 @@ def run_autograd(args, rank, world, local):
     from dummest_b200 import autograd as ag
     from dummest_b200 import synth
 
-    prof, reads = autograd_problem(args.seed, rank)
+    prof, reads = autograd_problem(args, rank)
     txt = synth.hmmer3_text([prof])
     _, values, params, bg = d.finalize_hmm(txt)
-    M = AG_M
+    M = args.ag_m
     ctx = d.Context(device=local)
     sids = ctx.add_dna(reads)
     cells = float(sum(len(r) for r in reads)) * (M + 1)
@@ -537,7 +541,7 @@ def run_autograd(args, rank, world, local):
         loss = -ag.log_likelihood(emit, par, slot) / len(reads)
         loss.backward()
         opt.step()
-        return float(loss)
+        return float(loss.detach())
 
     stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
     for _ in range(args.warmup):

@@ -1311,7 +1311,7 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     for (size_t k = 0; k < n; ++k) {
         const int L = ctx->seqLen[pairs[order[k]].seq];
         jobs[k] = AdjointJob{(int)k, 0, 0, 0, post ? 0 : -1};
-        needF[k] = adjStoreDoubles(M, L);
+        needF[k] = (adjStoreDoubles(M, L) + 31) & ~31LL;  // 256-byte aligned stores (cp.async)
         needB[k] = adjBoundDoubles(L);
         needP[k] = post ? 2LL * (M + 1) * L : 0;
     }
@@ -1346,8 +1346,10 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
                            ctx->stream),
            "upload adjoint jobs");
         const int blocks = (nj + kAdjWarps - 1) / kAdjWarps;
+        auto kern = post ? adjointKernel<true> : adjointKernel<false>;
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjSmem), "smem attribute");
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
-        adjointKernel<<<blocks, kAdjWarps * 32, 0, ctx->stream>>>(
+        kern<<<blocks, kAdjWarps * 32, kAdjSmem, ctx->stream>>>(
             ctx->dAdjJobs.p, nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
             ctx->dSeeds.p, ctx->dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
             post ? ctx->dPost.p : nullptr);

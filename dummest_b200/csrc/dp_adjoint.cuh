@@ -104,16 +104,43 @@ __device__ __forceinline__ double warpSumD(double v) {
     return v;
 }
 
+// Shared memory of a warp: the backward's ring of forward blocks (one block =
+// one forward step of a stripe: 32 lanes x (W0, Y0, Z0), plus the Y0 of the
+// row below the stripe that the block's step needs), then the per-lane
+// emission sums of the stripe.
+constexpr int kAdjRing = 8;          // slots (a power of two)
+constexpr int kAdjAhead = 6;         // blocks copied ahead of use
+constexpr int kAdjSlot = 32 * 3 + 2; // doubles per slot (16-byte multiple)
+constexpr size_t kAdjSmemWarp = (size_t)(kAdjRing * kAdjSlot + kNumCodes * 32) * sizeof(double);
+constexpr size_t kAdjSmem = kAdjWarps * kAdjSmemWarp;
+
+__device__ __forceinline__ void adjCp16(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void adjCp8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void adjCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void adjWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // grad: (M+2) x 11 Params gradients then (M+1) x 25 emission gradients of
 // the profile, accumulated over the pairs (each term already divided by the
-// pair's T).  logT: per job, natural log.  post: posterior tables (jobs with
-// pOff >= 0).
-__global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
+// pair's T).  logT: per job, natural log.  post: posterior tables (POST).
+// The forward store must start 16-byte aligned (the host pads each pair's).
+template <bool POST>
+__global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
     const AdjointJob *jobs, int nJobs, const DevPair *pairs, const DevProfile *profiles, const float *emit,
     const float *params, const uint8_t *codes, const float *seeds, const PairScales *scales, double *fstore,
     double *bstore, double *grad, double *logT, double *post) {
-    __shared__ double geS[kAdjWarps][kNumCodes][32];  // per-lane emission sums of the stripe
+    extern __shared__ __align__(16) double adjSmem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *ring = adjSmem + (size_t)warp * (kAdjSmemWarp / sizeof(double));
+    double *geS = ring + kAdjRing * kAdjSlot;  // [25][32]
     const int ji = blockIdx.x * kAdjWarps + warp;
     if (ji >= nJobs) return;  // whole warps only
     const AdjointJob job = jobs[ji];
@@ -130,11 +157,9 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
     double *F = fstore + job.fOff;
     double *Foff = F + (size_t)nS * (L + 31) * 32 * 3;  // per-stripe offsets
     double *Bnd = bstore + job.bOff;
-    double *cellP = job.pOff >= 0 ? post + job.pOff : nullptr;
-    double *matchP = cellP ? cellP + (size_t)(M + 1) * L : nullptr;
+    double *cellP = POST ? post + job.pOff : nullptr;
+    double *matchP = POST ? cellP + (size_t)(M + 1) * L : nullptr;
     auto code = [&](int j) -> int { return (j >= 0 && j < L) ? (int)cd[j] : kPad; };
-    auto bgc = [&](int j) -> double { return (double)pr.bg[code(j)]; };
-    auto e = [&](int i, int c) -> double { return (double)E[(size_t)c * rowPad + i]; };
     auto bnd = [&](int par2, int t, int j) -> double * { return Bnd + ((size_t)(par2 * 2 + t) * (L + 4) + j); };
     const int nSteps = L + 31;
 
@@ -156,44 +181,54 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
         const double d0 = q[6], eps = q[9];
         const double pEnter = ir > 0 ? (double)qp[10] * sC : 0.0, pd1 = ir > 0 ? (double)qp[7] * s2 : 0.0;
         const double pd2 = ir > 0 ? (double)qp[8] * s1 : 0.0;
+        const float *Eprev = E + (ir > 0 ? ir - 1 : 0);
         double w1 = 0, w2 = 0, w3 = 0, z1 = 0, z2 = 0, z3 = 0;  // own row at j-1, j-2, j-3
         double u1 = 0, u2 = 0, u3 = 0;                          // row i-1's W0 at j-1, j-2, j-3
         double pubW = 0, pubY = 0;                              // published at the previous step
         double part = 0.0, rowMax = 0.0;
-        double bW = 0, bY = 0;  // lane group's block of the boundary row (row 32s-1)
+        // lane c holds column 32b + c of row 32s-1 for the current block b
+        // (cW, cY) and the next one (nW, nY)
+        auto fetch = [&](int b, double &W, double &Y) {
+            const int jc = 32 * b + lane;
+            W = Y = 0.0;
+            if (s > 0 && jc < L) {
+                const size_t a = adjF(L, s - 1, jc + 31, 31);
+                W = F[a] * f;
+                Y = F[a + 1] * f;
+            }
+        };
+        double cW, cY, nW, nY;
+        fetch(0, nW, nY);
         for (int k = 0; k < nSteps; ++k) {
             const int j = k - lane;
-            // the row below: lane l-1's values of the previous step; lane 0
-            // reads row 32s-1 (lane 31 of the previous stripe, step j + 31)
-            if ((k & 31) == 0) {  // lane c of the warp fetches column k + c of row 32s-1
-                const int jc = k + lane;
-                bW = bY = 0.0;
-                if (s > 0 && jc < L) {
-                    const size_t a = adjF(L, s - 1, jc + 31, 31);
-                    bW = F[a] * f;
-                    bY = F[a + 1] * f;
-                }
+            if ((k & 31) == 0) {
+                cW = nW;
+                cY = nY;
+                fetch((k >> 5) + 1, nW, nY);
             }
+            // the row below: lane l-1's values of the previous step; lane 0
+            // takes row 32s-1 at column k
             double uj = __shfl_up_sync(0xffffffffu, pubW, 1);
             double yPrev = __shfl_up_sync(0xffffffffu, pubY, 1);
-            const double cW = __shfl_sync(0xffffffffu, bW, k & 31);
-            const double cY = __shfl_sync(0xffffffffu, bY, k & 31);
+            const double bw = __shfl_sync(0xffffffffu, cW, k & 31);
+            const double by = __shfl_sync(0xffffffffu, cY, k & 31);
             if (lane == 0) {
-                uj = cW;
-                yPrev = cY;
+                uj = bw;
+                yPrev = by;
             }
             double W0 = 0.0, Y0 = 0.0, Z0 = 0.0;
             if (rowOK && j >= 0 && j < L) {
                 const int c = code(j - 2);
-                const double win = pEnter * (ir > 0 ? e(ir - 1, c) : 0.0) * u3 + yPrev + pd1 * u2 + pd2 * u1;
-                Z0 = bgc(j - 2) * sC * (a0 * w3 + b0 * z3);
-                W0 = win + Z0 + a1 * w1 + a2 * w2 + (double)pre[j] * seedScale;
-                Y0 = d0 * W0 + eps * yPrev;
+                const double win = fma(pEnter * (double)Eprev[(size_t)c * rowPad], u3,
+                                       fma(pd1, u2, fma(pd2, u1, yPrev)));
+                Z0 = ((double)pr.bg[c] * sC) * fma(a0, w3, b0 * z3);
+                W0 = fma(a1, w1, fma(a2, w2, fma((double)pre[j], seedScale, win + Z0)));
+                Y0 = fma(d0, W0, eps * yPrev);
                 const size_t a = adjF(L, s, k, lane);
                 F[a] = W0;
                 F[a + 1] = Y0;
                 F[a + 2] = Z0;
-                part += W0 * (double)suf[j];
+                part = fma(W0, (double)suf[j], part);
                 rowMax = fmax(rowMax, fmax(W0, Y0));
             }
             w3 = w2; w2 = w1; w1 = W0;
@@ -234,68 +269,100 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
         const double enter = (double)q[10] * sC, d0 = q[6], d1 = (double)q[7] * s2, d2 = (double)q[8] * s1;
         const double a0 = (double)q[0] * sC, a1 = (double)q[1] * s1, a2 = (double)q[2] * s2;
         const double b0 = (double)q[3] * sC, eps = q[9], q10 = q[10];
+        const float *Erow = E + ir;
         const int rd = (s + 1) & 1, wr = s & 1;  // boundary parity read (row 32s+32) and written (row 32s)
         double gEnter = 0, gD0 = 0, gD1 = 0, gD2 = 0, gA0 = 0, gA1 = 0, gA2 = 0, gEps = 0, gB0 = 0;
 #pragma unroll
-        for (int c = 0; c < kNumCodes; ++c) geS[warp][c][lane] = 0.0;
+        for (int c = 0; c < kNumCodes; ++c) geS[c * 32 + lane] = 0.0;
+        // Forward blocks of this stripe into the ring: the block of forward
+        // step t holds every lane's (W0, Y0, Z0) of that step, and (lane 0's
+        // copy) the Y0 of row 32s-1 at forward step t + 31 of stripe s-1.
+        const bool below = s > 0;
+        auto issue = [&](int t) {
+            if (t >= 0 && t <= L + 30) {
+                double *dst = ring + (t & (kAdjRing - 1)) * kAdjSlot;
+                const double *src = F + adjF(L, s, t, 0);
+                adjCp16(dst + 2 * lane, src + 2 * lane);
+                if (lane < 16) adjCp16(dst + 64 + 2 * lane, src + 64 + 2 * lane);
+                if (lane == 16 && below && t + 31 <= L + 30) adjCp8(dst + 96, F + adjF(L, s - 1, t + 31, 31) + 1);
+            }
+            adjCommit();
+        };
+        const int t0 = L + 30;  // the forward step of backward step 0
+#pragma unroll
+        for (int d = 0; d < kAdjAhead; ++d) issue(t0 - d);
         double n1 = 0, n2 = 0, n3 = 0;     // row i+1 at j+1, j+2, j+3
         double c1 = 0, c2 = 0;             // own row at j+1, j+2
         double zz1 = 0, zz2 = 0, zz3 = 0;  // own Z at j+1, j+2, j+3
         double pubW = 0, pubY = 0;
         double rowMax = 0.0;
-        double bW = 0, bY = 0;
+        // lane c holds column L-1-(32b+c) of row 32s+32 for the current block
+        // b (cW, cY) and the next one (nW, nY)
+        auto fetch = [&](int b, double &W, double &Y) {
+            const int jc = L - 1 - (32 * b + lane);
+            W = Y = 0.0;
+            if (jc >= 0) {
+                W = *bnd(rd, 0, jc) * f;
+                Y = *bnd(rd, 1, jc) * f;
+            }
+        };
+        double cW, cY, nW, nY;
+        fetch(0, nW, nY);
         for (int k = 0; k < nSteps; ++k) {
             const int j = L - 1 - (k - lane);
-            if ((k & 31) == 0) {  // lane c fetches column L-1-(k+c) of row 32s+32
-                const int jc = L - 1 - (k + lane);
-                bW = bY = 0.0;
-                if (jc >= 0) {
-                    bW = *bnd(rd, 0, jc) * f;
-                    bY = *bnd(rd, 1, jc) * f;
-                }
+            const int t = t0 - k;
+            issue(t - kAdjAhead);
+            if ((k & 31) == 0) {
+                cW = nW;
+                cY = nY;
+                fetch((k >> 5) + 1, nW, nY);
             }
             double nj = __shfl_up_sync(0xffffffffu, pubW, 1);
             double ynj = __shfl_up_sync(0xffffffffu, pubY, 1);
-            const double cW = __shfl_sync(0xffffffffu, bW, k & 31);
-            const double cY = __shfl_sync(0xffffffffu, bY, k & 31);
+            const double bw = __shfl_sync(0xffffffffu, cW, k & 31);
+            const double by = __shfl_sync(0xffffffffu, cY, k & 31);
             if (lane == 0) {
-                nj = cW;
-                ynj = cY;
+                nj = bw;
+                ynj = by;
             }
+            adjWait<kAdjAhead - 1>();  // blocks t and t-1 are in
+            __syncwarp();
             double W = 0.0, Y = 0.0, Z = 0.0;
             if (rowOK && j >= 0 && j < L) {
                 const int c = code(j + 1);
-                const double ec = e(ir, c), bg1 = bgc(j + 1);
-                const double zbg = zz3 * bg1;
-                W = n3 * ec * enter + ynj * d0 + n2 * d1 + n1 * d2 + zbg * a0 + c2 * a2 + c1 * a1 +
-                    (double)suf[j] * seedScale;
-                Y = eps * ynj + W;
-                Z = b0 * zbg + W;
+                const double ec = (double)Erow[(size_t)c * rowPad];
+                const double zbg = zz3 * (double)pr.bg[c];
+                W = fma(n3 * ec, enter,
+                        fma(ynj, d0, fma(n2, d1, fma(n1, d2, fma(zbg, a0, fma(c2, a2, fma(c1, a1,
+                            (double)suf[j] * seedScale)))))));
+                Y = fma(eps, ynj, W);
+                Z = fma(b0, zbg, W);
                 rowMax = fmax(rowMax, Y);  // Y >= W
                 if (lane == 31) {          // row 32s: the boundary for the stripe below
                     *bnd(wr, 0, j) = W;
                     *bnd(wr, 1, j) = Y;
                 }
-                // forward values of the cell: stripe s, forward step L+30-k, lane 31-lane
-                const size_t a = adjF(L, s, L + 30 - k, 31 - lane);
-                const double wA = F[a], zA = F[a + 2];
+                // forward values of the cell: block t, lane 31-lane; Y0 of the
+                // row below: block t-1, lane 30-lane (row 32s-1: block t's extra)
+                const double *bt = ring + (t & (kAdjRing - 1)) * kAdjSlot;
+                const double wA = bt[3 * (31 - lane)], zA = bt[3 * (31 - lane) + 2];
                 double yA = 0.0;
                 if (lane < 31)
-                    yA = F[adjF(L, s, L + 29 - k, 30 - lane) + 1];
-                else if (s > 0)  // row 32s-1: lane 31 of stripe s-1, forward step j + 31
-                    yA = F[adjF(L, s - 1, L + 61 - k, 31) + 1];
+                    yA = ring[((t - 1) & (kAdjRing - 1)) * kAdjSlot + 3 * (30 - lane) + 1];
+                else if (below)
+                    yA = bt[96];
                 const double me = wA * n3 * sC;  // d/d(enter * e) without the other factor
-                gEnter += me * ec;
-                geS[warp][c][lane] += me * q10;
-                gD0 += wA * ynj;
-                gD1 += wA * n2 * s2;
-                gD2 += wA * n1 * s1;
-                gA0 += wA * zbg * sC;
-                gA1 += wA * c1 * s1;
-                gA2 += wA * c2 * s2;
-                gEps += yA * ynj;
-                gB0 += zA * zbg * sC;
-                if (cellP) {
+                gEnter = fma(me, ec, gEnter);
+                geS[c * 32 + lane] = fma(me, q10, geS[c * 32 + lane]);
+                gD0 = fma(wA, ynj, gD0);
+                gD1 = fma(wA, n2, gD1);
+                gD2 = fma(wA, n1, gD2);
+                gA0 = fma(wA, zbg, gA0);
+                gA1 = fma(wA, c1, gA1);
+                gA2 = fma(wA, c2, gA2);
+                gEps = fma(yA, ynj, gEps);
+                gB0 = fma(zA, zbg, gB0);
+                if (POST) {
                     cellP[(size_t)i * L + j] = ldexp(wA * W * invT, rowExp);
                     if (j + 3 < L) matchP[(size_t)i * L + j + 3] = ldexp(me * ec * q10 * invT, rowExp);
                     if (j < 3) matchP[(size_t)i * L + j] = 0.0;
@@ -307,17 +374,19 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
             pubW = W;
             pubY = Y;
         }
+        adjWait<0>();  // no copy outlives the stripe (the ring is reused)
         if (lane == 31)  // columns L..L+3 of the boundary row stay zero
             for (int j = L; j < L + 4; ++j) {
                 *bnd(wr, 0, j) = 0.0;
                 *bnd(wr, 1, j) = 0.0;
             }
         lastMaxB = rowMax;
-        __syncwarp();  // the boundary row before the next stripe reads it; geS complete
+        __syncwarp();  // the boundary row before the next stripe reads it; ring and geS complete
         // d log T = dT / T: each lane adds its row's sums times 2^(offsets) / T
+        // (the per-base scale of each coefficient applied here, once per row)
         if (rowOK) {
             double *g = gP + (size_t)i * kParamFloats;
-            const double v[9] = {gA0, gA1, gA2, gB0, gD0, gD1, gD2, gEps, gEnter};
+            const double v[9] = {gA0 * sC, gA1 * s1, gA2 * s2, gB0 * sC, gD0, gD1 * s2, gD2 * s1, gEps, gEnter};
             const int slot[9] = {0, 1, 2, 3, 6, 7, 8, 9, 10};
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
@@ -326,7 +395,7 @@ __global__ void __launch_bounds__(kAdjWarps * 32) adjointKernel(
             }
             double *gr = gE + (size_t)i * kNumCodes;
             for (int cc = 0; cc < kNumCodes; ++cc) {
-                const double x = ldexp(geS[warp][cc][lane] * invT, rowExp);
+                const double x = ldexp(geS[cc * 32 + lane] * invT, rowExp);
                 if (x != 0.0) atomicAdd(gr + cc, x);
             }
         }
