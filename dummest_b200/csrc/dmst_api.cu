@@ -937,7 +937,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
     const size_t nCounters = allChunks.size() + 3;
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
-    const size_t smem = (size_t)kNumCodes * ctx->maxRowPad * sizeof(float);
 
     // Null-model jobs: up to 32 pairs of one read per warp.
     std::vector<int> jobPairs(n);
@@ -1118,9 +1117,9 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         const size_t budget = std::max<size_t>(free / 2, (size_t)256 << 20);
         eo.resize(flagged.size());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        const size_t pipeSmem = kPipeWarps * sizeof(Window);
         if (!sequentialExact)
-            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(smem + sizeof(Window))),
+            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipeSmem),
                "smem attribute");
         size_t i0 = 0;
         while (i0 < flagged.size()) {
@@ -1130,13 +1129,16 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             size_t i1 = i0;
             while (i1 < flagged.size()) {
                 const DevPair &d = dp[flagged[i1]];
-                long long need = sequentialExact ? exactScratchFloats(d.M, d.L) : exactWaveScratch(d.M, d.L);
+                // warps per pair: one per stripe, at most kPipeWarps
+                const int nS = (d.M + 1 + kLanes * kExactR - 1) / (kLanes * kExactR);
+                const int W = std::min(nS, kPipeWarps);
+                long long need = sequentialExact ? exactScratchFloats(d.M, d.L) : exactWaveScratch(d.M, d.L, W);
                 need = (need + 63) / 64 * 64;
                 if (i1 > i0 && (size_t)(used + need) * 4 > budget) break;
                 if (sequentialExact)
                     jobs.push_back(ExactJob{flagged[i1], used});
                 else
-                    wjobs.push_back(ExactWaveJob{flagged[i1], 0, used});
+                    wjobs.push_back(ExactWaveJob{flagged[i1], W, used});
                 used += need;
                 ++i1;
             }
@@ -1157,11 +1159,11 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                 CK(cudaMemcpyAsync(ctx->dWaveJobs.p, wjobs.data(), nj * sizeof(ExactWaveJob),
                                    cudaMemcpyHostToDevice, ctx->stream),
                    "upload jobs");
-                const int blocks = (int)std::min<size_t>(nj, (size_t)ctx->smCount * 16);
-                exactWaveKernel<<<blocks, kLanes, smem + sizeof(Window), ctx->stream>>>(
+                // one CTA per SM (255 registers x 256 threads), persistent over the jobs
+                const int blocks = (int)std::min<size_t>(nj, (size_t)ctx->smCount);
+                exactWaveKernel<<<blocks, kPipeWarps * kLanes, pipeSmem, ctx->stream>>>(
                     ctx->dWaveJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p,
-                    kNumCodes * ctx->maxRowPad);
+                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
             }
             CK(cudaGetLastError(), "exact kernel");
             ++launches;
@@ -1174,6 +1176,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
         CK(cudaEventSynchronize(ctx->ev[4]), "event");
         exactMs = elapsedMs(ctx, ctx->ev[3], ctx->ev[4]);
+        for (size_t f = 0; f < eo.size(); ++f)
+            if (eo[f].failed)
+                return ctx->fail(DMST_ETIMEOUT, "exact path: the stripe pipeline of pair %d gave up a wait",
+                                 order[flagged[f]]);
     }
     ctx->lastExactMs = exactMs;
     ctx->lastExactPairs = (int)flagged.size();

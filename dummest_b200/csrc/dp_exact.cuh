@@ -56,6 +56,8 @@ struct ExactJob {
 struct ExactOut {
     XS mid;
     XS filt;
+    int failed;  // the pipelined kernel gave up a wait (the scores are not valid)
+    int pad;
 };
 
 // Scratch per job (floats): W1 (M+2) x (L+4), then four rows of L+4
@@ -227,6 +229,7 @@ __global__ void exactKernel(const ExactJob *jobs, int n, const DevPair *pairs, c
     }
     out[ji].mid = best;
     out[ji].filt = bestFilt;
+    out[ji].failed = 0;
 }
 
 }  // namespace dmst

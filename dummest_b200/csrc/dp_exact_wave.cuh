@@ -1,6 +1,7 @@
-// Exact row-rescaled DP on the wavefront, one warp per pair, for the pairs
-// the fast kernel cannot score exactly (a row maximum above RESCALE_THRESH,
-// or a product beyond float range).
+// Exact row-rescaled DP on the wavefront, for the pairs the fast kernel
+// cannot score exactly (a row maximum above RESCALE_THRESH, or a product
+// beyond float range).  One CTA per pair; its warps split the pair's stripes
+// (below).
 //
 // The reference decides each row's rescale after the whole row is known
 // (dummest-dp-backward.hh:560-573, dummest-dp-forward.hh:228-242), which a
@@ -23,6 +24,22 @@
 // forms them in double and rounds the mantissa to float,
 // dummest-batch.hh:146-235) and folded with the row's count sum into an
 // exact (mantissa, exponent) best.
+//
+// Stripe pipeline.  A pair's stripes (32 R rows each) are dealt round-robin
+// to the CTA's W warps: warp w runs stripes w, w + W, ... in processing order
+// (top-down in the backward, bottom-up in the forward).  The rows crossing
+// from stripe sp to sp+1 go through ring (sp mod 2W) in global memory.  Every
+// warp publishes, in shared memory, how far its ring-writing lane has got
+// (the position sp P' + column of the next column it computes), and before
+// each refill of its staging window a warp waits until the stripe before
+// each stripe it stages has written the ring columns the refill reads, and
+// until the ring slot it is about to overwrite has been read.  Every wait is
+// on a stripe earlier in processing order, and the stripe period P' = P + 128
+// is long enough that a warp's window never reaches its next stripe before
+// its current stripe's columns are all computed and published, so the waits
+// cannot form a cycle.  Every wait is bounded: past the limit it sets the
+// CTA's abort flag, all warps leave their sweeps at the next block, and the
+// pair's result is marked failed.
 #pragma once
 
 #include "dp_exact.cuh"
@@ -69,45 +86,217 @@ __device__ void scanCounts(const float *rowMax, const int *rowCnt, int *cnt, int
 
 struct ExactWaveJob {
     int pair;
-    int pad;
+    int warps;             // warps running the pair's stripes (<= kPipeWarps)
     long long scratchOff;  // float offset of this job's scratch
 };
 
-// Scratch per job (floats): W1 nS*D*32R, ring 4P, rowMax M+1, rowCnt M+1,
-// cntB M+2, cntF M+2.
-__host__ __device__ inline long long exactWaveScratch(int M, int L) {
+constexpr int kPipeWarps = 8;        // warps per CTA of the exact path
+constexpr int kPipeExtra = 128;      // stripe period P' = P + kPipeExtra
+constexpr int kPipeSpinLimit = 1 << 24;  // iterations of a wait (64 ns sleeps) before it gives up
+static_assert(kPipeExtra >= kLanes - 1 + 2 * kBlock, "a window never reaches the next stripe early");
+
+__host__ __device__ inline int pipePeriod(int L) { return wavePeriod(L) + kPipeExtra; }
+
+// Scratch per job (floats): W1 nS*D*32R, rings 2W x 4P, rowMax M+1, rowCnt
+// M+1, cntB M+2, cntF M+2.
+__host__ __device__ inline long long exactWaveScratch(int M, int L, int W) {
     const long long S = (long long)kLanes * kExactR;
     const long long nS = (M + 1 + S - 1) / S;
     const long long P = wavePeriod(L);
     const long long D = P + kLanes - 1;
-    return nS * D * S + 4 * P + 2LL * (M + 1) + 2LL * (M + 2) + 64;
+    return nS * D * S + 2LL * W * 4 * P + 2LL * (M + 1) + 2LL * (M + 2) + 64;
 }
 
-// One warp per CTA; dynamic shared memory = the emission table (tableFloats)
-// and one Window.
-__global__ void __launch_bounds__(kLanes) exactWaveKernel(const ExactWaveJob *jobs, int n, const DevPair *pairs,
-                                                           const DevProfile *profiles, const float *emit,
-                                                           const float *params, const uint8_t *codes,
-                                                           const float *seeds, const PairScales *scales,
-                                                           float *scratch, ExactOut *out, int tableFloats) {
+struct PipeSync {
+    volatile int *progress;  // [kPipeWarps]: ring-writer position of each warp
+    volatile int *abort;     // the CTA's abort flag
+    int W;                   // warps running stripes
+};
+
+// Position of this warp's ring-writing lane (local time t0 - 31) at block
+// boundary t0, and publication of it (after the lane's ring stores).
+__device__ __forceinline__ int pipePos(const SweepArgs &a, int lt) {
+    if (lt < 0) return a.sFirst * a.P;
+    const int k = lt / a.P;
+    if (k >= a.nMine) return INT_MAX;
+    return (a.sFirst + k * a.sStep) * a.P + (lt - k * a.P);
+}
+__device__ __forceinline__ void pipePublish(const PipeSync &ps, int warp, int pos, int lane) {
+    __threadfence_block();  // each lane's ring stores (lane 0 backward, lane 31 forward) ...
+    __syncwarp();
+    if (lane == 0) ps.progress[warp] = pos;  // ... before the position
+}
+
+// Lane 0 waits until warp w's position reaches target; false on abort.
+__device__ __forceinline__ bool pipeWaitOne(const PipeSync &ps, int w, int target) {
+    int it = 0;
+    while (ps.progress[w] < target) {
+        if (*ps.abort) return false;
+        if (++it > kPipeSpinLimit) {
+            *ps.abort = 1;
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// Before the block of local times [t0, t0 + kBlock) and the refill of the
+// window entries [fill, fill + kBlock): the ring columns the refill reads are
+// written, and the ring slots this block writes have been read.  Warp-uniform.
+__device__ __forceinline__ bool pipeReady(const PipeSync &ps, const SweepArgs &a, int t0, int fill, int lane) {
+    bool ok = true;
+    if (lane == 0) {
+        const int total = a.nMine * a.P;
+        // readers: the last entry of each stripe the refill touches
+        for (int u = fill; ok && u < fill + kBlock && u < total;) {
+            const int k = u / a.P;
+            const int kEnd = min(min(fill + kBlock, total), (k + 1) * a.P) - 1;  // last entry in stripe k
+            const int sp = a.sFirst + k * a.sStep;
+            const int jj = min(kEnd - k * a.P, a.L - 1);
+            if (sp > 0 && u - k * a.P < a.L) ok = pipeWaitOne(ps, (sp - 1) % ps.W, (sp - 1) * a.P + jj + 1);
+            u = (k + 1) * a.P;
+        }
+        // writers: before overwriting ring slot (sp mod 2W), stripe r = sp - 2W + 1 (which
+        // reads the slot's previous contents) has staged all its columns: its writer lane
+        // is past column L, and a warp's refills run at least 78 steps ahead of it
+        for (int lt = max(t0 - (kLanes - 1), 0); ok && lt < t0 + kBlock - (kLanes - 1) && lt < total;) {
+            const int k = lt / a.P;
+            const int sp = a.sFirst + k * a.sStep;
+            const int r = sp - a.ringSlots + 1;
+            if (sp < a.nS - 1 && r >= 1) ok = pipeWaitOne(ps, r % ps.W, r * a.P + a.L);
+            lt = (k + 1) * a.P;
+        }
+    }
+    ok = __shfl_sync(kFull, ok, 0);
+    __syncwarp();
+    __threadfence_block();  // the positions seen before the refill's ring loads
+    return ok;
+}
+
+template <int R, int MODE>
+__device__ bool backwardSweepPipe(const SweepArgs &a, Window &win, int warp, int lane, const PipeSync &ps,
+                                  const ExactRows *x, ExactBest *exact) {
+    BwdState<R, MODE> b;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) b.h[q][k] = b.z[q][k] = 0.0f;
+        b.rb[q] = 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        b.rmax[k] = 0.0f;
+        b.cOut[k] = 0;
+        b.fOut[k] = 1.0f;
+        b.rowBest[k] = 0.0;
+    }
+    b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
+    b.sendC = b.cnt = 0;
+    b.realRows = 0;
+    b.u = -(kLanes - 1 - lane);  // lane 31 leads
+    b.sp = a.sFirst;
+    b.jj = 0;
+    b.wp = a.w1;
+    const int total = a.nMine * a.P;
+    const int T = (total + (kLanes - 1) + 2) / 3 * 3;
+    if (!pipeReady(ps, a, -kBlock, 0, lane)) return false;
+    fillBlock<true, true>(win, a, 0, lane);
+    for (int t0 = 0; t0 < T; t0 += kBlock) {
+        pipePublish(ps, warp, pipePos(a, t0 - (kLanes - 1)), lane);
+        if (!pipeReady(ps, a, t0, t0 + kBlock, lane)) return false;
+        fillBlock<true, true>(win, a, t0 + kBlock, lane);
+        const int n = (t0 + kBlock < T ? kBlock : T - t0);
+#pragma unroll 1
+        for (int g = 0; g < n; g += 3) {
+            backwardStep<R, MODE, 0>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 1>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 2>(b, a, win, lane, total, x, exact);
+        }
+    }
+    pipePublish(ps, warp, INT_MAX, lane);
+    return true;
+}
+
+template <int R, int MODE>
+__device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int lane, const PipeSync &ps,
+                                 const ExactRows *x, ExactBest *exact) {
+    FwdState<R, MODE> f;
+#pragma unroll
+    for (int h = 0; h < 3; ++h)
+#pragma unroll
+        for (int k = 0; k < R; ++k) f.w[h][k] = f.z[h][k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        f.rmax[k] = 0.0f;
+        f.cIn[k] = f.cB[k] = 0;
+        f.fOut[k] = 1.0f;
+        f.rowBest[k] = 0.0;
+    }
+    f.sendIn = f.sendY = f.best = f.mx = 0.0f;
+    f.sendC = f.cnt = 0;
+    f.u = -lane;  // lane 0 leads
+    f.s = a.sFirst;
+    f.j = 0;
+    const int total = a.nMine * a.P;
+    const int T = (total + (kLanes - 1) + 5) / 6 * 6;
+    constexpr bool kReadW1 = MODE == kReplay;
+    W1Stage<R, true> st{-lane, a.sFirst, 0};
+    if (kReadW1) {
+#pragma unroll
+        for (int k = 0; k < kW1Ahead; ++k) st.issue(a, win, k, lane, total);
+    }
+    bool ok = pipeReady(ps, a, -kBlock, 0, lane);
+    if (ok) fillBlock<false, true>(win, a, 0, lane);
+    for (int t0 = 0; ok && t0 < T; t0 += kBlock) {
+        pipePublish(ps, warp, pipePos(a, t0 - (kLanes - 1)), lane);
+        ok = pipeReady(ps, a, t0, t0 + kBlock, lane);
+        if (!ok) break;
+        fillBlock<false, true>(win, a, t0 + kBlock, lane);
+        const int n = (t0 + kBlock < T ? kBlock : T - t0);
+#pragma unroll 1
+        for (int g = 0; g < n; g += 6) {
+            forwardStaged<R, MODE, 0>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 1>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 2>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 3>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 4>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 5>(f, a, win, lane, total, st, x, exact);
+        }
+    }
+    if (kReadW1) cpAsyncWait<0>();  // no copy outlives the sweep (the slots are reused)
+    if (ok) pipePublish(ps, warp, INT_MAX, lane);
+    return ok;
+}
+
+// One CTA of kPipeWarps warps per pair (persistent over the jobs); dynamic
+// shared memory = one Window per warp.  The emission table is read from
+// global memory (a stripe's 32 R rows x 25 codes stay in L1), so tall
+// profiles leave the shared memory to the windows.
+__global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
+    exactWaveKernel(const ExactWaveJob *jobs, int n, const DevPair *pairs, const DevProfile *profiles,
+                    const float *emit, const float *params, const uint8_t *codes, const float *seeds,
+                    const PairScales *scales, float *scratch, ExactOut *out) {
     extern __shared__ float4 smRaw[];
-    float *smE = reinterpret_cast<float *>(smRaw);
-    Window &win = *reinterpret_cast<Window *>(smE + tableFloats);
+    Window *wins = reinterpret_cast<Window *>(smRaw);
     __shared__ float smBg[32];
-    const int lane = threadIdx.x;
+    __shared__ int progress[kPipeWarps];
+    __shared__ int abortFlag;
+    __shared__ ExactBest bestF[kPipeWarps], bestM[kPipeWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Window &win = wins[warp];
+    PipeSync ps;
+    ps.progress = progress;
+    ps.abort = &abortFlag;
     for (int ji = blockIdx.x; ji < n; ji += gridDim.x) {
         const ExactWaveJob job = jobs[ji];
         const DevPair p = pairs[job.pair];
         const DevProfile &pr = profiles[p.prof];
-        const int rowPad = pr.rowPad;
-        __syncwarp();
-        {
-            const float4 *src = reinterpret_cast<const float4 *>(emit + pr.emitOff);
-            const int n4 = kNumCodes * rowPad / 4;
-            for (int k = lane; k < n4; k += kLanes) smRaw[k] = __ldg(src + k);
-            smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
-        }
-        __syncwarp();
+        const int W = job.warps;
+        ps.W = W;
+        __syncthreads();  // the previous job is done with the shared state
+        if (warp == 0) smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
+        if (threadIdx.x == 0) abortFlag = 0;
         if (lane == 0) {
             PairCold &c = win.cold;
             c.codes = codes + p.codeOff;
@@ -117,46 +306,69 @@ __global__ void __launch_bounds__(kLanes) exactWaveKernel(const ExactWaveJob *jo
             c.smBg = smBg;
             c.sc = scales[job.pair];
             c.M = p.M;
+            bestF[warp] = ExactBest{0.0, 0};
+            bestM[warp] = ExactBest{0.0, 0};
         }
-        __syncwarp();
         SweepArgs a;
         a.cold = &win.cold;
-        a.smE = smE;
+        a.smE = emit + pr.emitOff;
         a.L = p.L;
-        a.rowPad = rowPad;
+        a.rowPad = pr.rowPad;
         a.nS = (p.M + 1 + kLanes * kExactR - 1) / (kLanes * kExactR);
-        a.P = wavePeriod(p.L);
-        a.D = a.P + kLanes - 1;
+        const int Pw = wavePeriod(p.L);
+        a.P = Pw + kPipeExtra;
+        a.D = Pw + kLanes - 1;
+        a.sFirst = warp;
+        a.sStep = W;
+        a.nMine = warp < W ? (a.nS - warp + W - 1) / W : 0;
+        a.ringSlots = 2 * W;
+        a.ringStride = 4LL * Pw;
         float *base = scratch + job.scratchOff;
         a.w1 = base;
         a.ring = base + (size_t)a.nS * a.D * kLanes * kExactR;
         ExactRows x;
-        x.rowMax = a.ring + 4 * (size_t)a.P;
+        x.rowMax = a.ring + (size_t)a.ringSlots * a.ringStride;
         x.rowCnt = reinterpret_cast<int *>(x.rowMax + (p.M + 1));
         x.cntB = x.rowCnt + (p.M + 1);
         x.cntF = x.cntB + (p.M + 2);
         ExactBest filt{0.0, 0}, mid{0.0, 0};
-        float f0, f1;
-        backwardSweep<kExactR, kDiscover>(a, win, lane, f0, f1, &x, nullptr);
-        __syncwarp();
-        if (lane == 0) scanCounts(x.rowMax, x.rowCnt, x.cntB, p.M, true);
-        __syncwarp();
-        forwardSweep<kExactR, kDiscover>(a, win, lane, f0, f1, &x, nullptr);
-        __syncwarp();
-        if (lane == 0) scanCounts(x.rowMax, x.rowCnt, x.cntF, p.M, false);
-        __syncwarp();
-        backwardSweep<kExactR, kReplay>(a, win, lane, f0, f1, &x, &filt);
-        __syncwarp();
-        forwardSweep<kExactR, kReplay>(a, win, lane, f0, f1, &x, &mid);
+        bool ok = true;
+        // Four sweeps, each over every warp; the counts scan between them.
+        for (int phase = 0; phase < 4; ++phase) {
+            if (lane == 0) progress[warp] = warp < W ? pipePos(a, -1) : INT_MAX;
+            __syncthreads();
+            if (warp < W && ok) {
+                switch (phase) {
+                case 0: ok = backwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
+                case 1: ok = forwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
+                case 2: ok = backwardSweepPipe<kExactR, kReplay>(a, win, warp, lane, ps, &x, &filt); break;
+                default: ok = forwardSweepPipe<kExactR, kReplay>(a, win, warp, lane, ps, &x, &mid); break;
+                }
+            }
+            __syncthreads();
+            ok = ok && abortFlag == 0;
+            if (phase < 2 && threadIdx.x == 0 && ok) scanCounts(x.rowMax, x.rowCnt, phase == 0 ? x.cntB : x.cntF, p.M, phase == 0);
+        }
         filt = warpBest(filt);
         mid = warpBest(mid);
         if (lane == 0) {
+            bestF[warp] = filt;
+            bestM[warp] = mid;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            ExactBest f{0.0, 0}, m{0.0, 0};
+            for (int w = 0; w < W; ++w) {
+                const ExactBest bf = bestF[w], bm = bestM[w];
+                if (bf.m != 0.0 && (f.m == 0.0 || bf.e > f.e || (bf.e == f.e && bf.m > f.m))) f = bf;
+                if (bm.m != 0.0 && (m.m == 0.0 || bm.e > m.e || (bm.e == m.e && bm.m > m.m))) m = bm;
+            }
             ExactOut o;
-            o.mid = mid.m == 0.0 ? xsZero() : XS{__double2float_rn(mid.m), mid.e};
-            o.filt = filt.m == 0.0 ? xsZero() : XS{__double2float_rn(filt.m), filt.e};
+            o.mid = m.m == 0.0 ? xsZero() : XS{__double2float_rn(m.m), m.e};
+            o.filt = f.m == 0.0 ? xsZero() : XS{__double2float_rn(f.m), f.e};
+            o.failed = abortFlag != 0;
             out[ji] = o;
         }
-        __syncwarp();
     }
 }
 

@@ -64,10 +64,16 @@ struct PairCold {
 
 struct SweepArgs {
     PairCold *cold;         // in shared memory
-    const float *smE;       // emission table in shared memory, [25][rowPad]
+    const float *smE;       // emission table, [25][rowPad] (shared memory; the exact path reads it from global)
     float *w1;              // this warp's W1 slot
     float *ring;            // this warp's stripe-boundary ring (4 floats per column)
     int L, rowPad, nS, P, D;
+    // Stripes of this warp, in processing order: sFirst, sFirst + sStep, ...
+    // (nMine of them; the fast path: 0, 1, ..., nS-1).  The exact path runs a
+    // pair's stripes on several warps: the ring of stripe sp (processing
+    // order) is then ring + (sp % ringSlots) * ringStride.
+    int sFirst, sStep, nMine, ringSlots;
+    long long ringStride;
 
     __device__ __forceinline__ const uint8_t *codes() const {
         return *reinterpret_cast<const uint8_t *const volatile *>(&cold->codes);
@@ -242,18 +248,31 @@ __device__ __forceinline__ float fmax3(float a, float b, float c) {
     return r;
 }
 
+// The ring a stripe reads (written by the stripe before it in processing order).
+template <bool EXACT>
+__device__ __forceinline__ const float *ringOfPrev(const SweepArgs &a, int k) {
+    if (!EXACT) return a.ring;
+    const int sp = a.sFirst + k * a.sStep;
+    return a.ring + (size_t)((sp - 1) % a.ringSlots) * a.ringStride;
+}
+template <bool EXACT>
+__device__ __forceinline__ int stripeOf(const SweepArgs &a, int k) {
+    return EXACT ? a.sFirst + k * a.sStep : k;
+}
+
 // Backward window entry for local time u (the column of u is L-1 - u mod P).
+template <bool EXACT>
 __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
     float4 c = make_float4(__int_as_float(kPad * a.rowPad), 0.0f, 0.0f, 0.0f);
     float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (u >= 0 && u < a.nS * a.P) {
-        const int sp = u / a.P, jj = u - sp * a.P;
+    if (u >= 0 && u < a.nMine * a.P) {
+        const int k = u / a.P, jj = u - k * a.P;
         if (jj < a.L) {
             const int j = a.L - 1 - jj;
             const int code = (j + 1 < a.L) ? (int)__ldg(a.codes() + j + 1) : kPad;
             c = make_float4(__int_as_float(code * a.rowPad), a.smBg()[code], __ldg(a.suf() + j), __ldg(a.pre() + j));
-            if (sp > 0) r = ringLoad(a.ring, jj);
+            if (stripeOf<EXACT>(a, k) > 0) r = ringLoad(ringOfPrev<EXACT>(a, k), jj);
         }
     }
     w.col[e] = c;
@@ -261,16 +280,17 @@ __device__ __forceinline__ void fillBackward(Window &w, const SweepArgs &a, int 
 }
 
 // Forward window entry for local time u (the column of u is u mod P).
+template <bool EXACT>
 __device__ __forceinline__ void fillForward(Window &w, const SweepArgs &a, int u) {
     const int e = u & (kWin - 1);
     float4 c = make_float4(__int_as_float(kPad * a.rowPad), 0.0f, 0.0f, 0.0f);
     float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (u >= 0 && u < a.nS * a.P) {
-        const int s = u / a.P, j = u - s * a.P;
+    if (u >= 0 && u < a.nMine * a.P) {
+        const int k = u / a.P, j = u - k * a.P;
         if (j < a.L) {
             const int code = (j >= 2) ? (int)__ldg(a.codes() + j - 2) : kPad;
             c = make_float4(__int_as_float(code * a.rowPad), a.smBg()[code] * a.sc().sC, __ldg(a.pre() + j), 0.0f);
-            if (s > 0) r = ringLoad(a.ring, j);
+            if (stripeOf<EXACT>(a, k) > 0) r = ringLoad(ringOfPrev<EXACT>(a, k), j);
         }
     }
     w.col[e] = c;
@@ -359,6 +379,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
                                              int total, const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
     constexpr bool kStore = MODE == kMid || MODE == kReplay;
+    constexpr bool kExactMode = MODE == kDiscover || MODE == kReplay;
     constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
     float inW = __shfl_down_sync(kFull, b.sendW, 1);
     float inY = __shfl_down_sync(kFull, b.sendY, 1);
@@ -526,10 +547,11 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             b.wp += kLanes * R;
         }
         if (lane == 0 && b.sp < a.nS - 1) {
+            float *rg = kExactMode ? a.ring + (size_t)(b.sp % a.ringSlots) * a.ringStride : a.ring;
             if (MODE == kDiscover)
-                ringStore(a.ring, b.jj, b.sendW, b.sendY, b.sendC);
+                ringStore(rg, b.jj, b.sendW, b.sendY, b.sendC);
             else
-                ringStore(a.ring, b.jj, b.sendW, b.sendY);
+                ringStore(rg, b.jj, b.sendW, b.sendY);
         }
         if (b.jj == a.L - 1) {
             // the last column of these rows
@@ -551,22 +573,22 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
     }
     if (b.u >= 0 && ++b.jj == a.P) {
         b.jj = 0;
-        ++b.sp;
+        b.sp += kExactMode ? a.sStep : 1;
     }
     ++b.u;
 }
 
 // Window refills for a block of kBlock steps starting at t0: local times
 // [t0 + kBlock, t0 + 2 kBlock), one entry per lane and pass.
-template <bool BACKWARD>
+template <bool BACKWARD, bool EXACT = false>
 __device__ __forceinline__ void fillBlock(Window &win, const SweepArgs &a, int first, int lane) {
 #pragma unroll
     for (int o = 0; o < kBlock; o += kLanes) {
         if (o + lane < kBlock) {
             if (BACKWARD)
-                fillBackward(win, a, first + o + lane);
+                fillBackward<EXACT>(win, a, first + o + lane);
             else
-                fillForward(win, a, first + o + lane);
+                fillForward<EXACT>(win, a, first + o + lane);
         }
     }
 }
@@ -594,7 +616,7 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
     b.u = -(kLanes - 1 - lane);  // lane 31 leads
     b.sp = b.jj = 0;
     b.wp = a.w1;
-    const int total = a.nS * a.P;
+    const int total = a.nMine * a.P;
     const int T = (total + (kLanes - 1) + 2) / 3 * 3;  // whole groups of three steps
     __syncwarp();
     fillBlock<true>(win, a, 0, lane);
@@ -632,7 +654,7 @@ __device__ __forceinline__ void cpAsyncWait() {
 // W1 staging cursor of the forward sweep: the lane-local time whose W1 is
 // copied next (kW1Ahead steps ahead of the lane).  Every call commits one
 // group, empty for steps the lane does not compute.
-template <int R>
+template <int R, bool EXACT = false>
 struct W1Stage {
     int u, s, j;
     __device__ __forceinline__ void issue(const SweepArgs &a, Window &win, int slot, int lane, int total) {
@@ -643,7 +665,7 @@ struct W1Stage {
         cpAsyncCommit();
         if (u >= 0 && ++j == a.P) {
             j = 0;
-            ++s;
+            s += EXACT ? a.sStep : 1;
         }
         ++u;
     }
@@ -671,6 +693,7 @@ template <int R, int MODE, int PH>
 __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                             int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
+    constexpr bool kExactMode = MODE == kDiscover || MODE == kReplay;
     constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
     float inW = __shfl_up_sync(kFull, f.sendIn, 1);
     float inY = __shfl_up_sync(kFull, f.sendY, 1);
@@ -795,10 +818,11 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         f.sendIn = win0;
         f.sendY = yab;
         if (lane == kLanes - 1 && f.s < a.nS - 1) {
+            float *rg = kExactMode ? a.ring + (size_t)(f.s % a.ringSlots) * a.ringStride : a.ring;
             if (MODE == kDiscover)
-                ringStore(a.ring, f.j, f.sendIn, f.sendY, f.sendC);
+                ringStore(rg, f.j, f.sendIn, f.sendY, f.sendC);
             else
-                ringStore(a.ring, f.j, f.sendIn, f.sendY);
+                ringStore(rg, f.j, f.sendIn, f.sendY);
         }
         if (f.j == a.L - 1) {
 #pragma unroll
@@ -819,7 +843,7 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
     }
     if (f.u >= 0 && ++f.j == a.P) {
         f.j = 0;
-        ++f.s;
+        f.s += kExactMode ? a.sStep : 1;
     }
     ++f.u;
 }
@@ -829,7 +853,8 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
 // the step kW1Ahead later into the slot this lane read one step ago.
 template <int R, int MODE, int P6>
 __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
-                                              int total, W1Stage<R> &st, const ExactRows *x, ExactBest *exact) {
+                                              int total, W1Stage<R, MODE == kDiscover || MODE == kReplay> &st,
+                                              const ExactRows *x, ExactBest *exact) {
     constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
     float q[R];
     if (kReadW1) {
@@ -874,10 +899,10 @@ __device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &b
     f.sendC = f.cnt = 0;
     f.u = -lane;  // lane 0 leads
     f.s = f.j = 0;
-    const int total = a.nS * a.P;
+    const int total = a.nMine * a.P;
     const int T = (total + (kLanes - 1) + 5) / 6 * 6;  // whole groups of six steps
     constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
-    W1Stage<R> st{-lane, 0, 0};
+    W1Stage<R, MODE == kDiscover || MODE == kReplay> st{-lane, 0, 0};
     if (kReadW1) {
 #pragma unroll
         for (int k = 0; k < kW1Ahead; ++k) st.issue(a, win, k, lane, total);
@@ -953,6 +978,11 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     a.nS = (p.M + 1 + kLanes * R - 1) / (kLanes * R);
     a.P = wavePeriod(p.L);
     a.D = a.P + kLanes - 1;
+    a.sFirst = 0;
+    a.sStep = 1;
+    a.nMine = a.nS;
+    a.ringSlots = 1;
+    a.ringStride = 0;
     float filt, maxYb, mid = 0.0f, maxFw = 0.0f;
     if (MID) {
         backwardSweep<R, kMid>(a, win, lane, filt, maxYb);
