@@ -92,16 +92,23 @@ template <typename T>
 struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;  // elements
-    // Capacity for n elements, contents not kept.  Growth is geometric (x1.25)
+    // Capacity for n elements, contents not kept.  Growth is geometric (x1.25,
+    // or n x (1 + headroom) for buffers whose need varies from call to call)
     // so that calls whose sizes vary a little do not reallocate (cudaFree and
     // cudaMalloc synchronise the device).
-    cudaError_t ensure(size_t n) {
+    cudaError_t ensure(size_t n, double headroom = 0.0) {
         if (n <= cap && p) return cudaSuccess;
-        const size_t want = std::max<size_t>({n, cap + cap / 4, 1});
+        const size_t want = std::max<size_t>({n, cap + cap / 4, (size_t)((double)n * (1.0 + headroom)), 1});
         if (p) cudaFree(p);
         p = nullptr;
         cap = 0;
         cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e != cudaSuccess && want > n) {  // the headroom did not fit: the exact size
+            cudaGetLastError();
+            e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+            if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
+            return e;
+        }
         if (e == cudaSuccess) cap = want;
         return e;
     }
@@ -161,13 +168,20 @@ constexpr int kShapeWarps[2] = {kCtaWarps, kCtaWarpsNarrow};
 inline int rIndex(int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); }
 
 using DpKern = void (*)(DpArgs, int);
-template <bool MID, int W>
+template <bool MID, int W, bool GT>
 DpKern kernByR(int R) {
-    return R == 4 ? dpKernel<4, MID, W> : (R == 2 ? dpKernel<2, MID, W> : dpKernel<1, MID, W>);
+    return R == 4 ? dpKernel<4, MID, W, GT> : (R == 2 ? dpKernel<2, MID, W, GT> : dpKernel<1, MID, W, GT>);
 }
-DpKern dpKernelFor(int R, bool mid, int warps) {
-    if (warps == kCtaWarpsNarrow) return mid ? kernByR<true, kCtaWarpsNarrow>(R) : kernByR<false, kCtaWarpsNarrow>(R);
-    return mid ? kernByR<true, kCtaWarps>(R) : kernByR<false, kCtaWarps>(R);
+template <bool GT>
+DpKern dpKernelShape(int R, bool mid, int warps) {
+    if (warps == kCtaWarpsNarrow)
+        return mid ? kernByR<true, kCtaWarpsNarrow, GT>(R) : kernByR<false, kCtaWarpsNarrow, GT>(R);
+    return mid ? kernByR<true, kCtaWarps, GT>(R) : kernByR<false, kCtaWarps, GT>(R);
+}
+// gt: the emission table stays in global memory (profiles whose table would
+// leave shared memory for fewer than `warps` staging windows).
+DpKern dpKernelFor(int R, bool mid, int warps, bool gt) {
+    return gt ? dpKernelShape<true>(R, mid, warps) : dpKernelShape<false>(R, mid, warps);
 }
 
 // Rows of a profile as the kernel with R rows per lane computes them.
@@ -213,6 +227,7 @@ struct dmst_ctx {
     Rates rates;
     Tuning tune;
     cudaGraphExec_t graphExec = nullptr;  // DMST_MODE_GRAPH: the instantiated launch graph
+    bool exactAttrSet = false;            // the exact kernel's shared-memory attribute is set
     std::vector<uintptr_t> graphKey;      // the launch shape and buffers it was captured with
     int graphLaunches = 0;                // kernel launches in it
     int graphCaptures = 0;                // captures so far (replays reuse the last)
@@ -832,6 +847,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         int R, warps;     // warps launched per CTA (<= kernWarps when shared memory is short)
         int kernWarps;    // the kernel's CTA shape (warp slots per CTA)
         DpKern kern;
+        bool gt = false;  // emission table read from global memory
         std::vector<Chunk> chunks;
         std::vector<double> cost;
         int maxRowPad = 0;
@@ -845,12 +861,12 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         groups[q].R = kShapeR[q];
         groups[q].kernWarps = W;
         groups[q].warps = W;
-        groups[q].kern = dpKernelFor(kShapeR[q], mid, W);
+        groups[q].kern = dpKernelFor(kShapeR[q], mid, W, false);
     }
     auto groupOf = [](int R) { return rIndex(R); };
-    // Warps per CTA: tall profiles leave less shared memory for the windows.
-    // Chunks then hold four pairs per launched warp, fewer when the group has
-    // too few pairs to give each CTA four chunks.
+    // Warps per CTA: tall profiles leave less shared memory for the windows
+    // (or keep their table in global memory), and long pairs of tall profiles
+    // are capped by the device memory their W1 slots take.
     const size_t smemLimit = (size_t)ctx->maxSmemOptin - 1024;
     long long groupPairs[3] = {0, 0, 0};
     for (size_t k = 0; k < n && !nullOnly; ++k) {
@@ -858,17 +874,50 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         G.maxRowPad = std::max(G.maxRowPad, ctx->profiles[dp[k].prof].rowPad);
         ++groupPairs[groupOf(dp[k].R)];
     }
+    // Slot sizes rounded up to one of eight levels per power of two (at most
+    // 12.5% larger), so that calls of similar shape keep the same slot layout
+    // (and replay the same launch graph under DMST_MODE_GRAPH).
+    auto slotLevel = [](size_t v) {
+        v = std::max<size_t>(v, 64);
+        const int hb = 63 - __builtin_clzll((unsigned long long)v);
+        const size_t q = std::max<size_t>((size_t)1 << std::max(hb - 3, 6), 64);
+        return (v + q - 1) / q * q;
+    };
+    const size_t w1Slot = slotLevel(w1Max);
+    const size_t ringSlot = slotLevel(ringMax);
+    // Every launched warp holds one W1 slot: at most maxSlots of them fit the
+    // device budget (the call's budget, or 60% of the free memory counting the
+    // slots the context already holds).  Long pairs of tall profiles (80 MB of
+    // W1 at M = 2000 x 10 kb) then run fewer warps per CTA, or fewer CTAs.
+    size_t maxSlots = SIZE_MAX;
+    if (mid && !nullOnly) {
+        size_t freeB = 0, totalB = 0;
+        CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+        const size_t held = (ctx->dW1.cap + ctx->dRing.cap) * sizeof(float);
+        const size_t budget =
+            ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (size_t)(0.6 * (double)(freeB + held));
+        maxSlots = std::max<size_t>(1, budget / ((w1Slot + ringSlot) * sizeof(float)));
+    }
     int chunkPairsOf[3] = {1, 1, 1};
     for (int q = 0; q < 3; ++q) {
         Group &G = groups[q];
         if (!groupPairs[q]) continue;
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
-        if (table + sizeof(Window) > smemLimit)
-            return ctx->fail(DMST_ERANGE, "profile too long for the shared-memory emission table (M <= %d)",
-                             (int)((smemLimit - sizeof(Window)) / (kNumCodes * 4)) - 1);
-        G.warps = (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / sizeof(Window));
+        // A table that would leave room for fewer than the shape's warps stays
+        // in global memory instead (read through L1), and every warp runs.
+        G.gt = table + (size_t)G.kernWarps * sizeof(Window) > smemLimit;
+        if (G.gt) G.kern = dpKernelFor(G.R, mid, G.kernWarps, true);
+        G.warps = G.gt ? G.kernWarps : (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / sizeof(Window));
+        G.warps = (int)std::max<size_t>(1, std::min<size_t>(G.warps, maxSlots / ctx->smCount));
+        // Chunks of up to four pairs per launched warp, fewer when the group is
+        // too small to give each CTA four chunks, but never fewer pairs than the
+        // CTA's warps while there are that many pairs per SM (a chunk of fewer
+        // pairs leaves warps idle until the chunk's barrier).
         const long long perCta = groupPairs[q] / (4LL * ctx->smCount);
-        chunkPairsOf[q] = plain ? 1 : (int)std::max<long long>(1, std::min<long long>(4LL * G.warps, perCta));
+        const long long perSm = (groupPairs[q] + ctx->smCount - 1) / ctx->smCount;
+        const long long floorPairs = std::min<long long>(G.warps, perSm);
+        chunkPairsOf[q] =
+            plain ? 1 : (int)std::max<long long>(1, std::min<long long>(4LL * G.warps, std::max(floorPairs, perCta)));
     }
     for (size_t k = 0; k < n && !nullOnly;) {
         Group &G = groups[groupOf(dp[k].R)];
@@ -900,13 +949,14 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         allChunks.insert(allChunks.end(), G.chunks.begin(), G.chunks.end());
         // Shared memory: the emission table, then one staging window per warp.
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
-        G.smem = table + (size_t)G.warps * sizeof(Window);
+        G.smem = (G.gt ? 0 : table) + (size_t)G.warps * sizeof(Window);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
         int perSm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
         if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
         G.grid = plain ? 1 : (int)std::min<long long>((long long)perSm * ctx->smCount, (long long)G.chunks.size());
+        G.grid = (int)std::max<size_t>(1, std::min<size_t>(G.grid, maxSlots / G.warps));
         slotsMax = std::max(slotsMax, (size_t)G.grid * G.warps);
     }
 
@@ -921,17 +971,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk),
                            cudaMemcpyHostToDevice, ctx->stream),
            "upload chunks");
-    // Slot sizes rounded up to one of eight levels per power of two (at most
-    // 12.5% larger), so that calls of similar shape keep the same slot layout
-    // (and replay the same launch graph under DMST_MODE_GRAPH).
-    auto slotLevel = [](size_t v) {
-        v = std::max<size_t>(v, 64);
-        const int hb = 63 - __builtin_clzll((unsigned long long)v);
-        const size_t q = std::max<size_t>((size_t)1 << std::max(hb - 3, 6), 64);
-        return (v + q - 1) / q * q;
-    };
-    const size_t w1Slot = slotLevel(w1Max);
-    const size_t ringSlot = slotLevel(ringMax);
     // The groups run one after another on the stream, so they share the slots.
     CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
@@ -1023,7 +1062,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                         gk.chunks = ctx->dChunks.p + G.chunkBase + k;
                         gk.nChunks = 1;
                         gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
-                        G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
+                        G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                         ++launches;
                     }
                 } else {
@@ -1031,7 +1070,7 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                     gk.chunks = ctx->dChunks.p + G.chunkBase;
                     gk.nChunks = (int)G.chunks.size();
                     gk.chunkCounter = ctx->dCounter.p + gi;
-                    G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, kNumCodes * G.maxRowPad);
+                    G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                     ++launches;
                 }
                 CK(cudaGetLastError(), "DP kernel");
@@ -1118,9 +1157,11 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         eo.resize(flagged.size());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         const size_t pipeSmem = kPipeWarps * sizeof(Window);
-        if (!sequentialExact)
+        if (!sequentialExact && !ctx->exactAttrSet) {
             CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipeSmem),
                "smem attribute");
+            ctx->exactAttrSet = true;
+        }
         size_t i0 = 0;
         while (i0 < flagged.size()) {
             std::vector<ExactJob> jobs;
@@ -1143,7 +1184,8 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                 ++i1;
             }
             const size_t nj = i1 - i0;
-            CK(ctx->dExactScratch.ensure((size_t)used), "alloc exact scratch");
+            // the flagged pairs change from call to call: 50% headroom
+            CK(ctx->dExactScratch.ensure((size_t)used, 0.5), "alloc exact scratch");
             CK(ctx->dExactOut.ensure(nj), "alloc exact out");
             if (sequentialExact) {
                 CK(ctx->dJobs.ensure(nj), "alloc exact jobs");

@@ -1015,12 +1015,15 @@ constexpr int kCtaWarpsNarrow = 8;
 // the chunk's profile emission table in shared memory, and their warps pull
 // pairs from the chunk.  Dynamic shared memory: the table (tableFloats), then
 // one Window per warp (the launch may use fewer than WARPS warps when the
-// table leaves no room; W1 slots are indexed by the launched warps).
-template <int R, bool MID, int WARPS>
+// table leaves no room; W1 slots are indexed by the launched warps).  With
+// GT (tall profiles) the table stays in global memory, read through L1 (a
+// stripe's 32 R rows of 25 codes), and the shared memory holds the windows
+// of all WARPS warps.
+template <int R, bool MID, int WARPS, bool GT>
 __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
     extern __shared__ float4 smRaw[];
-    float *smE = reinterpret_cast<float *>(smRaw);
-    Window *wins = reinterpret_cast<Window *>(smE + tableFloats);
+    const float *smE = reinterpret_cast<const float *>(smRaw);
+    Window *wins = reinterpret_cast<Window *>(reinterpret_cast<float *>(smRaw) + tableFloats);
     __shared__ float smBg[32];
     __shared__ int smChunk, smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1041,9 +1044,13 @@ __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tabl
         const int rowPad = ch.rowPad;
         if (ch.prof != loaded) {
             const DevProfile *pr = g.profiles + ch.prof;
-            const float4 *src = reinterpret_cast<const float4 *>(g.emit + pr->emitOff);
-            const int n4 = kNumCodes * rowPad / 4;
-            for (int i = threadIdx.x; i < n4; i += blockDim.x) smRaw[i] = __ldg(src + i);
+            if (GT) {
+                smE = g.emit + pr->emitOff;
+            } else {
+                const float4 *src = reinterpret_cast<const float4 *>(g.emit + pr->emitOff);
+                const int n4 = kNumCodes * rowPad / 4;
+                for (int i = threadIdx.x; i < n4; i += blockDim.x) smRaw[i] = __ldg(src + i);
+            }
             if (threadIdx.x < 32) smBg[threadIdx.x] = threadIdx.x < kNumCodes ? pr->bg[threadIdx.x] : 0.0f;
             loaded = ch.prof;
         }
