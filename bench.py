@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--ag-lmax", type=int, default=2400, help="autograd workload: longest read")
     ap.add_argument("--no-autotune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
+    ap.add_argument("--no-async", action="store_true", help="synchronous calls (no submit/complete overlap)")
     return ap.parse_args()
 
 
@@ -392,15 +393,29 @@ def run_ours(args, rank, world, local):
     ev0.record(stream)
     launches, dp_ms, cells = 0, 0.0, 0.0
     results = []
-    parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0}
-    for k in range(args.warmup, n_steps):
-        results.append(ctx.score_pairs_raw(step_pairs[k], MODE))
+    parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0, "post_ms": 0.0, "wall_ms": 0.0}
+    # Calls are submitted one ahead of their completion, so that the host work
+    # of one step overlaps the device work of the previous one.
+    def account():
         t = ctx.last_timing()
+        nonlocal launches, dp_ms
         launches += t["launches"]
         dp_ms += t["dp_ms"]
         for key in parts:
             parts[key] += t[key]
+    for k in range(args.warmup, n_steps):
+        if args.no_async:
+            results.append(ctx.score_pairs_raw(step_pairs[k], MODE))
+            account()
+        else:
+            ctx.submit_raw(step_pairs[k], MODE)
+            if k > args.warmup:
+                results.append(ctx.complete())
+                account()
         cells += step_cells[k]
+    if not args.no_async:
+        results.append(ctx.complete())
+        account()
     ev1.record(stream)
     torch.cuda.synchronize()
     exact_pairs = sum(1 for res in results for r in res if r.flags & F.RES_EXACT_PATH)
@@ -429,35 +444,54 @@ def run_ours(args, rank, world, local):
     }
 
     # ---- e2e: host buffers through the C ABI every step ----
+    # Each step's reads are copied from host memory (2-bit packed) and decoded
+    # on the device, scored, and the results copied back; steps are submitted
+    # one ahead of their completion.  The reads of every step are appended
+    # (sequence ids continue), so the pair arrays are built beforehand.
     packed_of = {}
     for recs in steps:  # the genome workload repeats one step's records
         if id(recs) not in packed_of:
             packed_of[id(recs)] = d.pack_dna(recs)
     packed = [packed_of[id(recs)] for recs in steps]
+    ctx.clear_sequences()
+    base = 0
+    e2e_pairs = []
+    for k in range(n_steps):
+        e2e_pairs.append(pairs_for(list(range(base, base + len(steps[k])))))
+        base += len(steps[k])
     h2d = d2h = 0
     for w in range(args.warmup):
-        ctx.clear_sequences()
         words, mask, lens = packed[w]
-        sids = ctx.add_packed(words, lens, mask)
-        ctx.score_pairs_raw(pairs_for(sids), MODE)
-    # After a clear, sequence ids restart at 0, so every step's pair list is
-    # the same array (built once, outside the timed region).
-    e2e_pairs = pairs_for(list(range(len(steps[0]))))
+        ctx.add_packed(words, lens, mask)
+        if args.no_async:
+            ctx.score_pairs_raw(e2e_pairs[w], MODE)
+        else:
+            ctx.submit_raw(e2e_pairs[w], MODE)
+    while ctx.complete() is not None:
+        pass
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    next_id = sum(len(steps[w]) for w in range(args.warmup))
     for k in range(args.warmup, n_steps):
-        ctx.clear_sequences()
         words, mask, lens = packed[k]
         sids = ctx.add_packed(words, lens, mask)
-        assert sids[0] == 0 and len(sids) == len(lens)
-        pr = e2e_pairs
-        res = ctx.score_pairs_raw(pr, MODE)
+        assert sids[0] == next_id and len(sids) == len(lens)
+        next_id += len(lens)
+        pr = e2e_pairs[k]
+        if args.no_async:
+            ctx.score_pairs_raw(pr, MODE)
+        else:
+            ctx.submit_raw(pr, MODE)
+            if k > args.warmup:
+                ctx.complete()
         # packed reads + mask + offsets, then the per-pair descriptors the
-        # library uploads (32 B pair + 8 B scratch offset) and the 16-byte
-        # per-pair results it reads back
+        # library uploads (32 B pair + 8 B scratch offset) and the per-pair
+        # results it reads back (16 B, and 24 B of exact-path results)
         h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 40 * len(pr)
-        d2h += 16 * len(pr)
+        d2h += 40 * len(pr)
+    while ctx.complete() is not None:
+        pass
     torch.cuda.synchronize()
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
     e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
@@ -496,7 +530,7 @@ def run_ours(args, rank, world, local):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
             "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
-            "launch": {"cuda_graph": not args.no_graph, "autotune": tuning},
+            "launch": {"cuda_graph": not args.no_graph, "async_submit": not args.no_async, "autotune": tuning},
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -113,6 +113,9 @@ SIGNATURES = [
     ("dmst_loglik_grad", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double),
       C.POINTER(C.c_double)]),
+    ("dmst_score_pairs_submit", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.c_int, C.POINTER(Result)]),
+    ("dmst_score_pairs_complete", C.c_int, [C.c_void_p]),
+    ("dmst_pending_calls", C.c_int, [C.c_void_p]),
     ("dmst_posteriors", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("dmst_seq_length", C.c_int, [C.c_void_p, C.c_int]),

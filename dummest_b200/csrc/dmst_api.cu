@@ -99,7 +99,10 @@ struct DevBuf {
     cudaError_t ensure(size_t n, double headroom = 0.0) {
         if (n <= cap && p) return cudaSuccess;
         const size_t want = std::max<size_t>({n, cap + cap / 4, (size_t)((double)n * (1.0 + headroom)), 1});
-        if (p) cudaFree(p);
+        if (p) {
+            cudaDeviceSynchronize();  // no call in flight still reads the old buffer
+            cudaFree(p);
+        }
         p = nullptr;
         cap = 0;
         cudaError_t e = cudaMalloc(&p, want * sizeof(T));
@@ -134,6 +137,28 @@ struct DevBuf {
     }
     void release() {
         if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Page-locked host staging (uploads and downloads that run asynchronously).
+template <class T>
+struct PinnedBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        const size_t want = std::max<size_t>({n, cap + cap / 2, 64});
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMallocHost((void **)&p, want * sizeof(T));
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
         p = nullptr;
         cap = 0;
     }
@@ -222,6 +247,43 @@ int rowsPerLane(int M, int forced, const Tuning &t) {
 
 }  // namespace
 
+// The per-call state of a scoring call in flight.  A context has two, so
+// that one call's host work overlaps the other's device work: the buffers the
+// call reads after its DP kernels (pairs, seeds, scales, for the exact path)
+// and its page-locked staging are per slot; buffers used only by the call's
+// own stream-ordered kernels are shared.
+struct CallSlot {
+    DevBuf<DevPair> dPairs;
+    DevBuf<float> dSeeds;
+    DevBuf<PairScales> dScales;
+    DevBuf<PairOut> dOut;
+    DevBuf<ExactOut> dExOut;  // exact-path results, by pair position
+    DevBuf<int> dQueue;       // exact-path queue, by queue position
+    DevBuf<int> dQueueCount;  // [0] queued pairs, [1] next queue position
+    PinnedBuf<DevPair> hPairs;
+    PinnedBuf<Chunk> hChunks;
+    PinnedBuf<NullJob> hNullJobs;
+    PinnedBuf<int> hJobPairs;
+    PinnedBuf<long long> hNullTmpOff;
+    PinnedBuf<PairOut> hOut;
+    PinnedBuf<ExactOut> hExOut;
+    cudaEvent_t ev[5] = {};  // null start, DP start, DP end, exact end, results copied
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<uintptr_t> graphKey;
+    int graphLaunches = 0;
+    // the pending call
+    bool pending = false;
+    size_t n = 0;
+    int mode = 0;
+    bool mid = false, nullOnly = false, sequentialExact = false, exactOnDevice = false;
+    dmst_result *out = nullptr;
+    std::vector<int> order;
+    std::vector<DevPair> dp;
+    int launches = 0;
+    double hostMs = 0;
+    std::chrono::steady_clock::time_point t0;
+};
+
 struct dmst_ctx {
     dmst_opts opts;
     Rates rates;
@@ -252,24 +314,24 @@ struct dmst_ctx {
     DevBuf<long long> dStageOff;
     DevBuf<int> dStageLen;
 
-    // per call
-    DevBuf<DevPair> dPairs;
-    DevBuf<float> dSeeds;
+    // per call (shared by the slots: used only by a call's stream-ordered kernels)
     DevBuf<XS> dNullTmp;
     DevBuf<NullJob> dNullJobs;
     DevBuf<int> dNullJobPairs;
     DevBuf<long long> dNullTmpOff;
-    DevBuf<PairScales> dScales;
-    DevBuf<PairOut> dOut;
     DevBuf<Chunk> dChunks;
     DevBuf<int> dCounter;
     DevBuf<float> dW1, dRing;
     DevBuf<ExactJob> dJobs;
-    DevBuf<ExactWaveJob> dWaveJobs;
     DevBuf<AdjointJob> dAdjJobs;             // dmst_loglik_grad, dmst_posteriors
     DevBuf<double> dPost;                    // dmst_posteriors: the batch's posterior tables
     DevBuf<double> dAdjF, dAdjB, dGrad, dLogT;
     std::vector<int> lastOrder;              // sorted position -> caller's pair index of the last call
+    CallSlot slot[2];
+    int nextSlot = 0;                        // the slot the next submit uses
+    int oldest = 0;                          // the oldest pending call's slot
+    int lastSlot = 0;                        // the slot of the last completed call
+    DevBuf<float> dExactPool;                // exact-path scratch: one slot per CTA
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
 
@@ -303,6 +365,8 @@ struct dmst_ctx {
     } while (0)
 
 extern "C" {
+
+static int drainCalls(dmst_ctx *ctx);
 
 void dmst_opts_default(dmst_opts *o) {
     if (!o) return;
@@ -359,6 +423,8 @@ int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out) {
         return DMST_EDEVICE;
     }
     for (auto &e : ctx->ev) cudaEventCreate(&e);
+    for (auto &sl : ctx->slot)
+        for (auto &e : sl.ev) cudaEventCreate(&e);
     uint8_t table[64];
     standardCodeTable(table);
     if (cudaMemcpyToSymbol(cCodonTable, table, 64) != cudaSuccess) {
@@ -374,6 +440,26 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
+    for (auto &sl : ctx->slot) {
+        if (sl.graphExec) cudaGraphExecDestroy(sl.graphExec);
+        sl.dPairs.release();
+        sl.dSeeds.release();
+        sl.dScales.release();
+        sl.dOut.release();
+        sl.dExOut.release();
+        sl.dQueue.release();
+        sl.dQueueCount.release();
+        sl.hPairs.release();
+        sl.hChunks.release();
+        sl.hNullJobs.release();
+        sl.hJobPairs.release();
+        sl.hNullTmpOff.release();
+        sl.hOut.release();
+        sl.hExOut.release();
+        for (auto &e : sl.ev)
+            if (e) cudaEventDestroy(e);
+    }
+    ctx->dExactPool.release();
     ctx->dEmit.release();
     ctx->dParams.release();
     ctx->dProfiles.release();
@@ -381,20 +467,15 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dStage.release();
     ctx->dStageOff.release();
     ctx->dStageLen.release();
-    ctx->dPairs.release();
-    ctx->dSeeds.release();
     ctx->dNullTmp.release();
     ctx->dNullJobs.release();
     ctx->dNullJobPairs.release();
     ctx->dNullTmpOff.release();
-    ctx->dScales.release();
-    ctx->dOut.release();
     ctx->dChunks.release();
     ctx->dCounter.release();
     ctx->dW1.release();
     ctx->dRing.release();
     ctx->dJobs.release();
-    ctx->dWaveJobs.release();
     ctx->dAdjJobs.release();
     ctx->dAdjF.release();
     ctx->dAdjB.release();
@@ -667,6 +748,10 @@ int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *m
 }
 
 int dmst_seqs_clear(dmst_ctx *ctx) {
+    if (ctx && ctx->slot[ctx->oldest].pending) {  // pending calls read the sequences being dropped
+        const int ds = drainCalls(ctx);
+        if (ds) return ds;
+    }
     if (!ctx) return DMST_EINVAL;
     ctx->seqOff.clear();
     ctx->seqLen.clear();
@@ -743,7 +828,9 @@ static float elapsedMs(dmst_ctx *ctx, cudaEvent_t a, cudaEvent_t b) {
 // device pair descriptors, seeds and scales of the call stay in the context).
 constexpr int kModeNullOnly = 0x10000;
 
-int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
+// Host setup, uploads and the launches of a call into slot ctx->nextSlot
+// (which must be free); the call completes in completeCall.
+static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
     const bool nullOnly = (mode & kModeNullOnly) != 0;
     if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
     const int base = mode & 0xff;
@@ -752,12 +839,10 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     const bool sequentialExact = (mode & DMST_MODE_EXACT_SEQUENTIAL) != 0;
     if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
     const bool mid = base == DMST_MODE_MID;
-    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = ctx->lastExactMs = ctx->lastHostMs = 0;
-    ctx->lastPostMs = ctx->lastWallMs = 0;
-    ctx->lastLaunches = 0;
-    ctx->lastExactPairs = 0;
     const auto hostT0 = std::chrono::steady_clock::now();
-    if (n == 0) return DMST_OK;
+    const int si = ctx->nextSlot;
+    CallSlot &S = ctx->slot[si];
+    if (S.pending) return ctx->fail(DMST_EINVAL, "scoring call: no free slot");
     if (n > (size_t)INT32_MAX / 2) return ctx->fail(DMST_ERANGE, "too many pairs");
     CK(cudaSetDevice(ctx->device), "set device");
     int st = uploadProfiles(ctx);
@@ -820,7 +905,6 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
             }
         }
     }
-    ctx->lastOrder = order;
     std::vector<DevPair> dp(n);
     long long seedFloats = 0;
     size_t w1Max = 0, ringMax = 0;
@@ -960,17 +1044,22 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         slotsMax = std::max(slotsMax, (size_t)G.grid * G.warps);
     }
 
-    CK(ctx->dPairs.ensure(n), "alloc pairs");
-    CK(ctx->dSeeds.ensure((size_t)seedFloats), "alloc seeds");
-    CK(ctx->dScales.ensure(n), "alloc scales");
-    CK(ctx->dOut.ensure(n), "alloc out");
+    // Uploads go through the slot's page-locked staging, so that they queue
+    // behind the previous call's kernels without waiting for them.
+    auto upload = [&](auto &pinned, auto *dst, const auto *src, size_t cnt, const char *what) -> int {
+        if (!cnt) return DMST_OK;
+        CK(pinned.ensure(cnt), what);
+        std::memcpy(pinned.p, src, cnt * sizeof(*src));
+        CK(cudaMemcpyAsync(dst, pinned.p, cnt * sizeof(*src), cudaMemcpyHostToDevice, ctx->stream), what);
+        return DMST_OK;
+    };
+    CK(S.dPairs.ensure(n), "alloc pairs");
+    CK(S.dSeeds.ensure((size_t)seedFloats), "alloc seeds");
+    CK(S.dScales.ensure(n), "alloc scales");
+    CK(S.dOut.ensure(n), "alloc out");
     CK(ctx->dChunks.ensure(allChunks.size()), "alloc chunks");
-    CK(cudaMemcpyAsync(ctx->dPairs.p, dp.data(), n * sizeof(DevPair), cudaMemcpyHostToDevice, ctx->stream),
-       "upload pairs");
-    if (!allChunks.empty())
-        CK(cudaMemcpyAsync(ctx->dChunks.p, allChunks.data(), allChunks.size() * sizeof(Chunk),
-                           cudaMemcpyHostToDevice, ctx->stream),
-           "upload chunks");
+    if ((st = upload(S.hPairs, S.dPairs.p, dp.data(), n, "upload pairs"))) return st;
+    if ((st = upload(S.hChunks, ctx->dChunks.p, allChunks.data(), allChunks.size(), "upload chunks"))) return st;
     // The groups run one after another on the stream, so they share the slots.
     CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
@@ -1002,34 +1091,59 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     CK(ctx->dNullJobPairs.ensure(n), "alloc null jobs");
     CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries), "alloc null tmp");
     CK(ctx->dNullTmpOff.ensure(nullJobs.size()), "alloc null tmp");
-    CK(cudaMemcpyAsync(ctx->dNullJobs.p, nullJobs.data(), nullJobs.size() * sizeof(NullJob), cudaMemcpyHostToDevice,
-                       ctx->stream),
-       "upload null jobs");
-    CK(cudaMemcpyAsync(ctx->dNullJobPairs.p, jobPairs.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
-       "upload null jobs");
-    CK(cudaMemcpyAsync(ctx->dNullTmpOff.p, nullTmpOff.data(), nullTmpOff.size() * sizeof(long long),
-                       cudaMemcpyHostToDevice, ctx->stream),
-       "upload null jobs");
+    if ((st = upload(S.hNullJobs, ctx->dNullJobs.p, nullJobs.data(), nullJobs.size(), "upload null jobs"))) return st;
+    if ((st = upload(S.hJobPairs, ctx->dNullJobPairs.p, jobPairs.data(), n, "upload null jobs"))) return st;
+    if ((st = upload(S.hNullTmpOff, ctx->dNullTmpOff.p, nullTmpOff.data(), nullTmpOff.size(), "upload null jobs")))
+        return st;
 
-    ctx->lastHostMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostT0).count();
+    // The exact path on the device: flagged pairs go to a queue that
+    // persistent CTAs of the exact kernel drain, each CTA with a scratch slot
+    // sized for the largest pair of the call.
+    const bool exactOnDevice = mid && !nullOnly && !sequentialExact;
+    long long poolSlot = 0;
+    int exactGrid = 0;
+    if (exactOnDevice) {
+        for (size_t k = 0; k < n; ++k)
+            poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L, exactWarps(dp[k].M)));
+        poolSlot = (poolSlot + 63) / 64 * 64;
+        size_t freeB = 0, totalB = 0;
+        CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+        const size_t poolBudget = std::max<size_t>((freeB + ctx->dExactPool.cap * sizeof(float)) / 4, (size_t)256 << 20);
+        exactGrid = (int)std::max<size_t>(
+            1, std::min<size_t>((size_t)ctx->smCount, poolBudget / ((size_t)poolSlot * sizeof(float))));
+        CK(ctx->dExactPool.ensure((size_t)exactGrid * poolSlot), "alloc exact scratch");
+        CK(S.dExOut.ensure(n), "alloc exact out");
+        CK(S.dQueue.ensure(n), "alloc exact queue");
+        CK(S.dQueueCount.ensure(2), "alloc exact queue");
+        CK(S.hExOut.ensure(n), "alloc exact out");
+        if (!ctx->exactAttrSet) {
+            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
+            ctx->exactAttrSet = true;
+        }
+    }
+    CK(S.hOut.ensure(n), "alloc results");
+
+    S.hostMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostT0).count();
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
     const int nj = (int)nullJobs.size();
     const int nullBlocks = std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * 16));
     DpArgs g;
-    g.pairs = ctx->dPairs.p;
+    g.pairs = S.dPairs.p;
     g.profiles = ctx->dProfiles.p;
     g.emit = ctx->dEmit.p;
     g.params = ctx->dParams.p;
     g.codes = ctx->dCodes.p;
-    g.seeds = ctx->dSeeds.p;
-    g.scales = ctx->dScales.p;
+    g.seeds = S.dSeeds.p;
+    g.scales = S.dScales.p;
     g.w1 = ctx->dW1.p;
     g.w1SlotFloats = w1Slot;
     g.ring = ctx->dRing.p;
     g.ringSlotFloats = ringSlot;
-    g.out = ctx->dOut.p;
+    g.out = S.dOut.p;
     // The device work of the call up to the DP results: counter reset,
     // null-model kernel, the DP kernels of each rows-per-lane group, and the
     // timing events between them.
@@ -1044,13 +1158,14 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     auto enqueue = [&]() -> int {
         launches = 0;
         CK(cudaMemsetAsync(ctx->dCounter.p, 0, nCounters * sizeof(int), ctx->stream), "zero counters");
-        CK(record(ctx->ev[0]), "event");
+        if (exactOnDevice) CK(cudaMemsetAsync(S.dQueueCount.p, 0, 2 * sizeof(int), ctx->stream), "zero queue");
+        CK(record(S.ev[0]), "event");
         nullModelKernel<<<nullBlocks, kNullWarps * 32, 0, ctx->stream>>>(
-            ctx->dNullJobs.p, nj, ctx->dNullJobPairs.p, ctx->dPairs.p, ctx->dProfiles.p, ctx->dCodes.p,
-            ctx->dSeeds.p, ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+            ctx->dNullJobs.p, nj, ctx->dNullJobPairs.p, S.dPairs.p, ctx->dProfiles.p, ctx->dCodes.p,
+            S.dSeeds.p, ctx->dNullTmp.p, ctx->dNullTmpOff.p, S.dScales.p, nr);
         CK(cudaGetLastError(), "null-model kernel");
         ++launches;
-        CK(record(ctx->ev[1]), "event");
+        CK(record(S.ev[1]), "event");
         if (!forceExact && !nullOnly) {
             for (int gi = 0; gi < 3; ++gi) {
                 Group &G = groups[gi];
@@ -1076,28 +1191,51 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                 CK(cudaGetLastError(), "DP kernel");
             }
         }
-        CK(record(ctx->ev[2]), "event");
+        CK(record(S.ev[2]), "event");
+        if (exactOnDevice) {
+            flagKernel<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(S.dOut.p, (int)n, forceExact ? 1 : 0,
+                                                                        S.dQueue.p, S.dQueueCount.p);
+            CK(cudaGetLastError(), "flag kernel");
+            exactWaveKernel<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), ctx->stream>>>(
+                S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+                ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p);
+            CK(cudaGetLastError(), "exact kernel");
+            launches += 2;
+        }
+        CK(record(S.ev[3]), "event");
+        if (!nullOnly) {
+            CK(cudaMemcpyAsync(S.hOut.p, S.dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
+               "download results");
+            if (exactOnDevice)
+                CK(cudaMemcpyAsync(S.hExOut.p, S.dExOut.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost,
+                                   ctx->stream),
+                   "download exact results");
+        }
         return DMST_OK;
     };
-    if ((mode & DMST_MODE_GRAPH) && !plain && !nullOnly) {
+    if ((mode & DMST_MODE_GRAPH) && !plain && !nullOnly && !sequentialExact) {
         // Replay the captured graph when the launch shape and the buffers are
         // those of the last capture; otherwise capture again and update the
         // executable graph (or instantiate a new one).
         std::vector<uintptr_t> key = {(uintptr_t)nCounters, (uintptr_t)nj, (uintptr_t)nullBlocks,
                                       (uintptr_t)forceExact, (uintptr_t)ctx->dCounter.p, (uintptr_t)ctx->dNullJobs.p,
-                                      (uintptr_t)ctx->dNullJobPairs.p, (uintptr_t)ctx->dPairs.p,
-                                      (uintptr_t)ctx->dProfiles.p, (uintptr_t)ctx->dCodes.p, (uintptr_t)ctx->dSeeds.p,
+                                      (uintptr_t)ctx->dNullJobPairs.p, (uintptr_t)S.dPairs.p,
+                                      (uintptr_t)ctx->dProfiles.p, (uintptr_t)ctx->dCodes.p, (uintptr_t)S.dSeeds.p,
                                       (uintptr_t)ctx->dNullTmp.p, (uintptr_t)ctx->dNullTmpOff.p,
-                                      (uintptr_t)ctx->dScales.p, (uintptr_t)ctx->dEmit.p, (uintptr_t)ctx->dParams.p,
-                                      (uintptr_t)ctx->dW1.p, (uintptr_t)ctx->dRing.p, (uintptr_t)ctx->dOut.p,
-                                      (uintptr_t)ctx->dChunks.p, (uintptr_t)w1Slot, (uintptr_t)ringSlot};
+                                      (uintptr_t)S.dScales.p, (uintptr_t)ctx->dEmit.p, (uintptr_t)ctx->dParams.p,
+                                      (uintptr_t)ctx->dW1.p, (uintptr_t)ctx->dRing.p, (uintptr_t)S.dOut.p,
+                                      (uintptr_t)ctx->dChunks.p, (uintptr_t)w1Slot, (uintptr_t)ringSlot,
+                                      (uintptr_t)n, (uintptr_t)exactOnDevice, (uintptr_t)forceExact,
+                                      (uintptr_t)exactGrid, (uintptr_t)poolSlot, (uintptr_t)ctx->dExactPool.p,
+                                      (uintptr_t)S.dExOut.p, (uintptr_t)S.dQueue.p, (uintptr_t)S.dQueueCount.p,
+                                      (uintptr_t)S.hOut.p, (uintptr_t)S.hExOut.p};
         for (const Group &G : groups) {
             const uintptr_t v[8] = {(uintptr_t)G.kern, (uintptr_t)G.grid,         (uintptr_t)G.warps,
                                     (uintptr_t)G.smem, (uintptr_t)G.chunks.size(), (uintptr_t)G.chunkBase,
                                     (uintptr_t)G.maxRowPad, (uintptr_t)G.kernWarps};
             key.insert(key.end(), v, v + 8);
         }
-        if (!ctx->graphExec || key != ctx->graphKey) {
+        if (!S.graphExec || key != S.graphKey) {
             cudaGraph_t graph = nullptr;
             CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
             capturing = true;
@@ -1109,35 +1247,74 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
                 return st;
             }
             CK(ce, "end capture");
-            if (ctx->graphExec) {
+            if (S.graphExec) {
                 cudaGraphExecUpdateResultInfo info;
-                if (cudaGraphExecUpdate(ctx->graphExec, graph, &info) != cudaSuccess) {
+                if (cudaGraphExecUpdate(S.graphExec, graph, &info) != cudaSuccess) {
                     cudaGetLastError();
-                    cudaGraphExecDestroy(ctx->graphExec);
-                    ctx->graphExec = nullptr;
+                    cudaGraphExecDestroy(S.graphExec);
+                    S.graphExec = nullptr;
                 }
             }
             cudaError_t ie = cudaSuccess;
-            if (!ctx->graphExec) ie = cudaGraphInstantiate(&ctx->graphExec, graph, 0);
+            if (!S.graphExec) ie = cudaGraphInstantiate(&S.graphExec, graph, 0);
             cudaGraphDestroy(graph);
             CK(ie, "instantiate graph");
-            ctx->graphKey = key;
-            ctx->graphLaunches = launches;
+            S.graphKey = key;
+            S.graphLaunches = launches;
             ++ctx->graphCaptures;
         }
-        CK(cudaGraphLaunch(ctx->graphExec, ctx->stream), "graph launch");
-        launches = ctx->graphLaunches;
+        CK(cudaGraphLaunch(S.graphExec, ctx->stream), "graph launch");
+        launches = S.graphLaunches;
     } else {
         const int st = enqueue();
         if (st) return st;
     }
-    std::vector<PairOut> po(nullOnly ? 0 : n);
-    if (!forceExact && !nullOnly)
-        CK(cudaMemcpyAsync(po.data(), ctx->dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
-           "download results");
-    CK(cudaStreamSynchronize(ctx->stream), "DP kernel");
-    if (nullOnly) return DMST_OK;
+    CK(cudaEventRecord(S.ev[4], ctx->stream), "event");
+    S.pending = true;
+    S.n = n;
+    S.mode = mode;
+    S.mid = mid;
+    S.nullOnly = nullOnly;
+    S.sequentialExact = sequentialExact;
+    S.exactOnDevice = exactOnDevice;
+    S.out = out;
+    S.order.swap(order);
+    S.dp.swap(dp);
+    S.launches = launches;
+    S.t0 = hostT0;
+    ctx->nextSlot = si ^ 1;
+    return DMST_OK;
+}
 
+// Waits for the oldest pending call and writes its results.
+static int completeCall(dmst_ctx *ctx) {
+    const int si = ctx->oldest;
+    CallSlot &S = ctx->slot[si];
+    if (!S.pending) return DMST_OK;
+    S.pending = false;
+    ctx->oldest = si ^ 1;
+    ctx->lastSlot = si;
+    ctx->lastOrder = S.order;
+    const size_t n = S.n;
+    const bool mid = S.mid, nullOnly = S.nullOnly;
+    const bool forceExact = (S.mode & (DMST_MODE_FORCE_EXACT | DMST_MODE_EXACT_SEQUENTIAL)) != 0;
+    const std::vector<int> &order = S.order;
+    const std::vector<DevPair> &dp = S.dp;
+    dmst_result *out = S.out;
+    int launches = S.launches;
+    const auto hostT0 = S.t0;
+    ctx->lastHostMs = S.hostMs;
+    ctx->lastExactMs = 0;
+    ctx->lastExactPairs = 0;
+    CK(cudaEventSynchronize(S.ev[4]), "scoring kernels");
+    if (nullOnly) {
+        ctx->lastNullMs = elapsedMs(ctx, S.ev[0], S.ev[1]);
+        ctx->lastDpMs = 0;
+        ctx->lastTotalMs = ctx->lastNullMs;
+        ctx->lastLaunches = launches;
+        return DMST_OK;
+    }
+    const PairOut *po = S.hOut.p;
     // Pairs outside the fast path's exact range go to the row-rescaled kernel.
     std::vector<int> flagged;
     for (size_t k = 0; k < n; ++k) {
@@ -1149,64 +1326,41 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     }
     std::vector<ExactOut> eo;
     float exactMs = 0;
-    if (!flagged.empty()) {
-        // Batch the flagged pairs under a scratch budget.
+    if (S.exactOnDevice) {
+        exactMs = elapsedMs(ctx, S.ev[2], S.ev[3]);
+        eo.resize(flagged.size());
+        for (size_t f = 0; f < flagged.size(); ++f) eo[f] = S.hExOut.p[flagged[f]];
+    } else if (!flagged.empty()) {
+        // The one-thread-per-pair restatement (DMST_MODE_EXACT_SEQUENTIAL), in
+        // batches under a scratch budget.
         size_t free = 0, total = 0;
         cudaMemGetInfo(&free, &total);
         const size_t budget = std::max<size_t>(free / 2, (size_t)256 << 20);
         eo.resize(flagged.size());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
-        const size_t pipeSmem = kPipeWarps * sizeof(Window);
-        if (!sequentialExact && !ctx->exactAttrSet) {
-            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pipeSmem),
-               "smem attribute");
-            ctx->exactAttrSet = true;
-        }
         size_t i0 = 0;
         while (i0 < flagged.size()) {
             std::vector<ExactJob> jobs;
-            std::vector<ExactWaveJob> wjobs;
             long long used = 0;
             size_t i1 = i0;
             while (i1 < flagged.size()) {
                 const DevPair &d = dp[flagged[i1]];
-                // warps per pair: one per stripe, at most kPipeWarps
-                const int nS = (d.M + 1 + kLanes * kExactR - 1) / (kLanes * kExactR);
-                const int W = std::min(nS, kPipeWarps);
-                long long need = sequentialExact ? exactScratchFloats(d.M, d.L) : exactWaveScratch(d.M, d.L, W);
-                need = (need + 63) / 64 * 64;
+                long long need = (exactScratchFloats(d.M, d.L) + 63) / 64 * 64;
                 if (i1 > i0 && (size_t)(used + need) * 4 > budget) break;
-                if (sequentialExact)
-                    jobs.push_back(ExactJob{flagged[i1], used});
-                else
-                    wjobs.push_back(ExactWaveJob{flagged[i1], W, used});
+                jobs.push_back(ExactJob{flagged[i1], used});
                 used += need;
                 ++i1;
             }
             const size_t nj = i1 - i0;
-            // the flagged pairs change from call to call: 50% headroom
             CK(ctx->dExactScratch.ensure((size_t)used, 0.5), "alloc exact scratch");
             CK(ctx->dExactOut.ensure(nj), "alloc exact out");
-            if (sequentialExact) {
-                CK(ctx->dJobs.ensure(nj), "alloc exact jobs");
-                CK(cudaMemcpyAsync(ctx->dJobs.p, jobs.data(), nj * sizeof(ExactJob), cudaMemcpyHostToDevice,
-                                   ctx->stream),
-                   "upload jobs");
-                const int tpb = 32;
-                exactKernel<<<(int)((nj + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
-                    ctx->dJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
-            } else {
-                CK(ctx->dWaveJobs.ensure(nj), "alloc exact jobs");
-                CK(cudaMemcpyAsync(ctx->dWaveJobs.p, wjobs.data(), nj * sizeof(ExactWaveJob),
-                                   cudaMemcpyHostToDevice, ctx->stream),
-                   "upload jobs");
-                // one CTA per SM (255 registers x 256 threads), persistent over the jobs
-                const int blocks = (int)std::min<size_t>(nj, (size_t)ctx->smCount);
-                exactWaveKernel<<<blocks, kPipeWarps * kLanes, pipeSmem, ctx->stream>>>(
-                    ctx->dWaveJobs.p, (int)nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                    ctx->dCodes.p, ctx->dSeeds.p, ctx->dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
-            }
+            CK(ctx->dJobs.ensure(nj), "alloc exact jobs");
+            CK(cudaMemcpyAsync(ctx->dJobs.p, jobs.data(), nj * sizeof(ExactJob), cudaMemcpyHostToDevice, ctx->stream),
+               "upload jobs");
+            const int tpb = 32;
+            exactKernel<<<(int)((nj + tpb - 1) / tpb), tpb, 0, ctx->stream>>>(
+                ctx->dJobs.p, (int)nj, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
+                S.dSeeds.p, S.dScales.p, ctx->dExactScratch.p, ctx->dExactOut.p);
             CK(cudaGetLastError(), "exact kernel");
             ++launches;
             CK(cudaMemcpyAsync(eo.data() + i0, ctx->dExactOut.p, nj * sizeof(ExactOut), cudaMemcpyDeviceToHost,
@@ -1218,17 +1372,17 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
         CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
         CK(cudaEventSynchronize(ctx->ev[4]), "event");
         exactMs = elapsedMs(ctx, ctx->ev[3], ctx->ev[4]);
-        for (size_t f = 0; f < eo.size(); ++f)
-            if (eo[f].failed)
-                return ctx->fail(DMST_ETIMEOUT, "exact path: the stripe pipeline of pair %d gave up a wait",
-                                 order[flagged[f]]);
     }
+    for (size_t f = 0; f < eo.size(); ++f)
+        if (eo[f].failed)
+            return ctx->fail(DMST_ETIMEOUT, "exact path: the stripe pipeline of pair %d gave up a wait",
+                             order[flagged[f]]);
     ctx->lastExactMs = exactMs;
     ctx->lastExactPairs = (int)flagged.size();
 
     float nullMs = 0, dpMs = 0;
-    nullMs = elapsedMs(ctx, ctx->ev[0], ctx->ev[1]);
-    dpMs = elapsedMs(ctx, ctx->ev[1], ctx->ev[2]);
+    nullMs = elapsedMs(ctx, S.ev[0], S.ev[1]);
+    dpMs = elapsedMs(ctx, S.ev[1], S.ev[2]);
     ctx->lastNullMs = nullMs;
     ctx->lastDpMs = dpMs;
     ctx->lastTotalMs = nullMs + dpMs + exactMs;
@@ -1261,6 +1415,63 @@ int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, 
     ctx->lastPostMs = std::chrono::duration<double, std::milli>(endT - postT0).count();
     ctx->lastWallMs = std::chrono::duration<double, std::milli>(endT - hostT0).count();
     return DMST_OK;
+}
+
+// Completes every pending call (before anything that changes what pending
+// calls read: sequences, profiles, the shared buffers of another entry point).
+static int drainCalls(dmst_ctx *ctx) {
+    int first = DMST_OK;
+    while (ctx->slot[ctx->oldest].pending) {
+        const int st = completeCall(ctx);
+        if (st && !first) first = st;
+    }
+    return first;
+}
+
+int dmst_score_pairs_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
+    const bool nullOnly = (mode & kModeNullOnly) != 0;
+    if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
+    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = ctx->lastExactMs = ctx->lastHostMs = 0;
+    ctx->lastPostMs = ctx->lastWallMs = 0;
+    ctx->lastLaunches = 0;
+    ctx->lastExactPairs = 0;
+    if (n == 0) return DMST_OK;
+    // Modes that run the exact path on the host, or profiles to re-upload,
+    // need the pending calls done first; otherwise a third call waits for
+    // the oldest.
+    if ((mode & DMST_MODE_EXACT_SEQUENTIAL) || ctx->profilesDirty) {
+        const int st = drainCalls(ctx);
+        if (st) return st;
+    }
+    if (ctx->slot[ctx->nextSlot].pending) {
+        const int st = completeCall(ctx);
+        if (st) return st;
+    }
+    const int st = submitCall(ctx, pairs, n, mode, out);
+    if (st) {
+        // a failed submit leaves nothing pending in its slot; drop the others' launches too
+        drainCalls(ctx);
+    }
+    return st;
+}
+
+int dmst_score_pairs_complete(dmst_ctx *ctx) {
+    if (!ctx) return DMST_EINVAL;
+    return completeCall(ctx);
+}
+
+int dmst_pending_calls(const dmst_ctx *ctx) {
+    return ctx ? (int)ctx->slot[0].pending + (int)ctx->slot[1].pending : 0;
+}
+
+int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
+    if (!ctx) return DMST_EINVAL;
+    int st = drainCalls(ctx);
+    if (st) return st;
+    ctx->nextSlot = ctx->oldest = 0;  // nothing pending: synchronous calls share slot 0 (and its graph)
+    st = dmst_score_pairs_submit(ctx, pairs, n, mode, out);
+    if (st || n == 0) return st;
+    return completeCall(ctx);
 }
 
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n) {
@@ -1340,7 +1551,8 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     const auto wallT0 = std::chrono::steady_clock::now();
     int st = dmst_score_pairs(ctx, pairs, n, DMST_MODE_MID | kModeNullOnly, nullptr);
     if (st) return st;
-    const double nullMs = elapsedMs(ctx, ctx->ev[0], ctx->ev[1]);
+    CallSlot &S = ctx->slot[ctx->lastSlot];  // the pairs, seeds and scales of that call
+    const double nullMs = elapsedMs(ctx, S.ev[0], S.ev[1]);
     double adjMs = 0.0;
     int launches = 1;
     const std::vector<int> order = ctx->lastOrder;
@@ -1398,8 +1610,8 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjSmem), "smem attribute");
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         kern<<<blocks, kAdjWarps * 32, kAdjSmem, ctx->stream>>>(
-            ctx->dAdjJobs.p, nj, ctx->dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
-            ctx->dSeeds.p, ctx->dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
+            ctx->dAdjJobs.p, nj, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
+            S.dSeeds.p, S.dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
             post ? ctx->dPost.p : nullptr);
         CK(cudaGetLastError(), "adjoint kernel");
         CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
@@ -1453,7 +1665,9 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
     if (!ctx || seq < 0 || seq >= (int)ctx->seqLen.size() || profile < 0 || profile >= (int)ctx->profiles.size())
         return DMST_EINVAL;
     CK(cudaSetDevice(ctx->device), "set device");
-    int st = uploadProfiles(ctx);
+    int st = drainCalls(ctx);
+    if (st) return st;
+    st = uploadProfiles(ctx);
     if (st) return st;
     DevPair d;
     d.codeOff = ctx->seqOff[seq];
@@ -1465,29 +1679,29 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
     long long zero = 0;
     const int pairIndex = 0;
     const NullJob job{0, 1};
-    CK(ctx->dPairs.ensure(1), "alloc");
-    CK(ctx->dSeeds.ensure(2 * (size_t)d.L), "alloc");
+    CK(ctx->slot[0].dPairs.ensure(1), "alloc");
+    CK(ctx->slot[0].dSeeds.ensure(2 * (size_t)d.L), "alloc");
     CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries(d.L)), "alloc");
     CK(ctx->dNullTmpOff.ensure(1), "alloc");
     CK(ctx->dNullJobs.ensure(1), "alloc");
     CK(ctx->dNullJobPairs.ensure(1), "alloc");
-    CK(ctx->dScales.ensure(1), "alloc");
-    CK(cudaMemcpy(ctx->dPairs.p, &d, sizeof d, cudaMemcpyHostToDevice), "upload");
+    CK(ctx->slot[0].dScales.ensure(1), "alloc");
+    CK(cudaMemcpy(ctx->slot[0].dPairs.p, &d, sizeof d, cudaMemcpyHostToDevice), "upload");
     CK(cudaMemcpy(ctx->dNullTmpOff.p, &zero, sizeof zero, cudaMemcpyHostToDevice), "upload");
     CK(cudaMemcpy(ctx->dNullJobs.p, &job, sizeof job, cudaMemcpyHostToDevice), "upload");
     CK(cudaMemcpy(ctx->dNullJobPairs.p, &pairIndex, sizeof pairIndex, cudaMemcpyHostToDevice), "upload");
     NullRates nr;
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
-    nullModelKernel<<<1, kNullWarps * 32, 0, ctx->stream>>>(ctx->dNullJobs.p, 1, ctx->dNullJobPairs.p, ctx->dPairs.p,
-                                                           ctx->dProfiles.p, ctx->dCodes.p, ctx->dSeeds.p,
-                                                           ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->dScales.p, nr);
+    nullModelKernel<<<1, kNullWarps * 32, 0, ctx->stream>>>(ctx->dNullJobs.p, 1, ctx->dNullJobPairs.p, ctx->slot[0].dPairs.p,
+                                                           ctx->dProfiles.p, ctx->dCodes.p, ctx->slot[0].dSeeds.p,
+                                                           ctx->dNullTmp.p, ctx->dNullTmpOff.p, ctx->slot[0].dScales.p, nr);
     CK(cudaGetLastError(), "null-model kernel");
     CK(cudaStreamSynchronize(ctx->stream), "null-model kernel");
     std::vector<float> s(2 * (size_t)d.L);
     PairScales sc;
-    CK(cudaMemcpy(s.data(), ctx->dSeeds.p, s.size() * 4, cudaMemcpyDeviceToHost), "download");
-    CK(cudaMemcpy(&sc, ctx->dScales.p, sizeof sc, cudaMemcpyDeviceToHost), "download");
+    CK(cudaMemcpy(s.data(), ctx->slot[0].dSeeds.p, s.size() * 4, cudaMemcpyDeviceToHost), "download");
+    CK(cudaMemcpy(&sc, ctx->slot[0].dScales.p, sizeof sc, cudaMemcpyDeviceToHost), "download");
     if (prefix_seed) std::memcpy(prefix_seed, s.data(), (size_t)d.L * 4);
     if (suffix_seed) std::memcpy(suffix_seed, s.data() + d.L, (size_t)d.L * 4);
     if (scales3) {

@@ -84,12 +84,6 @@ __device__ void scanCounts(const float *rowMax, const int *rowCnt, int *cnt, int
     }
 }
 
-struct ExactWaveJob {
-    int pair;
-    int warps;             // warps running the pair's stripes (<= kPipeWarps)
-    long long scratchOff;  // float offset of this job's scratch
-};
-
 constexpr int kPipeWarps = 8;        // warps per CTA of the exact path
 constexpr int kPipeExtra = 128;      // stripe period P' = P + kPipeExtra
 constexpr int kPipeSpinLimit = 1 << 24;  // iterations of a wait (64 ns sleeps) before it gives up
@@ -269,32 +263,58 @@ __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int 
     return ok;
 }
 
-// One CTA of kPipeWarps warps per pair (persistent over the jobs); dynamic
-// shared memory = one Window per warp.  The emission table is read from
-// global memory (a stripe's 32 R rows x 25 codes stay in L1), so tall
+// Warps running a pair's stripes: one per stripe, at most kPipeWarps.
+__host__ __device__ inline int exactWarps(int M) {
+    const int nS = (M + 1 + kLanes * kExactR - 1) / (kLanes * kExactR);
+    return nS < kPipeWarps ? nS : kPipeWarps;
+}
+
+// Pairs the fast kernel could not score exactly (a row maximum above
+// RESCALE_THRESH in either sweep, a score beyond float range, or a mid
+// product too small for a normal float), or every pair when force is set, go
+// to the queue of the exact path.  queueCount[0] counts them.
+__global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int *queueCount) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const PairOut o = po[k];
+    const bool ok = !force && o.maxYb <= kRescaleThresh && o.maxFw <= kRescaleThresh && o.mid < INFINITY &&
+                    o.filt < INFINITY && o.mid >= 0x1p-100f;
+    if (!ok) queue[atomicAdd(queueCount, 1)] = k;
+}
+
+// Persistent CTAs of kPipeWarps warps take the queued pairs one at a time
+// (queueCount[1] is the next queue position) and score each with its stripes
+// spread over the CTA's warps; CTA b uses scratch slot b (slotFloats floats).
+// Dynamic shared memory = one Window per warp.  The emission table is read
+// from global memory (a stripe's 32 R rows x 25 codes stay in L1), so tall
 // profiles leave the shared memory to the windows.
 __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
-    exactWaveKernel(const ExactWaveJob *jobs, int n, const DevPair *pairs, const DevProfile *profiles,
+    exactWaveKernel(const int *queue, int *queueCount, const DevPair *pairs, const DevProfile *profiles,
                     const float *emit, const float *params, const uint8_t *codes, const float *seeds,
-                    const PairScales *scales, float *scratch, ExactOut *out) {
+                    const PairScales *scales, float *pool, long long slotFloats, ExactOut *out) {
     extern __shared__ float4 smRaw[];
     Window *wins = reinterpret_cast<Window *>(smRaw);
     __shared__ float smBg[32];
     __shared__ int progress[kPipeWarps];
     __shared__ int abortFlag;
     __shared__ ExactBest bestF[kPipeWarps], bestM[kPipeWarps];
+    __shared__ int smNext;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Window &win = wins[warp];
     PipeSync ps;
     ps.progress = progress;
     ps.abort = &abortFlag;
-    for (int ji = blockIdx.x; ji < n; ji += gridDim.x) {
-        const ExactWaveJob job = jobs[ji];
-        const DevPair p = pairs[job.pair];
+    for (;;) {
+        __syncthreads();  // the previous pair is done with the shared state
+        if (threadIdx.x == 0) smNext = atomicAdd(queueCount + 1, 1);
+        __syncthreads();
+        const int qi = smNext;
+        if (qi >= queueCount[0]) break;
+        const int pi = queue[qi];
+        const DevPair p = pairs[pi];
         const DevProfile &pr = profiles[p.prof];
-        const int W = job.warps;
+        const int W = exactWarps(p.M);
         ps.W = W;
-        __syncthreads();  // the previous job is done with the shared state
         if (warp == 0) smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
         if (threadIdx.x == 0) abortFlag = 0;
         if (lane == 0) {
@@ -304,7 +324,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
             c.suf = c.pre + p.L;
             c.params = params + pr.paramOff;
             c.smBg = smBg;
-            c.sc = scales[job.pair];
+            c.sc = scales[pi];
             c.M = p.M;
             bestF[warp] = ExactBest{0.0, 0};
             bestM[warp] = ExactBest{0.0, 0};
@@ -323,7 +343,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         a.nMine = warp < W ? (a.nS - warp + W - 1) / W : 0;
         a.ringSlots = 2 * W;
         a.ringStride = 4LL * Pw;
-        float *base = scratch + job.scratchOff;
+        float *base = pool + (size_t)blockIdx.x * slotFloats;
         a.w1 = base;
         a.ring = base + (size_t)a.nS * a.D * kLanes * kExactR;
         ExactRows x;
@@ -367,7 +387,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
             o.mid = m.m == 0.0 ? xsZero() : XS{__double2float_rn(m.m), m.e};
             o.filt = f.m == 0.0 ? xsZero() : XS{__double2float_rn(f.m), f.e};
             o.failed = abortFlag != 0;
-            out[ji] = o;
+            out[pi] = o;
         }
     }
 }

@@ -71,6 +71,7 @@ class Context:
     """One device context (one per host thread)."""
 
     def __init__(self, device: int = 0, rates: dict | None = None, rows_per_lane: int = 0):
+        self._pending = []  # (pairs, results) of submitted calls, oldest first
         self.lib = F.load()
         o = default_opts()
         o.device = device
@@ -212,6 +213,31 @@ class Context:
         st = self.lib.dmst_score_pairs(self.h, pairs, n, mode, res)
         self._check(st, "dmst_score_pairs")
         return res
+
+    def submit_raw(self, pairs, mode: int) -> "C.Array":
+        """Queue a scoring call (dmst_score_pairs_submit); its ctypes Result
+        array is filled when the call completes (complete(), or a later
+        submit once two calls are pending).  The Pair array may be reused at
+        once; the Result array must be kept until then."""
+        n = len(pairs)
+        res = (F.Result * n)()
+        self._pending.append((pairs, res))
+        st = self.lib.dmst_score_pairs_submit(self.h, pairs, n, mode, res)
+        if st != F.DMST_OK:
+            self._pending.pop()
+        self._check(st, "dmst_score_pairs_submit")
+        while len(self._pending) > self.lib.dmst_pending_calls(self.h):
+            self._pending.pop(0)  # completed inside the submit
+        return res
+
+    def complete(self):
+        """Complete the oldest pending call (dmst_score_pairs_complete); returns its Result array."""
+        if not self._pending:
+            return None
+        st = self.lib.dmst_score_pairs_complete(self.h)
+        done = self._pending.pop(0)
+        self._check(st, "dmst_score_pairs_complete")
+        return done[1]
 
     def set_profile(self, pid: int, values: np.ndarray, params: np.ndarray, bg: np.ndarray) -> None:
         """Replace profile pid (dmst_profile_set); shapes as for add_profile."""

@@ -195,6 +195,23 @@ int dmst_encode_dna(const char *ascii, int L, char *letters);
  * with DMST_MODE_PLAIN / DMST_MODE_FORCE_EXACT.  Synchronous. */
 int dmst_score_pairs(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out);
 
+/* Asynchronous scoring.  dmst_score_pairs_submit does the host work of a call
+ * (sorting, descriptors, uploads through page-locked staging) and queues its
+ * device work: null model, DP kernels, the exact path (flagged pairs are
+ * queued and re-scored on the device) and the copy of the results back; it
+ * returns without waiting.  dmst_score_pairs_complete waits for the oldest
+ * pending call and writes its results into the `out` array given at submit
+ * (which must stay valid until then).  At most two calls are pending per
+ * context: a third submit completes the oldest first, so that the host work
+ * of one call overlaps the device work of the other.  Adding sequences or
+ * profiles, and every other entry point, completes the pending calls first.
+ * dmst_score_pairs is submit + complete.  The reference batches pairs
+ * synchronously per thread (dummest-search.hh:76-285). */
+int dmst_score_pairs_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out);
+int dmst_score_pairs_complete(dmst_ctx *ctx);
+/* Calls submitted and not yet completed (0, 1 or 2). */
+int dmst_pending_calls(const dmst_ctx *ctx);
+
 /* Timing of the last dmst_score_pairs call, from CUDA events on the context's
  * stream: total device ms and the ms of the main DP kernel(s). */
 int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, double *null_ms, int *launches);
