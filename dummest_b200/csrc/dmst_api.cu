@@ -128,9 +128,11 @@ struct DevBuf {
                 cudaFree(q);
                 return e;
             }
-            cudaStreamSynchronize(st);
         }
-        if (p) cudaFree(p);
+        if (p) {
+            cudaDeviceSynchronize();  // the copy, and every call in flight (either stream) that reads the old buffer
+            cudaFree(p);
+        }
         p = q;
         cap = want;
         return cudaSuccess;
@@ -268,6 +270,7 @@ struct CallSlot {
     PinnedBuf<PairOut> hOut;
     PinnedBuf<ExactOut> hExOut;
     cudaEvent_t ev[5] = {};  // null start, DP start, DP end, exact end, results copied
+    cudaEvent_t evFork = nullptr;  // the flag kernel done: the exact path may start
     cudaGraphExec_t graphExec = nullptr;
     std::vector<uintptr_t> graphKey;
     int graphLaunches = 0;
@@ -297,6 +300,7 @@ struct dmst_ctx {
     int smCount = 0;
     int maxSmemOptin = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // the exact path and result copies of scoring calls
     cudaEvent_t ev[6] = {};
     std::string err;
 
@@ -339,6 +343,7 @@ struct dmst_ctx {
     double lastPostMs = 0, lastWallMs = 0;
     int lastExactPairs = 0;
     int lastLaunches = 0;
+    int lastFlagged = 0;  // pairs the last completed mid-score call sent to the exact path
 
     int fail(int status, const char *fmt, ...) {
         char buf[512];
@@ -418,13 +423,16 @@ int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out) {
     ctx->device = o.device;
     ctx->smCount = prop.multiProcessorCount;
     ctx->maxSmemOptin = (int)prop.sharedMemPerBlockOptin;
-    if (cudaSetDevice(o.device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaSetDevice(o.device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return DMST_EDEVICE;
     }
     for (auto &e : ctx->ev) cudaEventCreate(&e);
-    for (auto &sl : ctx->slot)
+    for (auto &sl : ctx->slot) {
         for (auto &e : sl.ev) cudaEventCreate(&e);
+        cudaEventCreateWithFlags(&sl.evFork, cudaEventDisableTiming);
+    }
     uint8_t table[64];
     standardCodeTable(table);
     if (cudaMemcpyToSymbol(cCodonTable, table, 64) != cudaSuccess) {
@@ -439,6 +447,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
     if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
     for (auto &sl : ctx->slot) {
         if (sl.graphExec) cudaGraphExecDestroy(sl.graphExec);
@@ -458,6 +467,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
         sl.hExOut.release();
         for (auto &e : sl.ev)
             if (e) cudaEventDestroy(e);
+        if (sl.evFork) cudaEventDestroy(sl.evFork);
     }
     ctx->dExactPool.release();
     ctx->dEmit.release();
@@ -487,6 +497,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     delete ctx;
 }
 
@@ -1196,20 +1207,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             flagKernel<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(S.dOut.p, (int)n, forceExact ? 1 : 0,
                                                                         S.dQueue.p, S.dQueueCount.p);
             CK(cudaGetLastError(), "flag kernel");
-            exactWaveKernel<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), ctx->stream>>>(
-                S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-                ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p);
-            CK(cudaGetLastError(), "exact kernel");
-            launches += 2;
-        }
-        CK(record(S.ev[3]), "event");
-        if (!nullOnly) {
-            CK(cudaMemcpyAsync(S.hOut.p, S.dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, ctx->stream),
-               "download results");
-            if (exactOnDevice)
-                CK(cudaMemcpyAsync(S.hExOut.p, S.dExOut.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost,
-                                   ctx->stream),
-                   "download exact results");
+            ++launches;
         }
         return DMST_OK;
     };
@@ -1269,7 +1267,33 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         const int st = enqueue();
         if (st) return st;
     }
-    CK(cudaEventRecord(S.ev[4], ctx->stream), "event");
+    // The exact path and the result copies go on the second stream, after the
+    // flag kernel, when the exact path is expected to leave SMs idle (the
+    // previous call flagged fewer pairs than three quarters of the SMs, each
+    // pair taking one CTA): the next call's null model and DP kernels (first
+    // stream) then fill them.  A larger exact path keeps the stream order.
+    const bool overlapExact = exactOnDevice && ctx->lastFlagged * 4 < ctx->smCount * 3;
+    cudaStream_t tail = overlapExact ? ctx->stream2 : ctx->stream;
+    if (exactOnDevice) {
+        if (overlapExact) {
+            CK(cudaEventRecord(S.evFork, ctx->stream), "event");
+            CK(cudaStreamWaitEvent(ctx->stream2, S.evFork, 0), "stream dependency");
+        }
+        exactWaveKernel<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), tail>>>(
+            S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+            ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p);
+        CK(cudaGetLastError(), "exact kernel");
+        ++launches;
+    }
+    CK(cudaEventRecord(S.ev[3], tail), "event");
+    if (!nullOnly) {
+        CK(cudaMemcpyAsync(S.hOut.p, S.dOut.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, tail),
+           "download results");
+        if (exactOnDevice)
+            CK(cudaMemcpyAsync(S.hExOut.p, S.dExOut.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost, tail),
+               "download exact results");
+    }
+    CK(cudaEventRecord(S.ev[4], tail), "event");
     S.pending = true;
     S.n = n;
     S.mode = mode;
@@ -1379,6 +1403,7 @@ static int completeCall(dmst_ctx *ctx) {
                              order[flagged[f]]);
     ctx->lastExactMs = exactMs;
     ctx->lastExactPairs = (int)flagged.size();
+    if (mid) ctx->lastFlagged = (int)flagged.size();
 
     float nullMs = 0, dpMs = 0;
     nullMs = elapsedMs(ctx, S.ev[0], S.ev[1]);
