@@ -13,6 +13,8 @@ from ._ffi import (  # noqa: F401
     MODE_GRAPH,
     MODE_MID,
     MODE_PLAIN,
+    RES_EXACT_PATH,
+    RES_SURVIVOR,
     load,
 )
 from .engine import (  # noqa: F401
@@ -25,6 +27,7 @@ from .engine import (  # noqa: F401
     decode_letters,
     encode_dna,
     estimate_gumbel,
+    filter_threshold,
     finalize_hmm,
     pack_dna,
 )

@@ -28,6 +28,7 @@ MODE_EXACT_SEQUENTIAL = 0x400
 MODE_GRAPH = 0x800
 NOALLOC_MAX_LEN = 16384  # DMST_NOALLOC_MAX_LEN
 RES_EXACT_PATH = 1
+RES_SURVIVOR = 2
 
 
 class Params(C.Structure):
@@ -115,6 +116,12 @@ SIGNATURES = [
       C.POINTER(C.c_double)]),
     ("dmst_score_pairs_submit", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.c_int, C.POINTER(Result)]),
     ("dmst_score_pairs_complete", C.c_int, [C.c_void_p]),
+    ("dmst_search", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
+    ("dmst_search_submit", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
+    ("dmst_filter_threshold", C.c_int,
+     [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_float)]),
     ("dmst_pending_calls", C.c_int, [C.c_void_p]),
     ("dmst_posteriors", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]),

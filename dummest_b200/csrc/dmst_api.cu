@@ -6,6 +6,7 @@
 #include "dp_exact.cuh"
 #include "dp_adjoint.cuh"
 #include "dp_exact_wave.cuh"
+#include "dp_search.cuh"
 #include "dp_wavefront.cuh"
 #include "host_model.h"
 #include "null_model.cuh"
@@ -262,6 +263,11 @@ struct CallSlot {
     DevBuf<ExactOut> dExOut;  // exact-path results, by pair position
     DevBuf<int> dQueue;       // exact-path queue, by queue position
     DevBuf<int> dQueueCount;  // [0] queued pairs, [1] next queue position
+    DevBuf<PairOut> dOutF;    // search: the filter wave's results
+    DevBuf<uint8_t> dMask;    // search: survivors
+    PinnedBuf<PairOut> hOutF;
+    PinnedBuf<uint8_t> hMask;
+    PinnedBuf<float> hMinBest;
     PinnedBuf<DevPair> hPairs;
     PinnedBuf<Chunk> hChunks;
     PinnedBuf<NullJob> hNullJobs;
@@ -278,7 +284,7 @@ struct CallSlot {
     bool pending = false;
     size_t n = 0;
     int mode = 0;
-    bool mid = false, nullOnly = false, sequentialExact = false, exactOnDevice = false;
+    bool mid = false, nullOnly = false, sequentialExact = false, exactOnDevice = false, search = false;
     dmst_result *out = nullptr;
     std::vector<int> order;
     std::vector<DevPair> dp;
@@ -336,6 +342,9 @@ struct dmst_ctx {
     int oldest = 0;                          // the oldest pending call's slot
     int lastSlot = 0;                        // the slot of the last completed call
     DevBuf<float> dExactPool;                // exact-path scratch: one slot per CTA
+    DevBuf<Chunk> dMidChunks;                // search: the survivors' chunks
+    DevBuf<int> dSurvivors;                  // search: survivor pair indices by chunk
+    DevBuf<float> dMinBest;                  // search: per-profile filter gate
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
 
@@ -465,11 +474,19 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
         sl.hNullTmpOff.release();
         sl.hOut.release();
         sl.hExOut.release();
+        sl.dOutF.release();
+        sl.dMask.release();
+        sl.hOutF.release();
+        sl.hMask.release();
+        sl.hMinBest.release();
         for (auto &e : sl.ev)
             if (e) cudaEventDestroy(e);
         if (sl.evFork) cudaEventDestroy(sl.evFork);
     }
     ctx->dExactPool.release();
+    ctx->dMidChunks.release();
+    ctx->dSurvivors.release();
+    ctx->dMinBest.release();
     ctx->dEmit.release();
     ctx->dParams.release();
     ctx->dProfiles.release();
@@ -841,8 +858,12 @@ constexpr int kModeNullOnly = 0x10000;
 
 // Host setup, uploads and the launches of a call into slot ctx->nextSlot
 // (which must be free); the call completes in completeCall.
-static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out) {
+// minBest (search only): per profile id, the filter wave's gate (the smallest
+// float best that survives); the call then runs both waves.
+static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out,
+                      const float *minBest = nullptr) {
     const bool nullOnly = (mode & kModeNullOnly) != 0;
+    const bool search = minBest != nullptr;
     if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
     const int base = mode & 0xff;
     const bool plain = (mode & DMST_MODE_PLAIN) != 0;
@@ -942,6 +963,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         int R, warps;     // warps launched per CTA (<= kernWarps when shared memory is short)
         int kernWarps;    // the kernel's CTA shape (warp slots per CTA)
         DpKern kern;
+        DpKern kernF = nullptr;  // search: the filter wave's kernel of the same shape
         bool gt = false;  // emission table read from global memory
         std::vector<Chunk> chunks;
         std::vector<double> cost;
@@ -1002,6 +1024,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         // in global memory instead (read through L1), and every warp runs.
         G.gt = table + (size_t)G.kernWarps * sizeof(Window) > smemLimit;
         if (G.gt) G.kern = dpKernelFor(G.R, mid, G.kernWarps, true);
+        if (search) G.kernF = dpKernelFor(G.R, false, G.kernWarps, G.gt);
         G.warps = G.gt ? G.kernWarps : (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / sizeof(Window));
         G.warps = (int)std::max<size_t>(1, std::min<size_t>(G.warps, maxSlots / ctx->smCount));
         // Chunks of up to four pairs per launched warp, fewer when the group is
@@ -1047,6 +1070,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         G.smem = (G.gt ? 0 : table) + (size_t)G.warps * sizeof(Window);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
+        if (search)
+            CK(cudaFuncSetAttribute(G.kernF, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
+               "smem attribute");
         int perSm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, G.kern, G.warps * kLanes, G.smem), "occupancy");
         if (perSm < 1) return ctx->fail(DMST_ERANGE, "kernel does not fit on an SM");
@@ -1074,7 +1100,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // The groups run one after another on the stream, so they share the slots.
     CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
-    const size_t nCounters = allChunks.size() + 3;
+    const size_t nCounters = std::max<size_t>(allChunks.size() + 3, 6);  // search: the second wave's at 3..5
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
 
     // Null-model jobs: up to 32 pairs of one read per warp.
@@ -1135,6 +1161,19 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         }
     }
     CK(S.hOut.ensure(n), "alloc results");
+    int chunkStride = 1;
+    if (search) {
+        for (const Chunk &c : allChunks) chunkStride = std::max(chunkStride, c.count);
+        const size_t nProf = ctx->profiles.size();
+        CK(S.dOutF.ensure(n), "alloc filter results");
+        CK(S.dMask.ensure(n), "alloc survivors");
+        CK(S.hOutF.ensure(n), "alloc filter results");
+        CK(S.hMask.ensure(n), "alloc survivors");
+        CK(ctx->dMidChunks.ensure(std::max<size_t>(allChunks.size(), 1)), "alloc survivor chunks");
+        CK(ctx->dSurvivors.ensure(std::max<size_t>(allChunks.size() * chunkStride, 1)), "alloc survivors");
+        CK(ctx->dMinBest.ensure(nProf), "alloc filter gates");
+        if ((st = upload(S.hMinBest, ctx->dMinBest.p, minBest, nProf, "upload filter gates"))) return st;
+    }
 
     S.hostMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - hostT0).count();
     NullRates nr;
@@ -1155,6 +1194,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     g.ring = ctx->dRing.p;
     g.ringSlotFloats = ringSlot;
     g.out = S.dOut.p;
+    g.pairIdx = nullptr;
     // The device work of the call up to the DP results: counter reset,
     // null-model kernel, the DP kernels of each rows-per-lane group, and the
     // timing events between them.
@@ -1177,6 +1217,27 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(cudaGetLastError(), "null-model kernel");
         ++launches;
         CK(record(S.ev[1]), "event");
+        if (search) {
+            // the filter wave over every pair, then each chunk's survivors
+            for (int gi = 0; gi < 3; ++gi) {
+                Group &G = groups[gi];
+                if (G.chunks.empty()) continue;
+                DpArgs gk = g;
+                gk.out = S.dOutF.p;
+                gk.chunks = ctx->dChunks.p + G.chunkBase;
+                gk.nChunks = (int)G.chunks.size();
+                gk.chunkCounter = ctx->dCounter.p + gi;
+                G.kernF<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
+                CK(cudaGetLastError(), "filter kernel");
+                ++launches;
+            }
+            const int nc = (int)allChunks.size();
+            survivorKernel<<<(nc + 7) / 8, 256, 0, ctx->stream>>>(ctx->dChunks.p, nc, S.dOutF.p, ctx->dMinBest.p,
+                                                                  ctx->dMidChunks.p, ctx->dSurvivors.p, chunkStride,
+                                                                  S.dMask.p);
+            CK(cudaGetLastError(), "survivor kernel");
+            ++launches;
+        }
         if (!forceExact && !nullOnly) {
             for (int gi = 0; gi < 3; ++gi) {
                 Group &G = groups[gi];
@@ -1193,9 +1254,10 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                     }
                 } else {
                     DpArgs gk = g;
-                    gk.chunks = ctx->dChunks.p + G.chunkBase;
+                    gk.chunks = (search ? ctx->dMidChunks.p : ctx->dChunks.p) + G.chunkBase;
                     gk.nChunks = (int)G.chunks.size();
-                    gk.chunkCounter = ctx->dCounter.p + gi;
+                    gk.chunkCounter = ctx->dCounter.p + (search ? 3 : 0) + gi;
+                    if (search) gk.pairIdx = ctx->dSurvivors.p;
                     G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                     ++launches;
                 }
@@ -1205,13 +1267,14 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(record(S.ev[2]), "event");
         if (exactOnDevice) {
             flagKernel<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(S.dOut.p, (int)n, forceExact ? 1 : 0,
-                                                                        S.dQueue.p, S.dQueueCount.p);
+                                                                        S.dQueue.p, S.dQueueCount.p,
+                                                                        search ? S.dMask.p : nullptr);
             CK(cudaGetLastError(), "flag kernel");
             ++launches;
         }
         return DMST_OK;
     };
-    if ((mode & DMST_MODE_GRAPH) && !plain && !nullOnly && !sequentialExact) {
+    if ((mode & DMST_MODE_GRAPH) && !plain && !nullOnly && !sequentialExact && !search) {
         // Replay the captured graph when the launch shape and the buffers are
         // those of the last capture; otherwise capture again and update the
         // executable graph (or instantiate a new one).
@@ -1292,6 +1355,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         if (exactOnDevice)
             CK(cudaMemcpyAsync(S.hExOut.p, S.dExOut.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost, tail),
                "download exact results");
+        if (search) {
+            CK(cudaMemcpyAsync(S.hOutF.p, S.dOutF.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, tail),
+               "download filter results");
+            CK(cudaMemcpyAsync(S.hMask.p, S.dMask.p, n, cudaMemcpyDeviceToHost, tail), "download survivors");
+        }
     }
     CK(cudaEventRecord(S.ev[4], tail), "event");
     S.pending = true;
@@ -1301,6 +1369,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     S.nullOnly = nullOnly;
     S.sequentialExact = sequentialExact;
     S.exactOnDevice = exactOnDevice;
+    S.search = search;
     S.out = out;
     S.order.swap(order);
     S.dp.swap(dp);
@@ -1339,10 +1408,13 @@ static int completeCall(dmst_ctx *ctx) {
         return DMST_OK;
     }
     const PairOut *po = S.hOut.p;
+    const bool search = S.search;
+    const uint8_t *survived = search ? S.hMask.p : nullptr;
+    const PairOut *pf = search ? S.hOutF.p : nullptr;
     // Pairs outside the fast path's exact range go to the row-rescaled kernel.
     std::vector<int> flagged;
     for (size_t k = 0; k < n; ++k) {
-        if (!mid) continue;
+        if (!mid || (survived && !survived[k])) continue;
         const PairOut &o = po[k];
         const bool ok = !forceExact && o.maxYb <= kRescaleThresh && o.maxFw <= kRescaleThresh &&
                         o.mid < INFINITY && o.filt < INFINITY && o.mid >= 0x1p-100f;
@@ -1419,7 +1491,12 @@ static int completeCall(dmst_ctx *ctx) {
     for (size_t k = 0; k < n; ++k) {
         dmst_result &r = out[order[k]];
         std::memset(&r, 0, sizeof r);
-        if (mid) {
+        if (search && !survived[k]) {  // filtered out: the filter wave's score only
+            const float f = pf[k].filt;
+            r.filter_f = f;
+            r.filter_ln = std::log((double)f);
+            r.mid_ln = -INFINITY;
+        } else if (mid) {
             if (flagAt[k] >= 0) {
                 scoreToResult(eo[flagAt[k]].mid, &r.mid, &r.mid_ln);
                 scoreToResult(eo[flagAt[k]].filt, &r.filter, &r.filter_ln);
@@ -1429,6 +1506,10 @@ static int completeCall(dmst_ctx *ctx) {
                 fillResult(r, po[k].filt, false, &r.filter, &r.filter_ln);
             }
             r.filter_f = po[k].filt;
+            if (search) {
+                r.filter_f = pf[k].filt;  // the float filter of the first wave
+                r.flags |= DMST_RES_SURVIVOR;
+            }
         } else {
             const float f = po[k].filt;
             r.filter_f = f;
@@ -1478,6 +1559,79 @@ int dmst_score_pairs_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int
         drainCalls(ctx);
     }
     return st;
+}
+
+int dmst_search_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *filter_min_best, int mode,
+                       dmst_result *out) {
+    if (!ctx || !filter_min_best || (n && (!pairs || !out))) return DMST_EINVAL;
+    if ((mode & 0xff) != DMST_MODE_MID || (mode & (DMST_MODE_PLAIN | DMST_MODE_EXACT_SEQUENTIAL | kModeNullOnly)))
+        return ctx->fail(DMST_EINVAL, "dmst_search: mode must be DMST_MODE_MID (with FORCE_EXACT or GRAPH at most)");
+    ctx->lastTotalMs = ctx->lastDpMs = ctx->lastNullMs = ctx->lastExactMs = ctx->lastHostMs = 0;
+    ctx->lastPostMs = ctx->lastWallMs = 0;
+    ctx->lastLaunches = 0;
+    ctx->lastExactPairs = 0;
+    if (n == 0) return DMST_OK;
+    if (ctx->profilesDirty) {
+        const int st = drainCalls(ctx);
+        if (st) return st;
+    }
+    if (ctx->slot[ctx->nextSlot].pending) {
+        const int st = completeCall(ctx);
+        if (st) return st;
+    }
+    const int st = submitCall(ctx, pairs, n, mode, out, filter_min_best);
+    if (st) drainCalls(ctx);
+    return st;
+}
+
+int dmst_search(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *filter_min_best, int mode,
+                dmst_result *out) {
+    if (!ctx) return DMST_EINVAL;
+    int st = drainCalls(ctx);
+    if (st) return st;
+    ctx->nextSlot = ctx->oldest = 0;
+    st = dmst_search_submit(ctx, pairs, n, filter_min_best, mode, out);
+    if (st || n == 0) return st;
+    return completeCall(ctx);
+}
+
+int dmst_filter_threshold(double lambda_filter, double k_filter, double total_length, double filter_evalue,
+                          float *min_best) {
+    if (!min_best || !(lambda_filter > 0) || !(k_filter > 0) || !(total_length > 0) || !(filter_evalue >= 0))
+        return DMST_EINVAL;
+    // The reference's gate for a float best b > 0 (dummest-search.hh:158-166):
+    //   E(b) = K T / exp(log((double)b) * lambda) <= E_filter
+    // E(b) decreases with b: the smallest passing float is found by bisection
+    // over the positive floats' bit patterns (ordered like their values).
+    auto passes = [&](float b) {
+        const double lp = std::log((double)b);
+        const double probRatio = std::exp(lp * lambda_filter);
+        const double evalue = k_filter * total_length / probRatio;
+        return evalue <= filter_evalue;
+    };
+    uint32_t lo = 1, hi = 0x7f7fffffu;  // smallest subnormal .. FLT_MAX
+    float f;
+    std::memcpy(&f, &hi, 4);
+    if (!passes(f)) {
+        *min_best = INFINITY;  // only +inf survives
+        return DMST_OK;
+    }
+    std::memcpy(&f, &lo, 4);
+    if (passes(f)) {
+        *min_best = f;
+        return DMST_OK;
+    }
+    while (hi - lo > 1) {  // passes(hi), !passes(lo)
+        const uint32_t m = lo + (hi - lo) / 2;
+        std::memcpy(&f, &m, 4);
+        if (passes(f))
+            hi = m;
+        else
+            lo = m;
+    }
+    std::memcpy(&f, &hi, 4);
+    *min_best = f;
+    return DMST_OK;
 }
 
 int dmst_score_pairs_complete(dmst_ctx *ctx) {

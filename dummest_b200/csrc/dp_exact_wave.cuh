@@ -272,10 +272,11 @@ __host__ __device__ inline int exactWarps(int M) {
 // Pairs the fast kernel could not score exactly (a row maximum above
 // RESCALE_THRESH in either sweep, a score beyond float range, or a mid
 // product too small for a normal float), or every pair when force is set, go
-// to the queue of the exact path.  queueCount[0] counts them.
-__global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int *queueCount) {
+// to the queue of the exact path.  queueCount[0] counts them.  With `only`,
+// pairs whose entry is 0 are skipped.
+__global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int *queueCount, const uint8_t *only) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= n || (only && !only[k])) return;  // only: the pairs that have mid scores (search survivors)
     const PairOut o = po[k];
     const bool ok = !force && o.maxYb <= kRescaleThresh && o.maxFw <= kRescaleThresh && o.mid < INFINITY &&
                     o.filt < INFINITY && o.mid >= 0x1p-100f;

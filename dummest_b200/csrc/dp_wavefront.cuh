@@ -950,6 +950,7 @@ struct DpArgs {
     float *ring;
     size_t ringSlotFloats;
     PairOut *out;
+    const int *pairIdx;  // null: chunk c holds pairs first .. first+count-1; else pairIdx[first + k]
 };
 
 template <int R, bool MID>
@@ -1041,6 +1042,10 @@ __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tabl
         const int ci = smChunk;
         if (ci >= g.nChunks) break;
         const Chunk ch = g.chunks[ci];
+        if (ch.count == 0) {  // a chunk of the second search wave with no survivors
+            __syncthreads();
+            continue;
+        }
         const int rowPad = ch.rowPad;
         if (ch.prof != loaded) {
             const DevProfile *pr = g.profiles + ch.prof;
@@ -1060,7 +1065,8 @@ __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tabl
             if (lane == 0) k = atomicAdd(&smNext, 1);
             k = __shfl_sync(kFull, k, 0);
             if (k >= ch.count) break;
-            scorePair<R, MID>(g, ch.first + k, smE, rowPad, smBg, win, w1, ring, lane);
+            const int pi = g.pairIdx ? g.pairIdx[ch.first + k] : ch.first + k;
+            scorePair<R, MID>(g, pi, smE, rowPad, smBg, win, w1, ring, lane);
         }
         __syncthreads();
     }

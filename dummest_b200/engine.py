@@ -230,6 +230,16 @@ class Context:
             self._pending.pop(0)  # completed inside the submit
         return res
 
+    def search_raw(self, pairs, min_best, mode: int = F.MODE_MID) -> "C.Array":
+        """Two-wave search (dmst_search) over a ctypes Pair array; min_best: the
+        filter gate per profile id (float32, len = number of profiles)."""
+        n = len(pairs)
+        res = (F.Result * n)()
+        mb = np.ascontiguousarray(min_best, dtype=np.float32)
+        st = self.lib.dmst_search(self.h, pairs, n, mb.ctypes.data_as(C.POINTER(C.c_float)), mode, res)
+        self._check(st, "dmst_search")
+        return res
+
     def complete(self):
         """Complete the oldest pending call (dmst_score_pairs_complete); returns its Result array."""
         if not self._pending:
@@ -450,3 +460,14 @@ def pack_dna(seqs: Sequence[str | bytes]) -> tuple[np.ndarray, np.ndarray, list[
         masks.append((mm.reshape(nm, 32) << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32))
         lens.append(L)
     return np.concatenate(words), np.concatenate(masks), lens
+
+
+def filter_threshold(lambda_filter: float, k_filter: float, total_length: float, filter_evalue: float) -> float:
+    """The smallest float filter best that passes the E-value gate (dmst_filter_threshold)."""
+    lib = F.load()
+    out = C.c_float()
+    st = lib.dmst_filter_threshold(lambda_filter, k_filter, total_length, filter_evalue, C.byref(out))
+    if st != F.DMST_OK:
+        raise ValueError(f"dmst_filter_threshold: status {st}")
+    return out.value
+

@@ -72,6 +72,7 @@ extern "C" {
 
 /* ---- per-result flags -------------------------------------------------- */
 #define DMST_RES_EXACT_PATH 1 /* pair was scored by the exact row-rescaled kernel */
+#define DMST_RES_SURVIVOR 2   /* dmst_search: the pair passed the filter wave and has a mid score */
 
 /* Reference Params (dummest-core.hh:233-239), FP32 engine layout. */
 typedef struct dmst_params {
@@ -211,6 +212,29 @@ int dmst_score_pairs_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int
 int dmst_score_pairs_complete(dmst_ctx *ctx);
 /* Calls submitted and not yet completed (0, 1 or 2). */
 int dmst_pending_calls(const dmst_ctx *ctx);
+
+/* Two-wave search (findFinalSimilaritiesBatched's filter pass and slow wave,
+ * dummest-search.hh:119-193), both waves on the device with no host round
+ * trip: the float filter (findSimilaritiesBackwardOnly) of every pair, then
+ * the mid-anchored score of the survivors.  A pair survives when its float
+ * best b > 0 and b >= filter_min_best[profile id] or b = +inf (one gate per
+ * profile id of the context, from dmst_filter_threshold).  Every result has
+ * filter_f / filter_ln (the float filter); survivors also have the mid and
+ * exact filter scores of dmst_score_pairs (DMST_MODE_MID) and
+ * DMST_RES_SURVIVOR set; the others have mid_ln = -inf.  mode:
+ * DMST_MODE_MID, optionally with DMST_MODE_FORCE_EXACT.  dmst_search_submit
+ * queues the call like dmst_score_pairs_submit (completed by
+ * dmst_score_pairs_complete); dmst_search waits for it. */
+int dmst_search(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *filter_min_best, int mode,
+                dmst_result *out);
+int dmst_search_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *filter_min_best, int mode,
+                       dmst_result *out);
+/* The filter gate as a float threshold: the smallest float best b whose
+ * E-value K_filter * total_length / exp(ln(b) * lambda_filter) is at most
+ * filter_evalue (the reference's expression, dummest-search.hh:158-166, in
+ * double); +inf when no finite best passes. */
+int dmst_filter_threshold(double lambda_filter, double k_filter, double total_length, double filter_evalue,
+                          float *min_best);
 
 /* Timing of the last dmst_score_pairs call, from CUDA events on the context's
  * stream: total device ms and the ms of the main DP kernel(s). */
