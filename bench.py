@@ -47,6 +47,8 @@ sys.path.insert(0, ROOT)
 
 FLOPS_PER_CELL = 52  # 24 backward + 28 forward with the mid product
 AG_BYTES_PER_CELL = 48              # adjoint: (W0, Y0, Z0) written, (W0, Z0, Y0 of the row below) read, FP64
+SEARCH_E = 10.0                     # -e and the filter E-value by default (dummest-core.hh:60, dummest.cc:297-298)
+FILTER_FLOPS_PER_CELL = 25          # the float filter: backward only
 METRIC = "fwd+bwd GCUPS (batched persistent kernel)"
 
 
@@ -63,10 +65,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
-    ap.add_argument("--workload", choices=["batched", "genome", "autograd"], default="batched",
+    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search"], default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
                          "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
-                         "profile over 4096 implant reads (L 600-2400), one SGD step per step")
+                         "profile over 4096 implant reads (L 600-2400), one SGD step per step; search: the "
+                         "batched pairs through the two-wave search (filter, then mid on survivors)")
     ap.add_argument("--ag-reads", type=int, default=4096, help="autograd workload: reads per rank")
     ap.add_argument("--ag-m", type=int, default=400, help="autograd workload: profile length")
     ap.add_argument("--ag-lmin", type=int, default=600, help="autograd workload: shortest read")
@@ -151,6 +154,17 @@ def workload_config(args, world: int) -> dict:
                         "one SGD step of the emission/transition/frameshift logits per step",
             "profiles": 1, "pairs_per_step": args.ag_reads, "l2": "inputs larger than L2 (forward store)",
             "parallelism": f"replicas x{world} (reads sharded per rank)",
+        }
+    if args.workload == "search":
+        return {
+            "workload": f"two-wave search (float filter on every pair, mid-anchored score on survivors, E <= "
+                        f"{SEARCH_E:g}): {args.profiles} profiles M log-uniform 50-800 x reads L log-uniform "
+                        "150-3000 nt, GC 0.4-0.6, 10% implants, both strands; gates from each profile's "
+                        "calibration (200 x 3 kb random sequences)",
+            "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
+            "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
+            "l2": "inputs larger than L2 (W1 slots)",
+            "parallelism": f"replicas x{world} (pairs sharded per rank)",
         }
     if args.workload == "genome":
         return {
@@ -318,10 +332,90 @@ def cpu_baseline(hmm_text, records, n_profiles, seconds, seed):
 
 
 # ---------------------------------------------------------------------------
+def search_gates(fits, total_length):
+    """Per-profile float gates of the filter wave (dmst_filter_threshold)."""
+    import dummest_b200 as d
+    return np.array([d.filter_threshold(f["lambda_filter"], f["K_filter"], total_length, SEARCH_E) for f in fits],
+                    np.float32)
+
+
+def cpu_search_baseline(hmm_text, records, gates, seconds, seed):
+    """The reference engine's two waves on a bounded sample: its float filter
+    (findSimilaritiesBackwardOnly) on every record x profile, then its mid
+    score (findSimilarities) on the survivors, all host threads."""
+    from oracle.ref import RefEngine, available
+    if not available(32):
+        return None
+    e = RefEngine(32)
+    e.set_rates()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(hmm_text)
+        path = f.name
+    n = e.load_profiles(path)
+    os.unlink(path)
+    Ms = [e.profile(p)[1].shape[0] for p in range(n)]
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    codes = [e.decode(e.encode(r)) for r in records]
+    lens = np.array([len(c) for c in codes], dtype=np.float64)
+    done_cells, done_s, used, surv = 0.0, 0.0, 0, 0
+    for p in rng.permutation(n):
+        t = time.perf_counter()
+        # mode 1 gives log((double)best); b >= gate (floats) <=> log b >= log gate
+        _, flt = e.score_many(int(p), codes, threads=threads, mode=1)
+        lg = np.log(np.float64(gates[p]))
+        keep = [k for k, lb in enumerate(flt) if lb > -np.inf and (lb >= lg or lb == np.inf)]
+        if keep:
+            e.score_many(int(p), [codes[k] for k in keep], threads=threads, mode=0)
+        done_s += time.perf_counter() - t
+        done_cells += Ms[p] * lens.sum()
+        surv += len(keep)
+        used += 1
+        if done_s >= seconds:
+            break
+    return {"value": done_cells / done_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"{used} of {n} profiles x {len(codes)} records of one step ({surv} survivors), "
+                      f"{done_cells:.3e} cells in {done_s:.1f} s: the reference's float filter on every pair, "
+                      "then its mid score on the survivors"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     profiles, txt, steps = make_workload(args, 0, 1)
+    if args.workload == "search":
+        import dummest_b200 as d
+        rng = np.random.default_rng(args.seed)
+        # gates from the library's calibration fits would need a GPU; the
+        # reference arm calibrates with its own engine (estimateK, 200 x 3 kb)
+        from oracle.ref import RefEngine
+        e = RefEngine(32)
+        e.set_rates()
+        with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+            f.write(txt)
+            path = f.name
+        e.load_profiles(path)
+        os.unlink(path)
+        fits = []
+        for p in range(len(profiles)):
+            lam, k, lamf, kf = e.estimate_k(p, 3000, 100, 200, threads=os.cpu_count() or 1)
+            fits.append({"lambda_filter": lamf, "K_filter": kf})
+        gates = search_gates(fits, float(sum(len(r) for r in steps[0])))
+        vals = []
+        per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+        cb = None
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_search_baseline(txt, steps[0], gates, per_step, int(rng.integers(1 << 30)))
+            vals.append(cb["value"])
+        v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else vals[-1]
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": "two-wave search GCUPS (cells of every pair)", "value": v,
+            "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args, world), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return
     vals = []
     cb = None
     per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
@@ -536,6 +630,134 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
+def run_search(args, rank, world, local):
+    import dummest_b200 as d
+    from dummest_b200 import _ffi as F
+    import torch
+
+    n_steps = args.warmup + args.steps
+    profiles, txt, steps = make_workload(args, rank, n_steps)
+    ctx = d.Context(device=local)
+    pids = ctx.load_hmm(txt)
+    Ms = np.array([ctx.profile_length(p) for p in pids])
+
+    def pairs_for(sids):
+        arr = (F.Pair * (len(sids) * len(pids)))()
+        k = 0
+        for p in pids:
+            for s in sids:
+                arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
+                k += 1
+        return arr
+
+    # untimed: each profile's calibration (the filter wave's lambda and K) and
+    # the kernel shapes
+    fits = [ctx.estimate_k(p, 3000, 100, 200) for p in pids]
+    step_sids = [ctx.add_dna(recs) for recs in steps]
+    step_pairs = [pairs_for(sids) for sids in step_sids]
+    gates = [search_gates(fits, float(sum(len(r) for r in recs))) for recs in steps]
+    cells_step = [float(sum(len(r) for r in recs)) * float((Ms + 1).sum()) for recs in steps]
+    samp = step_sids[0]
+    ctx.autotune([s for _ in pids for s in samp], [p for p in pids for _ in samp])
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    for w in range(args.warmup):
+        ctx.search_submit_raw(step_pairs[w], gates[w])
+    while ctx.complete() is not None:
+        pass
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    results, dp_ms, launches, cells = [], 0.0, 0, 0.0
+    parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0}
+
+    def account():
+        nonlocal dp_ms, launches
+        t = ctx.last_timing()
+        dp_ms += t["dp_ms"]
+        launches += t["launches"]
+        for key in parts:
+            parts[key] += t[key]
+    for k in range(args.warmup, n_steps):
+        ctx.search_submit_raw(step_pairs[k], gates[k])
+        if k > args.warmup:
+            results.append(ctx.complete())
+            account()
+        cells += cells_step[k]
+    results.append(ctx.complete())
+    account()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    value, ms_max, cells_all = aggregate(cells, ms, world)
+    # survivors' cells (the second wave's work)
+    surv_cells = surv = 0
+    for k, res in zip(range(args.warmup, n_steps), results):
+        lens = np.array([len(r) for r in steps[k]], np.float64)
+        for i, r in enumerate(res):
+            if r.flags & F.RES_SURVIVOR:
+                surv += 1
+                surv_cells += (Ms[i // len(lens)] + 1) * lens[i % len(lens)]
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = n_sm * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = (FILTER_FLOPS_PER_CELL * cells + FLOPS_PER_CELL * surv_cells) / (dp_ms / 1e3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": f"derived: {n_sm} SMs x 128 FP32 lanes x 2 x sm_max_mhz {sm_max:g}",
+                "kernel": "both waves' DP kernels and the survivor compaction, CUDA events on the library stream",
+                "algorithmic_flops_per_cell": {"filter": FILTER_FLOPS_PER_CELL, "mid": FLOPS_PER_CELL}}
+    # e2e: each step's reads copied (2-bit packed), decoded, searched, results copied back
+    packed = [d.pack_dna(recs) for recs in steps]
+    ctx.clear_sequences()
+    base, e2e_pairs = 0, []
+    for k in range(n_steps):
+        e2e_pairs.append(pairs_for(list(range(base, base + len(steps[k])))))
+        base += len(steps[k])
+    for w in range(args.warmup):
+        words, mask, lens = packed[w]
+        ctx.add_packed(words, lens, mask)
+        ctx.search_submit_raw(e2e_pairs[w], gates[w])
+    while ctx.complete() is not None:
+        pass
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for k in range(args.warmup, n_steps):
+        words, mask, lens = packed[k]
+        ctx.add_packed(words, lens, mask)
+        ctx.search_submit_raw(e2e_pairs[k], gates[k])
+        if k > args.warmup:
+            ctx.complete()
+        h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 40 * len(e2e_pairs[k]) + 4 * len(pids)
+        d2h += 57 * len(e2e_pairs[k])
+    while ctx.complete() is not None:
+        pass
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
+           "d2h_bytes_per_step": d2h // args.steps}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_search_baseline(txt, steps[args.warmup], gates[args.warmup], args.cpu_seconds, args.seed)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "two-wave search GCUPS (cells of every pair)", "value": value, "unit": "GCUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk,
+            "survivors_per_step": surv / args.steps, "survivor_cell_fraction": surv_cells / cells,
+            "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()}}), flush=True)
+    ctx.close()
+
+
 def autograd_problem(args, rank):
     """The profile and one rank's reads."""
     from dummest_b200 import synth
@@ -683,6 +905,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "autograd":
             run_autograd(args, rank, world, local)
+        elif args.workload == "search":
+            run_search(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -240,6 +240,20 @@ class Context:
         self._check(st, "dmst_search")
         return res
 
+    def search_submit_raw(self, pairs, min_best, mode: int = F.MODE_MID) -> "C.Array":
+        """Queue a two-wave search (dmst_search_submit); completed like submit_raw's calls."""
+        n = len(pairs)
+        res = (F.Result * n)()
+        mb = np.ascontiguousarray(min_best, dtype=np.float32)
+        self._pending.append((pairs, res, mb))
+        st = self.lib.dmst_search_submit(self.h, pairs, n, mb.ctypes.data_as(C.POINTER(C.c_float)), mode, res)
+        if st != F.DMST_OK:
+            self._pending.pop()
+        self._check(st, "dmst_search_submit")
+        while len(self._pending) > self.lib.dmst_pending_calls(self.h):
+            self._pending.pop(0)
+        return res
+
     def complete(self):
         """Complete the oldest pending call (dmst_score_pairs_complete); returns its Result array."""
         if not self._pending:
