@@ -120,6 +120,8 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
     ("dmst_search_submit", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
+    ("dmst_anchors", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Score), C.POINTER(C.c_int), C.POINTER(Result)]),
     ("dmst_filter_threshold", C.c_int,
      [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_float)]),
     ("dmst_pending_calls", C.c_int, [C.c_void_p]),

@@ -268,6 +268,12 @@ struct CallSlot {
     PinnedBuf<PairOut> hOutF;
     PinnedBuf<uint8_t> hMask;
     PinnedBuf<float> hMinBest;
+    DevBuf<long long> dAnchorOff;  // anchors: per pair position, the offset of its columns
+    DevBuf<float> dAnchorM;
+    DevBuf<int> dAnchorE, dAnchorRow;
+    PinnedBuf<long long> hAnchorOff;
+    PinnedBuf<float> hAnchorM;
+    PinnedBuf<int> hAnchorE, hAnchorRow;
     PinnedBuf<DevPair> hPairs;
     PinnedBuf<Chunk> hChunks;
     PinnedBuf<NullJob> hNullJobs;
@@ -285,6 +291,9 @@ struct CallSlot {
     size_t n = 0;
     int mode = 0;
     bool mid = false, nullOnly = false, sequentialExact = false, exactOnDevice = false, search = false;
+    dmst_score *anchorBest = nullptr;  // anchors: the caller's outputs (columns in the caller's pair order)
+    int *anchorRowOut = nullptr;
+    long long anchorCols = 0;
     dmst_result *out = nullptr;
     std::vector<int> order;
     std::vector<DevPair> dp;
@@ -479,6 +488,14 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
         sl.hOutF.release();
         sl.hMask.release();
         sl.hMinBest.release();
+        sl.dAnchorOff.release();
+        sl.dAnchorM.release();
+        sl.dAnchorE.release();
+        sl.dAnchorRow.release();
+        sl.hAnchorOff.release();
+        sl.hAnchorM.release();
+        sl.hAnchorE.release();
+        sl.hAnchorRow.release();
         for (auto &e : sl.ev)
             if (e) cudaEventDestroy(e);
         if (sl.evFork) cudaEventDestroy(sl.evFork);
@@ -860,10 +877,14 @@ constexpr int kModeNullOnly = 0x10000;
 // (which must be free); the call completes in completeCall.
 // minBest (search only): per profile id, the filter wave's gate (the smallest
 // float best that survives); the call then runs both waves.
+// anchorBest/anchorRow (anchors only): the per-column anchors of every pair,
+// scored on the exact path.
 static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out,
-                      const float *minBest = nullptr) {
+                      const float *minBest = nullptr, dmst_score *anchorBest = nullptr, int *anchorRow = nullptr) {
     const bool nullOnly = (mode & kModeNullOnly) != 0;
     const bool search = minBest != nullptr;
+    const bool anchors = anchorBest != nullptr;
+    if (anchors) mode |= DMST_MODE_FORCE_EXACT;
     if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
     const int base = mode & 0xff;
     const bool plain = (mode & DMST_MODE_PLAIN) != 0;
@@ -1141,7 +1162,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     int exactGrid = 0;
     if (exactOnDevice) {
         for (size_t k = 0; k < n; ++k)
-            poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L, exactWarps(dp[k].M)));
+            poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L, exactWarps(dp[k].M), anchors));
         poolSlot = (poolSlot + 63) / 64 * 64;
         size_t freeB = 0, totalB = 0;
         CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
@@ -1154,13 +1175,35 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(S.dQueueCount.ensure(2), "alloc exact queue");
         CK(S.hExOut.ensure(n), "alloc exact out");
         if (!ctx->exactAttrSet) {
-            CK(cudaFuncSetAttribute(exactWaveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            CK(cudaFuncSetAttribute(exactWaveKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
+            CK(cudaFuncSetAttribute(exactWaveKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(kPipeWarps * sizeof(Window))),
                "smem attribute");
             ctx->exactAttrSet = true;
         }
     }
     CK(S.hOut.ensure(n), "alloc results");
+    long long anchorCols = 0;
+    if (anchors) {
+        // columns of each pair, in the caller's order; pair position k -> offset
+        std::vector<long long> callerOff(n);
+        for (size_t i = 0; i < n; ++i) {
+            callerOff[i] = anchorCols;
+            anchorCols += ctx->seqLen[pairs[i].seq];
+        }
+        std::vector<long long> off(n);
+        for (size_t k = 0; k < n; ++k) off[k] = callerOff[order[k]];
+        CK(S.dAnchorM.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.dAnchorE.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.dAnchorRow.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.hAnchorM.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.hAnchorE.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.hAnchorRow.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.dAnchorOff.ensure(n), "alloc anchors");
+        if ((st = upload(S.hAnchorOff, S.dAnchorOff.p, off.data(), n, "upload anchors"))) return st;
+    }
     int chunkStride = 1;
     if (search) {
         for (const Chunk &c : allChunks) chunkStride = std::max(chunkStride, c.count);
@@ -1342,9 +1385,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             CK(cudaEventRecord(S.evFork, ctx->stream), "event");
             CK(cudaStreamWaitEvent(ctx->stream2, S.evFork, 0), "stream dependency");
         }
-        exactWaveKernel<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), tail>>>(
+        auto ek = anchors ? exactWaveKernel<true> : exactWaveKernel<false>;
+        ek<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), tail>>>(
             S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
-            ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p);
+            ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p,
+            anchors ? S.dAnchorOff.p : nullptr, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p);
         CK(cudaGetLastError(), "exact kernel");
         ++launches;
     }
@@ -1355,6 +1400,16 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         if (exactOnDevice)
             CK(cudaMemcpyAsync(S.hExOut.p, S.dExOut.p, n * sizeof(ExactOut), cudaMemcpyDeviceToHost, tail),
                "download exact results");
+        if (anchors) {
+            CK(cudaMemcpyAsync(S.hAnchorM.p, S.dAnchorM.p, anchorCols * sizeof(float), cudaMemcpyDeviceToHost,
+                               tail),
+               "download anchors");
+            CK(cudaMemcpyAsync(S.hAnchorE.p, S.dAnchorE.p, anchorCols * sizeof(int), cudaMemcpyDeviceToHost, tail),
+               "download anchors");
+            CK(cudaMemcpyAsync(S.hAnchorRow.p, S.dAnchorRow.p, anchorCols * sizeof(int), cudaMemcpyDeviceToHost,
+                               tail),
+               "download anchors");
+        }
         if (search) {
             CK(cudaMemcpyAsync(S.hOutF.p, S.dOutF.p, n * sizeof(PairOut), cudaMemcpyDeviceToHost, tail),
                "download filter results");
@@ -1370,6 +1425,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     S.sequentialExact = sequentialExact;
     S.exactOnDevice = exactOnDevice;
     S.search = search;
+    S.anchorBest = anchorBest;
+    S.anchorRowOut = anchorRow;
+    S.anchorCols = anchorCols;
     S.out = out;
     S.order.swap(order);
     S.dp.swap(dp);
@@ -1517,6 +1575,15 @@ static int completeCall(dmst_ctx *ctx) {
             r.mid_ln = -INFINITY;
         }
     }
+    if (S.anchorBest) {
+        for (long long c = 0; c < S.anchorCols; ++c) {
+            S.anchorBest[c].m = S.hAnchorM.p[c];
+            S.anchorBest[c].e = S.hAnchorE.p[c];
+            S.anchorRowOut[c] = S.hAnchorRow.p[c];
+        }
+        S.anchorBest = nullptr;
+        S.anchorRowOut = nullptr;
+    }
     const auto endT = std::chrono::steady_clock::now();
     ctx->lastPostMs = std::chrono::duration<double, std::milli>(endT - postT0).count();
     ctx->lastWallMs = std::chrono::duration<double, std::milli>(endT - hostT0).count();
@@ -1592,6 +1659,29 @@ int dmst_search(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *fi
     ctx->nextSlot = ctx->oldest = 0;
     st = dmst_search_submit(ctx, pairs, n, filter_min_best, mode, out);
     if (st || n == 0) return st;
+    return completeCall(ctx);
+}
+
+int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *best, int *row, dmst_result *out) {
+    if (!ctx || (n && (!pairs || !best || !row))) return DMST_EINVAL;
+    int st = drainCalls(ctx);
+    if (st) return st;
+    ctx->nextSlot = ctx->oldest = 0;
+    if (n == 0) return DMST_OK;
+    std::vector<dmst_result> tmp;
+    if (!out) {
+        tmp.resize(n);
+        out = tmp.data();
+    }
+    if (ctx->profilesDirty) {
+        st = drainCalls(ctx);
+        if (st) return st;
+    }
+    st = submitCall(ctx, pairs, n, DMST_MODE_MID, out, nullptr, best, row);
+    if (st) {
+        drainCalls(ctx);
+        return st;
+    }
     return completeCall(ctx);
 }
 

@@ -92,13 +92,14 @@ static_assert(kPipeExtra >= kLanes - 1 + 2 * kBlock, "a window never reaches the
 __host__ __device__ inline int pipePeriod(int L) { return wavePeriod(L) + kPipeExtra; }
 
 // Scratch per job (floats): W1 nS*D*32R, rings 2W x 4P, rowMax M+1, rowCnt
-// M+1, cntB M+2, cntF M+2.
-__host__ __device__ inline long long exactWaveScratch(int M, int L, int W) {
+// M+1, cntB M+2, cntF M+2, and with anchors the stripes' column partials
+// nS x L x 3.
+__host__ __device__ inline long long exactWaveScratch(int M, int L, int W, bool anchors = false) {
     const long long S = (long long)kLanes * kExactR;
     const long long nS = (M + 1 + S - 1) / S;
     const long long P = wavePeriod(L);
     const long long D = P + kLanes - 1;
-    return nS * D * S + 2LL * W * 4 * P + 2LL * (M + 1) + 2LL * (M + 2) + 64;
+    return nS * D * S + 2LL * W * 4 * P + 2LL * (M + 1) + 2LL * (M + 2) + 64 + (anchors ? nS * L * 3 : 0);
 }
 
 struct PipeSync {
@@ -212,7 +213,7 @@ __device__ bool backwardSweepPipe(const SweepArgs &a, Window &win, int warp, int
     return true;
 }
 
-template <int R, int MODE>
+template <int R, int MODE, bool ANCH = false>
 __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int lane, const PipeSync &ps,
                                  const ExactRows *x, ExactBest *exact) {
     FwdState<R, MODE> f;
@@ -229,6 +230,8 @@ __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int 
     }
     f.sendIn = f.sendY = f.best = f.mx = 0.0f;
     f.sendC = f.cnt = 0;
+    f.sendAM = 0.0f;
+    f.sendAE = f.sendAR = 0;
     f.u = -lane;  // lane 0 leads
     f.s = a.sFirst;
     f.j = 0;
@@ -250,12 +253,12 @@ __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int 
         const int n = (t0 + kBlock < T ? kBlock : T - t0);
 #pragma unroll 1
         for (int g = 0; g < n; g += 6) {
-            forwardStaged<R, MODE, 0>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 1>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 2>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 3>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 4>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 5>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 0, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 1, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 2, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 3, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 4, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 5, ANCH>(f, a, win, lane, total, st, x, exact);
         }
     }
     if (kReadW1) cpAsyncWait<0>();  // no copy outlives the sweep (the slots are reused)
@@ -289,10 +292,14 @@ __global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int 
 // Dynamic shared memory = one Window per warp.  The emission table is read
 // from global memory (a stripe's 32 R rows x 25 codes stay in L1), so tall
 // profiles leave the shared memory to the windows.
+// ANCH: also the per-column anchors of each pair (anchorOff[pair] >= 0: the
+// offset of its L columns in anchorM / anchorE / anchorRow).
+template <bool ANCH>
 __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
     exactWaveKernel(const int *queue, int *queueCount, const DevPair *pairs, const DevProfile *profiles,
                     const float *emit, const float *params, const uint8_t *codes, const float *seeds,
-                    const PairScales *scales, float *pool, long long slotFloats, ExactOut *out) {
+                    const PairScales *scales, float *pool, long long slotFloats, ExactOut *out,
+                    const long long *anchorOff, float *anchorM, int *anchorE, int *anchorRow) {
     extern __shared__ float4 smRaw[];
     Window *wins = reinterpret_cast<Window *>(smRaw);
     __shared__ float smBg[32];
@@ -352,6 +359,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         x.rowCnt = reinterpret_cast<int *>(x.rowMax + (p.M + 1));
         x.cntB = x.rowCnt + (p.M + 1);
         x.cntF = x.cntB + (p.M + 2);
+        x.anchorPart = reinterpret_cast<float *>(x.cntF + (p.M + 2));
         ExactBest filt{0.0, 0}, mid{0.0, 0};
         bool ok = true;
         // Four sweeps, each over every warp; the counts scan between them.
@@ -363,12 +371,33 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
                 case 0: ok = backwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
                 case 1: ok = forwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
                 case 2: ok = backwardSweepPipe<kExactR, kReplay>(a, win, warp, lane, ps, &x, &filt); break;
-                default: ok = forwardSweepPipe<kExactR, kReplay>(a, win, warp, lane, ps, &x, &mid); break;
+                default: ok = forwardSweepPipe<kExactR, kReplay, ANCH>(a, win, warp, lane, ps, &x, &mid); break;
                 }
             }
             __syncthreads();
             ok = ok && abortFlag == 0;
             if (phase < 2 && threadIdx.x == 0 && ok) scanCounts(x.rowMax, x.rowCnt, phase == 0 ? x.cntB : x.cntF, p.M, phase == 0);
+        }
+        if (ANCH && ok && anchorOff[pi] >= 0) {
+            // fold the stripes' partials of each column in row order
+            const long long o = anchorOff[pi];
+            for (int j = threadIdx.x; j < p.L; j += blockDim.x) {
+                float bm = 0.0f;
+                int be = 0, br = 0;
+                for (int s2 = 0; s2 < a.nS; ++s2) {
+                    const float *pp = x.anchorPart + ((size_t)s2 * p.L + j) * 3;
+                    const float cm = pp[0];
+                    const int ce = __float_as_int(pp[1]);
+                    if (xsLessMe(bm, be, cm, ce)) {
+                        bm = cm;
+                        be = ce;
+                        br = __float_as_int(pp[2]);
+                    }
+                }
+                anchorM[o + j] = bm;
+                anchorE[o + j] = be;
+                anchorRow[o + j] = br;
+            }
         }
         filt = warpBest(filt);
         mid = warpBest(mid);

@@ -345,7 +345,16 @@ struct ExactRows {
     int *rowCnt;    // M+1: discovery counts at the row ends
     int *cntB;      // M+2: reference backward counts, cntB[M+1] = 0
     int *cntF;      // M+2: reference forward counts, cntF[i+1] = row i, cntF[0] = 0
+    float *anchorPart;  // replay with anchors: [stripe][column] x (mantissa, exponent, row), 3 words
 };
+
+// scoreLess (dummest-score.hh:70-76) on (mantissa, exponent) pairs.
+__device__ __forceinline__ bool xsLessMe(float am, int ae, float bm, int be) {
+    if (am == 0.0f) return bm != 0.0f;
+    if (bm == 0.0f) return false;
+    if (ae != be) return ae < be;
+    return am < bm;
+}
 
 // ---------------------------------------------------------------------------
 // Backward sweep (dummest-dp-backward.hh:473-574; the float filter :367-430).
@@ -677,6 +686,9 @@ struct FwdState {
     float w[3][R], z[3][R];  // W0 and Z0 history slots (rotating roles, see backwardStep)
     float sendIn, sendY, best, mx;
     int sendC;
+    // anchors: the column's best wMid over the rows below and this lane's (mantissa, exponent, row)
+    float sendAM;
+    int sendAE, sendAR;
     int u, s, j;
     // exact-path state (see BwdState)
     int cnt;
@@ -689,7 +701,13 @@ struct FwdState {
 // One forward step of a lane (dummest-dp-forward.hh:112-223) at phase PH;
 // q holds the W1 values of this step.  Slot (3-PH)%3 holds column j-1,
 // (4-PH)%3 column j-2, (5-PH)%3 column j-3, which the new column j replaces.
-template <int R, int MODE, int PH>
+// ANCH (replay only): also the per-column anchors of the hit path
+// (dummest-dp-forward.hh:196-206): each column's best wMid over the rows and
+// its row passes up the lanes with the column, each lane folding its rows in
+// ascending order with scoreLess (the first row wins ties); the stripe's top
+// lane writes the stripe's partial, and the stripes are folded in order after
+// the sweep.
+template <int R, int MODE, int PH, bool ANCH = false>
 __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                             int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
@@ -697,6 +715,17 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
     constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
     float inW = __shfl_up_sync(kFull, f.sendIn, 1);
     float inY = __shfl_up_sync(kFull, f.sendY, 1);
+    float aM = 0.0f;
+    int aE = 0, aR = 0;
+    if (ANCH) {
+        aM = __shfl_up_sync(kFull, f.sendAM, 1);
+        aE = __shfl_up_sync(kFull, f.sendAE, 1);
+        aR = __shfl_up_sync(kFull, f.sendAR, 1);
+        if (lane == 0) {  // the rows below are the previous stripe's: a partial of this stripe
+            aM = 0.0f;
+            aE = aR = 0;
+        }
+    }
     int inC = 0;
     if (MODE == kDiscover) inC = __shfl_up_sync(kFull, f.sendC, 1);
     if (f.u >= 0 && f.u < total && f.j < a.L) {
@@ -776,6 +805,22 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             const float W0 = (MODE == kMid) ? win0 + __fadd_rn(zs, prev) : win0 + __fmaf_rn(prev, f.c.rs[k], zs);
             if (MODE == kMid) bv[k] = W0 * q[k];
             if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
+            if (ANCH) {
+                // wMid = promote(W0) * promote(W1): the exact double product,
+                // its mantissa rounded to float (dummest-batch.hh:216-235)
+                const double v = (double)W0 * (double)q[k];
+                if (rowBase + k <= a.M() && v > 0.0) {
+                    int ev;
+                    const double mv = frexp(v, &ev);
+                    const float cm = __double2float_rn(mv);
+                    const int ce = ev + kRescaleBits * (f.cIn[k] + f.cB[k]);
+                    if (xsLessMe(aM, aE, cm, ce)) {
+                        aM = cm;
+                        aE = ce;
+                        aR = rowBase + k;
+                    }
+                }
+            }
             const float Y0 = __fmaf_rn(f.c.eps[k], yab, f.c.d0[k] * W0);
             if (MODE == kMid) f.mx = fmax3(f.mx, W0, Y0);
             const float nin = __fmaf_rn(f.c.d2[k], w1, __fmaf_rn(f.c.d1[k], w2, X + Y0));
@@ -817,6 +862,17 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         }
         f.sendIn = win0;
         f.sendY = yab;
+        if (ANCH) {
+            f.sendAM = aM;
+            f.sendAE = aE;
+            f.sendAR = aR;
+            if (lane == kLanes - 1) {
+                float *pp = x->anchorPart + ((size_t)f.s * a.L + f.j) * 3;
+                pp[0] = aM;
+                pp[1] = __int_as_float(aE);
+                pp[2] = __int_as_float(aR);
+            }
+        }
         if (lane == kLanes - 1 && f.s < a.nS - 1) {
             float *rg = kExactMode ? a.ring + (size_t)(f.s % a.ringSlots) * a.ringStride : a.ring;
             if (MODE == kDiscover)
@@ -840,6 +896,10 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         f.sendIn = 0.0f;
         f.sendY = 0.0f;
         f.sendC = 0;
+        if (ANCH) {
+            f.sendAM = 0.0f;
+            f.sendAE = f.sendAR = 0;
+        }
     }
     if (f.u >= 0 && ++f.j == a.P) {
         f.j = 0;
@@ -851,7 +911,7 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
 // One forward step at position P6 of a six-step group: wait for this step's
 // W1 copy, read it from the staging ring, run the step, and stage the W1 of
 // the step kW1Ahead later into the slot this lane read one step ago.
-template <int R, int MODE, int P6>
+template <int R, int MODE, int P6, bool ANCH = false>
 __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                               int total, W1Stage<R, MODE == kDiscover || MODE == kReplay> &st,
                                               const ExactRows *x, ExactBest *exact) {
@@ -870,7 +930,7 @@ __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepA
 #pragma unroll
         for (int k = 0; k < R; ++k) q[k] = 0.0f;
     }
-    forwardStep<R, MODE, P6 % 3>(f, a, win, lane, total, q, x, exact);
+    forwardStep<R, MODE, P6 % 3, ANCH>(f, a, win, lane, total, q, x, exact);
     if (kReadW1) st.issue(a, win, (P6 + kW1Ahead) % kW1Slots, lane, total);
 }
 

@@ -254,6 +254,27 @@ class Context:
             self._pending.pop(0)
         return res
 
+    def anchors(self, seq_ids: Sequence[int], pid: int):
+        """Per-column anchors of each read against profile pid (dmst_anchors):
+        a list of (mantissa (L,), exponent (L,), row (L,)) arrays, and the results."""
+        n = len(seq_ids)
+        lens = [self.seq_length(s) for s in seq_ids]
+        pairs = (F.Pair * n)()
+        for k, s in enumerate(seq_ids):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, pid, -2.0
+        tot = sum(lens)
+        best = (F.Score * tot)()
+        row = np.zeros(tot, np.int32)
+        res = (F.Result * n)()
+        st = self.lib.dmst_anchors(self.h, pairs, n, best, row.ctypes.data_as(C.POINTER(C.c_int)), res)
+        self._check(st, "dmst_anchors")
+        m = np.frombuffer(best, dtype=np.dtype([("m", np.float32), ("e", np.int32)]))
+        out, o = [], 0
+        for L in lens:
+            out.append((m["m"][o:o + L].copy(), m["e"][o:o + L].copy(), row[o:o + L].copy()))
+            o += L
+        return out, res
+
     def complete(self):
         """Complete the oldest pending call (dmst_score_pairs_complete); returns its Result array."""
         if not self._pending:

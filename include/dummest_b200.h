@@ -229,6 +229,16 @@ int dmst_search(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *fi
                 dmst_result *out);
 int dmst_search_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const float *filter_min_best, int mode,
                        dmst_result *out);
+/* Per-column anchors of the hit path (dummest-dp-forward.hh:196-206,
+ * :456-469), the starting points the reference sorts (descending) and traces
+ * back from (dummest-traceback.hh).  For pair k (the caller's order) and
+ * column j < L_k, at offset sum_{k'<k} L_k' + j: best = the largest mid
+ * product wMid = promote(W0) promote(W1) over the profile rows (ExpScore) and
+ * row = its row, the first on ties; columns whose products are all 0 have
+ * best = {0, 0}.  Scored on the exact path; out (may be NULL) gets the
+ * pairs' scores as from dmst_score_pairs(DMST_MODE_MID).  Synchronous. */
+int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *best, int *row, dmst_result *out);
+
 /* The filter gate as a float threshold: the smallest float best b whose
  * E-value K_filter * total_length / exp(ln(b) * lambda_filter) is at most
  * filter_evalue (the reference's expression, dummest-search.hh:158-166, in

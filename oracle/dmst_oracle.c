@@ -460,9 +460,19 @@ int dmsto_backward_matrix(const float *values, const float *params, const float 
     return st;
 }
 
-int dmsto_score_pair(const float *values, const float *params, const float *bg, int M, const uint8_t *codes, int L,
-                     dmsto_rates r, dmsto_score *mid, dmsto_score *filter) {
+/* findSimilarities' scores, and (colBest/colRow non-NULL) the per-column
+ * anchors of its hit path: for each column j the largest wMid over the rows
+ * and its row, rows in ascending order with a strict comparison, so the
+ * first row wins ties (dummest-dp-forward.hh:196-206). */
+static int score_pair_impl(const float *values, const float *params, const float *bg, int M, const uint8_t *codes,
+                           int L, dmsto_rates r, dmsto_score *mid, dmsto_score *filter, dmsto_score *colBest,
+                           int *colRow) {
     if (!values || !params || !bg || !codes || M < 1 || L < 3 || !mid || !filter) return -1;
+    if (colBest)
+        for (int j = 0; j < L; ++j) {
+            colBest[j] = XS0;
+            colRow[j] = 0;
+        }
     const unsigned csr = ftz_enter();
     pair_ctx p;
     float *seeds = NULL;
@@ -519,6 +529,10 @@ int dmsto_score_pair(const float *values, const float *params, const float *bg, 
                 rowMax = vmax(rowMax, w0);
                 const xs wm = batch_mul(promote(w0, cntF[i]), promote(w1row[j], cntB[i]));
                 if (score_less(best, wm)) best = wm;
+                if (colBest && score_less(colBest[j], wm)) {
+                    colBest[j] = wm;
+                    colRow[j] = i;
+                }
                 w0cur[j] = w0;
                 ws2 = ws1;
                 ws1 = ws0;
@@ -556,6 +570,18 @@ done:
     free(seeds);
     ftz_leave(csr);
     return st;
+}
+
+int dmsto_score_pair(const float *values, const float *params, const float *bg, int M, const uint8_t *codes, int L,
+                     dmsto_rates r, dmsto_score *mid, dmsto_score *filter) {
+    return score_pair_impl(values, params, bg, M, codes, L, r, mid, filter, NULL, NULL);
+}
+
+int dmsto_anchors(const float *values, const float *params, const float *bg, int M, const uint8_t *codes, int L,
+                  dmsto_rates r, dmsto_score *colBest, int *colRow) {
+    if (!colBest || !colRow) return -1;
+    dmsto_score mid, filter;
+    return score_pair_impl(values, params, bg, M, codes, L, r, &mid, &filter, colBest, colRow);
 }
 
 int dmsto_filter_pair(const float *values, const float *params, const float *bg, int M, const uint8_t *codes, int L,

@@ -64,6 +64,12 @@ int dmsto_filter_pair(const float *values, const float *params, const float *bg,
 int dmsto_backward_matrix(const float *values, const float *params, const float *bg, int M, const uint8_t *codes,
                           int L, dmsto_rates r, float *w1, int *counts);
 
+/* Per-column anchors of the hit path (dummest-dp-forward.hh:196-206): for
+ * each column j < L the largest wMid = promote(W0) * promote(W1) over the
+ * rows, and its row (the first row on ties). */
+int dmsto_anchors(const float *values, const float *params, const float *bg, int M, const uint8_t *codes, int L,
+                  dmsto_rates r, dmsto_score *colBest, int *colRow);
+
 /* log T in FP64: T = sum over cells of prefixSeed * W1 (the total weight of
  * all local alignments), the backward recurrence in double on double profile
  * arrays (values (M+1) x 29, params (M+2) x 11), the reference's null model

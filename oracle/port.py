@@ -55,6 +55,8 @@ def lib() -> C.CDLL:
         D = C.POINTER(C.c_double)
         L.dmsto_log_total.restype = C.c_int
         L.dmsto_log_total.argtypes = [D, D, F, C.c_int, U8, C.c_int, Rates, D]
+        L.dmsto_anchors.restype = C.c_int
+        L.dmsto_anchors.argtypes = [F, F, F, C.c_int, U8, C.c_int, Rates, C.POINTER(Score), C.POINTER(C.c_int)]
         L.dmsto_posteriors.restype = C.c_int
         L.dmsto_posteriors.argtypes = [D, D, F, C.c_int, U8, C.c_int, Rates, D, D, D, D]
         L.dmsto_last_rescales.restype = None
@@ -147,6 +149,20 @@ def log_total(values, params, bg, codes, r: Rates | None = None) -> float:
     if st:
         raise ValueError("oracle log_total rejected the pair")
     return out.value
+
+
+def anchors(values, params, bg, codes, r: Rates | None = None):
+    """(best (L,) as (mantissa, exponent) arrays, row (L,)) per column: the hit path's anchors."""
+    values, params, bg, codes = _prep(values, params, bg, codes)
+    L = len(codes)
+    best = (Score * L)()
+    row = np.zeros(L, np.int32)
+    st = lib().dmsto_anchors(_f(values), _f(params), _f(bg), values.shape[0] - 1,
+                             codes.ctypes.data_as(C.POINTER(C.c_uint8)), L, r or rates(), best,
+                             row.ctypes.data_as(C.POINTER(C.c_int)))
+    if st:
+        raise ValueError("oracle anchors rejected the pair")
+    return np.array([b.m for b in best], np.float32), np.array([b.e for b in best], np.int32), row
 
 
 def posteriors(values, params, bg, codes, r: Rates | None = None):

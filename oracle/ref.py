@@ -51,6 +51,7 @@ def lib(bits: int = 32) -> C.CDLL:
         "dmstref_find_similarities": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float),
                                                 P(C.c_int), P(C.c_double), P(C.c_float), P(C.c_int)]),
         "dmstref_backward_only": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float)]),
+        "dmstref_anchors": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_int), P(C.c_int)]),
         "dmstref_score_many": (C.c_int, [C.c_int, P(C.c_uint8), P(C.c_int64), C.c_int, C.c_int, C.c_int,
                                          P(C.c_double), P(C.c_double)]),
         "dmstref_null_model": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_float),
@@ -138,6 +139,19 @@ class RefEngine:
                 raise ValueError("reference findSimilarities rejected the batch")
             out += [(mm[k], me[k], ml[k], fm[k], fe[k]) for k in range(n)]
         return out
+
+    def anchors(self, p: int, codes):
+        """The reference's per-column anchors of one sequence: (mantissa, exponent, row) arrays."""
+        codes = np.ascontiguousarray(codes, np.uint8)
+        L = len(codes)
+        m = np.zeros(L, np.float32)
+        e = np.zeros(L, np.int32)
+        row = np.zeros(L, np.int32)
+        P = C.POINTER
+        if self.L.dmstref_anchors(p, codes.ctypes.data_as(P(C.c_uint8)), L, m.ctypes.data_as(P(C.c_float)),
+                                  e.ctypes.data_as(P(C.c_int)), row.ctypes.data_as(P(C.c_int))) != 0:
+            raise ValueError("reference anchors failed")
+        return m, e, row
 
     def backward_only(self, p: int, seqs) -> list[float]:
         out = []

@@ -243,6 +243,29 @@ int dmstref_find_similarities(int p, const uint8_t *const *decoded, const int *l
     return 0;
 }
 
+// The per-column anchors of one sequence's hit path, read from the
+// reference's own trackers after findSimilarities: for each column j the
+// largest wMid over the rows (bestMidScorePhys) and its row (bestMidRowPhys)
+// (dummest-dp-forward.hh:196-206).
+int dmstref_anchors(int p, const uint8_t *codes, int L, float *bestM, int *bestE, int *row) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || L < 3 || !bestM || !bestE || !row) return -1;
+    std::vector<std::vector<uint8_t>> seqs(1);
+    seqs[0].assign(codes, codes + L);
+    DPScratch scratch;
+    ExpScore mid[simdWidth], flt[simdWidth];
+    double ln[simdWidth];
+    runBatch(*pr, seqs, 1, scratch, mid, ln, flt);
+    for (int j = 0; j < L; ++j) {
+        bestM[j] = scratch.bestMidScorePhys[j][0].m;
+        bestE[j] = scratch.bestMidScorePhys[j][0].e;
+        row[j] = scratch.bestMidRowPhys[j][0];
+    }
+    return 0;
+}
+
 // The lean float filter (findSimilaritiesBackwardOnly) on n <= simdWidth lanes.
 int dmstref_backward_only(int p, const uint8_t *const *decoded, const int *lens, int n, float *best) {
     ensureInit();

@@ -120,3 +120,26 @@ def test_reference_unit_tests_pass(binary):
         pytest.fail(f"{exe} missing: run `make -C oracle`")
     res = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+
+
+def test_oracle_anchors_equal_reference_trackers(ref32, tmp_path):
+    """The oracle's per-column anchors against the reference engine's own
+    bestMidScorePhys / bestMidRowPhys after findSimilarities
+    (dummest-dp-forward.hh:196-206), rescaled rows included."""
+    rng = np.random.default_rng(77)
+    profs = [synth.make_profile(rng, M, f"an{M}") for M in (40, 150, 400)]
+    txt = synth.hmmer3_text(profs)
+    path = tmp_path / "an.hmm"
+    path.write_text(txt)
+    assert ref32.load_profiles(str(path)) == len(profs)
+    import dummest_b200 as d
+    for p, prof in enumerate(profs):
+        _, v, pa, bg = d.finalize_hmm(txt, index=p)
+        for s in (synth.random_dna(rng, 300), synth.sample_homolog(rng, prof, prof.M),
+                  synth.sample_homolog(rng, prof, prof.M) * 2):
+            c = d.decode_dna(s)
+            rm, re, rr = ref32.anchors(p, c)
+            om, oe, orow = port.anchors(v, pa, bg, c)
+            assert np.array_equal(rm, om) and np.array_equal(re, oe)
+            nz = rm != 0
+            assert np.array_equal(rr[nz], orow[nz])
