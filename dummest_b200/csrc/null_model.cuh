@@ -48,6 +48,19 @@ __device__ __forceinline__ XS scaleScore(XS a, double f) {
     return splitNorm(__dmul_rn((double)a.m, f), a.e);
 }
 
+// scaleScore by a positive finite factor below 1 (the frameshift emission
+// rates): the product of a float mantissa in [0.5, 1] and f is 0 or a normal
+// double, so splitNorm's infinity and subnormal cases cannot occur; the
+// result is scaleScore's.
+__device__ __forceinline__ XS scaleByRate(XS a, double f) {
+    if (a.m == 0.0f) return xsZero();
+    const double x = __dmul_rn((double)a.m, f);
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    const int ef = (int)((u >> 52) & 0x7FFULL);
+    const double m = __longlong_as_double((long long)((u & 0xFFFFFFFFFFFFFULL) | (1022ULL << 52)));
+    return XS{__double2float_rn(m), a.e + ef - 1022};
+}
+
 // batchAddScores (dummest-batch.hh:78-108).
 __device__ __forceinline__ XS batchAdd(XS a, XS b) {
     if (a.m == 0.0f) return b;
@@ -102,10 +115,15 @@ __device__ __forceinline__ XS scalarMul(XS a, XS b) {
     return splitNorm(__dmul_rn((double)a.m, (double)b.m), a.e + b.e);
 }
 
-// scoreToFloatClamped (dummest-score.hh:224-230), FP32 engine: exponent capped at 120.
+// scoreToFloatClamped (dummest-score.hh:224-230), FP32 engine: exponent capped
+// at 120.  With the mantissa in [0.5, 1], m 2^e is a normal float for
+// -125 <= e <= 120, where it is the exact product of m and the power of two
+// built from its exponent bits; smaller exponents (subnormal or zero results)
+// go through ldexpf.
 __device__ __forceinline__ float packScore(XS a) {
     if (a.m == 0.0f) return 0.0f;
-    int e = a.e > 120 ? 120 : a.e;
+    const int e = a.e > 120 ? 120 : a.e;
+    if (e >= -125) return __fmul_rn(a.m, __int_as_float((e + 127) << 23));
     return ldexpf(a.m, e);
 }
 
@@ -134,8 +152,8 @@ __device__ __forceinline__ XS prefixStep(int i, const float *bg, const uint8_t *
         codon = scaleScore(pow2Score(-4), frame);
     else
         codon = scaleScore(pow2Score(-2), frame);
-    XS single = scaleScore(i > 0 ? p1 : xsZero(), sNE);
-    XS dbl = scaleScore(i >= 2 ? p2 : xsZero(), dNE);
+    XS single = scaleByRate(i > 0 ? p1 : xsZero(), sNE);
+    XS dbl = scaleByRate(i >= 2 ? p2 : xsZero(), dNE);
     return batchAdd(codon, batchAdd(single, dbl));
 }
 
@@ -207,9 +225,9 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
             p1 = q;
             const int i = L - 1 - k;
             const double codonScale = __dmul_rn((double)bgAt(bg, cd, L, i), keep);
-            const XS single = scaleScore(s1, sNE);
+            const XS single = scaleByRate(s1, sNE);
             const XS dIn = (i + 1 < L) ? s2 : pow2Score(2);
-            const XS dbl = scaleScore(dIn, dNE);
+            const XS dbl = scaleByRate(dIn, dNE);
             const XS codon = (i + 2 < L) ? scaleScore(s3, codonScale) : XS{trailing.m, trailing.e - 2 * (L - i) + 1};
             const XS v = batchAdd(codon, batchAdd(single, dbl));
             sfx[(size_t)i * 32 + lane] = v;
@@ -246,11 +264,21 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
         XS runPre = perBase;
         for (int j0 = 0; j0 < L; j0 += 32) {
             const int ncol = L - j0 < 32 ? L - j0 : 32;
-            for (int c = 0; c < ncol; ++c) {
-                const int j = j0 + c;
-                stage[c][lane] = packScore(batchMul(pfx[(size_t)j * 32 + lane], runPre));
-                runPre = batchMul(runPre, perBase);
-                if (j < L - 1) running = batchMul(running, perBase);
+            for (int c0 = 0; c0 < ncol; c0 += 8) {
+                // the kept prefix values of 8 columns, loaded before the chain uses them
+                XS v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    v[u] = (c0 + u < ncol) ? pfx[(size_t)(j0 + c0 + u) * 32 + lane] : xsZero();
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int c = c0 + u;
+                    if (c >= ncol) break;
+                    const int j = j0 + c;
+                    stage[c][lane] = packScore(batchMul(v[u], runPre));
+                    runPre = batchMul(runPre, perBase);
+                    if (j < L - 1) running = batchMul(running, perBase);
+                }
             }
             flushSeeds(stage, dstAll[warp][0], job.count, j0, ncol, lane);
         }
@@ -258,11 +286,20 @@ __global__ void __launch_bounds__(kNullWarps * 32) nullModelKernel(const NullJob
         // Pass 3: suffix seeds (dummest-dp-backward.hh:146-154).
         for (int j0 = 0; j0 < L; j0 += 32) {
             const int ncol = L - j0 < 32 ? L - j0 : 32;
-            for (int c = 0; c < ncol; ++c) {
-                const int j = j0 + c;
-                const XS nx = (j + 1 < L) ? sfx[(size_t)(j + 1) * 32 + lane] : pow2Score(0);
-                stage[c][lane] = packScore(batchMul(nx, running));
-                running = batchMul(running, perBaseInv);
+            for (int c0 = 0; c0 < ncol; c0 += 8) {
+                XS v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int j = j0 + c0 + u;
+                    v[u] = (c0 + u < ncol && j + 1 < L) ? sfx[(size_t)(j + 1) * 32 + lane] : pow2Score(0);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int c = c0 + u;
+                    if (c >= ncol) break;
+                    stage[c][lane] = packScore(batchMul(v[u], running));
+                    running = batchMul(running, perBaseInv);
+                }
             }
             flushSeeds(stage, dstAll[warp][1], job.count, j0, ncol, lane);
         }
