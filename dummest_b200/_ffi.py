@@ -63,6 +63,23 @@ class Pair(C.Structure):
     _fields_ = [("seq", C.c_int32), ("profile", C.c_int32), ("min_prob_ratio", C.c_float)]
 
 
+class Alignment(C.Structure):
+    _fields_ = [
+        ("pair", C.c_int32),
+        ("score", Score),
+        ("ln_score", C.c_double),
+        ("anchor1", C.c_int32),
+        ("anchor2", C.c_int32),
+        ("seg_begin", C.c_int64),
+        ("seg_count", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
+class Segment(C.Structure):
+    _fields_ = [("start1", C.c_int32), ("start2", C.c_int32), ("length", C.c_int32)]
+
+
 class Result(C.Structure):
     _fields_ = [
         ("mid", Score),
@@ -122,6 +139,10 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
     ("dmst_anchors", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Score), C.POINTER(C.c_int), C.POINTER(Result)]),
+    ("dmst_align", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    ("dmst_align_fetch", C.c_int,
+     [C.c_void_p, C.POINTER(Alignment), C.c_size_t, C.POINTER(Segment), C.c_size_t]),
     ("dmst_filter_threshold", C.c_int,
      [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_float)]),
     ("dmst_pending_calls", C.c_int, [C.c_void_p]),

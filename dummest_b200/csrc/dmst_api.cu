@@ -7,6 +7,7 @@
 #include "dp_adjoint.cuh"
 #include "dp_exact_wave.cuh"
 #include "dp_search.cuh"
+#include "dp_traceback.cuh"
 #include "dp_wavefront.cuh"
 #include "host_model.h"
 #include "null_model.cuh"
@@ -356,6 +357,17 @@ struct dmst_ctx {
     DevBuf<float> dMinBest;                  // search: per-profile filter gate
     DevBuf<float> dExactScratch;
     DevBuf<ExactOut> dExactOut;
+    // dmst_align: the traceback buffers (dp_traceback.cuh) and the last call's results
+    DevBuf<AlignJob> dAlignJobs;
+    DevBuf<int> dAlignJobOf, dAlignRows, dAlignCand, dAlignCounts;
+    DevBuf<float> dAlignCells, dAlignColR, dAlignColF;
+    DevBuf<XS> dAlignX, dAlignSuf, dAlignWork, dAlignRev, dAlignFwd;
+    DevBuf<uint8_t> dAlignMark;
+    DevBuf<AlignSim> dAlignSims, dAlignSimOut;
+    DevBuf<Seg> dAlignSegs, dAlignSegOut;
+    DevBuf<long long> dAlignBase;
+    std::vector<dmst_alignment> alignOut;
+    std::vector<dmst_segment> alignSegOut;
 
     double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0, lastHostMs = 0;
     double lastPostMs = 0, lastWallMs = 0;
@@ -501,6 +513,25 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
         if (sl.evFork) cudaEventDestroy(sl.evFork);
     }
     ctx->dExactPool.release();
+    ctx->dAlignJobs.release();
+    ctx->dAlignJobOf.release();
+    ctx->dAlignRows.release();
+    ctx->dAlignCand.release();
+    ctx->dAlignCounts.release();
+    ctx->dAlignCells.release();
+    ctx->dAlignColR.release();
+    ctx->dAlignColF.release();
+    ctx->dAlignX.release();
+    ctx->dAlignSuf.release();
+    ctx->dAlignWork.release();
+    ctx->dAlignRev.release();
+    ctx->dAlignFwd.release();
+    ctx->dAlignMark.release();
+    ctx->dAlignSims.release();
+    ctx->dAlignSimOut.release();
+    ctx->dAlignSegs.release();
+    ctx->dAlignSegOut.release();
+    ctx->dAlignBase.release();
     ctx->dMidChunks.release();
     ctx->dSurvivors.release();
     ctx->dMinBest.release();
@@ -827,7 +858,10 @@ int dmst_encode_dna(const char *ascii, int L, char *letters) {
 // scoreToLog (dummest-score.hh:202-207): std::log of the float mantissa is the
 // float overload, so the logarithm is taken in single precision and then
 // added to e * ln 2 in double, as the reference's logProbRatio is.
-static double scoreLn(float m, int e) { return (double)std::log(m) + (double)e * 0.6931471805599453; }
+// scoreToLog (dummest-score.hh:203-208) as the reference's x86-64-v3 build
+// evaluates it: the float log of the mantissa, then e ln 2 added in one fused
+// multiply-add (GCC contracts the expression at -O3).
+static double scoreLn(float m, int e) { return std::fma((double)e, 0.6931471805599453, (double)std::log(m)); }
 
 static void fillResult(dmst_result &r, float v, bool isFilterF, dmst_score *dst, double *ln) {
     (void)isFilterF;
@@ -878,9 +912,13 @@ constexpr int kModeNullOnly = 0x10000;
 // minBest (search only): per profile id, the filter wave's gate (the smallest
 // float best that survives); the call then runs both waves.
 // anchorBest/anchorRow (anchors only): the per-column anchors of every pair,
-// scored on the exact path.
+// scored on the exact path.  alignJobs (with anchors): every pair is a
+// traceback job (job k = pair k; the exact kernel keeps its W0, W1 and
+// rescale counts); the jobs' pair fields become the pairs' internal positions
+// and the jobs go to ctx->dAlignJobs.
 static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode, dmst_result *out,
-                      const float *minBest = nullptr, dmst_score *anchorBest = nullptr, int *anchorRow = nullptr) {
+                      const float *minBest = nullptr, dmst_score *anchorBest = nullptr, int *anchorRow = nullptr,
+                      std::vector<AlignJob> *alignJobs = nullptr) {
     const bool nullOnly = (mode & kModeNullOnly) != 0;
     const bool search = minBest != nullptr;
     const bool anchors = anchorBest != nullptr;
@@ -1181,6 +1219,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             CK(cudaFuncSetAttribute(exactWaveKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(kPipeWarps * sizeof(Window))),
                "smem attribute");
+            CK(cudaFuncSetAttribute(exactWaveKernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
             ctx->exactAttrSet = true;
         }
     }
@@ -1203,6 +1244,23 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(S.hAnchorRow.ensure((size_t)anchorCols), "alloc anchors");
         CK(S.dAnchorOff.ensure(n), "alloc anchors");
         if ((st = upload(S.hAnchorOff, S.dAnchorOff.p, off.data(), n, "upload anchors"))) return st;
+    }
+    const bool align = anchors && alignJobs != nullptr;
+    if (align) {
+        std::vector<int> pos(n), jobOf(n);
+        for (size_t k = 0; k < n; ++k) {
+            pos[order[k]] = (int)k;
+            jobOf[k] = order[k];
+        }
+        for (AlignJob &jb : *alignJobs) jb.pair = pos[jb.pair];
+        CK(ctx->dAlignJobs.ensure(n), "alloc traceback jobs");
+        CK(ctx->dAlignJobOf.ensure(n), "alloc traceback jobs");
+        CK(cudaMemcpyAsync(ctx->dAlignJobs.p, alignJobs->data(), n * sizeof(AlignJob), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload traceback jobs");
+        CK(cudaMemcpyAsync(ctx->dAlignJobOf.p, jobOf.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+           "upload traceback jobs");
+        CK(cudaStreamSynchronize(ctx->stream), "upload traceback jobs");  // the host vectors go out of scope
     }
     int chunkStride = 1;
     if (search) {
@@ -1378,18 +1436,20 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // previous call flagged fewer pairs than three quarters of the SMs, each
     // pair taking one CTA): the next call's null model and DP kernels (first
     // stream) then fill them.  A larger exact path keeps the stream order.
-    const bool overlapExact = exactOnDevice && ctx->lastFlagged * 4 < ctx->smCount * 3;
+    const bool overlapExact = exactOnDevice && !align && ctx->lastFlagged * 4 < ctx->smCount * 3;
     cudaStream_t tail = overlapExact ? ctx->stream2 : ctx->stream;
     if (exactOnDevice) {
         if (overlapExact) {
             CK(cudaEventRecord(S.evFork, ctx->stream), "event");
             CK(cudaStreamWaitEvent(ctx->stream2, S.evFork, 0), "stream dependency");
         }
-        auto ek = anchors ? exactWaveKernel<true> : exactWaveKernel<false>;
+        auto ek = align ? exactWaveKernel<true, true> : (anchors ? exactWaveKernel<true> : exactWaveKernel<false>);
         ek<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), tail>>>(
             S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
             ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p,
-            anchors ? S.dAnchorOff.p : nullptr, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p);
+            anchors ? S.dAnchorOff.p : nullptr, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p,
+            align ? ctx->dAlignJobOf.p : nullptr, align ? ctx->dAlignJobs.p : nullptr,
+            align ? ctx->dAlignCells.p : nullptr, align ? ctx->dAlignRows.p : nullptr);
         CK(cudaGetLastError(), "exact kernel");
         ++launches;
     }
@@ -1683,6 +1743,261 @@ int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *be
         return st;
     }
     return completeCall(ctx);
+}
+
+// The traceback of the hit path.  The call's pairs are scored; the hits go,
+// in batches whose traceback buffers fit half the free device memory, through
+// the exact kernel (anchors, W0, W1 and rescale counts kept), the table
+// kernels of dp_traceback.cuh, the reference's anchor sort on the host, the
+// walks and a gather of their results.
+static size_t alignJobBytes(int M, int L) {
+    const size_t cells = (size_t)(M + 1) * L;
+    return cells * (8 + 8 + 8) + (size_t)L * (4 + 4 + 16 + 8 + 8 + 4 + 1 + 2 * sizeof(AlignSim) + 12) +
+           (size_t)alignSegs(M, L) * sizeof(Seg) * 2 + (size_t)alignRowInts(M) * 4 + 256;
+}
+
+static bool lessScore(dmst_score a, dmst_score b) {  // scoreLess (dummest-score.hh:70-76)
+    if (a.m == 0.0f) return b.m != 0.0f;
+    if (b.m == 0.0f) return false;
+    if (a.e != b.e) return a.e < b.e;
+    return a.m < b.m;
+}
+
+int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out, size_t *n_alignments,
+               size_t *n_segments) {
+    if (!ctx || (n && !pairs) || !n_alignments || !n_segments) return DMST_EINVAL;
+    int st = drainCalls(ctx);
+    if (st) return st;
+    ctx->nextSlot = ctx->oldest = 0;
+    ctx->alignOut.clear();
+    ctx->alignSegOut.clear();
+    *n_alignments = *n_segments = 0;
+    if (n == 0) return DMST_OK;
+    std::vector<dmst_result> tmp;
+    if (!out) {
+        tmp.resize(n);
+        out = tmp.data();
+    }
+    st = submitCall(ctx, pairs, n, DMST_MODE_MID, out);
+    if (st) {
+        drainCalls(ctx);
+        return st;
+    }
+    if ((st = completeCall(ctx))) return st;
+
+    // hits: laneHit with a report (dummest-dp-forward.hh:262-274, :489-490);
+    // the gate is normalizeScore((double)minProbRatio, 0)
+    std::vector<int> hits;
+    std::vector<dmst_score> gates;
+    for (size_t k = 0; k < n; ++k) {
+        if (!(pairs[k].min_prob_ratio >= 0.0f)) continue;
+        dmst_score g{0.0f, 0};
+        if (pairs[k].min_prob_ratio != 0.0f) {
+            int ex = 0;
+            const double m = std::frexp((double)pairs[k].min_prob_ratio, &ex);
+            g = dmst_score{(float)m, ex};
+        }
+        if (out[k].mid.m != 0.0f && !lessScore(out[k].mid, g)) {
+            hits.push_back((int)k);
+            gates.push_back(g);
+        }
+    }
+    if (hits.empty()) return DMST_OK;
+
+    size_t freeB = 0, totalB = 0;
+    CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+    const size_t held = ctx->dAlignCells.cap * sizeof(float) + (ctx->dAlignX.cap + ctx->dAlignSuf.cap) * sizeof(XS);
+    const size_t budget = std::max<size_t>((freeB + held) / 2, (size_t)256 << 20);
+    NullRates nr;
+    nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
+    nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
+    for (size_t b0 = 0; b0 < hits.size();) {
+        // the batch: hits b0 .. b1-1
+        size_t b1 = b0, bytes = 0;
+        while (b1 < hits.size() && b1 - b0 < 65535) {
+            const dmst_pair &pp = pairs[hits[b1]];
+            const size_t jb = alignJobBytes(ctx->profiles[pp.profile].M, ctx->seqLen[pp.seq]);
+            if (b1 > b0 && bytes + jb > budget) break;
+            bytes += jb;
+            ++b1;
+        }
+        const int nb = (int)(b1 - b0);
+        std::vector<AlignJob> jobs(nb);
+        std::vector<dmst_pair> bp(nb);
+        long long cells = 0, cols = 0, rowsN = 0, segsN = 0;
+        int maxL = 0, maxM = 0;
+        for (int j = 0; j < nb; ++j) {
+            const dmst_pair &pp = pairs[hits[b0 + j]];
+            bp[j] = pp;
+            AlignJob &jb = jobs[j];
+            jb.pair = j;
+            jb.M = ctx->profiles[pp.profile].M;
+            jb.L = ctx->seqLen[pp.seq];
+            jb.nCand = 0;
+            jb.cellOff = cells;
+            jb.colOff = cols;
+            jb.rowOff = rowsN;
+            jb.segOff = segsN;
+            jb.minM = gates[b0 + j].m;
+            jb.minE = gates[b0 + j].e;
+            cells += (long long)(jb.M + 1) * jb.L;
+            cols += jb.L;
+            rowsN += alignRowInts(jb.M);
+            segsN += alignSegs(jb.M, jb.L);
+            maxL = std::max(maxL, jb.L);
+            maxM = std::max(maxM, jb.M);
+        }
+        CK(ctx->dAlignCells.ensure((size_t)cells * 2), "alloc traceback tables");
+        CK(ctx->dAlignX.ensure((size_t)cells), "alloc traceback tables");
+        CK(ctx->dAlignSuf.ensure((size_t)cells), "alloc traceback tables");
+        CK(ctx->dAlignRows.ensure((size_t)rowsN), "alloc traceback rows");
+        CK(ctx->dAlignColR.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignColF.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignWork.ensure((size_t)(2 * cols + 8LL * nb)), "alloc traceback columns");
+        CK(ctx->dAlignRev.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignFwd.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignCand.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignMark.ensure((size_t)cols), "alloc traceback columns");
+        CK(ctx->dAlignSims.ensure((size_t)cols), "alloc traceback output");
+        CK(ctx->dAlignSegs.ensure((size_t)segsN), "alloc traceback output");
+        CK(ctx->dAlignCounts.ensure((size_t)2 * nb), "alloc traceback output");
+        CK(ctx->dAlignBase.ensure((size_t)2 * nb), "alloc traceback output");
+
+        // the exact path with the traceback stores, then the tables
+        std::vector<dmst_score> best((size_t)cols);
+        std::vector<int> row((size_t)cols);
+        std::vector<dmst_result> bres(nb);
+        const int si = ctx->nextSlot;
+        st = submitCall(ctx, bp.data(), nb, DMST_MODE_MID, bres.data(), nullptr, best.data(), row.data(), &jobs);
+        if (st) {
+            drainCalls(ctx);
+            return st;
+        }
+        CallSlot &S = ctx->slot[si];
+        sidesKernel<<<dim3((maxL + 127) / 128, nb), 128, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, ctx->dAlignCells.p, ctx->dAlignRows.p, ctx->dAlignColR.p, ctx->dAlignColF.p);
+        flankKernel<<<(nb + 31) / 32, 32, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, nb, S.dPairs.p, ctx->dProfiles.p, ctx->dCodes.p, S.dSeeds.p, S.dScales.p, nr,
+            ctx->dAlignColR.p, ctx->dAlignColF.p, ctx->dAlignRows.p, ctx->dAlignWork.p, ctx->dAlignRev.p,
+            ctx->dAlignFwd.p);
+        xTableKernel<<<dim3((maxL + 127) / 128, (maxM + 1 + kXRows - 1) / kXRows, nb), 128, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p, S.dScales.p,
+            ctx->dAlignCells.p, ctx->dAlignRows.p, ctx->dAlignX.p);
+        optimalKernel<<<nb, kOptThreads, 0, ctx->stream>>>(ctx->dAlignJobs.p, ctx->dAlignCells.p, ctx->dAlignRows.p,
+                                                          ctx->dAlignX.p, ctx->dAlignRev.p, ctx->dAlignFwd.p,
+                                                          ctx->dAlignSuf.p);
+        CK(cudaGetLastError(), "traceback table kernels");
+        if ((st = completeCall(ctx))) return st;
+
+        // The reference's sort of each hit's anchors (std::ranges::sort with
+        // std::greater<>, dummest-dp-forward.hh:494, which libstdc++ runs as
+        // std::sort with the same comparisons, so ties land as there): every
+        // column, zero columns as placeholders; the candidates are the leading
+        // entries at or above the gate.
+        struct Entry {
+            dmst_score pair;
+            int col;
+        };
+        std::vector<int> cand((size_t)cols);
+        std::vector<Entry> ent;
+        for (int j = 0; j < nb; ++j) {
+            AlignJob &jb = jobs[j];
+            ent.resize(jb.L);
+            for (int c = 0; c < jb.L; ++c) {
+                const dmst_score a = best[jb.colOff + c];
+                ent[c] = a.m != 0.0f ? Entry{a, c} : Entry{dmst_score{0.0f, 0}, 0};
+            }
+            std::sort(ent.begin(), ent.end(),
+                      [](const Entry &x, const Entry &y) { return lessScore(y.pair, x.pair); });
+            const dmst_score g{jb.minM, jb.minE};
+            int nc = 0;
+            while (nc < jb.L && ent[nc].pair.m != 0.0f && !lessScore(ent[nc].pair, g)) {
+                cand[jb.colOff + nc] = ent[nc].col;
+                ++nc;
+            }
+            jb.nCand = nc;
+        }
+        CK(cudaMemcpyAsync(ctx->dAlignJobs.p, jobs.data(), nb * sizeof(AlignJob), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload traceback jobs");
+        CK(cudaMemcpyAsync(ctx->dAlignCand.p, cand.data(), (size_t)cols * sizeof(int), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload traceback candidates");
+        CK(cudaMemsetAsync(ctx->dAlignMark.p, 0, (size_t)cols, ctx->stream), "zero aligned flags");
+        walkKernel<<<(nb + 31) / 32, 32, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, nb, ctx->dAlignCand.p, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p, ctx->dAlignCells.p,
+            ctx->dAlignX.p, ctx->dAlignSuf.p, ctx->dAlignRev.p, ctx->dAlignFwd.p, ctx->dAlignMark.p,
+            ctx->dAlignSims.p, ctx->dAlignSegs.p, ctx->dAlignCounts.p);
+        CK(cudaGetLastError(), "traceback walk kernel");
+        std::vector<int> counts(2 * nb);
+        CK(cudaMemcpyAsync(counts.data(), ctx->dAlignCounts.p, 2 * nb * sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "download traceback counts");
+        CK(cudaStreamSynchronize(ctx->stream), "traceback walks");
+        std::vector<long long> base(2 * nb);
+        long long ns = 0, ng = 0;
+        for (int j = 0; j < nb; ++j) {
+            if (counts[2 * j] < 0) return ctx->fail(DMST_ERANGE, "traceback: segment space of a hit exhausted");
+            base[j] = ns;
+            base[nb + j] = ng;
+            ns += counts[2 * j];
+            ng += counts[2 * j + 1];
+        }
+        std::vector<AlignSim> simH((size_t)ns);
+        std::vector<Seg> segH((size_t)ng);
+        if (ns > 0) {
+            CK(ctx->dAlignSimOut.ensure((size_t)ns), "alloc traceback output");
+            CK(ctx->dAlignSegOut.ensure((size_t)std::max<long long>(ng, 1)), "alloc traceback output");
+            CK(cudaMemcpyAsync(ctx->dAlignBase.p, base.data(), 2 * nb * sizeof(long long), cudaMemcpyHostToDevice,
+                               ctx->stream),
+               "upload traceback offsets");
+            gatherKernel<<<nb, 128, 0, ctx->stream>>>(ctx->dAlignJobs.p, ctx->dAlignSims.p, ctx->dAlignSegs.p,
+                                                      ctx->dAlignCounts.p, ctx->dAlignBase.p, ctx->dAlignBase.p + nb,
+                                                      ctx->dAlignSimOut.p, ctx->dAlignSegOut.p);
+            CK(cudaGetLastError(), "traceback gather kernel");
+            CK(cudaMemcpyAsync(simH.data(), ctx->dAlignSimOut.p, ns * sizeof(AlignSim), cudaMemcpyDeviceToHost,
+                               ctx->stream),
+               "download alignments");
+            if (ng > 0)
+                CK(cudaMemcpyAsync(segH.data(), ctx->dAlignSegOut.p, ng * sizeof(Seg), cudaMemcpyDeviceToHost,
+                                   ctx->stream),
+                   "download segments");
+            CK(cudaStreamSynchronize(ctx->stream), "traceback results");
+        }
+        const long long segBase0 = (long long)ctx->alignSegOut.size();
+        for (int j = 0; j < nb; ++j) {
+            for (int q = 0; q < counts[2 * j]; ++q) {
+                const AlignSim &a = simH[base[j] + q];
+                dmst_alignment o;
+                o.pair = hits[b0 + j];
+                o.score = dmst_score{a.m, a.e};
+                o.ln_score = scoreLn(a.m, a.e);
+                o.anchor1 = a.anchor1;
+                o.anchor2 = a.anchor2;
+                o.seg_begin = segBase0 + base[nb + j] + a.segBegin;
+                o.seg_count = a.segCount;
+                o.pad = 0;
+                ctx->alignOut.push_back(o);
+            }
+        }
+        for (long long q = 0; q < ng; ++q)
+            ctx->alignSegOut.push_back(dmst_segment{segH[q].start1, segH[q].start2, segH[q].length});
+        b0 = b1;
+    }
+    *n_alignments = ctx->alignOut.size();
+    *n_segments = ctx->alignSegOut.size();
+    return DMST_OK;
+}
+
+int dmst_align_fetch(const dmst_ctx *ctx, dmst_alignment *alignments, size_t cap_alignments, dmst_segment *segments,
+                     size_t cap_segments) {
+    if (!ctx) return DMST_EINVAL;
+    const size_t na = ctx->alignOut.size(), ns = ctx->alignSegOut.size();
+    if (cap_alignments < na || cap_segments < ns) return DMST_ERANGE;
+    if ((na && !alignments) || (ns && !segments)) return DMST_EINVAL;
+    if (na) std::memcpy(alignments, ctx->alignOut.data(), na * sizeof(dmst_alignment));
+    if (ns) std::memcpy(segments, ctx->alignSegOut.data(), ns * sizeof(dmst_segment));
+    return DMST_OK;
 }
 
 int dmst_filter_threshold(double lambda_filter, double k_filter, double total_length, double filter_evalue,

@@ -43,6 +43,7 @@
 #pragma once
 
 #include "dp_exact.cuh"
+#include "dp_traceback_job.cuh"
 #include "dp_wavefront.cuh"
 
 namespace dmst {
@@ -294,12 +295,20 @@ __global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int 
 // profiles leave the shared memory to the windows.
 // ANCH: also the per-column anchors of each pair (anchorOff[pair] >= 0: the
 // offset of its L columns in anchorM / anchorE / anchorRow).
-template <bool ANCH>
+// ALIGN (with ANCH): pairs with a traceback job (jobOf[pair] >= 0) also keep
+// what the traceback tables are built from: the replay sweeps' row-major W0
+// and W1 before each row's rescale (at float offset 2 AlignJob::cellOff in
+// alignCells: W0 at [0, (M+1) L), W1 at [(M+1) L, 2 (M+1) L)) and the
+// reference's rescale counts (AlignJob::rowOff in alignRows: cntB at
+// [0, M+2), cntF at [M+2, 2 (M+2))).
+template <bool ANCH, bool ALIGN = false>
 __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
     exactWaveKernel(const int *queue, int *queueCount, const DevPair *pairs, const DevProfile *profiles,
                     const float *emit, const float *params, const uint8_t *codes, const float *seeds,
                     const PairScales *scales, float *pool, long long slotFloats, ExactOut *out,
-                    const long long *anchorOff, float *anchorM, int *anchorE, int *anchorRow) {
+                    const long long *anchorOff, float *anchorM, int *anchorE, int *anchorRow,
+                    const int *jobOf = nullptr, const AlignJob *jobs = nullptr, float *alignCells = nullptr,
+                    int *alignRows = nullptr) {
     extern __shared__ float4 smRaw[];
     Window *wins = reinterpret_cast<Window *>(smRaw);
     __shared__ float smBg[32];
@@ -362,10 +371,19 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         x.anchorPart = reinterpret_cast<float *>(x.cntF + (p.M + 2));
         ExactBest filt{0.0, 0}, mid{0.0, 0};
         bool ok = true;
+        float *alignW0 = nullptr, *alignW1 = nullptr;
+        int *alignCnt = nullptr;
+        if (ALIGN && jobOf[pi] >= 0) {
+            const AlignJob &jb = jobs[jobOf[pi]];
+            alignW0 = alignCells + 2 * jb.cellOff;  // two floats per cell
+            alignW1 = alignW0 + (size_t)(p.M + 1) * p.L;
+            alignCnt = alignRows + jb.rowOff;
+        }
         // Four sweeps, each over every warp; the counts scan between them.
         for (int phase = 0; phase < 4; ++phase) {
             if (lane == 0) progress[warp] = warp < W ? pipePos(a, -1) : INT_MAX;
             __syncthreads();
+            a.alignOut = phase == 2 ? alignW1 : (phase == 3 ? alignW0 : nullptr);
             if (warp < W && ok) {
                 switch (phase) {
                 case 0: ok = backwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
@@ -377,6 +395,12 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
             __syncthreads();
             ok = ok && abortFlag == 0;
             if (phase < 2 && threadIdx.x == 0 && ok) scanCounts(x.rowMax, x.rowCnt, phase == 0 ? x.cntB : x.cntF, p.M, phase == 0);
+        }
+        if (ALIGN && ok && alignCnt != nullptr) {
+            for (int i = threadIdx.x; i < p.M + 2; i += blockDim.x) {
+                alignCnt[i] = x.cntB[i];
+                alignCnt[p.M + 2 + i] = x.cntF[i];
+            }
         }
         if (ANCH && ok && anchorOff[pi] >= 0) {
             // fold the stripes' partials of each column in row order

@@ -1,0 +1,548 @@
+// Traceback of the hit path (dummest-dp-forward.hh:276-453, :471-535,
+// dummest-dp.hh:119-268, dummest-traceback.hh:6-118), for the jobs of
+// dp_traceback_job.cuh, after the exact kernel's replay stored each job's W0,
+// W1 and rescale counts:
+//
+//   sidesKernel     column masses: reverseSide[j] = sum over rows (M..0) of W1
+//                   and forwardSide[j] = sum over rows (0..M) of W0, each
+//                   scaled down with its rows' rescales (the reference's
+//                   per-cell fma(1, w, side) and per-row rescaleRow);
+//   flankKernel     buildFlankEVs: the entry and exit flank totals as exact
+//                   scores, and their largest exponents;
+//   xTableKernel    X(i, j) = promote(X_ij, cntF_i) * promote(W1[i+1][j],
+//                   cntB_{i+1}), the forward's combined match scores, and
+//                   each row's largest exponent;
+//   optimalKernel   the prefix- and suffix-optimal tables in the row-scaled
+//                   float form of dummest-scalerow.hh: each row is a running
+//                   maximum (a block-wide max scan) of candidates read from
+//                   the row before;
+//   walkKernel      the anchors in the reference's sorted order: for each
+//                   anchor not yet covered, the forward and reverse walks
+//                   and the overlap test against the columns already aligned.
+//
+// Columns at or past a pair's length are not built: the reference's values
+// there are zero (W1 is masked, so X and the exit flank totals are 0) or
+// never read (the prefix table right of the anchor), so a per-pair width L
+// gives the reference's tables and walks whatever its batch width.
+#pragma once
+
+#include "dp_common.cuh"
+#include "dp_exact.cuh"
+#include "dp_traceback_job.cuh"
+#include "null_model.cuh"
+
+namespace dmst {
+
+// promoteRescaledScore, the scalar form (dummest-score.hh:107-116).
+__device__ __forceinline__ XS promoteScalar(float v, int cum) {
+    if (!(v > 0.0f)) return xsZero();
+    cum = clampCount(cum);
+    if (!(v < INFINITY)) return XS{0.99999994f, 1023 + kRescaleBits * cum};
+    return splitNorm((double)v, kRescaleBits * cum);
+}
+
+// scoreToRowScale / scoreFromRowScale (dummest-scalerow.hh:26-55): the score
+// moved to row exponent E by rewriting the exponent field, and back.
+__device__ __forceinline__ float toRow(XS s, int E) {
+    const unsigned u = __float_as_uint(s.m);
+    int d = s.e - E;
+    d = d > 0 ? 0 : (d < -1000 ? -1000 : d);
+    const int ne = 126 + d;
+    const float r = __uint_as_float((u & 0x807FFFFFu) | ((unsigned)(ne > 0 ? ne : 0) << 23));
+    return (s.m == 0.0f || ne <= 0) ? 0.0f : r;
+}
+__device__ __forceinline__ XS fromRow(float s, int E) {
+    const unsigned u = __float_as_uint(s);
+    const unsigned ef = (u >> 23) & 0xFFu;
+    const bool live = (s > 0.0f) && ef != 0;
+    const XS o{__uint_as_float((u & 0x807FFFFFu) | (126u << 23)), (int)ef - 126 + E};
+    return live ? o : xsZero();
+}
+
+__device__ __forceinline__ XS ldXS(const XS *p) {
+    const float2 v = *reinterpret_cast<const float2 *>(p);
+    return XS{v.x, __float_as_int(v.y)};
+}
+__device__ __forceinline__ void stXS(XS *p, XS s) {
+    *reinterpret_cast<float2 *>(p) = make_float2(s.m, __int_as_float(s.e));
+}
+
+// Column masses, one thread per (job, column).  Block 0 of a job also resets
+// the X table's row maxima (INT_MIN, dummest-dp-backward.hh:265-269).
+__global__ void sidesKernel(const AlignJob *jobs, const float *cells, int *rows, float *colR, float *colF) {
+    const AlignJob jb = jobs[blockIdx.y];
+    const int M = jb.M, L = jb.L;
+    int *cntB = rows + jb.rowOff, *cntF = cntB + (M + 2), *rowMaxX = cntF + (M + 2);
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < M + 2; i += blockDim.x) rowMaxX[i] = INT_MIN;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    const float *W0 = cells + 2 * jb.cellOff;
+    const float *W1 = W0 + (size_t)(M + 1) * L;
+    float r = 0.0f;
+    for (int i = M; i >= 0; --i) {
+        r = __fadd_rn(r, W1[(size_t)i * L + j]);
+        if (cntB[i] != cntB[i + 1]) r = __fmul_rn(r, stepsDown(cntB[i] - cntB[i + 1]));
+    }
+    float f = 0.0f;
+    for (int i = 0; i <= M; ++i) {
+        f = __fadd_rn(f, W0[(size_t)i * L + j]);
+        if (cntF[i + 1] != cntF[i]) f = __fmul_rn(f, stepsDown(cntF[i + 1] - cntF[i]));
+    }
+    colR[jb.colOff + j] = r;
+    colF[jb.colOff + j] = f;
+}
+
+// buildFlankEVs for one job per thread (dummest-dp.hh:137-256).  work holds
+// 2 (L + 4) scores per job: the middle entry masses and the suffix rest
+// masses; revEv receives the entry totals (reverseSideEv), fwdEv the exit
+// totals (forwardSideEv).
+__global__ void flankKernel(const AlignJob *jobs, int nJobs, const DevPair *pairs, const DevProfile *profiles,
+                            const uint8_t *codes, const float *seeds, const PairScales *scales, NullRates nr,
+                            const float *colR, const float *colF, int *rows, XS *work, XS *revEv, XS *fwdEv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nJobs) return;
+    const AlignJob jb = jobs[t];
+    const DevPair p = pairs[jb.pair];
+    const float *bg = profiles[p.prof].bg;
+    const uint8_t *cd = codes + p.codeOff;
+    const float *pre = seeds + p.seedOff;
+    const PairScales sc = scales[jb.pair];
+    const int M = jb.M, L = jb.L;
+    const int *cntB = rows + jb.rowOff, *cntF = cntB + (M + 2);
+    int *sideMax = rows + jb.rowOff + 3 * (M + 2);
+    const float *cR = colR + jb.colOff, *cF = colF + jb.colOff;
+    XS *mid = work + 2 * (jb.colOff + 4LL * t);
+    XS *rest = mid + (L + 4);
+    XS *rev = revEv + jb.colOff, *fwd = fwdEv + jb.colOff;
+
+    const double sr = nr.single, dr = nr.dbl;
+    const double keep = 1.0 - sr - dr;
+    const double third = 1.0 / 3.0;
+    const XS aS1 = splitNorm((double)sc.s1, 0), aS2 = splitNorm((double)sc.s2, 0), aSC = splitNorm((double)sc.sC, 0);
+    const XS bS1 = scaleScore(aS1, 4.0), bS2 = scaleScore(aS2, 16.0);
+    auto bgc = [&](int pos) { return (pos >= 0 && pos < L) ? splitNorm((double)bg[cd[pos]], 0) : xsZero(); };
+    auto preS = [&](int pos) { return splitNorm((double)pre[pos], 0); };
+    const int cB0 = cntB[0], cFM = cntF[M + 1];
+
+    // middle entry masses, run backward
+    for (int q = L; q < L + 4; ++q) mid[q] = xsZero();
+    for (int j = L - 1; j >= 0; --j) {
+        XS c = scalarMul(scaleScore(mid[j + 1], sr), aS1);
+        c = scalarAdd(c, scalarMul(scaleScore(mid[j + 2], dr), aS2));
+        c = scalarAdd(c, scalarMul(scaleScore(scalarMul(mid[j + 3], aSC), keep), bgc(j + 1)));
+        mid[j] = scalarAdd(promoteScalar(cR[j], cB0), c);
+    }
+    // cover of [j, end): the empty rest at the end counts 1
+    for (int q = 0; q < L + 4; ++q) rest[q] = xsZero();
+    rest[L] = pow2Score(0);
+    for (int j = L - 1; j >= 0; --j) {
+        const XS one = scalarMul(scaleScore(rest[j + 1], sr), aS1);
+        const XS two = (j + 1 <= L - 1) ? scalarMul(scaleScore(rest[j + 2], dr), aS2) : scaleScore(bS1, dr * 0.25);
+        XS three;
+        if (j + 2 <= L - 1)
+            three = scalarMul(scaleScore(scalarMul(rest[j + 3], aSC), keep), bgc(j));
+        else if (j + 1 <= L - 1)
+            three = scaleScore(bS2, keep * 0.0625);
+        else
+            three = scaleScore(bS1, keep * 0.25);
+        rest[j] = scalarAdd(one, scalarAdd(two, three));
+    }
+    // forward arrival masses (rolling), entry tiles and the per-base amounts;
+    // the entry totals accumulate forward, the amounts wait in fwd
+    XS fa1 = xsZero(), fa2 = xsZero(), fa3 = xsZero();  // arrival at j-1, j-2, j-3
+    XS cum = xsZero();
+    int revMax = INT_MIN;
+    for (int j = 0; j < L; ++j) {
+        XS single = xsZero(), dbl = xsZero(), codon = xsZero();
+        if (j == 0) single = preS(0);
+        else single = scalarMul(scaleScore(preS(j - 1), sr), aS1);
+        if (j == 1) dbl = scaleScore(aS2, third);
+        else if (j >= 2) dbl = scalarMul(scaleScore(preS(j - 2), dr), aS2);
+        if (j == 2) codon = scalarMul(scaleScore(aSC, third), bgc(0));
+        else if (j >= 3) codon = scalarMul(scaleScore(scalarMul(preS(j - 3), aSC), keep), bgc(j - 2));
+        const XS weighted = scalarAdd(single, scalarAdd(scaleScore(dbl, 2.0), scaleScore(codon, 3.0)));
+        XS total = scalarMul(mid[j], weighted);
+        if (j >= 1) {
+            const XS exit1 = scalarMul(scaleScore(rest[j + 1], sr), aS1);
+            total = scalarAdd(total, scalarMul(fa1, exit1));
+        }
+        if (j >= 2) {
+            const XS exit2 = scalarMul(scaleScore(rest[j + 1], dr), aS2);
+            total = scalarAdd(total, scaleScore(scalarMul(fa2, exit2), 2.0));
+        }
+        if (j >= 3) {
+            const XS exit3 = scalarMul(scaleScore(scalarMul(rest[j + 1], aSC), keep), bgc(j - 2));
+            total = scalarAdd(total, scaleScore(scalarMul(fa3, exit3), 3.0));
+        }
+        if (j == L - 1) {  // leftover endings at the last base
+            total = scalarAdd(total, scaleScore(scalarMul(fa1, scaleScore(bS1, dr * 0.25)), 2.0));
+            total = scalarAdd(total, scaleScore(scalarMul(fa1, scaleScore(bS1, keep * 0.25)), 3.0));
+            if (j - 2 >= 0) total = scalarAdd(total, scaleScore(scalarMul(fa2, scaleScore(bS2, keep * 0.0625)), 3.0));
+        }
+        const XS unified = scaleScore(total, third);
+        fwd[j] = unified;
+        cum = scalarAdd(cum, unified);
+        rev[j] = cum;
+        if (cum.m != 0.0f && cum.e > revMax) revMax = cum.e;
+        // this column's arrival, for the columns after it
+        XS arr = promoteScalar(cF[j], cFM);
+        if (j >= 1) arr = scalarAdd(arr, scalarMul(scaleScore(fa1, sr), aS1));
+        if (j >= 2) arr = scalarAdd(arr, scalarMul(scaleScore(fa2, dr), aS2));
+        if (j >= 3) arr = scalarAdd(arr, scalarMul(scaleScore(scalarMul(fa3, aSC), keep), bgc(j - 2)));
+        fa3 = fa2;
+        fa2 = fa1;
+        fa1 = arr;
+    }
+    // exit totals accumulate backward
+    cum = xsZero();
+    int fwdMax = INT_MIN;
+    for (int j = L - 1; j >= 0; --j) {
+        cum = scalarAdd(cum, fwd[j]);
+        fwd[j] = cum;
+        if (cum.m != 0.0f && cum.e > fwdMax) fwdMax = cum.e;
+    }
+    sideMax[0] = revMax;
+    sideMax[1] = fwdMax;
+}
+
+// X table, one thread per (job, column, group of kXRows rows).
+constexpr int kXRows = 8;
+__global__ void xTableKernel(const AlignJob *jobs, const DevPair *pairs, const DevProfile *profiles, const float *emit,
+                             const float *params, const uint8_t *codes, const PairScales *scales, const float *cells,
+                             int *rows, XS *X) {
+    const AlignJob jb = jobs[blockIdx.z];
+    const int M = jb.M, L = jb.L;
+    const int i0 = blockIdx.y * kXRows;
+    if (i0 > M) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevPair p = pairs[jb.pair];
+    const DevProfile &pr = profiles[p.prof];
+    const float sC = scales[jb.pair].sC;
+    const int *cntB = rows + jb.rowOff, *cntF = cntB + (M + 2);
+    int *rowMaxX = rows + jb.rowOff + 2 * (M + 2);
+    const float *W0 = cells + 2 * jb.cellOff;
+    const float *W1 = W0 + (size_t)(M + 1) * L;
+    const int code = (j >= 2 && j < L) ? (int)codes[p.codeOff + j - 2] : kPad;
+    const float *em = emit + pr.emitOff + (size_t)code * pr.rowPad;
+    for (int i = i0; i < i0 + kXRows && i <= M; ++i) {
+        int e = INT_MIN;
+        if (j < L) {
+            const float enter = __fmul_rn(params[pr.paramOff + (size_t)i * kParamFloats + 10], sC);
+            const float w3 = j >= 3 ? W0[(size_t)i * L + j - 3] : 0.0f;
+            const float xf = __fmul_rn(__fmul_rn(enter, em[i]), w3);
+            float w1n = 0.0f;
+            if (i + 1 <= M) w1n = __fmul_rn(W1[(size_t)(i + 1) * L + j], stepsDown(cntB[i + 1] - cntB[i + 2]));
+            const XS x = planeMul(promote(xf, cntF[i]), promote(w1n, cntB[i + 1]));
+            stXS(X + jb.cellOff + (size_t)i * L + j, x);
+            if (x.m != 0.0f) e = x.e;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+        if ((threadIdx.x & 31) == 0 && e != INT_MIN) atomicMax(rowMaxX + i, e);
+    }
+}
+
+// Max scans over a row of kOptThreads x kOptPer columns at a time.
+constexpr int kOptThreads = 512;
+constexpr int kOptPer = 8;
+
+// Exclusive max of the threads' values in thread order (reverse: from the
+// last thread down); all values >= 0, and 0 where nothing comes before.
+__device__ __forceinline__ float blockExclusiveMax(float v, float *sm, bool reverse) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nw = kOptThreads / 32;
+    float incl = v;
+    if (!reverse) {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl = fmaxf(incl, t);
+        }
+    } else {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float t = __shfl_down_sync(0xffffffffu, incl, o);
+            if (lane + o < 32) incl = fmaxf(incl, t);
+        }
+    }
+    if (reverse ? lane == 0 : lane == 31) sm[warp] = incl;
+    __syncthreads();
+    float before = 0.0f;
+    if (!reverse) {
+        for (int w = 0; w < warp; ++w) before = fmaxf(before, sm[w]);
+        const float t = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane >= 1) before = fmaxf(before, t);
+    } else {
+        for (int w = warp + 1; w < nw; ++w) before = fmaxf(before, sm[w]);
+        const float t = __shfl_down_sync(0xffffffffu, incl, 1);
+        if (lane + 1 < 32) before = fmaxf(before, t);
+    }
+    __syncthreads();
+    return before;
+}
+
+// Prefix- and suffix-optimal tables of one job per CTA
+// (dummest-dp-forward.hh:295-451).  The prefix table overwrites the job's W0
+// and W1 (no longer read); the suffix table has its own array.
+__global__ void __launch_bounds__(kOptThreads) optimalKernel(const AlignJob *jobs, float *cells, const int *rows,
+                                                             const XS *X, const XS *revEv, const XS *fwdEv,
+                                                             XS *suffix) {
+    __shared__ float sm[kOptThreads / 32];
+    __shared__ float carry;
+    const AlignJob jb = jobs[blockIdx.x];
+    const int M = jb.M, L = jb.L;
+    const int *rowMaxX = rows + jb.rowOff + 2 * (M + 2);
+    const int revMax = rows[jb.rowOff + 3 * (M + 2)], fwdMax = rows[jb.rowOff + 3 * (M + 2) + 1];
+    XS *pre = reinterpret_cast<XS *>(cells + 2 * jb.cellOff);
+    const XS *Xj = X + jb.cellOff;
+    XS *suf = suffix + jb.cellOff;
+    const XS *rev = revEv + jb.colOff, *fwd = fwdEv + jb.colOff;
+    constexpr int chunk = kOptThreads * kOptPer;
+
+    // prefix-optimal: rows 0..M, each a running maximum left to right
+    int runMax = INT_MIN;
+    for (int i = 0; i <= M; ++i) {
+        runMax = max(runMax, rowMaxX[i]);
+        const int E = max(runMax, revMax) + 1;
+        if (threadIdx.x == 0) carry = 0.0f;
+        __syncthreads();
+        for (int c0 = 0; c0 < L; c0 += chunk) {
+            float v[kOptPer];
+            float run = 0.0f;
+            const int jb0 = c0 + threadIdx.x * kOptPer;
+#pragma unroll
+            for (int q = 0; q < kOptPer; ++q) {
+                const int j = jb0 + q;
+                float cand = 0.0f;
+                if (j < L) {
+                    const float comb = toRow(ldXS(Xj + (size_t)i * L + j), E);
+                    const float rs = toRow(ldXS(rev + j), E);
+                    if (i == 0) {
+                        cand = fmaxf(comb, rs);
+                    } else {
+                        const XS *pp = pre + (size_t)(i - 1) * L;
+                        const float up = toRow(ldXS(pp + j), E);
+                        const float succ = j >= 3 ? toRow(ldXS(pp + j - 3), E) : 0.0f;
+                        cand = fmaxf(fmaxf(up, __fadd_rn(comb, succ)), rs);
+                    }
+                }
+                run = fmaxf(run, cand);
+                v[q] = run;
+            }
+            const float before = fmaxf(blockExclusiveMax(run, sm, false), carry);
+            __syncthreads();  // every thread has read carry
+#pragma unroll
+            for (int q = 0; q < kOptPer; ++q) {
+                const int j = jb0 + q;
+                if (j < L) stXS(pre + (size_t)i * L + j, fromRow(fmaxf(before, v[q]), E));
+            }
+            if (threadIdx.x == kOptThreads - 1) carry = fmaxf(before, run);
+            __syncthreads();
+        }
+    }
+    // suffix-optimal: rows M..0, each a running maximum right to left
+    runMax = INT_MIN;
+    const int nChunks = (L + chunk - 1) / chunk;
+    for (int i = M; i >= 0; --i) {
+        runMax = max(runMax, rowMaxX[i]);
+        const int E = max(runMax, fwdMax) + 1;
+        if (threadIdx.x == 0) carry = 0.0f;
+        __syncthreads();
+        for (int cc = nChunks - 1; cc >= 0; --cc) {
+            const int c0 = cc * chunk;
+            float v[kOptPer];
+            float run = 0.0f;
+            const int jb0 = c0 + threadIdx.x * kOptPer;
+#pragma unroll
+            for (int q = kOptPer - 1; q >= 0; --q) {
+                const int j = jb0 + q;
+                float cand = 0.0f;
+                if (j < L) {
+                    const float fs = toRow(ldXS(fwd + j), E);
+                    if (i == M) {
+                        cand = fs;
+                    } else {
+                        const XS *np = suf + (size_t)(i + 1) * L;
+                        const float down = toRow(ldXS(np + j), E);
+                        float cps = 0.0f;
+                        if (j + 3 < L)
+                            cps = __fadd_rn(toRow(ldXS(Xj + (size_t)i * L + j + 3), E), toRow(ldXS(np + j + 3), E));
+                        cand = fmaxf(fmaxf(down, fs), cps);
+                    }
+                }
+                run = fmaxf(run, cand);
+                v[q] = run;
+            }
+            const float after = fmaxf(blockExclusiveMax(run, sm, true), carry);
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < kOptPer; ++q) {
+                const int j = jb0 + q;
+                if (j < L) stXS(suf + (size_t)i * L + j, fromRow(fmaxf(after, v[q]), E));
+            }
+            if (threadIdx.x == 0) carry = fmaxf(after, run);
+            __syncthreads();
+        }
+    }
+}
+
+// One similarity of the traceback output.
+struct AlignSim {
+    float m;   // the anchor's exact score (AlignedSimilarity::pair)
+    int e;
+    int anchor1, anchor2;
+    int segBegin, segCount;  // in the job's segment pairs
+};
+
+struct Seg {
+    int start1, start2, length;
+};
+
+// The walks of one job per thread (dummest-traceback.hh:35-118) over the
+// candidates in order (dummest-dp-forward.hh:497-532).  counts[2 t] =
+// similarities, counts[2 t + 1] = segments; counts[2 t] = -1 if the segment
+// space ran out (it cannot for alignments of the reference's shape).
+__global__ void walkKernel(const AlignJob *jobs, int nJobs, const int *cand, const float *anchorM,
+                           const int *anchorE, const int *anchorRow, const float *cells, const XS *X,
+                           const XS *suffix, const XS *revEv, const XS *fwdEv, uint8_t *aligned, AlignSim *sims,
+                           Seg *segs, int *counts) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nJobs) return;
+    const AlignJob jb = jobs[t];
+    const int M = jb.M, L = jb.L;
+    const XS *pre = reinterpret_cast<const XS *>(cells + 2 * jb.cellOff);
+    const XS *Xj = X + jb.cellOff;
+    const XS *suf = suffix + jb.cellOff;
+    const XS *rev = revEv + jb.colOff, *fwd = fwdEv + jb.colOff;
+    uint8_t *mark = aligned + jb.colOff;
+    Seg *out = segs + jb.segOff;
+    const long long cap = alignSegCap(M, L);
+    Seg *rtmp = out + cap;  // the reverse walk's matches, in walk order (M + 2 entries)
+    AlignSim *sv = sims + jb.colOff;
+    auto S = [&](int i, int j) { return (i <= M && j < L) ? ldXS(suf + (size_t)i * L + j) : xsZero(); };
+    auto P = [&](int i, int j) { return ldXS(pre + (size_t)i * L + j); };
+    int nSims = 0, top = 0;
+    bool overflow = false;
+    for (int c = 0; c < jb.nCand && !overflow; ++c) {
+        const int a2 = cand[jb.colOff + c];
+        if (mark[a2]) continue;
+        const int a1 = anchorRow[jb.colOff + a2];
+        // forward walk: matches appended after the accepted segments
+        int nf = 0;
+        {
+            int i = a1, pos = a2;
+            while (i <= M && pos < L) {
+                XS best = xsZero();
+                int bi = INT_MAX, bj = INT_MAX;
+                bool emit = false;
+                if (pos + 3 < L) {
+                    const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos + 3), S(i + 1, pos + 3));
+                    if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos + 3; emit = true; }
+                }
+                XS cd = S(i + 1, pos);
+                if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos; emit = false; }
+                cd = S(i, pos + 1);
+                if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos + 1; emit = false; }
+                cd = ldXS(fwd + pos);
+                if (scoreLess(best, cd)) { best = cd; bi = INT_MAX; bj = INT_MAX; emit = false; }
+                if (emit) {  // addForwardMatch(i, pos + 1)
+                    const int p1 = i, p2 = pos + 1;
+                    bool add = true;
+                    if (nf > 0) {
+                        Seg &x = out[top + nf - 1];
+                        if (x.start1 + x.length == p1 && x.start2 + x.length == p2) ++x.length;
+                        if (x.start1 + x.length > p1 || x.start2 + x.length > p2) add = false;
+                    }
+                    if (add) {
+                        if (top + nf >= cap) { overflow = true; break; }
+                        out[top + nf++] = Seg{p1, p2, 1};
+                    }
+                }
+                i = bi;
+                pos = bj;
+            }
+        }
+        if (overflow) break;
+        // reverse walk: each match goes before the segments so far; the one it
+        // may extend is the first of them
+        int nr = 0;
+        {
+            int i = a1 - 1, pos = a2;
+            while (i >= 0 && pos >= 0) {
+                XS best = xsZero();
+                int bi = -1, bj = -1;
+                bool emit = false;
+                if (pos >= 3) {
+                    const XS succ = i >= 1 ? P(i - 1, pos - 3) : xsZero();
+                    const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos), succ);
+                    if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos - 3; emit = true; }
+                }
+                if (i >= 1) {
+                    const XS cd = P(i - 1, pos);
+                    if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos; emit = false; }
+                }
+                if (pos > 0) {
+                    const XS cd = P(i, pos - 1);
+                    if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos - 1; emit = false; }
+                }
+                const XS cd = ldXS(rev + pos);
+                if (scoreLess(best, cd)) { best = cd; bi = -1; bj = -1; emit = false; }
+                if (emit) {  // addReverseMatch(i, pos - 2)
+                    const int p1 = i, p2 = pos - 2;
+                    bool add = true;
+                    Seg *x = nr > 0 ? &rtmp[nr - 1] : (nf > 0 ? &out[top] : nullptr);
+                    if (x) {
+                        if (x->start1 - 1 == p1 && x->start2 - 1 == p2) {
+                            --x->start1;
+                            --x->start2;
+                            ++x->length;
+                        }
+                        if (x->start1 <= p1 || x->start2 <= p2) add = false;
+                    }
+                    if (add) {
+                        if (nr >= M + 2 || top + nf + nr >= cap) { overflow = true; break; }
+                        rtmp[nr++] = Seg{p1, p2, 1};
+                    }
+                }
+                i = bi;
+                pos = bj;
+            }
+        }
+        if (overflow) break;
+        // final order: reverse matches (last found first), then the forward ones
+        if (nr > 0) {
+            for (int q = nf - 1; q >= 0; --q) out[top + nr + q] = out[top + q];
+            for (int q = 0; q < nr; ++q) out[top + q] = rtmp[nr - 1 - q];
+        }
+        const int n = nf + nr;
+        int beg = n == 0 ? a2 : out[top].start2;
+        int end = n == 0 ? a2 : out[top + n - 1].start2 + out[top + n - 1].length;
+        beg = max(beg, 0);
+        end = min(end, L);
+        bool overlaps = false;
+        for (int q = beg; q < end; ++q)
+            if (mark[q]) {
+                overlaps = true;
+                break;
+            }
+        if (overlaps) continue;
+        for (int q = beg; q < end; ++q) mark[q] = 1;
+        sv[nSims++] = AlignSim{anchorM[jb.colOff + a2], anchorE[jb.colOff + a2], a1, a2, top, n};
+        top += n;
+    }
+    counts[2 * t] = overflow ? -1 : nSims;
+    counts[2 * t + 1] = top;
+}
+
+// Gathers the jobs' similarities and segments into one list each
+// (simBase / segBase: exclusive sums of the counts), one CTA per job.
+__global__ void gatherKernel(const AlignJob *jobs, const AlignSim *sims, const Seg *segs, const int *counts,
+                             const long long *simBase, const long long *segBase, AlignSim *simOut, Seg *segOut) {
+    const AlignJob jb = jobs[blockIdx.x];
+    const int ns = counts[2 * blockIdx.x], ng = counts[2 * blockIdx.x + 1];
+    for (int q = threadIdx.x; q < ns; q += blockDim.x) simOut[simBase[blockIdx.x] + q] = sims[jb.colOff + q];
+    for (int q = threadIdx.x; q < ng; q += blockDim.x) segOut[segBase[blockIdx.x] + q] = segs[jb.segOff + q];
+}
+
+}  // namespace dmst

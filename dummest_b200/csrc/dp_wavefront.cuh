@@ -74,6 +74,10 @@ struct SweepArgs {
     // order) is then ring + (sp % ringSlots) * ringStride.
     int sFirst, sStep, nMine, ringSlots;
     long long ringStride;
+    // Exact replay for the traceback: the row-major (M+1) x L matrix that takes
+    // each cell's value before its row's rescale (backward: W1, forward: W0),
+    // or null.
+    float *alignOut;
 
     __device__ __forceinline__ const uint8_t *codes() const {
         return *reinterpret_cast<const uint8_t *const volatile *>(&cold->codes);
@@ -499,6 +503,8 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
                 stepMax = fmaxf(stepMax, Y);
             }
             if (MODE == kReplay) {
+                if (a.alignOut != nullptr && rowBase + k <= a.M())
+                    a.alignOut[(size_t)(rowBase + k) * a.L + (a.L - 1 - b.jj)] = W;
                 // What leaves the row is scaled by the row's own decision.
                 const float Wo = W * b.fOut[k];
                 b.rowBest[k] = fmax(b.rowBest[k], (double)Wo * (double)prev);
@@ -804,7 +810,10 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             // their seed, which reaches no real row and multiplies a zero W1.
             const float W0 = (MODE == kMid) ? win0 + __fadd_rn(zs, prev) : win0 + __fmaf_rn(prev, f.c.rs[k], zs);
             if (MODE == kMid) bv[k] = W0 * q[k];
-            if (MODE == kReplay) f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
+            if (MODE == kReplay) {
+                f.rowBest[k] = fmax(f.rowBest[k], (double)W0 * (double)q[k]);
+                if (a.alignOut != nullptr && rowBase + k <= a.M()) a.alignOut[(size_t)(rowBase + k) * a.L + f.j] = W0;
+            }
             if (ANCH) {
                 // wMid = promote(W0) * promote(W1): the exact double product,
                 // its mantissa rounded to float (dummest-batch.hh:216-235)
@@ -1030,6 +1039,7 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
     }
     __syncwarp();
     SweepArgs a;
+    a.alignOut = nullptr;
     a.cold = &win.cold;
     a.smE = smE;
     a.w1 = w1;

@@ -275,6 +275,40 @@ class Context:
             o += L
         return out, res
 
+    def align_raw(self, pairs, out=None):
+        """The traceback of the hit path (dmst_align) on a ctypes Pair array:
+        (alignments, segments) as ctypes arrays (Alignment, Segment)."""
+        n = len(pairs)
+        na, ns = C.c_size_t(0), C.c_size_t(0)
+        st = self.lib.dmst_align(self.h, pairs, n, out, C.byref(na), C.byref(ns))
+        self._check(st, "dmst_align")
+        al = (F.Alignment * max(na.value, 1))()
+        sg = (F.Segment * max(ns.value, 1))()
+        st = self.lib.dmst_align_fetch(self.h, al, na.value, sg, ns.value)
+        self._check(st, "dmst_align_fetch")
+        return al[:na.value], sg[:ns.value]
+
+    def align(self, seq_ids: Sequence[int], pids, min_prob_ratio):
+        """Alignments of each (read, profile) pair with its gate (dmst_align).
+        pids and min_prob_ratio are per pair (or one value for all).  Returns,
+        per pair, a list of (m, e, ln_score, anchor1, anchor2, segments) with
+        segments an (n, 3) int array of (start1, start2, length), and the
+        pairs' Result array."""
+        n = len(seq_ids)
+        pids = list(pids) if hasattr(pids, "__len__") else [pids] * n
+        mpr = list(min_prob_ratio) if hasattr(min_prob_ratio, "__len__") else [min_prob_ratio] * n
+        pairs = (F.Pair * n)()
+        for k in range(n):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = seq_ids[k], pids[k], mpr[k]
+        res = (F.Result * n)()
+        al, sg = self.align_raw(pairs, res)
+        segs = np.array([(s.start1, s.start2, s.length) for s in sg], np.int32).reshape(-1, 3)
+        out = [[] for _ in range(n)]
+        for a in al:
+            out[a.pair].append((a.score.m, a.score.e, a.ln_score, a.anchor1, a.anchor2,
+                                segs[a.seg_begin:a.seg_begin + a.seg_count].copy()))
+        return out, res
+
     def complete(self):
         """Complete the oldest pending call (dmst_score_pairs_complete); returns its Result array."""
         if not self._pending:

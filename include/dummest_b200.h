@@ -239,6 +239,47 @@ int dmst_search_submit(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, const fl
  * pairs' scores as from dmst_score_pairs(DMST_MODE_MID).  Synchronous. */
 int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *best, int *row, dmst_result *out);
 
+/* One alignment of the hit path: the reference's AlignedSimilarity
+ * (dummest-core.hh:298-317). */
+typedef struct dmst_alignment {
+    int32_t pair;       /* the pair's index in the dmst_align call */
+    dmst_score score;   /* the anchor's exact mid score (AlignedSimilarity::pair) */
+    double ln_score;    /* scoreToLog(score) (AlignedSimilarity::logProbRatio) */
+    int32_t anchor1;    /* profile row of the anchor */
+    int32_t anchor2;    /* sequence column of the anchor */
+    int64_t seg_begin;  /* its first segment pair in dmst_align_fetch's list */
+    int32_t seg_count;  /* 0: the walks from the anchor matched nothing (no MAF record) */
+    int32_t pad;
+} dmst_alignment;
+
+/* A gapless piece of an alignment (SegmentPair, dummest-core.hh:273-275):
+ * profile rows start1.., sequence columns start2.., length of them. */
+typedef struct dmst_segment {
+    int32_t start1, start2, length;
+} dmst_segment;
+
+/* The hit path with its traceback: findSimilarities(needAlign = true)
+ * (dummest-search.hh:9-17; dummest-dp-forward.hh:252-535;
+ * dummest-traceback.hh:35-118; dummest-dp.hh:119-268).  Every pair is scored
+ * (out, may be NULL, as from dmst_score_pairs(DMST_MODE_MID)); a pair whose
+ * min_prob_ratio is >= 0 and whose mid score is nonzero and at least
+ * normalizeScore(min_prob_ratio) is a hit, and its alignments are traced on
+ * the device: its per-column anchors in the reference's sorted order (the
+ * reference's std::ranges::sort, descending), each anchor at or above the
+ * gate and not inside an earlier alignment walked forward and backward over
+ * the prefix- and suffix-optimal tables, and kept unless its sequence span
+ * overlaps one kept before.  The alignments are kept in the context, the
+ * pairs' lists in the call's pair order, each in the reference's order;
+ * *n_alignments and *n_segments get their counts (dmst_align_fetch copies
+ * them).  Pairs with min_prob_ratio < 0 (the calibration call's "report")
+ * and misses have none.  Synchronous. */
+int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out, size_t *n_alignments,
+               size_t *n_segments);
+/* Copies the last dmst_align call's alignments and segment pairs (capacities
+ * at least its counts, else DMST_ERANGE). */
+int dmst_align_fetch(const dmst_ctx *ctx, dmst_alignment *alignments, size_t cap_alignments,
+                     dmst_segment *segments, size_t cap_segments);
+
 /* The filter gate as a float threshold: the smallest float best b whose
  * E-value K_filter * total_length / exp(ln(b) * lambda_filter) is at most
  * filter_evalue (the reference's expression, dummest-search.hh:158-166, in

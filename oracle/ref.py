@@ -52,6 +52,9 @@ def lib(bits: int = 32) -> C.CDLL:
                                                 P(C.c_int), P(C.c_double), P(C.c_float), P(C.c_int)]),
         "dmstref_backward_only": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float)]),
         "dmstref_anchors": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_int), P(C.c_int)]),
+        "dmstref_align": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), P(C.c_float), C.c_int, C.c_int,
+                                    P(C.c_int), P(C.c_float), P(C.c_int), P(C.c_double), P(C.c_int), P(C.c_int),
+                                    P(C.c_int), C.c_int, P(C.c_int), P(C.c_int)]),
         "dmstref_score_many": (C.c_int, [C.c_int, P(C.c_uint8), P(C.c_int64), C.c_int, C.c_int, C.c_int,
                                          P(C.c_double), P(C.c_double)]),
         "dmstref_null_model": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_float),
@@ -152,6 +155,44 @@ class RefEngine:
                                   e.ctypes.data_as(P(C.c_int)), row.ctypes.data_as(P(C.c_int))) != 0:
             raise ValueError("reference anchors failed")
         return m, e, row
+
+    def align(self, p: int, seqs, min_prob_ratio):
+        """The reference's alignments (findSimilarities with needAlign) of up to
+        simdWidth sequences in one batch, per-sequence minProbRatio.  Returns, per
+        sequence, a list of (m, e, log_prob_ratio, anchor1, anchor2, segments)
+        with segments an (n, 3) int array of (start1, start2, length)."""
+        n = len(seqs)
+        arrs, ptrs, lens = self._ptrs(seqs)
+        mpr = (C.c_float * n)(*[float(x) for x in min_prob_ratio])
+        cap = sum(len(s) for s in seqs) + 8 * n
+        segcap = 4 * cap
+        P = C.POINTER
+        ip = lambda a: a.ctypes.data_as(P(C.c_int))
+        while True:
+            lane = np.zeros(cap, np.int32)
+            pm = np.zeros(cap, np.float32)
+            pe = np.zeros(cap, np.int32)
+            lr = np.zeros(cap, np.float64)
+            a1 = np.zeros(cap, np.int32)
+            a2 = np.zeros(cap, np.int32)
+            off = np.zeros(cap + 1, np.int32)
+            segs = np.zeros(3 * segcap, np.int32)
+            need = C.c_int(0)
+            r = self.L.dmstref_align(p, ptrs, lens, mpr, n, cap, ip(lane), pm.ctypes.data_as(P(C.c_float)),
+                                     ip(pe), lr.ctypes.data_as(P(C.c_double)), ip(a1), ip(a2), ip(off), segcap,
+                                     ip(segs), C.byref(need))
+            if r == -1:
+                raise ValueError("reference align rejected the batch")
+            if r < 0:
+                cap = max(cap, -r - 1)
+                segcap = max(segcap, need.value)
+                continue
+            break
+        out = [[] for _ in range(n)]
+        for s in range(r):
+            sg = segs[3 * off[s]:3 * off[s + 1]].reshape(-1, 3).copy()
+            out[lane[s]].append((float(pm[s]), int(pe[s]), float(lr[s]), int(a1[s]), int(a2[s]), sg))
+        return out
 
     def backward_only(self, p: int, seqs) -> list[float]:
         out = []

@@ -266,6 +266,65 @@ int dmstref_anchors(int p, const uint8_t *codes, int L, float *bestM, int *bestE
     return 0;
 }
 
+// The hit path with alignments: findSimilarities(needAlign=true) on n <=
+// simdWidth lanes with per-lane minProbRatio (dummest-search.hh:9-17,
+// dummest-dp-forward.hh:471-535, dummest-traceback.hh:35-118).  Every
+// AlignedSimilarity of every lane, in the order the engine produced them:
+// lane[s], pair (m, e), logProbRatio, anchor1, anchor2, and its segment pairs
+// segs[3 k .. 3 k + 3) = (start1, start2, length) for k in
+// [segOff[s], segOff[s + 1]).  Returns the number of similarities; -1 on bad
+// input; -(1 + similarities) when simCap or segCap is too small (then
+// *needSegs holds the segments needed and nothing else is written).
+int dmstref_align(int p, const uint8_t *const *decoded, const int *lens, const float *minProbRatio, int n,
+                  int simCap, int *lane, float *pairM, int *pairE, double *logRatio, int *anchor1, int *anchor2,
+                  int *segOff, int segCap, int *segs, int *needSegs) {
+    ensureInit();
+    FtzScope ftz;
+    const Profile *pr = getProfile(p);
+    if (!pr || n < 1 || n > (int)simdWidth) return -1;
+    std::vector<std::vector<uint8_t>> seqs(n);
+    std::array<std::vector<uint8_t> *, simdWidth> ptrs{};
+    std::array<Float, simdWidth> mpr;
+    mpr.fill((Float)-2.0);
+    for (int k = 0; k < n; ++k) {
+        if (lens[k] < 3) return -1;
+        seqs[k].assign(decoded[k], decoded[k] + lens[k]);
+        ptrs[k] = &seqs[k];
+        mpr[k] = (Float)minProbRatio[k];
+    }
+    DPScratch scratch;
+    std::array<std::vector<AlignedSimilarity>, simdWidth> sims;
+    findSimilarities(sims, *pr, ptrs, mpr, scratch, n, nullptr, true);
+    int ns = 0, nseg = 0;
+    for (int k = 0; k < n; ++k)
+        for (const auto &x : sims[k]) {
+            ++ns;
+            nseg += (int)x.alignment.size();
+        }
+    if (needSegs) *needSegs = nseg;
+    if (ns > simCap || nseg > segCap) return -(1 + ns);
+    int s = 0, g = 0;
+    for (int k = 0; k < n; ++k)
+        for (const auto &x : sims[k]) {
+            lane[s] = k;
+            pairM[s] = x.pair.m;
+            pairE[s] = x.pair.e;
+            logRatio[s] = x.logProbRatio;
+            anchor1[s] = x.anchor1;
+            anchor2[s] = x.anchor2;
+            segOff[s] = g;
+            for (const auto &a : x.alignment) {
+                segs[3 * g] = a.start1;
+                segs[3 * g + 1] = a.start2;
+                segs[3 * g + 2] = a.length;
+                ++g;
+            }
+            ++s;
+        }
+    segOff[s] = g;
+    return ns;
+}
+
 // The lean float filter (findSimilaritiesBackwardOnly) on n <= simdWidth lanes.
 int dmstref_backward_only(int p, const uint8_t *const *decoded, const int *lens, int n, float *best) {
     ensureInit();

@@ -1,0 +1,97 @@
+"""Traceback of the hit path on the GPU (dmst_align) against the reference
+engine's own alignments (tests/golden/align.npz, made by
+tests/golden/make_align_golden.py from findSimilarities with needAlign):
+the herpes and medium overflow records at two gates and synthetic pairs
+(homologs, doubled homologs, frameshifted and implanted reads, random reads)
+at four gates, all in one call.  Every alignment must be the reference's,
+in the reference's order: anchor score (mantissa, exponent), its log, anchor
+row and column, and every segment pair; integer and exact-score work, so the
+bar is equality.  Also: pairs that report (min_prob_ratio < 0) and pairs
+below their gate have no alignments, and the call's scores are
+dmst_score_pairs'."""
+import os
+
+import numpy as np
+import pytest
+
+import dummest_b200 as d
+from dummest_b200 import _ffi as F
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _golden_sims(g, k):
+    idx = np.flatnonzero(g["sim_pair"] == k)
+    return [(float(g["sim_m"][s]), int(g["sim_e"][s]), float(g["sim_ln"][s]), int(g["sim_a1"][s]),
+             int(g["sim_a2"][s]), g["segs"][g["sim_segoff"][s]:g["sim_segoff"][s + 1]]) for s in idx]
+
+
+@pytest.fixture(scope="module")
+def golden_align(regression):
+    g = dict(np.load(os.path.join(GOLDEN, "align.npz")))
+    with d.Context(device=0) as ctx:
+        herpes = ctx.add_profile(regression["profile_values"], regression["profile_params"],
+                                 regression["profile_bg"])
+        synth_ids = ctx.load_hmm(str(g["synth_hmm"]))
+        off = np.concatenate([[0], np.cumsum(g["pair_len"])])
+        codes = [g["pair_codes"][off[k]:off[k + 1]] for k in range(len(g["pair_len"]))]
+        sids = ctx.add_decoded(codes)
+        pids = [herpes if src == 0 else synth_ids[p] for src, p in zip(g["pair_src"], g["pair_prof"])]
+        got, res = ctx.align(sids, pids, [float(x) for x in g["pair_mpr"]])
+        mids = ctx.score_pairs_raw(_pairs(sids, pids, -2.0), d.MODE_MID)
+        # the same pairs reporting (min_prob_ratio < 0): no alignments
+        rep, _ = ctx.align(sids, pids, -2.0)
+        # the largest float gate: only the scores beyond float range (herpes, 2^2242) pass
+        miss, _ = ctx.align(sids, pids, 3.0e38)
+        # the call again: the context's buffers are reused
+        again, _ = ctx.align(sids[::-1], pids[::-1], [float(x) for x in g["pair_mpr"][::-1]])
+    return g, got, res, mids, rep, miss, again[::-1]
+
+
+def _pairs(sids, pids, mpr):
+    arr = (F.Pair * len(sids))()
+    for k, (s, p) in enumerate(zip(sids, pids)):
+        arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, mpr
+    return arr
+
+
+def _assert_same(got, want, k):
+    assert len(got) == len(want), (k, len(got), len(want))
+    for q, (x, y) in enumerate(zip(got, want)):
+        assert (x[0], x[1], x[3], x[4]) == (y[0], y[1], y[3], y[4]), (k, q, x[:5], y[:5])
+        assert x[2] == y[2], (k, q)
+        assert np.array_equal(x[5], y[5]), (k, q, x[5][:5], y[5][:5])
+
+
+def test_alignments_equal_reference(golden_align):
+    g, got, res, *_ = golden_align
+    for k in range(len(g["pair_len"])):
+        _assert_same(got[k], _golden_sims(g, k), k)
+    assert sum(len(x) for x in got) == len(g["sim_pair"])
+    assert sum(1 for x in got for a in x if len(a[5])) >= 20  # real alignments, not only empty walks
+
+
+def test_known_answers_on_overflow_records(golden_align):
+    # test_overflow.sh:66-71: herpes anchor 981,5942, spans 1/1358 and 3003/4072;
+    # medium anchor 531,2302, spans 428/504 and 1994/1510
+    _, got, *_ = golden_align
+    for k, anchor, spans in ((0, (981, 5942), (1, 1358, 3003, 4072)), (4, (531, 2302), (428, 504, 1994, 1510))):
+        m, e, ln, a1, a2, sg = got[k][0]
+        assert (a1, a2) == anchor
+        s1, e1, s2, e2 = sg[0, 0], sg[-1, 0] + sg[-1, 2], sg[0, 1], sg[-1, 1] + sg[-1, 2]
+        assert (s1, e1 - s1, s2, e2 - s2) == spans
+
+
+def test_scores_reports_misses_and_reuse(golden_align):
+    g, got, res, mids, rep, miss, again = golden_align
+    for r, m in zip(res, mids):
+        assert (r.mid.m, r.mid.e, r.filter.m, r.filter.e) == (m.mid.m, m.mid.e, m.filter.m, m.filter.e)
+    assert all(len(x) == 0 for x in rep)
+    gate = np.log(np.float64(np.float32(3.0e38)))
+    for r, x in zip(res, miss):
+        assert (len(x) > 0) == (r.mid_ln >= gate), (r.mid_ln, len(x))
+    assert any(len(x) for x in miss) and not all(len(x) for x in miss)
+    for k in range(len(g["pair_len"])):
+        _assert_same(again[k], got[k], k)

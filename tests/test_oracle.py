@@ -143,3 +143,58 @@ def test_oracle_anchors_equal_reference_trackers(ref32, tmp_path):
             assert np.array_equal(rm, om) and np.array_equal(re, oe)
             nz = rm != 0
             assert np.array_equal(rr[nz], orow[nz])
+
+
+def _align_golden():
+    return dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "align.npz")))
+
+
+def _golden_sims(g, k):
+    idx = np.flatnonzero(g["sim_pair"] == k)
+    return [(float(g["sim_m"][s]), int(g["sim_e"][s]), float(g["sim_ln"][s]), int(g["sim_a1"][s]),
+             int(g["sim_a2"][s]), g["segs"][g["sim_segoff"][s]:g["sim_segoff"][s + 1]]) for s in idx]
+
+
+def test_align_golden_pins_reference_known_answers():
+    """The traceback fixture (tests/golden/align.npz, the reference engine's own
+    alignments) against the reference's known answers for its overflow records
+    (tests/test_overflow.sh:66-71): the top alignment's score, anchor and MAF
+    spans (start, size) on the profile and on the sequence."""
+    g = _align_golden()
+    want = {0: (2242.35, 6, (981, 5942), (1, 1358, 3003, 4072)),   # herpes0+, gates 0 and 2^40
+            4: (754.34, 1, (531, 2302), (428, 504, 1994, 1510))}  # medium0+
+    for k0, (bits, tol, anchor, spans) in want.items():
+        for k in (k0, k0 + 1):
+            sims = _golden_sims(g, k)
+            assert sims, k
+            m, e, ln, a1, a2, sg = sims[0]  # the first similarity is the best anchor's
+            assert abs(ln / LN2 - bits) <= tol
+            assert (a1, a2) == anchor
+            s1, e1 = sg[0, 0], sg[-1, 0] + sg[-1, 2]
+            s2, e2 = sg[0, 1], sg[-1, 1] + sg[-1, 2]
+            assert (s1, e1 - s1, s2, e2 - s2) == spans
+
+
+def test_align_golden_equals_reference_engine(ref32, tmp_path):
+    """The fixture's synthetic alignments are the reference engine's (run here
+    on the stored codes and gates; the zero gate on the shorter reads only, to
+    bound the time)."""
+    g = _align_golden()
+    path = tmp_path / "tb.hmm"
+    path.write_text(str(g["synth_hmm"]))
+    assert ref32.load_profiles(str(path)) == 4
+    off = np.concatenate([[0], np.cumsum(g["pair_len"])])
+    checked = 0
+    for k in np.flatnonzero(g["pair_src"] == 1):
+        codes = g["pair_codes"][off[k]:off[k + 1]]
+        mpr = float(g["pair_mpr"][k])
+        if mpr == 0.0 and len(codes) > 1500:
+            continue
+        got = ref32.align(int(g["pair_prof"][k]), [codes], [mpr])[0]
+        want = _golden_sims(g, k)
+        assert len(got) == len(want), k
+        for x, y in zip(got, want):
+            assert x[:2] == y[:2] and x[3:5] == y[3:5] and x[2] == y[2]
+            assert np.array_equal(x[5], y[5])
+        checked += 1
+    assert checked >= 20
