@@ -359,13 +359,12 @@ struct dmst_ctx {
     DevBuf<ExactOut> dExactOut;
     // dmst_align: the traceback buffers (dp_traceback.cuh) and the last call's results
     DevBuf<AlignJob> dAlignJobs;
-    DevBuf<int> dAlignJobOf, dAlignRows, dAlignCand, dAlignCounts;
+    DevBuf<int> dAlignJobOf, dAlignRows, dAlignCand;
     DevBuf<float> dAlignCells, dAlignColR, dAlignColF;
     DevBuf<XS> dAlignX, dAlignSuf, dAlignWork, dAlignRev, dAlignFwd;
-    DevBuf<uint8_t> dAlignMark;
-    DevBuf<AlignSim> dAlignSims, dAlignSimOut;
-    DevBuf<Seg> dAlignSegs, dAlignSegOut;
-    DevBuf<long long> dAlignBase;
+    DevBuf<WalkSpan> dAlignSpan;
+    DevBuf<WalkItem> dAlignItems;
+    DevBuf<Seg> dAlignSegOut;
     std::vector<dmst_alignment> alignOut;
     std::vector<dmst_segment> alignSegOut;
 
@@ -517,7 +516,6 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dAlignJobOf.release();
     ctx->dAlignRows.release();
     ctx->dAlignCand.release();
-    ctx->dAlignCounts.release();
     ctx->dAlignCells.release();
     ctx->dAlignColR.release();
     ctx->dAlignColF.release();
@@ -526,12 +524,9 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dAlignWork.release();
     ctx->dAlignRev.release();
     ctx->dAlignFwd.release();
-    ctx->dAlignMark.release();
-    ctx->dAlignSims.release();
-    ctx->dAlignSimOut.release();
-    ctx->dAlignSegs.release();
+    ctx->dAlignSpan.release();
+    ctx->dAlignItems.release();
     ctx->dAlignSegOut.release();
-    ctx->dAlignBase.release();
     ctx->dMidChunks.release();
     ctx->dSurvivors.release();
     ctx->dMinBest.release();
@@ -1749,11 +1744,12 @@ int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *be
 // in batches whose traceback buffers fit half the free device memory, through
 // the exact kernel (anchors, W0, W1 and rescale counts kept), the table
 // kernels of dp_traceback.cuh, the reference's anchor sort on the host, the
-// walks and a gather of their results.
+// span pass over every candidate, the reference's sequential choice of
+// anchors on the host (from the spans), and the store pass for the kept ones.
 static size_t alignJobBytes(int M, int L) {
     const size_t cells = (size_t)(M + 1) * L;
-    return cells * (8 + 8 + 8) + (size_t)L * (4 + 4 + 16 + 8 + 8 + 4 + 1 + 2 * sizeof(AlignSim) + 12) +
-           (size_t)alignSegs(M, L) * sizeof(Seg) * 2 + (size_t)alignRowInts(M) * 4 + 256;
+    return cells * (8 + 8 + 8) + (size_t)L * (4 + 4 + 16 + 8 + 8 + 4 + sizeof(WalkSpan) + 2 * sizeof(Seg)) +
+           (size_t)alignRowInts(M) * 4 + 256;
 }
 
 static bool lessScore(dmst_score a, dmst_score b) {  // scoreLess (dummest-score.hh:70-76)
@@ -1824,7 +1820,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         const int nb = (int)(b1 - b0);
         std::vector<AlignJob> jobs(nb);
         std::vector<dmst_pair> bp(nb);
-        long long cells = 0, cols = 0, rowsN = 0, segsN = 0;
+        long long cells = 0, cols = 0, rowsN = 0;
         int maxL = 0, maxM = 0;
         for (int j = 0; j < nb; ++j) {
             const dmst_pair &pp = pairs[hits[b0 + j]];
@@ -1837,13 +1833,11 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
             jb.cellOff = cells;
             jb.colOff = cols;
             jb.rowOff = rowsN;
-            jb.segOff = segsN;
             jb.minM = gates[b0 + j].m;
             jb.minE = gates[b0 + j].e;
             cells += (long long)(jb.M + 1) * jb.L;
             cols += jb.L;
             rowsN += alignRowInts(jb.M);
-            segsN += alignSegs(jb.M, jb.L);
             maxL = std::max(maxL, jb.L);
             maxM = std::max(maxM, jb.M);
         }
@@ -1857,11 +1851,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         CK(ctx->dAlignRev.ensure((size_t)cols), "alloc traceback columns");
         CK(ctx->dAlignFwd.ensure((size_t)cols), "alloc traceback columns");
         CK(ctx->dAlignCand.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignMark.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignSims.ensure((size_t)cols), "alloc traceback output");
-        CK(ctx->dAlignSegs.ensure((size_t)segsN), "alloc traceback output");
-        CK(ctx->dAlignCounts.ensure((size_t)2 * nb), "alloc traceback output");
-        CK(ctx->dAlignBase.ensure((size_t)2 * nb), "alloc traceback output");
+        CK(ctx->dAlignSpan.ensure((size_t)cols), "alloc traceback columns");
 
         // the exact path with the traceback stores, then the tables
         std::vector<dmst_score> best((size_t)cols);
@@ -1917,71 +1907,80 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
             }
             jb.nCand = nc;
         }
+        int maxCand = 1;
+        for (const AlignJob &jb : jobs) maxCand = std::max(maxCand, jb.nCand);
         CK(cudaMemcpyAsync(ctx->dAlignJobs.p, jobs.data(), nb * sizeof(AlignJob), cudaMemcpyHostToDevice,
                            ctx->stream),
            "upload traceback jobs");
         CK(cudaMemcpyAsync(ctx->dAlignCand.p, cand.data(), (size_t)cols * sizeof(int), cudaMemcpyHostToDevice,
                            ctx->stream),
            "upload traceback candidates");
-        CK(cudaMemsetAsync(ctx->dAlignMark.p, 0, (size_t)cols, ctx->stream), "zero aligned flags");
-        walkKernel<<<(nb + 31) / 32, 32, 0, ctx->stream>>>(
-            ctx->dAlignJobs.p, nb, ctx->dAlignCand.p, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p, ctx->dAlignCells.p,
-            ctx->dAlignX.p, ctx->dAlignSuf.p, ctx->dAlignRev.p, ctx->dAlignFwd.p, ctx->dAlignMark.p,
-            ctx->dAlignSims.p, ctx->dAlignSegs.p, ctx->dAlignCounts.p);
-        CK(cudaGetLastError(), "traceback walk kernel");
-        std::vector<int> counts(2 * nb);
-        CK(cudaMemcpyAsync(counts.data(), ctx->dAlignCounts.p, 2 * nb * sizeof(int), cudaMemcpyDeviceToHost,
+        spanKernel<<<dim3((maxCand + 127) / 128, nb), 128, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, ctx->dAlignCand.p, S.dAnchorRow.p, ctx->dAlignCells.p, ctx->dAlignX.p,
+            ctx->dAlignSuf.p, ctx->dAlignRev.p, ctx->dAlignFwd.p, ctx->dAlignSpan.p);
+        CK(cudaGetLastError(), "traceback span kernel");
+        std::vector<WalkSpan> spans((size_t)cols);
+        CK(cudaMemcpyAsync(spans.data(), ctx->dAlignSpan.p, (size_t)cols * sizeof(WalkSpan), cudaMemcpyDeviceToHost,
                            ctx->stream),
-           "download traceback counts");
-        CK(cudaStreamSynchronize(ctx->stream), "traceback walks");
-        std::vector<long long> base(2 * nb);
-        long long ns = 0, ng = 0;
+           "download traceback spans");
+        CK(cudaStreamSynchronize(ctx->stream), "traceback spans");
+
+        // The reference's choice (dummest-dp-forward.hh:497-531): in sorted
+        // order, an anchor inside a kept alignment is skipped, and one whose
+        // clamped span meets a kept alignment's columns is dropped; the rest
+        // are kept and mark their columns.  marked[] holds prefix counts of
+        // the marked columns, rebuilt when a kept span marks some.
+        std::vector<WalkItem> items;
+        std::vector<uint8_t> mark;
+        std::vector<int> marked;
+        long long ng = 0;
         for (int j = 0; j < nb; ++j) {
-            if (counts[2 * j] < 0) return ctx->fail(DMST_ERANGE, "traceback: segment space of a hit exhausted");
-            base[j] = ns;
-            base[nb + j] = ng;
-            ns += counts[2 * j];
-            ng += counts[2 * j + 1];
-        }
-        std::vector<AlignSim> simH((size_t)ns);
-        std::vector<Seg> segH((size_t)ng);
-        if (ns > 0) {
-            CK(ctx->dAlignSimOut.ensure((size_t)ns), "alloc traceback output");
-            CK(ctx->dAlignSegOut.ensure((size_t)std::max<long long>(ng, 1)), "alloc traceback output");
-            CK(cudaMemcpyAsync(ctx->dAlignBase.p, base.data(), 2 * nb * sizeof(long long), cudaMemcpyHostToDevice,
-                               ctx->stream),
-               "upload traceback offsets");
-            gatherKernel<<<nb, 128, 0, ctx->stream>>>(ctx->dAlignJobs.p, ctx->dAlignSims.p, ctx->dAlignSegs.p,
-                                                      ctx->dAlignCounts.p, ctx->dAlignBase.p, ctx->dAlignBase.p + nb,
-                                                      ctx->dAlignSimOut.p, ctx->dAlignSegOut.p);
-            CK(cudaGetLastError(), "traceback gather kernel");
-            CK(cudaMemcpyAsync(simH.data(), ctx->dAlignSimOut.p, ns * sizeof(AlignSim), cudaMemcpyDeviceToHost,
-                               ctx->stream),
-               "download alignments");
-            if (ng > 0)
-                CK(cudaMemcpyAsync(segH.data(), ctx->dAlignSegOut.p, ng * sizeof(Seg), cudaMemcpyDeviceToHost,
-                                   ctx->stream),
-                   "download segments");
-            CK(cudaStreamSynchronize(ctx->stream), "traceback results");
-        }
-        const long long segBase0 = (long long)ctx->alignSegOut.size();
-        for (int j = 0; j < nb; ++j) {
-            for (int q = 0; q < counts[2 * j]; ++q) {
-                const AlignSim &a = simH[base[j] + q];
+            const AlignJob &jb = jobs[j];
+            mark.assign(jb.L, 0);
+            marked.assign(jb.L + 1, 0);
+            for (int c = 0; c < jb.nCand; ++c) {
+                const int a2 = cand[jb.colOff + c];
+                if (mark[a2]) continue;
+                const WalkSpan &w = spans[jb.colOff + c];
+                const int beg = std::max(w.beg, 0), end = std::min(w.end, jb.L);
+                if (beg < end && marked[end] - marked[beg] > 0) continue;
+                if (beg < end) {
+                    std::fill(mark.begin() + beg, mark.begin() + end, (uint8_t)1);
+                    for (int q = 0; q < jb.L; ++q) marked[q + 1] = marked[q] + mark[q];
+                }
+                const int n = w.nf + w.nr;
                 dmst_alignment o;
                 o.pair = hits[b0 + j];
-                o.score = dmst_score{a.m, a.e};
-                o.ln_score = scoreLn(a.m, a.e);
-                o.anchor1 = a.anchor1;
-                o.anchor2 = a.anchor2;
-                o.seg_begin = segBase0 + base[nb + j] + a.segBegin;
-                o.seg_count = a.segCount;
+                o.score = best[jb.colOff + a2];
+                o.ln_score = scoreLn(o.score.m, o.score.e);
+                o.anchor1 = row[jb.colOff + a2];
+                o.anchor2 = a2;
+                o.seg_begin = (long long)ctx->alignSegOut.size() + ng;
+                o.seg_count = n;
                 o.pad = 0;
                 ctx->alignOut.push_back(o);
+                if (n > 0) items.push_back(WalkItem{j, a2, w.nr, 0, ng});
+                ng += n;
             }
         }
-        for (long long q = 0; q < ng; ++q)
-            ctx->alignSegOut.push_back(dmst_segment{segH[q].start1, segH[q].start2, segH[q].length});
+        if (!items.empty()) {
+            CK(ctx->dAlignItems.ensure(items.size()), "alloc traceback output");
+            CK(ctx->dAlignSegOut.ensure((size_t)ng), "alloc traceback output");
+            CK(cudaMemcpyAsync(ctx->dAlignItems.p, items.data(), items.size() * sizeof(WalkItem),
+                               cudaMemcpyHostToDevice, ctx->stream),
+               "upload traceback walks");
+            storeWalkKernel<<<(int)((items.size() + 127) / 128), 128, 0, ctx->stream>>>(
+                ctx->dAlignJobs.p, ctx->dAlignItems.p, (int)items.size(), S.dAnchorRow.p, ctx->dAlignCells.p,
+                ctx->dAlignX.p, ctx->dAlignSuf.p, ctx->dAlignRev.p, ctx->dAlignFwd.p, ctx->dAlignSegOut.p);
+            CK(cudaGetLastError(), "traceback store kernel");
+            const size_t first = ctx->alignSegOut.size();
+            ctx->alignSegOut.resize(first + (size_t)ng);
+            static_assert(sizeof(Seg) == sizeof(dmst_segment), "segment layout");
+            CK(cudaMemcpyAsync(ctx->alignSegOut.data() + first, ctx->dAlignSegOut.p, (size_t)ng * sizeof(Seg),
+                               cudaMemcpyDeviceToHost, ctx->stream),
+               "download segments");
+            CK(cudaStreamSynchronize(ctx->stream), "traceback segments");
+        }
         b0 = b1;
     }
     *n_alignments = ctx->alignOut.size();

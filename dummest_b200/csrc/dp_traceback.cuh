@@ -16,9 +16,12 @@
 //                   float form of dummest-scalerow.hh: each row is a running
 //                   maximum (a block-wide max scan) of candidates read from
 //                   the row before;
-//   walkKernel      the anchors in the reference's sorted order: for each
-//                   anchor not yet covered, the forward and reverse walks
-//                   and the overlap test against the columns already aligned.
+//   spanKernel      the forward and reverse walks of every candidate anchor
+//                   at once (they do not depend on which anchors are kept):
+//                   each walk's sequence span and match counts; the host
+//                   then takes the anchors in the reference's sorted order,
+//                   skipping those inside or overlapping kept ones;
+//   storeWalkKernel the kept anchors' walks again, writing their segments.
 //
 // Columns at or past a pair's length are not built: the reference's values
 // there are zero (W1 is masked, so X and the exit flank totals are 0) or
@@ -387,162 +390,167 @@ __global__ void __launch_bounds__(kOptThreads) optimalKernel(const AlignJob *job
     }
 }
 
-// One similarity of the traceback output.
-struct AlignSim {
-    float m;   // the anchor's exact score (AlignedSimilarity::pair)
-    int e;
-    int anchor1, anchor2;
-    int segBegin, segCount;  // in the job's segment pairs
-};
-
 struct Seg {
     int start1, start2, length;
 };
 
-// The walks of one job per thread (dummest-traceback.hh:35-118) over the
-// candidates in order (dummest-dp-forward.hh:497-532).  counts[2 t] =
-// similarities, counts[2 t + 1] = segments; counts[2 t] = -1 if the segment
-// space ran out (it cannot for alignments of the reference's shape).
-__global__ void walkKernel(const AlignJob *jobs, int nJobs, const int *cand, const float *anchorM,
-                           const int *anchorE, const int *anchorRow, const float *cells, const XS *X,
-                           const XS *suffix, const XS *revEv, const XS *fwdEv, uint8_t *aligned, AlignSim *sims,
-                           Seg *segs, int *counts) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nJobs) return;
-    const AlignJob jb = jobs[t];
+// A candidate's walks in brief: its sequence span [beg, end) (before the
+// clamp to [0, L)) and its forward and reverse match counts.
+struct WalkSpan {
+    int beg, end, nf, nr;
+};
+
+// One anchor's walks (dummest-traceback.hh:35-118): forward from (anchor1,
+// anchor2) over the suffix-optimal table, then backward from (anchor1 - 1,
+// anchor2) over the prefix-optimal table, with the reference's merging of
+// adjacent matches.  The alignment is the reverse matches, last found first,
+// then the forward ones; addForwardMatch consults only the last forward
+// match and addReverseMatch only the current first segment, so the walk keeps
+// those in registers.  STORE: the segments go to out[0, nr + nf), with nrKnown
+// the reverse match count (from the span pass): forward match q at
+// out[nrKnown + q], reverse match q at out[nrKnown - 1 - q].
+template <bool STORE>
+__device__ WalkSpan walkAnchor(const AlignJob &jb, int a1, int a2, const XS *pre, const XS *Xj, const XS *suf,
+                               const XS *rev, const XS *fwd, Seg *out, int nrKnown) {
     const int M = jb.M, L = jb.L;
-    const XS *pre = reinterpret_cast<const XS *>(cells + 2 * jb.cellOff);
-    const XS *Xj = X + jb.cellOff;
-    const XS *suf = suffix + jb.cellOff;
-    const XS *rev = revEv + jb.colOff, *fwd = fwdEv + jb.colOff;
-    uint8_t *mark = aligned + jb.colOff;
-    Seg *out = segs + jb.segOff;
-    const long long cap = alignSegCap(M, L);
-    Seg *rtmp = out + cap;  // the reverse walk's matches, in walk order (M + 2 entries)
-    AlignSim *sv = sims + jb.colOff;
     auto S = [&](int i, int j) { return (i <= M && j < L) ? ldXS(suf + (size_t)i * L + j) : xsZero(); };
     auto P = [&](int i, int j) { return ldXS(pre + (size_t)i * L + j); };
-    int nSims = 0, top = 0;
-    bool overflow = false;
-    for (int c = 0; c < jb.nCand && !overflow; ++c) {
-        const int a2 = cand[jb.colOff + c];
-        if (mark[a2]) continue;
-        const int a1 = anchorRow[jb.colOff + a2];
-        // forward walk: matches appended after the accepted segments
-        int nf = 0;
-        {
-            int i = a1, pos = a2;
-            while (i <= M && pos < L) {
-                XS best = xsZero();
-                int bi = INT_MAX, bj = INT_MAX;
-                bool emit = false;
-                if (pos + 3 < L) {
-                    const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos + 3), S(i + 1, pos + 3));
-                    if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos + 3; emit = true; }
-                }
-                XS cd = S(i + 1, pos);
-                if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos; emit = false; }
-                cd = S(i, pos + 1);
-                if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos + 1; emit = false; }
-                cd = ldXS(fwd + pos);
-                if (scoreLess(best, cd)) { best = cd; bi = INT_MAX; bj = INT_MAX; emit = false; }
-                if (emit) {  // addForwardMatch(i, pos + 1)
-                    const int p1 = i, p2 = pos + 1;
-                    bool add = true;
-                    if (nf > 0) {
-                        Seg &x = out[top + nf - 1];
-                        if (x.start1 + x.length == p1 && x.start2 + x.length == p2) ++x.length;
-                        if (x.start1 + x.length > p1 || x.start2 + x.length > p2) add = false;
-                    }
-                    if (add) {
-                        if (top + nf >= cap) { overflow = true; break; }
-                        out[top + nf++] = Seg{p1, p2, 1};
-                    }
-                }
-                i = bi;
-                pos = bj;
+    Seg fFirst{0, 0, 0}, fLast{0, 0, 0}, rFirst{0, 0, 0}, rFront{0, 0, 0};
+    int nf = 0, nr = 0;
+    {
+        int i = a1, pos = a2;
+        while (i <= M && pos < L) {
+            XS best = xsZero();
+            int bi = INT_MAX, bj = INT_MAX;
+            bool emit = false;
+            if (pos + 3 < L) {
+                const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos + 3), S(i + 1, pos + 3));
+                if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos + 3; emit = true; }
             }
-        }
-        if (overflow) break;
-        // reverse walk: each match goes before the segments so far; the one it
-        // may extend is the first of them
-        int nr = 0;
-        {
-            int i = a1 - 1, pos = a2;
-            while (i >= 0 && pos >= 0) {
-                XS best = xsZero();
-                int bi = -1, bj = -1;
-                bool emit = false;
-                if (pos >= 3) {
-                    const XS succ = i >= 1 ? P(i - 1, pos - 3) : xsZero();
-                    const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos), succ);
-                    if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos - 3; emit = true; }
+            XS cd = S(i + 1, pos);
+            if (scoreLess(best, cd)) { best = cd; bi = i + 1; bj = pos; emit = false; }
+            cd = S(i, pos + 1);
+            if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos + 1; emit = false; }
+            cd = ldXS(fwd + pos);
+            if (scoreLess(best, cd)) { best = cd; bi = INT_MAX; bj = INT_MAX; emit = false; }
+            if (emit) {  // addForwardMatch(i, pos + 1)
+                const int p1 = i, p2 = pos + 1;
+                bool add = true;
+                if (nf > 0) {
+                    Seg &x = fLast;
+                    if (x.start1 + x.length == p1 && x.start2 + x.length == p2) ++x.length;
+                    if (x.start1 + x.length > p1 || x.start2 + x.length > p2) add = false;
+                    if (nf == 1) fFirst = fLast;
+                    if (STORE) out[nrKnown + nf - 1] = fLast;
                 }
-                if (i >= 1) {
-                    const XS cd = P(i - 1, pos);
-                    if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos; emit = false; }
+                if (add) {
+                    const Seg s{p1, p2, 1};
+                    if (nf == 0) fFirst = s;
+                    fLast = s;
+                    if (STORE) out[nrKnown + nf] = s;
+                    ++nf;
                 }
-                if (pos > 0) {
-                    const XS cd = P(i, pos - 1);
-                    if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos - 1; emit = false; }
-                }
-                const XS cd = ldXS(rev + pos);
-                if (scoreLess(best, cd)) { best = cd; bi = -1; bj = -1; emit = false; }
-                if (emit) {  // addReverseMatch(i, pos - 2)
-                    const int p1 = i, p2 = pos - 2;
-                    bool add = true;
-                    Seg *x = nr > 0 ? &rtmp[nr - 1] : (nf > 0 ? &out[top] : nullptr);
-                    if (x) {
-                        if (x->start1 - 1 == p1 && x->start2 - 1 == p2) {
-                            --x->start1;
-                            --x->start2;
-                            ++x->length;
-                        }
-                        if (x->start1 <= p1 || x->start2 <= p2) add = false;
-                    }
-                    if (add) {
-                        if (nr >= M + 2 || top + nf + nr >= cap) { overflow = true; break; }
-                        rtmp[nr++] = Seg{p1, p2, 1};
-                    }
-                }
-                i = bi;
-                pos = bj;
             }
+            i = bi;
+            pos = bj;
         }
-        if (overflow) break;
-        // final order: reverse matches (last found first), then the forward ones
-        if (nr > 0) {
-            for (int q = nf - 1; q >= 0; --q) out[top + nr + q] = out[top + q];
-            for (int q = 0; q < nr; ++q) out[top + q] = rtmp[nr - 1 - q];
-        }
-        const int n = nf + nr;
-        int beg = n == 0 ? a2 : out[top].start2;
-        int end = n == 0 ? a2 : out[top + n - 1].start2 + out[top + n - 1].length;
-        beg = max(beg, 0);
-        end = min(end, L);
-        bool overlaps = false;
-        for (int q = beg; q < end; ++q)
-            if (mark[q]) {
-                overlaps = true;
-                break;
-            }
-        if (overlaps) continue;
-        for (int q = beg; q < end; ++q) mark[q] = 1;
-        sv[nSims++] = AlignSim{anchorM[jb.colOff + a2], anchorE[jb.colOff + a2], a1, a2, top, n};
-        top += n;
     }
-    counts[2 * t] = overflow ? -1 : nSims;
-    counts[2 * t + 1] = top;
+    {
+        int i = a1 - 1, pos = a2;
+        while (i >= 0 && pos >= 0) {
+            XS best = xsZero();
+            int bi = -1, bj = -1;
+            bool emit = false;
+            if (pos >= 3) {
+                const XS succ = i >= 1 ? P(i - 1, pos - 3) : xsZero();
+                const XS cd = scalarAdd(ldXS(Xj + (size_t)i * L + pos), succ);
+                if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos - 3; emit = true; }
+            }
+            if (i >= 1) {
+                const XS cd = P(i - 1, pos);
+                if (scoreLess(best, cd)) { best = cd; bi = i - 1; bj = pos; emit = false; }
+            }
+            if (pos > 0) {
+                const XS cd = P(i, pos - 1);
+                if (scoreLess(best, cd)) { best = cd; bi = i; bj = pos - 1; emit = false; }
+            }
+            const XS cd = ldXS(rev + pos);
+            if (scoreLess(best, cd)) { best = cd; bi = -1; bj = -1; emit = false; }
+            if (emit) {  // addReverseMatch(i, pos - 2)
+                const int p1 = i, p2 = pos - 2;
+                bool add = true;
+                if (nr > 0 || nf > 0) {
+                    Seg &x = nr > 0 ? rFront : fFirst;
+                    if (x.start1 - 1 == p1 && x.start2 - 1 == p2) {
+                        --x.start1;
+                        --x.start2;
+                        ++x.length;
+                    }
+                    if (x.start1 <= p1 || x.start2 <= p2) add = false;
+                    if (nr > 0) {
+                        if (nr == 1) rFirst = rFront;
+                        if (STORE) out[nrKnown - nr] = rFront;
+                    } else {
+                        if (nf == 1) fLast = fFirst;
+                        if (STORE) out[nrKnown] = fFirst;
+                    }
+                }
+                if (add) {
+                    const Seg s{p1, p2, 1};
+                    if (nr == 0) rFirst = s;
+                    rFront = s;
+                    ++nr;
+                    if (STORE) out[nrKnown - nr] = s;
+                }
+            }
+            i = bi;
+            pos = bj;
+        }
+    }
+    WalkSpan w;
+    w.nf = nf;
+    w.nr = nr;
+    if (nf + nr == 0) {
+        w.beg = w.end = a2;
+    } else {
+        w.beg = nr > 0 ? rFront.start2 : fFirst.start2;
+        w.end = nf > 0 ? fLast.start2 + fLast.length : rFirst.start2 + rFirst.length;
+    }
+    return w;
 }
 
-// Gathers the jobs' similarities and segments into one list each
-// (simBase / segBase: exclusive sums of the counts), one CTA per job.
-__global__ void gatherKernel(const AlignJob *jobs, const AlignSim *sims, const Seg *segs, const int *counts,
-                             const long long *simBase, const long long *segBase, AlignSim *simOut, Seg *segOut) {
-    const AlignJob jb = jobs[blockIdx.x];
-    const int ns = counts[2 * blockIdx.x], ng = counts[2 * blockIdx.x + 1];
-    for (int q = threadIdx.x; q < ns; q += blockDim.x) simOut[simBase[blockIdx.x] + q] = sims[jb.colOff + q];
-    for (int q = threadIdx.x; q < ng; q += blockDim.x) segOut[segBase[blockIdx.x] + q] = segs[jb.segOff + q];
+// The span pass: every candidate of every job at once, one thread each
+// (grid.y = job); spans[colOff + c] for candidate c.
+__global__ void spanKernel(const AlignJob *jobs, const int *cand, const int *anchorRow, const float *cells,
+                           const XS *X, const XS *suffix, const XS *revEv, const XS *fwdEv, WalkSpan *spans) {
+    const AlignJob jb = jobs[blockIdx.y];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= jb.nCand) return;
+    const int a2 = cand[jb.colOff + c];
+    const int a1 = anchorRow[jb.colOff + a2];
+    spans[jb.colOff + c] = walkAnchor<false>(jb, a1, a2, reinterpret_cast<const XS *>(cells + 2 * jb.cellOff),
+                                             X + jb.cellOff, suffix + jb.cellOff, revEv + jb.colOff,
+                                             fwdEv + jb.colOff, nullptr, 0);
+}
+
+// An accepted candidate whose segments are written.
+struct WalkItem {
+    int job, anchor2, nr, pad;
+    long long segOff;  // in the output segment list
+};
+
+// The store pass: the accepted candidates' walks again, segments written in
+// place (the walks are deterministic, so the counts are the span pass's).
+__global__ void storeWalkKernel(const AlignJob *jobs, const WalkItem *items, int nItems, const int *anchorRow,
+                                const float *cells, const XS *X, const XS *suffix, const XS *revEv,
+                                const XS *fwdEv, Seg *segOut) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nItems) return;
+    const WalkItem it = items[t];
+    const AlignJob jb = jobs[it.job];
+    const int a1 = anchorRow[jb.colOff + it.anchor2];
+    walkAnchor<true>(jb, a1, it.anchor2, reinterpret_cast<const XS *>(cells + 2 * jb.cellOff), X + jb.cellOff,
+                     suffix + jb.cellOff, revEv + jb.colOff, fwdEv + jb.colOff, segOut + it.segOff, it.nr);
 }
 
 }  // namespace dmst

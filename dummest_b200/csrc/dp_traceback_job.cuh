@@ -6,11 +6,9 @@
 //          bytes; the X table and the suffix-optimal table (one ExpScore per
 //          cell) in their own arrays at the same cell offset;
 //   cols   L entries per column array: anchors, column masses, flank scores,
-//          candidates, aligned flags, similarities;
+//          candidates and their walks' spans;
 //   rows   the reference's rescale counts cntB[M+2], cntF[M+2], the X table's
-//          row maxima [M+2] and the two flank maxima;
-//   segs   the segment pairs out ((L + M + 2) entries) and the reverse walk's
-//          scratch (M + 2 entries).
+//          row maxima [M+2] and the two flank maxima.
 #pragma once
 
 namespace dmst {
@@ -22,13 +20,10 @@ struct AlignJob {
     long long cellOff;   // cells
     long long colOff;    // columns
     long long rowOff;    // ints
-    long long segOff;    // segment pairs
     float minM;          // the gate, normalizeScore(minProbRatio, 0)
     int minE;
 };
 
 __host__ __device__ inline long long alignRowInts(int M) { return 3LL * (M + 2) + 2; }
-__host__ __device__ inline long long alignSegCap(int M, int L) { return (long long)L + M + 2; }
-__host__ __device__ inline long long alignSegs(int M, int L) { return alignSegCap(M, L) + M + 2; }
 
 }  // namespace dmst
