@@ -65,11 +65,16 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
-    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search"], default="batched",
+    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align"], default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
                          "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
                          "profile over 4096 implant reads (L 600-2400), one SGD step per step; search: the "
-                         "batched pairs through the two-wave search (filter, then mid on survivors)")
+                         "batched pairs through the two-wave search (filter, then mid on survivors); align: "
+                         "the hit path with its traceback (an M=400 profile against homolog-carrying reads, "
+                         "both strands, the hits' alignments traced)")
+    ap.add_argument("--al-reads", type=int, default=256, help="align workload: reads per step (x2 strands)")
+    ap.add_argument("--al-m", type=int, default=400, help="align workload: profile length")
+    ap.add_argument("--al-gate", type=float, default=1e6, help="align workload: minProbRatio of every pair")
     ap.add_argument("--ag-reads", type=int, default=4096, help="autograd workload: reads per rank")
     ap.add_argument("--ag-m", type=int, default=400, help="autograd workload: profile length")
     ap.add_argument("--ag-lmin", type=int, default=600, help="autograd workload: shortest read")
@@ -166,6 +171,16 @@ def workload_config(args, world: int) -> dict:
             "l2": "inputs larger than L2 (W1 slots)",
             "parallelism": f"replicas x{world} (pairs sharded per rank)",
         }
+    if args.workload == "align":
+        return {
+            "workload": f"hit path with traceback (findSimilarities needAlign): 1 profile M={args.al_m} x "
+                        f"{args.al_reads} reads (a frameshifted homolog of the whole profile between two 500 nt "
+                        f"random flanks), both strands, minProbRatio {args.al_gate:g}: every pair scored, the "
+                        "hits' alignments traced",
+            "profiles": 1, "reads_per_step": args.al_reads, "pairs_per_step": 2 * args.al_reads,
+            "l2": "inputs larger than L2 (traceback tables)",
+            "parallelism": f"replicas x{world} (reads sharded per rank)",
+        }
     if args.workload == "genome":
         return {
             "workload": "long-profile genome scan: 1 profile M=2000 x a 10 Mbp synthetic genome (GC 0.45, "
@@ -198,6 +213,17 @@ def make_workload(args, rank: int, n_steps: int):
         from dummest_b200 import synth
         prof, windows = synth.genome_scan_config(seed=rank_seed(args.seed, rank))
         return [prof], synth.hmmer3_text([prof]), [windows] * n_steps
+    if args.workload == "align":
+        from dummest_b200 import synth
+        rng = np.random.default_rng(args.seed)
+        prof = synth.make_profile(rng, args.al_m, "align")
+        rng = np.random.default_rng(rank_seed(args.seed, rank))
+        steps = []
+        for _ in range(n_steps):
+            reads = [synth.random_dna(rng, 500) + synth.sample_homolog(rng, prof, args.al_m, fs_rate=0.01)
+                     + synth.random_dna(rng, 500) for _ in range(args.al_reads)]
+            steps.append(synth.both_strands(reads))
+        return [prof], synth.hmmer3_text([prof]), steps
     profiles, txt = make_profiles(args.seed, args.profiles)
     return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step)
 
@@ -379,10 +405,158 @@ def cpu_search_baseline(hmm_text, records, gates, seconds, seed):
                       "then its mid score on the survivors"}
 
 
+def cpu_align_baseline(hmm_text, records, gate, seconds):
+    """The reference's hit path with its traceback (findSimilarities with
+    needAlign, oracle/_ref) on the box's cores: 8-record SIMD batches of the
+    step, one per thread at a time, until the time budget is spent."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.ref import RefEngine, available
+    if not available(32):
+        return None
+    e = RefEngine(32)
+    e.set_rates()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(hmm_text)
+        path = f.name
+    e.load_profiles(path)
+    os.unlink(path)
+    M1 = e.profile(0)[1].shape[0]
+    codes = [e.decode(e.encode(r)) for r in records]
+    threads = os.cpu_count() or 1
+    batches = [codes[b:b + 8] for b in range(0, len(codes), 8)]
+    done_cells, done_b, t0 = 0.0, 0, time.perf_counter()
+    with ThreadPoolExecutor(threads) as pool:
+        while time.perf_counter() - t0 < seconds and done_b < len(batches):
+            chunk = batches[done_b:done_b + threads]
+            list(pool.map(lambda b: e.align(0, b, [gate] * len(b)), chunk))
+            done_b += len(chunk)
+            done_cells += M1 * sum(len(c) for b in chunk for c in b)
+    dt = time.perf_counter() - t0
+    return {"value": done_cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"{done_b} 8-record batches of one step ({done_cells:.3e} cells) in {dt:.1f} s, reference "
+                      "FP32 engine, findSimilarities with needAlign (scores, anchors, traceback)"}
+
+
+def run_align(args, rank, world, local):
+    import dummest_b200 as d
+    from dummest_b200 import _ffi as F
+    import torch
+
+    n_steps = args.warmup + args.steps
+    profiles, txt, steps = make_workload(args, rank, n_steps)
+    ctx = d.Context(device=local)
+    pid = ctx.load_hmm(txt)[0]
+    M = ctx.profile_length(pid)
+
+    def pairs_for(sids):
+        arr = (F.Pair * len(sids))()
+        for k, s in enumerate(sids):
+            arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, pid, args.al_gate
+        return arr
+
+    step_pairs = [pairs_for(ctx.add_dna(recs)) for recs in steps]
+    cells_step = [float(sum(len(r) for r in recs)) * (M + 1) for recs in steps]
+    for w in range(args.warmup):
+        ctx.align_raw(step_pairs[w])
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    cells, exact_ms, outs = 0.0, 0.0, []
+    phases = {}
+    for k in range(args.warmup, n_steps):
+        outs.append(ctx.align_raw(step_pairs[k]))
+        exact_ms += ctx.last_timing()["exact_ms"]  # the traced hits' exact replay
+        for key, v in ctx.last_align_timing().items():
+            phases[key] = phases.get(key, 0.0) + v
+        cells += cells_step[k]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    value, ms_max, cells_all = aggregate(cells, ms, world)
+    n_al = n_seg = 0
+    hit_cells = 0.0
+    for k, (al, sg) in zip(range(args.warmup, n_steps), outs):
+        hits = {a.pair for a in al}
+        hit_cells += sum(len(steps[k][i]) * (M + 1) for i in hits)
+        n_al += len(al)
+        n_seg += len(sg)
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = n_sm * 128 * 2 * sm_max * 1e6 / 1e12
+    # the exact replay of the hits: discovery and replay sweeps in both directions
+    achieved = 2 * FLOPS_PER_CELL * hit_cells / (exact_ms / 1e3) / 1e12 if exact_ms > 0 else None
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak if achieved else None, "traffic": None,
+                "peak_source": f"derived: {n_sm} SMs x 128 FP32 lanes x 2 x sm_max_mhz {sm_max:g}",
+                "kernel": "the exact kernel's discovery + replay sweeps with the traceback stores, over the hits",
+                "algorithmic_flops_per_cell": 2 * FLOPS_PER_CELL}
+    # e2e: each step's reads copied (2-bit packed) and decoded, the call, its alignments copied back
+    packed = [d.pack_dna(recs) for recs in steps]
+    ctx.clear_sequences()
+    base, e2e_pairs = 0, []
+    for k in range(n_steps):
+        e2e_pairs.append(pairs_for(list(range(base, base + len(steps[k])))))
+        base += len(steps[k])
+    for w in range(args.warmup):
+        words, mask, lens = packed[w]
+        ctx.add_packed(words, lens, mask)
+        ctx.align_raw(e2e_pairs[w])
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for k in range(args.warmup, n_steps):
+        words, mask, lens = packed[k]
+        ctx.add_packed(words, lens, mask)
+        al, sg = ctx.align_raw(e2e_pairs[k])
+        h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 12 * len(e2e_pairs[k])
+        d2h += 40 * len(al) + 12 * len(sg)
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
+           "d2h_bytes_per_step": d2h // args.steps}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_align_baseline(txt, steps[args.warmup], args.al_gate, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "hit-path traceback GCUPS (cells of every pair; hits traced)", "value": value, "unit": "GCUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+            "gpu_launches": None, "alignments_per_step": n_al / args.steps, "segments_per_step": n_seg / args.steps,
+            "hit_cell_fraction": hit_cells / cells, "exact_ms_per_step": exact_ms / args.steps,
+            "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()}}), flush=True)
+    ctx.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     profiles, txt, steps = make_workload(args, 0, 1)
+    if args.workload == "align":
+        vals, cb = [], None
+        per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_align_baseline(txt, steps[0], args.al_gate, per_step)
+            vals.append(cb["value"])
+        v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else vals[-1]
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": "hit-path traceback GCUPS (cells of every pair; hits traced)",
+            "value": v, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(args, world), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return
     if args.workload == "search":
         import dummest_b200 as d
         rng = np.random.default_rng(args.seed)
@@ -907,6 +1081,8 @@ def main():
             run_autograd(args, rank, world, local)
         elif args.workload == "search":
             run_search(args, rank, world, local)
+        elif args.workload == "align":
+            run_align(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -143,6 +143,7 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("dmst_align_fetch", C.c_int,
      [C.c_void_p, C.POINTER(Alignment), C.c_size_t, C.POINTER(Segment), C.c_size_t]),
+    ("dmst_last_align_timing", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("dmst_filter_threshold", C.c_int,
      [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_float)]),
     ("dmst_pending_calls", C.c_int, [C.c_void_p]),

@@ -13,6 +13,7 @@
 #include "null_model.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -23,6 +24,7 @@
 #include <new>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace dmst;
@@ -367,6 +369,7 @@ struct dmst_ctx {
     DevBuf<Seg> dAlignSegOut;
     std::vector<dmst_alignment> alignOut;
     std::vector<dmst_segment> alignSegOut;
+    double alignMs[8] = {};  // dmst_last_align_timing
 
     double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0, lastHostMs = 0;
     double lastPostMs = 0, lastWallMs = 0;
@@ -1748,7 +1751,7 @@ int dmst_anchors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_score *be
 // anchors on the host (from the spans), and the store pass for the kept ones.
 static size_t alignJobBytes(int M, int L) {
     const size_t cells = (size_t)(M + 1) * L;
-    return cells * (8 + 8 + 8) + (size_t)L * (4 + 4 + 16 + 8 + 8 + 4 + sizeof(WalkSpan) + 2 * sizeof(Seg)) +
+    return cells * (8 + 8 + 8) + (size_t)L * (4 + 4 + 8 * kFlankArrays + 8 + 8 + 4 + sizeof(WalkSpan) + 2 * sizeof(Seg)) +
            (size_t)alignRowInts(M) * 4 + 256;
 }
 
@@ -1764,6 +1767,13 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
     if (!ctx || (n && !pairs) || !n_alignments || !n_segments) return DMST_EINVAL;
     int st = drainCalls(ctx);
     if (st) return st;
+    using Clock = std::chrono::steady_clock;
+    auto msSince = [](Clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+    };
+    const auto tCall = Clock::now();
+    double *tm = ctx->alignMs;
+    for (int q = 0; q < 8; ++q) tm[q] = 0.0;
     ctx->nextSlot = ctx->oldest = 0;
     ctx->alignOut.clear();
     ctx->alignSegOut.clear();
@@ -1780,6 +1790,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         return st;
     }
     if ((st = completeCall(ctx))) return st;
+    tm[1] = msSince(tCall);
 
     // hits: laneHit with a report (dummest-dp-forward.hh:262-274, :489-490);
     // the gate is normalizeScore((double)minProbRatio, 0)
@@ -1798,7 +1809,11 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
             gates.push_back(g);
         }
     }
-    if (hits.empty()) return DMST_OK;
+    tm[7] = (double)hits.size();
+    if (hits.empty()) {
+        tm[0] = msSince(tCall);
+        return DMST_OK;
+    }
 
     size_t freeB = 0, totalB = 0;
     CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
@@ -1847,7 +1862,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         CK(ctx->dAlignRows.ensure((size_t)rowsN), "alloc traceback rows");
         CK(ctx->dAlignColR.ensure((size_t)cols), "alloc traceback columns");
         CK(ctx->dAlignColF.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignWork.ensure((size_t)(2 * cols + 8LL * nb)), "alloc traceback columns");
+        CK(ctx->dAlignWork.ensure((size_t)kFlankArrays * (cols + 4LL * nb)), "alloc traceback columns");
         CK(ctx->dAlignRev.ensure((size_t)cols), "alloc traceback columns");
         CK(ctx->dAlignFwd.ensure((size_t)cols), "alloc traceback columns");
         CK(ctx->dAlignCand.ensure((size_t)cols), "alloc traceback columns");
@@ -1858,6 +1873,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         std::vector<int> row((size_t)cols);
         std::vector<dmst_result> bres(nb);
         const int si = ctx->nextSlot;
+        auto tPhase = Clock::now();
         st = submitCall(ctx, bp.data(), nb, DMST_MODE_MID, bres.data(), nullptr, best.data(), row.data(), &jobs);
         if (st) {
             drainCalls(ctx);
@@ -1866,10 +1882,14 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         CallSlot &S = ctx->slot[si];
         sidesKernel<<<dim3((maxL + 127) / 128, nb), 128, 0, ctx->stream>>>(
             ctx->dAlignJobs.p, ctx->dAlignCells.p, ctx->dAlignRows.p, ctx->dAlignColR.p, ctx->dAlignColF.p);
-        flankKernel<<<(nb + 31) / 32, 32, 0, ctx->stream>>>(
-            ctx->dAlignJobs.p, nb, S.dPairs.p, ctx->dProfiles.p, ctx->dCodes.p, S.dSeeds.p, S.dScales.p, nr,
-            ctx->dAlignColR.p, ctx->dAlignColF.p, ctx->dAlignRows.p, ctx->dAlignWork.p, ctx->dAlignRev.p,
-            ctx->dAlignFwd.p);
+        flankPrepKernel<<<dim3((maxL + 4 + 127) / 128, nb), 128, 0, ctx->stream>>>(
+            ctx->dAlignJobs.p, S.dPairs.p, ctx->dProfiles.p, ctx->dCodes.p, S.dSeeds.p, S.dScales.p, nr,
+            ctx->dAlignColR.p, ctx->dAlignColF.p, ctx->dAlignRows.p, ctx->dAlignWork.p);
+        flankChainKernel<<<nb, 96, 0, ctx->stream>>>(ctx->dAlignJobs.p, S.dScales.p, nr, ctx->dAlignWork.p);
+        flankUnifyKernel<<<dim3((maxL + 127) / 128, nb), 128, 0, ctx->stream>>>(ctx->dAlignJobs.p, S.dScales.p, nr,
+                                                                                 ctx->dAlignWork.p);
+        flankSumKernel<<<nb, 64, 0, ctx->stream>>>(ctx->dAlignJobs.p, ctx->dAlignWork.p, ctx->dAlignRows.p,
+                                                   ctx->dAlignRev.p, ctx->dAlignFwd.p);
         xTableKernel<<<dim3((maxL + 127) / 128, (maxM + 1 + kXRows - 1) / kXRows, nb), 128, 0, ctx->stream>>>(
             ctx->dAlignJobs.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p, S.dScales.p,
             ctx->dAlignCells.p, ctx->dAlignRows.p, ctx->dAlignX.p);
@@ -1878,35 +1898,66 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
                                                           ctx->dAlignSuf.p);
         CK(cudaGetLastError(), "traceback table kernels");
         if ((st = completeCall(ctx))) return st;
+        CK(cudaStreamSynchronize(ctx->stream), "traceback tables");
+        tm[2] += msSince(tPhase);
+        tPhase = Clock::now();
 
         // The reference's sort of each hit's anchors (std::ranges::sort with
         // std::greater<>, dummest-dp-forward.hh:494, which libstdc++ runs as
-        // std::sort with the same comparisons, so ties land as there): every
-        // column, zero columns as placeholders; the candidates are the leading
-        // entries at or above the gate.
+        // std::sort with the same comparisons): every column, zero columns as
+        // placeholders; the candidates are the leading entries at or above the
+        // gate.  Entries below the gate sort after every passing one, so the
+        // passing entries alone, sorted, are the candidates in order unless two
+        // of them are equal scores: then where the reference's sort puts the
+        // tied ones depends on all L entries, and the full sort runs.  Hits are
+        // shared among host threads.
         struct Entry {
             dmst_score pair;
             int col;
         };
         std::vector<int> cand((size_t)cols);
-        std::vector<Entry> ent;
-        for (int j = 0; j < nb; ++j) {
+        auto sortJob = [&](int j, std::vector<Entry> &ent) {
             AlignJob &jb = jobs[j];
-            ent.resize(jb.L);
+            const dmst_score g{jb.minM, jb.minE};
+            auto greater = [](const Entry &x, const Entry &y) { return lessScore(y.pair, x.pair); };
+            ent.clear();
             for (int c = 0; c < jb.L; ++c) {
                 const dmst_score a = best[jb.colOff + c];
-                ent[c] = a.m != 0.0f ? Entry{a, c} : Entry{dmst_score{0.0f, 0}, 0};
+                if (a.m != 0.0f && !lessScore(a, g)) ent.push_back(Entry{a, c});
             }
-            std::sort(ent.begin(), ent.end(),
-                      [](const Entry &x, const Entry &y) { return lessScore(y.pair, x.pair); });
-            const dmst_score g{jb.minM, jb.minE};
+            std::sort(ent.begin(), ent.end(), greater);
+            bool tie = false;
+            for (size_t q = 1; q < ent.size() && !tie; ++q)
+                tie = ent[q].pair.m == ent[q - 1].pair.m && ent[q].pair.e == ent[q - 1].pair.e;
+            if (tie) {
+                ent.resize(jb.L);
+                for (int c = 0; c < jb.L; ++c) {
+                    const dmst_score a = best[jb.colOff + c];
+                    ent[c] = a.m != 0.0f ? Entry{a, c} : Entry{dmst_score{0.0f, 0}, 0};
+                }
+                std::sort(ent.begin(), ent.end(), greater);
+            }
             int nc = 0;
-            while (nc < jb.L && ent[nc].pair.m != 0.0f && !lessScore(ent[nc].pair, g)) {
+            while (nc < (int)ent.size() && ent[nc].pair.m != 0.0f && !lessScore(ent[nc].pair, g)) {
                 cand[jb.colOff + nc] = ent[nc].col;
                 ++nc;
             }
             jb.nCand = nc;
+        };
+        {
+            const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), nb / 8));
+            std::atomic<int> next{0};
+            auto worker = [&]() {
+                std::vector<Entry> ent;
+                for (int j; (j = next.fetch_add(1)) < nb;) sortJob(j, ent);
+            };
+            std::vector<std::thread> pool;
+            for (int q = 1; q < nt; ++q) pool.emplace_back(worker);
+            worker();
+            for (auto &th : pool) th.join();
         }
+        tm[3] += msSince(tPhase);
+        tPhase = Clock::now();
         int maxCand = 1;
         for (const AlignJob &jb : jobs) maxCand = std::max(maxCand, jb.nCand);
         CK(cudaMemcpyAsync(ctx->dAlignJobs.p, jobs.data(), nb * sizeof(AlignJob), cudaMemcpyHostToDevice,
@@ -1924,6 +1975,8 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
                            ctx->stream),
            "download traceback spans");
         CK(cudaStreamSynchronize(ctx->stream), "traceback spans");
+        tm[4] += msSince(tPhase);
+        tPhase = Clock::now();
 
         // The reference's choice (dummest-dp-forward.hh:497-531): in sorted
         // order, an anchor inside a kept alignment is skipped, and one whose
@@ -1963,6 +2016,8 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
                 ng += n;
             }
         }
+        tm[5] += msSince(tPhase);
+        tPhase = Clock::now();
         if (!items.empty()) {
             CK(ctx->dAlignItems.ensure(items.size()), "alloc traceback output");
             CK(ctx->dAlignSegOut.ensure((size_t)ng), "alloc traceback output");
@@ -1981,10 +2036,18 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
                "download segments");
             CK(cudaStreamSynchronize(ctx->stream), "traceback segments");
         }
+        tm[6] += msSince(tPhase);
         b0 = b1;
     }
     *n_alignments = ctx->alignOut.size();
     *n_segments = ctx->alignSegOut.size();
+    tm[0] = msSince(tCall);
+    return DMST_OK;
+}
+
+int dmst_last_align_timing(const dmst_ctx *ctx, double *out, int n) {
+    if (!ctx || !out || n < 0) return DMST_EINVAL;
+    for (int i = 0; i < n && i < 8; ++i) out[i] = ctx->alignMs[i];
     return DMST_OK;
 }
 

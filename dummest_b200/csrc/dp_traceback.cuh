@@ -7,7 +7,7 @@
 //                   and forwardSide[j] = sum over rows (0..M) of W0, each
 //                   scaled down with its rows' rescales (the reference's
 //                   per-cell fma(1, w, side) and per-row rescaleRow);
-//   flankKernel     buildFlankEVs: the entry and exit flank totals as exact
+//   flank*Kernel    buildFlankEVs: the entry and exit flank totals as exact
 //                   scores, and their largest exponents;
 //   xTableKernel    X(i, j) = promote(X_ij, cntF_i) * promote(W1[i+1][j],
 //                   cntB_{i+1}), the forward's combined match scores, and
@@ -96,117 +96,256 @@ __global__ void sidesKernel(const AlignJob *jobs, const float *cells, int *rows,
     colF[jb.colOff + j] = f;
 }
 
-// buildFlankEVs for one job per thread (dummest-dp.hh:137-256).  work holds
-// 2 (L + 4) scores per job: the middle entry masses and the suffix rest
-// masses; revEv receives the entry totals (reverseSideEv), fwdEv the exit
-// totals (forwardSideEv).
-__global__ void flankKernel(const AlignJob *jobs, int nJobs, const DevPair *pairs, const DevProfile *profiles,
-                            const uint8_t *codes, const float *seeds, const PairScales *scales, NullRates nr,
-                            const float *colR, const float *colF, int *rows, XS *work, XS *revEv, XS *fwdEv) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nJobs) return;
+// buildFlankEVs (dummest-dp.hh:137-256) in four kernels.  The reference's
+// per-lane loops hold three independent recurrences (the middle entry masses
+// and the suffix rest masses, run backward; the arrival masses, run forward),
+// an elementwise combination and two running sums; each recurrence stays one
+// sequential chain (ExpScore sums round at every step), but the chains run
+// side by side, and whatever depends on the column alone is computed in
+// parallel first.  Per job, work holds kFlankArrays arrays of L + 4 scores.
+constexpr int kFlankArrays = 9;
+enum FlankArray { kFBg = 0, kFPre, kFColR, kFColF, kFWeighted, kFMid, kFRest, kFArrival, kFUnified };
+
+struct FlankRates {
+    double sr, dr, keep, third;
+};
+__device__ __forceinline__ FlankRates flankRates(NullRates nr) {
+    FlankRates f;
+    f.sr = nr.single;
+    f.dr = nr.dbl;
+    f.keep = 1.0 - nr.single - nr.dbl;
+    f.third = 1.0 / 3.0;
+    return f;
+}
+__device__ __forceinline__ XS *flankArray(XS *work, const AlignJob &jb, int job, int a) {
+    return work + (size_t)kFlankArrays * (jb.colOff + 4LL * job) + (size_t)a * (jb.L + 4);
+}
+
+// Per column: the background codon score bgc(j), the prefix seed's score,
+// both column masses as exact scores, and the entry tiles' weighted sum.
+__global__ void flankPrepKernel(const AlignJob *jobs, const DevPair *pairs, const DevProfile *profiles,
+                                const uint8_t *codes, const float *seeds, const PairScales *scales, NullRates nr,
+                                const float *colR, const float *colF, const int *rows, XS *work) {
+    const int t = blockIdx.y;
     const AlignJob jb = jobs[t];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int L = jb.L;
+    if (j >= L + 4) return;
+    XS *bgx = flankArray(work, jb, t, kFBg), *prex = flankArray(work, jb, t, kFPre);
+    if (j >= L) {  // the arrays' tails stay zero
+        for (int a = 0; a < kFlankArrays; ++a) flankArray(work, jb, t, a)[j] = xsZero();
+        return;
+    }
     const DevPair p = pairs[jb.pair];
     const float *bg = profiles[p.prof].bg;
     const uint8_t *cd = codes + p.codeOff;
     const float *pre = seeds + p.seedOff;
     const PairScales sc = scales[jb.pair];
-    const int M = jb.M, L = jb.L;
+    const int M = jb.M;
     const int *cntB = rows + jb.rowOff, *cntF = cntB + (M + 2);
-    int *sideMax = rows + jb.rowOff + 3 * (M + 2);
-    const float *cR = colR + jb.colOff, *cF = colF + jb.colOff;
-    XS *mid = work + 2 * (jb.colOff + 4LL * t);
-    XS *rest = mid + (L + 4);
-    XS *rev = revEv + jb.colOff, *fwd = fwdEv + jb.colOff;
-
-    const double sr = nr.single, dr = nr.dbl;
-    const double keep = 1.0 - sr - dr;
-    const double third = 1.0 / 3.0;
-    const XS aS1 = splitNorm((double)sc.s1, 0), aS2 = splitNorm((double)sc.s2, 0), aSC = splitNorm((double)sc.sC, 0);
-    const XS bS1 = scaleScore(aS1, 4.0), bS2 = scaleScore(aS2, 16.0);
+    const FlankRates r = flankRates(nr);
     auto bgc = [&](int pos) { return (pos >= 0 && pos < L) ? splitNorm((double)bg[cd[pos]], 0) : xsZero(); };
     auto preS = [&](int pos) { return splitNorm((double)pre[pos], 0); };
-    const int cB0 = cntB[0], cFM = cntF[M + 1];
+    const XS aS1 = splitNorm((double)sc.s1, 0), aS2 = splitNorm((double)sc.s2, 0), aSC = splitNorm((double)sc.sC, 0);
+    bgx[j] = bgc(j);
+    prex[j] = preS(j);
+    flankArray(work, jb, t, kFColR)[j] = promoteScalar(colR[jb.colOff + j], cntB[0]);
+    flankArray(work, jb, t, kFColF)[j] = promoteScalar(colF[jb.colOff + j], cntF[M + 1]);
+    // entry tiles ending at j (the first piece weighs 1/3)
+    XS single = xsZero(), dbl = xsZero(), codon = xsZero();
+    if (j == 0) single = preS(0);
+    else single = scalarMul(scaleScore(preS(j - 1), r.sr), aS1);
+    if (j == 1) dbl = scaleScore(aS2, r.third);
+    else if (j >= 2) dbl = scalarMul(scaleScore(preS(j - 2), r.dr), aS2);
+    if (j == 2) codon = scalarMul(scaleScore(aSC, r.third), bgc(0));
+    else if (j >= 3) codon = scalarMul(scaleScore(scalarMul(preS(j - 3), aSC), r.keep), bgc(j - 2));
+    flankArray(work, jb, t, kFWeighted)[j] =
+        scalarAdd(single, scalarAdd(scaleScore(dbl, 2.0), scaleScore(codon, 3.0)));
+}
 
-    // middle entry masses, run backward
-    for (int q = L; q < L + 4; ++q) mid[q] = xsZero();
-    for (int j = L - 1; j >= 0; --j) {
-        XS c = scalarMul(scaleScore(mid[j + 1], sr), aS1);
-        c = scalarAdd(c, scalarMul(scaleScore(mid[j + 2], dr), aS2));
-        c = scalarAdd(c, scalarMul(scaleScore(scalarMul(mid[j + 3], aSC), keep), bgc(j + 1)));
-        mid[j] = scalarAdd(promoteScalar(cR[j], cB0), c);
+// The three recurrences, one per warp (thread 0 of warps 0, 1, 2), inputs
+// loaded kFlankAhead columns at a time ahead of the chain.
+constexpr int kFlankAhead = 8;
+__global__ void flankChainKernel(const AlignJob *jobs, const PairScales *scales, NullRates nr, XS *work) {
+    const int t = blockIdx.x;
+    if ((threadIdx.x & 31) != 0) return;
+    const int w = threadIdx.x >> 5;
+    const AlignJob jb = jobs[t];
+    const int L = jb.L;
+    const PairScales sc = scales[jb.pair];
+    const FlankRates r = flankRates(nr);
+    const XS aS1 = splitNorm((double)sc.s1, 0), aS2 = splitNorm((double)sc.s2, 0), aSC = splitNorm((double)sc.sC, 0);
+    const XS *__restrict__ bgx = flankArray(work, jb, t, kFBg);
+    if (w == 0) {
+        // middle entry masses, backward: mid[j] = colR[j] + cover of j+1.. continued
+        const XS *__restrict__ cR = flankArray(work, jb, t, kFColR);
+        XS *__restrict__ mid = flankArray(work, jb, t, kFMid);
+        XS m1 = xsZero(), m2 = xsZero(), m3 = xsZero();  // mid[j+1], mid[j+2], mid[j+3]
+        for (int q = L; q < L + 4; ++q) mid[q] = xsZero();
+        for (int hi = L - 1; hi >= 0; hi -= kFlankAhead) {
+            XS vc[kFlankAhead], vb[kFlankAhead];
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) {
+                const int j = hi - u;
+                vc[u] = j >= 0 ? ldXS(cR + j) : xsZero();
+                vb[u] = j >= 0 ? ldXS(bgx + j + 1) : xsZero();
+            }
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) {
+                const int j = hi - u;
+                if (j < 0) break;
+                XS c = scalarMul(scaleScore(m1, r.sr), aS1);
+                c = scalarAdd(c, scalarMul(scaleScore(m2, r.dr), aS2));
+                c = scalarAdd(c, scalarMul(scaleScore(scalarMul(m3, aSC), r.keep), vb[u]));
+                const XS m = scalarAdd(vc[u], c);
+                stXS(mid + j, m);
+                m3 = m2;
+                m2 = m1;
+                m1 = m;
+            }
+        }
+    } else if (w == 1) {
+        // cover of [j, end): the empty rest at the end counts 1
+        XS *__restrict__ rest = flankArray(work, jb, t, kFRest);
+        const XS bS1 = scaleScore(aS1, 4.0), bS2 = scaleScore(aS2, 16.0);
+        for (int q = L; q < L + 4; ++q) rest[q] = xsZero();
+        rest[L] = pow2Score(0);
+        XS r1 = pow2Score(0), r2 = xsZero(), r3 = xsZero();  // rest[j+1], rest[j+2], rest[j+3]
+        for (int hi = L - 1; hi >= 0; hi -= kFlankAhead) {
+            XS vb[kFlankAhead];
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) vb[u] = hi - u >= 0 ? ldXS(bgx + hi - u) : xsZero();
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) {
+                const int j = hi - u;
+                if (j < 0) break;
+                const XS one = scalarMul(scaleScore(r1, r.sr), aS1);
+                const XS two = (j + 1 <= L - 1) ? scalarMul(scaleScore(r2, r.dr), aS2) : scaleScore(bS1, r.dr * 0.25);
+                XS three;
+                if (j + 2 <= L - 1)
+                    three = scalarMul(scaleScore(scalarMul(r3, aSC), r.keep), vb[u]);
+                else if (j + 1 <= L - 1)
+                    three = scaleScore(bS2, r.keep * 0.0625);
+                else
+                    three = scaleScore(bS1, r.keep * 0.25);
+                const XS v = scalarAdd(one, scalarAdd(two, three));
+                stXS(rest + j, v);
+                r3 = r2;
+                r2 = r1;
+                r1 = v;
+            }
+        }
+    } else if (w == 2) {
+        // arrival masses, forward: cover ending at j grown from the cut masses
+        const XS *__restrict__ cF = flankArray(work, jb, t, kFColF);
+        XS *__restrict__ fa = flankArray(work, jb, t, kFArrival);
+        XS f1 = xsZero(), f2 = xsZero(), f3 = xsZero();  // arrival at j-1, j-2, j-3
+        for (int lo = 0; lo < L; lo += kFlankAhead) {
+            XS vc[kFlankAhead], vb[kFlankAhead];
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) {
+                const int j = lo + u;
+                vc[u] = j < L ? ldXS(cF + j) : xsZero();
+                vb[u] = (j < L && j >= 2) ? ldXS(bgx + j - 2) : xsZero();
+            }
+#pragma unroll
+            for (int u = 0; u < kFlankAhead; ++u) {
+                const int j = lo + u;
+                if (j >= L) break;
+                XS a = vc[u];
+                if (j >= 1) a = scalarAdd(a, scalarMul(scaleScore(f1, r.sr), aS1));
+                if (j >= 2) a = scalarAdd(a, scalarMul(scaleScore(f2, r.dr), aS2));
+                if (j >= 3) a = scalarAdd(a, scalarMul(scaleScore(scalarMul(f3, aSC), r.keep), vb[u]));
+                stXS(fa + j, a);
+                f3 = f2;
+                f2 = f1;
+                f1 = a;
+            }
+        }
     }
-    // cover of [j, end): the empty rest at the end counts 1
-    for (int q = 0; q < L + 4; ++q) rest[q] = xsZero();
-    rest[L] = pow2Score(0);
-    for (int j = L - 1; j >= 0; --j) {
-        const XS one = scalarMul(scaleScore(rest[j + 1], sr), aS1);
-        const XS two = (j + 1 <= L - 1) ? scalarMul(scaleScore(rest[j + 2], dr), aS2) : scaleScore(bS1, dr * 0.25);
-        XS three;
-        if (j + 2 <= L - 1)
-            three = scalarMul(scaleScore(scalarMul(rest[j + 3], aSC), keep), bgc(j));
-        else if (j + 1 <= L - 1)
-            three = scaleScore(bS2, keep * 0.0625);
-        else
-            three = scaleScore(bS1, keep * 0.25);
-        rest[j] = scalarAdd(one, scalarAdd(two, three));
+}
+
+// Per-base amounts (start pieces plus end pieces), one thread per column.
+__global__ void flankUnifyKernel(const AlignJob *jobs, const PairScales *scales, NullRates nr, XS *work) {
+    const int t = blockIdx.y;
+    const AlignJob jb = jobs[t];
+    const int L = jb.L;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= L) return;
+    const PairScales sc = scales[jb.pair];
+    const FlankRates r = flankRates(nr);
+    const XS aS1 = splitNorm((double)sc.s1, 0), aS2 = splitNorm((double)sc.s2, 0), aSC = splitNorm((double)sc.sC, 0);
+    const XS bS1 = scaleScore(aS1, 4.0), bS2 = scaleScore(aS2, 16.0);
+    const XS *bgx = flankArray(work, jb, t, kFBg);
+    const XS *mid = flankArray(work, jb, t, kFMid), *rest = flankArray(work, jb, t, kFRest);
+    const XS *fa = flankArray(work, jb, t, kFArrival);
+    XS total = scalarMul(ldXS(mid + j), ldXS(flankArray(work, jb, t, kFWeighted) + j));
+    const XS rn = ldXS(rest + j + 1);
+    if (j >= 1) {
+        const XS exit1 = scalarMul(scaleScore(rn, r.sr), aS1);
+        total = scalarAdd(total, scalarMul(ldXS(fa + j - 1), exit1));
     }
-    // forward arrival masses (rolling), entry tiles and the per-base amounts;
-    // the entry totals accumulate forward, the amounts wait in fwd
-    XS fa1 = xsZero(), fa2 = xsZero(), fa3 = xsZero();  // arrival at j-1, j-2, j-3
+    if (j >= 2) {
+        const XS exit2 = scalarMul(scaleScore(rn, r.dr), aS2);
+        total = scalarAdd(total, scaleScore(scalarMul(ldXS(fa + j - 2), exit2), 2.0));
+    }
+    if (j >= 3) {
+        const XS exit3 = scalarMul(scaleScore(scalarMul(rn, aSC), r.keep), ldXS(bgx + j - 2));
+        total = scalarAdd(total, scaleScore(scalarMul(ldXS(fa + j - 3), exit3), 3.0));
+    }
+    if (j == L - 1) {  // leftover endings at the last base
+        const XS f1 = ldXS(fa + j - 1);
+        total = scalarAdd(total, scaleScore(scalarMul(f1, scaleScore(bS1, r.dr * 0.25)), 2.0));
+        total = scalarAdd(total, scaleScore(scalarMul(f1, scaleScore(bS1, r.keep * 0.25)), 3.0));
+        if (j - 2 >= 0)
+            total = scalarAdd(total, scaleScore(scalarMul(ldXS(fa + j - 2), scaleScore(bS2, r.keep * 0.0625)), 3.0));
+    }
+    stXS(flankArray(work, jb, t, kFUnified) + j, scaleScore(total, r.third));
+}
+
+// The entry totals (running forward, warp 0) and the exit totals (running
+// backward, warp 1) with their largest exponents.
+__global__ void flankSumKernel(const AlignJob *jobs, const XS *work, int *rows, XS *revEv, XS *fwdEv) {
+    const int t = blockIdx.x;
+    if ((threadIdx.x & 31) != 0) return;
+    const int w = threadIdx.x >> 5;
+    const AlignJob jb = jobs[t];
+    const int L = jb.L;
+    const XS *__restrict__ u = flankArray(const_cast<XS *>(work), jb, t, kFUnified);
+    int *sideMax = rows + jb.rowOff + 3 * (jb.M + 2);
     XS cum = xsZero();
-    int revMax = INT_MIN;
-    for (int j = 0; j < L; ++j) {
-        XS single = xsZero(), dbl = xsZero(), codon = xsZero();
-        if (j == 0) single = preS(0);
-        else single = scalarMul(scaleScore(preS(j - 1), sr), aS1);
-        if (j == 1) dbl = scaleScore(aS2, third);
-        else if (j >= 2) dbl = scalarMul(scaleScore(preS(j - 2), dr), aS2);
-        if (j == 2) codon = scalarMul(scaleScore(aSC, third), bgc(0));
-        else if (j >= 3) codon = scalarMul(scaleScore(scalarMul(preS(j - 3), aSC), keep), bgc(j - 2));
-        const XS weighted = scalarAdd(single, scalarAdd(scaleScore(dbl, 2.0), scaleScore(codon, 3.0)));
-        XS total = scalarMul(mid[j], weighted);
-        if (j >= 1) {
-            const XS exit1 = scalarMul(scaleScore(rest[j + 1], sr), aS1);
-            total = scalarAdd(total, scalarMul(fa1, exit1));
+    int mx = INT_MIN;
+    if (w == 0) {
+        XS *__restrict__ rev = revEv + jb.colOff;
+        for (int lo = 0; lo < L; lo += kFlankAhead) {
+            XS v[kFlankAhead];
+#pragma unroll
+            for (int q = 0; q < kFlankAhead; ++q) v[q] = lo + q < L ? ldXS(u + lo + q) : xsZero();
+#pragma unroll
+            for (int q = 0; q < kFlankAhead; ++q) {
+                if (lo + q >= L) break;
+                cum = scalarAdd(cum, v[q]);
+                stXS(rev + lo + q, cum);
+                if (cum.m != 0.0f && cum.e > mx) mx = cum.e;
+            }
         }
-        if (j >= 2) {
-            const XS exit2 = scalarMul(scaleScore(rest[j + 1], dr), aS2);
-            total = scalarAdd(total, scaleScore(scalarMul(fa2, exit2), 2.0));
+        sideMax[0] = mx;
+    } else if (w == 1) {
+        XS *__restrict__ fwd = fwdEv + jb.colOff;
+        for (int hi = L - 1; hi >= 0; hi -= kFlankAhead) {
+            XS v[kFlankAhead];
+#pragma unroll
+            for (int q = 0; q < kFlankAhead; ++q) v[q] = hi - q >= 0 ? ldXS(u + hi - q) : xsZero();
+#pragma unroll
+            for (int q = 0; q < kFlankAhead; ++q) {
+                if (hi - q < 0) break;
+                cum = scalarAdd(cum, v[q]);
+                stXS(fwd + hi - q, cum);
+                if (cum.m != 0.0f && cum.e > mx) mx = cum.e;
+            }
         }
-        if (j >= 3) {
-            const XS exit3 = scalarMul(scaleScore(scalarMul(rest[j + 1], aSC), keep), bgc(j - 2));
-            total = scalarAdd(total, scaleScore(scalarMul(fa3, exit3), 3.0));
-        }
-        if (j == L - 1) {  // leftover endings at the last base
-            total = scalarAdd(total, scaleScore(scalarMul(fa1, scaleScore(bS1, dr * 0.25)), 2.0));
-            total = scalarAdd(total, scaleScore(scalarMul(fa1, scaleScore(bS1, keep * 0.25)), 3.0));
-            if (j - 2 >= 0) total = scalarAdd(total, scaleScore(scalarMul(fa2, scaleScore(bS2, keep * 0.0625)), 3.0));
-        }
-        const XS unified = scaleScore(total, third);
-        fwd[j] = unified;
-        cum = scalarAdd(cum, unified);
-        rev[j] = cum;
-        if (cum.m != 0.0f && cum.e > revMax) revMax = cum.e;
-        // this column's arrival, for the columns after it
-        XS arr = promoteScalar(cF[j], cFM);
-        if (j >= 1) arr = scalarAdd(arr, scalarMul(scaleScore(fa1, sr), aS1));
-        if (j >= 2) arr = scalarAdd(arr, scalarMul(scaleScore(fa2, dr), aS2));
-        if (j >= 3) arr = scalarAdd(arr, scalarMul(scaleScore(scalarMul(fa3, aSC), keep), bgc(j - 2)));
-        fa3 = fa2;
-        fa2 = fa1;
-        fa1 = arr;
+        sideMax[1] = mx;
     }
-    // exit totals accumulate backward
-    cum = xsZero();
-    int fwdMax = INT_MIN;
-    for (int j = L - 1; j >= 0; --j) {
-        cum = scalarAdd(cum, fwd[j]);
-        fwd[j] = cum;
-        if (cum.m != 0.0f && cum.e > fwdMax) fwdMax = cum.e;
-    }
-    sideMax[0] = revMax;
-    sideMax[1] = fwdMax;
 }
 
 // X table, one thread per (job, column, group of kXRows rows).

@@ -277,16 +277,17 @@ class Context:
 
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
-        (alignments, segments) as ctypes arrays (Alignment, Segment)."""
+        (alignments, segments): a ctypes Alignment array and an (n, 3) int32
+        array of (start1, start2, length)."""
         n = len(pairs)
         na, ns = C.c_size_t(0), C.c_size_t(0)
         st = self.lib.dmst_align(self.h, pairs, n, out, C.byref(na), C.byref(ns))
         self._check(st, "dmst_align")
-        al = (F.Alignment * max(na.value, 1))()
-        sg = (F.Segment * max(ns.value, 1))()
-        st = self.lib.dmst_align_fetch(self.h, al, na.value, sg, ns.value)
+        al = (F.Alignment * na.value)()
+        sg = np.empty((ns.value, 3), np.int32)
+        st = self.lib.dmst_align_fetch(self.h, al, na.value, sg.ctypes.data_as(C.POINTER(F.Segment)), ns.value)
         self._check(st, "dmst_align_fetch")
-        return al[:na.value], sg[:ns.value]
+        return al, sg
 
     def align(self, seq_ids: Sequence[int], pids, min_prob_ratio):
         """Alignments of each (read, profile) pair with its gate (dmst_align).
@@ -301,8 +302,7 @@ class Context:
         for k in range(n):
             pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = seq_ids[k], pids[k], mpr[k]
         res = (F.Result * n)()
-        al, sg = self.align_raw(pairs, res)
-        segs = np.array([(s.start1, s.start2, s.length) for s in sg], np.int32).reshape(-1, 3)
+        al, segs = self.align_raw(pairs, res)
         out = [[] for _ in range(n)]
         for a in al:
             out[a.pair].append((a.score.m, a.score.e, a.ln_score, a.anchor1, a.anchor2,
@@ -385,6 +385,15 @@ class Context:
         r, w = C.c_int(), C.c_int()
         self._check(self.lib.dmst_tuned_shape(self.h, M, C.byref(r), C.byref(w)), "dmst_tuned_shape")
         return r.value, w.value
+
+    def last_align_timing(self) -> dict:
+        """Wall-clock phases (ms) of the last align call (dmst_last_align_timing)."""
+        v = (C.c_double * 8)()
+        self.lib.dmst_last_align_timing(self.h, v, 8)
+        keys = ("wall_ms", "score_ms", "tables_ms", "sort_ms", "span_ms", "choice_ms", "store_ms")
+        out = {k: v[i] for i, k in enumerate(keys)}
+        out["hits"] = int(v[7])
+        return out
 
     def last_timing(self) -> dict:
         v = (C.c_double * 10)()

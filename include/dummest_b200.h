@@ -279,6 +279,11 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
  * at least its counts, else DMST_ERANGE). */
 int dmst_align_fetch(const dmst_ctx *ctx, dmst_alignment *alignments, size_t cap_alignments,
                      dmst_segment *segments, size_t cap_segments);
+/* Wall-clock phases of the last dmst_align call (ms): out[0] the whole call,
+ * [1] scoring every pair, [2] the hits' exact replay and traceback tables,
+ * [3] the anchor sort, [4] the walks' span pass, [5] the choice of anchors,
+ * [6] the kept walks and the segment copy, [7] hits traced.  n <= 8. */
+int dmst_last_align_timing(const dmst_ctx *ctx, double *out, int n);
 
 /* The filter gate as a float threshold: the smallest float best b whose
  * E-value K_filter * total_length / exp(ln(b) * lambda_filter) is at most
