@@ -27,6 +27,7 @@ from .engine import (  # noqa: F401
     decode_letters,
     encode_dna,
     estimate_gumbel,
+    fasta_contigs,
     filter_threshold,
     finalize_hmm,
     pack_dna,

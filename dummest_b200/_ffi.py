@@ -63,6 +63,19 @@ class Pair(C.Structure):
     _fields_ = [("seq", C.c_int32), ("profile", C.c_int32), ("min_prob_ratio", C.c_float)]
 
 
+class Contig(C.Structure):
+    _fields_ = [
+        ("record", C.c_int32),
+        ("start", C.c_int32),
+        ("length", C.c_int32),
+        ("seq_id", C.c_int32),
+        ("name_off", C.c_int64),
+        ("name_len", C.c_int32),
+        ("pad", C.c_int32),
+        ("letter_off", C.c_int64),
+    ]
+
+
 class Alignment(C.Structure):
     _fields_ = [
         ("pair", C.c_int32),
@@ -139,6 +152,11 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
     ("dmst_anchors", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Score), C.POINTER(C.c_int), C.POINTER(Result)]),
+    ("dmst_fasta_contigs", C.c_int,
+     [C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
+      C.POINTER(C.c_size_t)]),
+    ("dmst_seqs_add_fasta", C.c_int,
+     [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_align", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("dmst_align_fetch", C.c_int,

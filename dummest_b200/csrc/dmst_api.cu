@@ -776,6 +776,65 @@ int dmst_seqs_add_dna(dmst_ctx *ctx, const char *ascii, const int64_t *offsets, 
     return DMST_OK;
 }
 
+static void fillContig(dmst_contig &o, const FastaContig &c, int seqId) {
+    o.record = c.record;
+    o.start = c.start;
+    o.length = c.length;
+    o.seq_id = seqId;
+    o.name_off = (int64_t)c.nameOff;
+    o.name_len = c.nameLen;
+    o.pad = 0;
+    o.letter_off = (int64_t)c.letterOff;
+}
+
+int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs, size_t *n_contigs,
+                       char *letters, size_t cap_letters, size_t *n_letters) {
+    if ((!text && len) || !n_contigs || !n_letters) return DMST_EINVAL;
+    std::vector<FastaContig> cs;
+    std::string lt;
+    if (fastaContigs(text, len, cs, lt, nullptr)) return DMST_EPARSE;
+    *n_contigs = cs.size();
+    *n_letters = lt.size();
+    if (cap_contigs < cs.size() || cap_letters < lt.size()) return DMST_ERANGE;
+    if ((cs.size() && !contigs) || (lt.size() && !letters)) return DMST_EINVAL;
+    for (size_t k = 0; k < cs.size(); ++k) fillContig(contigs[k], cs[k], -1);
+    if (!lt.empty()) std::memcpy(letters, lt.data(), lt.size());
+    return DMST_OK;
+}
+
+int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs,
+                        size_t *n_contigs) {
+    if (!ctx || (!text && len) || !n_contigs) return DMST_EINVAL;
+    std::vector<FastaContig> cs;
+    std::string lt, perr;
+    if (fastaContigs(text, len, cs, lt, &perr)) return ctx->fail(DMST_EPARSE, "FASTA: %s", perr.c_str());
+    *n_contigs = cs.size();
+    if (cap_contigs < cs.size()) return ctx->fail(DMST_ERANGE, "FASTA: %zu contigs, capacity %zu", cs.size(), cap_contigs);
+    if (cs.size() && !contigs) return DMST_EINVAL;
+    // Contigs of 3 or more letters as ASCII: A, C, G, T as they are, every
+    // other letter as 'N' (decodeSequence reads any non-ACGT letter alike).
+    std::string ascii;
+    std::vector<int64_t> off(1, 0);
+    std::vector<int> which;
+    for (size_t k = 0; k < cs.size(); ++k) {
+        if (cs[k].length < 3) continue;
+        for (int q = 0; q < cs[k].length; ++q) {
+            const char v = lt[cs[k].letterOff + q];
+            ascii.push_back(v == 0 ? 'A' : v == 1 ? 'C' : v == 5 ? 'G' : v == 16 ? 'T' : 'N');
+        }
+        off.push_back((int64_t)ascii.size());
+        which.push_back((int)k);
+    }
+    int first = (int)ctx->seqLen.size();
+    if (!which.empty()) {
+        const int st = dmst_seqs_add_dna(ctx, ascii.data(), off.data(), (int)which.size(), &first);
+        if (st) return st;
+    }
+    for (size_t k = 0; k < cs.size(); ++k) fillContig(contigs[k], cs[k], -1);
+    for (size_t q = 0; q < which.size(); ++q) contigs[which[q]].seq_id = first + (int)q;
+    return DMST_OK;
+}
+
 int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *mask_bits, const int64_t *offsets,
                          int nseq, int *first_id) {
     if (!ctx || (!words && nseq > 0)) return DMST_EINVAL;

@@ -303,6 +303,102 @@ int encodeDna(const char *ascii, int L, char *letters) {
     return L;
 }
 
+// The FASTA reader's character classes (dummest.cc:445-456): 125 for
+// characters up to ' ' (skipped), 126 for '>' (a record starts), the
+// protein alphabet's letter codes (either case), IUPAC ambiguity codes
+// RYSWKMBDHVN as 22 (either case), 127 for everything else (ends a contig).
+static const unsigned char *fastaClasses() {
+    static unsigned char t[256];
+    static bool built = false;
+    if (!built) {
+        for (int c = 0; c < 256; ++c) t[c] = c <= ' ' ? 125 : 127;
+        t[(unsigned char)'>'] = 126;
+        for (int i = 0; kAlphabet[i]; ++i) {
+            const int c = (unsigned char)kAlphabet[i];
+            t[toupper(c)] = t[tolower(c)] = (unsigned char)i;
+        }
+        for (const char *q = "RYSWKMBDHVN"; *q; ++q) t[(unsigned char)*q] = t[tolower((unsigned char)*q)] = 22;
+        built = true;
+    }
+    return t;
+}
+
+// readContig (dummest-sequence.hh:6-82) over a whole text: a record is '>'
+// and a name (the first word of the line); its sequence, up to the next
+// '>', is cut into contigs at characters outside the classes above (each
+// such character counts one position of the record, so a contig's start is
+// its position in the record), with characters up to ' ' skipped.
+// Empty contigs are not reported.
+int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
+                 std::string *err) {
+    const unsigned char *cls = fastaClasses();
+    size_t i = 0;
+    int record = -1;
+    int recLen = 0;
+    size_t nameOff = 0;
+    int nameLen = 0;
+    bool inRecord = false;
+    while (i < len) {
+        if (!inRecord) {
+            while (i < len && isspace((unsigned char)text[i])) ++i;  // istream >> char
+            if (i >= len) break;
+            if (text[i] != '>') {
+                if (err) *err = "bad sequence data: no '>'";
+                return -1;
+            }
+            ++i;
+            size_t lineEnd = i;
+            while (lineEnd < len && text[lineEnd] != '\n') ++lineEnd;
+            size_t w = i;
+            while (w < lineEnd && isspace((unsigned char)text[w])) ++w;
+            size_t we = w;
+            while (we < lineEnd && !isspace((unsigned char)text[we])) ++we;
+            if (we == w) {
+                if (err) *err = "bad sequence data: no name";
+                return -1;
+            }
+            ++record;
+            nameOff = w;
+            nameLen = (int)(we - w);
+            recLen = 0;
+            i = lineEnd < len ? lineEnd + 1 : len;
+            inRecord = true;
+        }
+        // skip symbols that cannot start a contig, counting the visible ones
+        while (i < len && text[i] != '>') {
+            const unsigned char c = (unsigned char)text[i];
+            if (cls[c] < 125) break;
+            if (c > ' ') ++recLen;
+            ++i;
+        }
+        const size_t first = letters.size();
+        while (i < len && cls[(unsigned char)text[i]] < 126) {
+            const unsigned char c = (unsigned char)text[i];
+            if (c > ' ') letters.push_back((char)cls[c]);
+            ++i;
+        }
+        const size_t n = letters.size() - first;
+        if (n > (size_t)INT32_MAX / 2) {
+            if (err) *err = "sequence is too long";
+            return -1;
+        }
+        if (n == 0) {  // the record's end: the next character is '>' or the text ends
+            inRecord = false;
+            continue;
+        }
+        FastaContig fc;
+        fc.record = record;
+        fc.start = recLen;
+        fc.length = (int)n;
+        fc.nameOff = nameOff;
+        fc.nameLen = nameLen;
+        fc.letterOff = first;
+        recLen += (int)n;
+        out.push_back(fc);
+    }
+    return 0;
+}
+
 // Letter code -> 2-bit base, or -1 when it is not one of A, C, G, T.
 static int letterToBase(char v) {
     switch (v) {

@@ -52,6 +52,18 @@ void standardCodeTable(uint8_t out[64]);
 int parseHmmText(const char *text, size_t len, std::vector<RawProfile> &out, std::string *err);
 int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err);
 int encodeDna(const char *ascii, int L, char *letters);
+
+// One contig of a FASTA text (readContig, dummest-sequence.hh:6-82).
+struct FastaContig {
+    int record;          // index of its record
+    int start;           // Contig::start: position in the record, skipped symbols counted
+    int length;
+    size_t nameOff;      // the record name: the first word of its header line, in the text
+    int nameLen;
+    size_t letterOff;    // its letter codes in the output string
+};
+int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
+                 std::string *err);
 int decodeLetters(const char *letters, int L, uint8_t *codes);
 int calibrationSequence(const float *letterFreqs, float bgStop, const Rates &r, int trial, int seqLen, int border,
                         char *out);

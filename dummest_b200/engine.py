@@ -275,6 +275,21 @@ class Context:
             o += L
         return out, res
 
+    def add_fasta(self, text: str | bytes) -> list[dict]:
+        """Contigs of a FASTA text added as sequences (dmst_seqs_add_fasta):
+        per contig {record, name, start, length, seq_id} (seq_id -1: shorter
+        than 3, not added)."""
+        b = text.encode() if isinstance(text, str) else text
+        n = C.c_size_t(0)
+        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), None, 0, C.byref(n))
+        if st != F.DMST_ERANGE and st != 0:
+            self._check(st, "dmst_seqs_add_fasta")
+        arr = (F.Contig * max(n.value, 1))()
+        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), arr, n.value, C.byref(n))
+        self._check(st, "dmst_seqs_add_fasta")
+        return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
+                 "length": c.length, "seq_id": c.seq_id} for c in arr[:n.value]]
+
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
         (alignments, segments): a ctypes Alignment array and an (n, 3) int32
@@ -548,4 +563,23 @@ def filter_threshold(lambda_filter: float, k_filter: float, total_length: float,
     if st != F.DMST_OK:
         raise ValueError(f"dmst_filter_threshold: status {st}")
     return out.value
+
+
+def fasta_contigs(text: str | bytes):
+    """The reference reader's contigs of a FASTA text (dmst_fasta_contigs, no
+    GPU): per contig {record, name, start, length} and its letter codes."""
+    lib = F.load()
+    b = text.encode() if isinstance(text, str) else text
+    n, nl = C.c_size_t(0), C.c_size_t(0)
+    st = lib.dmst_fasta_contigs(b, len(b), None, 0, C.byref(n), None, 0, C.byref(nl))
+    if st not in (0, F.DMST_ERANGE):
+        raise ValueError(f"dmst_fasta_contigs: status {st}")
+    arr = (F.Contig * max(n.value, 1))()
+    lt = C.create_string_buffer(max(nl.value, 1))
+    st = lib.dmst_fasta_contigs(b, len(b), arr, n.value, C.byref(n), lt, nl.value, C.byref(nl))
+    if st != 0:
+        raise ValueError(f"dmst_fasta_contigs: status {st}")
+    letters = np.frombuffer(lt.raw[:nl.value], np.uint8).copy()
+    return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
+             "length": c.length, "letters": letters[c.letter_off:c.letter_off + c.length]} for c in arr[:n.value]]
 

@@ -179,6 +179,45 @@ int dmst_seqs_add_decoded(dmst_ctx *ctx, const uint8_t *codes, const int64_t *of
 int dmst_seqs_add_dna(dmst_ctx *ctx, const char *ascii, const int64_t *offsets, int nseq, int *first_id);
 int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *mask_bits, const int64_t *offsets,
                          int nseq, int *first_id);
+/* One contig of a FASTA text, as the reference's reader cuts it (readContig,
+ * dummest-sequence.hh:6-82, with the IUPAC character classes of
+ * dummest.cc:445-456): a record is '>' and a name (the first word of the
+ * line); its sequence runs to the next '>' and is cut into contigs at
+ * characters that are neither letters of the protein alphabet
+ * ("ACDEFGHIKLMNPQRSTVWYUO?*", either case), IUPAC codes (RYSWKMBDHVN, read
+ * as 22) nor characters up to ' ' (skipped); each cutting character counts
+ * one position of the record. */
+typedef struct dmst_contig {
+    int32_t record;      /* index of its record in the text */
+    int32_t start;       /* Contig::start: its position in the record */
+    int32_t length;      /* letters */
+    int32_t seq_id;      /* dmst_seqs_add_fasta: its sequence id (-1: shorter than 3, not added) */
+    int64_t name_off;    /* the record's name in the text */
+    int32_t name_len;
+    int32_t pad;
+    int64_t letter_off;  /* dmst_fasta_contigs: its letter codes in letters */
+} dmst_contig;
+
+/* The contigs of a FASTA text and their letter codes (the reader's
+ * charToNumber values: A=0 C=1 G=5 T=16, IUPAC 22, other letters their
+ * protein codes), host only.  *n_contigs and *n_letters get the counts; with
+ * capacities below them nothing is written and DMST_ERANGE is returned.
+ * A text not starting with '>' (after whitespace) or a header without a name
+ * is DMST_EPARSE, as the reader fails.  A '*' inside DNA (code 23) is read
+ * as a letter, which the reference's decodeSequence does not accept (it
+ * asserts codes <= 22); the library decodes it as any non-ACGT letter. */
+int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs, size_t *n_contigs,
+                       char *letters, size_t cap_letters, size_t *n_letters);
+/* Reads a FASTA text (dummest.cc:553-606's readContig loop) and adds each
+ * contig of length >= 3 as one sequence, decoded as the engine decodes it
+ * (decodeSequence: a triplet with any letter other than A, C, G, T is '?').
+ * Masking (the reference's tantan pass, makeMaskedSequence) stays with the
+ * caller: a base written as 'N' decodes as the reference's masked copy
+ * does.  contigs (cap_contigs entries)
+ * gets every contig with its sequence id; with too small a capacity nothing
+ * is added and DMST_ERANGE is returned, *n_contigs holding the count. */
+int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs,
+                        size_t *n_contigs);
 /* Drop all sequences (device memory is kept for reuse). */
 int dmst_seqs_clear(dmst_ctx *ctx);
 int dmst_seq_count(const dmst_ctx *ctx);

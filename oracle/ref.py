@@ -52,6 +52,8 @@ def lib(bits: int = 32) -> C.CDLL:
                                                 P(C.c_int), P(C.c_double), P(C.c_float), P(C.c_int)]),
         "dmstref_backward_only": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), C.c_int, P(C.c_float)]),
         "dmstref_anchors": (C.c_int, [C.c_int, P(C.c_uint8), C.c_int, P(C.c_float), P(C.c_int), P(C.c_int)]),
+        "dmstref_read_fasta": (C.c_int, [C.c_char_p, C.c_longlong, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int,
+                                         C.c_char_p, C.c_longlong, C.c_char_p, C.c_longlong]),
         "dmstref_align": (C.c_int, [C.c_int, P(P(C.c_uint8)), P(C.c_int), P(C.c_float), C.c_int, C.c_int,
                                     P(C.c_int), P(C.c_float), P(C.c_int), P(C.c_double), P(C.c_int), P(C.c_int),
                                     P(C.c_int), C.c_int, P(C.c_int), P(C.c_int)]),
@@ -155,6 +157,24 @@ class RefEngine:
                                   e.ctypes.data_as(P(C.c_int)), row.ctypes.data_as(P(C.c_int))) != 0:
             raise ValueError("reference anchors failed")
         return m, e, row
+
+    def read_fasta(self, text: bytes):
+        """The reference reader's contigs of a well-formed FASTA text: (records,
+        starts, lengths, letters (uint8), names)."""
+        cap = len(text) + 16
+        rec = np.zeros(cap, np.int32)
+        st = np.zeros(cap, np.int32)
+        ln = np.zeros(cap, np.int32)
+        lt = C.create_string_buffer(cap)
+        nm = C.create_string_buffer(cap)
+        P = C.POINTER
+        ip = lambda a: a.ctypes.data_as(P(C.c_int))
+        n = self.L.dmstref_read_fasta(text, len(text), ip(rec), ip(st), ip(ln), cap, lt, cap, nm, cap)
+        if n < 0:
+            raise ValueError("reference reader capacity")
+        tot = int(ln[:n].sum())
+        names = nm.raw.split(b"\0")[0].decode().split("\n")[:-1]
+        return rec[:n].copy(), st[:n].copy(), ln[:n].copy(), np.frombuffer(lt.raw[:tot], np.uint8).copy(), names
 
     def align(self, p: int, seqs, min_prob_ratio):
         """The reference's alignments (findSimilarities with needAlign) of up to

@@ -325,6 +325,59 @@ int dmstref_align(int p, const uint8_t *const *decoded, const int *lens, const f
     return ns;
 }
 
+// The reference's FASTA reader over a text: readContig (dummest-sequence.hh:6-82)
+// with the IUPAC character classes the engine builds for protein profiles
+// (dummest.cc:445-456), called in the engine's loop (dummest.cc:553-555).
+// Per contig: its record index, Contig::start and length; letters = the
+// contigs' codes concatenated; names = each record's name followed by '\n'.
+// Returns the number of contigs, or -(2 + needed) when a capacity is too
+// small.  The reader aborts on malformed input (dummest-util.hh:19-22): only
+// well-formed texts may be given.
+int dmstref_read_fasta(const char *text, long long len, int *record, int *start, int *length, int cap,
+                       char *letters, long long capLetters, char *names, long long capNames) {
+    ensureInit();
+    const char *alphabet = getAlphabet(20);
+    char charToNumber[256];
+    memset(charToNumber, 127, 256);
+    memset(charToNumber, 125, ' ' + 1);
+    charToNumber['>'] = 126;
+    setCharToNumber(charToNumber, alphabet);
+    char iupac[256];
+    std::copy(charToNumber, charToNumber + 256, iupac);
+    for (auto c : "RYSWKMBDHVN")
+        if (c != '\0') iupac[(unsigned char)c] = iupac[tolower(c)] = 22;
+    std::istringstream in(std::string(text, (size_t)len));
+    Sequence sequence{};
+    Contig contig{0, 0};
+    std::vector<char> vec;
+    std::vector<int> rec, st, ln;
+    std::string lt, nm;
+    size_t lastName = (size_t)-1;
+    int nrec = -1;
+    while (readContig(in, sequence, contig, vec, iupac)) {
+        if (sequence.nameIdx != lastName) {
+            lastName = sequence.nameIdx;
+            ++nrec;
+            nm += std::string(&vec[sequence.nameIdx]) + "\n";
+        }
+        if (contig.length == 0) continue;
+        rec.push_back(nrec);
+        st.push_back(contig.start);
+        ln.push_back(contig.length);
+        lt.append(&vec[vec.size() - contig.length], contig.length);
+    }
+    if ((int)rec.size() > cap || (long long)lt.size() > capLetters || (long long)nm.size() > capNames)
+        return -(2 + (int)std::max({rec.size(), lt.size(), nm.size()}));
+    for (size_t k = 0; k < rec.size(); ++k) {
+        record[k] = rec[k];
+        start[k] = st[k];
+        length[k] = ln[k];
+    }
+    std::memcpy(letters, lt.data(), lt.size());
+    std::memcpy(names, nm.data(), nm.size());
+    return (int)rec.size();
+}
+
 // The lean float filter (findSimilaritiesBackwardOnly) on n <= simdWidth lanes.
 int dmstref_backward_only(int p, const uint8_t *const *decoded, const int *lens, int n, float *best) {
     ensureInit();

@@ -1,0 +1,43 @@
+"""The FASTA input path on the device (dmst_seqs_add_fasta): each contig of 3
+or more letters becomes a sequence whose scores equal those of the same
+contig's letters decoded on the host (dmst_fasta_contigs + decodeSequence,
+pinned to the reference's reader in tests/test_fasta.py); shorter contigs are
+reported with seq_id -1 and not added."""
+import numpy as np
+import pytest
+
+import dummest_b200 as d
+from dummest_b200 import _ffi as F
+from dummest_b200 import synth
+from test_fasta import _text
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fasta_contigs_score_as_host_decoded():
+    rng = np.random.default_rng(9)
+    prof = synth.make_profile(rng, 60, "fa")
+    homolog = synth.sample_homolog(rng, prof, 60)
+    text = _text(rng, 20) + f">hit some words\n{homolog[:70]}\n{homolog[70:]}\n>short\nAC\n".encode()
+    host = d.fasta_contigs(text)
+    with d.Context(device=0) as ctx:
+        pid = ctx.load_hmm(synth.hmmer3_text([prof]))[0]
+        contigs = ctx.add_fasta(text)
+        assert [(c["record"], c["start"], c["length"], c["name"]) for c in contigs] == \
+            [(c["record"], c["start"], c["length"], c["name"]) for c in host]
+        keep = [k for k, c in enumerate(host) if c["length"] >= 3]
+        assert all(contigs[k]["seq_id"] >= 0 for k in keep)
+        assert all(c["seq_id"] == -1 for c in contigs if c["length"] < 3)
+        assert contigs[-1]["name"] == "short" and contigs[-1]["seq_id"] == -1
+        ids2 = ctx.add_decoded([d.decode_letters(host[k]["letters"].astype(np.int8)) for k in keep])
+        a = ctx.score_pairs([contigs[k]["seq_id"] for k in keep], pid, d.MODE_MID)
+        b = ctx.score_pairs(ids2, pid, d.MODE_MID)
+        assert [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in a] == \
+            [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in b]
+        assert max(x.mid_ln for x in a) / np.log(2) > 20  # the homolog contig is a hit
+        # too small a capacity: nothing added, the count returned
+        n = F.C.c_size_t(0)
+        before = ctx.lib.dmst_seq_count(ctx.h)
+        st = ctx.lib.dmst_seqs_add_fasta(ctx.h, text, len(text), None, 0, F.C.byref(n))
+        assert st == F.DMST_ERANGE and n.value == len(host)
+        assert ctx.lib.dmst_seq_count(ctx.h) == before
