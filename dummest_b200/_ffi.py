@@ -19,6 +19,7 @@ DMST_EDEVICE = -3
 DMST_ETIMEOUT = -4
 DMST_EPARSE = -5
 DMST_ERANGE = -6
+FASTA_REVCOMP = 1  # dmst_seqs_add_fasta: also the reverse complements
 
 MODE_MID = 0
 MODE_FILTER = 1
@@ -71,8 +72,10 @@ class Contig(C.Structure):
         ("seq_id", C.c_int32),
         ("name_off", C.c_int64),
         ("name_len", C.c_int32),
-        ("pad", C.c_int32),
+        ("seq_id_rc", C.c_int32),
         ("letter_off", C.c_int64),
+        ("record_length", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -156,7 +159,7 @@ SIGNATURES = [
      [C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
       C.POINTER(C.c_size_t)]),
     ("dmst_seqs_add_fasta", C.c_int,
-     [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
+     [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_align", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("dmst_align_fetch", C.c_int,

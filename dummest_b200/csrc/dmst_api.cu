@@ -783,8 +783,10 @@ static void fillContig(dmst_contig &o, const FastaContig &c, int seqId) {
     o.seq_id = seqId;
     o.name_off = (int64_t)c.nameOff;
     o.name_len = c.nameLen;
-    o.pad = 0;
+    o.seq_id_rc = -1;
     o.letter_off = (int64_t)c.letterOff;
+    o.record_length = c.recordLength;
+    o.pad = 0;
 }
 
 int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs, size_t *n_contigs,
@@ -802,36 +804,60 @@ int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_
     return DMST_OK;
 }
 
-int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs,
-                        size_t *n_contigs) {
-    if (!ctx || (!text && len) || !n_contigs) return DMST_EINVAL;
+int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, int flags, dmst_contig *contigs,
+                        size_t cap_contigs, size_t *n_contigs) {
+    if (!ctx || (!text && len) || !n_contigs || (flags & ~DMST_FASTA_REVCOMP)) return DMST_EINVAL;
     std::vector<FastaContig> cs;
     std::string lt, perr;
     if (fastaContigs(text, len, cs, lt, &perr)) return ctx->fail(DMST_EPARSE, "FASTA: %s", perr.c_str());
     *n_contigs = cs.size();
     if (cap_contigs < cs.size()) return ctx->fail(DMST_ERANGE, "FASTA: %zu contigs, capacity %zu", cs.size(), cap_contigs);
     if (cs.size() && !contigs) return DMST_EINVAL;
-    // Contigs of 3 or more letters as ASCII: A, C, G, T as they are, every
-    // other letter as 'N' (decodeSequence reads any non-ACGT letter alike).
-    std::string ascii;
+    const bool rc = (flags & DMST_FASTA_REVCOMP) != 0;
+    // The sequences in id order: per record its contigs of >= 3 letters, then
+    // (rc) their reverse complements, last contig first.  Each is packed 2
+    // bits per base (A 0, C 1, G 2, T 3; each sequence on a fresh word) with
+    // the other letters in the bitmap.
+    std::vector<uint32_t> words, mask;
     std::vector<int64_t> off(1, 0);
-    std::vector<int> which;
-    for (size_t k = 0; k < cs.size(); ++k) {
-        if (cs[k].length < 3) continue;
-        for (int q = 0; q < cs[k].length; ++q) {
-            const char v = lt[cs[k].letterOff + q];
-            ascii.push_back(v == 0 ? 'A' : v == 1 ? 'C' : v == 5 ? 'G' : v == 16 ? 'T' : 'N');
+    std::vector<std::pair<int, bool>> which;  // (contig, reverse complement)
+    auto base2 = [](char v) { return v == 0 ? 0 : v == 1 ? 1 : v == 5 ? 2 : v == 16 ? 3 : -1; };
+    auto pack = [&](size_t k, bool rev) {
+        const FastaContig &c = cs[k];
+        const size_t w0 = words.size(), m0 = mask.size();
+        words.resize(w0 + (c.length + 15) / 16, 0u);
+        mask.resize(m0 + (c.length + 31) / 32, 0u);
+        for (int q = 0; q < c.length; ++q) {
+            int b = base2(lt[c.letterOff + (rev ? c.length - 1 - q : q)]);
+            if (rev && b >= 0) b = 3 - b;  // A-T, C-G
+            if (b < 0)
+                mask[m0 + q / 32] |= 1u << (q % 32);
+            else
+                words[w0 + q / 16] |= (uint32_t)b << (2 * (q % 16));
         }
-        off.push_back((int64_t)ascii.size());
-        which.push_back((int)k);
+        off.push_back(off.back() + c.length);
+        which.emplace_back((int)k, rev);
+    };
+    for (size_t k0 = 0; k0 < cs.size();) {
+        size_t k1 = k0;
+        while (k1 < cs.size() && cs[k1].record == cs[k0].record) ++k1;
+        for (size_t k = k0; k < k1; ++k)
+            if (cs[k].length >= 3) pack(k, false);
+        if (rc)
+            for (size_t k = k1; k-- > k0;)
+                if (cs[k].length >= 3) pack(k, true);
+        k0 = k1;
     }
     int first = (int)ctx->seqLen.size();
     if (!which.empty()) {
-        const int st = dmst_seqs_add_dna(ctx, ascii.data(), off.data(), (int)which.size(), &first);
+        const int st = dmst_seqs_add_packed(ctx, words.data(), mask.data(), off.data(), (int)which.size(), &first);
         if (st) return st;
     }
     for (size_t k = 0; k < cs.size(); ++k) fillContig(contigs[k], cs[k], -1);
-    for (size_t q = 0; q < which.size(); ++q) contigs[which[q]].seq_id = first + (int)q;
+    for (size_t q = 0; q < which.size(); ++q) {
+        dmst_contig &o = contigs[which[q].first];
+        (which[q].second ? o.seq_id_rc : o.seq_id) = first + (int)q;
+    }
     return DMST_OK;
 }
 

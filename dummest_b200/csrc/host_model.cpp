@@ -383,6 +383,7 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
             return -1;
         }
         if (n == 0) {  // the record's end: the next character is '>' or the text ends
+            for (size_t k = out.size(); k-- > 0 && out[k].record == record;) out[k].recordLength = recLen;
             inRecord = false;
             continue;
         }
@@ -393,9 +394,12 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
         fc.nameOff = nameOff;
         fc.nameLen = nameLen;
         fc.letterOff = first;
+        fc.recordLength = 0;
         recLen += (int)n;
         out.push_back(fc);
     }
+    for (size_t k = out.size(); k-- > 0 && out[k].record == record && out[k].recordLength == 0;)
+        out[k].recordLength = recLen;  // a text ending inside its last record
     return 0;
 }
 

@@ -61,6 +61,7 @@ struct FastaContig {
     size_t nameOff;      // the record name: the first word of its header line, in the text
     int nameLen;
     size_t letterOff;    // its letter codes in the output string
+    int recordLength;    // its record's length (contigs and cutting characters)
 };
 int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
                  std::string *err);

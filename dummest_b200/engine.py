@@ -275,20 +275,22 @@ class Context:
             o += L
         return out, res
 
-    def add_fasta(self, text: str | bytes) -> list[dict]:
+    def add_fasta(self, text: str | bytes, revcomp: bool = False) -> list[dict]:
         """Contigs of a FASTA text added as sequences (dmst_seqs_add_fasta):
-        per contig {record, name, start, length, seq_id} (seq_id -1: shorter
-        than 3, not added)."""
+        per contig {record, name, start, length, record_length, seq_id,
+        seq_id_rc} (-1: shorter than 3, not added; seq_id_rc with revcomp)."""
         b = text.encode() if isinstance(text, str) else text
+        flags = F.FASTA_REVCOMP if revcomp else 0
         n = C.c_size_t(0)
-        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), None, 0, C.byref(n))
+        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), flags, None, 0, C.byref(n))
         if st != F.DMST_ERANGE and st != 0:
             self._check(st, "dmst_seqs_add_fasta")
         arr = (F.Contig * max(n.value, 1))()
-        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), arr, n.value, C.byref(n))
+        st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), flags, arr, n.value, C.byref(n))
         self._check(st, "dmst_seqs_add_fasta")
         return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
-                 "length": c.length, "seq_id": c.seq_id} for c in arr[:n.value]]
+                 "length": c.length, "record_length": c.record_length, "seq_id": c.seq_id,
+                 "seq_id_rc": c.seq_id_rc} for c in arr[:n.value]]
 
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
@@ -581,5 +583,6 @@ def fasta_contigs(text: str | bytes):
         raise ValueError(f"dmst_fasta_contigs: status {st}")
     letters = np.frombuffer(lt.raw[:nl.value], np.uint8).copy()
     return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
-             "length": c.length, "letters": letters[c.letter_off:c.letter_off + c.length]} for c in arr[:n.value]]
+             "length": c.length, "record_length": c.record_length,
+             "letters": letters[c.letter_off:c.letter_off + c.length]} for c in arr[:n.value]]
 

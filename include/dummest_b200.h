@@ -194,9 +194,18 @@ typedef struct dmst_contig {
     int32_t seq_id;      /* dmst_seqs_add_fasta: its sequence id (-1: shorter than 3, not added) */
     int64_t name_off;    /* the record's name in the text */
     int32_t name_len;
-    int32_t pad;
+    int32_t seq_id_rc;   /* dmst_seqs_add_fasta with DMST_FASTA_REVCOMP: its reverse complement's id */
     int64_t letter_off;  /* dmst_fasta_contigs: its letter codes in letters */
+    int32_t record_length; /* the record's length (its contigs and cutting characters) */
+    int32_t pad;
 } dmst_contig;
+
+/* dmst_seqs_add_fasta flags: also add each contig's reverse complement (A-T
+ * and C-G swapped, other letters kept, order reversed), as the pipeline's
+ * minus_strand_revcomp record of the same sequence (bin/dummest:236-264)
+ * cuts it; in that record the contig starts at record_length - start -
+ * length. */
+#define DMST_FASTA_REVCOMP 1
 
 /* The contigs of a FASTA text and their letter codes (the reader's
  * charToNumber values: A=0 C=1 G=5 T=16, IUPAC 22, other letters their
@@ -210,14 +219,17 @@ int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_
                        char *letters, size_t cap_letters, size_t *n_letters);
 /* Reads a FASTA text (dummest.cc:553-606's readContig loop) and adds each
  * contig of length >= 3 as one sequence, decoded as the engine decodes it
- * (decodeSequence: a triplet with any letter other than A, C, G, T is '?').
+ * (decodeSequence: a triplet with any letter other than A, C, G, T is '?'),
+ * uploaded 2-bit packed with a bitmap of the other letters.  Sequence ids
+ * follow the text: per record its contigs, then (DMST_FASTA_REVCOMP) the
+ * reverse complements in the minus record's order.
  * Masking (the reference's tantan pass, makeMaskedSequence) stays with the
  * caller: a base written as 'N' decodes as the reference's masked copy
  * does.  contigs (cap_contigs entries)
  * gets every contig with its sequence id; with too small a capacity nothing
  * is added and DMST_ERANGE is returned, *n_contigs holding the count. */
-int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs,
-                        size_t *n_contigs);
+int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, int flags, dmst_contig *contigs,
+                        size_t cap_contigs, size_t *n_contigs);
 /* Drop all sequences (device memory is kept for reuse). */
 int dmst_seqs_clear(dmst_ctx *ctx);
 int dmst_seq_count(const dmst_ctx *ctx);

@@ -62,3 +62,41 @@ def test_reader_failures_are_parse_errors():
         assert st == F.DMST_EPARSE, bad
     st = lib.dmst_fasta_contigs(b"", 0, None, 0, F.C.byref(n), None, 0, F.C.byref(nl))
     assert st == 0 and n.value == 0
+
+
+COMP = bytes.maketrans(b"ACGTacgt", b"TGCAtgca")  # the pipeline's complement (bin/dummest:494)
+
+
+def _minus_records(text):
+    """Each record's minus strand as the pipeline writes it: the sequence
+    without whitespace, complemented (ACGTacgt) and reversed."""
+    out = []
+    for rec in text.split(b">")[1:]:
+        head, _, body = rec.partition(b"\n")
+        seq = bytes(c for c in body if c > 32)
+        out.append(b">" + head.split()[0] + b"_rc\n" + seq.translate(COMP)[::-1] + b"\n")
+    return b"".join(out)
+
+
+@pytest.mark.parametrize("seed", [4, 5])
+def test_reverse_complement_contigs_equal_reference_reader_on_minus_records(ref32, seed):
+    """The reverse-complement contigs dmst_seqs_add_fasta adds (DMST_FASTA_REVCOMP):
+    letters complemented (A-T, C-G) and reversed, starting at record_length -
+    start - length, are the contigs the reference's reader cuts from the
+    pipeline's minus_strand_revcomp records."""
+    rng = np.random.default_rng(seed)
+    text = _text(rng, 20)
+    plus = d.fasta_contigs(text)
+    rec, st, ln, letters, _ = ref32.read_fasta(_minus_records(text))
+    want = {}
+    off = 0
+    for r, s0, n in zip(rec, st, ln):
+        want[(int(r), int(s0))] = letters[off:off + n]
+        off += n
+    comp = np.arange(256, dtype=np.uint8)
+    comp[0], comp[16], comp[1], comp[5] = 16, 0, 5, 1
+    assert len(want) == len(plus)
+    for c in plus:
+        key = (c["record"], c["record_length"] - c["start"] - c["length"])
+        assert key in want, key
+        assert np.array_equal(want[key], comp[c["letters"][::-1]])

@@ -1,8 +1,9 @@
 """The FASTA input path on the device (dmst_seqs_add_fasta): each contig of 3
 or more letters becomes a sequence whose scores equal those of the same
 contig's letters decoded on the host (dmst_fasta_contigs + decodeSequence,
-pinned to the reference's reader in tests/test_fasta.py); shorter contigs are
-reported with seq_id -1 and not added."""
+pinned to the reference's reader in tests/test_fasta.py), and so do the
+reverse complements of DMST_FASTA_REVCOMP; shorter contigs are reported with
+seq_id -1 and not added; sequence ids follow the text."""
 import numpy as np
 import pytest
 
@@ -22,7 +23,7 @@ def test_fasta_contigs_score_as_host_decoded():
     host = d.fasta_contigs(text)
     with d.Context(device=0) as ctx:
         pid = ctx.load_hmm(synth.hmmer3_text([prof]))[0]
-        contigs = ctx.add_fasta(text)
+        contigs = ctx.add_fasta(text, revcomp=True)
         assert [(c["record"], c["start"], c["length"], c["name"]) for c in contigs] == \
             [(c["record"], c["start"], c["length"], c["name"]) for c in host]
         keep = [k for k, c in enumerate(host) if c["length"] >= 3]
@@ -35,9 +36,23 @@ def test_fasta_contigs_score_as_host_decoded():
         assert [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in a] == \
             [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in b]
         assert max(x.mid_ln for x in a) / np.log(2) > 20  # the homolog contig is a hit
+        # the reverse complements (A-T, C-G swapped, reversed) score as host-decoded ones
+        comp = np.arange(256, dtype=np.uint8)
+        comp[0], comp[16], comp[1], comp[5] = 16, 0, 5, 1
+        ids3 = ctx.add_decoded([d.decode_letters(comp[host[k]["letters"][::-1]].astype(np.int8)) for k in keep])
+        a = ctx.score_pairs([contigs[k]["seq_id_rc"] for k in keep], pid, d.MODE_MID)
+        b = ctx.score_pairs(ids3, pid, d.MODE_MID)
+        assert [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in a] == \
+            [(x.mid.m, x.mid.e, x.filter.m, x.filter.e) for x in b]
+        # ids in text order: per record its contigs, then their reverse complements last first
+        ids = []
+        for r in sorted({c["record"] for c in contigs}):
+            cr = [c for c in contigs if c["record"] == r and c["seq_id"] >= 0]
+            ids += [c["seq_id"] for c in cr] + [c["seq_id_rc"] for c in cr[::-1]]
+        assert ids == list(range(ids[0], ids[0] + len(ids)))
         # too small a capacity: nothing added, the count returned
         n = F.C.c_size_t(0)
         before = ctx.lib.dmst_seq_count(ctx.h)
-        st = ctx.lib.dmst_seqs_add_fasta(ctx.h, text, len(text), None, 0, F.C.byref(n))
+        st = ctx.lib.dmst_seqs_add_fasta(ctx.h, text, len(text), 0, None, 0, F.C.byref(n))
         assert st == F.DMST_ERANGE and n.value == len(host)
         assert ctx.lib.dmst_seq_count(ctx.h) == before
