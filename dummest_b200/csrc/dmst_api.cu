@@ -1276,21 +1276,28 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         return st;
 
     // The exact path on the device: flagged pairs go to a queue that
-    // persistent CTAs of the exact kernel drain, each CTA with a scratch slot
-    // sized for the largest pair of the call.
+    // persistent CTAs of the exact kernel drain, each CTA (or, when no pair of
+    // the call has more than kPipeWarps / 2 stripes, each half of a CTA) with a
+    // scratch slot sized for the largest pair of the call.
     const bool exactOnDevice = mid && !nullOnly && !sequentialExact;
     long long poolSlot = 0;
-    int exactGrid = 0;
+    int exactGrid = 0, exactGroups = 1;
     if (exactOnDevice) {
+        int maxWarps = 1;
+        for (size_t k = 0; k < n; ++k) maxWarps = std::max(maxWarps, exactWarps(dp[k].M));
+        exactGroups = maxWarps <= kPipeWarps / 2 ? 2 : 1;
         for (size_t k = 0; k < n; ++k)
-            poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L, exactWarps(dp[k].M), anchors));
+            poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L,
+                                                           std::min(exactWarps(dp[k].M), kPipeWarps / exactGroups),
+                                                           anchors));
         poolSlot = (poolSlot + 63) / 64 * 64;
         size_t freeB = 0, totalB = 0;
         CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
         const size_t poolBudget = std::max<size_t>((freeB + ctx->dExactPool.cap * sizeof(float)) / 4, (size_t)256 << 20);
         exactGrid = (int)std::max<size_t>(
-            1, std::min<size_t>((size_t)ctx->smCount, poolBudget / ((size_t)poolSlot * sizeof(float))));
-        CK(ctx->dExactPool.ensure((size_t)exactGrid * poolSlot), "alloc exact scratch");
+            1, std::min<size_t>((size_t)ctx->smCount,
+                                poolBudget / ((size_t)poolSlot * exactGroups * sizeof(float))));
+        CK(ctx->dExactPool.ensure((size_t)exactGrid * exactGroups * poolSlot), "alloc exact scratch");
         CK(S.dExOut.ensure(n), "alloc exact out");
         CK(S.dQueue.ensure(n), "alloc exact queue");
         CK(S.dQueueCount.ensure(2), "alloc exact queue");
@@ -1303,6 +1310,15 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                                     (int)(kPipeWarps * sizeof(Window))),
                "smem attribute");
             CK(cudaFuncSetAttribute(exactWaveKernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
+            CK(cudaFuncSetAttribute(exactWaveKernel<false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
+            CK(cudaFuncSetAttribute(exactWaveKernel<true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kPipeWarps * sizeof(Window))),
+               "smem attribute");
+            CK(cudaFuncSetAttribute(exactWaveKernel<true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)(kPipeWarps * sizeof(Window))),
                "smem attribute");
             ctx->exactAttrSet = true;
@@ -1472,6 +1488,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                                       (uintptr_t)ctx->dChunks.p, (uintptr_t)w1Slot, (uintptr_t)ringSlot,
                                       (uintptr_t)n, (uintptr_t)exactOnDevice, (uintptr_t)forceExact,
                                       (uintptr_t)exactGrid, (uintptr_t)poolSlot, (uintptr_t)ctx->dExactPool.p,
+                                      (uintptr_t)exactGroups,
                                       (uintptr_t)S.dExOut.p, (uintptr_t)S.dQueue.p, (uintptr_t)S.dQueueCount.p,
                                       (uintptr_t)S.hOut.p, (uintptr_t)S.hExOut.p};
         for (const Group &G : groups) {
@@ -1526,7 +1543,10 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             CK(cudaEventRecord(S.evFork, ctx->stream), "event");
             CK(cudaStreamWaitEvent(ctx->stream2, S.evFork, 0), "stream dependency");
         }
-        auto ek = align ? exactWaveKernel<true, true> : (anchors ? exactWaveKernel<true> : exactWaveKernel<false>);
+        auto ek = exactGroups == 2
+                      ? (align ? exactWaveKernel<true, true, 2>
+                               : (anchors ? exactWaveKernel<true, false, 2> : exactWaveKernel<false, false, 2>))
+                      : (align ? exactWaveKernel<true, true> : (anchors ? exactWaveKernel<true> : exactWaveKernel<false>));
         ek<<<exactGrid, kPipeWarps * kLanes, kPipeWarps * sizeof(Window), tail>>>(
             S.dQueue.p, S.dQueueCount.p, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
             ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p,

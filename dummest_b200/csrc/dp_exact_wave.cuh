@@ -301,7 +301,12 @@ __global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int 
 // alignCells: W0 at [0, (M+1) L), W1 at [(M+1) L, 2 (M+1) L)) and the
 // reference's rescale counts (AlignJob::rowOff in alignRows: cntB at
 // [0, M+2), cntF at [M+2, 2 (M+2))).
-template <bool ANCH, bool ALIGN = false>
+// GROUPS = 2: the CTA's warps form two groups of kPipeWarps / 2 that run
+// pairs independently (each its own queue position, shared state, scratch
+// slot blockIdx.x * 2 + group and named barrier), a pair taking at most
+// kPipeWarps / 2 warps: for calls whose pairs have at most that many stripes,
+// twice the pairs per CTA, the same per-pair work.
+template <bool ANCH, bool ALIGN = false, int GROUPS = 1>
 __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
     exactWaveKernel(const int *queue, int *queueCount, const DevPair *pairs, const DevProfile *profiles,
                     const float *emit, const float *params, const uint8_t *codes, const float *seeds,
@@ -309,31 +314,46 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
                     const long long *anchorOff, float *anchorM, int *anchorE, int *anchorRow,
                     const int *jobOf = nullptr, const AlignJob *jobs = nullptr, float *alignCells = nullptr,
                     int *alignRows = nullptr) {
+    static_assert(GROUPS == 1 || GROUPS == 2, "one or two groups");
+    constexpr int GW = kPipeWarps / GROUPS;  // warps of a group
+    constexpr int GT = GW * kLanes;          // threads of a group
     extern __shared__ float4 smRaw[];
     Window *wins = reinterpret_cast<Window *>(smRaw);
-    __shared__ float smBg[32];
-    __shared__ int progress[kPipeWarps];
-    __shared__ int abortFlag;
-    __shared__ ExactBest bestF[kPipeWarps], bestM[kPipeWarps];
-    __shared__ int smNext;
+    __shared__ float smBgG[GROUPS][32];
+    __shared__ int progressG[GROUPS][GW];
+    __shared__ int abortG[GROUPS];
+    __shared__ ExactBest bestFG[GROUPS][GW], bestMG[GROUPS][GW];
+    __shared__ int smNextG[GROUPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = warp / GW, gw = warp % GW, gt = threadIdx.x % GT;
+    float *smBg = smBgG[group];
+    int *progress = progressG[group];
+    int &abortFlag = abortG[group];
+    ExactBest *bestF = bestFG[group], *bestM = bestMG[group];
+    int &smNext = smNextG[group];
+    auto gsync = [&]() {
+        if (GROUPS == 1)
+            __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + group), "r"(GT) : "memory");
+    };
     Window &win = wins[warp];
     PipeSync ps;
     ps.progress = progress;
     ps.abort = &abortFlag;
     for (;;) {
-        __syncthreads();  // the previous pair is done with the shared state
-        if (threadIdx.x == 0) smNext = atomicAdd(queueCount + 1, 1);
-        __syncthreads();
+        gsync();  // the previous pair is done with the shared state
+        if (gt == 0) smNext = atomicAdd(queueCount + 1, 1);
+        gsync();
         const int qi = smNext;
         if (qi >= queueCount[0]) break;
         const int pi = queue[qi];
         const DevPair p = pairs[pi];
         const DevProfile &pr = profiles[p.prof];
-        const int W = exactWarps(p.M);
+        const int W = min(exactWarps(p.M), GW);
         ps.W = W;
-        if (warp == 0) smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
-        if (threadIdx.x == 0) abortFlag = 0;
+        if (gw == 0) smBg[lane] = lane < kNumCodes ? pr.bg[lane] : 0.0f;
+        if (gt == 0) abortFlag = 0;
         if (lane == 0) {
             PairCold &c = win.cold;
             c.codes = codes + p.codeOff;
@@ -343,8 +363,8 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
             c.smBg = smBg;
             c.sc = scales[pi];
             c.M = p.M;
-            bestF[warp] = ExactBest{0.0, 0};
-            bestM[warp] = ExactBest{0.0, 0};
+            bestF[gw] = ExactBest{0.0, 0};
+            bestM[gw] = ExactBest{0.0, 0};
         }
         SweepArgs a;
         a.cold = &win.cold;
@@ -355,12 +375,12 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         const int Pw = wavePeriod(p.L);
         a.P = Pw + kPipeExtra;
         a.D = Pw + kLanes - 1;
-        a.sFirst = warp;
+        a.sFirst = gw;
         a.sStep = W;
-        a.nMine = warp < W ? (a.nS - warp + W - 1) / W : 0;
+        a.nMine = gw < W ? (a.nS - gw + W - 1) / W : 0;
         a.ringSlots = 2 * W;
         a.ringStride = 4LL * Pw;
-        float *base = pool + (size_t)blockIdx.x * slotFloats;
+        float *base = pool + (size_t)(blockIdx.x * GROUPS + group) * slotFloats;
         a.w1 = base;
         a.ring = base + (size_t)a.nS * a.D * kLanes * kExactR;
         ExactRows x;
@@ -381,23 +401,23 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         }
         // Four sweeps, each over every warp; the counts scan between them.
         for (int phase = 0; phase < 4; ++phase) {
-            if (lane == 0) progress[warp] = warp < W ? pipePos(a, -1) : INT_MAX;
-            __syncthreads();
+            if (lane == 0) progress[gw] = gw < W ? pipePos(a, -1) : INT_MAX;
+            gsync();
             a.alignOut = phase == 2 ? alignW1 : (phase == 3 ? alignW0 : nullptr);
-            if (warp < W && ok) {
+            if (gw < W && ok) {
                 switch (phase) {
-                case 0: ok = backwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
-                case 1: ok = forwardSweepPipe<kExactR, kDiscover>(a, win, warp, lane, ps, &x, nullptr); break;
-                case 2: ok = backwardSweepPipe<kExactR, kReplay>(a, win, warp, lane, ps, &x, &filt); break;
-                default: ok = forwardSweepPipe<kExactR, kReplay, ANCH>(a, win, warp, lane, ps, &x, &mid); break;
+                case 0: ok = backwardSweepPipe<kExactR, kDiscover>(a, win, gw, lane, ps, &x, nullptr); break;
+                case 1: ok = forwardSweepPipe<kExactR, kDiscover>(a, win, gw, lane, ps, &x, nullptr); break;
+                case 2: ok = backwardSweepPipe<kExactR, kReplay>(a, win, gw, lane, ps, &x, &filt); break;
+                default: ok = forwardSweepPipe<kExactR, kReplay, ANCH>(a, win, gw, lane, ps, &x, &mid); break;
                 }
             }
-            __syncthreads();
+            gsync();
             ok = ok && abortFlag == 0;
-            if (phase < 2 && threadIdx.x == 0 && ok) scanCounts(x.rowMax, x.rowCnt, phase == 0 ? x.cntB : x.cntF, p.M, phase == 0);
+            if (phase < 2 && gt == 0 && ok) scanCounts(x.rowMax, x.rowCnt, phase == 0 ? x.cntB : x.cntF, p.M, phase == 0);
         }
         if (ALIGN && ok && alignCnt != nullptr) {
-            for (int i = threadIdx.x; i < p.M + 2; i += blockDim.x) {
+            for (int i = gt; i < p.M + 2; i += GT) {
                 alignCnt[i] = x.cntB[i];
                 alignCnt[p.M + 2 + i] = x.cntF[i];
             }
@@ -405,7 +425,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         if (ANCH && ok && anchorOff[pi] >= 0) {
             // fold the stripes' partials of each column in row order
             const long long o = anchorOff[pi];
-            for (int j = threadIdx.x; j < p.L; j += blockDim.x) {
+            for (int j = gt; j < p.L; j += GT) {
                 float bm = 0.0f;
                 int be = 0, br = 0;
                 for (int s2 = 0; s2 < a.nS; ++s2) {
@@ -426,11 +446,11 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
         filt = warpBest(filt);
         mid = warpBest(mid);
         if (lane == 0) {
-            bestF[warp] = filt;
-            bestM[warp] = mid;
+            bestF[gw] = filt;
+            bestM[gw] = mid;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        gsync();
+        if (gt == 0) {
             ExactBest f{0.0, 0}, m{0.0, 0};
             for (int w = 0; w < W; ++w) {
                 const ExactBest bf = bestF[w], bm = bestM[w];

@@ -47,7 +47,12 @@ def golden_align(regression):
         miss, _ = ctx.align(sids, pids, 3.0e38)
         # the call again: the context's buffers are reused
         again, _ = ctx.align(sids[::-1], pids[::-1], [float(x) for x in g["pair_mpr"][::-1]])
-    return g, got, res, mids, rep, miss, again[::-1]
+        # the pairs of the profiles with at most 4 stripes (M <= 511) alone: the exact kernel then
+        # runs two pairs per CTA
+        small = [k for k in range(len(sids)) if g["pair_src"][k] == 1 and g["pair_prof"][k] <= 2]
+        got_small, _ = ctx.align([sids[k] for k in small], [pids[k] for k in small],
+                                 [float(g["pair_mpr"][k]) for k in small])
+    return g, got, res, mids, rep, miss, again[::-1], small, got_small
 
 
 def _pairs(sids, pids, mpr):
@@ -73,6 +78,13 @@ def test_alignments_equal_reference(golden_align):
     assert sum(1 for x in got for a in x if len(a[5])) >= 20  # real alignments, not only empty walks
 
 
+def test_alignments_of_small_profiles_alone_equal_reference(golden_align):
+    g, *_, small, got_small = golden_align
+    assert len(small) >= 20
+    for k, x in zip(small, got_small):
+        _assert_same(x, _golden_sims(g, k), k)
+
+
 def test_known_answers_on_overflow_records(golden_align):
     # test_overflow.sh:66-71: herpes anchor 981,5942, spans 1/1358 and 3003/4072;
     # medium anchor 531,2302, spans 428/504 and 1994/1510
@@ -85,7 +97,7 @@ def test_known_answers_on_overflow_records(golden_align):
 
 
 def test_scores_reports_misses_and_reuse(golden_align):
-    g, got, res, mids, rep, miss, again = golden_align
+    g, got, res, mids, rep, miss, again, *_ = golden_align
     for r, m in zip(res, mids):
         assert (r.mid.m, r.mid.e, r.filter.m, r.filter.e) == (m.mid.m, m.mid.e, m.filter.m, m.filter.e)
     assert all(len(x) == 0 for x in rep)
