@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--ag-m", type=int, default=400, help="autograd workload: profile length")
     ap.add_argument("--ag-lmin", type=int, default=600, help="autograd workload: shortest read")
     ap.add_argument("--ag-lmax", type=int, default=2400, help="autograd workload: longest read")
+    ap.add_argument("--ag-ckpt", choices=["on", "off", "auto"], default="on",
+                    help="autograd workload: the adjoint's column checkpointing (every 64 columns)")
     ap.add_argument("--no-autotune", action="store_true", help="skip the kernel-shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA-graph replay")
     ap.add_argument("--no-async", action="store_true", help="synchronous calls (no submit/complete overlap)")
@@ -156,7 +158,8 @@ def workload_config(args, world: int) -> dict:
         return {
             "workload": f"log-likelihood + gradient (adjoint, FP64): 1 profile M={args.ag_m} x {args.ag_reads} "
                         f"reads L uniform {args.ag_lmin}-{args.ag_lmax} nt, each carrying a frameshifted homolog, "
-                        "one SGD step of the emission/transition/frameshift logits per step",
+                        "one SGD step of the emission/transition/frameshift logits per step; column "
+                        f"checkpointing every 64 nt: {args.ag_ckpt}",
             "profiles": 1, "pairs_per_step": args.ag_reads, "l2": "inputs larger than L2 (forward store)",
             "parallelism": f"replicas x{world} (reads sharded per rank)",
         }
@@ -954,6 +957,8 @@ def run_autograd(args, rank, world, local):
     _, values, params, bg = d.finalize_hmm(txt)
     M = args.ag_m
     ctx = d.Context(device=local)
+    from dummest_b200 import _ffi as Fc
+    ctx.adjoint_checkpoint({"on": Fc.ADJ_CKPT_ON, "off": Fc.ADJ_CKPT_OFF, "auto": Fc.ADJ_CKPT_AUTO}[args.ag_ckpt])
     sids = ctx.add_dna(reads)
     cells = float(sum(len(r) for r in reads)) * (M + 1)
     slot = ag.ProfileSlot(ctx, values, params, bg, sids)

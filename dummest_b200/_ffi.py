@@ -20,6 +20,7 @@ DMST_ETIMEOUT = -4
 DMST_EPARSE = -5
 DMST_ERANGE = -6
 FASTA_REVCOMP = 1  # dmst_seqs_add_fasta: also the reverse complements
+ADJ_CKPT_AUTO, ADJ_CKPT_ON, ADJ_CKPT_OFF = 0, 1, 2  # dmst_adjoint_checkpoint
 
 MODE_MID = 0
 MODE_FILTER = 1
@@ -155,6 +156,7 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_float), C.c_int, C.POINTER(Result)]),
     ("dmst_anchors", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Score), C.POINTER(C.c_int), C.POINTER(Result)]),
+    ("dmst_adjoint_checkpoint", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("dmst_fasta_contigs", C.c_int,
      [C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
       C.POINTER(C.c_size_t)]),

@@ -346,6 +346,8 @@ struct dmst_ctx {
     DevBuf<float> dW1, dRing;
     DevBuf<ExactJob> dJobs;
     DevBuf<AdjointJob> dAdjJobs;             // dmst_loglik_grad, dmst_posteriors
+    int adjCheckpoint = DMST_ADJ_CKPT_AUTO;   // dmst_adjoint_checkpoint
+    bool lastAdjCheckpointed = false;
     DevBuf<double> dPost;                    // dmst_posteriors: the batch's posterior tables
     DevBuf<double> dAdjF, dAdjB, dGrad, dLogT;
     std::vector<int> lastOrder;              // sorted position -> caller's pair index of the last call
@@ -2319,24 +2321,36 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     }
     std::vector<AdjointJob> jobs(n);
     std::vector<long long> needF(n), needB(n), needP(n);
+    // Batches of pairs under the device budget.  The full forward store is
+    // 24 bytes per cell; the checkpointed one keeps the stripes' top rows and
+    // a checkpoint every kAdjCk columns (about 1/12 of it) and recomputes.
+    // Auto: the full store when every pair's fits the budget at once.
+    size_t freeB = 0, totalB = 0;
+    CK(cudaSetDevice(ctx->device), "set device");
+    CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+    const size_t held = (ctx->dAdjF.cap + ctx->dAdjB.cap + ctx->dPost.cap) * sizeof(double);
+    const size_t budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (freeB + held) / 2;
+    long long fullAll = 0;
+    for (size_t k = 0; k < n; ++k) {
+        const int L = ctx->seqLen[pairs[order[k]].seq];
+        fullAll += ((adjStoreDoubles(M, L) + 31) & ~31LL) + adjBoundDoubles(L) + (post ? 2LL * (M + 1) * L : 0);
+    }
+    const bool ckpt = ctx->adjCheckpoint == DMST_ADJ_CKPT_ON ||
+                      (ctx->adjCheckpoint == DMST_ADJ_CKPT_AUTO && (size_t)fullAll * 8 > budget);
+    ctx->lastAdjCheckpointed = ckpt;
     for (size_t k = 0; k < n; ++k) {
         const int L = ctx->seqLen[pairs[order[k]].seq];
         jobs[k] = AdjointJob{(int)k, 0, 0, 0, post ? 0 : -1};
-        needF[k] = (adjStoreDoubles(M, L) + 31) & ~31LL;  // 256-byte aligned stores (cp.async)
+        // 256-byte aligned stores (cp.async)
+        needF[k] = ((ckpt ? adjCkptDoubles(M, L) : adjStoreDoubles(M, L)) + 31) & ~31LL;
         needB[k] = adjBoundDoubles(L);
         needP[k] = post ? 2LL * (M + 1) * L : 0;
     }
     const size_t gN = (size_t)(M + 2) * kParamFloats + (size_t)(M + 1) * kNumCodes;
-    CK(cudaSetDevice(ctx->device), "set device");
     CK(ctx->dGrad.ensure(gN), "alloc gradient");
     CK(ctx->dLogT.ensure(n), "alloc log T");
     CK(ctx->dAdjJobs.ensure(n), "alloc adjoint jobs");
     CK(cudaMemsetAsync(ctx->dGrad.p, 0, gN * sizeof(double), ctx->stream), "zero gradient");
-    // Batches of pairs under the device budget (the forward store is 24
-    // bytes per cell, the posterior tables 16).
-    size_t freeB = 0, totalB = 0;
-    CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
-    const size_t budget = ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : freeB / 2;
     for (size_t k0 = 0; k0 < n;) {
         size_t k1 = k0;
         long long f = 0, b = 0, pp = 0;
@@ -2357,7 +2371,8 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
                            ctx->stream),
            "upload adjoint jobs");
         const int blocks = (nj + kAdjWarps - 1) / kAdjWarps;
-        auto kern = post ? adjointKernel<true> : adjointKernel<false>;
+        auto kern = ckpt ? (post ? adjointKernel<true, true> : adjointKernel<false, true>)
+                         : (post ? adjointKernel<true> : adjointKernel<false>);
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjSmem), "smem attribute");
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         kern<<<blocks, kAdjWarps * 32, kAdjSmem, ctx->stream>>>(
@@ -2391,6 +2406,15 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     if (grad_params) std::memcpy(grad_params, g.data(), (size_t)(M + 2) * kParamFloats * sizeof(double));
     if (grad_emit)
         std::memcpy(grad_emit, g.data() + (size_t)(M + 2) * kParamFloats, (size_t)(M + 1) * kNumCodes * sizeof(double));
+    return DMST_OK;
+}
+
+int dmst_adjoint_checkpoint(dmst_ctx *ctx, int mode, int *last_checkpointed) {
+    if (!ctx) return DMST_EINVAL;
+    if (last_checkpointed) *last_checkpointed = ctx->lastAdjCheckpointed ? 1 : 0;
+    if (mode < 0) return DMST_OK;  // query only
+    if (mode != DMST_ADJ_CKPT_AUTO && mode != DMST_ADJ_CKPT_ON && mode != DMST_ADJ_CKPT_OFF) return DMST_EINVAL;
+    ctx->adjCheckpoint = mode;
     return DMST_OK;
 }
 

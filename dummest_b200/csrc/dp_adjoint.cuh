@@ -72,6 +72,27 @@ __host__ __device__ __forceinline__ long long adjStoreDoubles(int M, int L) {
 __device__ __forceinline__ size_t adjF(int L, int s, int k, int lane) {
     return (((size_t)s * (L + 31) + k) * 32 + lane) * 3;
 }
+// Checkpointed store of a pair (CKPT): the forward pass keeps only what the
+// backward pass needs to recompute the forward blocks it reads, kAdjCk steps
+// at a time: each stripe's top row (W0, Y0 per column, which the next stripe
+// reads), the warp's state at every kAdjCk-th step of each stripe (per lane
+// its own row's W0 and Z0 at the three columns before, the row below's W0 at
+// the three columns before and the two values it publishes), the per-stripe
+// offsets, then the backward's two recompute buffers of kAdjCk forward blocks.
+constexpr int kAdjCk = 64;       // forward steps per checkpoint (64 columns)
+constexpr int kAdjCkVals = 11;   // doubles of a lane's state
+__host__ __device__ __forceinline__ int adjChunks(int L) { return (L + 31 + kAdjCk - 1) / kAdjCk; }
+__host__ __device__ __forceinline__ long long adjCkTopOff(int M, int L) { return 0; }
+__host__ __device__ __forceinline__ long long adjCkStateOff(int M, int L) { return (long long)adjStripes(M) * L * 2; }
+__host__ __device__ __forceinline__ long long adjCkOffsetsOff(int M, int L) {
+    return adjCkStateOff(M, L) + (long long)adjStripes(M) * adjChunks(L) * 32 * kAdjCkVals;
+}
+__host__ __device__ __forceinline__ long long adjCkBufOff(int M, int L) {
+    return adjCkOffsetsOff(M, L) + ((adjStripes(M) + 1) & ~1);
+}
+__host__ __device__ __forceinline__ long long adjCkptDoubles(int M, int L) {
+    return adjCkBufOff(M, L) + 2LL * kAdjCk * 96;
+}
 // Boundary rows of a pair: parity x (W1, Y) x (L + 4) columns.
 __host__ __device__ __forceinline__ long long adjBoundDoubles(int L) { return 2LL * 2 * (L + 4); }
 
@@ -128,11 +149,80 @@ __device__ __forceinline__ void adjWait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// The forward coefficients of a lane's row (row 32 s + lane) and its history
+// (own row at j-1, j-2, j-3; the row below at j-1, j-2, j-3; the values
+// published at the previous step).
+struct AdjRow {
+    double a0, a1, a2, b0, d0, eps, pEnter, pd1, pd2;
+    const float *Eprev;
+    bool rowOK;
+};
+struct AdjHist {
+    double w1, w2, w3, z1, z2, z3, u1, u2, u3, pubW, pubY;
+};
+__device__ __forceinline__ AdjRow adjRow(int s, int lane, int M, const float *par, const float *E, double sC,
+                                         double s1, double s2) {
+    AdjRow r;
+    const int i = 32 * s + lane;
+    r.rowOK = i <= M;
+    const int ir = r.rowOK ? i : M;
+    const float *q = par + (size_t)ir * kParamFloats;
+    const float *qp = par + (size_t)(ir > 0 ? ir - 1 : 0) * kParamFloats;
+    r.a0 = q[0];
+    r.a1 = (double)q[1] * s1;
+    r.a2 = (double)q[2] * s2;
+    r.b0 = q[3];
+    r.d0 = q[6];
+    r.eps = q[9];
+    r.pEnter = ir > 0 ? (double)qp[10] * sC : 0.0;
+    r.pd1 = ir > 0 ? (double)qp[7] * s2 : 0.0;
+    r.pd2 = ir > 0 ? (double)qp[8] * s1 : 0.0;
+    r.Eprev = E + (ir > 0 ? ir - 1 : 0);
+    return r;
+}
+// Forward step k of a stripe (lane l at column k - l): the row below comes
+// from lane l-1's previous step, or for lane 0 from (cW, cY), lane k mod 32
+// of which holds the row below the stripe at column k.  live: the cell is in
+// the matrix.
+__device__ __forceinline__ void adjFwdStep(const AdjRow &r, AdjHist &h, int k, int lane, int L, double cW, double cY,
+                                           const uint8_t *cd, const float *pre, const float *bg, int rowPad,
+                                           double sC, double seedScale, double &W0, double &Y0, double &Z0,
+                                           bool &live) {
+    const int j = k - lane;
+    double uj = __shfl_up_sync(0xffffffffu, h.pubW, 1);
+    double yPrev = __shfl_up_sync(0xffffffffu, h.pubY, 1);
+    const double bw = __shfl_sync(0xffffffffu, cW, k & 31);
+    const double by = __shfl_sync(0xffffffffu, cY, k & 31);
+    if (lane == 0) {
+        uj = bw;
+        yPrev = by;
+    }
+    W0 = Y0 = Z0 = 0.0;
+    live = r.rowOK && j >= 0 && j < L;
+    if (live) {
+        const int c = (j - 2 >= 0 && j - 2 < L) ? (int)cd[j - 2] : kPad;
+        const double win = fma(r.pEnter * (double)r.Eprev[(size_t)c * rowPad], h.u3,
+                               fma(r.pd1, h.u2, fma(r.pd2, h.u1, yPrev)));
+        Z0 = ((double)bg[c] * sC) * fma(r.a0, h.w3, r.b0 * h.z3);
+        W0 = fma(r.a1, h.w1, fma(r.a2, h.w2, fma((double)pre[j], seedScale, win + Z0)));
+        Y0 = fma(r.d0, W0, r.eps * yPrev);
+    }
+    h.w3 = h.w2; h.w2 = h.w1; h.w1 = W0;
+    h.z3 = h.z2; h.z2 = h.z1; h.z1 = Z0;
+    h.u3 = h.u2; h.u2 = h.u1; h.u1 = uj;
+    h.pubW = W0;
+    h.pubY = Y0;
+}
+
 // grad: (M+2) x 11 Params gradients then (M+1) x 25 emission gradients of
 // the profile, accumulated over the pairs (each term already divided by the
 // pair's T).  logT: per job, natural log.  post: posterior tables (POST).
 // The forward store must start 16-byte aligned (the host pads each pair's).
-template <bool POST>
+// CKPT: the checkpointed store (adjCkptDoubles per pair) instead of the full
+// one; the backward pass recomputes each kAdjCk-step chunk of forward blocks
+// from its checkpoint (the same step function, so the same values) into one
+// of two buffers before its look-ahead reads the chunk.
+template <bool POST, bool CKPT = false>
 __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
     const AdjointJob *jobs, int nJobs, const DevPair *pairs, const DevProfile *profiles, const float *emit,
     const float *params, const uint8_t *codes, const float *seeds, const PairScales *scales, double *fstore,
@@ -155,7 +245,11 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
     const PairScales sc = scales[job.pair];
     const double sC = sc.sC, s1 = sc.s1, s2 = sc.s2;
     double *F = fstore + job.fOff;
-    double *Foff = F + (size_t)nS * (L + 31) * 32 * 3;  // per-stripe offsets
+    double *Foff = CKPT ? F + adjCkOffsetsOff(M, L) : F + (size_t)nS * (L + 31) * 32 * 3;  // per-stripe offsets
+    double *Ftop = F + adjCkTopOff(M, L);      // CKPT: [stripe][column] x (W0, Y0)
+    double *Fck = F + adjCkStateOff(M, L);     // CKPT: [stripe][chunk][lane] x kAdjCkVals
+    double *Fbuf = F + adjCkBufOff(M, L);      // CKPT: [2][kAdjCk][96]
+    const int nCk = adjChunks(L);
     double *Bnd = bstore + job.bOff;
     double *cellP = POST ? post + job.pOff : nullptr;
     double *matchP = POST ? cellP + (size_t)(M + 1) * L : nullptr;
@@ -168,23 +262,12 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
     int te = 0, eS = 0;
     double lastMax = 0.0;  // lane 31: maximum of its row's W0 and Y0
     for (int s = 0; s < nS; ++s) {
-        const int i = 32 * s + lane;
-        const bool rowOK = i <= M;
         const int sh = s > 0 ? binExp(__shfl_sync(0xffffffffu, lastMax, 31)) : 0;
         eS += sh;
         const double f = ldexp(1.0, -sh), seedScale = ldexp(1.0, -eS);
         if (lane == 0) Foff[s] = (double)eS;
-        const int ir = rowOK ? i : M;
-        const float *q = par + (size_t)ir * kParamFloats;
-        const float *qp = par + (size_t)(ir > 0 ? ir - 1 : 0) * kParamFloats;
-        const double a0 = q[0], a1 = (double)q[1] * s1, a2 = (double)q[2] * s2, b0 = q[3];
-        const double d0 = q[6], eps = q[9];
-        const double pEnter = ir > 0 ? (double)qp[10] * sC : 0.0, pd1 = ir > 0 ? (double)qp[7] * s2 : 0.0;
-        const double pd2 = ir > 0 ? (double)qp[8] * s1 : 0.0;
-        const float *Eprev = E + (ir > 0 ? ir - 1 : 0);
-        double w1 = 0, w2 = 0, w3 = 0, z1 = 0, z2 = 0, z3 = 0;  // own row at j-1, j-2, j-3
-        double u1 = 0, u2 = 0, u3 = 0;                          // row i-1's W0 at j-1, j-2, j-3
-        double pubW = 0, pubY = 0;                              // published at the previous step
+        const AdjRow r = adjRow(s, lane, M, par, E, sC, s1, s2);
+        AdjHist h = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         double part = 0.0, rowMax = 0.0;
         // lane c holds column 32b + c of row 32s-1 for the current block b
         // (cW, cY) and the next one (nW, nY)
@@ -192,12 +275,18 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
             const int jc = 32 * b + lane;
             W = Y = 0.0;
             if (s > 0 && jc < L) {
-                const size_t a = adjF(L, s - 1, jc + 31, 31);
-                W = F[a] * f;
-                Y = F[a + 1] * f;
+                if (CKPT) {
+                    const double *a = Ftop + ((size_t)(s - 1) * L + jc) * 2;
+                    W = a[0] * f;
+                    Y = a[1] * f;
+                } else {
+                    const size_t a = adjF(L, s - 1, jc + 31, 31);
+                    W = F[a] * f;
+                    Y = F[a + 1] * f;
+                }
             }
         };
-        double cW, cY, nW, nY;
+        double cW = 0.0, cY = 0.0, nW, nY;
         fetch(0, nW, nY);
         for (int k = 0; k < nSteps; ++k) {
             const int j = k - lane;
@@ -206,36 +295,30 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
                 cY = nY;
                 fetch((k >> 5) + 1, nW, nY);
             }
-            // the row below: lane l-1's values of the previous step; lane 0
-            // takes row 32s-1 at column k
-            double uj = __shfl_up_sync(0xffffffffu, pubW, 1);
-            double yPrev = __shfl_up_sync(0xffffffffu, pubY, 1);
-            const double bw = __shfl_sync(0xffffffffu, cW, k & 31);
-            const double by = __shfl_sync(0xffffffffu, cY, k & 31);
-            if (lane == 0) {
-                uj = bw;
-                yPrev = by;
+            if (CKPT && k % kAdjCk == 0) {  // the state the recompute starts from
+                double *ck = Fck + (((size_t)s * nCk + k / kAdjCk) * 32 + lane) * kAdjCkVals;
+                ck[0] = h.w1; ck[1] = h.w2; ck[2] = h.w3; ck[3] = h.z1; ck[4] = h.z2; ck[5] = h.z3;
+                ck[6] = h.u1; ck[7] = h.u2; ck[8] = h.u3; ck[9] = h.pubW; ck[10] = h.pubY;
             }
-            double W0 = 0.0, Y0 = 0.0, Z0 = 0.0;
-            if (rowOK && j >= 0 && j < L) {
-                const int c = code(j - 2);
-                const double win = fma(pEnter * (double)Eprev[(size_t)c * rowPad], u3,
-                                       fma(pd1, u2, fma(pd2, u1, yPrev)));
-                Z0 = ((double)pr.bg[c] * sC) * fma(a0, w3, b0 * z3);
-                W0 = fma(a1, w1, fma(a2, w2, fma((double)pre[j], seedScale, win + Z0)));
-                Y0 = fma(d0, W0, eps * yPrev);
-                const size_t a = adjF(L, s, k, lane);
-                F[a] = W0;
-                F[a + 1] = Y0;
-                F[a + 2] = Z0;
+            double W0, Y0, Z0;
+            bool live;
+            adjFwdStep(r, h, k, lane, L, cW, cY, cd, pre, pr.bg, rowPad, sC, seedScale, W0, Y0, Z0, live);
+            if (live) {
+                if (CKPT) {
+                    if (lane == 31) {  // the top row, for the next stripe
+                        double *a = Ftop + ((size_t)s * L + j) * 2;
+                        a[0] = W0;
+                        a[1] = Y0;
+                    }
+                } else {
+                    const size_t a = adjF(L, s, k, lane);
+                    F[a] = W0;
+                    F[a + 1] = Y0;
+                    F[a + 2] = Z0;
+                }
                 part = fma(W0, (double)suf[j], part);
                 rowMax = fmax(rowMax, fmax(W0, Y0));
             }
-            w3 = w2; w2 = w1; w1 = W0;
-            z3 = z2; z2 = z1; z1 = Z0;
-            u3 = u2; u2 = u1; u1 = uj;
-            pubW = W0;
-            pubY = Y0;
         }
         dxAdd(tm, te, warpSumD(part), eS);
         lastMax = rowMax;
@@ -278,13 +361,58 @@ __global__ void __launch_bounds__(kAdjWarps * 32, 4) adjointKernel(
         // step t holds every lane's (W0, Y0, Z0) of that step, and (lane 0's
         // copy) the Y0 of row 32s-1 at forward step t + 31 of stripe s-1.
         const bool below = s > 0;
+        // CKPT: the forward blocks of chunk cc of this stripe, recomputed from
+        // its checkpoint into buffer cc & 1 (forward lane mapping: lane l is
+        // row 32 s + l), as the forward pass computed them.
+        int curChunk = -1;
+        auto recompute = [&](int cc) {
+            const AdjRow r = adjRow(s, lane, M, par, E, sC, s1, s2);
+            const double fF = s > 0 ? ldexp(1.0, -(eF - eFp)) : 1.0, seedF = ldexp(1.0, -eF);
+            const double *ck = Fck + (((size_t)s * nCk + cc) * 32 + lane) * kAdjCkVals;
+            AdjHist h = {ck[0], ck[1], ck[2], ck[3], ck[4], ck[5], ck[6], ck[7], ck[8], ck[9], ck[10]};
+            auto fetchTop = [&](int b, double &W, double &Y) {
+                const int jc = 32 * b + lane;
+                W = Y = 0.0;
+                if (s > 0 && jc < L) {
+                    const double *a = Ftop + ((size_t)(s - 1) * L + jc) * 2;
+                    W = a[0] * fF;
+                    Y = a[1] * fF;
+                }
+            };
+            const int k0 = cc * kAdjCk, k1 = min(k0 + kAdjCk, nSteps);
+            double *buf = Fbuf + (size_t)(cc & 1) * kAdjCk * 96;
+            double cW = 0.0, cY = 0.0, nW, nY;
+            fetchTop(k0 >> 5, nW, nY);
+            for (int k = k0; k < k1; ++k) {
+                if ((k & 31) == 0) {
+                    cW = nW;
+                    cY = nY;
+                    fetchTop((k >> 5) + 1, nW, nY);
+                }
+                double W0, Y0, Z0;
+                bool live;
+                adjFwdStep(r, h, k, lane, L, cW, cY, cd, pre, pr.bg, rowPad, sC, seedF, W0, Y0, Z0, live);
+                double *o = buf + (size_t)(k - k0) * 96 + 3 * lane;
+                o[0] = W0;
+                o[1] = Y0;
+                o[2] = Z0;
+            }
+            __threadfence_block();
+            __syncwarp();  // the buffer before the copies that read it
+        };
         auto issue = [&](int t) {
             if (t >= 0 && t <= L + 30) {
+                if (CKPT && t / kAdjCk != curChunk) {  // t descends: each chunk once, in order
+                    curChunk = t / kAdjCk;
+                    recompute(curChunk);
+                }
                 double *dst = ring + (t & (kAdjRing - 1)) * kAdjSlot;
-                const double *src = F + adjF(L, s, t, 0);
+                const double *src = CKPT ? Fbuf + ((size_t)((t / kAdjCk) & 1) * kAdjCk + t % kAdjCk) * 96
+                                         : F + adjF(L, s, t, 0);
                 adjCp16(dst + 2 * lane, src + 2 * lane);
                 if (lane < 16) adjCp16(dst + 64 + 2 * lane, src + 64 + 2 * lane);
-                if (lane == 16 && below && t + 31 <= L + 30) adjCp8(dst + 96, F + adjF(L, s - 1, t + 31, 31) + 1);
+                if (lane == 16 && below && t + 31 <= L + 30)
+                    adjCp8(dst + 96, CKPT ? Ftop + ((size_t)(s - 1) * L + t) * 2 + 1 : F + adjF(L, s - 1, t + 31, 31) + 1);
             }
             adjCommit();
         };

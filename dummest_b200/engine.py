@@ -403,6 +403,14 @@ class Context:
         self._check(self.lib.dmst_tuned_shape(self.h, M, C.byref(r), C.byref(w)), "dmst_tuned_shape")
         return r.value, w.value
 
+    def adjoint_checkpoint(self, mode: int | None = None) -> bool:
+        """Set the adjoint's column checkpointing (F.ADJ_CKPT_AUTO / _ON / _OFF;
+        None: leave it) and return whether the last adjoint call checkpointed."""
+        last = C.c_int(0)
+        st = self.lib.dmst_adjoint_checkpoint(self.h, -1 if mode is None else mode, C.byref(last))
+        self._check(st, "dmst_adjoint_checkpoint")
+        return bool(last.value)
+
     def last_align_timing(self) -> dict:
         """Wall-clock phases (ms) of the last align call (dmst_last_align_timing)."""
         v = (C.c_double * 8)()

@@ -368,6 +368,19 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
 /* The shape a call would use for a profile of length M. */
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta);
 
+/* Column checkpointing of the adjoint's forward pass (dmst_loglik_grad,
+ * dmst_posteriors): DMST_ADJ_CKPT_ON keeps the stripes' top rows and a
+ * checkpoint every 64 columns and recomputes the forward blocks in the
+ * backward pass (about 1/12 of the full store's 24 bytes per cell, one more
+ * forward pass of work); DMST_ADJ_CKPT_OFF keeps every cell's forward values;
+ * DMST_ADJ_CKPT_AUTO (the default) keeps them when every pair's full store
+ * fits the device budget at once.  The results are the same either way.
+ * mode < 0 only queries; last_checkpointed (may be NULL) gets whether the
+ * last adjoint call checkpointed.  No counterpart in the reference. */
+#define DMST_ADJ_CKPT_AUTO 0
+#define DMST_ADJ_CKPT_ON 1
+#define DMST_ADJ_CKPT_OFF 2
+int dmst_adjoint_checkpoint(dmst_ctx *ctx, int mode, int *last_checkpointed);
 /* ---- log-likelihood and its gradient --------------------------------------
  * For pairs of one profile: log_t[k] = log T of pair k, T the total weight of
  * all local alignments of the read under the profile, i.e. the sum over cells

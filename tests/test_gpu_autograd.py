@@ -137,3 +137,39 @@ def test_log_t_of_a_2242_bit_pair(regression):
     assert abs(logt[0] - want) <= 1e-10 * abs(want), (logt[0], want)
     assert np.all(np.isfinite(gp)) and np.all(np.isfinite(ge))
     assert np.abs(gp).max() > 0 and np.abs(ge).max() > 0
+
+
+@pytest.mark.parametrize("M", [30, 200])
+def test_checkpointed_adjoint_equals_full_store(M):
+    """Column checkpointing (a checkpoint every 64 columns, the forward blocks
+    recomputed in the backward pass) gives the full store's log T, gradient
+    and posterior tables bit for bit (the gradient to 1e-12: its sum over the
+    pairs is taken with atomic adds in no fixed order): reads of 3 nt to
+    several kb, lengths on and off the 64-column grid, homologs whose rows span
+    many binades."""
+    from dummest_b200 import _ffi as F
+    rng = np.random.default_rng(70 + M)
+    prof = synth.make_profile(rng, M, "ck")
+    txt = synth.hmmer3_text([prof])
+    reads = [synth.random_dna(rng, L) for L in (3, 31, 64, 65, 97, 128, 129)]
+    reads += [synth.sample_homolog(rng, prof, M) * 3, synth.random_dna(rng, 4000) + synth.sample_homolog(rng, prof, M)]
+    with d.Context(device=0) as ctx:
+        pid = ctx.load_hmm(txt)[0]
+        sids = ctx.add_dna(reads)
+        out = {}
+        for mode in (F.ADJ_CKPT_OFF, F.ADJ_CKPT_ON):
+            ctx.adjoint_checkpoint(mode)
+            g = ctx.loglik_grad(sids, pid)
+            assert ctx.adjoint_checkpoint() == (mode == F.ADJ_CKPT_ON)
+            p = ctx.posteriors(sids[:4] + sids[-2:], pid)
+            out[mode] = (g, p)
+        (lt0, gp0, ge0), (plt0, tabs0) = out[F.ADJ_CKPT_OFF]
+        (lt1, gp1, ge1), (plt1, tabs1) = out[F.ADJ_CKPT_ON]
+        assert np.array_equal(lt0, lt1)
+        # the gradient sums over pairs with atomic adds, whose order varies from run to run
+        for a, b in ((gp0, gp1), (ge0, ge1)):
+            np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+        assert np.array_equal(plt0, plt1)
+        for a, b in zip(tabs0, tabs1):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        assert min(lt0[7:]) > max(lt0[:7])  # the homolog reads score above the random ones
