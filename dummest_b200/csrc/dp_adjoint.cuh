@@ -223,7 +223,7 @@ __device__ __forceinline__ void adjFwdStep(const AdjRow &r, AdjHist &h, int k, i
 // from its checkpoint (the same step function, so the same values) into one
 // of two buffers before its look-ahead reads the chunk.
 template <bool POST, bool CKPT = false>
-__global__ void __launch_bounds__(kAdjWarps * 32, CKPT ? 3 : 4) adjointKernel(
+__global__ void __launch_bounds__(kAdjWarps * 32, 3) adjointKernel(
     const AdjointJob *jobs, int nJobs, const DevPair *pairs, const DevProfile *profiles, const float *emit,
     const float *params, const uint8_t *codes, const float *seeds, const PairScales *scales, double *fstore,
     double *bstore, double *grad, double *logT, double *post) {
