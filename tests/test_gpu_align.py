@@ -107,3 +107,37 @@ def test_scores_reports_misses_and_reuse(golden_align):
     assert any(len(x) for x in miss) and not all(len(x) for x in miss)
     for k in range(len(g["pair_len"])):
         _assert_same(again[k], got[k], k)
+
+
+def test_random_hits_equal_reference_engine(ref32, tmp_path):
+    """Seeded hits (four profiles M 25-520; full, partial, doubled and
+    frameshifted homologs, implanted and random reads; gates 0 to 2^40) in one
+    call against the reference engine's findSimilarities with needAlign run on
+    each pair (oracle/_ref): every alignment equal, in order."""
+    from dummest_b200 import synth
+    rng = np.random.default_rng(2026)
+    profs = [synth.make_profile(rng, M, f"rh{M}") for M in (25, 90, 260, 520)]
+    txt = synth.hmmer3_text(profs)
+    path = tmp_path / "rh.hmm"
+    path.write_text(txt)
+    assert ref32.load_profiles(str(path)) == len(profs)
+    reads, prof_of = [], []
+    for p, prof in enumerate(profs):
+        rs = [synth.sample_homolog(rng, prof, prof.M), synth.sample_homolog(rng, prof, prof.M // 3),
+              synth.sample_homolog(rng, prof, prof.M, fs_rate=0.03) + synth.random_dna(rng, 150)
+              + synth.sample_homolog(rng, prof, prof.M), synth.random_dna(rng, 700)]
+        rs += synth.make_reads(rng, 3, 200, 2000, [prof], 0.8)
+        reads += rs
+        prof_of += [p] * len(rs)
+    gates = [float(rng.choice([1.0, 2.0 ** 10, 2.0 ** 20, 2.0 ** 40])) for _ in reads]
+    codes = [d.decode_dna(r) for r in reads]
+    with d.Context(device=0) as ctx:
+        pids = ctx.load_hmm(txt)
+        sids = ctx.add_decoded(codes)
+        got, _ = ctx.align(sids, [pids[p] for p in prof_of], gates)
+    n_real = 0
+    for k, (c, p, gte) in enumerate(zip(codes, prof_of, gates)):
+        want = ref32.align(p, [c], [gte])[0]
+        _assert_same(got[k], want, k)
+        n_real += sum(1 for x in want if len(x[5]))
+    assert n_real >= 15
