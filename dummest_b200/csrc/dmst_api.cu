@@ -319,6 +319,9 @@ struct dmst_ctx {
     int maxSmemOptin = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;  // the exact path and result copies of scoring calls
+    PinnedBuf<char> hSeqStage[2];    // dmst_seqs_add_packed: host staging blocks, in turn
+    cudaEvent_t evSeqStage[2] = {};  // ... each block's copy done
+    int seqStageNext = 0;
     cudaEvent_t ev[6] = {};
     std::string err;
 
@@ -463,6 +466,7 @@ int dmst_ctx_create(const dmst_opts *opts, dmst_ctx **out) {
         return DMST_EDEVICE;
     }
     for (auto &e : ctx->ev) cudaEventCreate(&e);
+    for (auto &e : ctx->evSeqStage) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     for (auto &sl : ctx->slot) {
         for (auto &e : sl.ev) cudaEventCreate(&e);
         cudaEventCreateWithFlags(&sl.evFork, cudaEventDisableTiming);
@@ -517,6 +521,9 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
         if (sl.evFork) cudaEventDestroy(sl.evFork);
     }
     ctx->dExactPool.release();
+    for (auto &hb : ctx->hSeqStage) hb.release();
+    for (auto &e : ctx->evSeqStage)
+        if (e) cudaEventDestroy(e);
     ctx->dAlignJobs.release();
     ctx->dAlignJobOf.release();
     ctx->dAlignRows.release();
@@ -885,25 +892,34 @@ int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *m
         nw += (lens[i] + 15) / 16;
         nm += (lens[i] + 31) / 32;
     }
-    const size_t bytes = (size_t)nw * 4 + (mask_bits ? (size_t)nm * 4 : 0);
-    CK(ctx->dStage.ensure(bytes), "alloc staging");
-    CK(ctx->dStageOff.ensure(3 * (size_t)nseq), "alloc staging");
-    CK(ctx->dStageLen.ensure(nseq), "alloc staging");
-    uint32_t *dw = reinterpret_cast<uint32_t *>(ctx->dStage.p);
-    uint32_t *dm = mask_bits ? dw + nw : nullptr;
-    CK(cudaMemcpyAsync(dw, words, (size_t)nw * 4, cudaMemcpyHostToDevice, ctx->stream), "upload packed");
-    if (mask_bits) CK(cudaMemcpyAsync(dm, mask_bits, (size_t)nm * 4, cudaMemcpyHostToDevice, ctx->stream), "upload mask");
-    CK(cudaMemcpyAsync(ctx->dStageOff.p, wOff.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream), "upload offsets");
-    CK(cudaMemcpyAsync(ctx->dStageOff.p + nseq, mOff.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream),
-       "upload offsets");
-    CK(cudaMemcpyAsync(ctx->dStageOff.p + 2 * nseq, off.data(), nseq * 8, cudaMemcpyHostToDevice, ctx->stream),
-       "upload offsets");
-    CK(cudaMemcpyAsync(ctx->dStageLen.p, lens.data(), nseq * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
-       "upload lengths");
-    decodePackedKernel<<<nseq, 256, 0, ctx->stream>>>(dw, dm, ctx->dStageOff.p, ctx->dStageOff.p + nseq,
-                                                        ctx->dStageOff.p + 2 * nseq, ctx->dStageLen.p, ctx->dCodes.p);
+    // One pinned host block (words, mask words, the three offset arrays,
+    // lengths) per call, two of them in turn: the copy and the decode are
+    // queued on the context's stream without waiting, so a scoring call
+    // queued before keeps running while the host goes on (every later call on
+    // the stream finds the codes decoded).
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t bW = (size_t)nw * 4, bM = mask_bits ? (size_t)nm * 4 : 0, bO = (size_t)nseq * 8;
+    const size_t oM = up16(bW), oO = oM + up16(bM), oL = oO + up16(3 * bO), total = oL + (size_t)nseq * 4;
+    const int b = ctx->seqStageNext;
+    ctx->seqStageNext ^= 1;
+    CK(cudaEventSynchronize(ctx->evSeqStage[b]), "sequence staging");  // its previous copy is done
+    CK(ctx->hSeqStage[b].ensure(total), "alloc sequence staging");
+    char *h = ctx->hSeqStage[b].p;
+    std::memcpy(h, words, bW);
+    if (mask_bits) std::memcpy(h + oM, mask_bits, bM);
+    std::memcpy(h + oO, wOff.data(), bO);
+    std::memcpy(h + oO + bO, mOff.data(), bO);
+    std::memcpy(h + oO + 2 * bO, off.data(), bO);
+    std::memcpy(h + oL, lens.data(), (size_t)nseq * 4);
+    CK(ctx->dStage.ensure(total), "alloc staging");
+    char *dv = ctx->dStage.p;
+    CK(cudaMemcpyAsync(dv, h, total, cudaMemcpyHostToDevice, ctx->stream), "upload packed");
+    CK(cudaEventRecord(ctx->evSeqStage[b], ctx->stream), "event");
+    const long long *dOff = reinterpret_cast<const long long *>(dv + oO);
+    decodePackedKernel<<<nseq, 256, 0, ctx->stream>>>(
+        reinterpret_cast<const uint32_t *>(dv), mask_bits ? reinterpret_cast<const uint32_t *>(dv + oM) : nullptr,
+        dOff, dOff + nseq, dOff + 2 * nseq, reinterpret_cast<const int *>(dv + oL), ctx->dCodes.p);
     CK(cudaGetLastError(), "decode kernel");
-    CK(cudaStreamSynchronize(ctx->stream), "decode kernel");
     commitSeqs(ctx, off, lens, first_id);
     return DMST_OK;
 }

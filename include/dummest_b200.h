@@ -174,7 +174,11 @@ int dmst_profile_length(const dmst_ctx *ctx, int id);
  *             word k/32; NULL = none); decoded on the device.
  * offsets has nseq+1 entries (base offsets; packed: word offsets follow from
  * the base offsets rounded up to 16 per sequence).  Every sequence needs
- * L >= 3 (dummest-dp.hh:84).  first_id receives the id of the first one. */
+ * L >= 3 (dummest-dp.hh:84).  first_id receives the id of the first one.
+ * _packed copies its inputs into pinned staging and queues the upload and
+ * decode behind the context's pending calls without waiting for them: the
+ * caller's arrays may be reused at once, and every later call finds the
+ * sequences decoded. */
 int dmst_seqs_add_decoded(dmst_ctx *ctx, const uint8_t *codes, const int64_t *offsets, int nseq, int *first_id);
 int dmst_seqs_add_dna(dmst_ctx *ctx, const char *ascii, const int64_t *offsets, int nseq, int *first_id);
 int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *mask_bits, const int64_t *offsets,
