@@ -535,9 +535,9 @@ def run_align(args, rank, world, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
-            "gpu_launches": None, "alignments_per_step": n_al / args.steps, "segments_per_step": n_seg / args.steps,
+            "gpu_launches": int(phases.get("launches", 0)), "alignments_per_step": n_al / args.steps, "segments_per_step": n_seg / args.steps,
             "hit_cell_fraction": hit_cells / cells, "exact_ms_per_step": exact_ms / args.steps,
-            "phases_ms_per_step": {k: v / args.steps for k, v in phases.items()}}), flush=True)
+            "phases_ms_per_step": {k: v / args.steps for k, v in phases.items() if k != "launches"}}), flush=True)
     ctx.close()
 
 

@@ -374,7 +374,7 @@ struct dmst_ctx {
     DevBuf<Seg> dAlignSegOut;
     std::vector<dmst_alignment> alignOut;
     std::vector<dmst_segment> alignSegOut;
-    double alignMs[8] = {};  // dmst_last_align_timing
+    double alignMs[9] = {};  // dmst_last_align_timing
 
     double lastTotalMs = 0, lastDpMs = 0, lastNullMs = 0, lastExactMs = 0, lastHostMs = 0;
     double lastPostMs = 0, lastWallMs = 0;
@@ -1896,7 +1896,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
     };
     const auto tCall = Clock::now();
     double *tm = ctx->alignMs;
-    for (int q = 0; q < 8; ++q) tm[q] = 0.0;
+    for (int q = 0; q < 9; ++q) tm[q] = 0.0;
     ctx->nextSlot = ctx->oldest = 0;
     ctx->alignOut.clear();
     ctx->alignSegOut.clear();
@@ -1914,6 +1914,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
     }
     if ((st = completeCall(ctx))) return st;
     tm[1] = msSince(tCall);
+    tm[8] = ctx->lastLaunches;
 
     // hits: laneHit with a report (dummest-dp-forward.hh:262-274, :489-490);
     // the gate is normalizeScore((double)minProbRatio, 0)
@@ -2023,6 +2024,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         if ((st = completeCall(ctx))) return st;
         CK(cudaStreamSynchronize(ctx->stream), "traceback tables");
         tm[2] += msSince(tPhase);
+        tm[8] += ctx->lastLaunches + 7;  // the traceback call's, then sides, 4 flank, X and optimal kernels
         tPhase = Clock::now();
 
         // The reference's sort of each hit's anchors (std::ranges::sort with
@@ -2160,6 +2162,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
             CK(cudaStreamSynchronize(ctx->stream), "traceback segments");
         }
         tm[6] += msSince(tPhase);
+        tm[8] += 1 + (items.empty() ? 0 : 1);  // span and store passes
         b0 = b1;
     }
     *n_alignments = ctx->alignOut.size();
@@ -2170,7 +2173,7 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
 
 int dmst_last_align_timing(const dmst_ctx *ctx, double *out, int n) {
     if (!ctx || !out || n < 0) return DMST_EINVAL;
-    for (int i = 0; i < n && i < 8; ++i) out[i] = ctx->alignMs[i];
+    for (int i = 0; i < n && i < 9; ++i) out[i] = ctx->alignMs[i];
     return DMST_OK;
 }
 

@@ -413,11 +413,12 @@ class Context:
 
     def last_align_timing(self) -> dict:
         """Wall-clock phases (ms) of the last align call (dmst_last_align_timing)."""
-        v = (C.c_double * 8)()
-        self.lib.dmst_last_align_timing(self.h, v, 8)
+        v = (C.c_double * 9)()
+        self.lib.dmst_last_align_timing(self.h, v, 9)
         keys = ("wall_ms", "score_ms", "tables_ms", "sort_ms", "span_ms", "choice_ms", "store_ms")
         out = {k: v[i] for i, k in enumerate(keys)}
         out["hits"] = int(v[7])
+        out["launches"] = int(v[8])
         return out
 
     def last_timing(self) -> dict:

@@ -337,7 +337,8 @@ int dmst_align_fetch(const dmst_ctx *ctx, dmst_alignment *alignments, size_t cap
 /* Wall-clock phases of the last dmst_align call (ms): out[0] the whole call,
  * [1] scoring every pair, [2] the hits' exact replay and traceback tables,
  * [3] the anchor sort, [4] the walks' span pass, [5] the choice of anchors,
- * [6] the kept walks and the segment copy, [7] hits traced.  n <= 8. */
+ * [6] the kept walks and the segment copy, [7] hits traced, [8] kernel
+ * launches of the call.  n <= 9. */
 int dmst_last_align_timing(const dmst_ctx *ctx, double *out, int n);
 
 /* The filter gate as a float threshold: the smallest float best b whose
