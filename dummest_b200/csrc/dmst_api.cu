@@ -1295,15 +1295,21 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
 
     // The exact path on the device: flagged pairs go to a queue that
     // persistent CTAs of the exact kernel drain, each CTA (or, when no pair of
-    // the call has more than kPipeWarps / 2 stripes, each half of a CTA) with a
-    // scratch slot sized for the largest pair of the call.
+    // the call has more than kPipeWarps / 2 stripes and more pairs than SMs are
+    // expected, each half of a CTA) with a scratch slot sized for the largest
+    // pair of the call.
     const bool exactOnDevice = mid && !nullOnly && !sequentialExact;
     long long poolSlot = 0;
     int exactGrid = 0, exactGroups = 1;
     if (exactOnDevice) {
         int maxWarps = 1;
         for (size_t k = 0; k < n; ++k) maxWarps = std::max(maxWarps, exactWarps(dp[k].M));
-        exactGroups = maxWarps <= kPipeWarps / 2 ? 2 : 1;
+        // two groups pay only with more exact-path pairs than SMs (the
+        // grouped kernel holds more per thread; with fewer pairs, one pair per
+        // SM is faster): a forced call sends every pair, otherwise the last
+        // call's count stands in
+        const long long exactPairsExpected = forceExact ? (long long)n : (long long)ctx->lastFlagged;
+        exactGroups = maxWarps <= kPipeWarps / 2 && exactPairsExpected > ctx->smCount ? 2 : 1;
         for (size_t k = 0; k < n; ++k)
             poolSlot = std::max(poolSlot, exactWaveScratch(dp[k].M, dp[k].L,
                                                            std::min(exactWarps(dp[k].M), kPipeWarps / exactGroups),
@@ -1353,9 +1359,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         }
         std::vector<long long> off(n);
         for (size_t k = 0; k < n; ++k) off[k] = callerOff[order[k]];
-        CK(S.dAnchorM.ensure((size_t)anchorCols), "alloc anchors");
-        CK(S.dAnchorE.ensure((size_t)anchorCols), "alloc anchors");
-        CK(S.dAnchorRow.ensure((size_t)anchorCols), "alloc anchors");
+        CK(S.dAnchorM.ensure((size_t)anchorCols, 0.3), "alloc anchors");
+        CK(S.dAnchorE.ensure((size_t)anchorCols, 0.3), "alloc anchors");
+        CK(S.dAnchorRow.ensure((size_t)anchorCols, 0.3), "alloc anchors");
         CK(S.hAnchorM.ensure((size_t)anchorCols), "alloc anchors");
         CK(S.hAnchorE.ensure((size_t)anchorCols), "alloc anchors");
         CK(S.hAnchorRow.ensure((size_t)anchorCols), "alloc anchors");
@@ -1980,17 +1986,19 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
             maxL = std::max(maxL, jb.L);
             maxM = std::max(maxM, jb.M);
         }
-        CK(ctx->dAlignCells.ensure((size_t)cells * 2), "alloc traceback tables");
-        CK(ctx->dAlignX.ensure((size_t)cells), "alloc traceback tables");
-        CK(ctx->dAlignSuf.ensure((size_t)cells), "alloc traceback tables");
-        CK(ctx->dAlignRows.ensure((size_t)rowsN), "alloc traceback rows");
-        CK(ctx->dAlignColR.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignColF.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignWork.ensure((size_t)kFlankArrays * (cols + 4LL * nb)), "alloc traceback columns");
-        CK(ctx->dAlignRev.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignFwd.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignCand.ensure((size_t)cols), "alloc traceback columns");
-        CK(ctx->dAlignSpan.ensure((size_t)cols), "alloc traceback columns");
+        // headroom: calls whose hits differ a little reuse the buffers (a
+        // reallocation synchronises the device and costs a cudaMalloc of GBs)
+        CK(ctx->dAlignCells.ensure((size_t)cells * 2, 0.3), "alloc traceback tables");
+        CK(ctx->dAlignX.ensure((size_t)cells, 0.3), "alloc traceback tables");
+        CK(ctx->dAlignSuf.ensure((size_t)cells, 0.3), "alloc traceback tables");
+        CK(ctx->dAlignRows.ensure((size_t)rowsN, 0.3), "alloc traceback rows");
+        CK(ctx->dAlignColR.ensure((size_t)cols, 0.3), "alloc traceback columns");
+        CK(ctx->dAlignColF.ensure((size_t)cols, 0.3), "alloc traceback columns");
+        CK(ctx->dAlignWork.ensure((size_t)kFlankArrays * (cols + 4LL * nb), 0.3), "alloc traceback columns");
+        CK(ctx->dAlignRev.ensure((size_t)cols, 0.3), "alloc traceback columns");
+        CK(ctx->dAlignFwd.ensure((size_t)cols, 0.3), "alloc traceback columns");
+        CK(ctx->dAlignCand.ensure((size_t)cols, 0.3), "alloc traceback columns");
+        CK(ctx->dAlignSpan.ensure((size_t)cols, 0.3), "alloc traceback columns");
 
         // the exact path with the traceback stores, then the tables
         std::vector<dmst_score> best((size_t)cols);
@@ -2144,8 +2152,8 @@ int dmst_align(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, dmst_result *out
         tm[5] += msSince(tPhase);
         tPhase = Clock::now();
         if (!items.empty()) {
-            CK(ctx->dAlignItems.ensure(items.size()), "alloc traceback output");
-            CK(ctx->dAlignSegOut.ensure((size_t)ng), "alloc traceback output");
+            CK(ctx->dAlignItems.ensure(items.size(), 0.3), "alloc traceback output");
+            CK(ctx->dAlignSegOut.ensure((size_t)ng, 0.3), "alloc traceback output");
             CK(cudaMemcpyAsync(ctx->dAlignItems.p, items.data(), items.size() * sizeof(WalkItem),
                                cudaMemcpyHostToDevice, ctx->stream),
                "upload traceback walks");

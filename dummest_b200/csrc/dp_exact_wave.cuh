@@ -341,9 +341,18 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
     PipeSync ps;
     ps.progress = progress;
     ps.abort = &abortFlag;
+    // Queue positions: with two groups, group g of CTA b first takes position
+    // g * gridDim.x + b (so every CTA holds a pair before any holds two, which
+    // matters when there are fewer pairs than CTAs), then positions from
+    // 2 * gridDim.x on, dynamically.
+    bool first = true;
     for (;;) {
         gsync();  // the previous pair is done with the shared state
-        if (gt == 0) smNext = atomicAdd(queueCount + 1, 1);
+        if (gt == 0)
+            smNext = GROUPS == 1 ? atomicAdd(queueCount + 1, 1)
+                                 : (first ? group * (int)gridDim.x + (int)blockIdx.x
+                                          : 2 * (int)gridDim.x + atomicAdd(queueCount + 1, 1));
+        first = false;
         gsync();
         const int qi = smNext;
         if (qi >= queueCount[0]) break;

@@ -141,3 +141,25 @@ def test_random_hits_equal_reference_engine(ref32, tmp_path):
         _assert_same(got[k], want, k)
         n_real += sum(1 for x in want if len(x[5]))
     assert n_real >= 15
+
+
+def test_many_hits_equal_reference_engine(ref32, tmp_path):
+    """More hits than SMs on a short profile (two pairs per CTA in the exact
+    kernel): every alignment equal to the reference engine's."""
+    from dummest_b200 import synth
+    rng = np.random.default_rng(77)
+    prof = synth.make_profile(rng, 90, "many")
+    txt = synth.hmmer3_text([prof])
+    path = tmp_path / "many.hmm"
+    path.write_text(txt)
+    assert ref32.load_profiles(str(path)) == 1
+    reads = [synth.random_dna(rng, 80) + synth.sample_homolog(rng, prof, 90) + synth.random_dna(rng, 80)
+             for _ in range(160)]
+    codes = [d.decode_dna(r) for r in reads]
+    with d.Context(device=0) as ctx:
+        pid = ctx.load_hmm(txt)[0]
+        sids = ctx.add_decoded(codes)
+        got, _ = ctx.align(sids, pid, 2.0 ** 10)
+    assert sum(1 for x in got if x) > 148
+    for k, c in enumerate(codes):
+        _assert_same(got[k], ref32.align(0, [c], [2.0 ** 10])[0], k)

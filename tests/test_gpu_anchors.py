@@ -36,3 +36,26 @@ def test_anchors_equal_oracle(M):
         if nz.any():  # the best anchor is the mid score
             k = max(np.flatnonzero(nz), key=lambda j: (oe[j], om[j]))
             assert (om[k], oe[k]) == (sm.mid.m, sm.mid.e)
+
+
+def test_anchors_of_many_pairs_equal_oracle():
+    """More pairs than SMs on a short profile: the exact kernel then runs two
+    pairs per CTA (two 4-warp groups); anchors still equal the oracle's."""
+    rng = np.random.default_rng(404)
+    M = 60
+    prof = synth.make_profile(rng, M, "many")
+    txt = synth.hmmer3_text([prof])
+    _, values, params, bg = d.finalize_hmm(txt)
+    reads = [synth.sample_homolog(rng, prof, M) if k % 2 else synth.random_dna(rng, int(rng.integers(60, 500)))
+             for k in range(180)]
+    with d.Context(device=0) as ctx:
+        pid = ctx.load_hmm(txt)[0]
+        sids = ctx.add_dna(reads)
+        got, res = ctx.anchors(sids, pid)
+        mids = ctx.score_pairs(sids, pid, d.MODE_MID)
+    for r, (gm, ge, gr), rs, sm in zip(reads, got, res, mids):
+        om, oe, orow = port.anchors(values, params, bg, d.decode_dna(r))
+        assert np.array_equal(gm, om) and np.array_equal(ge, oe), len(r)
+        nz = om != 0
+        assert np.array_equal(gr[nz], orow[nz])
+        assert (rs.mid.m, rs.mid.e) == (sm.mid.m, sm.mid.e)
