@@ -83,18 +83,18 @@ __device__ __forceinline__ XS batchAdd(XS a, XS b) {
     return XS{__double2float_rn(s), e};
 }
 
-// addScores, the scalar form (dummest-score.hh:169-181).
+// addScores, the scalar form (dummest-score.hh:169-181).  ldexp(m, -d) for
+// 0 <= d <= 60 is the product of m and the power 2^-d built from its exponent
+// bits: both exact, so the same bits.
 __device__ __forceinline__ XS scalarAdd(XS a, XS b) {
     if (a.m == 0.0f) return b;
     if (b.m == 0.0f) return a;
-    if (a.e >= b.e) {
-        int d = a.e - b.e;
-        if (d > 60) return a;
-        return splitNorm(__dadd_rn((double)a.m, ldexp((double)b.m, -d)), a.e);
-    }
-    int d = b.e - a.e;
-    if (d > 60) return b;
-    return splitNorm(__dadd_rn((double)b.m, ldexp((double)a.m, -d)), b.e);
+    const bool agebe = a.e >= b.e;
+    const XS h = agebe ? a : b, l = agebe ? b : a;
+    const int d = h.e - l.e;
+    if (d > 60) return h;
+    const double inv = __longlong_as_double((long long)(1023 - d) << 52);
+    return splitNorm(__dadd_rn((double)h.m, __dmul_rn((double)l.m, inv)), h.e);
 }
 
 // batchMulScores with eFold = 0 (dummest-batch.hh:58-72).
