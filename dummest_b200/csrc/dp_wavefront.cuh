@@ -819,8 +819,11 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
                 // its mantissa rounded to float (dummest-batch.hh:216-235)
                 const double v = (double)W0 * (double)q[k];
                 if (rowBase + k <= a.M() && v > 0.0) {
-                    int ev;
-                    const double mv = frexp(v, &ev);
+                    // frexp of v from its bits: v, a product of two positive
+                    // normal floats, is a normal double
+                    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+                    const int ev = (int)((u >> 52) & 0x7FFULL) - 1022;
+                    const double mv = __longlong_as_double((long long)((u & 0xFFFFFFFFFFFFFULL) | (1022ULL << 52)));
                     const float cm = __double2float_rn(mv);
                     const int ce = ev + kRescaleBits * (f.cIn[k] + f.cB[k]);
                     if (xsLessMe(aM, aE, cm, ce)) {
