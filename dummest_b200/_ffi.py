@@ -20,6 +20,7 @@ DMST_ETIMEOUT = -4
 DMST_EPARSE = -5
 DMST_ERANGE = -6
 FASTA_REVCOMP = 1  # dmst_seqs_add_fasta: also the reverse complements
+FASTA_PIPELINE = 2  # the pipeline's headers
 ADJ_CKPT_AUTO, ADJ_CKPT_ON, ADJ_CKPT_OFF = 0, 1, 2  # dmst_adjoint_checkpoint
 
 MODE_MID = 0
@@ -76,6 +77,12 @@ class Contig(C.Structure):
         ("seq_id_rc", C.c_int32),
         ("letter_off", C.c_int64),
         ("record_length", C.c_int32),
+        ("pipeline", C.c_int32),
+        ("w_start", C.c_int64),
+        ("w_end", C.c_int64),
+        ("true_length", C.c_int64),
+        ("profile_off", C.c_int64),
+        ("profile_len", C.c_int32),
         ("pad", C.c_int32),
     ]
 
@@ -158,8 +165,8 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Score), C.POINTER(C.c_int), C.POINTER(Result)]),
     ("dmst_adjoint_checkpoint", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("dmst_fasta_contigs", C.c_int,
-     [C.c_char_p, C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p, C.c_size_t,
-      C.POINTER(C.c_size_t)]),
+     [C.c_char_p, C.c_size_t, C.c_int, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p,
+      C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_seqs_add_fasta", C.c_int,
      [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_align", C.c_int,

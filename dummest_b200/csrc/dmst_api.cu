@@ -795,15 +795,22 @@ static void fillContig(dmst_contig &o, const FastaContig &c, int seqId) {
     o.seq_id_rc = -1;
     o.letter_off = (int64_t)c.letterOff;
     o.record_length = c.recordLength;
+    o.pipeline = (c.hasPipeline ? 1 : 0) | (c.isPlus ? 2 : 0);
+    o.w_start = c.wStart;
+    o.w_end = c.wEnd;
+    o.true_length = c.trueLength;
+    o.profile_off = (int64_t)c.profileOff;
+    o.profile_len = c.profileLen;
     o.pad = 0;
 }
 
-int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs, size_t *n_contigs,
-                       char *letters, size_t cap_letters, size_t *n_letters) {
-    if ((!text && len) || !n_contigs || !n_letters) return DMST_EINVAL;
+int dmst_fasta_contigs(const char *text, size_t len, int flags, dmst_contig *contigs, size_t cap_contigs,
+                       size_t *n_contigs, char *letters, size_t cap_letters, size_t *n_letters) {
+    if ((!text && len) || !n_contigs || !n_letters || (flags & ~(DMST_FASTA_REVCOMP | DMST_FASTA_PIPELINE)))
+        return DMST_EINVAL;
     std::vector<FastaContig> cs;
     std::string lt;
-    if (fastaContigs(text, len, cs, lt, nullptr)) return DMST_EPARSE;
+    if (fastaContigs(text, len, cs, lt, nullptr, (flags & DMST_FASTA_PIPELINE) != 0)) return DMST_EPARSE;
     *n_contigs = cs.size();
     *n_letters = lt.size();
     if (cap_contigs < cs.size() || cap_letters < lt.size()) return DMST_ERANGE;
@@ -815,10 +822,12 @@ int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_
 
 int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, int flags, dmst_contig *contigs,
                         size_t cap_contigs, size_t *n_contigs) {
-    if (!ctx || (!text && len) || !n_contigs || (flags & ~DMST_FASTA_REVCOMP)) return DMST_EINVAL;
+    if (!ctx || (!text && len) || !n_contigs || (flags & ~(DMST_FASTA_REVCOMP | DMST_FASTA_PIPELINE)))
+        return DMST_EINVAL;
     std::vector<FastaContig> cs;
     std::string lt, perr;
-    if (fastaContigs(text, len, cs, lt, &perr)) return ctx->fail(DMST_EPARSE, "FASTA: %s", perr.c_str());
+    if (fastaContigs(text, len, cs, lt, &perr, (flags & DMST_FASTA_PIPELINE) != 0))
+        return ctx->fail(DMST_EPARSE, "FASTA: %s", perr.c_str());
     *n_contigs = cs.size();
     if (cap_contigs < cs.size()) return ctx->fail(DMST_ERANGE, "FASTA: %zu contigs, capacity %zu", cs.size(), cap_contigs);
     if (cs.size() && !contigs) return DMST_EINVAL;

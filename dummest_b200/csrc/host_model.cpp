@@ -10,6 +10,11 @@
 // so that the finalized profile is bit-identical to the reference's.
 #include "host_model.h"
 
+#include <cerrno>
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -329,8 +334,21 @@ static const unsigned char *fastaClasses() {
 // such character counts one position of the record, so a contig's start is
 // its position in the record), with characters up to ' ' skipped.
 // Empty contigs are not reported.
+// std::stoi / std::stoll on text[a, b): leading whitespace, a sign, digits;
+// false where they would throw (no digits, out of range).
+static bool parseInteger(const char *text, size_t a, size_t b, bool asInt, long long &v) {
+    std::string t(text + a, text + b);
+    errno = 0;
+    char *end = nullptr;
+    const long long x = std::strtoll(t.c_str(), &end, 10);
+    if (end == t.c_str() || errno == ERANGE) return false;
+    if (asInt && (x < INT32_MIN || x > INT32_MAX)) return false;
+    v = x;
+    return true;
+}
+
 int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
-                 std::string *err) {
+                 std::string *err, bool pipeline) {
     const unsigned char *cls = fastaClasses();
     size_t i = 0;
     int record = -1;
@@ -338,6 +356,12 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
     size_t nameOff = 0;
     int nameLen = 0;
     bool inRecord = false;
+    // the pipeline fields, kept from record to record as the reader's
+    // Sequence keeps them (dummest-sequence.hh:19-52)
+    bool hasPipeline = false, isPlus = false;
+    long long wStart = 0, wEnd = 0, trueLength = 0;
+    size_t profileOff = 0;
+    int profileLen = 0;
     while (i < len) {
         if (!inRecord) {
             while (i < len && isspace((unsigned char)text[i])) ++i;  // istream >> char
@@ -360,6 +384,57 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
             ++record;
             nameOff = w;
             nameLen = (int)(we - w);
+            size_t slash = w;
+            while (slash < we && text[slash] != '/') ++slash;
+            if (pipeline && slash < we) {  // "chr/start-end" then tokens
+                size_t dash = slash + 1;
+                while (dash < we && text[dash] != '-') ++dash;
+                if (dash < we) {
+                    if (!parseInteger(text, slash + 1, dash, true, wStart) ||
+                        !parseInteger(text, dash + 1, we, true, wEnd)) {
+                        if (err) *err = "bad window coordinates in a pipeline header";
+                        return -1;
+                    }
+                }
+                size_t lenA = 0, lenB = 0, profA = 0, profB = 0, strA = 0, strB = 0;
+                bool haveLength = false, haveProfile = false, haveStrand = false;
+                for (size_t t = we; t < lineEnd;) {
+                    while (t < lineEnd && isspace((unsigned char)text[t])) ++t;
+                    size_t te = t;
+                    while (te < lineEnd && !isspace((unsigned char)text[te])) ++te;
+                    if (te == t) break;
+                    auto starts = [&](const char *pfx) {
+                        const size_t n = strlen(pfx);
+                        return te - t >= n && std::memcmp(text + t, pfx, n) == 0;
+                    };
+                    if (starts("length=")) {
+                        lenA = t;
+                        lenB = te;
+                        haveLength = true;
+                    } else if (starts("profile=")) {
+                        profA = t;
+                        profB = te;
+                        haveProfile = true;
+                    } else if (starts("bitscore=")) {
+                    } else if (!haveStrand) {
+                        strA = t;
+                        strB = te;
+                        haveStrand = true;
+                    }
+                    t = te;
+                }
+                if (haveLength && haveProfile && haveStrand) {
+                    if (!parseInteger(text, lenA + 7, lenB, false, trueLength)) {
+                        if (err) *err = "bad length in a pipeline header";
+                        return -1;
+                    }
+                    profileOff = profA + 8;
+                    profileLen = (int)(profB - profA - 8);
+                    isPlus = std::string(text + strA, text + strB).find("plus_strand") != std::string::npos;
+                }
+                hasPipeline = true;
+                nameLen = (int)(slash - w);
+            }
             recLen = 0;
             i = lineEnd < len ? lineEnd + 1 : len;
             inRecord = true;
@@ -395,6 +470,13 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
         fc.nameLen = nameLen;
         fc.letterOff = first;
         fc.recordLength = 0;
+        fc.hasPipeline = hasPipeline;
+        fc.isPlus = isPlus;
+        fc.wStart = wStart;
+        fc.wEnd = wEnd;
+        fc.trueLength = trueLength;
+        fc.profileOff = profileOff;
+        fc.profileLen = profileLen;
         recLen += (int)n;
         out.push_back(fc);
     }

@@ -62,9 +62,15 @@ struct FastaContig {
     int nameLen;
     size_t letterOff;    // its letter codes in the output string
     int recordLength;    // its record's length (contigs and cutting characters)
+    // pipeline headers (the reader's PIPELINE_MODE): the fields as the reader
+    // holds them after its record's header
+    bool hasPipeline, isPlus;
+    long long wStart, wEnd, trueLength;
+    size_t profileOff;
+    int profileLen;
 };
 int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
-                 std::string *err);
+                 std::string *err, bool pipeline = false);
 int decodeLetters(const char *letters, int L, uint8_t *codes);
 int calibrationSequence(const float *letterFreqs, float bgStop, const Rates &r, int trial, int seqLen, int border,
                         char *out);

@@ -275,12 +275,13 @@ class Context:
             o += L
         return out, res
 
-    def add_fasta(self, text: str | bytes, revcomp: bool = False) -> list[dict]:
+    def add_fasta(self, text: str | bytes, revcomp: bool = False, pipeline: bool = False) -> list[dict]:
         """Contigs of a FASTA text added as sequences (dmst_seqs_add_fasta):
         per contig {record, name, start, length, record_length, seq_id,
-        seq_id_rc} (-1: shorter than 3, not added; seq_id_rc with revcomp)."""
+        seq_id_rc} (-1: shorter than 3, not added; seq_id_rc with revcomp)
+        and, with pipeline, the header fields as fasta_contigs gives them."""
         b = text.encode() if isinstance(text, str) else text
-        flags = F.FASTA_REVCOMP if revcomp else 0
+        flags = (F.FASTA_REVCOMP if revcomp else 0) | (F.FASTA_PIPELINE if pipeline else 0)
         n = C.c_size_t(0)
         st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), flags, None, 0, C.byref(n))
         if st != F.DMST_ERANGE and st != 0:
@@ -288,9 +289,12 @@ class Context:
         arr = (F.Contig * max(n.value, 1))()
         st = self.lib.dmst_seqs_add_fasta(self.h, b, len(b), flags, arr, n.value, C.byref(n))
         self._check(st, "dmst_seqs_add_fasta")
-        return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
-                 "length": c.length, "record_length": c.record_length, "seq_id": c.seq_id,
-                 "seq_id_rc": c.seq_id_rc} for c in arr[:n.value]]
+        out = []
+        for c in arr[:n.value]:
+            o = _contig(c, b, pipeline)
+            o.update(seq_id=c.seq_id, seq_id_rc=c.seq_id_rc)
+            out.append(o)
+        return out
 
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
@@ -576,22 +580,36 @@ def filter_threshold(lambda_filter: float, k_filter: float, total_length: float,
     return out.value
 
 
-def fasta_contigs(text: str | bytes):
+def fasta_contigs(text: str | bytes, pipeline: bool = False):
     """The reference reader's contigs of a FASTA text (dmst_fasta_contigs, no
-    GPU): per contig {record, name, start, length} and its letter codes."""
+    GPU): per contig {record, name, start, length, record_length, letters} and,
+    with pipeline, the header fields (has_fields, w_start, w_end, true_length,
+    plus, profile)."""
     lib = F.load()
     b = text.encode() if isinstance(text, str) else text
+    flags = F.FASTA_PIPELINE if pipeline else 0
     n, nl = C.c_size_t(0), C.c_size_t(0)
-    st = lib.dmst_fasta_contigs(b, len(b), None, 0, C.byref(n), None, 0, C.byref(nl))
+    st = lib.dmst_fasta_contigs(b, len(b), flags, None, 0, C.byref(n), None, 0, C.byref(nl))
     if st not in (0, F.DMST_ERANGE):
         raise ValueError(f"dmst_fasta_contigs: status {st}")
     arr = (F.Contig * max(n.value, 1))()
     lt = C.create_string_buffer(max(nl.value, 1))
-    st = lib.dmst_fasta_contigs(b, len(b), arr, n.value, C.byref(n), lt, nl.value, C.byref(nl))
+    st = lib.dmst_fasta_contigs(b, len(b), flags, arr, n.value, C.byref(n), lt, nl.value, C.byref(nl))
     if st != 0:
         raise ValueError(f"dmst_fasta_contigs: status {st}")
     letters = np.frombuffer(lt.raw[:nl.value], np.uint8).copy()
-    return [{"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
-             "length": c.length, "record_length": c.record_length,
-             "letters": letters[c.letter_off:c.letter_off + c.length]} for c in arr[:n.value]]
+    out = []
+    for c in arr[:n.value]:
+        o = _contig(c, b, pipeline)
+        o["letters"] = letters[c.letter_off:c.letter_off + c.length]
+        out.append(o)
+    return out
 
+
+def _contig(c, b: bytes, pipeline: bool) -> dict:
+    o = {"record": c.record, "name": b[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
+         "length": c.length, "record_length": c.record_length}
+    if pipeline:
+        o.update(has_fields=bool(c.pipeline & 1), plus=bool(c.pipeline & 2), w_start=c.w_start, w_end=c.w_end,
+                 true_length=c.true_length, profile=b[c.profile_off:c.profile_off + c.profile_len].decode())
+    return o

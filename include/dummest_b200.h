@@ -201,6 +201,11 @@ typedef struct dmst_contig {
     int32_t seq_id_rc;   /* dmst_seqs_add_fasta with DMST_FASTA_REVCOMP: its reverse complement's id */
     int64_t letter_off;  /* dmst_fasta_contigs: its letter codes in letters */
     int32_t record_length; /* the record's length (its contigs and cutting characters) */
+    int32_t pipeline;    /* DMST_FASTA_PIPELINE: bit 0 the header had pipeline fields, bit 1 plus strand */
+    int64_t w_start, w_end;  /* DMST_FASTA_PIPELINE: the window of the header's name "chr/start-end" */
+    int64_t true_length;     /* ... its "length=" field */
+    int64_t profile_off;     /* ... its "profile=" field in the text */
+    int32_t profile_len;
     int32_t pad;
 } dmst_contig;
 
@@ -210,6 +215,13 @@ typedef struct dmst_contig {
  * cuts it; in that record the contig starts at record_length - start -
  * length. */
 #define DMST_FASTA_REVCOMP 1
+/* dmst_fasta_contigs / dmst_seqs_add_fasta flags: read the pipeline's headers
+ * (">chr/start-end length=N profile=NAME plus_strand|minus_strand..." as
+ * bin/dummest writes them) as the reader of the reference's PIPELINE_MODE
+ * build does (dummest-sequence.hh:19-52): the name is the part before '/',
+ * and fields a header lacks keep the previous record's values, as the
+ * reader's reused Sequence keeps them (0 before any). */
+#define DMST_FASTA_PIPELINE 2
 
 /* The contigs of a FASTA text and their letter codes (the reader's
  * charToNumber values: A=0 C=1 G=5 T=16, IUPAC 22, other letters their
@@ -219,8 +231,8 @@ typedef struct dmst_contig {
  * is DMST_EPARSE, as the reader fails.  A '*' inside DNA (code 23) is read
  * as a letter, which the reference's decodeSequence does not accept (it
  * asserts codes <= 22); the library decodes it as any non-ACGT letter. */
-int dmst_fasta_contigs(const char *text, size_t len, dmst_contig *contigs, size_t cap_contigs, size_t *n_contigs,
-                       char *letters, size_t cap_letters, size_t *n_letters);
+int dmst_fasta_contigs(const char *text, size_t len, int flags, dmst_contig *contigs, size_t cap_contigs,
+                       size_t *n_contigs, char *letters, size_t cap_letters, size_t *n_letters);
 /* Reads a FASTA text (dummest.cc:553-606's readContig loop) and adds each
  * contig of length >= 3 as one sequence, decoded as the engine decodes it
  * (decodeSequence: a triplet with any letter other than A, C, G, T is '?'),

@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the reference engine built by
 oracle/Makefile (oracle/_ref/libdmst_ref32.so = FP32 engine "dummestl",
-oracle/_ref/libdmst_ref64.so = FP64 engine "dummest").  See ref_harness.cc
+oracle/_ref/libdmst_ref64.so = FP64 engine "dummest", oracle/_ref/libdmst_ref32p.so =
+the FP32 engine built with -DPIPELINE_MODE for its FASTA reader).  See ref_harness.cc
 for the reference functions each entry point calls.
 """
 from __future__ import annotations
@@ -15,6 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIBS = {32: os.path.join(REF_DIR, "libdmst_ref32.so"), 64: os.path.join(REF_DIR, "libdmst_ref64.so")}
 CLI = {32: os.path.join(REF_DIR, "dummestl_core"), 64: os.path.join(REF_DIR, "dummest_core")}
+
+PIPELINE_LIB = os.path.join(REF_DIR, "libdmst_ref32p.so")
 
 _libs: dict[int, C.CDLL] = {}
 
@@ -278,3 +281,31 @@ class RefEngine:
         if st != 0:
             raise ValueError("reference estimateK rejected the arguments")
         return np.array(out[:])
+
+
+def read_fasta_pipeline(text: bytes):
+    """The PIPELINE_MODE reference reader's contigs of a well-formed FASTA text
+    (dummest-sequence.hh:19-52): (records, starts, lengths, fields, names) with
+    fields an (n, 5) int64 array of (has_pipeline_fields, w_start, w_end,
+    true_length, is_plus) per contig and names a list of (name, profile) per
+    record."""
+    L = C.CDLL(PIPELINE_LIB)
+    P = C.POINTER
+    f = L.dmstref_read_fasta_pipeline
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.c_longlong, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_longlong), C.c_int,
+                  C.c_char_p, C.c_longlong]
+    cap = len(text) + 16
+    rec = np.zeros(cap, np.int32)
+    st = np.zeros(cap, np.int32)
+    ln = np.zeros(cap, np.int32)
+    fields = np.zeros((cap, 5), np.int64)
+    ncap = 2 * len(text) + 64
+    nm = C.create_string_buffer(ncap)
+    ip = lambda a: a.ctypes.data_as(P(C.c_int))
+    n = f(text, len(text), ip(rec), ip(st), ip(ln), fields.ctypes.data_as(P(C.c_longlong)), cap, nm, ncap)
+    if n < 0:
+        raise ValueError("reference reader capacity")
+    lines = nm.raw.split(b"\0")[0].decode().split("\n")[:-1]
+    names = [tuple(x.split("\t", 1)) for x in lines]
+    return rec[:n].copy(), st[:n].copy(), ln[:n].copy(), fields[:n].copy(), names

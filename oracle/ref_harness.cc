@@ -378,6 +378,57 @@ int dmstref_read_fasta(const char *text, long long len, int *record, int *start,
     return (int)rec.size();
 }
 
+#ifdef PIPELINE_MODE
+// The reader of the PIPELINE_MODE build (dummest-sequence.hh:19-52): per
+// contig also its record's header fields as the reader left them in
+// `sequence` (fields: has_pipeline_fields, w_start, w_end, true_length,
+// is_plus); names gets "name\tprofile\n" per record (name = the part before
+// '/').  Only well-formed texts (the reader throws or aborts otherwise).
+int dmstref_read_fasta_pipeline(const char *text, long long len, int *record, int *start, int *length,
+                                long long *fields, int cap, char *names, long long capNames) {
+    ensureInit();
+    const char *alphabet = getAlphabet(20);
+    char charToNumber[256];
+    memset(charToNumber, 127, 256);
+    memset(charToNumber, 125, ' ' + 1);
+    charToNumber['>'] = 126;
+    setCharToNumber(charToNumber, alphabet);
+    char iupac[256];
+    std::copy(charToNumber, charToNumber + 256, iupac);
+    for (auto c : "RYSWKMBDHVN")
+        if (c != '\0') iupac[(unsigned char)c] = iupac[tolower(c)] = 22;
+    std::istringstream in(std::string(text, (size_t)len));
+    Sequence sequence{};
+    Contig contig{0, 0};
+    std::vector<char> vec;
+    std::string nm;
+    size_t lastName = (size_t)-1;
+    int nrec = -1, n = 0;
+    while (readContig(in, sequence, contig, vec, iupac)) {
+        if (sequence.nameIdx != lastName) {
+            lastName = sequence.nameIdx;
+            ++nrec;
+            nm += std::string(&vec[sequence.nameIdx]) + "\t" + sequence.target_profile + "\n";
+        }
+        if (contig.length == 0) continue;
+        if (n >= cap) return -2;
+        record[n] = nrec;
+        start[n] = contig.start;
+        length[n] = contig.length;
+        long long *f = fields + 5 * n;
+        f[0] = sequence.has_pipeline_fields ? 1 : 0;
+        f[1] = (long long)sequence.w_start;
+        f[2] = (long long)sequence.w_end;
+        f[3] = (long long)sequence.true_length;
+        f[4] = sequence.is_plus ? 1 : 0;
+        ++n;
+    }
+    if ((long long)nm.size() > capNames) return -2;
+    std::memcpy(names, nm.data(), nm.size());
+    return n;
+}
+#endif
+
 // The lean float filter (findSimilaritiesBackwardOnly) on n <= simdWidth lanes.
 int dmstref_backward_only(int p, const uint8_t *const *decoded, const int *lens, int n, float *best) {
     ensureInit();

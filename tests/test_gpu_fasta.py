@@ -3,7 +3,8 @@ or more letters becomes a sequence whose scores equal those of the same
 contig's letters decoded on the host (dmst_fasta_contigs + decodeSequence,
 pinned to the reference's reader in tests/test_fasta.py), and so do the
 reverse complements of DMST_FASTA_REVCOMP; shorter contigs are reported with
-seq_id -1 and not added; sequence ids follow the text."""
+seq_id -1 and not added; sequence ids follow the text; the pipeline's header
+fields come back with the contigs (DMST_FASTA_PIPELINE)."""
 import numpy as np
 import pytest
 
@@ -56,3 +57,27 @@ def test_fasta_contigs_score_as_host_decoded():
         st = ctx.lib.dmst_seqs_add_fasta(ctx.h, text, len(text), 0, None, 0, F.C.byref(n))
         assert st == F.DMST_ERANGE and n.value == len(host)
         assert ctx.lib.dmst_seq_count(ctx.h) == before
+
+
+def test_pipeline_headers_added_with_their_fields():
+    """DMST_FASTA_PIPELINE on dmst_seqs_add_fasta: the contigs and header
+    fields are those of dmst_fasta_contigs with the flag (pinned to the
+    PIPELINE_MODE reader in tests/test_fasta.py); the sequences score as the
+    same text added without the flag."""
+    from test_fasta import _pipeline_text
+    rng = np.random.default_rng(10)
+    text = _pipeline_text(rng, 24)
+    host = d.fasta_contigs(text, pipeline=True)
+    prof = synth.make_profile(rng, 40, "pp")
+    with d.Context(device=0) as ctx:
+        pid = ctx.load_hmm(synth.hmmer3_text([prof]))[0]
+        got = ctx.add_fasta(text, pipeline=True)
+        plain = ctx.add_fasta(text)
+        keys = ("record", "start", "length", "name", "has_fields", "plus", "w_start", "w_end", "true_length",
+                "profile")
+        assert [tuple(c[k] for k in keys) for c in got] == [tuple(c[k] for k in keys) for c in host]
+        keep = [k for k, c in enumerate(got) if c["seq_id"] >= 0]
+        assert keep and all(plain[k]["seq_id"] >= 0 for k in keep)
+        a = ctx.score_pairs([got[k]["seq_id"] for k in keep], pid, d.MODE_MID)
+        b = ctx.score_pairs([plain[k]["seq_id"] for k in keep], pid, d.MODE_MID)
+        assert [(x.mid.m, x.mid.e) for x in a] == [(x.mid.m, x.mid.e) for x in b]
