@@ -28,6 +28,7 @@ from .engine import (  # noqa: F401
     encode_dna,
     estimate_gumbel,
     fasta_contigs,
+    windows_from_hits,
     filter_threshold,
     finalize_hmm,
     pack_dna,

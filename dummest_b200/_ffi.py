@@ -21,6 +21,7 @@ DMST_EPARSE = -5
 DMST_ERANGE = -6
 FASTA_REVCOMP = 1  # dmst_seqs_add_fasta: also the reverse complements
 FASTA_PIPELINE = 2  # the pipeline's headers
+HITS_TARGET_IS_CONTIG = 1  # dmst_windows_from_hits: targets are records, not six-frame translations
 ADJ_CKPT_AUTO, ADJ_CKPT_ON, ADJ_CKPT_OFF = 0, 1, 2  # dmst_adjoint_checkpoint
 
 MODE_MID = 0
@@ -64,6 +65,18 @@ class Opts(C.Structure):
 
 class Pair(C.Structure):
     _fields_ = [("seq", C.c_int32), ("profile", C.c_int32), ("min_prob_ratio", C.c_float)]
+
+
+class Window(C.Structure):
+    _fields_ = [
+        ("record", C.c_int32),
+        ("strand", C.c_int32),
+        ("start", C.c_int64),
+        ("end", C.c_int64),
+        ("profile_off", C.c_int64),
+        ("profile_len", C.c_int32),
+        ("profile", C.c_int32),
+    ]
 
 
 class Contig(C.Structure):
@@ -169,6 +182,14 @@ SIGNATURES = [
       C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_seqs_add_fasta", C.c_int,
      [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("dmst_windows_from_hits", C.c_int,
+     [C.c_char_p, C.c_size_t, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int64), C.c_int,
+      C.POINTER(C.c_char_p), C.POINTER(C.c_int64), C.c_int, C.POINTER(Window), C.c_size_t,
+      C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    ("dmst_genome_load", C.c_int,
+     [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int64), C.c_size_t]),
+    ("dmst_seqs_add_windows", C.c_int,
+     [C.c_void_p, C.POINTER(Window), C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
     ("dmst_align", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("dmst_align_fetch", C.c_int,

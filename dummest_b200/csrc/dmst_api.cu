@@ -89,6 +89,40 @@ __global__ void decodePackedKernel(const uint32_t *words, const uint32_t *mask, 
     }
 }
 
+// One contig of a window of the resident genome: the record's packed words
+// and mask words, the contig's first position in the record and its length;
+// rev: the sequence is the reverse complement (its base k is the complement of
+// the record's base pos + len - 1 - k).
+struct WinSeg {
+    long long wordOff, maskOff, outOff;
+    int pos, len, rev, pad;
+};
+
+// Windows of the resident genome -> codon codes, as decodePackedKernel decodes
+// the same letters uploaded packed (the last two codes 0).
+__global__ void windowDecodeKernel(const uint32_t *words, const uint32_t *mask, const WinSeg *segs, uint8_t *codes) {
+    const WinSeg sg = segs[blockIdx.x];
+    const uint32_t *w = words + sg.wordOff;
+    const uint32_t *mk = mask + sg.maskOff;
+    uint8_t *out = codes + sg.outOff;
+    for (int i = threadIdx.x; i < sg.len; i += blockDim.x) {
+        uint8_t c = 0;
+        if (i + 2 < sg.len) {
+            int b[3];
+            bool masked = false;
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const int p = sg.rev ? sg.pos + sg.len - 1 - (i + t) : sg.pos + i + t;
+                const int bb = (int)((__ldg(w + (p >> 4)) >> (2 * (p & 15))) & 3u);
+                if ((__ldg(mk + (p >> 5)) >> (p & 31)) & 1u) masked = true;
+                b[t] = sg.rev ? 3 - bb : bb;  // A-T, C-G
+            }
+            c = masked ? (uint8_t)kMaskCode : cCodonTable[16 * b[0] + 4 * b[1] + b[2]];
+        }
+        out[i] = c;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Small device buffer helper
 // ---------------------------------------------------------------------------
@@ -338,6 +372,19 @@ struct dmst_ctx {
     DevBuf<char> dStage;
     DevBuf<long long> dStageOff;
     DevBuf<int> dStageLen;
+
+    // the genome of dmst_genome_load: per record its name in the text, its
+    // length, its packed words and mask words, and its contigs (start, length)
+    struct GenomeRecord {
+        size_t nameOff;
+        int nameLen;
+        int length;
+        long long wordOff, maskOff;
+        std::vector<std::pair<int, int>> contigs;
+    };
+    std::vector<GenomeRecord> genome;
+    DevBuf<uint32_t> dGenomeWords, dGenomeMask;
+    DevBuf<WinSeg> dWinSegs;
 
     // per call (shared by the slots: used only by a call's stream-ordered kernels)
     DevBuf<XS> dNullTmp;
@@ -930,6 +977,188 @@ int dmst_seqs_add_packed(dmst_ctx *ctx, const uint32_t *words, const uint32_t *m
         dOff, dOff + nseq, dOff + 2 * nseq, reinterpret_cast<const int *>(dv + oL), ctx->dCodes.p);
     CK(cudaGetLastError(), "decode kernel");
     commitSeqs(ctx, off, lens, first_id);
+    return DMST_OK;
+}
+
+int dmst_windows_from_hits(const char *hits, size_t len, int flags, const char *const *record_names,
+                           const int64_t *record_lengths, int n_records, const char *const *profile_names,
+                           const int64_t *profile_lengths, int n_profiles, dmst_window *windows, size_t cap,
+                           size_t *n_windows, size_t *n_malformed, size_t *n_dropped) {
+    if ((!hits && len) || !n_windows || n_records < 0 || n_profiles < 0 || (n_records && (!record_names ||
+        !record_lengths)) || (n_profiles && (!profile_names || !profile_lengths)) ||
+        (flags & ~DMST_HITS_TARGET_IS_CONTIG))
+        return DMST_EINVAL;
+    std::vector<std::string> rn(n_records), pn(n_profiles);
+    std::vector<long long> rl(n_records), pl(n_profiles);
+    for (int k = 0; k < n_records; ++k) {
+        if (!record_names[k]) return DMST_EINVAL;
+        rn[k] = record_names[k];
+        rl[k] = record_lengths[k];
+    }
+    for (int k = 0; k < n_profiles; ++k) {
+        if (!profile_names[k]) return DMST_EINVAL;
+        pn[k] = profile_names[k];
+        pl[k] = profile_lengths[k];
+    }
+    std::vector<HitWindow> ws;
+    size_t malformed = 0, dropped = 0;
+    if (windowsFromHits(hits, len, (flags & DMST_HITS_TARGET_IS_CONTIG) != 0, rn, rl, pn, pl, ws, malformed, dropped,
+                        nullptr))
+        return DMST_EPARSE;
+    *n_windows = ws.size();
+    if (n_malformed) *n_malformed = malformed;
+    if (n_dropped) *n_dropped = dropped;
+    if (cap < ws.size()) return DMST_ERANGE;
+    if (ws.size() && !windows) return DMST_EINVAL;
+    for (size_t k = 0; k < ws.size(); ++k) {
+        dmst_window &o = windows[k];
+        o.record = ws[k].record;
+        o.strand = ws[k].strand;
+        o.start = ws[k].start;
+        o.end = ws[k].end;
+        o.profile_off = (int64_t)ws[k].profileOff;
+        o.profile_len = ws[k].profileLen;
+        o.profile = ws[k].profile;
+    }
+    return DMST_OK;
+}
+
+int dmst_genome_load(dmst_ctx *ctx, const char *text, size_t len, size_t *n_records, int64_t *record_lengths,
+                     size_t cap_records) {
+    if (!ctx || (!text && len) || !n_records) return DMST_EINVAL;
+    std::vector<FastaContig> cs;
+    std::vector<FastaRecord> recs;
+    std::string lt, perr;
+    if (fastaContigs(text, len, cs, lt, &perr, false, &recs)) return ctx->fail(DMST_EPARSE, "FASTA: %s", perr.c_str());
+    *n_records = recs.size();
+    if (record_lengths)
+        for (size_t k = 0; k < recs.size() && k < cap_records; ++k) record_lengths[k] = recs[k].length;
+    // every position of a record (its contigs' letters and its cutting
+    // characters) 2 bits, each record on fresh words; the positions that are
+    // not A, C, G or T (cutting characters included) set in the bitmap
+    std::vector<dmst_ctx::GenomeRecord> g(recs.size());
+    long long nw = 0, nm = 0;
+    for (size_t r = 0; r < recs.size(); ++r) {
+        g[r].nameOff = recs[r].nameOff;
+        g[r].nameLen = recs[r].nameLen;
+        g[r].length = recs[r].length;
+        g[r].wordOff = nw;
+        g[r].maskOff = nm;
+        nw += (recs[r].length + 15) / 16;
+        nm += (recs[r].length + 31) / 32;
+    }
+    std::vector<uint32_t> words((size_t)std::max(nw, 1LL), 0u), mask((size_t)std::max(nm, 1LL), ~0u);
+    for (const FastaContig &c : cs) {
+        dmst_ctx::GenomeRecord &gr = g[c.record];
+        gr.contigs.emplace_back(c.start, c.length);
+        for (int q = 0; q < c.length; ++q) {
+            const int p = c.start + q;
+            const char v = lt[c.letterOff + q];
+            const int b = v == 0 ? 0 : v == 1 ? 1 : v == 5 ? 2 : v == 16 ? 3 : -1;
+            if (b < 0) continue;
+            words[gr.wordOff + p / 16] |= (uint32_t)b << (2 * (p % 16));
+            mask[gr.maskOff + p / 32] &= ~(1u << (p % 32));
+        }
+    }
+    CK(cudaSetDevice(ctx->device), "set device");
+    CK(ctx->dGenomeWords.ensure(words.size()), "alloc genome");
+    CK(ctx->dGenomeMask.ensure(mask.size()), "alloc genome");
+    CK(cudaMemcpyAsync(ctx->dGenomeWords.p, words.data(), words.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+       "upload genome");
+    CK(cudaMemcpyAsync(ctx->dGenomeMask.p, mask.data(), mask.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+       "upload genome");
+    CK(cudaStreamSynchronize(ctx->stream), "upload genome");
+    ctx->genome = std::move(g);
+    return DMST_OK;
+}
+
+int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, dmst_contig *contigs,
+                          size_t cap_contigs, size_t *n_contigs) {
+    if (!ctx || (!windows && n) || !n_contigs) return DMST_EINVAL;
+    for (size_t k = 0; k < n; ++k) {
+        const dmst_window &w = windows[k];
+        if (w.record < 0 || w.record >= (int)ctx->genome.size() || (w.strand != 1 && w.strand != -1) ||
+            w.start < 0 || w.start > w.end || w.end > ctx->genome[w.record].length || w.profile_len < 0)
+            return ctx->fail(DMST_EINVAL, "window %zu outside its record (or no genome loaded)", k);
+    }
+    // per window the record's contigs it overlaps, in the window's text order
+    struct Piece {
+        int window, start, length;  // start in the window
+        int pos;                    // its first position in the record
+    };
+    std::vector<Piece> pieces;
+    for (size_t k = 0; k < n; ++k) {
+        const dmst_window &w = windows[k];
+        const auto &cl = ctx->genome[w.record].contigs;
+        auto it = std::upper_bound(cl.begin(), cl.end(), w.start,
+                                   [](long long s, const std::pair<int, int> &c) { return s < (long long)c.first + c.second; });
+        const size_t first = pieces.size();
+        for (; it != cl.end() && it->first < w.end; ++it) {
+            const long long a = std::max<long long>(w.start, it->first);
+            const long long b = std::min<long long>(w.end, (long long)it->first + it->second);
+            if (b <= a) continue;
+            const long long st = w.strand > 0 ? a - w.start : w.end - b;
+            pieces.push_back({(int)k, (int)st, (int)(b - a), (int)a});
+        }
+        if (w.strand < 0) std::reverse(pieces.begin() + first, pieces.end());
+    }
+    *n_contigs = pieces.size();
+    if (cap_contigs < pieces.size())
+        return ctx->fail(DMST_ERANGE, "windows: %zu contigs, capacity %zu", pieces.size(), cap_contigs);
+    if (pieces.size() && !contigs) return DMST_EINVAL;
+    std::vector<int64_t> off(1, 0);
+    std::vector<size_t> which;
+    for (size_t q = 0; q < pieces.size(); ++q)
+        if (pieces[q].length >= 3) {
+            off.push_back(off.back() + pieces[q].length);
+            which.push_back(q);
+        }
+    int first = (int)ctx->seqLen.size();
+    if (!which.empty()) {
+        CK(cudaSetDevice(ctx->device), "set device");
+        std::vector<long long> sOff;
+        std::vector<int> lens;
+        int st = reserveSeqs(ctx, off.data(), (int)which.size(), sOff, lens);
+        if (st) return st;
+        std::vector<WinSeg> segs(which.size());
+        for (size_t i = 0; i < which.size(); ++i) {
+            const Piece &pc = pieces[which[i]];
+            const dmst_window &w = windows[pc.window];
+            const dmst_ctx::GenomeRecord &gr = ctx->genome[w.record];
+            segs[i] = {gr.wordOff, gr.maskOff, sOff[i], pc.pos, pc.length, w.strand < 0 ? 1 : 0, 0};
+        }
+        CK(ctx->dWinSegs.ensure(segs.size(), 0.3), "alloc window segments");
+        CK(cudaMemcpyAsync(ctx->dWinSegs.p, segs.data(), segs.size() * sizeof(WinSeg), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload window segments");
+        windowDecodeKernel<<<(unsigned)segs.size(), 256, 0, ctx->stream>>>(ctx->dGenomeWords.p, ctx->dGenomeMask.p,
+                                                                          ctx->dWinSegs.p, ctx->dCodes.p);
+        CK(cudaGetLastError(), "window decode kernel");
+        commitSeqs(ctx, sOff, lens, &first);
+    }
+    size_t next = 0;
+    for (size_t q = 0; q < pieces.size(); ++q) {
+        const Piece &pc = pieces[q];
+        const dmst_window &w = windows[pc.window];
+        const dmst_ctx::GenomeRecord &gr = ctx->genome[w.record];
+        dmst_contig &o = contigs[q];
+        o.record = pc.window;
+        o.start = pc.start;
+        o.length = pc.length;
+        o.seq_id = pc.length >= 3 ? first + (int)next++ : -1;
+        o.name_off = (int64_t)gr.nameOff;
+        o.name_len = gr.nameLen;
+        o.seq_id_rc = -1;
+        o.letter_off = -1;
+        o.record_length = (int32_t)(w.end - w.start);
+        o.pipeline = 1 | (w.strand > 0 ? 2 : 0);
+        o.w_start = w.start + 1;
+        o.w_end = w.end;
+        o.true_length = gr.length;
+        o.profile_off = w.profile_off;
+        o.profile_len = w.profile_len;
+        o.pad = 0;
+    }
     return DMST_OK;
 }
 

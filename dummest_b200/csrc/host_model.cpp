@@ -348,7 +348,7 @@ static bool parseInteger(const char *text, size_t a, size_t b, bool asInt, long 
 }
 
 int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
-                 std::string *err, bool pipeline) {
+                 std::string *err, bool pipeline, std::vector<FastaRecord> *records) {
     const unsigned char *cls = fastaClasses();
     size_t i = 0;
     int record = -1;
@@ -436,6 +436,7 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
                 nameLen = (int)(slash - w);
             }
             recLen = 0;
+            if (records) records->push_back({nameOff, nameLen, 0});
             i = lineEnd < len ? lineEnd + 1 : len;
             inRecord = true;
         }
@@ -459,6 +460,7 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
         }
         if (n == 0) {  // the record's end: the next character is '>' or the text ends
             for (size_t k = out.size(); k-- > 0 && out[k].record == record;) out[k].recordLength = recLen;
+            if (records) records->back().length = recLen;
             inRecord = false;
             continue;
         }
@@ -482,6 +484,7 @@ int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, st
     }
     for (size_t k = out.size(); k-- > 0 && out[k].record == record && out[k].recordLength == 0;)
         out[k].recordLength = recLen;  // a text ending inside its last record
+    if (records && inRecord) records->back().length = recLen;
     return 0;
 }
 

@@ -69,8 +69,29 @@ struct FastaContig {
     size_t profileOff;
     int profileLen;
 };
+// One record of a FASTA text: its name and length (contigs and cutting characters).
+struct FastaRecord {
+    size_t nameOff;
+    int nameLen;
+    int length;
+};
 int fastaContigs(const char *text, size_t len, std::vector<FastaContig> &out, std::string &letters,
-                 std::string *err, bool pipeline = false);
+                 std::string *err, bool pipeline = false, std::vector<FastaRecord> *records = nullptr);
+
+// One window of the pipeline's prefilter hits: a merged interval of one
+// (target record, profile, strand), as bedtools getfasta -s cuts it.
+struct HitWindow {
+    int record;          // index among the record names
+    int strand;          // +1, or -1: reverse-complemented
+    long long start, end;
+    size_t profileOff;   // the profile name in the hits text
+    int profileLen;
+    int profile;         // index among the profile names, -1 when not among them
+};
+int windowsFromHits(const char *tab, size_t len, bool targetIsContig, const std::vector<std::string> &recordNames,
+                    const std::vector<long long> &recordLengths, const std::vector<std::string> &profileNames,
+                    const std::vector<long long> &profileLengths, std::vector<HitWindow> &out, size_t &malformed,
+                    size_t &dropped, std::string *err);
 int decodeLetters(const char *letters, int L, uint8_t *codes);
 int calibrationSequence(const float *letterFreqs, float bgStop, const Rates &r, int trial, int seqLen, int border,
                         char *out);

@@ -296,6 +296,42 @@ class Context:
             out.append(o)
         return out
 
+    def genome_load(self, text: str | bytes) -> np.ndarray:
+        """Keep a genome's records on the device for add_windows
+        (dmst_genome_load); returns the records' lengths.  The text object is
+        kept with the context: the windows' contigs name records by offset."""
+        b = text.encode() if isinstance(text, str) else text
+        n = C.c_size_t(0)
+        self._check(self.lib.dmst_genome_load(self.h, b, len(b), C.byref(n), None, 0), "dmst_genome_load")
+        lens = np.zeros(max(n.value, 1), np.int64)
+        self._check(self.lib.dmst_genome_load(self.h, b, len(b), C.byref(n),
+                                              lens.ctypes.data_as(C.POINTER(C.c_int64)), n.value),
+                    "dmst_genome_load")
+        self._genome_text = b
+        return lens[:n.value]
+
+    def add_windows(self, windows, hits: bytes | None = None) -> list[dict]:
+        """The windows (a ctypes Window array, as windows_from_hits gives)
+        of the loaded genome added as sequences (dmst_seqs_add_windows): per
+        contig the dict add_fasta(pipeline=True) gives for the pipeline's
+        windowed FASTA (profile decoded from hits when given)."""
+        n = C.c_size_t(0)
+        st = self.lib.dmst_seqs_add_windows(self.h, windows, len(windows), None, 0, C.byref(n))
+        if st != F.DMST_ERANGE and st != 0:
+            self._check(st, "dmst_seqs_add_windows")
+        arr = (F.Contig * max(n.value, 1))()
+        self._check(self.lib.dmst_seqs_add_windows(self.h, windows, len(windows), arr, n.value, C.byref(n)),
+                    "dmst_seqs_add_windows")
+        g = self._genome_text
+        out = []
+        for c in arr[:n.value]:
+            out.append({"record": c.record, "name": g[c.name_off:c.name_off + c.name_len].decode(), "start": c.start,
+                        "length": c.length, "record_length": c.record_length, "seq_id": c.seq_id,
+                        "seq_id_rc": c.seq_id_rc, "has_fields": bool(c.pipeline & 1), "plus": bool(c.pipeline & 2),
+                        "w_start": c.w_start, "w_end": c.w_end, "true_length": c.true_length,
+                        "profile": hits[c.profile_off:c.profile_off + c.profile_len].decode() if hits else None})
+        return out
+
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
         (alignments, segments): a ctypes Alignment array and an (n, 3) int32
@@ -604,6 +640,31 @@ def fasta_contigs(text: str | bytes, pipeline: bool = False):
         o["letters"] = letters[c.letter_off:c.letter_off + c.length]
         out.append(o)
     return out
+
+
+def windows_from_hits(hits: str | bytes, record_names, record_lengths, profile_names=(), profile_lengths=(),
+                      target_is_contig: bool = False):
+    """The windows of BLAST-tab hit rows (dmst_windows_from_hits, no GPU):
+    (a ctypes Window array, rows malformed, windows dropped)."""
+    lib = F.load()
+    b = hits.encode() if isinstance(hits, str) else hits
+    enc = lambda xs: [x.encode() if isinstance(x, str) else bytes(x) for x in xs]
+    rn, pn = enc(record_names), enc(profile_names)
+    rna = (C.c_char_p * max(len(rn), 1))(*rn)
+    pna = (C.c_char_p * max(len(pn), 1))(*pn)
+    rla = (C.c_int64 * max(len(rn), 1))(*[int(x) for x in record_lengths])
+    pla = (C.c_int64 * max(len(pn), 1))(*[int(x) for x in profile_lengths])
+    flags = F.HITS_TARGET_IS_CONTIG if target_is_contig else 0
+    n, nm, nd = C.c_size_t(0), C.c_size_t(0), C.c_size_t(0)
+    args = (b, len(b), flags, rna, rla, len(rn), pna, pla, len(pn))
+    st = lib.dmst_windows_from_hits(*args, None, 0, C.byref(n), C.byref(nm), C.byref(nd))
+    if st not in (0, F.DMST_ERANGE):
+        raise ValueError(f"dmst_windows_from_hits: status {st}")
+    arr = (F.Window * n.value)()
+    st = lib.dmst_windows_from_hits(*args, arr, n.value, C.byref(n), C.byref(nm), C.byref(nd))
+    if st != 0:
+        raise ValueError(f"dmst_windows_from_hits: status {st}")
+    return arr, nm.value, nd.value
 
 
 def _contig(c, b: bytes, pipeline: bool) -> dict:

@@ -246,6 +246,66 @@ int dmst_fasta_contigs(const char *text, size_t len, int flags, dmst_contig *con
  * is added and DMST_ERANGE is returned, *n_contigs holding the count. */
 int dmst_seqs_add_fasta(dmst_ctx *ctx, const char *text, size_t len, int flags, dmst_contig *contigs,
                         size_t cap_contigs, size_t *n_contigs);
+/* One window of the pipeline's prefilter hits (bin/dummest:91-183 and its
+ * bedtools sort | merge | getfasta -s stage, bin/dummest:663-676): a merged
+ * interval of one (target record, profile, strand). */
+typedef struct dmst_window {
+    int32_t record;      /* the target record: index among the record names (the genome's records) */
+    int32_t strand;      /* +1 plus_strand; -1 minus_strand_revcomp: the window is reverse-complemented */
+    int64_t start, end;  /* [start, end), 0-based positions of the record (the BED interval) */
+    int64_t profile_off; /* the profile's name (the hit rows' query) in the hits text */
+    int32_t profile_len;
+    int32_t profile;     /* its index among the profile names, -1 when not among them */
+} dmst_window;
+
+/* dmst_windows_from_hits flags: the hits' targets are the records themselves
+ * (the pipeline's ORF mode, coordinates in nucleotides, the strand from their
+ * order) rather than their six-frame translations "record_frame=+-N". */
+#define DMST_HITS_TARGET_IS_CONTIG 1
+
+/* The windows of BLAST-tab hit rows (mmseqs convertalis output), host only.
+ * Per row (12 or more fields; '#' lines and shorter rows skipped; rows whose
+ * coordinates or frame do not parse as Python's int() counted in
+ * *n_malformed and skipped; rows of a target not among the records, or of
+ * length 0, skipped) an interval centred on the hit and padded by 3 x the
+ * profile's length (0 for a profile not among profile_names) on each side,
+ * clipped to the record (_stream_bed_from_convertalis, bin/dummest:91-183).
+ * Per (target, query, strand), ordered as bedtools sort orders the names
+ * "target|query|strand" (bytes), the intervals are sorted by start and merged
+ * where the next starts at or before the current end (bedtools merge); the
+ * name is split back at its last two '|' (bin/dummest:77-88).  A window whose
+ * record is not among the names (a query holding '|') is skipped as bedtools
+ * getfasta skips it, counted in *n_dropped.  Names that repeat: the last one
+ * counts, as in the driver's dictionaries.  A row giving a start past its end
+ * is DMST_EPARSE (bedtools rejects the interval).  *n_windows gets the count;
+ * with cap below it nothing is written and DMST_ERANGE is returned. */
+int dmst_windows_from_hits(const char *hits, size_t len, int flags, const char *const *record_names,
+                           const int64_t *record_lengths, int n_records, const char *const *profile_names,
+                           const int64_t *profile_lengths, int n_profiles, dmst_window *windows, size_t cap,
+                           size_t *n_windows, size_t *n_malformed, size_t *n_dropped);
+/* Keep a genome on the device for dmst_seqs_add_windows: every record of a
+ * FASTA text (read as dmst_fasta_contigs reads it), 2 bits per position with a
+ * bitmap of the positions that are not A, C, G or T.  Replaces the previous
+ * genome; the text must stay valid while windows of it are added (their
+ * contigs name the record by its offset in it).  *n_records gets the record
+ * count; record_lengths (cap_records entries, may be NULL) each record's
+ * length (contigs and cutting characters). */
+int dmst_genome_load(dmst_ctx *ctx, const char *text, size_t len, size_t *n_records, int64_t *record_lengths,
+                     size_t cap_records);
+/* Add the windows of the loaded genome as sequences, decoded on the device
+ * from the resident genome (forward, or reverse-complemented for strand -1).
+ * Sequences and contigs are those dmst_seqs_add_fasta gives, with
+ * DMST_FASTA_PIPELINE, for the windowed FASTA the pipeline writes from the
+ * same windows (bedtools getfasta -s -name+ and _rewrite_fasta,
+ * bin/dummest:186-233): the contigs' record is the window's index, start and
+ * record_length are positions in the window, name the genome record's name
+ * in the genome text, w_start = start + 1, w_end = end, true_length the
+ * genome record's length, profile the window's (offsets in the hits text),
+ * pipeline bit 1 set for strand +1; letter_off is -1.  A window outside its
+ * record is DMST_EINVAL; with cap_contigs below the count nothing is added
+ * and DMST_ERANGE is returned, *n_contigs holding the count. */
+int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, dmst_contig *contigs,
+                          size_t cap_contigs, size_t *n_contigs);
 /* Drop all sequences (device memory is kept for reuse). */
 int dmst_seqs_clear(dmst_ctx *ctx);
 int dmst_seq_count(const dmst_ctx *ctx);
