@@ -65,13 +65,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
-    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align"], default="batched",
+    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align", "windows"],
+                    default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
                          "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
                          "profile over 4096 implant reads (L 600-2400), one SGD step per step; search: the "
                          "batched pairs through the two-wave search (filter, then mid on survivors); align: "
                          "the hit path with its traceback (an M=400 profile against homolog-carrying reads, "
-                         "both strands, the hits' alignments traced)")
+                         "both strands, the hits' alignments traced); windows: the prefilter's hit windows "
+                         "cut from a resident 256 Mbp genome and decoded on the device")
+    ap.add_argument("--win-mbp", type=int, default=256, help="windows workload: genome size (Mbp)")
+    ap.add_argument("--win-hits", type=int, default=60000, help="windows workload: hit rows per step")
     ap.add_argument("--al-reads", type=int, default=256, help="align workload: reads per step (x2 strands)")
     ap.add_argument("--al-m", type=int, default=400, help="align workload: profile length")
     ap.add_argument("--al-gate", type=float, default=1e6, help="align workload: minProbRatio of every pair")
@@ -183,6 +187,17 @@ def workload_config(args, world: int) -> dict:
             "profiles": 1, "reads_per_step": args.al_reads, "pairs_per_step": 2 * args.al_reads,
             "l2": "inputs larger than L2 (traceback tables)",
             "parallelism": f"replicas x{world} (reads sharded per rank)",
+        }
+    if args.workload == "windows":
+        return {
+            "workload": f"prefilter window stage: {args.win_hits} six-frame BLAST-tab hit rows of 8 profiles (M "
+                        f"log-uniform 100-800) on a {args.win_mbp} Mbp synthetic genome (64 records, GC 0.45, 1% "
+                        "lower case, N runs) -> merged windows (+-3M nt around each hit, both strands) -> "
+                        "codon codes of every window contig on the device",
+            "profiles": 8, "hits_per_step": args.win_hits,
+            "l2": "each step a different window set (codes written > L2); L2 flushed (256 MB) before each "
+                  "kernel-timed launch",
+            "parallelism": f"replicas x{world} (one genome per rank)",
         }
     if args.workload == "genome":
         return {
@@ -541,8 +556,187 @@ def run_align(args, rank, world, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# the prefilter window stage: hit rows -> windows -> sequences on the device
+# ---------------------------------------------------------------------------
+WIN_BYTES_PER_NT = 1.375  # per window nt: its code written (1 B) + its base read (2 bits + 1 mask bit)
+
+
+def windows_problem(args, rank):
+    """(genome FASTA text, record names, record lengths, profile names,
+    profile lengths, hit texts per step)."""
+    rng = np.random.default_rng(rank_seed(args.seed, rank))
+    n_rec = 64
+    per = args.win_mbp * 1_000_000 // n_rec
+    names = [f"chr{k + 1}" for k in range(n_rec)]
+    parts = []
+    for name in names:
+        seq = rng.choice(np.frombuffer(b"ACGT", np.uint8), size=per, p=[0.275, 0.225, 0.225, 0.275])
+        seq[rng.random(per) < 0.01] += 32
+        for _ in range(4):
+            a = int(rng.integers(0, per - 200))
+            seq[a:a + int(rng.integers(1, 200))] = ord("N")
+        rows = per // 60
+        body = np.full((rows, 61), ord("\n"), np.uint8)
+        body[:, :60] = seq[:rows * 60].reshape(rows, 60)
+        parts.append(b">" + name.encode() + b"\n" + body.tobytes() + seq[rows * 60:].tobytes() + b"\n")
+    genome = b"".join(parts)
+    Ms = np.exp(rng.uniform(np.log(100), np.log(800), size=8)).round().astype(int)
+    pnames = [f"PF{k:05d}.1" for k in range(8)]
+    frames = np.array([1, 2, 3, -1, -2, -3])
+    steps = []
+    for _ in range(args.warmup + args.steps):
+        r = rng.integers(0, n_rec, args.win_hits)
+        q = rng.integers(0, 8, args.win_hits)
+        f = frames[rng.integers(0, 6, args.win_hits)]
+        c = rng.integers(1, per // 3 - 1, args.win_hits)
+        h = rng.integers(0, 60, args.win_hits)
+        lines = [f"{pnames[q[k]]}\t{names[r[k]]}_frame={f[k]:+d}\t45.0\t90\t10\t1\t1\t30\t{max(1, c[k] - h[k])}"
+                 f"\t{c[k] + h[k]}\t1e-10\t55.0\n" for k in range(args.win_hits)]
+        steps.append("".join(lines).encode())
+    return genome, names, [per] * n_rec, pnames, Ms.tolist(), steps
+
+
+def cpu_windows_baseline(genome, windows, names, seconds):
+    """The engine side of the pipeline's text path on the host: the windowed
+    FASTA (bedtools getfasta -s, restated, not timed) read and decoded by the
+    reference's own code (readContig + decodeSequence of its PIPELINE_MODE
+    build, oracle/_ref: dmstref_read_decode), chunks of 64 windows on every host
+    thread (the ctypes call releases the interpreter lock), until the sample
+    time is spent."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import windows as W
+    from oracle import ref as R
+    recs = W.fasta_records(genome)
+    texts = []
+    for w in windows[:8192]:
+        name = names[w.record].encode()
+        seq = recs[name][w.start:w.end]
+        if w.strand < 0:
+            seq = seq.translate(W._COMP)[::-1]
+        texts.append(b">%s/%d-%d length=%d profile=P %s\n%s\n" % (
+            name, w.start + 1, w.end, len(recs[name]), b"plus_strand" if w.strand > 0 else b"minus_strand_revcomp",
+            seq))
+    chunks = [b"".join(texts[k:k + 64]) for k in range(0, len(texts), 64)]
+    R.read_decode(chunks[0])  # the harness's one-time set-up, before the threads
+    threads = os.cpu_count() or 1
+    nt, done, t0 = 0, 0, time.perf_counter()
+    with ThreadPoolExecutor(threads) as pool:
+        while time.perf_counter() - t0 < seconds:
+            batch = [chunks[(done + j) % len(chunks)] for j in range(4 * threads)]
+            nt += sum(n for n, _ in pool.map(R.read_decode, batch))
+            done += len(batch)
+    dt = time.perf_counter() - t0
+    return {"value": nt / dt / 1e9, "unit": "Gnt/s", "cores": threads, "kind": "reference",
+            "sample": f"{done} chunks of 64 windowed FASTA records ({nt} nt; the first {len(texts)} windows, "
+                      f"cycled) for {dt:.1f} s: the reference's readContig + decodeSequence (PIPELINE_MODE build, "
+                      f"oracle/_ref), {threads} threads; bedtools getfasta's own time not counted"}
+
+
+def run_windows(args, rank, world, local):
+    import dummest_b200 as d
+    from dummest_b200 import _ffi as F
+    import torch
+
+    genome, names, lens, pnames, plens, steps = windows_problem(args, rank)
+    ctx = d.Context(device=local)
+    ctx.genome_load(genome)
+    wins = [d.windows_from_hits(h, names, lens, pnames, plens)[0] for h in steps]
+    cap = [len(w) * 4 + 16 for w in wins]
+    outs = [(F.Contig * c)() for c in cap]
+    n_steps = args.warmup + args.steps
+    for k in list(range(n_steps)) + list(range(args.warmup)):  # device buffers sized for every step first
+        ctx.clear_sequences()
+        ctx.add_windows_raw(wins[k], outs[k])
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    counts = []
+    for k in range(args.warmup, n_steps):
+        ctx.clear_sequences()  # host bookkeeping only: the step's codes reuse the same device space
+        counts.append(ctx.add_windows_raw(wins[k], outs[k]))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    nt = 0
+    for k, n in zip(range(args.warmup, n_steps), counts):
+        nt += sum(c.length for c in outs[k][:n] if c.seq_id >= 0)
+    nt_all = allreduce_sum(float(nt), world)
+    ms_max = allreduce_max(ms, world)
+    value = nt_all / (ms_max / 1e3) / 1e9
+    # the decode kernel alone, one launch per step, L2 flushed before each
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    kern_ms = 0.0
+    for k in range(args.warmup, n_steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        ctx.clear_sequences()
+        ctx.add_windows_raw(wins[k], outs[k])
+        kern_ms += ctx.last_windows_ms()
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6451.2)
+    achieved = WIN_BYTES_PER_NT * nt / (kern_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "kernel": "windowDecodeKernel, CUDA events on the library stream around each launch",
+                "algorithmic_bytes_per_nt": WIN_BYTES_PER_NT, "kernel_ms_per_step": kern_ms / args.steps}
+    # e2e: from each step's hit rows in host memory: the windows (host), the
+    # contigs (host), the segment descriptors up and the decode on the device
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = 0
+    for k in range(args.warmup, n_steps):
+        w, _, _ = d.windows_from_hits(steps[k], names, lens, pnames, plens)
+        ctx.clear_sequences()
+        n = ctx.add_windows_raw(w, outs[k])
+        h2d += 40 * sum(1 for c in outs[k][:n] if c.seq_id >= 0)  # one 40-byte descriptor per sequence
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    e2e = {"value": nt_all / e2e_s / 1e9, "unit": "Gnt/s", "h2d_bytes_per_step": h2d // args.steps,
+           "d2h_bytes_per_step": 0,
+           "note": "the step's result (contigs, sequence ids) is host memory; the codes stay on the device"}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_windows_baseline(genome, wins[args.warmup], names, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "prefilter window stage: window nt decoded per second", "value": value, "unit": "Gnt/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": dict(workload_config(args, world), windows_per_step=sum(len(wins[k]) for k in
+                           range(args.warmup, n_steps)) / args.steps, nt_per_step=nt / args.steps),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clk,
+            "gpu_launches": args.steps}), flush=True)
+    ctx.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
+        return
+    if args.workload == "windows":
+        genome, names, lens, pnames, plens, steps = windows_problem(args, 0)
+        import dummest_b200 as d
+        wins = d.windows_from_hits(steps[0], names, lens, pnames, plens)[0]
+        vals, cb = [], None
+        per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_windows_baseline(genome, wins, names, per_step)
+            vals.append(cb["value"])
+        v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else vals[-1]
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": "prefilter window stage: window nt decoded per second", "value": v,
+            "unit": "Gnt/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": workload_config(args, world), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "Gnt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
         return
     profiles, txt, steps = make_workload(args, 0, 1)
     if args.workload == "align":
@@ -1088,6 +1282,8 @@ def main():
             run_search(args, rank, world, local)
         elif args.workload == "align":
             run_align(args, rank, world, local)
+        elif args.workload == "windows":
+            run_windows(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -190,6 +190,7 @@ SIGNATURES = [
      [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int64), C.c_size_t]),
     ("dmst_seqs_add_windows", C.c_int,
      [C.c_void_p, C.POINTER(Window), C.c_size_t, C.POINTER(Contig), C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("dmst_last_windows_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("dmst_align", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(Result), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("dmst_align_fetch", C.c_int,

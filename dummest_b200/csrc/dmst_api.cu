@@ -385,6 +385,8 @@ struct dmst_ctx {
     std::vector<GenomeRecord> genome;
     DevBuf<uint32_t> dGenomeWords, dGenomeMask;
     DevBuf<WinSeg> dWinSegs;
+    cudaEvent_t evWin[2] = {};  // around the last window decode kernel
+    bool winTimed = false;
 
     // per call (shared by the slots: used only by a call's stream-ordered kernels)
     DevBuf<XS> dNullTmp;
@@ -613,6 +615,11 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dPost.release();
     ctx->dExactScratch.release();
     ctx->dExactOut.release();
+    ctx->dGenomeWords.release();
+    ctx->dGenomeMask.release();
+    ctx->dWinSegs.release();
+    for (auto &e : ctx->evWin)
+        if (e) cudaEventDestroy(e);
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1131,9 +1138,14 @@ int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, d
         CK(cudaMemcpyAsync(ctx->dWinSegs.p, segs.data(), segs.size() * sizeof(WinSeg), cudaMemcpyHostToDevice,
                            ctx->stream),
            "upload window segments");
+        for (auto &e : ctx->evWin)
+            if (!e) CK(cudaEventCreate(&e), "event");
+        CK(cudaEventRecord(ctx->evWin[0], ctx->stream), "event");
         windowDecodeKernel<<<(unsigned)segs.size(), 256, 0, ctx->stream>>>(ctx->dGenomeWords.p, ctx->dGenomeMask.p,
                                                                           ctx->dWinSegs.p, ctx->dCodes.p);
         CK(cudaGetLastError(), "window decode kernel");
+        CK(cudaEventRecord(ctx->evWin[1], ctx->stream), "event");
+        ctx->winTimed = true;
         commitSeqs(ctx, sOff, lens, &first);
     }
     size_t next = 0;
@@ -1159,6 +1171,17 @@ int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, d
         o.profile_len = w.profile_len;
         o.pad = 0;
     }
+    return DMST_OK;
+}
+
+int dmst_last_windows_ms(dmst_ctx *ctx, double *ms) {
+    if (!ctx || !ms) return DMST_EINVAL;
+    *ms = -1.0;
+    if (!ctx->winTimed) return DMST_OK;
+    CK(cudaEventSynchronize(ctx->evWin[1]), "window timing");
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->evWin[0], ctx->evWin[1]), "window timing");
+    *ms = t;
     return DMST_OK;
 }
 

@@ -332,6 +332,19 @@ class Context:
                         "profile": hits[c.profile_off:c.profile_off + c.profile_len].decode() if hits else None})
         return out
 
+    def add_windows_raw(self, windows, out) -> int:
+        """dmst_seqs_add_windows into a ctypes Contig array: the contig count."""
+        n = C.c_size_t(0)
+        self._check(self.lib.dmst_seqs_add_windows(self.h, windows, len(windows), out, len(out), C.byref(n)),
+                    "dmst_seqs_add_windows")
+        return n.value
+
+    def last_windows_ms(self) -> float:
+        """Device ms of the last add_windows decode kernel (-1: none)."""
+        ms = C.c_double(0)
+        self._check(self.lib.dmst_last_windows_ms(self.h, C.byref(ms)), "dmst_last_windows_ms")
+        return ms.value
+
     def align_raw(self, pairs, out=None):
         """The traceback of the hit path (dmst_align) on a ctypes Pair array:
         (alignments, segments): a ctypes Alignment array and an (n, 3) int32

@@ -306,6 +306,9 @@ int dmst_genome_load(dmst_ctx *ctx, const char *text, size_t len, size_t *n_reco
  * and DMST_ERANGE is returned, *n_contigs holding the count. */
 int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, dmst_contig *contigs,
                           size_t cap_contigs, size_t *n_contigs);
+/* Device ms of the last dmst_seqs_add_windows decode kernel (waits for it);
+ * -1 when none has run. */
+int dmst_last_windows_ms(dmst_ctx *ctx, double *ms);
 /* Drop all sequences (device memory is kept for reuse). */
 int dmst_seqs_clear(dmst_ctx *ctx);
 int dmst_seq_count(const dmst_ctx *ctx);

@@ -309,3 +309,17 @@ def read_fasta_pipeline(text: bytes):
     lines = nm.raw.split(b"\0")[0].decode().split("\n")[:-1]
     names = [tuple(x.split("\t", 1)) for x in lines]
     return rec[:n].copy(), st[:n].copy(), ln[:n].copy(), fields[:n].copy(), names
+
+
+def read_decode(text: bytes, pipeline: bool = True) -> tuple[int, int]:
+    """The engine's sequence loop without scoring (dmstref_read_decode): every
+    contig of the text read and decoded by the reference's own code, in the
+    PIPELINE_MODE build (or the plain one).  Returns (total length, checksum of
+    the decoded codes).  The call releases the interpreter lock."""
+    L = C.CDLL(PIPELINE_LIB if pipeline else LIBS[32])
+    f = L.dmstref_read_decode
+    f.restype = C.c_longlong
+    f.argtypes = [C.c_char_p, C.c_longlong, C.POINTER(C.c_longlong)]
+    cs = C.c_longlong(0)
+    n = f(text, len(text), C.byref(cs))
+    return int(n), int(cs.value)

@@ -378,6 +378,41 @@ int dmstref_read_fasta(const char *text, long long len, int *record, int *start,
     return (int)rec.size();
 }
 
+// The engine's sequence loop without its scoring (dummest.cc:553-606, no
+// masking): every contig read (readContig with the IUPAC classes,
+// dummest.cc:445-456), padded as the engine pads it and decoded
+// (decodeSequence).  Returns the contigs' total length; *checksum gets the sum
+// of the decoded codes times their position + 1.
+long long dmstref_read_decode(const char *text, long long len, long long *checksum) {
+    ensureInit();
+    const char *alphabet = getAlphabet(20);
+    char charToNumber[256];
+    memset(charToNumber, 127, 256);
+    memset(charToNumber, 125, ' ' + 1);
+    charToNumber['>'] = 126;
+    setCharToNumber(charToNumber, alphabet);
+    char iupac[256];
+    std::copy(charToNumber, charToNumber + 256, iupac);
+    for (auto c : "RYSWKMBDHVN")
+        if (c != '\0') iupac[(unsigned char)c] = iupac[tolower(c)] = 22;
+    std::istringstream in(std::string(text, (size_t)len));
+    Sequence sequence{};
+    Contig contig{0, 0};
+    std::vector<char> vec;
+    long long total = 0, sum = 0;
+    while (readContig(in, sequence, contig, vec, iupac)) {
+        if (contig.length == 0) continue;
+        const size_t seqIdx = vec.size() - contig.length;
+        vec.resize(seqIdx + simdRoundUp(contig.length + 1));
+        std::vector<uint8_t> d = decodeSequence(&vec[seqIdx], contig.length, alphabet, charToNumber);
+        for (size_t k = 0; k < d.size(); ++k) sum += (long long)d[k] * (long long)(k + 1);
+        total += contig.length;
+        vec.resize(seqIdx);
+    }
+    if (checksum) *checksum = sum;
+    return total;
+}
+
 #ifdef PIPELINE_MODE
 // The reader of the PIPELINE_MODE build (dummest-sequence.hh:19-52): per
 // contig also its record's header fields as the reader left them in

@@ -138,3 +138,22 @@ def test_window_errors_and_capacity():
                                       C.byref(nm), C.byref(nd)) == F.DMST_EINVAL
     assert lib.dmst_windows_from_hits(b"", 0, 0, names, lens, 1, pn, pl, 1, None, 0, C.byref(n),
                                       C.byref(nm), C.byref(nd)) == 0 and n.value == 0
+
+
+@pytest.mark.parametrize("mode", ["frame", "contig"])
+def test_windowed_fasta_codes_equal_reference_decode(gold, mode):
+    """The codon codes of the windowed FASTA's contigs (dmst_fasta_contigs +
+    dmst_decode_letters) against the reference engine's own read-and-decode
+    loop (readContig + decodeSequence, dmstref_read_decode), by their total
+    length and position-weighted checksum."""
+    from oracle import ref as R
+    if not os.path.exists(R.PIPELINE_LIB):
+        pytest.skip("oracle/_ref/libdmst_ref32p.so not built (needs the reference sources)")
+    text = gold[f"{mode}_fasta"].tobytes()
+    n, cs = R.read_decode(text)
+    total, mine = 0, 0
+    for c in d.fasta_contigs(text, pipeline=True):
+        codes = d.decode_letters(c["letters"].astype(np.int8)).astype(np.int64)
+        mine += int((codes * np.arange(1, len(codes) + 1)).sum())
+        total += c["length"]
+    assert (total, mine) == (n, cs) and n > 50000
