@@ -95,32 +95,91 @@ __global__ void decodePackedKernel(const uint32_t *words, const uint32_t *mask, 
 // the record's base pos + len - 1 - k).
 struct WinSeg {
     long long wordOff, maskOff, outOff;
-    int pos, len, rev, pad;
+    int pos, len, rev;
+    int chunk;  // its first 16-code chunk: the call's sequences are consecutive whole chunks
 };
 
+// Words of padding before the first and after the last record of the resident
+// genome: a window's lanes read up to two words before and after its contig.
+constexpr long long kGenomePad = 2;
+
 // Windows of the resident genome -> codon codes, as decodePackedKernel decodes
-// the same letters uploaded packed (the last two codes 0).
-__global__ void windowDecodeKernel(const uint32_t *words, const uint32_t *mask, const WinSeg *segs, uint8_t *codes) {
-    const WinSeg sg = segs[blockIdx.x];
+// the same letters uploaded packed (the last two codes 0).  The call's
+// sequences lie back to back in whole 16-byte chunks (starts 16-byte aligned,
+// lengths reserved in 16-byte units), and each thread makes one chunk: 16
+// codes from the 18 bases they need (three 2-bit words and two mask words,
+// funnel-shifted into place), written with one 16-byte store, so every thread
+// has the same work whatever the contigs' lengths.  A block finds its threads'
+// contigs from the first contig of its first chunk (blockSeg, from the host).
+// The codon table sits in shared memory: the lanes' lookups differ, which a
+// constant-memory table would serialise.
+constexpr int kWinThreads = 256;
+__global__ void __launch_bounds__(kWinThreads)
+windowDecodeKernel(const uint32_t *words, const uint32_t *mask, const WinSeg *segs, const int *blockSeg, int nseg,
+                   long long nChunks, uint8_t *codes) {
+    // table[64 rev + y]: the code of the triplet whose three bases, in record
+    // order, are the 2-bit fields of y (lowest first): forward the codon
+    // (b0, b1, b2) = (y & 3, y >> 2 & 3, y >> 4); reverse-complemented the
+    // codon (3 - b2, 3 - b1, 3 - b0), whose codon-table index is 63 - y.
+    // nib[n]: 0xFF in the bytes whose bit of n is set.
+    __shared__ uint8_t table[128];
+    __shared__ uint32_t nib[16];
+    if (threadIdx.x < 64) {
+        const int y = threadIdx.x;
+        table[y] = cCodonTable[16 * (y & 3) + 4 * ((y >> 2) & 3) + (y >> 4)];
+        table[64 + y] = cCodonTable[63 - y];
+    } else if (threadIdx.x < 80) {
+        const int n = threadIdx.x - 64;
+        nib[n] = (n & 1 ? 0xFFu : 0u) | (n & 2 ? 0xFF00u : 0u) | (n & 4 ? 0xFF0000u : 0u) | (n & 8 ? 0xFF000000u : 0u);
+    }
+    __syncthreads();
+    const long long g = (long long)blockIdx.x * kWinThreads + threadIdx.x;
+    if (g >= nChunks) return;
+    int s = blockSeg[blockIdx.x];
+    while (s + 1 < nseg && segs[s + 1].chunk <= g) ++s;
+    const WinSeg sg = segs[s];
     const uint32_t *w = words + sg.wordOff;
     const uint32_t *mk = mask + sg.maskOff;
-    uint8_t *out = codes + sg.outOff;
-    for (int i = threadIdx.x; i < sg.len; i += blockDim.x) {
-        uint8_t c = 0;
-        if (i + 2 < sg.len) {
-            int b[3];
-            bool masked = false;
+    const int q0 = 16 * (int)(g - sg.chunk);
+    // the sequence's bases q0 .. q0 + 17 are the record's g0 .. g0 + 17
+    // (reversed and complemented for rev); g0 >= pos - 17 and the words read
+    // end at most two past the record's last
+    const int g0 = sg.rev ? sg.pos + sg.len - 18 - q0 : sg.pos + q0;
+    const int wi = g0 >> 4, o = g0 & 15, mi = g0 >> 5, mo = g0 & 31;
+    const uint32_t w0 = __ldg(w + wi), w1 = __ldg(w + wi + 1), w2 = __ldg(w + wi + 2);
+    const uint32_t lo = __funnelshift_r(w0, w1, 2 * o);  // bases g0 .. g0 + 15
+    const uint32_t hi = __funnelshift_r(w1, w2, 2 * o);  // bases g0 + 16 .. g0 + 31
+    const uint32_t m = __funnelshift_r(__ldg(mk + mi), __ldg(mk + mi + 1), mo);  // mask bits g0 .. g0 + 31
+    // the triplets at record positions g0 + j, j = 0 .. 15: forward the
+    // sequence's codes in order, reverse-complemented in reverse order
+    const uint32_t base = sg.rev ? 64u : 0u;
+    const uint32_t mm = m | (m >> 1) | (m >> 2);  // bit j: a base of triplet j is not A, C, G or T
+    uint32_t ow[4];
 #pragma unroll
-            for (int t = 0; t < 3; ++t) {
-                const int p = sg.rev ? sg.pos + sg.len - 1 - (i + t) : sg.pos + i + t;
-                const int bb = (int)((__ldg(w + (p >> 4)) >> (2 * (p & 15))) & 3u);
-                if ((__ldg(mk + (p >> 5)) >> (p & 31)) & 1u) masked = true;
-                b[t] = sg.rev ? 3 - bb : bb;  // A-T, C-G
-            }
-            c = masked ? (uint8_t)kMaskCode : cCodonTable[16 * b[0] + 4 * b[1] + b[2]];
+    for (int q = 0; q < 4; ++q) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int j = 4 * q + r;
+            v |= (uint32_t)table[(__funnelshift_r(lo, hi, 2 * j) & 63u) | base] << (8 * r);
         }
-        out[i] = c;
+        const uint32_t mb = nib[(mm >> (4 * q)) & 15u];
+        ow[q] = (v & ~mb) | ((uint32_t)kMaskCode * 0x01010101u & mb);
     }
+    if (sg.rev) {  // bytes in sequence order
+        const uint32_t t0 = __byte_perm(ow[3], 0, 0x0123), t1 = __byte_perm(ow[2], 0, 0x0123);
+        ow[2] = __byte_perm(ow[1], 0, 0x0123);
+        ow[3] = __byte_perm(ow[0], 0, 0x0123);
+        ow[0] = t0;
+        ow[1] = t1;
+    }
+    const int valid = sg.len - 2 - q0;  // codes k < valid are codons, the rest 0
+    if (valid < 16) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (k >= valid) ow[k >> 2] &= ~(0xFFu << (8 * (k & 3)));
+    }
+    *reinterpret_cast<uint4 *>(codes + sg.outOff + q0) = make_uint4(ow[0], ow[1], ow[2], ow[3]);
 }
 
 // ---------------------------------------------------------------------------
@@ -374,7 +433,9 @@ struct dmst_ctx {
     DevBuf<int> dStageLen;
 
     // the genome of dmst_genome_load: per record its name in the text, its
-    // length, its packed words and mask words, and its contigs (start, length)
+    // length, its packed words and mask words (offsets in buffers that hold
+    // kGenomePad words before the first record and after the last), and its
+    // contigs (start, length)
     struct GenomeRecord {
         size_t nameOff;
         int nameLen;
@@ -1044,7 +1105,7 @@ int dmst_genome_load(dmst_ctx *ctx, const char *text, size_t len, size_t *n_reco
     // characters) 2 bits, each record on fresh words; the positions that are
     // not A, C, G or T (cutting characters included) set in the bitmap
     std::vector<dmst_ctx::GenomeRecord> g(recs.size());
-    long long nw = 0, nm = 0;
+    long long nw = kGenomePad, nm = kGenomePad;
     for (size_t r = 0; r < recs.size(); ++r) {
         g[r].nameOff = recs[r].nameOff;
         g[r].nameLen = recs[r].nameLen;
@@ -1054,7 +1115,7 @@ int dmst_genome_load(dmst_ctx *ctx, const char *text, size_t len, size_t *n_reco
         nw += (recs[r].length + 15) / 16;
         nm += (recs[r].length + 31) / 32;
     }
-    std::vector<uint32_t> words((size_t)std::max(nw, 1LL), 0u), mask((size_t)std::max(nm, 1LL), ~0u);
+    std::vector<uint32_t> words((size_t)(nw + kGenomePad), 0u), mask((size_t)(nm + kGenomePad), ~0u);
     for (const FastaContig &c : cs) {
         dmst_ctx::GenomeRecord &gr = g[c.record];
         gr.contigs.emplace_back(c.start, c.length);
@@ -1127,22 +1188,39 @@ int dmst_seqs_add_windows(dmst_ctx *ctx, const dmst_window *windows, size_t n, d
         std::vector<int> lens;
         int st = reserveSeqs(ctx, off.data(), (int)which.size(), sOff, lens);
         if (st) return st;
+        // the sequences are reserved back to back in whole 16-byte chunks
         std::vector<WinSeg> segs(which.size());
+        long long nChunks = 0;
         for (size_t i = 0; i < which.size(); ++i) {
             const Piece &pc = pieces[which[i]];
             const dmst_window &w = windows[pc.window];
             const dmst_ctx::GenomeRecord &gr = ctx->genome[w.record];
-            segs[i] = {gr.wordOff, gr.maskOff, sOff[i], pc.pos, pc.length, w.strand < 0 ? 1 : 0, 0};
+            if (sOff[i] != sOff[0] + 16 * nChunks) return ctx->fail(DMST_EINVAL, "window sequences not contiguous");
+            segs[i] = {gr.wordOff, gr.maskOff, sOff[i], pc.pos, pc.length, w.strand < 0 ? 1 : 0, (int)nChunks};
+            nChunks += (pc.length + 15) / 16;
         }
-        CK(ctx->dWinSegs.ensure(segs.size(), 0.3), "alloc window segments");
-        CK(cudaMemcpyAsync(ctx->dWinSegs.p, segs.data(), segs.size() * sizeof(WinSeg), cudaMemcpyHostToDevice,
-                           ctx->stream),
+        if (nChunks >= INT32_MAX) return ctx->fail(DMST_EINVAL, "windows: %lld chunks of 16 nt, too many", nChunks);
+        const long long blocks = (nChunks + kWinThreads - 1) / kWinThreads;
+        std::vector<int> blockSeg((size_t)blocks);
+        for (long long bk = 0, sgi = 0; bk < blocks; ++bk) {  // the contig of each block's first chunk
+            while (sgi + 1 < (long long)segs.size() && segs[sgi + 1].chunk <= bk * kWinThreads) ++sgi;
+            blockSeg[bk] = (int)sgi;
+        }
+        // one upload: the descriptors, then the blocks' first contigs
+        const size_t segBytes = segs.size() * sizeof(WinSeg), total = segBytes + blockSeg.size() * sizeof(int);
+        CK(ctx->dWinSegs.ensure((total + sizeof(WinSeg) - 1) / sizeof(WinSeg), 0.3), "alloc window segments");
+        std::vector<char> up(total);
+        std::memcpy(up.data(), segs.data(), segBytes);
+        std::memcpy(up.data() + segBytes, blockSeg.data(), blockSeg.size() * sizeof(int));
+        CK(cudaMemcpyAsync(ctx->dWinSegs.p, up.data(), total, cudaMemcpyHostToDevice, ctx->stream),
            "upload window segments");
         for (auto &e : ctx->evWin)
             if (!e) CK(cudaEventCreate(&e), "event");
         CK(cudaEventRecord(ctx->evWin[0], ctx->stream), "event");
-        windowDecodeKernel<<<(unsigned)segs.size(), 256, 0, ctx->stream>>>(ctx->dGenomeWords.p, ctx->dGenomeMask.p,
-                                                                          ctx->dWinSegs.p, ctx->dCodes.p);
+        windowDecodeKernel<<<(unsigned)blocks, kWinThreads, 0, ctx->stream>>>(
+            ctx->dGenomeWords.p, ctx->dGenomeMask.p, ctx->dWinSegs.p,
+            reinterpret_cast<const int *>(reinterpret_cast<const char *>(ctx->dWinSegs.p) + segBytes),
+            (int)segs.size(), nChunks, ctx->dCodes.p);
         CK(cudaGetLastError(), "window decode kernel");
         CK(cudaEventRecord(ctx->evWin[1], ctx->stream), "event");
         ctx->winTimed = true;

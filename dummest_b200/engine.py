@@ -670,14 +670,12 @@ def windows_from_hits(hits: str | bytes, record_names, record_lengths, profile_n
     flags = F.HITS_TARGET_IS_CONTIG if target_is_contig else 0
     n, nm, nd = C.c_size_t(0), C.c_size_t(0), C.c_size_t(0)
     args = (b, len(b), flags, rna, rla, len(rn), pna, pla, len(pn))
-    st = lib.dmst_windows_from_hits(*args, None, 0, C.byref(n), C.byref(nm), C.byref(nd))
-    if st not in (0, F.DMST_ERANGE):
-        raise ValueError(f"dmst_windows_from_hits: status {st}")
-    arr = (F.Window * n.value)()
-    st = lib.dmst_windows_from_hits(*args, arr, n.value, C.byref(n), C.byref(nm), C.byref(nd))
+    cap = len(b) // 23 + 1  # at most one window per row of 12 fields (>= 23 bytes): one pass over the text
+    arr = (F.Window * cap)()
+    st = lib.dmst_windows_from_hits(*args, arr, cap, C.byref(n), C.byref(nm), C.byref(nd))
     if st != 0:
         raise ValueError(f"dmst_windows_from_hits: status {st}")
-    return arr, nm.value, nd.value
+    return (F.Window * n.value).from_buffer(arr), nm.value, nd.value
 
 
 def _contig(c, b: bytes, pipeline: bool) -> dict:
