@@ -157,3 +157,28 @@ def test_windowed_fasta_codes_equal_reference_decode(gold, mode):
         mine += int((codes * np.arange(1, len(codes) + 1)).sum())
         total += c["length"]
     assert (total, mine) == (n, cs) and n > 50000
+
+
+def test_coordinates_read_as_python_int():
+    """A row counts as malformed exactly when the driver's int() of one of its
+    coordinate fields raises (bin/dummest:108-113): signs, leading zeros,
+    single underscores between digits are numbers; doubled, leading or
+    trailing underscores, signs alone, letters and dots are not."""
+    rng = np.random.default_rng(21)
+    pieces = ["0", "7", "12", "007", "1_2", "1__2", "_1", "1_", "+5", "-5", "+", "-", "", "1.0", "1e3", "x",
+              "٣", "1 2", "+_1", "9_9_9"]
+    rows, want = [], 0
+    for k in range(400):
+        tok = str(rng.choice(pieces)) + str(rng.choice(pieces))
+        if not tok or " " in tok:
+            continue
+        field = int(rng.integers(6, 10))
+        f = ["P", "r1_frame=+1", "50", "90", "9", "0", "1", "30", "40", "41", "1e-9", "77.0"]
+        f[field] = tok
+        try:
+            int(tok.encode())
+        except ValueError:
+            want += 1
+        rows.append("\t".join(f) + "\n")
+    wins, malformed, dropped = d.windows_from_hits("".join(rows).encode("utf-8"), ["r1"], [10**12], ["P"], [10])
+    assert malformed == want and want > 50
