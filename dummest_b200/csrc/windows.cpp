@@ -25,6 +25,7 @@
 #include <climits>
 #include <string>
 #include <string_view>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -196,7 +197,12 @@ int windowsFromHits(const char *tab, size_t len, bool targetIsContig, const std:
         parseRange(0, len, parts[0]);
     } else {
         std::vector<std::thread> pool;
-        for (size_t k = 0; k < nParts; ++k) pool.emplace_back(parseRange, cut[k], cut[k + 1], std::ref(parts[k]));
+        try {
+            for (size_t k = 0; k < nParts; ++k)
+                pool.emplace_back(parseRange, cut[k], cut[k + 1], std::ref(parts[k]));
+        } catch (const std::system_error &) {  // no more threads: this one parses the parts left
+            for (size_t k = pool.size(); k < nParts; ++k) parseRange(cut[k], cut[k + 1], parts[k]);
+        }
         for (auto &t : pool) t.join();
     }
     std::unordered_map<unsigned long long, int> chromOf;  // (record, query id, strand) -> chroms index
