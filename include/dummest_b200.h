@@ -278,7 +278,9 @@ typedef struct dmst_window {
  * getfasta skips it, counted in *n_dropped.  Names that repeat: the last one
  * counts, as in the driver's dictionaries.  A row giving a start past its end
  * is DMST_EPARSE (bedtools rejects the interval).  *n_windows gets the count;
- * with cap below it nothing is written and DMST_ERANGE is returned. */
+ * with cap below it nothing is written and DMST_ERANGE is returned.  A text of
+ * 1 MB or more is parsed on up to 16 host threads (line-aligned parts, grouped
+ * in text order, so the result does not depend on the split). */
 int dmst_windows_from_hits(const char *hits, size_t len, int flags, const char *const *record_names,
                            const int64_t *record_lengths, int n_records, const char *const *profile_names,
                            const int64_t *profile_lengths, int n_profiles, dmst_window *windows, size_t cap,

@@ -182,3 +182,19 @@ def test_coordinates_read_as_python_int():
         rows.append("\t".join(f) + "\n")
     wins, malformed, dropped = d.windows_from_hits("".join(rows).encode("utf-8"), ["r1"], [10**12], ["P"], [10])
     assert malformed == want and want > 50
+
+
+@pytest.mark.parametrize("mode", ["frame", "contig"])
+def test_threaded_parse_equals_single(gold, mode):
+    """A text of 1 MB or more is parsed on several threads: the golden rows
+    repeated past 1 MB (each copy's intervals merge into the first's) give the
+    single text's windows, with the malformed rows counted once per copy."""
+    hits, names, (wins, malformed, dropped) = _windows(gold, mode)
+    copies = (1 << 20) // len(hits) + 2
+    big = hits * copies
+    wb, mb, db = d.windows_from_hits(big, names, gold["rec_lens"], [bytes(x) for x in gold["prof_names"]],
+                                     gold["prof_lens"], target_is_contig=(mode == "contig"))
+    key = lambda ws, t: [(w.record, w.strand, w.start, w.end, t[w.profile_off:w.profile_off + w.profile_len])
+                         for w in ws]
+    assert key(wb, big) == key(wins, hits)
+    assert mb == copies * malformed and db == dropped
