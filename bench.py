@@ -58,13 +58,21 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--reads-per-step", type=int, default=1024)
+    ap.add_argument("--reads-per-step", type=int, default=5000,
+                    help="reads per step (x2 strands x --profiles pairs); 20 steps of 5,000 reads are the "
+                         "batched configuration's 100,000 reads")
+    ap.add_argument("--parity-pairs", type=int, default=512,
+                    help="pairs of the timed steps re-scored by the reference engine after the timed region "
+                         "(0: none)")
     ap.add_argument("--profiles", type=int, default=64)
     ap.add_argument("--seed", type=int, default=20261205)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--lmax", type=int, default=3000,
+                    help="longest read of the batched workload (3000 in the stated configuration; smaller "
+                         "values only to keep a profiling capture's device memory small)")
     ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align", "windows"],
                     default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
@@ -208,7 +216,7 @@ def workload_config(args, world: int) -> dict:
         }
     return {
         "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform 50-800 x "
-                    "reads L log-uniform 150-3000 nt, GC 0.4-0.6, 10% implants, both strands",
+                    f"reads L log-uniform 150-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands",
         "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
         "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
         "l2": "inputs larger than L2 (W1 slots)",
@@ -243,17 +251,117 @@ def make_workload(args, rank: int, n_steps: int):
             steps.append(synth.both_strands(reads))
         return [prof], synth.hmmer3_text([prof]), steps
     profiles, txt = make_profiles(args.seed, args.profiles)
-    return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step)
+    return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step, args.lmax)
 
 
-def make_steps(seed, profiles, n_steps, reads_per_step):
+def make_steps(seed, profiles, n_steps, reads_per_step, lmax=3000):
     from dummest_b200 import synth
     rng = np.random.default_rng(seed)
     steps = []
     for _ in range(n_steps):
-        reads = synth.make_reads(rng, reads_per_step, 150, 3000, profiles, 0.10, gc_range=(0.4, 0.6))
+        reads = synth.make_reads(rng, reads_per_step, 150, lmax, profiles, 0.10, gc_range=(0.4, 0.6))
         steps.append(synth.both_strands(reads))
     return steps
+
+
+PAIR_DTYPE = np.dtype([("seq", "<i4"), ("profile", "<i4"), ("min_prob_ratio", "<f4")])
+RESULT_DTYPE = np.dtype([("mid_m", "<f4"), ("mid_e", "<i4"), ("flt_m", "<f4"), ("flt_e", "<i4"),
+                         ("mid_ln", "<f8"), ("flt_ln", "<f8"), ("filter_f", "<f4"), ("flags", "<i4")])
+
+
+def pair_array(sids, pids, min_prob_ratio=-2.0):
+    """Every (profile, record) pair, profile-major, as a ctypes dmst_pair
+    array backed by numpy (the pair of profile index a and record index b is
+    element a * len(sids) + b)."""
+    from dummest_b200 import _ffi as F
+    assert F.C.sizeof(F.Pair) == PAIR_DTYPE.itemsize
+    sids = np.asarray(sids, np.int32)
+    pids = np.asarray(pids, np.int32)
+    arr = np.empty(len(sids) * len(pids), PAIR_DTYPE)
+    arr["seq"] = np.tile(sids, len(pids))
+    arr["profile"] = np.repeat(pids, len(sids))
+    arr["min_prob_ratio"] = min_prob_ratio
+    out = (F.Pair * len(arr)).from_buffer(arr)
+    out._keep = arr  # the ctypes array views arr's memory
+    return out
+
+
+def result_view(res) -> np.ndarray:
+    """A ctypes dmst_result array as a numpy structured array (no copy)."""
+    from dummest_b200 import _ffi as F
+    assert F.C.sizeof(F.Result) == RESULT_DTYPE.itemsize
+    return np.frombuffer(res, dtype=RESULT_DTYPE)
+
+
+def parity_sample(hmm_text, steps, results, first_step, n_sample, seed):
+    """Scores a seeded sample of the timed steps' pairs with the reference
+    engine (oracle/_ref, FP32 findSimilarities needAlign=false) and compares
+    them with the results the timed calls returned: mid and filter ExpScores
+    bit for bit.  The sample holds n_sample random pairs plus, for every
+    timed step, its longest record against its longest profile.  results[i]
+    belongs to steps[first_step + i]; pairs are profile-major."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle.ref import RefEngine, available
+    if not available(32):
+        return {"checked": 0, "bit_equal": 0, "max_abs_bits": None, "note": "oracle/_ref not built"}
+    e = RefEngine(32)
+    e.set_rates()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(hmm_text)
+        path = f.name
+    n_prof = e.load_profiles(path)
+    os.unlink(path)
+    Ms = np.array([e.profile(p)[1].shape[0] - 1 for p in range(n_prof)])
+    rng = np.random.default_rng(seed + 77)
+    picks = set()
+    for i in range(len(results)):
+        recs = steps[first_step + i]
+        picks.add((i, int(np.argmax(Ms)), int(np.argmax([len(r) for r in recs]))))
+    n_rec = len(steps[first_step])
+    while len(picks) < n_sample + len(results):
+        i = int(rng.integers(0, len(results)))
+        picks.add((i, int(rng.integers(0, n_prof)), int(rng.integers(0, len(steps[first_step + i])))))
+    picks = sorted(picks, key=lambda t: (t[1], t[0], t[2]))
+    by_prof = {}
+    for t in picks:
+        by_prof.setdefault(t[1], []).append(t)
+    jobs = []
+    for p, lst in by_prof.items():
+        for b in range(0, len(lst), e.width):
+            jobs.append((p, lst[b:b + e.width]))
+
+    def run(job):
+        p, lst = job
+        codes = [e.decode(e.encode(steps[first_step + i][r])) for i, _, r in lst]
+        return job, e.find_similarities(p, codes)
+
+    t0 = time.perf_counter()
+    checked = equal = 0
+    worst = 0.0
+    cells = 0.0
+    largest = (0, 0)
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        for (p, lst), refs in ex.map(run, jobs):
+            for (i, _, r), (mm, me, ml, fm, fe) in zip(lst, refs):
+                n_r = len(steps[first_step + i])
+                got = result_view(results[i])[p * n_r + r]
+                same = (np.float32(got["mid_m"]) == np.float32(mm) and int(got["mid_e"]) == me
+                        and np.float32(got["flt_m"]) == np.float32(fm) and int(got["flt_e"]) == fe)
+                checked += 1
+                equal += int(same)
+                if np.isfinite(ml) and np.isfinite(got["mid_ln"]):
+                    worst = max(worst, abs(float(got["mid_ln"]) - ml) / np.log(2.0))
+                elif not (np.isinf(ml) and np.isinf(got["mid_ln"])):
+                    worst = float("inf")
+                L = len(steps[first_step + i][r])
+                cells += (Ms[p] + 1) * L
+                largest = max(largest, (int(Ms[p]), L))
+    return {"checked": checked, "bit_equal": equal, "max_abs_bits": worst,
+            "sample": f"{n_sample} seeded random pairs of the {len(results)} timed steps plus each step's "
+                      f"longest record x longest profile (M={largest[0]}, L up to "
+                      f"{max(len(r) for st in steps[first_step:first_step + len(results)] for r in st)}); "
+                      f"{cells:.3e} cells, reference FP32 engine, {time.perf_counter() - t0:.1f} s",
+            "compared": "mid and filter ExpScore (mantissa, exponent) of the timed calls' results"}
 
 
 # ---------------------------------------------------------------------------
@@ -308,6 +416,15 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_model() -> str:
+    """The host CPU's model name and logical CPU count (from /proc/cpuinfo)."""
+    try:
+        names = [ln.split(":", 1)[1].strip() for ln in open("/proc/cpuinfo") if ln.startswith("model name")]
+        return f"{names[0]} ({len(names)} logical CPUs)" if names else "unknown"
+    except OSError:
+        return "unknown"
 
 
 def measured_peaks():
@@ -367,7 +484,7 @@ def cpu_baseline(hmm_text, records, n_profiles, seconds, seed):
     return {
         "value": done_cells / done_s / 1e9,
         "unit": "GCUPS",
-        "cores": threads,
+        "cores": threads, "cpu_model": cpu_model(),
         "kind": "reference",
         "sample": f"{recs} record-profile pairs of one step ({used} of {n} profiles), "
                   f"{done_cells:.3e} cells in {done_s:.1f} s, reference FP32 engine "
@@ -417,7 +534,7 @@ def cpu_search_baseline(hmm_text, records, gates, seconds, seed):
         used += 1
         if done_s >= seconds:
             break
-    return {"value": done_cells / done_s / 1e9, "unit": "GCUPS", "cores": threads, "kind": "reference",
+    return {"value": done_cells / done_s / 1e9, "unit": "GCUPS", "cores": threads, "cpu_model": cpu_model(), "kind": "reference",
             "sample": f"{used} of {n} profiles x {len(codes)} records of one step ({surv} survivors), "
                       f"{done_cells:.3e} cells in {done_s:.1f} s: the reference's float filter on every pair, "
                       "then its mid score on the survivors"}
@@ -450,7 +567,7 @@ def cpu_align_baseline(hmm_text, records, gate, seconds):
             done_b += len(chunk)
             done_cells += M1 * sum(len(c) for b in chunk for c in b)
     dt = time.perf_counter() - t0
-    return {"value": done_cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": "reference",
+    return {"value": done_cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "cpu_model": cpu_model(), "kind": "reference",
             "sample": f"{done_b} 8-record batches of one step ({done_cells:.3e} cells) in {dt:.1f} s, reference "
                       "FP32 engine, findSimilarities with needAlign (scores, anchors, traceback)"}
 
@@ -627,7 +744,7 @@ def cpu_windows_baseline(genome, windows, names, seconds):
             nt += sum(n for n, _ in pool.map(R.read_decode, batch))
             done += len(batch)
     dt = time.perf_counter() - t0
-    return {"value": nt / dt / 1e9, "unit": "Gnt/s", "cores": threads, "kind": "reference",
+    return {"value": nt / dt / 1e9, "unit": "Gnt/s", "cores": threads, "cpu_model": cpu_model(), "kind": "reference",
             "sample": f"{done} chunks of 64 windowed FASTA records ({nt} nt; the first {len(texts)} windows, "
                       f"cycled) for {dt:.1f} s: the reference's readContig + decodeSequence (PIPELINE_MODE build, "
                       f"oracle/_ref), {threads} threads; bedtools getfasta's own time not counted"}
@@ -698,8 +815,15 @@ def run_windows(args, rank, world, local):
         added.append(ctx.add_windows_raw(w, outs[k]))
     torch.cuda.synchronize()
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
-    # one 40-byte descriptor per sequence (counted after the timed region)
-    h2d = sum(40 * sum(1 for c in outs[k][:n] if c.seq_id >= 0) for k, n in zip(range(args.warmup, n_steps), added))
+    # one upload per step (counted after the timed region): a 40-byte
+    # descriptor per sequence, then one int per decode block of 256 chunks of
+    # 16 nt (the contig of the block's first chunk).  The upload is a pageable
+    # copy, so it waits for the library stream; that wait is inside e2e.
+    h2d = 0
+    for k, n in zip(range(args.warmup, n_steps), added):
+        seqs = [c for c in outs[k][:n] if c.seq_id >= 0]
+        chunks = sum((c.length + 15) // 16 for c in seqs)
+        h2d += 40 * len(seqs) + 4 * ((chunks + 255) // 256)
     e2e = {"value": nt_all / e2e_s / 1e9, "unit": "Gnt/s", "h2d_bytes_per_step": h2d // args.steps,
            "d2h_bytes_per_step": 0,
            "note": "the step's result (contigs, sequence ids) is host memory; the codes stay on the device"}
@@ -819,14 +943,7 @@ def run_ours(args, rank, world, local):
     Ms = np.array([ctx.profile_length(p) for p in pids])
 
     def pairs_for(sids):
-        n = len(sids) * len(pids)
-        arr = (F.Pair * n)()
-        k = 0
-        for p in pids:
-            for s in sids:
-                arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
-                k += 1
-        return arr
+        return pair_array(sids, pids)
 
     # ---- value: reads resident in HBM ----
     step_sids, step_pairs, step_cells = [], [], []
@@ -884,11 +1001,15 @@ def run_ours(args, rank, world, local):
         account()
     ev1.record(stream)
     torch.cuda.synchronize()
-    exact_pairs = sum(1 for res in results for r in res if r.flags & F.RES_EXACT_PATH)
+    exact_pairs = int(sum(np.count_nonzero(result_view(res)["flags"] & F.RES_EXACT_PATH) for res in results))
     barrier(world)
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     value, ms_max, cells_all = aggregate(cells, ms, world)
+    # ---- parity of the timed results against the reference engine (after the timed region) ----
+    parity = None
+    if rank == 0 and args.parity_pairs > 0:
+        parity = parity_sample(txt, steps, results, args.warmup, args.parity_pairs, args.seed)
 
     # ---- roofline of the DP kernels (CUDA-event durations) ----
     peaks = measured_peaks()
@@ -993,7 +1114,7 @@ def run_ours(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain, "parity": parity,
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
             "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
             "launch": {"cuda_graph": not args.no_graph, "async_submit": not args.no_async, "autotune": tuning},
@@ -1014,13 +1135,7 @@ def run_search(args, rank, world, local):
     Ms = np.array([ctx.profile_length(p) for p in pids])
 
     def pairs_for(sids):
-        arr = (F.Pair * (len(sids) * len(pids)))()
-        k = 0
-        for p in pids:
-            for s in sids:
-                arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
-                k += 1
-        return arr
+        return pair_array(sids, pids)
 
     # untimed: each profile's calibration (the filter wave's lambda and K) and
     # the kernel shapes
@@ -1241,7 +1356,7 @@ def run_autograd(args, rank, world, local):
             n += 1
             if done_s >= args.cpu_seconds:
                 break
-        cb = {"value": done_c / done_s / 1e9, "unit": "GCUPS", "cores": 1, "kind": "port",
+        cb = {"value": done_c / done_s / 1e9, "unit": "GCUPS", "cores": 1, "cpu_model": cpu_model(), "kind": "port",
               "sample": f"{n} reads of the step, {done_c:.3e} cells in {done_s:.1f} s: the oracle's FP64 log T "
                         "(one backward sweep, no gradient: the reference computes none), one core"}
     if rank == 0:

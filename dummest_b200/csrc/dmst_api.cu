@@ -491,6 +491,7 @@ struct dmst_ctx {
     int lastExactPairs = 0;
     int lastLaunches = 0;
     int lastFlagged = 0;  // pairs the last completed mid-score call sent to the exact path
+    int waitLimit = 0;    // exact path: iterations of a stripe wait before it gives up (0: the default)
 
     int fail(int status, const char *fmt, ...) {
         char buf[512];
@@ -1915,7 +1916,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dExactPool.p, poolSlot, S.dExOut.p,
             anchors ? S.dAnchorOff.p : nullptr, S.dAnchorM.p, S.dAnchorE.p, S.dAnchorRow.p,
             align ? ctx->dAlignJobOf.p : nullptr, align ? ctx->dAlignJobs.p : nullptr,
-            align ? ctx->dAlignCells.p : nullptr, align ? ctx->dAlignRows.p : nullptr);
+            align ? ctx->dAlignCells.p : nullptr, align ? ctx->dAlignRows.p : nullptr, ctx->waitLimit);
         CK(cudaGetLastError(), "exact kernel");
         ++launches;
     }
@@ -2612,6 +2613,12 @@ int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, doubl
     return DMST_OK;
 }
 
+int dmst_set_wait_limit(dmst_ctx *ctx, int iterations) {
+    if (!ctx || iterations < 0) return DMST_EINVAL;
+    ctx->waitLimit = iterations;
+    return DMST_OK;
+}
+
 int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcups6) {
     if (!ctx || !sample || n == 0) return DMST_EINVAL;
     for (size_t i = 0; i < n; ++i)
@@ -2987,6 +2994,9 @@ extern "C" int dmst_null_model_noalloc(const uint8_t *codes, int length, const f
     if (!(o.insert1 >= 0 && o.insert1 < 1 && o.insert2 >= 0 && o.insert2 < 1 && o.delete1 >= 0 && o.delete1 < 1 &&
           o.delete2 >= 0 && o.delete2 < 1 && o.insert1 + o.insert2 + o.delete1 + o.delete2 < 1))
         return DMST_EINVAL;
+    // An error left pending by the caller's earlier CUDA work is reported as
+    // it is and left in place for the caller to read (not cleared here).
+    if (cudaPeekAtLastError() != cudaSuccess) return DMST_EDEVICE;
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
         cudaGetLastError();
@@ -3039,9 +3049,10 @@ extern "C" int dmst_null_model_noalloc(const uint8_t *codes, int length, const f
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     naHeaderKernel<<<1, 32, 0, s>>>(h, hdr);
+    if (cudaGetLastError() != cudaSuccess) return DMST_EDEVICE;  // nothing queued
     nullModelKernel<<<1, kNullWarps * 32, 0, s>>>(&hdr->job, 1, &hdr->jobPair, &hdr->pair, &hdr->profile, codes,
                                                   seeds, tmp, &hdr->tmpOff, reinterpret_cast<PairScales *>(scales4),
                                                   nr);
-    if (cudaGetLastError() != cudaSuccess) return DMST_EDEVICE;
+    if (cudaGetLastError() != cudaSuccess) return DMST_EDEVICE;  // the header write alone is queued
     return DMST_OK;
 }

@@ -87,7 +87,7 @@ __device__ void scanCounts(const float *rowMax, const int *rowCnt, int *cnt, int
 
 constexpr int kPipeWarps = 8;        // warps per CTA of the exact path
 constexpr int kPipeExtra = 128;      // stripe period P' = P + kPipeExtra
-constexpr int kPipeSpinLimit = 1 << 24;  // iterations of a wait (64 ns sleeps) before it gives up
+constexpr int kPipeSpinLimit = 1 << 24;  // default iterations of a wait (64 ns sleeps) before it gives up
 static_assert(kPipeExtra >= kLanes - 1 + 2 * kBlock, "a window never reaches the next stripe early");
 
 __host__ __device__ inline int pipePeriod(int L) { return wavePeriod(L) + kPipeExtra; }
@@ -107,6 +107,7 @@ struct PipeSync {
     volatile int *progress;  // [kPipeWarps]: ring-writer position of each warp
     volatile int *abort;     // the CTA's abort flag
     int W;                   // warps running stripes
+    int spinLimit;           // iterations of a wait before it gives up (sets the abort flag)
 };
 
 // Position of this warp's ring-writing lane (local time t0 - 31) at block
@@ -128,7 +129,7 @@ __device__ __forceinline__ bool pipeWaitOne(const PipeSync &ps, int w, int targe
     int it = 0;
     while (ps.progress[w] < target) {
         if (*ps.abort) return false;
-        if (++it > kPipeSpinLimit) {
+        if (++it > ps.spinLimit) {
             *ps.abort = 1;
             return false;
         }
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
                     const PairScales *scales, float *pool, long long slotFloats, ExactOut *out,
                     const long long *anchorOff, float *anchorM, int *anchorE, int *anchorRow,
                     const int *jobOf = nullptr, const AlignJob *jobs = nullptr, float *alignCells = nullptr,
-                    int *alignRows = nullptr) {
+                    int *alignRows = nullptr, int spinLimit = kPipeSpinLimit) {
     static_assert(GROUPS == 1 || GROUPS == 2, "one or two groups");
     constexpr int GW = kPipeWarps / GROUPS;  // warps of a group
     constexpr int GT = GW * kLanes;          // threads of a group
@@ -341,6 +342,7 @@ __global__ void __launch_bounds__(kPipeWarps * kLanes, 1)
     PipeSync ps;
     ps.progress = progress;
     ps.abort = &abortFlag;
+    ps.spinLimit = spinLimit > 0 ? spinLimit : kPipeSpinLimit;
     // Queue positions: with two groups, group g of CTA b first takes position
     // g * gridDim.x + b (so every CTA holds a pair before any holds two, which
     // matters when there are fewer pairs than CTAs), then positions from

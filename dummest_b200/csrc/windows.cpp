@@ -38,7 +38,8 @@ bool isSpaceByte(unsigned char c) { return c == ' ' || (c >= '\t' && c <= '\r');
 
 // Python's int() of a bytes token: an optional sign, then digits with single
 // underscores between them.  False where int() raises ValueError, and for
-// values outside int64 (which int() takes but no genome coordinate reaches).
+// values outside int64 (which int() takes but no genome coordinate reaches):
+// such a row counts as malformed and gives no window.
 bool pyInt(const char *a, const char *b, long long &v) {
     while (a < b && isSpaceByte((unsigned char)*a)) ++a;
     while (b > a && isSpaceByte((unsigned char)b[-1])) --b;
@@ -52,8 +53,10 @@ bool pyInt(const char *a, const char *b, long long &v) {
             continue;
         }
         if (!isdigit((unsigned char)*p)) return false;
-        x = x * 10 + (unsigned)(*p - '0');
-        if (x > (unsigned long long)LLONG_MAX) return false;
+        const unsigned digit = (unsigned)(*p - '0');
+        // checked before the multiply, so that no intermediate wraps past 2^64
+        if (x > ((unsigned long long)LLONG_MAX - digit) / 10) return false;
+        x = x * 10 + digit;
     }
     v = neg ? -(long long)x : (long long)x;
     return true;

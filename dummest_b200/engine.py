@@ -451,6 +451,10 @@ class Context:
         self._check(self.lib.dmst_autotune(self.h, pairs, n, out), "dmst_autotune")
         return {(r, w): out[i * 2 + j] for i, r in enumerate((4, 2, 1)) for j, w in enumerate((16, 8))}
 
+    def set_wait_limit(self, iterations: int = 0) -> None:
+        """The exact path's wait budget in 64 ns sleeps (dmst_set_wait_limit; 0: the default)."""
+        self._check(self.lib.dmst_set_wait_limit(self.h, int(iterations)), "dmst_set_wait_limit")
+
     def tuned_shape(self, M: int) -> tuple[int, int]:
         r, w = C.c_int(), C.c_int()
         self._check(self.lib.dmst_tuned_shape(self.h, M, C.byref(r), C.byref(w)), "dmst_tuned_shape")

@@ -42,6 +42,13 @@ class SynthProfile:
         self.name = name
         self.match = match  # (M, 20)
         self.insert = match.mean(axis=0)
+        # Cumulative rows for draws by inverse transform: searchsorted of one
+        # uniform double in the normalised cdf, the same draw and index that
+        # Generator.choice(20, p=row) makes, without its per-call checks.
+        cdf = np.cumsum(match, axis=1)
+        self.match_cdf = cdf / cdf[:, -1:]
+        icdf = np.cumsum(self.insert)
+        self.insert_cdf = icdf / icdf[-1]
 
     @property
     def M(self) -> int:
@@ -92,9 +99,12 @@ def hmmer3_text(profiles: list[SynthProfile]) -> str:
     return "".join(out)
 
 
+_ACGT = np.frombuffer(b"ACGT", np.uint8)
+
+
 def random_dna(rng: np.random.Generator, L: int, gc: float = 0.5) -> str:
     p = np.array([(1 - gc) / 2, gc / 2, gc / 2, (1 - gc) / 2])
-    return "".join(np.array(list("ACGT"))[rng.choice(4, size=L, p=p)])
+    return _ACGT[rng.choice(4, size=L, p=p)].tobytes().decode()
 
 
 def sample_homolog(rng: np.random.Generator, pr: SynthProfile, max_aa: int, fs_rate: float = 0.005) -> str:
@@ -107,12 +117,12 @@ def sample_homolog(rng: np.random.Generator, pr: SynthProfile, max_aa: int, fs_r
     k = start
     while k < start + length:
         if state == "M":
-            aas.append(AA[rng.choice(20, p=pr.match[k])])
+            aas.append(AA[int(pr.match_cdf[k].searchsorted(rng.random(), side="right"))])
             r = rng.random()
             state = "M" if r < T_MM else ("I" if r < T_MM + T_MI else "D")
             k += 1
         elif state == "I":
-            aas.append(AA[rng.choice(20, p=pr.insert)])
+            aas.append(AA[int(pr.insert_cdf.searchsorted(rng.random(), side="right"))])
             state = "I" if rng.random() < T_II else "M"
         else:
             k += 1

@@ -450,6 +450,16 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
 /* The shape a call would use for a profile of length M. */
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta);
 
+/* The exact path's wait budget: a warp of the stripe-pipelined exact kernel
+ * that waits for the stripe before its own (a flag in shared memory) gives up
+ * after this many 64 ns sleeps, marks its pair failed and lets the CTA's
+ * other warps leave at their next block; the call then returns DMST_ETIMEOUT
+ * and the context stays usable.  iterations = 0 restores the default (2^24,
+ * about a second); a small value makes a call with multi-stripe exact-path
+ * pairs time out on purpose (the test of the timeout path).  No counterpart
+ * in the reference (its threads never wait on one another inside a pair). */
+int dmst_set_wait_limit(dmst_ctx *ctx, int iterations);
+
 /* Column checkpointing of the adjoint's forward pass (dmst_loglik_grad,
  * dmst_posteriors): DMST_ADJ_CKPT_ON keeps the stripes' top rows and a
  * checkpoint every 64 columns and recomputes the forward blocks in the
@@ -527,9 +537,14 @@ int dmst_null_model(dmst_ctx *ctx, int seq, int profile, float *prefix_seed, flo
  * start at zero: the call writes every word it later reads.  Calls on one
  * device share the one scratch array, so calls whose work can overlap (two
  * streams, or two host threads) race; order them on one stream or wait for
- * the previous call's work.  Returns DMST_EINVAL for a null pointer, a length
- * below 1 or invalid rates, DMST_ERANGE beyond the maximum, DMST_EDEVICE for
- * a CUDA error (including set-up and launch). */
+ * the previous call's work.  The scratch address found at set-up is kept for
+ * the life of the process: after cudaDeviceReset (or anything else that
+ * destroys and recreates the device's primary context) it is stale, so do not
+ * call this entry point again in that process.  Returns DMST_EINVAL for a null
+ * pointer, a length below 1 or invalid rates, DMST_ERANGE beyond the maximum,
+ * DMST_EDEVICE for a CUDA error (including set-up and launch).  An error
+ * already pending from the caller's earlier CUDA work is reported as
+ * DMST_EDEVICE before anything is queued, and is not cleared. */
 #define DMST_NOALLOC_MAX_LEN 16384
 int dmst_null_model_noalloc(const uint8_t *codes, int length, const float *bg, const dmst_opts *opts,
                             float *seeds, float *scales4, void *stream);

@@ -26,8 +26,12 @@ def available(bits: int = 32) -> bool:
     return os.path.exists(LIBS[bits])
 
 
-def build(reference: str = "/root/reference") -> None:
+def build(reference: str | None = None) -> None:
     """Compile the oracle (needs the reference sources; not available on the GPU box)."""
+    from oracle import reference_dir
+    reference = reference or reference_dir()
+    if reference is None:
+        raise RuntimeError("reference sources not found: set DMST_REFERENCE")
     subprocess.run(["make", "-C", HERE, f"REF={reference}", "-j4", "all"], check=True, capture_output=True)
 
 

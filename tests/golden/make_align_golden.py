@@ -41,6 +41,7 @@ sys.path.insert(0, ROOT)
 
 import dummest_b200 as d  # noqa: E402
 from dummest_b200 import synth  # noqa: E402
+from oracle import reference_dir  # noqa: E402
 from oracle.ref import RefEngine  # noqa: E402
 
 
@@ -67,7 +68,8 @@ def run(e: RefEngine, p: int, codes: list, mprs: list) -> list:
     return alone
 
 
-def main(ref_root: str = "/root/reference"):
+def main(ref_root: str | None = None):
+    ref_root = ref_root or reference_dir()
     e = RefEngine(32)
     e.set_rates()
     g = dict(np.load(os.path.join(HERE, "regression.npz")))

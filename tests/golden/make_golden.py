@@ -24,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle import reference_dir  # noqa: E402
 from oracle.ref import RefEngine  # noqa: E402
 
 COMP = str.maketrans("ACGTacgt", "TGCAtgca")
@@ -44,7 +45,8 @@ def read_fasta(path):
     return seqs
 
 
-def main(ref_root: str = "/root/reference"):
+def main(ref_root: str | None = None):
+    ref_root = ref_root or reference_dir()
     fx = os.path.join(ref_root, "tests", "fixtures")
     out = {}
     engines = {32: RefEngine(32), 64: RefEngine(64)}

@@ -47,6 +47,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
+from oracle import reference_dir  # noqa: E402
 from oracle import windows as W  # noqa: E402
 
 
@@ -164,7 +165,8 @@ def run_stage(mod, genome: bytes, hits: bytes, dna_lens, hmm_lens, contig: bool)
     return bed.getvalue(), malformed, kept, skipped, out.getvalue()
 
 
-def main(reference: str = "/root/reference") -> None:
+def main(reference: str | None = None) -> None:
+    reference = reference or reference_dir()
     mod = load_pipeline(reference)
     rng = np.random.default_rng(2024)
     genome = make_genome(rng)

@@ -15,9 +15,10 @@ import pytest
 
 import dummest_b200 as d
 from dummest_b200 import _ffi as F
+from oracle import reference_dir
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "windows.npz")
-REFERENCE = "/root/reference"
+REFERENCE = reference_dir() or ""
 
 
 @pytest.fixture(scope="module")
@@ -182,6 +183,30 @@ def test_coordinates_read_as_python_int():
         rows.append("\t".join(f) + "\n")
     wins, malformed, dropped = d.windows_from_hits("".join(rows).encode("utf-8"), ["r1"], [10**12], ["P"], [10])
     assert malformed == want and want > 50
+
+
+def test_coordinates_outside_int64_are_malformed():
+    """Coordinates past int64 (which int() would take, but no genome
+    coordinate reaches) make the row malformed: it gives no window, and no
+    digit string wraps around to a valid-looking coordinate."""
+    f = ["P", "r1_frame=+1", "50", "90", "9", "0", "1", "30", "40", "41", "1e-9", "77.0"]
+    ok = "\t".join(f) + "\n"
+    rows = [ok]
+    for tok in ["20000000000000000000", "9223372036854775808", "-9223372036854775809",
+                "18446744073709551616" + "7" * 5, "9_223_372_036_854_775_808"]:
+        for field in (6, 8, 9):
+            g = list(f)
+            g[field] = tok
+            rows.append("\t".join(g) + "\n")
+    wins, malformed, dropped = d.windows_from_hits("".join(rows).encode(), ["r1"], [10**6], ["P"], [10])
+    assert malformed == len(rows) - 1
+    single, m1, _ = d.windows_from_hits(ok.encode(), ["r1"], [10**6], ["P"], [10])
+    assert m1 == 0 and len(wins) == len(single)
+    # the largest int64 itself is a number (here in the query start field, which no window uses)
+    g = list(f)
+    g[6] = "9223372036854775807"
+    _, m2, _ = d.windows_from_hits(("\t".join(g) + "\n").encode(), ["r1"], [10**6], ["P"], [10])
+    assert m2 == 0
 
 
 @pytest.mark.parametrize("mode", ["frame", "contig"])
