@@ -73,7 +73,8 @@ def parse():
     ap.add_argument("--lmax", type=int, default=3000,
                     help="longest read of the batched workload (3000 in the stated configuration; smaller "
                          "values only to keep a profiling capture's device memory small)")
-    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align", "windows"],
+    ap.add_argument("--workload", choices=["batched", "genome", "autograd", "search", "align", "windows",
+                                           "calibration"],
                     default="batched",
                     help="batched: 64 profiles x reads (the headline); genome: one M=2000 profile against a "
                          "10 Mbp genome in 10 kb windows; autograd: log-likelihood + gradient of an M=400 "
@@ -81,7 +82,12 @@ def parse():
                          "batched pairs through the two-wave search (filter, then mid on survivors); align: "
                          "the hit path with its traceback (an M=400 profile against homolog-carrying reads, "
                          "both strands, the hits' alignments traced); windows: the prefilter's hit windows "
-                         "cut from a resident 256 Mbp genome and decoded on the device")
+                         "cut from a resident 256 Mbp genome and decoded on the device; calibration: the Gumbel "
+                         "calibration batch, 500 profiles (M uniform 50-1500) x 200 i.i.d. uniform ACGT "
+                         "sequences of 3000 nt each, mid scores and the FP64 fits")
+    ap.add_argument("--cal-profiles", type=int, default=500, help="calibration workload: profiles")
+    ap.add_argument("--cal-trials", type=int, default=200, help="calibration workload: sequences per profile")
+    ap.add_argument("--cal-len", type=int, default=3000, help="calibration workload: sequence length")
     ap.add_argument("--win-mbp", type=int, default=256, help="windows workload: genome size (Mbp)")
     ap.add_argument("--win-hits", type=int, default=60000, help="windows workload: hit rows per step")
     ap.add_argument("--al-reads", type=int, default=256, help="align workload: reads per step (x2 strands)")
@@ -207,6 +213,15 @@ def workload_config(args, world: int) -> dict:
                   "kernel-timed launch",
             "parallelism": f"replicas x{world} (one genome per rank)",
         }
+    if args.workload == "calibration":
+        return {
+            "workload": f"Gumbel calibration batch: {args.cal_profiles} profiles M uniform 50-1500 x "
+                        f"{args.cal_trials} i.i.d. uniform ACGT sequences of {args.cal_len} nt per profile, mid "
+                        "scores (fwd+bwd) in one call, lambda/K fitted on the host in FP64 (estimateGumbel)",
+            "profiles": args.cal_profiles, "pairs_per_step": args.cal_profiles * args.cal_trials,
+            "l2": "inputs larger than L2 (W1 slots)",
+            "parallelism": f"replicas x{world}",
+        }
     if args.workload == "genome":
         return {
             "workload": "long-profile genome scan: 1 profile M=2000 x a 10 Mbp synthetic genome (GC 0.45, "
@@ -232,13 +247,17 @@ def make_profiles(seed, n):
     return profiles, synth.hmmer3_text(profiles)
 
 
-def make_workload(args, rank: int, n_steps: int):
+def make_workload(args, rank: int, n_steps: int, world: int = 0):
     """(profiles, HMMER3 text, steps): each step a list of records scored
-    against every profile."""
+    against every profile.  With world >= 1 (the batched workload sharded
+    over `world` ranks) every rank builds the same read sets, world x
+    reads_per_step reads each: n_steps distinct sets at one rank, else enough
+    to cover the configuration's 100,000 reads (the steps cycle through
+    them); world = 0 gives each rank its own reads."""
     if args.workload == "genome":
         from dummest_b200 import synth
         prof, windows = synth.genome_scan_config(seed=rank_seed(args.seed, rank))
-        return [prof], synth.hmmer3_text([prof]), [windows] * n_steps
+        return [prof], synth.hmmer3_text([prof]), [windows] * (1 if world >= 1 else n_steps)
     if args.workload == "align":
         from dummest_b200 import synth
         rng = np.random.default_rng(args.seed)
@@ -251,6 +270,10 @@ def make_workload(args, rank: int, n_steps: int):
             steps.append(synth.both_strands(reads))
         return [prof], synth.hmmer3_text([prof]), steps
     profiles, txt = make_profiles(args.seed, args.profiles)
+    if world >= 1:
+        per = world * args.reads_per_step
+        n_sets = n_steps if world == 1 else min(n_steps, args.warmup + -(-100_000 // per))
+        return profiles, txt, make_steps(rank_seed(args.seed, 0), profiles, n_sets, per, args.lmax)
     return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step, args.lmax)
 
 
@@ -264,9 +287,7 @@ def make_steps(seed, profiles, n_steps, reads_per_step, lmax=3000):
     return steps
 
 
-PAIR_DTYPE = np.dtype([("seq", "<i4"), ("profile", "<i4"), ("min_prob_ratio", "<f4")])
-RESULT_DTYPE = np.dtype([("mid_m", "<f4"), ("mid_e", "<i4"), ("flt_m", "<f4"), ("flt_e", "<i4"),
-                         ("mid_ln", "<f8"), ("flt_ln", "<f8"), ("filter_f", "<f4"), ("flags", "<i4")])
+from dummest_b200.shards import PAIR_DTYPE, RESULT_DTYPE  # noqa: E402
 
 
 def pair_array(sids, pids, min_prob_ratio=-2.0):
@@ -287,19 +308,22 @@ def pair_array(sids, pids, min_prob_ratio=-2.0):
 
 
 def result_view(res) -> np.ndarray:
-    """A ctypes dmst_result array as a numpy structured array (no copy)."""
+    """A ctypes dmst_result array as a numpy structured array (no copy);
+    numpy result arrays pass through."""
     from dummest_b200 import _ffi as F
+    if isinstance(res, np.ndarray):
+        return res
     assert F.C.sizeof(F.Result) == RESULT_DTYPE.itemsize
     return np.frombuffer(res, dtype=RESULT_DTYPE)
 
 
-def parity_sample(hmm_text, steps, results, first_step, n_sample, seed):
-    """Scores a seeded sample of the timed steps' pairs with the reference
-    engine (oracle/_ref, FP32 findSimilarities needAlign=false) and compares
-    them with the results the timed calls returned: mid and filter ExpScores
-    bit for bit.  The sample holds n_sample random pairs plus, for every
-    timed step, its longest record against its longest profile.  results[i]
-    belongs to steps[first_step + i]; pairs are profile-major."""
+def parity_sample(hmm_text, checked_steps, n_sample, seed):
+    """Scores a seeded sample of timed pairs with the reference engine
+    (oracle/_ref, FP32 findSimilarities needAlign=false) and compares them
+    with the results the timed calls returned: mid and filter ExpScores bit
+    for bit.  checked_steps: (records, results) of timed steps, results in
+    profile-major pair order.  The sample holds n_sample random pairs plus,
+    for every step, its longest record against its longest profile."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle.ref import RefEngine, available
     if not available(32):
@@ -314,37 +338,29 @@ def parity_sample(hmm_text, steps, results, first_step, n_sample, seed):
     Ms = np.array([e.profile(p)[1].shape[0] - 1 for p in range(n_prof)])
     rng = np.random.default_rng(seed + 77)
     picks = set()
-    for i in range(len(results)):
-        recs = steps[first_step + i]
+    for i, (recs, _) in enumerate(checked_steps):
         picks.add((i, int(np.argmax(Ms)), int(np.argmax([len(r) for r in recs]))))
-    n_rec = len(steps[first_step])
-    while len(picks) < n_sample + len(results):
-        i = int(rng.integers(0, len(results)))
-        picks.add((i, int(rng.integers(0, n_prof)), int(rng.integers(0, len(steps[first_step + i])))))
-    picks = sorted(picks, key=lambda t: (t[1], t[0], t[2]))
+    while len(picks) < n_sample + len(checked_steps):
+        i = int(rng.integers(0, len(checked_steps)))
+        picks.add((i, int(rng.integers(0, n_prof)), int(rng.integers(0, len(checked_steps[i][0])))))
     by_prof = {}
-    for t in picks:
+    for t in sorted(picks, key=lambda t: (t[1], t[0], t[2])):
         by_prof.setdefault(t[1], []).append(t)
-    jobs = []
-    for p, lst in by_prof.items():
-        for b in range(0, len(lst), e.width):
-            jobs.append((p, lst[b:b + e.width]))
+    jobs = [(p, lst[b:b + e.width]) for p, lst in by_prof.items() for b in range(0, len(lst), e.width)]
 
     def run(job):
         p, lst = job
-        codes = [e.decode(e.encode(steps[first_step + i][r])) for i, _, r in lst]
+        codes = [e.decode(e.encode(checked_steps[i][0][r])) for i, _, r in lst]
         return job, e.find_similarities(p, codes)
 
     t0 = time.perf_counter()
     checked = equal = 0
-    worst = 0.0
-    cells = 0.0
-    largest = (0, 0)
+    worst, cells, largest = 0.0, 0.0, (0, 0)
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
         for (p, lst), refs in ex.map(run, jobs):
             for (i, _, r), (mm, me, ml, fm, fe) in zip(lst, refs):
-                n_r = len(steps[first_step + i])
-                got = result_view(results[i])[p * n_r + r]
+                recs, res = checked_steps[i]
+                got = result_view(res)[p * len(recs) + r]
                 same = (np.float32(got["mid_m"]) == np.float32(mm) and int(got["mid_e"]) == me
                         and np.float32(got["flt_m"]) == np.float32(fm) and int(got["flt_e"]) == fe)
                 checked += 1
@@ -353,13 +369,12 @@ def parity_sample(hmm_text, steps, results, first_step, n_sample, seed):
                     worst = max(worst, abs(float(got["mid_ln"]) - ml) / np.log(2.0))
                 elif not (np.isinf(ml) and np.isinf(got["mid_ln"])):
                     worst = float("inf")
-                L = len(steps[first_step + i][r])
-                cells += (Ms[p] + 1) * L
-                largest = max(largest, (int(Ms[p]), L))
+                cells += (Ms[p] + 1) * len(recs[r])
+                largest = max(largest, (int(Ms[p]), len(recs[r])))
+    lmax = max(len(r) for recs, _ in checked_steps for r in recs)
     return {"checked": checked, "bit_equal": equal, "max_abs_bits": worst,
-            "sample": f"{n_sample} seeded random pairs of the {len(results)} timed steps plus each step's "
-                      f"longest record x longest profile (M={largest[0]}, L up to "
-                      f"{max(len(r) for st in steps[first_step:first_step + len(results)] for r in st)}); "
+            "sample": f"{n_sample} seeded random pairs of {len(checked_steps)} timed steps (every 4th) plus each "
+                      f"step's longest record x longest profile (M={largest[0]}, L up to {lmax}); "
                       f"{cells:.3e} cells, reference FP32 engine, {time.perf_counter() - t0:.1f} s",
             "compared": "mid and filter ExpScore (mantissa, exponent) of the timed calls' results"}
 
@@ -842,6 +857,213 @@ def run_windows(args, rank, world, local):
     ctx.close()
 
 
+def calibration_problem(args, rank):
+    """(profiles, HMMER3 text, sequences) of the calibration batch: profile p
+    is scored against sequences[p * trials : (p + 1) * trials]."""
+    from dummest_b200 import synth
+    rng = np.random.default_rng(rank_seed(args.seed + 3, rank))
+    Ms = rng.integers(50, 1501, size=args.cal_profiles)
+    profiles = [synth.make_profile(rng, int(M), f"cal{k:03d}") for k, M in enumerate(Ms)]
+    seqs = [synth.random_dna(rng, args.cal_len, 0.5) for _ in range(args.cal_profiles * args.cal_trials)]
+    return profiles, synth.hmmer3_text(profiles), seqs
+
+
+def _ref_engine(hmm_text):
+    from oracle.ref import RefEngine, available
+    if not available(32):
+        return None
+    e = RefEngine(32)
+    e.set_rates()
+    with tempfile.NamedTemporaryFile("w", suffix=".hmm", delete=False) as f:
+        f.write(hmm_text)
+        path = f.name
+    e.load_profiles(path)
+    os.unlink(path)
+    return e
+
+
+def cpu_calibration_baseline(hmm_text, seqs, trials, seconds, seed):
+    """The reference engine on a bounded sample of the calibration batch:
+    whole profiles (their trials, findSimilarities needAlign=false on all
+    host threads) in random order until the time budget is spent."""
+    e = _ref_engine(hmm_text)
+    if e is None:
+        return None
+    threads = os.cpu_count() or 1
+    n = len(seqs) // trials
+    Ms = [e.profile(p)[1].shape[0] for p in range(n)]
+    rng = np.random.default_rng(seed)
+    done_cells, done_s, used = 0.0, 0.0, 0
+    for p in rng.permutation(n):
+        codes = [e.decode(e.encode(s)) for s in seqs[p * trials:(p + 1) * trials]]
+        t = time.perf_counter()
+        e.score_many(int(p), codes, threads=threads, mode=0)
+        done_s += time.perf_counter() - t
+        done_cells += Ms[p] * float(sum(len(c) for c in codes))
+        used += 1
+        if done_s >= seconds:
+            break
+    return {"value": done_cells / done_s / 1e9, "unit": "GCUPS", "cores": threads, "cpu_model": cpu_model(),
+            "kind": "reference",
+            "sample": f"{used} of {n} profiles x {trials} sequences, {done_cells:.3e} cells in {done_s:.1f} s, "
+                      "reference FP32 engine (the calibration call, findSimilarities needAlign=false)"}
+
+
+def calibration_parity(hmm_text, seqs, trials, Ms, res, seq_len):
+    """Three profiles of the batch (the longest, the median and the shortest)
+    re-scored by the reference engine: trial ln-scores compared bit for bit,
+    and the E-values of the two FP64 fits (estimateGumbel) compared over the
+    range from the median score to 60 bits above it."""
+    import dummest_b200 as d
+    e = _ref_engine(hmm_text)
+    if e is None:
+        return None
+    order = np.argsort(Ms, kind="stable")
+    picks = sorted({int(order[-1]), int(order[len(order) // 2]), int(order[0])})
+    checked = equal = 0
+    worst_e = 0.0
+    t0 = time.perf_counter()
+    for p in picks:
+        codes = [e.decode(e.encode(s)) for s in seqs[p * trials:(p + 1) * trials]]
+        rm, rf = e.score_many(p, codes, threads=os.cpu_count() or 1, mode=0)
+        got = res[p * trials:(p + 1) * trials]
+        checked += 2 * trials
+        equal += int(np.sum(got["mid_ln"] == rm)) + int(np.sum(got["flt_ln"] == rf))
+        for ours, theirs in ((got["mid_ln"], rm), (got["flt_ln"], rf)):
+            g, w = d.estimate_gumbel(ours, seq_len), e.estimate_gumbel(theirs, seq_len)
+            s_nats = np.linspace(np.median(theirs), np.median(theirs) + 60 * np.log(2.0), 31)
+            ratio = (g[1] * np.exp(-g[0] * s_nats)) / (w[1] * np.exp(-w[0] * s_nats))
+            worst_e = max(worst_e, float(np.max(np.abs(ratio - 1.0))))
+    return {"checked": checked, "bit_equal": equal, "max_evalue_rel_err": worst_e,
+            "sample": f"profiles M={[int(Ms[p]) for p in picks]}, {trials} sequences each, mid and filter "
+                      f"ln-scores; reference FP32 engine, {time.perf_counter() - t0:.1f} s"}
+
+
+def run_calibration(args, rank, world, local):
+    import dummest_b200 as d
+    from dummest_b200 import _ffi as F
+    import torch
+
+    profiles, txt, seqs = calibration_problem(args, rank)
+    T, n_steps = args.cal_trials, args.warmup + args.steps
+    ctx = d.Context(device=local, rows_per_lane=args.rows_per_lane)
+    pids = ctx.load_hmm(txt)
+    Ms = np.array([ctx.profile_length(p) for p in pids])
+
+    def pairs_for(sids):
+        arr = np.zeros(len(sids), PAIR_DTYPE)
+        arr["seq"] = sids
+        arr["profile"] = np.repeat(np.asarray(pids, np.int32), T)
+        arr["min_prob_ratio"] = -2.0
+        out = (F.Pair * len(arr)).from_buffer(arr)
+        out._keep = arr
+        return out
+
+    def fit_all(res):
+        """FP64 lambda and K of every profile (mid, then filter scores)."""
+        r = result_view(res)
+        fits = np.zeros((len(pids), 4))
+        for p in range(len(pids)):
+            sl = slice(p * T, (p + 1) * T)
+            fits[p, 0:2] = d.estimate_gumbel(r["mid_ln"][sl], args.cal_len)[:2]
+            fits[p, 2:4] = d.estimate_gumbel(r["flt_ln"][sl], args.cal_len)[:2]
+        return fits
+
+    sids = ctx.add_dna(seqs)
+    pairs = pairs_for(sids)
+    cells = float(args.cal_len) * float((Ms + 1).sum()) * T
+    stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
+    tuning = None
+    if not args.no_autotune and args.rows_per_lane == 0:
+        samp = [k for p in range(len(pids)) for k in range(p * T, p * T + 8)]
+        rates = ctx.autotune([sids[k] for k in samp], [pids[k // T] for k in samp])
+        tuning = {"gcups_computed_cells": {f"R{r}/W{w}": round(v, 2) for (r, w), v in rates.items()}}
+    MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
+    for _ in range(args.warmup):
+        ctx.score_pairs_raw(pairs, MODE)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    launches, dp_ms, last = 0, 0.0, None
+    for k in range(args.steps):
+        ctx.submit_raw(pairs, MODE)
+        if k > 0:
+            last = ctx.complete()
+            t = ctx.last_timing()
+            launches += t["launches"]
+            dp_ms += t["dp_ms"]
+    last = ctx.complete()
+    t = ctx.last_timing()
+    launches += t["launches"]
+    dp_ms += t["dp_ms"]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    value, ms_max, cells_all = aggregate(cells * args.steps, ms, world)
+    res = result_view(last).copy()
+    fits = fit_all(res)
+    parity = calibration_parity(txt, seqs, T, Ms, res, args.cal_len) if rank == 0 and args.parity_pairs > 0 else None
+
+    peaks = measured_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = n_sm * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = cells * args.steps * FLOPS_PER_CELL / (dp_ms / 1e3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": f"derived: {n_sm} SMs x 128 FP32 lanes x 2 x sm_max_mhz {sm_max:g} (of measured "
+                               "clock; MEASURED_PEAKS.json has no FP32 figure)",
+                "kernel": "dpKernel (mid), CUDA events on the library stream, per step",
+                "algorithmic_flops_per_cell": FLOPS_PER_CELL}
+
+    # e2e: each step copies the batch's sequences (2-bit packed) from host
+    # memory, scores, copies the results back and fits every profile (FP64)
+    words, mask, lens = d.pack_dna(seqs)
+    ctx.clear_sequences()
+    base = 0
+    step_pairs = []
+    for k in range(args.warmup + args.steps):
+        step_pairs.append(pairs_for(list(range(base, base + len(seqs)))))
+        base += len(seqs)
+    for k in range(args.warmup):
+        ctx.add_packed(words, lens, mask)
+        ctx.score_pairs_raw(step_pairs[k], MODE)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.warmup, n_steps):
+        ctx.add_packed(words, lens, mask)
+        ctx.submit_raw(step_pairs[k], MODE)
+        if k > args.warmup:
+            fit_all(ctx.complete())
+    fit_all(ctx.complete())
+    torch.cuda.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world)
+    h2d = words.nbytes + mask.nbytes + 12 * len(lens) + 40 * len(seqs)
+    e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": 40 * len(seqs), "note": "includes the FP64 fits of every profile on the host"}
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_calibration_baseline(txt, seqs, T, args.cpu_seconds, args.seed)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "calibration batch fwd+bwd GCUPS (mid scores of every trial)", "value": value, "unit": "GCUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(workload_config(args, world), cells_per_step=cells),
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "parity": parity,
+            "fits": {"lambda_median": float(np.median(fits[:, 0])), "K_median": float(np.median(fits[:, 1])),
+                     "lambda_filter_median": float(np.median(fits[:, 2]))},
+            "gpu_launches": launches, "clocks": clk, "dp_ms_per_step": dp_ms / args.steps,
+            "launch": {"cuda_graph": not args.no_graph, "async_submit": True, "autotune": tuning}}), flush=True)
+    ctx.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -862,6 +1084,22 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": workload_config(args, world), "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "Gnt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    if args.workload == "calibration":
+        profiles, txt, seqs = calibration_problem(args, 0)
+        vals, cb = [], None
+        per_step = max(args.cpu_seconds / max(args.steps, 1), 2.0)
+        for k in range(args.warmup + args.steps):
+            cb = cpu_calibration_baseline(txt, seqs, args.cal_trials, per_step, args.seed + k)
+            vals.append(cb["value"])
+        v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else vals[-1]
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": "calibration batch fwd+bwd GCUPS (mid scores of every trial)",
+            "value": v, "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(args, world), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
         return
     profiles, txt, steps = make_workload(args, 0, 1)
     if args.workload == "align":
@@ -931,87 +1169,157 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def genome_posterior_pass(ctx, sids, pid, windows, res, scan_ms):
+    """The posterior pass of the genome scan: the windows whose mid score
+    passes the hit gate minProbRatio = (K N / E)^(1/lambda) (dummest.cc:583-587,
+    lambda and K from the profile's calibration, untimed; N the scanned
+    length, E = 10) through dmst_posterior_summary (FP64 adjoint with the
+    posterior tables reduced on the device), timed on its own."""
+    import torch
+    fit = ctx.estimate_k(pid, sequence_length=3000, border=100, trials=200)
+    n_tot = float(sum(len(w) for w in windows))
+    gate_ln = (np.log(fit["K"]) + np.log(n_tot) - np.log(SEARCH_E)) / fit["lambda"]
+    above = np.nonzero(result_view(res)["mid_ln"] >= gate_ln)[0]
+    if len(above) == 0:
+        return {"windows_above": 0, "gate_bits": gate_ln / np.log(2.0)}
+    M = ctx.profile_length(pid)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    logt, summ = ctx.posterior_summary([sids[k] for k in above], pid)
+    wall = (time.perf_counter() - t0) * 1e3
+    t = ctx.last_timing()
+    cells = float(sum(len(windows[k]) for k in above)) * (M + 1)
+    return {"windows_above": int(len(above)), "windows": len(windows), "gate_bits": gate_ln / np.log(2.0),
+            "cells": cells, "wall_ms": wall, "adjoint_ms": t["dp_ms"], "null_ms": t["null_ms"],
+            "gcups": cells / (wall / 1e3) / 1e9, "scan_plus_posterior_ms": scan_ms + wall,
+            "output": "per window: column track of the largest cell posterior and its row, row sums of the match "
+                      "posteriors (FP64; tables reduced on the device)"}
+
+
 def run_ours(args, rank, world, local):
     import dummest_b200 as d
     from dummest_b200 import _ffi as F
+    from dummest_b200 import shards
     import torch
 
     n_steps = args.warmup + args.steps
-    profiles, txt, steps = make_workload(args, rank, n_steps)
+    profiles, txt, sets = make_workload(args, rank, n_steps, world)
+    # Step k scores read set k mod len(sets): every set is distinct at one GPU
+    # (20 timed steps of 5,000 reads are the configuration's 100,000 reads);
+    # with N GPUs a step holds N times the reads, and the sets cycle.
+    step_set = [k % len(sets) for k in range(n_steps)]
+    # Batched pairs shard over the ranks (the cost-sorted pair queue, dealt
+    # by strided interleaving; results gathered); the genome workload runs
+    # one genome per rank.
+    sharded = world > 1 and args.workload == "batched"
+    dev = torch.device("cuda", local)
     ctx = d.Context(device=local, rows_per_lane=args.rows_per_lane)
     pids = ctx.load_hmm(txt)
     Ms = np.array([ctx.profile_length(p) for p in pids])
 
-    def pairs_for(sids):
-        return pair_array(sids, pids)
+    def shares_of(recs):
+        """Every rank's pair indices (profile-major pair order) and this rank's cells."""
+        lens = np.array([len(r) for r in recs], np.int64)
+        if not sharded:
+            return [np.arange(len(lens) * len(pids))], float(lens.sum()) * float((Ms + 1).sum())
+        costs = np.repeat(Ms + 1, len(lens)) * np.tile(lens, len(pids))
+        shares = [shards.shard_indices(costs, world, r) for r in range(world)]
+        return shares, float(costs[shares[rank]].sum())
+
+    def rank_pairs(sids, shares):
+        full = pair_array(sids, pids)
+        if not sharded:
+            return full
+        mine = np.ascontiguousarray(full._keep[shares[rank]])
+        out = (F.Pair * len(mine)).from_buffer(mine)
+        out._keep = mine
+        return out
+
+    def finish(res, si):
+        """A completed call's results: this rank's (one GPU), or every rank's
+        gathered in pair order (NCCL all-gather through device memory)."""
+        if not sharded:
+            return res
+        sh = set_shares[si]
+        return shards.gather_results(result_view(res), sh[rank], n_pairs[si], sh, device=dev)
 
     # ---- value: reads resident in HBM ----
-    step_sids, step_pairs, step_cells = [], [], []
-    for recs in steps:
+    set_sids, set_pairs, set_cells, set_shares, n_pairs = [], [], [], [], []
+    for recs in sets:
         sids = ctx.add_dna(recs)
-        step_sids.append(sids)
-        step_pairs.append(pairs_for(sids))
-        step_cells.append(float(sum(len(r) for r in recs)) * float((Ms + 1).sum()))
+        shares, c = shares_of(recs)
+        set_sids.append(sids)
+        set_shares.append(shares)
+        set_pairs.append(rank_pairs(sids, shares))
+        set_cells.append(c)
+        n_pairs.append(len(sids) * len(pids))
     stream = torch.cuda.ExternalStream(ctx.stream_handle, device=local)
     # Kernel shapes from the autotuner (untimed): every shape on the first
     # (warm-up) step's pairs, a sample large enough to fill the GPU.
     tuning = None
     if not args.no_autotune and args.rows_per_lane == 0:
-        samp = step_sids[0]
+        samp = set_sids[0][:2048]
         rates = ctx.autotune([s for _ in pids for s in samp], [p for p in pids for _ in samp])
         shapes = {}
         for M in Ms:
             key = "R%d/W%d" % ctx.tuned_shape(int(M))
             shapes[key] = shapes.get(key, 0) + 1
         tuning = {"gcups_computed_cells": {f"R{r}/W{w}": round(v, 2) for (r, w), v in rates.items()},
-                  "profiles_per_shape": shapes}
+                  "profiles_per_shape": shapes, "sample_pairs": len(samp) * len(pids)}
     MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
     for w in range(args.warmup):
-        ctx.score_pairs_raw(step_pairs[w], MODE)
+        finish(ctx.score_pairs_raw(set_pairs[step_set[w]], MODE), step_set[w])
     barrier(world)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    launches, dp_ms, cells = 0, 0.0, 0.0
-    results = []
+    launches, dp_ms, cells, exact_pairs = 0, 0.0, 0.0, 0
+    kept = []  # (timed step, results) of every 4th timed step, for the parity sample
     parts = {"null_ms": 0.0, "dp_ms": 0.0, "exact_ms": 0.0, "host_ms": 0.0, "post_ms": 0.0, "wall_ms": 0.0}
-    # Calls are submitted one ahead of their completion, so that the host work
-    # of one step overlaps the device work of the previous one.
-    def account():
+
+    def account(res, k):
         t = ctx.last_timing()
-        nonlocal launches, dp_ms
+        nonlocal launches, dp_ms, exact_pairs
         launches += t["launches"]
         dp_ms += t["dp_ms"]
         for key in parts:
             parts[key] += t[key]
+        exact_pairs += int(np.count_nonzero(result_view(res)["flags"] & F.RES_EXACT_PATH))
+        full = finish(res, step_set[k])
+        if (k - args.warmup) % 4 == 0:
+            kept.append((k, full))
+
+    # Calls are submitted one ahead of their completion, so that the host work
+    # of one step overlaps the device work of the previous one.
     for k in range(args.warmup, n_steps):
         if args.no_async:
-            results.append(ctx.score_pairs_raw(step_pairs[k], MODE))
-            account()
+            account(ctx.score_pairs_raw(set_pairs[step_set[k]], MODE), k)
         else:
-            ctx.submit_raw(step_pairs[k], MODE)
+            ctx.submit_raw(set_pairs[step_set[k]], MODE)
             if k > args.warmup:
-                results.append(ctx.complete())
-                account()
-        cells += step_cells[k]
+                account(ctx.complete(), k - 1)
+        cells += set_cells[step_set[k]]
     if not args.no_async:
-        results.append(ctx.complete())
-        account()
+        account(ctx.complete(), n_steps - 1)
     ev1.record(stream)
     torch.cuda.synchronize()
-    exact_pairs = int(sum(np.count_nonzero(result_view(res)["flags"] & F.RES_EXACT_PATH) for res in results))
     barrier(world)
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     value, ms_max, cells_all = aggregate(cells, ms, world)
+    exact_pairs = int(allreduce_sum(float(exact_pairs), world))
     # ---- parity of the timed results against the reference engine (after the timed region) ----
     parity = None
     if rank == 0 and args.parity_pairs > 0:
-        parity = parity_sample(txt, steps, results, args.warmup, args.parity_pairs, args.seed)
+        parity = parity_sample(txt, [(sets[step_set[k]], r) for k, r in kept], args.parity_pairs, args.seed)
+    posterior_pass = None
+    if args.workload == "genome" and rank == 0:
+        posterior_pass = genome_posterior_pass(ctx, set_sids[0], pids[0], sets[0], kept[-1][1], ms_max / args.steps)
+    del kept
 
-    # ---- roofline of the DP kernels (CUDA-event durations) ----
+    # ---- roofline of the DP kernels (CUDA-event durations, this GPU) ----
     peaks = measured_peaks()
     sm_max = peaks.get("sm_max_mhz", 1965.0)
     n_sm = torch.cuda.get_device_properties(local).multi_processor_count
@@ -1032,63 +1340,64 @@ def run_ours(args, rank, world, local):
 
     # ---- e2e: host buffers through the C ABI every step ----
     # Each step's reads are copied from host memory (2-bit packed) and decoded
-    # on the device, scored, and the results copied back; steps are submitted
-    # one ahead of their completion.  The reads of every step are appended
-    # (sequence ids continue), so the pair arrays are built beforehand.
-    packed_of = {}
-    for recs in steps:  # the genome workload repeats one step's records
-        if id(recs) not in packed_of:
-            packed_of[id(recs)] = d.pack_dna(recs)
-    packed = [packed_of[id(recs)] for recs in steps]
+    # on the device, scored, and the results copied back (and, with N GPUs,
+    # gathered); steps are submitted one ahead of their completion.  The reads
+    # of every step are appended (sequence ids continue), so the pair arrays
+    # are built beforehand.
+    packed = [d.pack_dna(recs) for recs in sets]
     ctx.clear_sequences()
     base = 0
     e2e_pairs = []
     for k in range(n_steps):
-        e2e_pairs.append(pairs_for(list(range(base, base + len(steps[k])))))
-        base += len(steps[k])
+        si = step_set[k]
+        e2e_pairs.append(rank_pairs(list(range(base, base + len(sets[si]))), set_shares[si]))
+        base += len(sets[si])
     h2d = d2h = 0
     for w in range(args.warmup):
-        words, mask, lens = packed[w]
+        words, mask, lens = packed[step_set[w]]
         ctx.add_packed(words, lens, mask)
-        if args.no_async:
-            ctx.score_pairs_raw(e2e_pairs[w], MODE)
-        else:
-            ctx.submit_raw(e2e_pairs[w], MODE)
-    while ctx.complete() is not None:
-        pass
+        finish(ctx.score_pairs_raw(e2e_pairs[w], MODE), step_set[w])
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    next_id = sum(len(steps[w]) for w in range(args.warmup))
+    next_id = sum(len(sets[step_set[w]]) for w in range(args.warmup))
     for k in range(args.warmup, n_steps):
-        words, mask, lens = packed[k]
+        si = step_set[k]
+        words, mask, lens = packed[si]
         sids = ctx.add_packed(words, lens, mask)
         assert sids[0] == next_id and len(sids) == len(lens)
         next_id += len(lens)
         pr = e2e_pairs[k]
         if args.no_async:
-            ctx.score_pairs_raw(pr, MODE)
+            finish(ctx.score_pairs_raw(pr, MODE), si)
         else:
             ctx.submit_raw(pr, MODE)
             if k > args.warmup:
-                ctx.complete()
+                finish(ctx.complete(), step_set[k - 1])
         # packed reads + mask + offsets, then the per-pair descriptors the
         # library uploads (32 B pair + 8 B scratch offset) and the per-pair
-        # results it reads back (16 B, and 24 B of exact-path results)
+        # results it reads back (16 B, and 24 B of exact-path results); with
+        # N GPUs also this rank's results up for the all-gather and every
+        # rank's results back down
         h2d += words.nbytes + mask.nbytes + 12 * len(lens) + 40 * len(pr)
         d2h += 40 * len(pr)
-    while ctx.complete() is not None:
-        pass
+        if sharded:
+            h2d += 40 * len(pr)
+            d2h += 40 * n_pairs[si]
+    if not args.no_async:
+        finish(ctx.complete(), step_set[n_steps - 1])
     torch.cuda.synchronize()
     e2e_s = allreduce_max(time.perf_counter() - t0, world)
     e2e = {"value": cells_all / e2e_s / 1e9, "unit": "GCUPS", "h2d_bytes_per_step": h2d // args.steps,
            "d2h_bytes_per_step": d2h // args.steps}
+    if world > 1:
+        e2e["bytes_note"] = "per rank"
 
     # ---- plain schedule on a sample of step pairs ----
     plain = None
     if rank == 0 and args.plain_pairs > 0:
         ctx.clear_sequences()
-        recs = steps[args.warmup]
+        recs = sets[step_set[args.warmup]]
         sids = ctx.add_dna(recs)
         rng = np.random.default_rng(args.seed)
         sel = rng.choice(len(sids) * len(pids), size=min(args.plain_pairs, len(sids) * len(pids)), replace=False)
@@ -1106,15 +1415,18 @@ def run_ours(args, rank, world, local):
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
-        cb = cpu_baseline(txt, steps[args.warmup], len(profiles), args.cpu_seconds, args.seed)
+        cb = cpu_baseline(txt, sets[step_set[args.warmup]][:2 * args.reads_per_step], len(profiles),
+                          args.cpu_seconds, args.seed)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(workload_config(args, world), cells_per_step=cells / args.steps),
+            "config": dict(workload_config(args, world), cells_per_step=cells_all / args.steps,
+                           distinct_read_sets=len(sets)),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "plain": plain, "parity": parity,
+            **({"posterior_pass": posterior_pass} if posterior_pass else {}),
             "gpu_launches": launches, "exact_path_pairs": exact_pairs, "clocks": clk,
             "breakdown_ms_per_step": {k: v / args.steps for k, v in parts.items()},
             "launch": {"cuda_graph": not args.no_graph, "async_submit": not args.no_async, "autotune": tuning},
@@ -1373,8 +1685,23 @@ def run_autograd(args, rank, world, local):
     ctx.close()
 
 
+def relaunch(n: int) -> int:
+    """Runs this command again as n ranks, one process per GPU (torchrun on
+    127.0.0.1); returns the launcher's exit status."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # `bench.py --gpus N` outside a launcher: start the N ranks here
+        sys.exit(relaunch(args.gpus))
     if args.impl == "reference" and args.workload == "autograd":
         rank, _, _ = dist_env()
         if rank == 0:
@@ -1400,6 +1727,8 @@ def main():
             run_align(args, rank, world, local)
         elif args.workload == "windows":
             run_windows(args, rank, world, local)
+        elif args.workload == "calibration":
+            run_calibration(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

@@ -205,6 +205,9 @@ SIGNATURES = [
     ("dmst_autotune", C.c_int, [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double)]),
     ("dmst_tuned_shape", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("dmst_set_wait_limit", C.c_int, [C.c_void_p, C.c_int]),
+    ("dmst_posterior_summary", C.c_int,
+     [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
+      C.POINTER(C.c_double)]),
     ("dmst_null_model_noalloc", C.c_int,
      [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(Opts), C.c_void_p, C.c_void_p, C.c_void_p]),
     ("dmst_estimate_gumbel", C.c_int, [C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double)]),

@@ -5,6 +5,7 @@
 #include "dp_common.cuh"
 #include "dp_exact.cuh"
 #include "dp_adjoint.cuh"
+#include "dp_posterior.cuh"
 #include "dp_exact_wave.cuh"
 #include "dp_search.cuh"
 #include "dp_traceback.cuh"
@@ -462,6 +463,9 @@ struct dmst_ctx {
     int adjCheckpoint = DMST_ADJ_CKPT_AUTO;   // dmst_adjoint_checkpoint
     bool lastAdjCheckpointed = false;
     DevBuf<double> dPost;                    // dmst_posteriors: the batch's posterior tables
+    DevBuf<PostSumJob> dPostJobs;            // dmst_posterior_summary: the batch's reductions
+    DevBuf<double> dColPost, dRowMatch;      // dmst_posterior_summary outputs (the call's pairs)
+    DevBuf<int> dColRow;
     DevBuf<double> dAdjF, dAdjB, dGrad, dLogT;
     std::vector<int> lastOrder;              // sorted position -> caller's pair index of the last call
     CallSlot slot[2];
@@ -675,6 +679,10 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     ctx->dGrad.release();
     ctx->dLogT.release();
     ctx->dPost.release();
+    ctx->dPostJobs.release();
+    ctx->dColPost.release();
+    ctx->dColRow.release();
+    ctx->dRowMatch.release();
     ctx->dExactScratch.release();
     ctx->dExactOut.release();
     ctx->dGenomeWords.release();
@@ -2666,8 +2674,13 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
 // gradient of log T (Params then emissions) and, if post is given, each
 // pair's posterior tables at the offsets of dmst_posteriors.
 static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *grad_params,
-                      double *grad_emit, double *post, const char *what) {
+                      double *grad_emit, double *post, const char *what, double *colPost = nullptr,
+                      int *colRow = nullptr, double *rowMatch = nullptr) {
     if (!ctx || !pairs || n == 0 || (n >> 31)) return DMST_EINVAL;
+    // The kernel writes the posterior tables (device) when the caller wants
+    // them (post, host) or a reduction of them (the summary outputs).
+    const bool summary = colPost || colRow || rowMatch;
+    const bool tables = post || summary;
     const int prof = pairs[0].profile;
     for (size_t i = 0; i < n; ++i)
         if (pairs[i].profile != prof)
@@ -2706,31 +2719,43 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     long long fullAll = 0;
     for (size_t k = 0; k < n; ++k) {
         const int L = ctx->seqLen[pairs[order[k]].seq];
-        fullAll += ((adjStoreDoubles(M, L) + 31) & ~31LL) + adjBoundDoubles(L) + (post ? 2LL * (M + 1) * L : 0);
+        fullAll += ((adjStoreDoubles(M, L) + 31) & ~31LL) + adjBoundDoubles(L) + (tables ? 2LL * (M + 1) * L : 0);
     }
     const bool ckpt = ctx->adjCheckpoint == DMST_ADJ_CKPT_ON ||
                       (ctx->adjCheckpoint == DMST_ADJ_CKPT_AUTO && (size_t)fullAll * 8 > budget);
     ctx->lastAdjCheckpointed = ckpt;
     for (size_t k = 0; k < n; ++k) {
         const int L = ctx->seqLen[pairs[order[k]].seq];
-        jobs[k] = AdjointJob{(int)k, 0, 0, 0, post ? 0 : -1};
+        jobs[k] = AdjointJob{(int)k, 0, 0, 0, tables ? 0 : -1};
         // 256-byte aligned stores (cp.async)
         needF[k] = ((ckpt ? adjCkptDoubles(M, L) : adjStoreDoubles(M, L)) + 31) & ~31LL;
         needB[k] = adjBoundDoubles(L);
-        needP[k] = post ? 2LL * (M + 1) * L : 0;
+        needP[k] = tables ? 2LL * (M + 1) * L : 0;
     }
     const size_t gN = (size_t)(M + 2) * kParamFloats + (size_t)(M + 1) * kNumCodes;
     CK(ctx->dGrad.ensure(gN), "alloc gradient");
     CK(ctx->dLogT.ensure(n), "alloc log T");
     CK(ctx->dAdjJobs.ensure(n), "alloc adjoint jobs");
     CK(cudaMemsetAsync(ctx->dGrad.p, 0, gN * sizeof(double), ctx->stream), "zero gradient");
+    // Summary outputs in the caller's order: pair i's columns at the sum of
+    // the earlier pairs' lengths, its rows at i (M+1).
+    std::vector<long long> colOff(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) colOff[i + 1] = colOff[i] + ctx->seqLen[pairs[i].seq];
+    std::vector<PostSumJob> sumJobs;
+    if (summary) {
+        CK(ctx->dPostJobs.ensure(n), "alloc summary jobs");
+        CK(ctx->dColPost.ensure((size_t)colOff[n]), "alloc column posteriors");
+        CK(ctx->dColRow.ensure((size_t)colOff[n]), "alloc column rows");
+        CK(ctx->dRowMatch.ensure(n * (size_t)(M + 1)), "alloc row sums");
+        sumJobs.resize(n);
+    }
     for (size_t k0 = 0; k0 < n;) {
         size_t k1 = k0;
         long long f = 0, b = 0, pp = 0;
         while (k1 < n && (k1 == k0 || (size_t)(f + needF[k1] + b + needB[k1] + pp + needP[k1]) * 8 <= budget)) {
             jobs[k1].fOff = f;
             jobs[k1].bOff = b;
-            if (post) jobs[k1].pOff = pp;
+            if (tables) jobs[k1].pOff = pp;
             f += needF[k1];
             b += needB[k1];
             pp += needP[k1];
@@ -2739,22 +2764,47 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
         const int nj = (int)(k1 - k0);
         CK(ctx->dAdjF.ensure((size_t)f), "alloc adjoint store");
         CK(ctx->dAdjB.ensure((size_t)b), "alloc adjoint rows");
-        if (post) CK(ctx->dPost.ensure((size_t)std::max<long long>(pp, 1)), "alloc posterior tables");
+        if (tables) CK(ctx->dPost.ensure((size_t)std::max<long long>(pp, 1)), "alloc posterior tables");
         CK(cudaMemcpyAsync(ctx->dAdjJobs.p, jobs.data() + k0, nj * sizeof(AdjointJob), cudaMemcpyHostToDevice,
                            ctx->stream),
            "upload adjoint jobs");
         const int blocks = (nj + kAdjWarps - 1) / kAdjWarps;
-        auto kern = ckpt ? (post ? adjointKernel<true, true> : adjointKernel<false, true>)
-                         : (post ? adjointKernel<true> : adjointKernel<false>);
+        auto kern = ckpt ? (tables ? adjointKernel<true, true> : adjointKernel<false, true>)
+                         : (tables ? adjointKernel<true> : adjointKernel<false>);
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjSmem), "smem attribute");
         CK(cudaEventRecord(ctx->ev[3], ctx->stream), "event");
         kern<<<blocks, kAdjWarps * 32, kAdjSmem, ctx->stream>>>(
             ctx->dAdjJobs.p, nj, S.dPairs.p, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p, ctx->dCodes.p,
             S.dSeeds.p, S.dScales.p, ctx->dAdjF.p, ctx->dAdjB.p, ctx->dGrad.p, ctx->dLogT.p + k0,
-            post ? ctx->dPost.p : nullptr);
+            tables ? ctx->dPost.p : nullptr);
         CK(cudaGetLastError(), "adjoint kernel");
-        CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
         ++launches;
+        if (summary) {
+            int maxL = 0;
+            for (size_t k = k0; k < k1; ++k) {
+                const int ci = order[k];
+                const int L = ctx->seqLen[pairs[ci].seq];
+                sumJobs[k] = PostSumJob{jobs[k].pOff, colOff[ci], (long long)ci * (M + 1), M, L};
+                maxL = std::max(maxL, L);
+            }
+            CK(cudaMemcpyAsync(ctx->dPostJobs.p, sumJobs.data() + k0, nj * sizeof(PostSumJob),
+                               cudaMemcpyHostToDevice, ctx->stream),
+               "upload summary jobs");
+            if (colPost || colRow) {
+                postColumnKernel<<<dim3((maxL + kPostThreads - 1) / kPostThreads, nj), kPostThreads, 0, ctx->stream>>>(
+                    ctx->dPostJobs.p, ctx->dPost.p, ctx->dColPost.p, ctx->dColRow.p);
+                CK(cudaGetLastError(), "posterior column kernel");
+                ++launches;
+            }
+            if (rowMatch) {
+                const int rowsPer = kPostThreads / kLanes;
+                postRowKernel<<<dim3((M + 1 + rowsPer - 1) / rowsPer, nj), kPostThreads, 0, ctx->stream>>>(
+                    ctx->dPostJobs.p, ctx->dPost.p, ctx->dRowMatch.p);
+                CK(cudaGetLastError(), "posterior row kernel");
+                ++launches;
+            }
+        }
+        CK(cudaEventRecord(ctx->ev[4], ctx->stream), "event");
         if (post)
             for (size_t k = k0; k < k1; ++k)
                 CK(cudaMemcpyAsync(post + postOff[order[k]], ctx->dPost.p + jobs[k].pOff,
@@ -2779,6 +2829,15 @@ static int runAdjoint(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *l
     if (grad_params) std::memcpy(grad_params, g.data(), (size_t)(M + 2) * kParamFloats * sizeof(double));
     if (grad_emit)
         std::memcpy(grad_emit, g.data() + (size_t)(M + 2) * kParamFloats, (size_t)(M + 1) * kNumCodes * sizeof(double));
+    if (colPost)
+        CK(cudaMemcpy(colPost, ctx->dColPost.p, (size_t)colOff[n] * sizeof(double), cudaMemcpyDeviceToHost),
+           "download column posteriors");
+    if (colRow)
+        CK(cudaMemcpy(colRow, ctx->dColRow.p, (size_t)colOff[n] * sizeof(int), cudaMemcpyDeviceToHost),
+           "download column rows");
+    if (rowMatch)
+        CK(cudaMemcpy(rowMatch, ctx->dRowMatch.p, n * (size_t)(M + 1) * sizeof(double), cudaMemcpyDeviceToHost),
+           "download row sums");
     return DMST_OK;
 }
 
@@ -2799,6 +2858,13 @@ int dmst_loglik_grad(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *lo
 int dmst_posteriors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *post) {
     if (!post) return DMST_EINVAL;
     return runAdjoint(ctx, pairs, n, log_t, nullptr, nullptr, post, "dmst_posteriors");
+}
+
+int dmst_posterior_summary(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *col_post,
+                           int *col_row, double *row_match) {
+    if (!col_post && !col_row && !row_match) return DMST_EINVAL;
+    return runAdjoint(ctx, pairs, n, log_t, nullptr, nullptr, nullptr, "dmst_posterior_summary", col_post, col_row,
+                      row_match);
 }
 
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta) {

@@ -440,6 +440,31 @@ class Context:
             o += 2 * (M + 1) * L
         return logt, out
 
+    def posterior_summary(self, seq_ids: Sequence[int], pid: int):
+        """(log T per pair, [(column max cell posterior (L,), its row (L,),
+        row sums of match posteriors (M+1,)) per pair]) for the reads seq_ids
+        against profile pid (dmst_posterior_summary: the tables stay on the
+        device)."""
+        n = len(seq_ids)
+        M = self.profile_length(pid)
+        pairs = (F.Pair * n)()
+        lens = [self.seq_length(s) for s in seq_ids]
+        for k, s in enumerate(seq_ids):
+            pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, pid, -2.0
+        logt = np.zeros(n, np.float64)
+        cp = np.zeros(sum(lens), np.float64)
+        cr = np.zeros(sum(lens), np.int32)
+        rm = np.zeros(n * (M + 1), np.float64)
+        D = C.POINTER(C.c_double)
+        st = self.lib.dmst_posterior_summary(self.h, pairs, n, logt.ctypes.data_as(D), cp.ctypes.data_as(D),
+                                             cr.ctypes.data_as(C.POINTER(C.c_int)), rm.ctypes.data_as(D))
+        self._check(st, "dmst_posterior_summary")
+        out, o = [], 0
+        for k, L in enumerate(lens):
+            out.append((cp[o:o + L], cr[o:o + L], rm[k * (M + 1):(k + 1) * (M + 1)]))
+            o += L
+        return logt, out
+
     def autotune(self, seq_ids: Sequence[int], profile_ids: Sequence[int]) -> dict:
         """Time every kernel shape on these pairs (dmst_autotune); returns the
         rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)."""

@@ -91,8 +91,11 @@ def hmmer3_text(profiles: list[SynthProfile]) -> str:
 
         out.append(ins)
         out.append(trans(False, True))
+        # -ln p of every match emission at once (match rows are > 0), each
+        # printed with 5 decimals as _nl prints it
+        nl = (-np.log(pr.match)).tolist()
         for k in range(M):
-            out.append(f"  {k + 1:5d}   " + "  ".join(_nl(x) for x in pr.match[k]) + f"  {k + 1} - - - -\n")
+            out.append(f"  {k + 1:5d}   " + "  ".join(["%.5f" % x for x in nl[k]]) + f"  {k + 1} - - - -\n")
             out.append(ins)
             out.append(trans(k == M - 1, False))
         out.append("//\n")

@@ -499,6 +499,20 @@ int dmst_loglik_grad(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *lo
  * so max_ij cell * T is that score. */
 int dmst_posteriors(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *post);
 
+/* The posterior pass of a genome scan's windows above threshold, reduced on
+ * the device: the tables of dmst_posteriors are computed in device memory and
+ * only these leave it.  For pair k (the caller's order), at
+ * col_post + sum_{k'<k} L_k' (and col_row likewise): per column j the largest
+ * cell posterior max_i W0[i][j] W1[i][j] / T and its row i (the first on
+ * ties), the posterior-decoded track of the alignment; at row_match +
+ * k (M+1): per row i the sum over the columns of the match posteriors, the
+ * expected number of match emissions of profile row i.  FP64; any output
+ * may be NULL, but not all three.  The reference has no posterior pass; the
+ * tables follow its forward and backward recurrences
+ * (dummest-dp-forward.hh:125-157, dummest-dp-backward.hh:473-574). */
+int dmst_posterior_summary(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, double *log_t, double *col_post,
+                           int *col_row, double *row_match);
+
 /* Per-pair null model (testing aid): prefixSeed[0..L), suffixSeedFromNext[0..L)
  * and the three per-base scales (one-nt, two-nt, codon) for one pair, computed
  * by the device prologue kernel.  Replaces the null half of setupBatch

@@ -1,10 +1,11 @@
 """Multi-rank logic of bench.py on CPU (gloo, world size 2).
 
-The search path shards pairs across ranks with no data-path collective: each
-rank scores its own reads, and the only collectives are the barrier and the
-reductions of the timed region (max of the device time, sum of the cells).
-These tests run that logic in two gloo processes, and check that the
-reference arm runs on rank 0 alone.
+The timed region ends with the barrier and the reductions of the whole job
+(max of the device time over ranks, sum of the cells).  These tests run that
+logic in two gloo processes, check that the reference arm runs on rank 0
+alone, and that `--gpus N` starts its N ranks itself.  (The partition of the
+pair queue and the gather of the results are tested in
+test_shards_multirank.py.)
 """
 import json
 import os
@@ -72,3 +73,18 @@ def test_reference_arm_runs_on_rank_zero_only(tmp_path):
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+
+
+def test_gpus_flag_launches_the_ranks_itself(tmp_path):
+    """`bench.py --gpus 2` without a launcher starts two ranks (torchrun on
+    127.0.0.1); the reference arm then prints one line, from rank 0, with
+    n_gpus 2."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    args = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+            "--warmup", "0", "--reads-per-step", "4", "--profiles", "2", "--cpu-seconds", "0.5"]
+    res = subprocess.run(args, env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [json.loads(l) for l in res.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, res.stdout
+    assert lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2

@@ -5,6 +5,7 @@ in FP64.  Bar: E-values within 1% relative over the range of reported scores;
 the per-trial scores are compared directly as well.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -58,3 +59,41 @@ def test_calibration_evalues_match_reference(ref32, tmp_path, M, L, B, N):
     assert rel <= 1e-2 and rel_f <= 1e-2
     # The scores are the reference's bit for bit, so the FP64 fit is too.
     assert np.array_equal(got, want), (got, want)
+
+
+def test_calibration_batch_at_the_configured_shape(ref32, tmp_path):
+    """The Gumbel calibration batch at its configured shape: profiles of M up
+    to 1500, each scored against 200 i.i.d. uniform ACGT sequences of 3000 nt
+    (mode MID, one call for all profiles).  Every trial's mid and filter
+    ln-score equals the reference engine's on the same sequence bit for bit,
+    and the E-values of the FP64 fit (estimateGumbel,
+    dummest-calibration.hh:97-104) agree within 1% relative -- here exactly,
+    since the scores do."""
+    rng = np.random.default_rng(3003)
+    Ms = [1500, 731, 50]
+    profs = [synth.make_profile(rng, M, f"c3_{M}") for M in Ms]
+    txt = synth.hmmer3_text(profs)
+    path = tmp_path / "c3.hmm"
+    path.write_text(txt)
+    assert ref32.load_profiles(str(path)) == len(Ms)
+    T, L = 200, 3000
+    seqs = [[synth.random_dna(rng, L, 0.5) for _ in range(T)] for _ in Ms]
+    with d.Context(device=0) as ctx:
+        pids = ctx.load_hmm(txt)
+        sids = [ctx.add_dna(s) for s in seqs]
+        res = ctx.score_pairs([s for ss in sids for s in ss], [p for p, ss in zip(pids, sids) for _ in ss])
+    for p in range(len(Ms)):
+        got = res[p * T:(p + 1) * T]
+        mid = np.array([r.mid_ln for r in got])
+        flt = np.array([r.filter_ln for r in got])
+        codes = [ref32.decode(ref32.encode(s)) for s in seqs[p]]
+        ref_mid, ref_flt = ref32.score_many(p, codes, threads=os.cpu_count() or 1, mode=0)
+        assert np.array_equal(mid, ref_mid), (Ms[p], np.argwhere(mid != ref_mid)[:5])
+        assert np.array_equal(flt, ref_flt), (Ms[p], np.argwhere(flt != ref_flt)[:5])
+        for ours, theirs in ((mid, ref_mid), (flt, ref_flt)):
+            g = d.estimate_gumbel(ours, L)
+            w = ref32.estimate_gumbel(theirs, L)
+            bits = np.linspace(np.median(theirs) / LN2, np.median(theirs) / LN2 + 60.0, 31)
+            rel = np.max(np.abs(_evalue(g[1], g[0], 1e9, bits) / _evalue(w[1], w[0], 1e9, bits) - 1.0))
+            assert rel <= 1e-2, (Ms[p], rel)
+            assert np.array_equal(g[:2], w[:2])
