@@ -190,7 +190,6 @@ __device__ bool backwardSweepPipe(const SweepArgs &a, Window &win, int warp, int
     }
     b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
     b.sendC = b.cnt = 0;
-    b.realRows = 0;
     b.u = -(kLanes - 1 - lane);  // lane 31 leads
     b.sp = a.sFirst;
     b.jj = 0;

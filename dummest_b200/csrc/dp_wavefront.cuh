@@ -376,7 +376,6 @@ struct BwdState {
     float rb[3];             // the row below (the next lane's top row): W1 history slots
     float sendW, sendY, filt, maxY;
     int sendC;
-    int realRows;            // rows of this lane at or above row M (the rest are padding)
     int u, sp, jj;           // lane-local time, stripe from the bottom, column from the right
     float *wp;               // W1 store pointer of the current step
     // exact-path state
@@ -404,7 +403,6 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
         const int rowBase = s * S + lane * R;
         if (b.jj == 0) {
             loadBackwardCoef<R>(b.c, a, rowBase);
-            b.realRows = min(max(a.M() - rowBase + 1, 0), R);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
 #pragma unroll
@@ -487,11 +485,11 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             acc = __fmaf_rn(zbg, b.c.a0[k], acc);
             acc = __fmaf_rn(b.h[I2][k], b.c.a2[k], acc);
             acc = __fmaf_rn(b.h[I1][k], b.c.a1[k], acc);
-            // Seed term fma(suf, rs, acc): rs is 1 on real rows, so the fast
-            // modes add suf exactly; rows past M (zero coefficients and inputs)
-            // accumulate exactly 0 and must stay 0, so they take no seed.
-            const float W = (MODE == kFilter || MODE == kMid) ? __fadd_rn(acc, k < b.realRows ? sufv : 0.0f)
-                                                             : __fmaf_rn(sufv, b.c.rs[k], acc);
+            // Seed term fma(suf, rs, acc): in the fast modes rs is 1 on real
+            // rows, where the fma is the exact sum suf + acc (one rounding, as
+            // the reference's add), and 0 on rows past M, which accumulate
+            // exactly 0 and must stay 0.
+            const float W = __fmaf_rn(sufv, b.c.rs[k], acc);
             const float Y = __fmaf_rn(b.c.eps[k], bY, W);
             const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
             if (MODE == kFilter || MODE == kMid) {
@@ -627,7 +625,6 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
     }
     b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
     b.sendC = b.cnt = 0;
-    b.realRows = 0;
     b.u = -(kLanes - 1 - lane);  // lane 31 leads
     b.sp = b.jj = 0;
     b.wp = a.w1;
