@@ -1407,11 +1407,17 @@ def run_ours(args, rank, world, local):
             p, s = pids[idx // len(sids)], sids[idx % len(sids)]
             arr[k].seq, arr[k].profile, arr[k].min_prob_ratio = s, p, -2.0
             pc += (Ms[p] + 1) * len(recs[idx % len(sids)])
-        ctx.score_pairs_raw(arr, d.MODE_MID | d.MODE_PLAIN)
-        ctx.score_pairs_raw(arr, d.MODE_MID | d.MODE_PLAIN)
-        tp = ctx.last_timing()
-        plain = {"gcups": pc / (tp["dp_ms"] / 1e3) / 1e9, "pairs": len(sel), "launches": tp["launches"]}
-        plain["batched_over_plain"] = value / world / plain["gcups"]
+        plain = {"pairs": len(sel), "cells": pc,
+                 "kernel": "one pair per launch: one CTA of 8 warps sharing the pair's stripes (stripe pipeline, "
+                           "fast-path arithmetic)",
+                 "kernel_1warp": "one pair per launch: the batched kernel on a one-pair chunk (one warp computes)"}
+        for key, flag in (("", d.MODE_PLAIN), ("_1warp", d.MODE_PLAIN | d.MODE_PLAIN_1WARP)):
+            ctx.score_pairs_raw(arr, d.MODE_MID | flag)
+            ctx.score_pairs_raw(arr, d.MODE_MID | flag)
+            tp = ctx.last_timing()
+            plain["gcups" + key] = pc / (tp["dp_ms"] / 1e3) / 1e9
+            plain["launches" + key] = tp["launches"]
+            plain["batched_over_plain" + key] = value / world / plain["gcups" + key]
 
     cb = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -13,6 +13,7 @@ from ._ffi import (  # noqa: F401
     MODE_GRAPH,
     MODE_MID,
     MODE_PLAIN,
+    MODE_PLAIN_1WARP,
     RES_EXACT_PATH,
     RES_SURVIVOR,
     load,

@@ -27,6 +27,7 @@ ADJ_CKPT_AUTO, ADJ_CKPT_ON, ADJ_CKPT_OFF = 0, 1, 2  # dmst_adjoint_checkpoint
 MODE_MID = 0
 MODE_FILTER = 1
 MODE_PLAIN = 0x100
+MODE_PLAIN_1WARP = 0x1000
 MODE_FORCE_EXACT = 0x200
 MODE_EXACT_SEQUENTIAL = 0x400
 MODE_GRAPH = 0x800

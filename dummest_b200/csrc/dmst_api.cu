@@ -6,6 +6,7 @@
 #include "dp_exact.cuh"
 #include "dp_adjoint.cuh"
 #include "dp_posterior.cuh"
+#include "dp_plain.cuh"
 #include "dp_exact_wave.cuh"
 #include "dp_search.cuh"
 #include "dp_traceback.cuh"
@@ -307,6 +308,26 @@ DpKern dpKernelShape(int R, bool mid, int warps) {
 // leave shared memory for fewer than `warps` staging windows).
 DpKern dpKernelFor(int R, bool mid, int warps, bool gt) {
     return gt ? dpKernelShape<true>(R, mid, warps) : dpKernelShape<false>(R, mid, warps);
+}
+
+using PlainKern = void (*)(const DevPair *, int, const DevProfile *, const float *, const float *, const uint8_t *,
+                          const float *, const PairScales *, float *, PairOut *, int);
+template <bool MID>
+PlainKern plainKernelByR(int R) {
+    return R == 4 ? plainKernel<4, MID> : (R == 2 ? plainKernel<2, MID> : plainKernel<1, MID>);
+}
+// The plain schedule's kernel for R rows per lane; its dynamic shared memory
+// (a window per warp) is allowed once.
+PlainKern plainKernelFor(int R, bool mid) {
+    static bool attrSet = false;
+    if (!attrSet) {
+        for (int r : {4, 2, 1})
+            for (bool m : {true, false})
+                cudaFuncSetAttribute(m ? plainKernelByR<true>(r) : plainKernelByR<false>(r),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPlainWarps * sizeof(Window)));
+        attrSet = true;
+    }
+    return mid ? plainKernelByR<true>(R) : plainKernelByR<false>(R);
 }
 
 // Rows of a profile as the kernel with R rows per lane computes them.
@@ -1374,7 +1395,10 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     if (anchors) mode |= DMST_MODE_FORCE_EXACT;
     if (!ctx || (n && (!pairs || (!out && !nullOnly)))) return DMST_EINVAL;
     const int base = mode & 0xff;
-    const bool plain = (mode & DMST_MODE_PLAIN) != 0;
+    const bool plain = (mode & (DMST_MODE_PLAIN | DMST_MODE_PLAIN_1WARP)) != 0;
+    // the plain schedule's kernel: the pair's stripes on the CTA's warps, or
+    // (DMST_MODE_PLAIN_1WARP) the batched kernel's one warp per pair
+    const bool plainStriped = plain && !(mode & DMST_MODE_PLAIN_1WARP);
     const bool forceExact = (mode & (DMST_MODE_FORCE_EXACT | DMST_MODE_EXACT_SEQUENTIAL)) != 0;
     const bool sequentialExact = (mode & DMST_MODE_EXACT_SEQUENTIAL) != 0;
     if (base != DMST_MODE_MID && base != DMST_MODE_FILTER) return DMST_EINVAL;
@@ -1606,7 +1630,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     if ((st = upload(S.hPairs, S.dPairs.p, dp.data(), n, "upload pairs"))) return st;
     if ((st = upload(S.hChunks, ctx->dChunks.p, allChunks.data(), allChunks.size(), "upload chunks"))) return st;
     // The groups run one after another on the stream, so they share the slots.
-    CK(ctx->dW1.ensure(std::max<size_t>(slotsMax * w1Slot, 1)), "alloc W1 slots");
+    size_t plainScratch = 0;
+    if (plainStriped)
+        for (size_t k = 0; k < n; ++k)
+            plainScratch = std::max(plainScratch, (size_t)plainScratchFloats(dp[k].M, dp[k].L, dp[k].R));
+    CK(ctx->dW1.ensure(std::max<size_t>(std::max(slotsMax * w1Slot, plainScratch), 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
     const size_t nCounters = std::max<size_t>(allChunks.size() + 3, 6);  // search: the second wave's at 3..5
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
@@ -1814,7 +1842,16 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             for (int gi = 0; gi < 3; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
-                if (plain) {
+                if (plainStriped) {
+                    // One pair per launch, its stripes on the CTA's warps.
+                    auto pk = plainKernelFor(G.R, mid);
+                    for (size_t k = 0; k < G.chunks.size(); ++k) {
+                        pk<<<1, kPlainWarps * kLanes, kPlainWarps * sizeof(Window), ctx->stream>>>(
+                            S.dPairs.p, G.chunks[k].first, ctx->dProfiles.p, ctx->dEmit.p, ctx->dParams.p,
+                            ctx->dCodes.p, S.dSeeds.p, S.dScales.p, ctx->dW1.p, S.dOut.p, ctx->waitLimit);
+                        ++launches;
+                    }
+                } else if (plain) {
                     // One pair per launch: a one-CTA grid over a one-pair chunk.
                     for (size_t k = 0; k < G.chunks.size(); ++k) {
                         DpArgs gk = g;

@@ -171,9 +171,14 @@ __device__ __forceinline__ bool pipeReady(const PipeSync &ps, const SweepArgs &a
     return ok;
 }
 
+// The sweeps of one warp in a stripe pipeline.  The fast mode (kMid) also
+// gives the warp's share of the float maxima (filter best and largest Y in
+// the backward, mid and largest W0 / Y0 in the forward) through the optional
+// outputs; warps reduce them afterwards.
 template <int R, int MODE>
 __device__ bool backwardSweepPipe(const SweepArgs &a, Window &win, int warp, int lane, const PipeSync &ps,
-                                  const ExactRows *x, ExactBest *exact) {
+                                  const ExactRows *x, ExactBest *exact, float *filtOut = nullptr,
+                                  float *maxYOut = nullptr) {
     BwdState<R, MODE> b;
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -205,18 +210,21 @@ __device__ bool backwardSweepPipe(const SweepArgs &a, Window &win, int warp, int
         const int n = (t0 + kBlock < T ? kBlock : T - t0);
 #pragma unroll 1
         for (int g = 0; g < n; g += 3) {
-            backwardStep<R, MODE, 0>(b, a, win, lane, total, x, exact);
-            backwardStep<R, MODE, 1>(b, a, win, lane, total, x, exact);
-            backwardStep<R, MODE, 2>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 0, true>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 1, true>(b, a, win, lane, total, x, exact);
+            backwardStep<R, MODE, 2, true>(b, a, win, lane, total, x, exact);
         }
     }
     pipePublish(ps, warp, INT_MAX, lane);
+    if (filtOut) *filtOut = b.filt;
+    if (maxYOut) *maxYOut = b.maxY;
     return true;
 }
 
 template <int R, int MODE, bool ANCH = false>
 __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int lane, const PipeSync &ps,
-                                 const ExactRows *x, ExactBest *exact) {
+                                 const ExactRows *x, ExactBest *exact, float *bestOut = nullptr,
+                                 float *maxOut = nullptr) {
     FwdState<R, MODE> f;
 #pragma unroll
     for (int h = 0; h < 3; ++h)
@@ -238,7 +246,7 @@ __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int 
     f.j = 0;
     const int total = a.nMine * a.P;
     const int T = (total + (kLanes - 1) + 5) / 6 * 6;
-    constexpr bool kReadW1 = MODE == kReplay;
+    constexpr bool kReadW1 = MODE == kReplay || MODE == kMid;
     W1Stage<R, true> st{-lane, a.sFirst, 0};
     if (kReadW1) {
 #pragma unroll
@@ -254,16 +262,18 @@ __device__ bool forwardSweepPipe(const SweepArgs &a, Window &win, int warp, int 
         const int n = (t0 + kBlock < T ? kBlock : T - t0);
 #pragma unroll 1
         for (int g = 0; g < n; g += 6) {
-            forwardStaged<R, MODE, 0, ANCH>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 1, ANCH>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 2, ANCH>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 3, ANCH>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 4, ANCH>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 5, ANCH>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 0, ANCH, true>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 1, ANCH, true>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 2, ANCH, true>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 3, ANCH, true>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 4, ANCH, true>(f, a, win, lane, total, st, x, exact);
+            forwardStaged<R, MODE, 5, ANCH, true>(f, a, win, lane, total, st, x, exact);
         }
     }
     if (kReadW1) cpAsyncWait<0>();  // no copy outlives the sweep (the slots are reused)
     if (ok) pipePublish(ps, warp, INT_MAX, lane);
+    if (bestOut) *bestOut = f.best;
+    if (maxOut) *maxOut = f.mx;
     return ok;
 }
 

@@ -386,7 +386,9 @@ struct BwdState {
     double rowBest[R];       // replay: per-row max of W1 * prefixSeed
 };
 
-template <int R, int MODE, int PH>
+// PIPE: the sweep runs one of several warps' stripes of a pair (a stripe
+// pipeline: stripes sFirst, sFirst + sStep, ...; ring slot per stripe).
+template <int R, int MODE, int PH, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
 __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepArgs &a, Window &win, int lane,
                                              int total, const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
@@ -560,7 +562,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             b.wp += kLanes * R;
         }
         if (lane == 0 && b.sp < a.nS - 1) {
-            float *rg = kExactMode ? a.ring + (size_t)(b.sp % a.ringSlots) * a.ringStride : a.ring;
+            float *rg = PIPE ? a.ring + (size_t)(b.sp % a.ringSlots) * a.ringStride : a.ring;
             if (MODE == kDiscover)
                 ringStore(rg, b.jj, b.sendW, b.sendY, b.sendC);
             else
@@ -586,7 +588,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
     }
     if (b.u >= 0 && ++b.jj == a.P) {
         b.jj = 0;
-        b.sp += kExactMode ? a.sStep : 1;
+        b.sp += PIPE ? a.sStep : 1;
     }
     ++b.u;
 }
@@ -710,7 +712,7 @@ struct FwdState {
 // ascending order with scoreLess (the first row wins ties); the stripe's top
 // lane writes the stripe's partial, and the stripes are folded in order after
 // the sweep.
-template <int R, int MODE, int PH, bool ANCH = false>
+template <int R, int MODE, int PH, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
 __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                             int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
@@ -883,7 +885,7 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
             }
         }
         if (lane == kLanes - 1 && f.s < a.nS - 1) {
-            float *rg = kExactMode ? a.ring + (size_t)(f.s % a.ringSlots) * a.ringStride : a.ring;
+            float *rg = PIPE ? a.ring + (size_t)(f.s % a.ringSlots) * a.ringStride : a.ring;
             if (MODE == kDiscover)
                 ringStore(rg, f.j, f.sendIn, f.sendY, f.sendC);
             else
@@ -912,7 +914,7 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
     }
     if (f.u >= 0 && ++f.j == a.P) {
         f.j = 0;
-        f.s += kExactMode ? a.sStep : 1;
+        f.s += PIPE ? a.sStep : 1;
     }
     ++f.u;
 }
@@ -920,9 +922,9 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
 // One forward step at position P6 of a six-step group: wait for this step's
 // W1 copy, read it from the staging ring, run the step, and stage the W1 of
 // the step kW1Ahead later into the slot this lane read one step ago.
-template <int R, int MODE, int P6, bool ANCH = false>
+template <int R, int MODE, int P6, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
 __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
-                                              int total, W1Stage<R, MODE == kDiscover || MODE == kReplay> &st,
+                                              int total, W1Stage<R, PIPE> &st,
                                               const ExactRows *x, ExactBest *exact) {
     constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
     float q[R];
@@ -939,7 +941,7 @@ __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepA
 #pragma unroll
         for (int k = 0; k < R; ++k) q[k] = 0.0f;
     }
-    forwardStep<R, MODE, P6 % 3, ANCH>(f, a, win, lane, total, q, x, exact);
+    forwardStep<R, MODE, P6 % 3, ANCH, PIPE>(f, a, win, lane, total, q, x, exact);
     if (kReadW1) st.issue(a, win, (P6 + kW1Ahead) % kW1Slots, lane, total);
 }
 

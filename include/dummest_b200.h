@@ -49,10 +49,16 @@ extern "C" {
  * float W1 with no row rescaling, score = max W1[i][j]*prefixSeed[j], which
  * may be +inf ("inf always survives", dummest-search.hh:163-168). */
 #define DMST_MODE_FILTER 1
-/* Flag for either mode: run the plain schedule, one pair per kernel launch
- * (same per-pair code), the baseline the batched persistent kernel is
- * measured against. */
+/* Flag for either mode: run the plain schedule, one pair per kernel launch,
+ * the baseline the batched persistent kernel is measured against.  The
+ * launch is one CTA of 8 warps that share the pair: its stripes (32 R profile
+ * rows each) are dealt to the warps and run as a stripe pipeline, with the
+ * same per-cell arithmetic (results bit for bit those of the batched call).
+ * No counterpart in the reference (its unit of work is a SIMD batch). */
 #define DMST_MODE_PLAIN 0x100
+/* With DMST_MODE_PLAIN: the earlier plain form, the batched kernel launched
+ * on a one-pair chunk, where one warp computes the pair. */
+#define DMST_MODE_PLAIN_1WARP 0x1000
 /* Flag: route every pair through the exact row-rescaled wavefront path
  * (the path taken by pairs whose rows the reference would rescale). */
 #define DMST_MODE_FORCE_EXACT 0x200

@@ -164,16 +164,23 @@ def test_force_exact_path_matches(gpu_ctx, ref32, tmp_path):
 
 
 def test_plain_schedule_equals_batched(gpu_ctx, ref32, tmp_path):
-    rng, profs, txt = _setup_profiles(tmp_path, ref32, [60, 300], seed=31)
+    # M = 1100: 9 stripes of 128 rows on 8 warps (one warp runs two)
+    rng, profs, txt = _setup_profiles(tmp_path, ref32, [60, 300, 1100], seed=31)
     pids = gpu_ctx.load_hmm(txt)
     reads = _mk_reads(rng, profs, [100, 700, 1500])
     sids = gpu_ctx.add_dna(reads)
     for pid in pids:
         a = gpu_ctx.score_pairs(sids, pid, d.MODE_MID)
-        b = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | d.MODE_PLAIN)
-        for x, y in zip(a, b):
-            assert x.mid.m == y.mid.m and x.mid.e == y.mid.e
-            assert x.filter.m == y.filter.m and x.filter.e == y.filter.e
+        fa = gpu_ctx.score_pairs(sids, pid, d.MODE_FILTER)
+        # the plain schedule: the pair's stripes on one CTA's warps, and the one-warp form
+        for plain in (d.MODE_PLAIN, d.MODE_PLAIN | d.MODE_PLAIN_1WARP):
+            b = gpu_ctx.score_pairs(sids, pid, d.MODE_MID | plain)
+            for x, y in zip(a, b):
+                assert x.mid.m == y.mid.m and x.mid.e == y.mid.e
+                assert x.filter.m == y.filter.m and x.filter.e == y.filter.e
+                assert x.exact_path == y.exact_path
+            fb = gpu_ctx.score_pairs(sids, pid, d.MODE_FILTER | plain)
+            assert [x.filter_f for x in fa] == [y.filter_f for y in fb]
 
 
 def test_input_paths_agree(gpu_ctx, ref32, tmp_path):
