@@ -46,7 +46,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FLOPS_PER_CELL = 52  # 24 backward + 28 forward with the mid product
-AG_BYTES_PER_CELL = 48              # adjoint: (W0, Y0, Z0) written, (W0, Z0, Y0 of the row below) read, FP64
+# adjoint, FP64 flops per cell counted from csrc/dp_adjoint.cuh: the forward
+# recurrence with the T sum 24, the backward recurrence 21 and the gradient
+# sums 22 (the checkpointed variant's forward recompute, 24 more, is not
+# algorithmic work)
+AG_FLOPS_PER_CELL = 67
 SEARCH_E = 10.0                     # -e and the filter E-value by default (dummest-core.hh:60, dummest.cc:297-298)
 FILTER_FLOPS_PER_CELL = 25          # the float filter: backward only
 METRIC = "fwd+bwd GCUPS (batched persistent kernel)"
@@ -1632,15 +1636,20 @@ def run_autograd(args, rank, world, local):
     total_cells = cells * args.steps
     value, ms_max, cells_all = aggregate(total_cells, ms, world)
     peaks = measured_peaks()
-    hbm = peaks.get("hbm_gbs", 6451.2)
-    achieved = AG_BYTES_PER_CELL * total_cells / (adj_ms / 1e3) / 1e9
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp64_peak = n_sm * 64 * 2 * sm_max * 1e6 / 1e12  # TFLOP/s: 64 FP64 lanes per SM
+    achieved = AG_FLOPS_PER_CELL * total_cells / (adj_ms / 1e3) / 1e12
     roofline = {
-        "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-        "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-        "kernel": "adjointKernel (forward store + backward with gradient sums), CUDA events on the library "
+        "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+        "traffic": None,
+        "peak_source": f"derived: {n_sm} SMs x 64 FP64 lanes x 2 x sm_max_mhz {sm_max:g} (of measured clock; "
+                       "MEASURED_PEAKS.json has no FP64 figure)",
+        "kernel": "adjointKernel (forward, then backward with the gradient sums), CUDA events on the library "
                   "stream, summed over the step's launches",
-        "algorithmic_bytes_per_cell": AG_BYTES_PER_CELL,
+        "algorithmic_flops_per_cell": AG_FLOPS_PER_CELL,
         "adjoint_gcups": total_cells / (adj_ms / 1e3) / 1e9,
+        "note": "latency-bound FP64 chains (a warp per pair, one row per lane): the fraction is low by design",
     }
     # e2e: the reads re-uploaded from host memory (2-bit packed) every step
     words, mask, lens = d.pack_dna(reads)

@@ -18,6 +18,8 @@
 // call adds its batch's decoded sequences and clears them afterwards.
 #pragma once
 
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -81,6 +83,14 @@ inline std::vector<dmst_pair> addLanes(Ctx &c, const Profile &profile,
                                        const Float *minProbRatio) {
     std::vector<int64_t> off(activeCount + 1, 0);
     for (int k = 0; k < activeCount; ++k) off[k + 1] = off[k] + (int64_t)decoded[k]->size();
+    // The widest batch the engine has scored, which it reports at the end
+    // (setupBatch keeps it, dummest-dp-backward.hh:203-209; both entry points
+    // pass through setupBatch there, and through here in this build).
+    size_t width = 0;
+    for (int k = 0; k < activeCount; ++k) width = std::max(width, decoded[k]->size());
+    size_t cur = g_maxDpWidth.load(std::memory_order_relaxed);
+    while (width > cur && !g_maxDpWidth.compare_exchange_weak(cur, width, std::memory_order_relaxed))
+        ;
     std::vector<uint8_t> codes((size_t)off[activeCount]);
     for (int k = 0; k < activeCount; ++k)
         std::memcpy(codes.data() + off[k], decoded[k]->data(), decoded[k]->size());

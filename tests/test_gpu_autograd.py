@@ -13,6 +13,7 @@ dmst_posteriors, and the torch.autograd.Function over it.
   than the double range: log T against the oracle.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -102,6 +103,65 @@ def test_log_likelihood_and_gradient_match_fp64_finite_differences():
     assert not bad, bad[:10]
     nz = sum(1 for name, idx in coords if abs(grads[name][idx]) > 1e-3)
     assert nz >= 100  # most coordinates carry a real gradient
+
+
+def test_gradient_at_the_configured_shape():
+    """The differentiation configuration's shape: M = 400 and 64 reads of
+    600-2400 nt, each carrying a frameshifted homolog (the bench's generator).
+    log T of every read equals the FP64 oracle's to 1e-10, and the gradient
+    equals FP64 central differences (h = 1e-4) to 1e-4 relative on 60 logits
+    (emission, transition, frameshift).  The oracle's evaluations run on the
+    host's threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    rng = np.random.default_rng(20261208)
+    M = 400
+    prof = synth.make_profile(rng, M, "g400")
+    txt = synth.hmmer3_text([prof])
+    _, values, params, bg = d.finalize_hmm(txt)
+    reads = synth.make_reads(rng, 64, 600, 2400, [prof], 1.0, gc_range=(0.4, 0.6), log_uniform=False)
+    codes = [d.decode_dna(r) for r in reads]
+    em0 = torch.tensor(np.log(prof.match))
+    MI, MD, II, DD = synth.T_MI, synth.T_MD, synth.T_II, synth.T_DD
+    tr0 = torch.tensor(np.tile(np.log([1 - MI - MD, MI, MD, 1 - II, II, 1 - DD, DD]), (M + 1, 1))
+                       + rng.normal(scale=0.05, size=(M + 1, 7)))
+    fs0 = torch.tensor(np.log(FS))
+    bg_row = torch.tensor(values[-1, 4:29], dtype=torch.float64)
+    with d.Context(device=0) as ctx:
+        sids = ctx.add_dna(reads)
+        slot = ag.ProfileSlot(ctx, values, params, bg, sids)
+        em, tr, fs = (t.clone().requires_grad_(True) for t in (em0, tr0, fs0))
+        emit, par = ag.profile_params(em, tr, fs, bg_row)
+        ag.log_likelihood(emit, par, slot).backward()
+        logt = slot.last_log_t
+    v32 = slot.values.astype(np.float64)
+    p32 = par.detach().numpy().astype(np.float32).astype(np.float64)
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+        want = list(ex.map(lambda c: port.log_total(v32, p32, bg, c), codes))
+        for k in range(len(codes)):
+            assert abs(logt[k] - want[k]) <= 1e-10 * max(1.0, abs(want[k])), (k, logt[k], want[k])
+        coords = [("em", (int(i), int(a))) for i, a in zip(rng.integers(0, M, 30), rng.integers(0, 20, 30))]
+        coords += [("tr", (int(i), int(a))) for i, a in zip(rng.integers(0, M + 1, 26), rng.integers(0, 7, 26))]
+        coords += [("fs", (k,)) for k in range(4)]
+        grads = {"em": em.grad.numpy(), "tr": tr.grad.numpy(), "fs": fs.grad.numpy()}
+        base = {"em": em0, "tr": tr0, "fs": fs0}
+        h = 1e-4
+
+        def total(name, idx, step):
+            t = {k: v.clone() for k, v in base.items()}
+            t[name][idx] += step
+            e, p = ag.profile_params(t["em"], t["tr"], t["fs"], bg_row)
+            vals = np.zeros((e.shape[0], 29))
+            vals[:, 4:29] = e.numpy()
+            pn = p.numpy()
+            return math.fsum(ex.map(lambda c: port.log_total(vals, pn, bg, c), codes))
+
+        bad = []
+        for name, idx in coords:
+            fd = (total(name, idx, h) - total(name, idx, -h)) / (2 * h)
+            g = float(grads[name][idx])
+            if abs(g - fd) > 1e-4 * abs(fd) + 1e-7:
+                bad.append((name, idx, g, fd))
+    assert not bad, bad[:10]
 
 
 def test_posterior_tables_match_oracle():

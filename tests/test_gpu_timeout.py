@@ -43,5 +43,5 @@ def test_exact_path_wait_runs_out_and_context_recovers():
 
 def test_wait_limit_rejects_negative():
     with d.Context(device=0) as ctx:
-        with pytest.raises(d.DmstError):
+        with pytest.raises(ValueError):  # DMST_EINVAL
             ctx.set_wait_limit(-1)
