@@ -185,6 +185,59 @@ windowDecodeKernel(const uint32_t *words, const uint32_t *mask, const WinSeg *se
 }
 
 // ---------------------------------------------------------------------------
+// Buffers replaced while calls may be in flight.  cudaFree and cudaFreeHost
+// synchronise the whole device, so freeing a buffer that a call outgrew would
+// make the host wait for every queued call (with calls submitted one ahead of
+// their completion, a whole call's device time).  The old buffer is kept here
+// instead and freed when its context has no call in flight (drainCalls,
+// dmst_ctx_destroy), or at once when the kept bytes pass kGraveLimit.
+// ---------------------------------------------------------------------------
+struct Grave {
+    void *p;
+    bool host;
+    int device;
+    size_t bytes;
+};
+std::mutex gGraveMutex;
+std::vector<Grave> gGraves;
+size_t gGraveBytes = 0;
+constexpr size_t kGraveLimit = (size_t)16 << 30;
+
+void reapGraves() {
+    std::vector<Grave> g;
+    {
+        std::lock_guard<std::mutex> lock(gGraveMutex);
+        g.swap(gGraves);
+        gGraveBytes = 0;
+    }
+    if (g.empty()) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    for (const Grave &x : g) {
+        if (x.host) {
+            cudaFreeHost(x.p);
+        } else {
+            cudaSetDevice(x.device);
+            cudaFree(x.p);
+        }
+    }
+    if (cur >= 0) cudaSetDevice(cur);
+}
+
+void bury(void *p, bool host, size_t bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    bool full;
+    {
+        std::lock_guard<std::mutex> lock(gGraveMutex);
+        gGraves.push_back(Grave{p, host, dev, bytes});
+        gGraveBytes += bytes;
+        full = gGraveBytes > kGraveLimit;
+    }
+    if (full) reapGraves();  // frees synchronise the device, as before the graveyard
+}
+
+// ---------------------------------------------------------------------------
 // Small device buffer helper
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -193,15 +246,12 @@ struct DevBuf {
     size_t cap = 0;  // elements
     // Capacity for n elements, contents not kept.  Growth is geometric (x1.25,
     // or n x (1 + headroom) for buffers whose need varies from call to call)
-    // so that calls whose sizes vary a little do not reallocate (cudaFree and
-    // cudaMalloc synchronise the device).
+    // so that calls whose sizes vary a little do not reallocate; the old
+    // buffer, which a call in flight may still read, goes to the graveyard.
     cudaError_t ensure(size_t n, double headroom = 0.0) {
         if (n <= cap && p) return cudaSuccess;
         const size_t want = std::max<size_t>({n, cap + cap / 4, (size_t)((double)n * (1.0 + headroom)), 1});
-        if (p) {
-            cudaDeviceSynchronize();  // no call in flight still reads the old buffer
-            cudaFree(p);
-        }
+        if (p) bury(p, false, cap * sizeof(T));
         p = nullptr;
         cap = 0;
         cudaError_t e = cudaMalloc(&p, want * sizeof(T));
@@ -228,10 +278,7 @@ struct DevBuf {
                 return e;
             }
         }
-        if (p) {
-            cudaDeviceSynchronize();  // the copy, and every call in flight (either stream) that reads the old buffer
-            cudaFree(p);
-        }
+        if (p) bury(p, false, cap * sizeof(T));  // the copy, and calls in flight, still read it
         p = q;
         cap = want;
         return cudaSuccess;
@@ -251,7 +298,7 @@ struct PinnedBuf {
     cudaError_t ensure(size_t n) {
         if (n <= cap && p) return cudaSuccess;
         const size_t want = std::max<size_t>({n, cap + cap / 2, 64});
-        if (p) cudaFreeHost(p);
+        if (p) bury(p, true, cap * sizeof(T));  // an async copy in flight may still use it
         p = nullptr;
         cap = 0;
         cudaError_t e = cudaMallocHost((void **)&p, want * sizeof(T));
@@ -622,6 +669,7 @@ void dmst_ctx_destroy(dmst_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
+    reapGraves();
     if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
     for (auto &sl : ctx->slot) {
         if (sl.graphExec) cudaGraphExecDestroy(sl.graphExec);
@@ -1623,10 +1671,10 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         return DMST_OK;
     };
     CK(S.dPairs.ensure(n), "alloc pairs");
-    CK(S.dSeeds.ensure((size_t)seedFloats), "alloc seeds");
+    CK(S.dSeeds.ensure((size_t)seedFloats, 0.1), "alloc seeds");
     CK(S.dScales.ensure(n), "alloc scales");
     CK(S.dOut.ensure(n), "alloc out");
-    CK(ctx->dChunks.ensure(allChunks.size()), "alloc chunks");
+    CK(ctx->dChunks.ensure(allChunks.size(), 0.25), "alloc chunks");
     if ((st = upload(S.hPairs, S.dPairs.p, dp.data(), n, "upload pairs"))) return st;
     if ((st = upload(S.hChunks, ctx->dChunks.p, allChunks.data(), allChunks.size(), "upload chunks"))) return st;
     // The groups run one after another on the stream, so they share the slots.
@@ -1660,10 +1708,10 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         nullTmpEntries += dmst::nullTmpEntries(dp[jobPairs[k]].L);
         k = e;
     }
-    CK(ctx->dNullJobs.ensure(nullJobs.size()), "alloc null jobs");
+    CK(ctx->dNullJobs.ensure(nullJobs.size(), 0.25), "alloc null jobs");
     CK(ctx->dNullJobPairs.ensure(n), "alloc null jobs");
-    CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries), "alloc null tmp");
-    CK(ctx->dNullTmpOff.ensure(nullJobs.size()), "alloc null tmp");
+    CK(ctx->dNullTmp.ensure((size_t)nullTmpEntries, 0.1), "alloc null tmp");
+    CK(ctx->dNullTmpOff.ensure(nullJobs.size(), 0.25), "alloc null tmp");
     if ((st = upload(S.hNullJobs, ctx->dNullJobs.p, nullJobs.data(), nullJobs.size(), "upload null jobs"))) return st;
     if ((st = upload(S.hJobPairs, ctx->dNullJobPairs.p, jobPairs.data(), n, "upload null jobs"))) return st;
     if ((st = upload(S.hNullTmpOff, ctx->dNullTmpOff.p, nullTmpOff.data(), nullTmpOff.size(), "upload null jobs")))
@@ -2170,6 +2218,7 @@ static int drainCalls(dmst_ctx *ctx) {
         const int st = completeCall(ctx);
         if (st && !first) first = st;
     }
+    reapGraves();  // no call of this context is in flight
     return first;
 }
 
