@@ -337,7 +337,7 @@ const char *statusText(int s) {
 // Kernel shapes the autotuner chooses among: rows per lane (the stripe is
 // 32 R rows) and warps per CTA.
 constexpr int kShapeR[3] = {4, 2, 1};
-constexpr int kShapeWarps[2] = {kCtaWarps, kCtaWarpsNarrow};
+constexpr int kShapeWarps[3] = {kCtaWarps, kCtaWarpsNarrow, kCtaWarpsMid};
 inline int rIndex(int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); }
 
 using DpKern = void (*)(DpArgs, int);
@@ -349,6 +349,8 @@ template <bool GT>
 DpKern dpKernelShape(int R, bool mid, int warps) {
     if (warps == kCtaWarpsNarrow)
         return mid ? kernByR<true, kCtaWarpsNarrow, GT>(R) : kernByR<false, kCtaWarpsNarrow, GT>(R);
+    if (warps == kCtaWarpsMid)
+        return mid ? kernByR<true, kCtaWarpsMid, GT>(R) : kernByR<false, kCtaWarpsMid, GT>(R);
     return mid ? kernByR<true, kCtaWarps, GT>(R) : kernByR<false, kCtaWarps, GT>(R);
 }
 // gt: the emission table stays in global memory (profiles whose table would
@@ -389,6 +391,7 @@ struct Tuning {
     bool tuned = false;
     int warps[3] = {kCtaWarps, kCtaWarps, kCtaWarps};
     double rate[3] = {0, 0, 0};
+    double rates[3][3] = {};  // per R, per kShapeWarps: the measured rates (cells per ms), for dmst_tuned_rates
     int forceR = 0, forceWarps = 0;  // set while the autotuner measures one shape
 };
 
@@ -2727,7 +2730,7 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
         for (size_t i = 0; i < n; ++i)
             padded += (double)paddedRows(ctx->profiles[sample[i].profile].M, R) * ctx->seqLen[sample[i].seq];
         double bestRate = 0;
-        for (int w = 0; w < 2; ++w) {
+        for (int w = 0; w < 3; ++w) {
             ctx->tune.forceR = R;
             ctx->tune.forceWarps = kShapeWarps[w];
             double ms = 0;
@@ -2742,7 +2745,8 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
                 return st;
             }
             const double rate = ms > 0 ? padded / ms : 0;  // padded cells per ms
-            if (gcups6) gcups6[q * 2 + w] = rate / 1e6;
+            if (gcups6 && w < 2) gcups6[q * 2 + w] = rate / 1e6;
+            t.rates[q][w] = rate;
             if (rate > bestRate) {
                 bestRate = rate;
                 t.warps[q] = kShapeWarps[w];
@@ -2753,6 +2757,13 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
     t.tuned = true;
     t.forceR = t.forceWarps = 0;
     ctx->tune = t;
+    return DMST_OK;
+}
+
+int dmst_tuned_rates(const dmst_ctx *ctx, double *gcups9) {
+    if (!ctx || !gcups9) return DMST_EINVAL;
+    for (int q = 0; q < 3; ++q)
+        for (int w = 0; w < 3; ++w) gcups9[q * 3 + w] = ctx->tune.rates[q][w] / 1e6;
     return DMST_OK;
 }
 

@@ -404,7 +404,7 @@ struct BwdState {
 
 // PIPE: the sweep runs one of several warps' stripes of a pair (a stripe
 // pipeline: stripes sFirst, sFirst + sStep, ...; ring slot per stripe).
-template <int R, int MODE, int PH, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
+template <int R, int MODE, int PH, bool PIPE = (MODE == kDiscover || MODE == kReplay), bool SH = false>
 __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepArgs &a, Window &win, int lane,
                                              int total, const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
@@ -480,7 +480,10 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
         const int eOff = __float_as_int(col.x);  // code * rowPad
         const float bgv = col.y, sufv = col.z, prev = col.w;
         float e[R];
-        loadEmit<R>(e, a.smE + eOff + rowBase);
+        if (SH)  // the table in shared memory: a plain shared load
+            loadEmitS<R>(e, (unsigned)__cvta_generic_to_shared(a.smE) + 4u * (unsigned)(eOff + rowBase));
+        else
+            loadEmit<R>(e, a.smE + eOff + rowBase);
         // First products (W1[i+1][j+3] * e) * enter, taken before any row of
         // this step overwrites its column-j+3 slot.
         float p[R];
@@ -747,21 +750,52 @@ __device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &
         __syncwarp();
         fillBlock<true>(win, a, t0 + kBlock, lane);
         const int n = (t0 + kBlock < T ? kBlock : T - t0);
-        if ((MODE == kFilter || MODE == kMid) && interiorBlock(a, t0, n, total, 0)) {
+        if (MODE == kFilter || MODE == kMid) {
+            // Groups of three steps from g: the interior ones (see interiorBlock)
+            // form at most two runs, one per stripe the block touches (a block
+            // and the lanes' skew span fewer steps than a stripe), so the runs'
+            // bounds are found once per block and the steps between them are
+            // the general ones.
             constexpr int S = kLanes * R;
-            const float *eBase = a.smE + (a.nS - 1 - b.sp) * S + lane * R;
-            const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
-            const bool ringWriter = lane == 0 && b.sp < a.nS - 1;
+            const int u0 = t0 - (kLanes - 1);  // lane 0's local time at the block's first step
+            const int k0 = u0 >= 0 ? u0 / a.P : -1;
+            int g = 0;
 #pragma unroll 1
-            for (int g = 0; g < n; g += 3) {
-                backwardInterior<R, MODE, 0, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
-                backwardInterior<R, MODE, 1, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
-                backwardInterior<R, MODE, 2, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
+            for (int kk = 0; kk < 2; ++kk) {
+                const int kb = (k0 + kk) * a.P;  // the stripe's first local time
+                if (kb < 0) continue;
+                int gA = kb + kLanes - t0;       // lane 0 past its column 0
+                gA = gA < 0 ? 0 : (gA + 2) / 3 * 3;
+                int gB = min(kb + a.L - 3, total - 3) - t0;  // lane 31's group ends by column L-1
+                gB = min(gB, n - 3);
+                if (gB < gA) continue;
+                gB = gB / 3 * 3;
+#pragma unroll 1
+                for (; g < gA; g += 3) {
+                    backwardStep<R, MODE, 0, false, SH>(b, a, win, lane, total, x, exact);
+                    backwardStep<R, MODE, 1, false, SH>(b, a, win, lane, total, x, exact);
+                    backwardStep<R, MODE, 2, false, SH>(b, a, win, lane, total, x, exact);
+                }
+                const float *eBase = a.smE + (a.nS - 1 - b.sp) * S + lane * R;
+                const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
+                const bool ringWriter = lane == 0 && b.sp < a.nS - 1;
+#pragma unroll 1
+                for (; g <= gB; g += 3) {
+                    backwardInterior<R, MODE, 0, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
+                    backwardInterior<R, MODE, 1, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
+                    backwardInterior<R, MODE, 2, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
+                }
+                // a lane whose last step was its stripe's column L-1 = P-1 moves to the next stripe
+                if (b.jj == a.P) {
+                    b.jj = 0;
+                    ++b.sp;
+                }
             }
-            // a lane whose last step was its stripe's column L-1 = P-1 moves to the next stripe
-            if (b.jj == a.P) {
-                b.jj = 0;
-                ++b.sp;
+#pragma unroll 1
+            for (; g < n; g += 3) {
+                backwardStep<R, MODE, 0, false, SH>(b, a, win, lane, total, x, exact);
+                backwardStep<R, MODE, 1, false, SH>(b, a, win, lane, total, x, exact);
+                backwardStep<R, MODE, 2, false, SH>(b, a, win, lane, total, x, exact);
             }
             continue;
         }
@@ -839,7 +873,8 @@ struct FwdState {
 // ascending order with scoreLess (the first row wins ties); the stripe's top
 // lane writes the stripe's partial, and the stripes are folded in order after
 // the sweep.
-template <int R, int MODE, int PH, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
+template <int R, int MODE, int PH, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay),
+          bool SH = false>
 __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                             int total, const float (&q)[R], const ExactRows *x, ExactBest *exact) {
     constexpr int S = kLanes * R;
@@ -917,7 +952,10 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
         const int eOff = __float_as_int(col.x);  // code * rowPad
         const float bgsC = col.y, prev = col.z;
         float e[R];
-        loadEmit<R>(e, a.smE + eOff + rowBase);
+        if (SH)  // the table in shared memory: a plain shared load
+            loadEmitS<R>(e, (unsigned)__cvta_generic_to_shared(a.smE) + 4u * (unsigned)(eOff + rowBase));
+        else
+            loadEmit<R>(e, a.smE + eOff + rowBase);
         float win0 = inW, yab = inY;
         float stepMax = 0.0f;
         float bv[R];
@@ -1115,7 +1153,8 @@ __device__ __forceinline__ void forwardInterior(FwdState<R, MODE> &f, const Swee
 // One forward step at position P6 of a six-step group: wait for this step's
 // W1 copy, read it from the staging ring, run the step, and stage the W1 of
 // the step kW1Ahead later into the slot this lane read one step ago.
-template <int R, int MODE, int P6, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay)>
+template <int R, int MODE, int P6, bool ANCH = false, bool PIPE = (MODE == kDiscover || MODE == kReplay),
+          bool SH = false>
 __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
                                               int total, W1Stage<R, PIPE> &st,
                                               const ExactRows *x, ExactBest *exact) {
@@ -1134,7 +1173,7 @@ __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepA
 #pragma unroll
         for (int k = 0; k < R; ++k) q[k] = 0.0f;
     }
-    forwardStep<R, MODE, P6 % 3, ANCH, PIPE>(f, a, win, lane, total, q, x, exact);
+    forwardStep<R, MODE, P6 % 3, ANCH, PIPE, SH>(f, a, win, lane, total, q, x, exact);
     if (kReadW1) st.issue(a, win, (P6 + kW1Ahead) % kW1Slots, lane, total);
 }
 
@@ -1177,31 +1216,66 @@ __device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &b
         __syncwarp();
         fillBlock<false>(win, a, t0 + kBlock, lane);
         const int n = (t0 + kBlock < T ? kBlock : T - t0);
-        if (MODE == kMid && interiorBlock(a, t0, n, total, kW1Ahead)) {
+        if (MODE == kMid) {
+            // Interior runs of six-step groups, found per block as in
+            // backwardSweep; an interior group also needs its W1 staging
+            // (kW1Ahead steps further) inside the stripe.
             constexpr int S = kLanes * R;
-            const float *eBase = a.smE + f.s * S + lane * R;
-            const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
-            const bool ringWriter = lane == kLanes - 1 && f.s < a.nS - 1;
-            // the staging cursor is kW1Ahead steps ahead, in the same stripe
-            const float *w1src =
-                a.w1 + (((size_t)f.s * a.D + (a.L - 1 - (f.j + kW1Ahead)) + (kLanes - 1 - lane)) * kLanes + lane) * R;
+            const int u0 = t0 - (kLanes - 1);  // lane 31's local time at the block's first step
+            const int k0 = u0 >= 0 ? u0 / a.P : -1;
+            int g = 0;
 #pragma unroll 1
-            for (int g = 0; g < n; g += 6) {
-                forwardInterior<R, MODE, 0, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                forwardInterior<R, MODE, 1, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                forwardInterior<R, MODE, 2, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                forwardInterior<R, MODE, 3, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                forwardInterior<R, MODE, 4, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                forwardInterior<R, MODE, 5, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+            for (int kk = 0; kk < 2; ++kk) {
+                const int kb = (k0 + kk) * a.P;
+                if (kb < 0) continue;
+                int gA = kb + kLanes - t0;
+                gA = gA < 0 ? 0 : (gA + 5) / 6 * 6;
+                int gB = min(kb + a.L - 6 - kW1Ahead, total - 6 - kW1Ahead) - t0;
+                gB = min(gB, n - 6);
+                if (gB < gA) continue;
+                gB = gB / 6 * 6;
+#pragma unroll 1
+                for (; g < gA; g += 6) {
+                    forwardStaged<R, MODE, 0, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                    forwardStaged<R, MODE, 1, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                    forwardStaged<R, MODE, 2, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                    forwardStaged<R, MODE, 3, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                    forwardStaged<R, MODE, 4, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                    forwardStaged<R, MODE, 5, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                }
+                const float *eBase = a.smE + f.s * S + lane * R;
+                const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
+                const bool ringWriter = lane == kLanes - 1 && f.s < a.nS - 1;
+                // the staging cursor is kW1Ahead steps ahead, in the same stripe
+                const float *w1src =
+                    a.w1 + (((size_t)f.s * a.D + (a.L - 1 - (f.j + kW1Ahead)) + (kLanes - 1 - lane)) * kLanes + lane) * R;
+#pragma unroll 1
+                for (; g <= gB; g += 6) {
+                    forwardInterior<R, MODE, 0, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                    forwardInterior<R, MODE, 1, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                    forwardInterior<R, MODE, 2, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                    forwardInterior<R, MODE, 3, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                    forwardInterior<R, MODE, 4, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                    forwardInterior<R, MODE, 5, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
+                }
+                // the staging cursor stays kW1Ahead steps ahead: in the same stripe
+                // (f ends at most at column L-5), or at the next stripe's start
+                st.u = f.u + kW1Ahead;
+                st.j = f.j + kW1Ahead;
+                st.s = f.s;
+                if (st.j == a.P) {
+                    st.j = 0;
+                    ++st.s;
+                }
             }
-            // the staging cursor stays kW1Ahead steps ahead: in the same stripe
-            // (f ends at most at column L-5), or at the next stripe's start
-            st.u = f.u + kW1Ahead;
-            st.j = f.j + kW1Ahead;
-            st.s = f.s;
-            if (st.j == a.P) {
-                st.j = 0;
-                ++st.s;
+#pragma unroll 1
+            for (; g < n; g += 6) {
+                forwardStaged<R, MODE, 0, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                forwardStaged<R, MODE, 1, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                forwardStaged<R, MODE, 2, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                forwardStaged<R, MODE, 3, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                forwardStaged<R, MODE, 4, false, false, SH>(f, a, win, lane, total, st, x, exact);
+                forwardStaged<R, MODE, 5, false, false, SH>(f, a, win, lane, total, st, x, exact);
             }
             continue;
         }
@@ -1300,9 +1374,11 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
 
 // CTA shapes: WARPS warps share one shared-memory copy of the profile's
 // emission table, one CTA per SM; 16 warps leave 128 registers per thread,
-// 8 warps 255.  The autotuner picks the shape per rows-per-lane value.
+// 12 warps 168 and 8 warps 255.  The autotuner picks the shape per
+// rows-per-lane value.
 constexpr int kCtaWarps = 16;       // the default (and widest) shape
 constexpr int kCtaWarpsNarrow = 8;
+constexpr int kCtaWarpsMid = 12;
 
 // Persistent kernel for one rows-per-lane value: CTAs pull chunks
 // (same-profile runs of pairs, costliest first) from a global counter, stage

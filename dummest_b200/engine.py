@@ -467,14 +467,16 @@ class Context:
 
     def autotune(self, seq_ids: Sequence[int], profile_ids: Sequence[int]) -> dict:
         """Time every kernel shape on these pairs (dmst_autotune); returns the
-        rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)."""
+        rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)
+        (dmst_tuned_rates)."""
         n = len(seq_ids)
         pairs = (F.Pair * n)()
         for k, (s, p) in enumerate(zip(seq_ids, profile_ids)):
             pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, p, -2.0
-        out = (C.c_double * 6)()
-        self._check(self.lib.dmst_autotune(self.h, pairs, n, out), "dmst_autotune")
-        return {(r, w): out[i * 2 + j] for i, r in enumerate((4, 2, 1)) for j, w in enumerate((16, 8))}
+        self._check(self.lib.dmst_autotune(self.h, pairs, n, None), "dmst_autotune")
+        out = (C.c_double * 9)()
+        self._check(self.lib.dmst_tuned_rates(self.h, out), "dmst_tuned_rates")
+        return {(r, w): out[i * 3 + j] for i, r in enumerate((4, 2, 1)) for j, w in enumerate((16, 8, 12))}
 
     def set_wait_limit(self, iterations: int = 0) -> None:
         """The exact path's wait budget in 64 ns sleeps (dmst_set_wait_limit; 0: the default)."""
