@@ -237,6 +237,43 @@ void bury(void *p, bool host, size_t bytes) {
     if (full) reapGraves();  // frees synchronise the device, as before the graveyard
 }
 
+// cudaMalloc / cudaMallocHost that, when the device (or host) is out of
+// memory, frees the graveyard (synchronising the device) and tries once more:
+// kept buffers never make an allocation fail that would fit without them.
+cudaError_t devAlloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        bool kept;
+        {
+            std::lock_guard<std::mutex> lock(gGraveMutex);
+            kept = !gGraves.empty();
+        }
+        if (kept) {
+            cudaGetLastError();
+            reapGraves();
+            e = cudaMalloc(p, bytes);
+        }
+    }
+    return e;
+}
+
+cudaError_t hostAlloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMallocHost(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        bool kept;
+        {
+            std::lock_guard<std::mutex> lock(gGraveMutex);
+            kept = !gGraves.empty();
+        }
+        if (kept) {
+            cudaGetLastError();
+            reapGraves();
+            e = cudaMallocHost(p, bytes);
+        }
+    }
+    return e;
+}
+
 // ---------------------------------------------------------------------------
 // Small device buffer helper
 // ---------------------------------------------------------------------------
@@ -254,10 +291,10 @@ struct DevBuf {
         if (p) bury(p, false, cap * sizeof(T));
         p = nullptr;
         cap = 0;
-        cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        cudaError_t e = devAlloc((void **)&p, want * sizeof(T));
         if (e != cudaSuccess && want > n) {  // the headroom did not fit: the exact size
             cudaGetLastError();
-            e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+            e = devAlloc((void **)&p, std::max<size_t>(n, 1) * sizeof(T));
             if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
             return e;
         }
@@ -269,7 +306,7 @@ struct DevBuf {
         if (n <= cap && p) return cudaSuccess;
         size_t want = std::max(n, cap * 2);
         T *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, want * sizeof(T));
+        cudaError_t e = devAlloc((void **)&q, want * sizeof(T));
         if (e != cudaSuccess) return e;
         if (p && keep) {
             e = cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
@@ -301,7 +338,7 @@ struct PinnedBuf {
         if (p) bury(p, true, cap * sizeof(T));  // an async copy in flight may still use it
         p = nullptr;
         cap = 0;
-        cudaError_t e = cudaMallocHost((void **)&p, want * sizeof(T));
+        cudaError_t e = hostAlloc((void **)&p, want * sizeof(T));
         if (e == cudaSuccess) cap = want;
         return e;
     }
@@ -1589,14 +1626,26 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // device budget (the call's budget, or 60% of the free memory counting the
     // slots the context already holds).  Long pairs of tall profiles (80 MB of
     // W1 at M = 2000 x 10 kb) then run fewer warps per CTA, or fewer CTAs.
+    // The stores of an earlier posterior or gradient call (dmst_posteriors
+    // and the like keep them for the next such call) are given up when the
+    // slots of a full GPU (every SM at the widest CTA) would not fit without them.
     size_t maxSlots = SIZE_MAX;
     if (mid && !nullOnly) {
         size_t freeB = 0, totalB = 0;
         CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
         const size_t held = (ctx->dW1.cap + ctx->dRing.cap) * sizeof(float);
+        const size_t slotBytes = (w1Slot + ringSlot) * sizeof(float);
+        const size_t adjHeld = (ctx->dAdjF.cap + ctx->dAdjB.cap + ctx->dPost.cap) * sizeof(double);
+        const size_t fullGpu = (size_t)ctx->smCount * kCtaWarps * slotBytes;
+        if (!ctx->opts.device_budget_bytes && adjHeld && 0.6 * (double)(freeB + held) < (double)fullGpu) {
+            ctx->dAdjF.release();  // synchronises the device, once
+            ctx->dAdjB.release();
+            ctx->dPost.release();
+            CK(cudaMemGetInfo(&freeB, &totalB), "memory info");
+        }
         const size_t budget =
             ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (size_t)(0.6 * (double)(freeB + held));
-        maxSlots = std::max<size_t>(1, budget / ((w1Slot + ringSlot) * sizeof(float)));
+        maxSlots = std::max<size_t>(1, budget / slotBytes);
     }
     int chunkPairsOf[3] = {1, 1, 1};
     for (int q = 0; q < 3; ++q) {
@@ -1690,14 +1739,28 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     const size_t nCounters = std::max<size_t>(allChunks.size() + 3, 6);  // search: the second wave's at 3..5
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
 
-    // Null-model jobs: up to 32 pairs of one read per warp.
+    // Null-model jobs: up to 32 pairs of reads of one length per warp (the
+    // lanes run in lock step over the columns), the pairs of one read
+    // side by side.
     std::vector<int> jobPairs(n);
     {
-        // Counting sort of the (profile-major) pair slots by sequence id.
+        // A counting sort of the (profile-major) pair slots by read, with the
+        // call's reads taken in (length, id) order.
         const size_t nSeq = ctx->seqLen.size();
-        std::vector<int> start(nSeq + 1, 0);
-        for (size_t k = 0; k < n; ++k) ++start[pairs[order[k]].seq + 1];
-        for (size_t q = 0; q < nSeq; ++q) start[q + 1] += start[q];
+        std::vector<int> start(nSeq, 0);  // pairs of each read, then where they start
+        for (size_t k = 0; k < n; ++k) ++start[pairs[order[k]].seq];
+        std::vector<int> used;
+        for (size_t q = 0; q < nSeq; ++q)
+            if (start[q]) used.push_back((int)q);
+        std::sort(used.begin(), used.end(), [&](int x, int y) {
+            return ctx->seqLen[x] != ctx->seqLen[y] ? ctx->seqLen[x] < ctx->seqLen[y] : x < y;
+        });
+        int at = 0;
+        for (int q : used) {
+            const int c = start[q];
+            start[q] = at;
+            at += c;
+        }
         for (size_t k = 0; k < n; ++k) jobPairs[start[pairs[order[k]].seq]++] = (int)k;
     }
     std::vector<NullJob> nullJobs;
@@ -1705,7 +1768,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     long long nullTmpEntries = 0;
     for (size_t k = 0; k < n;) {
         size_t e = k;
-        while (e < n && e - k < 32 && dp[jobPairs[e]].codeOff == dp[jobPairs[k]].codeOff) ++e;
+        while (e < n && e - k < 32 && dp[jobPairs[e]].L == dp[jobPairs[k]].L) ++e;
         nullJobs.push_back(NullJob{(int)k, (int)(e - k)});
         nullTmpOff.push_back(nullTmpEntries);
         nullTmpEntries += dmst::nullTmpEntries(dp[jobPairs[k]].L);

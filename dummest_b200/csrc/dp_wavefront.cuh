@@ -268,6 +268,22 @@ __device__ __forceinline__ float fmax3(float a, float b, float c) {
     return r;
 }
 
+// The step's share of the float filter best, max over the lane's rows of
+// W1 * prefixSeed[j] (fast modes).  A correctly rounded product by prev >= 0
+// is monotone in W (with flush to zero as well), so the largest product is
+// the product of the largest W, and a NaN W (an overflowed value times a zero
+// factor) is passed over by the max in both forms: the same bits with R - 2
+// fewer multiplies at R = 4.
+template <int R>
+__device__ __forceinline__ float stepFilt(float filt, const float (&wv)[R], float prev) {
+    if constexpr (R == 4)
+        return fmax3(filt, fmax3(wv[0], wv[1], wv[2]) * prev, wv[3] * prev);
+    else if constexpr (R == 2)
+        return fmax3(filt, wv[0] * prev, wv[1] * prev);
+    else
+        return fmaxf(filt, wv[0] * prev);
+}
+
 // The ring a stripe reads (written by the stripe before it in processing order).
 template <bool EXACT>
 __device__ __forceinline__ const float *ringOfPrev(const SweepArgs &a, int k) {
@@ -494,7 +510,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             p[k] = (h3 * e[k]) * b.c.enter[k];
         }
         float bW1 = b.rb[I1], bW2 = b.rb[I2], bY = inY;
-        float wv[R], yv[R], fv[R];
+        float wv[R], yv[R];
         float stepMax = 0.0f;
 #pragma unroll
         for (int k = R - 1; k >= 0; --k) {
@@ -513,10 +529,7 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
             const float W = __fmaf_rn(sufv, b.c.rs[k], acc);
             const float Y = __fmaf_rn(b.c.eps[k], bY, W);
             const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
-            if (MODE == kFilter || MODE == kMid) {
-                yv[k] = Y;
-                fv[k] = W * prev;
-            }
+            if (MODE == kFilter || MODE == kMid) yv[k] = Y;
             if (MODE == kDiscover) {
                 b.rmax[k] = fmaxf(b.rmax[k], Y);  // Y >= W1 at every cell
                 stepMax = fmaxf(stepMax, Y);
@@ -543,15 +556,8 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
         if (MODE == kFilter || MODE == kMid) {
             // running maxima, two rows per three-input max
 #pragma unroll
-            for (int k = 0; k < R; k += 2) {
-                if (k + 1 < R) {
-                    b.maxY = fmax3(b.maxY, yv[k], yv[k + 1]);
-                    b.filt = fmax3(b.filt, fv[k], fv[k + 1]);
-                } else {
-                    b.maxY = fmaxf(b.maxY, yv[k]);
-                    b.filt = fmaxf(b.filt, fv[k]);
-                }
-            }
+            for (int k = 0; k < R; k += 2) b.maxY = (k + 1 < R) ? fmax3(b.maxY, yv[k], yv[k + 1]) : fmaxf(b.maxY, yv[k]);
+            b.filt = stepFilt<R>(b.filt, wv, prev);
         }
         b.rb[I3] = inW;
         b.sendW = wv[0];
@@ -660,7 +666,7 @@ __device__ __forceinline__ void backwardInterior(BwdState<R, MODE> &b, const Swe
 #pragma unroll
     for (int k = 0; k < R - 1; ++k) p[k] = (b.h[I3][k + 1] * e[k]) * b.c.enter[k];
     float bW1 = b.rb[I1], bW2 = b.rb[I2], bY = inY;
-    float wv[R], yv[R], fv[R];
+    float wv[R], yv[R];
 #pragma unroll
     for (int k = R - 1; k >= 0; --k) {
         float acc = p[k];
@@ -675,7 +681,6 @@ __device__ __forceinline__ void backwardInterior(BwdState<R, MODE> &b, const Swe
         const float Y = __fmaf_rn(b.c.eps[k], bY, W);
         const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
         yv[k] = Y;
-        fv[k] = W * prev;
         bW1 = b.h[I1][k];
         bW2 = b.h[I2][k];
         bY = Y;
@@ -684,15 +689,8 @@ __device__ __forceinline__ void backwardInterior(BwdState<R, MODE> &b, const Swe
         b.z[I3][k] = Z;
     }
 #pragma unroll
-    for (int k = 0; k < R; k += 2) {
-        if (k + 1 < R) {
-            b.maxY = fmax3(b.maxY, yv[k], yv[k + 1]);
-            b.filt = fmax3(b.filt, fv[k], fv[k + 1]);
-        } else {
-            b.maxY = fmaxf(b.maxY, yv[k]);
-            b.filt = fmaxf(b.filt, fv[k]);
-        }
-    }
+    for (int k = 0; k < R; k += 2) b.maxY = (k + 1 < R) ? fmax3(b.maxY, yv[k], yv[k + 1]) : fmaxf(b.maxY, yv[k]);
+    b.filt = stepFilt<R>(b.filt, wv, prev);
     b.rb[I3] = inW;
     b.sendW = wv[0];
     b.sendY = bY;

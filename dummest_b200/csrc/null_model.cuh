@@ -157,11 +157,12 @@ __device__ __forceinline__ XS prefixStep(int i, const float *bg, const uint8_t *
     return batchAdd(codon, batchAdd(single, dbl));
 }
 
-// Pairs that share a read are scored by one warp, one lane per pair: the
-// lanes run in lock step over the same codon codes (one broadcast load per
-// column), keep the suffix recurrence in registers, store the temporary
-// suffix probabilities interleaved (one coalesced 256-byte store per column),
-// and write their seed vectors through a shared-memory transpose, so that each
+// Pairs whose reads have one length are scored by one warp, one lane per
+// pair (the pairs of one read side by side, so that their codon loads are
+// broadcasts): the lanes run in lock step over the L columns, keep the
+// suffix recurrence in registers, store the temporary prefix and suffix
+// probabilities interleaved (one coalesced 256-byte store per column), and
+// write their seed vectors through a shared-memory transpose, so that each
 // store instruction writes 32 consecutive seeds of one pair.
 // Temporary ExpScores of one null-model job: the prefix [L][32] and the
 // suffix [L+1][32] probabilities of its (up to) 32 pairs, interleaved.
