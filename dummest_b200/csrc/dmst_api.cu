@@ -896,12 +896,14 @@ int dmst_profile_length(const dmst_ctx *ctx, int id) {
 
 static int uploadProfiles(dmst_ctx *ctx) {
     if (!ctx->profilesDirty) return DMST_OK;
+    // Per profile: its (M+2) x 11 Params, then its DP coefficient planes
+    // (coefOffOf).
     size_t nE = 0, nP = 0;
     for (auto &p : ctx->profiles) {
         nE += p.emit.size();
-        nP += p.params.size();
+        nP = (size_t)coefOffOf((long long)nP, p.M) + (size_t)kCoefPlanes * p.rowPad;
     }
-    std::vector<float> emit(nE), par(nP);
+    std::vector<float> emit(nE), par(nP, 0.0f);
     std::vector<DevProfile> desc(ctx->profiles.size());
     size_t oE = 0, oP = 0;
     ctx->maxRowPad = 0;
@@ -909,6 +911,12 @@ static int uploadProfiles(dmst_ctx *ctx) {
         auto &p = ctx->profiles[i];
         std::copy(p.emit.begin(), p.emit.end(), emit.begin() + oE);
         std::copy(p.params.begin(), p.params.end(), par.begin() + oP);
+        const size_t oC = (size_t)coefOffOf((long long)oP, p.M);
+        for (int r = 0; r <= p.M; ++r) {
+            for (int q = 0; q < kCoefPlanes - 1; ++q)
+                par[oC + (size_t)q * p.rowPad + r] = p.params[(size_t)r * kParamFloats + kCoefParam[q]];
+            par[oC + (size_t)kPRs * p.rowPad + r] = 1.0f;
+        }
         DevProfile &d = desc[i];
         d.M = p.M;
         d.rowPad = p.rowPad;
@@ -916,7 +924,7 @@ static int uploadProfiles(dmst_ctx *ctx) {
         d.paramOff = (long long)oP;
         std::memcpy(d.bg, p.bg, sizeof d.bg);
         oE += p.emit.size();
-        oP += p.params.size();
+        oP = oC + (size_t)kCoefPlanes * p.rowPad;
         ctx->maxRowPad = std::max(ctx->maxRowPad, p.rowPad);
     }
     CK(ctx->dEmit.ensure(nE), "alloc emission tables");

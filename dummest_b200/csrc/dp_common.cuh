@@ -29,6 +29,17 @@ struct DevProfile {
 };
 static_assert(sizeof(DevProfile) == 128, "DevProfile layout");
 
+// The DP coefficient planes of a profile follow its Params in the params
+// buffer, 16-byte aligned: kCoefPlanes planes of rowPad floats, one value per
+// profile row (the Params entry the recurrences read), 0 on the padding rows
+// past M; the last plane holds 1 on rows 0..M (the seed term's row factor).
+// A lane loads its R consecutive rows of a plane with one vector load.
+enum CoefPlane { kPA0, kPA1, kPA2, kPB0, kPD0, kPD1, kPD2, kPEps, kPEnter, kPRs, kCoefPlanes };
+constexpr int kCoefParam[kCoefPlanes - 1] = {0, 1, 2, 3, 6, 7, 8, 9, 10};  // Params index of each plane
+__host__ __device__ constexpr long long coefOffOf(long long paramOff, int M) {
+    return (paramOff + (long long)(M + 2) * kParamFloats + 3) / 4 * 4;
+}
+
 // One (sequence, profile) pair of a scoring call.
 struct DevPair {
     long long codeOff;  // byte offset of the sequence's codon codes

@@ -54,7 +54,8 @@ __global__ void __launch_bounds__(kPlainWarps * kLanes, 1)
         c.codes = codes + p.codeOff;
         c.pre = seeds + p.seedOff;
         c.suf = c.pre + p.L;
-        c.params = params + pr.paramOff;
+        c.coef = params + coefOffOf(pr.paramOff, pr.M);
+        c.coefStride = pr.rowPad;
         c.smBg = smBg;
         c.sc = scales[pi];
         c.M = p.M;

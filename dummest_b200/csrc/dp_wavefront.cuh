@@ -55,11 +55,12 @@ struct PairCold {
     const uint8_t *codes;   // codon codes of the read
     const float *pre;       // prefixSeed[L]
     const float *suf;       // suffixSeedFromNext[L]
-    const float *params;    // the profile's (M+2) x 11 Params
+    const float *coef;      // the profile's DP coefficient planes (coefOffOf)
     const float *smBg;      // bg_probs[4 + c] in shared memory
     PairScales sc;
     int M;
-    int pad[3];
+    int coefStride;         // floats between planes (the profile's rowPad)
+    int pad[2];
 };
 
 struct SweepArgs {
@@ -88,8 +89,11 @@ struct SweepArgs {
     __device__ __forceinline__ const float *suf() const {
         return *reinterpret_cast<const float *const volatile *>(&cold->suf);
     }
-    __device__ __forceinline__ const float *params() const {
-        return *reinterpret_cast<const float *const volatile *>(&cold->params);
+    __device__ __forceinline__ const float *coef() const {
+        return *reinterpret_cast<const float *const volatile *>(&cold->coef);
+    }
+    __device__ __forceinline__ int coefStride() const {
+        return *reinterpret_cast<const volatile int *>(&cold->coefStride);
     }
     __device__ __forceinline__ const float *smBg() const {
         return *reinterpret_cast<const float *const volatile *>(&cold->smBg);
@@ -106,61 +110,65 @@ struct Coef {
     float enter[R], a0[R], a1[R], a2[R], b0[R], d0[R], d1[R], d2[R], eps[R], rs[R];
 };
 
-// Backward coefficients of rows rowBase..rowBase+R-1 (dummest-dp-backward.hh:481-494).
+// R consecutive rows of a coefficient plane (read-only in every kernel).
+template <int R>
+__device__ __forceinline__ void loadRows(float (&v)[R], const float *p) {
+    if constexpr (R == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (R == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+
+// v[k] = plane[row k] * s, rounded as the reference's float product; a
+// padding row (plane value 0) gives 0, as the scales are finite.
+template <int R>
+__device__ __forceinline__ void loadScaled(float (&v)[R], const float *p, float s) {
+    loadRows<R>(v, p);
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = v[k] * s;
+}
+
+// Backward coefficients of rows rowBase..rowBase+R-1 (dummest-dp-backward.hh:481-494):
+// the Params products with the pair's scales; rows past M get 0 (rs 0).
 template <int R>
 __device__ __forceinline__ void loadBackwardCoef(Coef<R> &c, const SweepArgs &a, int rowBase) {
-    const int M = a.M();
-    const float *params = a.params();
+    const float *q = a.coef() + rowBase;
+    const int st = a.coefStride();
     const PairScales sc = a.sc();
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int i = rowBase + k;
-        if (i <= M) {
-            const float *q = params + (size_t)i * kParamFloats;
-            c.enter[k] = q[10] * sc.sC;
-            c.d0[k] = q[6];
-            c.d1[k] = q[7] * sc.s2;
-            c.d2[k] = q[8] * sc.s1;
-            c.a0[k] = q[0] * sc.sC;
-            c.a1[k] = q[1] * sc.s1;
-            c.a2[k] = q[2] * sc.s2;
-            c.b0[k] = q[3] * sc.sC;
-            c.eps[k] = q[9];
-            c.rs[k] = 1.0f;
-        } else {
-            c.enter[k] = c.d0[k] = c.d1[k] = c.d2[k] = c.a0[k] = c.a1[k] = c.a2[k] = c.b0[k] = c.eps[k] = 0.0f;
-            c.rs[k] = 0.0f;
-        }
-    }
+    loadScaled<R>(c.enter, q + kPEnter * st, sc.sC);
+    loadRows<R>(c.d0, q + kPD0 * st);
+    loadScaled<R>(c.d1, q + kPD1 * st, sc.s2);
+    loadScaled<R>(c.d2, q + kPD2 * st, sc.s1);
+    loadScaled<R>(c.a0, q + kPA0 * st, sc.sC);
+    loadScaled<R>(c.a1, q + kPA1 * st, sc.s1);
+    loadScaled<R>(c.a2, q + kPA2 * st, sc.s2);
+    loadScaled<R>(c.b0, q + kPB0 * st, sc.sC);
+    loadRows<R>(c.eps, q + kPEps * st);
+    loadRows<R>(c.rs, q + kPRs * st);
 }
 
 // Forward coefficients (dummest-dp-forward.hh:72-83): alpha'0 and beta'0 stay
 // unscaled here, the codon scale multiplies the background term instead.
 template <int R>
 __device__ __forceinline__ void loadForwardCoef(Coef<R> &c, const SweepArgs &a, int rowBase) {
-    const int M = a.M();
-    const float *params = a.params();
+    const float *q = a.coef() + rowBase;
+    const int st = a.coefStride();
     const PairScales sc = a.sc();
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const int i = rowBase + k;
-        if (i <= M) {
-            const float *q = params + (size_t)i * kParamFloats;
-            c.enter[k] = q[10] * sc.sC;
-            c.a0[k] = q[0];
-            c.a1[k] = q[1] * sc.s1;
-            c.a2[k] = q[2] * sc.s2;
-            c.b0[k] = q[3];
-            c.d0[k] = q[6];
-            c.d1[k] = q[7] * sc.s2;
-            c.d2[k] = q[8] * sc.s1;
-            c.eps[k] = q[9];
-            c.rs[k] = 1.0f;
-        } else {
-            c.enter[k] = c.d0[k] = c.d1[k] = c.d2[k] = c.a0[k] = c.a1[k] = c.a2[k] = c.b0[k] = c.eps[k] = 0.0f;
-            c.rs[k] = 0.0f;
-        }
-    }
+    loadScaled<R>(c.enter, q + kPEnter * st, sc.sC);
+    loadRows<R>(c.a0, q + kPA0 * st);
+    loadScaled<R>(c.a1, q + kPA1 * st, sc.s1);
+    loadScaled<R>(c.a2, q + kPA2 * st, sc.s2);
+    loadRows<R>(c.b0, q + kPB0 * st);
+    loadRows<R>(c.d0, q + kPD0 * st);
+    loadScaled<R>(c.d1, q + kPD1 * st, sc.s2);
+    loadScaled<R>(c.d2, q + kPD2 * st, sc.s1);
+    loadRows<R>(c.eps, q + kPEps * st);
+    loadRows<R>(c.rs, q + kPRs * st);
 }
 
 template <int R>
@@ -1327,7 +1335,9 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
         c.codes = g.codes + p.codeOff;
         c.pre = g.seeds + p.seedOff;
         c.suf = c.pre + p.L;
-        c.params = g.params + g.profiles[p.prof].paramOff;
+        const DevProfile &pr = g.profiles[p.prof];
+        c.coef = g.params + coefOffOf(pr.paramOff, pr.M);
+        c.coefStride = pr.rowPad;
         c.smBg = smBg;
         c.sc = g.scales[pi];
         c.M = p.M;
