@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--mmax", type=int, default=800,
+                    help="batched workload: longest profile (M log-uniform from 50; smaller cases for profiling)")
     ap.add_argument("--lmax", type=int, default=3000,
                     help="longest read of the batched workload (3000 in the stated configuration; smaller "
                          "values only to keep a profiling capture's device memory small)")
@@ -188,8 +190,8 @@ def workload_config(args, world: int) -> dict:
     if args.workload == "search":
         return {
             "workload": f"two-wave search (float filter on every pair, mid-anchored score on survivors, E <= "
-                        f"{SEARCH_E:g}): {args.profiles} profiles M log-uniform 50-800 x reads L log-uniform "
-                        "150-3000 nt, GC 0.4-0.6, 10% implants, both strands; gates from each profile's "
+                        f"{SEARCH_E:g}): {args.profiles} profiles M log-uniform 50-{args.mmax} x reads L "
+                        f"log-uniform 150-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands; gates from each profile's "
                         "calibration (200 x 3 kb random sequences)",
             "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
             "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
@@ -234,7 +236,7 @@ def workload_config(args, world: int) -> dict:
             "parallelism": f"replicas x{world} (one genome per rank)",
         }
     return {
-        "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform 50-800 x "
+        "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform 50-{args.mmax} x "
                     f"reads L log-uniform 150-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands",
         "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
         "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
@@ -243,10 +245,10 @@ def workload_config(args, world: int) -> dict:
     }
 
 
-def make_profiles(seed, n):
+def make_profiles(seed, n, mmax=800):
     from dummest_b200 import synth
     rng = np.random.default_rng(seed)
-    Ms = np.exp(rng.uniform(np.log(50), np.log(800), size=n)).round().astype(int)
+    Ms = np.exp(rng.uniform(np.log(50), np.log(mmax), size=n)).round().astype(int)
     profiles = [synth.make_profile(rng, int(M), f"synth{k:03d}") for k, M in enumerate(Ms)]
     return profiles, synth.hmmer3_text(profiles)
 
@@ -273,7 +275,7 @@ def make_workload(args, rank: int, n_steps: int, world: int = 0):
                      + synth.random_dna(rng, 500) for _ in range(args.al_reads)]
             steps.append(synth.both_strands(reads))
         return [prof], synth.hmmer3_text([prof]), steps
-    profiles, txt = make_profiles(args.seed, args.profiles)
+    profiles, txt = make_profiles(args.seed, args.profiles, args.mmax)
     if world >= 1:
         per = world * args.reads_per_step
         n_sets = n_steps if world == 1 else min(n_steps, args.warmup + -(-100_000 // per))

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("DMST_LIB") or os.path.join(HERE, "libdummest_b200.so")
 
 DMST_OK = 0
+DMST_HMM_MASK = 0x100
 DMST_EINVAL = -1
 DMST_ENOMEM = -2
 DMST_EDEVICE = -3
@@ -61,6 +62,7 @@ class Opts(C.Structure):
         ("device", C.c_int),
         ("rows_per_lane", C.c_int),
         ("device_budget_bytes", C.c_size_t),
+        ("tantan_threshold", C.c_double),
     ]
 
 

@@ -644,6 +644,7 @@ void dmst_opts_default(dmst_opts *o) {
     o->device = 0;
     o->rows_per_lane = 0;
     o->device_budget_bytes = 0;
+    o->tantan_threshold = 0.5;
 }
 
 const char *dmst_strerror(int status) { return statusText(status); }
@@ -858,7 +859,9 @@ int dmst_hmm_finalize(const char *text, size_t len, int index, int background_ty
     Rates r{(float)o.insert1, (float)o.insert2, (float)o.delete1, (float)o.delete2, (float)o.stop_codon_prob,
             (float)o.bg_stop_codon_prob};
     FinalProfile f;
-    if (finalizeProfile(raws[index], r, background_type ? background_type : 'G', f, nullptr) < 0) return DMST_EPARSE;
+    const int type = background_type & 0xff;
+    const double maskAt = (background_type & DMST_HMM_MASK) ? o.tantan_threshold : -1.0;
+    if (finalizeProfile(raws[index], r, type ? type : 'G', f, nullptr, maskAt) < 0) return DMST_EPARSE;
     std::memcpy(values, f.values.data(), f.values.size() * sizeof(float));
     if (params) std::memcpy(params, f.params.data(), f.params.size() * sizeof(Params));
     if (bg) std::memcpy(bg, f.bg.data(), f.bg.size() * sizeof(float));
@@ -875,9 +878,11 @@ int dmst_profile_load_hmm(dmst_ctx *ctx, const char *text, size_t len, int backg
     std::string e;
     if (parseHmmText(text, len, raws, &e) < 0) return ctx->fail(DMST_EPARSE, "HMMER3: %s", e.c_str());
     int first = (int)ctx->profiles.size();
+    const int type = background_type & 0xff;
+    const double maskAt = (background_type & DMST_HMM_MASK) ? ctx->opts.tantan_threshold : -1.0;
     for (auto &raw : raws) {
         FinalProfile f;
-        if (finalizeProfile(raw, ctx->rates, background_type ? background_type : 'G', f, &e) < 0)
+        if (finalizeProfile(raw, ctx->rates, type ? type : 'G', f, &e, maskAt) < 0)
             return ctx->fail(DMST_EPARSE, "profile %s: %s", raw.name.c_str(), e.c_str());
         int st = dmst_profile_add(ctx, f.values.data(), f.width, f.M,
                                   reinterpret_cast<const dmst_params *>(f.params.data()), f.bg.data(), nullptr);

@@ -184,16 +184,143 @@ int parseHmmText(const char *text, size_t len, std::vector<RawProfile> &out, std
 }
 
 // ---------------------------------------------------------------------------
-// finalizeProfile (dummest-profile.hh:105-233), FP32 engine, no tantan masking
-// and no letter-probability filtering.
+// Repeat probabilities of a protein sequence: tantan (M. C. Frith, "A new
+// repeat-masking method enables specific detection of homologous sequences",
+// Nucleic Acids Res. 39:e23, 2011).  A hidden Markov model with a background
+// state and one repeat state per offset k = 1..K, in which a letter is
+// emitted with the likelihood ratio of its pair with the letter k back.  The
+// forward pass runs over the sequence with the states rescaled every 16
+// letters, the backward pass returns over it with the same factors, and the
+// repeat probability of a letter is 1 - P(background at the letter).  The
+// parameters are the ones the reference engine passes for a profile's
+// consensus (tantan-wrapper.hh:13-72, the protein case): BLOSUM62 likelihood
+// ratios exp(lambda s) with lambda = 0.32403216734804408 and s = -4 for
+// letters outside the 20, K = 50, repeat start 0.005, repeat end 0.05, offset
+// weights decaying by 0.9, no gaps.  The sums over offsets are taken as four
+// interleaved partial sums, as the reference's 4-wide build takes them.
+// ---------------------------------------------------------------------------
+static void tantanProteinProbs(const uint8_t *seq, int n, float *prob) {
+    // BLOSUM62 (Henikoff & Henikoff 1992), rows and columns in the order
+    // ARNDCQEGHILKMFPSTWYV, as usually published.
+    static const char kOrder[] = "ARNDCQEGHILKMFPSTWYV";
+    static const signed char kBlosum[20][20] = {
+        {4, -1, -2, -2, 0, -1, -1, 0, -2, -1, -1, -1, -1, -2, -1, 1, 0, -3, -2, 0},
+        {-1, 5, 0, -2, -3, 1, 0, -2, 0, -3, -2, 2, -1, -3, -2, -1, -1, -3, -2, -3},
+        {-2, 0, 6, 1, -3, 0, 0, 0, 1, -3, -3, 0, -2, -3, -2, 1, 0, -4, -2, -3},
+        {-2, -2, 1, 6, -3, 0, 2, -1, -1, -3, -4, -1, -3, -3, -1, 0, -1, -4, -3, -3},
+        {0, -3, -3, -3, 9, -3, -4, -3, -3, -1, -1, -3, -1, -2, -3, -1, -1, -2, -2, -1},
+        {-1, 1, 0, 0, -3, 5, 2, -2, 0, -3, -2, 1, 0, -3, -1, 0, -1, -2, -1, -2},
+        {-1, 0, 0, 2, -4, 2, 5, -2, 0, -3, -3, 1, -2, -3, -1, 0, -1, -3, -2, -2},
+        {0, -2, 0, -1, -3, -2, -2, 6, -2, -4, -4, -2, -3, -3, -2, 0, -2, -2, -3, -3},
+        {-2, 0, 1, -1, -3, 0, 0, -2, 8, -3, -3, -1, -2, -1, -2, -1, -2, -2, 2, -3},
+        {-1, -3, -3, -3, -1, -3, -3, -4, -3, 4, 2, -3, 1, 0, -3, -2, -1, -3, -1, 3},
+        {-1, -2, -3, -4, -1, -2, -3, -4, -3, 2, 4, -2, 2, 0, -3, -2, -1, -2, -1, 1},
+        {-1, 2, 0, -1, -3, 1, 1, -2, -1, -3, -2, 5, -1, -3, -1, 0, -1, -3, -2, -2},
+        {-1, -1, -2, -3, -1, 0, -2, -3, -2, 1, 2, -1, 5, 0, -2, -1, -1, -1, -1, 1},
+        {-2, -3, -3, -3, -2, -3, -3, -3, -1, 0, 0, -3, 0, 6, -4, -2, -2, 1, 3, -1},
+        {-1, -2, -2, -1, -3, -1, -1, -2, -2, -3, -3, -1, -2, -4, 7, -1, -1, -4, -3, -2},
+        {1, -1, 1, 0, -1, 0, 0, 0, -1, -2, -2, 0, -1, -2, -1, 4, 1, -3, -2, -2},
+        {0, -1, 0, -1, -1, -1, -1, -2, -2, -1, -1, -1, -1, -2, -1, 1, 5, -2, -2, 0},
+        {-3, -3, -4, -4, -2, -2, -3, -2, -2, -3, -2, -3, -1, 1, -4, -3, -2, 11, 2, -3},
+        {-2, -2, -2, -3, -2, -1, -2, -3, 2, -1, -1, -2, -1, 3, -3, -2, -2, 2, 7, -1},
+        {0, -3, -3, -3, -1, -2, -2, -3, -3, 3, 1, -2, 1, -1, -2, -2, 0, -3, -1, 4},
+    };
+    constexpr int kLetters = 22;  // codes 20, 21 (U, O) score as the minimum
+    constexpr double kLambda = 0.32403216734804408;
+    constexpr int K = 50;
+    constexpr double kStart = 0.005, kEnd = 0.05, kDecay = 0.9;
+    constexpr int kScaleStep = 16;
+    double lr[kLetters][kLetters];
+    int at[20];  // the published order's index of each of our letters (ACDEFGHIKLMNPQRSTVWY)
+    for (int a = 0; a < 20; ++a) at[a] = (int)(strchr(kOrder, kAlphabet[a]) - kOrder);
+    for (int a = 0; a < kLetters; ++a)
+        for (int b = 0; b < kLetters; ++b)
+            lr[a][b] = std::exp(kLambda * (a < 20 && b < 20 ? kBlosum[at[a]][at[b]] : -4));
+    auto letter = [&](int i) { return seq[i] < kLetters ? seq[i] : kLetters - 1; };
+
+    const double b2b = 1 - kStart, f2b = kEnd, f2f = 1 - kEnd;
+    std::vector<double> b2f(K), fg(K, 0.0), scale(n / kScaleStep);
+    double w = kStart * ((1 - kDecay) / (1 - std::pow(kDecay, K)));  // the first offset's share
+    for (int k = 0; k < K; ++k, w *= kDecay) b2f[k] = w;
+
+    // Forward: prob[i] holds P(prefix ending in the background at i), scaled.
+    double bg = 1.0;
+    for (int i = 0; i < n; ++i) {
+        const double *row = lr[letter(i)];
+        const int off = std::min(i, K);
+        double part[4] = {0, 0, 0, 0};
+        int k = 0;
+        for (; k + 4 <= off; k += 4)
+            for (int q = 0; q < 4; ++q) {
+                const double f = fg[k + q];
+                part[q] += f;
+                fg[k + q] = (bg * b2f[k + q] + f * f2f) * row[letter(i - k - q - 1)];
+            }
+        double fromFg = (part[0] + part[2]) + (part[1] + part[3]);
+        for (; k < off; ++k) {
+            const double f = fg[k];
+            fromFg += f;
+            fg[k] = (bg * b2f[k] + f * f2f) * row[letter(i - k - 1)];
+        }
+        bg = bg * b2b + fromFg * f2b;
+        if (i % kScaleStep == kScaleStep - 1) {
+            const double c = 1 / bg;
+            scale[i / kScaleStep] = c;
+            bg *= c;
+            for (double &x : fg) x *= c;
+        }
+        prob[i] = (float)bg;
+    }
+    double fromFg = 0;
+    for (double x : fg) fromFg += x;
+    const double z = bg * b2b + fromFg * f2b;
+
+    // Backward, folding each position's posterior as it passes.
+    bg = b2b;
+    std::fill(fg.begin(), fg.end(), f2b);
+    for (int i = n - 1; i >= 0; --i) {
+        const double nonRepeat = prob[i] * bg / z;
+        prob[i] = 1 - (float)nonRepeat;
+        if (i % kScaleStep == kScaleStep - 1) {
+            const double c = scale[i / kScaleStep];
+            bg *= c;
+            for (double &x : fg) x *= c;
+        }
+        const double *row = lr[letter(i)];
+        const int off = std::min(i, K);
+        const double toBg = f2b * bg;
+        double part[4] = {0, 0, 0, 0};
+        int k = 0;
+        for (; k + 4 <= off; k += 4)
+            for (int q = 0; q < 4; ++q) {
+                const double f = fg[k + q] * row[letter(i - k - q - 1)];
+                part[q] += b2f[k + q] * f;
+                fg[k + q] = toBg + f2f * f;
+            }
+        double toFg = (part[0] + part[2]) + (part[1] + part[3]);
+        for (; k < off; ++k) {
+            const double f = fg[k] * row[letter(i - k - 1)];
+            toFg += b2f[k] * f;
+            fg[k] = toBg + f2f * f;
+        }
+        bg = b2b * bg + toFg;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// finalizeProfile (dummest-profile.hh:105-233), FP32 engine, with the
+// reference's tantan masking of the consensus (isMask) and without
+// letter-probability filtering.
 // ---------------------------------------------------------------------------
 
-// myMean over `length` rows at `step` (dummest-profile.hh:37-62), unmasked.
-static double columnMean(const float *values, int length, int step, int meanType) {
+// myMean over `length` rows at `step` (dummest-profile.hh:37-62), skipping
+// the masked rows (mask may be null).
+static double columnMean(const float *values, int length, int step, int meanType, const char *mask) {
     double mean = 0;
     int n = 0;
     std::vector<float> forMedian;
     for (int i = 0; i < length; ++i) {
+        if (mask && mask[i]) continue;
         double v = values[(size_t)i * step];
         if (meanType == 'G') mean += std::log(std::max(v, 1e-6));
         if (meanType == 'A') mean += v;
@@ -203,10 +330,11 @@ static double columnMean(const float *values, int length, int step, int meanType
     if (meanType == 'G') return std::exp(mean / n);
     if (meanType == 'A') return mean / n;
     std::sort(forMedian.begin(), forMedian.end());
-    return forMedian[n / 2];
+    return n ? forMedian[n / 2] : 0.0;
 }
 
-int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err) {
+int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err,
+                    double maskThreshold) {
     const int W = p.width, M = p.M;
     const int alphabetSize = W - kNonLetterWidth;
     if (alphabetSize != 20) {
@@ -218,11 +346,32 @@ int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProf
     const float I1 = r.insert1, I2 = r.insert2, D1 = r.delete1, D2 = r.delete2;
     const float STOP = r.stop, BGSTOP = r.bgStop;
 
-    if (end[3] <= 0) end[3] = (float)columnMean(vals + W + 3, M - 1, W, 'G');
+    if (end[3] <= 0) end[3] = (float)columnMean(vals + W + 3, M - 1, W, 'G', nullptr);
+
+    // The consensus: each match row's most probable letter, the first on
+    // ties, as read (dummest-profile.hh:310-312); its letters with repeat
+    // probability >= the threshold are masked (dummest-profile.hh:122-125).
+    std::vector<char> masked(M, 0);
+    f.maskedRows = 0;
+    if (maskThreshold >= 0) {
+        std::vector<uint8_t> consensus(M);
+        for (int i = 0; i < M; ++i) {
+            const float *letters = vals + (size_t)i * W + 4;
+            consensus[i] = (uint8_t)(std::max_element(letters, letters + alphabetSize) - letters);
+        }
+        std::vector<float> prob(M);
+        tantanProteinProbs(consensus.data(), M, prob.data());
+        const float threshold = (float)maskThreshold;  // the reference's Float option
+        for (int i = 0; i < M; ++i) {
+            masked[i] = prob[i] >= threshold;
+            f.maskedRows += masked[i];
+        }
+    }
+    const char *mask = masked.data();
 
     double sumOfMeans = 0;
     for (int k = 4; k < 4 + alphabetSize; ++k) {
-        double mean = columnMean(vals + k, M, W, backgroundType);
+        double mean = columnMean(vals + k, M, W, backgroundType, mask);
         end[k] = (float)mean;
         sumOfMeans += mean;
     }
@@ -269,6 +418,10 @@ int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProf
         probs[2] = (float)delta;
         probs[3] = (float)epsilon;
         for (int k = 4; k < 4 + alphabetSize; ++k) {
+            if (masked[i]) {  // a masked row emits the background
+                probs[k] = end[k];
+                continue;
+            }
             double pr = probs[k];
             int nc = codonCount(kAlphabet[k - 4]);
             probs[k] = (float)((1 - STOP) * pr / nc);

@@ -45,12 +45,16 @@ struct FinalProfile {
     std::vector<float> values;  // (M+1) * width after finalize
     std::vector<Params> params; // M + 2
     std::vector<float> bg;      // width
+    int maskedRows = 0;         // consensus letters masked by tantan
 };
 
 int codonCount(char aa);
 void standardCodeTable(uint8_t out[64]);
 int parseHmmText(const char *text, size_t len, std::vector<RawProfile> &out, std::string *err);
-int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err);
+// maskThreshold >= 0: tantan-mask the consensus (rows whose repeat
+// probability is >= the threshold emit the background and leave the means).
+int finalizeProfile(RawProfile &p, const Rates &r, int backgroundType, FinalProfile &f, std::string *err,
+                    double maskThreshold = -1.0);
 int encodeDna(const char *ascii, int L, char *letters);
 
 // One contig of a FASTA text (readContig, dummest-sequence.hh:6-82).

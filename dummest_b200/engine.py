@@ -127,11 +127,13 @@ class Context:
         self._check(st, "dmst_profile_add")
         return pid.value
 
-    def load_hmm(self, text: str | bytes, background_type: str = "G") -> list[int]:
+    def load_hmm(self, text: str | bytes, background_type: str = "G", mask: bool = False) -> list[int]:
+        """Profile ids of the HMMER3 text's profiles; mask: tantan-mask each
+        consensus as the reference's default (-m 1/3) does."""
         b = text.encode() if isinstance(text, str) else text
         first, count = C.c_int(), C.c_int()
-        st = self.lib.dmst_profile_load_hmm(self.h, b, len(b), ord(background_type), C.byref(first),
-                                            C.byref(count))
+        btype = ord(background_type) | (F.DMST_HMM_MASK if mask else 0)
+        st = self.lib.dmst_profile_load_hmm(self.h, b, len(b), btype, C.byref(first), C.byref(count))
         self._check(st, "dmst_profile_load_hmm")
         return list(range(first.value, first.value + count.value))
 
@@ -573,15 +575,19 @@ def decode_dna(ascii: str | bytes) -> np.ndarray:
     return decode_letters(encode_dna(ascii))
 
 
-def finalize_hmm(text: str | bytes, index: int = 0, background_type: str = "G", rates: dict | None = None):
-    """(name, values (M+1,29), params (M+2,11), bg (29,)) of profile `index`."""
+def finalize_hmm(text: str | bytes, index: int = 0, background_type: str = "G", rates: dict | None = None,
+                 mask: bool = False, tantan_threshold: float = 0.5):
+    """(name, values (M+1,29), params (M+2,11), bg (29,)) of profile `index`;
+    mask: tantan-mask the consensus as the reference's default (-m 1/3) does."""
     lib = F.load()
     b = text.encode() if isinstance(text, str) else text
     o = default_opts()
     for k, v in (rates or {}).items():
         setattr(o, k, float(v))
+    o.tantan_threshold = float(tantan_threshold)
+    btype = ord(background_type) | (F.DMST_HMM_MASK if mask else 0)
     M = C.c_int()
-    st = lib.dmst_hmm_finalize(b, len(b), index, ord(background_type), C.byref(o), C.byref(M), None, None, None,
+    st = lib.dmst_hmm_finalize(b, len(b), index, btype, C.byref(o), C.byref(M), None, None, None,
                                None, 0)
     if st != F.DMST_OK:
         raise ValueError(f"dmst_hmm_finalize: status {st}")
@@ -590,7 +596,7 @@ def finalize_hmm(text: str | bytes, index: int = 0, background_type: str = "G", 
     params = np.zeros((M + 2, 11), np.float32)
     bg = np.zeros(29, np.float32)
     name = C.create_string_buffer(256)
-    st = lib.dmst_hmm_finalize(b, len(b), index, ord(background_type), C.byref(o), C.byref(C.c_int()),
+    st = lib.dmst_hmm_finalize(b, len(b), index, btype, C.byref(o), C.byref(C.c_int()),
                                values.ctypes.data_as(C.POINTER(C.c_float)),
                                params.ctypes.data_as(C.POINTER(F.Params)), bg.ctypes.data_as(C.POINTER(C.c_float)),
                                name, 256)

@@ -62,6 +62,24 @@ def make_profile(rng: np.random.Generator, M: int, name: str) -> SynthProfile:
     return SynthProfile(name, match)
 
 
+def repeat_profile(rng: np.random.Generator, M: int, name: str, motifs) -> SynthProfile:
+    """A profile whose consensus carries tandem repeats: for each (start,
+    period, copies) the most probable letters of rows start, start+1, ...
+    repeat a random motif of that period (peaked emissions, so the consensus
+    is the motif); the other rows as make_profile draws them."""
+    p = make_profile(rng, M, name)
+    for start, period, copies in motifs:
+        motif = rng.integers(0, 20, size=period)
+        for r in range(period * copies):
+            i = start + r
+            if i >= M:
+                break
+            row = rng.dirichlet(np.full(20, 0.5)) * 0.4
+            row[motif[r % period]] += 0.6
+            p.match[i] = row / row.sum()
+    return p
+
+
 def _nl(p: float) -> str:
     if p <= 0:
         return "*"

@@ -105,6 +105,7 @@ typedef struct dmst_opts {
     int device;                                /* CUDA device ordinal */
     int rows_per_lane;                         /* 0 = autotuned, else 1, 2 or 4 */
     size_t device_budget_bytes;                /* 0 = 60% of free device memory */
+    double tantan_threshold;                   /* TANTAN_MASK_THRESHOLD (OPT_tantan, 0.5) for DMST_HMM_MASK */
 } dmst_opts;
 
 /* One (sequence, profile) pair; min_prob_ratio < 0 means "report" as in the
@@ -153,14 +154,21 @@ int dmst_profile_set(dmst_ctx *ctx, int id, const float *values, int width, int 
                      const float *bg);
 
 /* Parse HMMER3 text and finalize each profile with the reference's semantics
- * (readProfiles + finalizeProfile without tantan masking or filtering;
- * background type 'G', 'A' or 'M').  Replaces: readProfiles
- * (dummest-profile.hh:235-329).  first_id/count receive the new ids. */
+ * (readProfiles + finalizeProfile without letter-probability filtering).
+ * background_type: 'G', 'A' or 'M', or-ed with DMST_HMM_MASK to tantan-mask
+ * each profile's consensus as the reference does by default (-m 1 or 3,
+ * readProfiles' isMask; dummest-profile.hh:105-233): consensus letters whose
+ * repeat probability reaches the context's tantan_threshold emit the
+ * background and are left out of the background means.  Replaces:
+ * readProfiles (dummest-profile.hh:235-329).  first_id/count receive the new
+ * ids. */
+#define DMST_HMM_MASK 0x100
 int dmst_profile_load_hmm(dmst_ctx *ctx, const char *text, size_t len, int background_type, int *first_id,
                           int *count);
 
 /* Host-side finalize without a context (for tests and tools): fills values
- * ((M+1)*29), params (M+2) and bg (29) of profile number `index` in the text.
+ * ((M+1)*29), params (M+2) and bg (29) of profile number `index` in the text
+ * (background_type as for dmst_profile_load_hmm, the threshold from opts).
  * Returns its M via *M.  Call with values == NULL first to learn M. */
 int dmst_hmm_finalize(const char *text, size_t len, int index, int background_type, const dmst_opts *opts,
                       int *M, float *values, dmst_params *params, float *bg, char *name, size_t name_cap);

@@ -81,3 +81,50 @@ def test_calibration_generator_matches_reference_estimate_k(ref32, profiles):
     g_flt = d.estimate_gumbel(flt.copy(), L)
     got = np.array([g_mid[0], g_mid[1], g_flt[0], g_flt[1]])
     assert np.array_equal(got, want), (got, want)
+
+
+@pytest.fixture(scope="module")
+def repeat_profiles(ref32, tmp_path_factory):
+    rng = np.random.default_rng(23)
+    profs = [
+        synth.repeat_profile(rng, 120, "rep120", [(10, 7, 8)]),
+        synth.repeat_profile(rng, 400, "rep400", [(0, 3, 20), (150, 12, 6), (330, 1, 25)]),
+        synth.repeat_profile(rng, 64, "rep64", [(5, 16, 3)]),
+        synth.make_profile(rng, 90, "norep90"),
+    ]
+    txt = synth.hmmer3_text(profs)
+    path = tmp_path_factory.mktemp("hmmask") / "m.hmm"
+    path.write_text(txt)
+    assert ref32.load_profiles(str(path), mask=True) == len(profs)
+    return txt, profs
+
+
+def test_masked_finalize_matches_reference(ref32, repeat_profiles):
+    """tantan masking of the consensus (the reference's default -m 3,
+    readProfiles with isMask; dummest-profile.hh:105-233) restated on the host:
+    masked rows emit the background and leave the background means, so values,
+    Params and bg equal the reference's loaded with masking on."""
+    txt, profs = repeat_profiles
+    n_changed = 0
+    for p in range(len(profs)):
+        name, values, params, bg = d.finalize_hmm(txt, index=p, mask=True)
+        rname, rvalues, rparams, rbg = ref32.profile(p)
+        assert name == rname
+        assert np.array_equal(values, rvalues), (name, np.argwhere(values != rvalues)[:5])
+        assert np.array_equal(params, rparams), (name, np.argwhere(params != rparams)[:5])
+        assert np.array_equal(bg, rbg), name
+        _, plain, _, _ = d.finalize_hmm(txt, index=p)
+        n_changed += int(not np.array_equal(plain, values))
+    assert n_changed >= 3  # the repeats were masked (the profile without repeats may stay as it was)
+
+
+def test_mask_threshold_option(ref32, repeat_profiles):
+    """The threshold reaches the finalize (TANTAN_MASK_THRESHOLD): above 1
+    nothing is masked; at the default 0.5 the repeats are."""
+    txt, _ = repeat_profiles
+    plain = d.finalize_hmm(txt, index=0)
+    never = d.finalize_hmm(txt, index=0, mask=True, tantan_threshold=1.01)
+    for a, b in zip(plain[1:], never[1:]):
+        assert np.array_equal(a, b)
+    default = d.finalize_hmm(txt, index=0, mask=True)
+    assert not np.array_equal(default[1], plain[1])
