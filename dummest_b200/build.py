@@ -22,7 +22,8 @@ LIB = os.path.join(HERE, "libdummest_b200.so")
 
 SOURCES = ["dmst_api.cu", "host_model.cpp", "windows.cpp"]
 HEADERS = ["dp_common.cuh", "dp_wavefront.cuh", "dp_exact.cuh", "dp_exact_wave.cuh", "null_model.cuh", "host_model.h",
-           "dp_adjoint.cuh", "dp_posterior.cuh", "dp_search.cuh", "dp_traceback.cuh", "dp_traceback_job.cuh"]
+           "dp_adjoint.cuh", "dp_posterior.cuh", "dp_search.cuh", "dp_traceback.cuh", "dp_traceback_job.cuh",
+           "dp_stagger.cuh", "dp_plain.cuh"]
 
 NVCC_FLAGS = [
     "-O3",

@@ -9,6 +9,7 @@
 #include "dp_plain.cuh"
 #include "dp_exact_wave.cuh"
 #include "dp_search.cuh"
+#include "dp_stagger.cuh"
 #include "dp_traceback.cuh"
 #include "dp_wavefront.cuh"
 #include "host_model.h"
@@ -1583,12 +1584,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         d.R = profR[q.profile];
         d.seedOff = seedFloats;
         seedFloats += 2LL * d.L;
-        const int S = kLanes * d.R;
-        const size_t nS = (size_t)(d.M + 1 + S - 1) / S;
-        const size_t P = (size_t)wavePeriod(d.L);
-        const size_t D = P + kLanes - 1;
-        if (mid) w1Max = std::max(w1Max, nS * D * (size_t)S);
-        ringMax = std::max(ringMax, 4 * P);
+        // the staggered kernel's W1 groups (one per step) and its ring (W, Y per column)
+        if (mid) w1Max = std::max(w1Max, (size_t)stagSlotFloats(d.M, d.L, d.R));
+        ringMax = std::max(ringMax, 2 * (size_t)stagPeriod(d.L, d.R));
     }
     // Kernel groups by rows per lane (fixed per profile).  Chunks: runs of up to
     // 2 x warps pairs of one profile, costliest first within each group.
@@ -1667,10 +1665,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
         // A table that would leave room for fewer than the shape's warps stays
         // in global memory instead (read through L1), and every warp runs.
-        G.gt = table + (size_t)G.kernWarps * sizeof(Window) > smemLimit;
+        const size_t winBytes = stagWindowBytes(G.R);
+        G.gt = table + (size_t)G.kernWarps * winBytes > smemLimit;
         if (G.gt) G.kern = dpKernelFor(G.R, mid, G.kernWarps, true);
         if (search) G.kernF = dpKernelFor(G.R, false, G.kernWarps, G.gt);
-        G.warps = G.gt ? G.kernWarps : (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / sizeof(Window));
+        G.warps = G.gt ? G.kernWarps : (int)std::min<size_t>(G.kernWarps, (smemLimit - table) / winBytes);
         G.warps = (int)std::max<size_t>(1, std::min<size_t>(G.warps, maxSlots / ctx->smCount));
         // Chunks of up to four pairs per launched warp, fewer when the group is
         // too small to give each CTA four chunks, but never fewer pairs than the
@@ -1712,7 +1711,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         allChunks.insert(allChunks.end(), G.chunks.begin(), G.chunks.end());
         // Shared memory: the emission table, then one staging window per warp.
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
-        G.smem = (G.gt ? 0 : table) + (size_t)G.warps * sizeof(Window);
+        G.smem = (G.gt ? 0 : table) + (size_t)G.warps * stagWindowBytes(G.R);
         CK(cudaFuncSetAttribute(G.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem),
            "smem attribute");
         if (search)

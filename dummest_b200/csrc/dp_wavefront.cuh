@@ -1325,61 +1325,6 @@ struct DpArgs {
     const int *pairIdx;  // null: chunk c holds pairs first .. first+count-1; else pairIdx[first + k]
 };
 
-template <int R, bool MID, bool SH = false>
-__device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad, const float *smBg, Window &win,
-                          float *w1, float *ring, int lane) {
-    const DevPair p = g.pairs[pi];
-    __syncwarp();
-    if (lane == 0) {
-        PairCold &c = win.cold;
-        c.codes = g.codes + p.codeOff;
-        c.pre = g.seeds + p.seedOff;
-        c.suf = c.pre + p.L;
-        const DevProfile &pr = g.profiles[p.prof];
-        c.coef = g.params + coefOffOf(pr.paramOff, pr.M);
-        c.coefStride = pr.rowPad;
-        c.smBg = smBg;
-        c.sc = g.scales[pi];
-        c.M = p.M;
-    }
-    __syncwarp();
-    SweepArgs a;
-    a.alignOut = nullptr;
-    a.cold = &win.cold;
-    a.smE = smE;
-    a.w1 = w1;
-    a.ring = ring;
-    a.L = p.L;
-    a.rowPad = rowPad;
-    a.nS = (p.M + 1 + kLanes * R - 1) / (kLanes * R);
-    a.P = wavePeriod(p.L);
-    a.D = a.P + kLanes - 1;
-    a.sFirst = 0;
-    a.sStep = 1;
-    a.nMine = a.nS;
-    a.ringSlots = 1;
-    a.ringStride = 0;
-    float filt, maxYb, mid = 0.0f, maxFw = 0.0f;
-    if (MID) {
-        backwardSweep<R, kMid, SH>(a, win, lane, filt, maxYb);
-        forwardSweep<R, kMid, SH>(a, win, lane, mid, maxFw);
-    } else {
-        backwardSweep<R, kFilter, SH>(a, win, lane, filt, maxYb);
-    }
-    filt = warpMax(filt);
-    maxYb = warpMax(maxYb);
-    mid = warpMax(mid);
-    maxFw = warpMax(maxFw);
-    if (lane == 0) {
-        PairOut o;
-        o.mid = mid;
-        o.filt = filt;
-        o.maxYb = maxYb;
-        o.maxFw = maxFw;
-        g.out[pi] = o;
-    }
-}
-
 // CTA shapes: WARPS warps share one shared-memory copy of the profile's
 // emission table, one CTA per SM; 16 warps leave 128 registers per thread,
 // 12 warps 168 and 8 warps 255.  The autotuner picks the shape per
@@ -1387,66 +1332,5 @@ __device__ void scorePair(const DpArgs &g, int pi, const float *smE, int rowPad,
 constexpr int kCtaWarps = 16;       // the default (and widest) shape
 constexpr int kCtaWarpsNarrow = 8;
 constexpr int kCtaWarpsMid = 12;
-
-// Persistent kernel for one rows-per-lane value: CTAs pull chunks
-// (same-profile runs of pairs, costliest first) from a global counter, stage
-// the chunk's profile emission table in shared memory, and their warps pull
-// pairs from the chunk.  Dynamic shared memory: the table (tableFloats), then
-// one Window per warp (the launch may use fewer than WARPS warps when the
-// table leaves no room; W1 slots are indexed by the launched warps).  With
-// GT (tall profiles) the table stays in global memory, read through L1 (a
-// stripe's 32 R rows of 25 codes), and the shared memory holds the windows
-// of all WARPS warps.
-template <int R, bool MID, int WARPS, bool GT>
-__global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tableFloats) {
-    extern __shared__ float4 smRaw[];
-    const float *smE = reinterpret_cast<const float *>(smRaw);
-    Window *wins = reinterpret_cast<Window *>(reinterpret_cast<float *>(smRaw) + tableFloats);
-    __shared__ float smBg[32];
-    __shared__ int smChunk, smNext;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t slot = (size_t)blockIdx.x * (blockDim.x >> 5) + warp;  // launched warps, not WARPS
-    float *w1 = g.w1 + slot * g.w1SlotFloats;
-    float *ring = g.ring + slot * g.ringSlotFloats;
-    Window &win = wins[warp];
-    int loaded = -1;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            smChunk = atomicAdd(g.chunkCounter, 1);
-            smNext = 0;
-        }
-        __syncthreads();
-        const int ci = smChunk;
-        if (ci >= g.nChunks) break;
-        const Chunk ch = g.chunks[ci];
-        if (ch.count == 0) {  // a chunk of the second search wave with no survivors
-            __syncthreads();
-            continue;
-        }
-        const int rowPad = ch.rowPad;
-        if (ch.prof != loaded) {
-            const DevProfile *pr = g.profiles + ch.prof;
-            if (GT) {
-                smE = g.emit + pr->emitOff;
-            } else {
-                const float4 *src = reinterpret_cast<const float4 *>(g.emit + pr->emitOff);
-                const int n4 = kNumCodes * rowPad / 4;
-                for (int i = threadIdx.x; i < n4; i += blockDim.x) smRaw[i] = __ldg(src + i);
-            }
-            if (threadIdx.x < 32) smBg[threadIdx.x] = threadIdx.x < kNumCodes ? pr->bg[threadIdx.x] : 0.0f;
-            loaded = ch.prof;
-        }
-        __syncthreads();
-        for (;;) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(&smNext, 1);
-            k = __shfl_sync(kFull, k, 0);
-            if (k >= ch.count) break;
-            const int pi = g.pairIdx ? g.pairIdx[ch.first + k] : ch.first + k;
-            scorePair<R, MID, !GT>(g, pi, smE, rowPad, smBg, win, w1, ring, lane);
-        }
-        __syncthreads();
-    }
-}
 
 }  // namespace dmst
