@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=48)
     ap.add_argument("--rows-per-lane", type=int, default=0)
+    ap.add_argument("--mmin", type=int, default=50,
+                    help="batched workload: shortest profile (M log-uniform from here to --mmax)")
+    ap.add_argument("--lmin", type=int, default=150,
+                    help="batched workload: shortest read (L log-uniform from here to --lmax)")
     ap.add_argument("--mmax", type=int, default=800,
                     help="batched workload: longest profile (M log-uniform from 50; smaller cases for profiling)")
     ap.add_argument("--lmax", type=int, default=3000,
@@ -190,8 +194,8 @@ def workload_config(args, world: int) -> dict:
     if args.workload == "search":
         return {
             "workload": f"two-wave search (float filter on every pair, mid-anchored score on survivors, E <= "
-                        f"{SEARCH_E:g}): {args.profiles} profiles M log-uniform 50-{args.mmax} x reads L "
-                        f"log-uniform 150-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands; gates from each profile's "
+                        f"{SEARCH_E:g}): {args.profiles} profiles M log-uniform {args.mmin}-{args.mmax} x reads L "
+                        f"log-uniform {args.lmin}-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands; gates from each profile's "
                         "calibration (200 x 3 kb random sequences)",
             "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
             "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
@@ -236,8 +240,8 @@ def workload_config(args, world: int) -> dict:
             "parallelism": f"replicas x{world} (one genome per rank)",
         }
     return {
-        "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform 50-{args.mmax} x "
-                    f"reads L log-uniform 150-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands",
+        "workload": f"batched fwd+bwd (mid-anchored score): {args.profiles} profiles M log-uniform {args.mmin}-{args.mmax} x "
+                    f"reads L log-uniform {args.lmin}-{args.lmax} nt, GC 0.4-0.6, 10% implants, both strands",
         "reads_per_step": args.reads_per_step, "records_per_step": 2 * args.reads_per_step,
         "profiles": args.profiles, "pairs_per_step": 2 * args.reads_per_step * args.profiles,
         "l2": "inputs larger than L2 (W1 slots)",
@@ -245,10 +249,10 @@ def workload_config(args, world: int) -> dict:
     }
 
 
-def make_profiles(seed, n, mmax=800):
+def make_profiles(seed, n, mmax=800, mmin=50):
     from dummest_b200 import synth
     rng = np.random.default_rng(seed)
-    Ms = np.exp(rng.uniform(np.log(50), np.log(mmax), size=n)).round().astype(int)
+    Ms = np.exp(rng.uniform(np.log(mmin), np.log(mmax), size=n)).round().astype(int)
     profiles = [synth.make_profile(rng, int(M), f"synth{k:03d}") for k, M in enumerate(Ms)]
     return profiles, synth.hmmer3_text(profiles)
 
@@ -275,20 +279,21 @@ def make_workload(args, rank: int, n_steps: int, world: int = 0):
                      + synth.random_dna(rng, 500) for _ in range(args.al_reads)]
             steps.append(synth.both_strands(reads))
         return [prof], synth.hmmer3_text([prof]), steps
-    profiles, txt = make_profiles(args.seed, args.profiles, args.mmax)
+    profiles, txt = make_profiles(args.seed, args.profiles, args.mmax, args.mmin)
     if world >= 1:
         per = world * args.reads_per_step
         n_sets = n_steps if world == 1 else min(n_steps, args.warmup + -(-100_000 // per))
-        return profiles, txt, make_steps(rank_seed(args.seed, 0), profiles, n_sets, per, args.lmax)
-    return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step, args.lmax)
+        return profiles, txt, make_steps(rank_seed(args.seed, 0), profiles, n_sets, per, args.lmax, args.lmin)
+    return profiles, txt, make_steps(rank_seed(args.seed, rank), profiles, n_steps, args.reads_per_step, args.lmax,
+                                     args.lmin)
 
 
-def make_steps(seed, profiles, n_steps, reads_per_step, lmax=3000):
+def make_steps(seed, profiles, n_steps, reads_per_step, lmax=3000, lmin=150):
     from dummest_b200 import synth
     rng = np.random.default_rng(seed)
     steps = []
     for _ in range(n_steps):
-        reads = synth.make_reads(rng, reads_per_step, 150, lmax, profiles, 0.10, gc_range=(0.4, 0.6))
+        reads = synth.make_reads(rng, reads_per_step, lmin, lmax, profiles, 0.10, gc_range=(0.4, 0.6))
         steps.append(synth.both_strands(reads))
     return steps
 
@@ -458,7 +463,7 @@ def measured_peaks():
 def traffic_per_cell():
     """DRAM bytes per cell of the mid kernel from the committed ncu summary."""
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "dpKernel_mid_8192pairs_traffic.json")))["dram_bytes_per_cell"]
+        return json.load(open(os.path.join(ROOT, "profiles", "dpKernel_stagger_640000pairs_traffic.json")))["dram_bytes_per_cell"]
     except (OSError, KeyError, ValueError):
         return None
 
@@ -1280,6 +1285,8 @@ def run_ours(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the timed calls' launches form the NVTX range "timed" (ncu --nvtx --nvtx-include timed/)
+    torch.cuda.nvtx.range_push("timed")
     ev0.record(stream)
     launches, dp_ms, cells, exact_pairs = 0, 0.0, 0.0, 0
     kept = []  # (timed step, results) of every 4th timed step, for the parity sample
@@ -1310,6 +1317,7 @@ def run_ours(args, rank, world, local):
     if not args.no_async:
         account(ctx.complete(), n_steps - 1)
     ev1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(world)
     clk = clocks.stop()

@@ -1,4 +1,7 @@
-// The batched wavefront DP: one warp per (read, profile) pair.
+// The row-contiguous stripe wavefront: the step functions of the exact
+// row-rescaled path (dp_exact_wave.cuh, dp_exact.cuh) and of the plain
+// one-pair-per-launch schedule (dp_plain.cuh).  The batched kernel of the
+// fast path is dp_stagger.cuh.
 //
 // Layout.  The profile's rows are striped across the 32 lanes of a warp: a
 // stripe is S = 32*R consecutive rows, lane l owns rows l*R .. l*R+R-1 of the
@@ -29,12 +32,13 @@
 // diagonal-major order ([stripe][diagonal][lane][R]) so that both the store
 // and the load of one step are one contiguous 32*R*4-byte access.
 //
-// Row rescaling.  The kernel computes with every rescale count at zero, which
-// is exactly the reference's arithmetic for a pair whose row maxima never
-// exceed RESCALE_THRESH.  It reports the largest backward Y (Y >= W1 at every
-// cell) and the largest forward W0/Y0, so the host can tell whether the
-// reference would have rescaled; such pairs are re-scored by the exact
-// row-rescaled path (dp_exact_wave.cuh).
+// Row rescaling.  The fast modes compute with every rescale count at zero,
+// which is exactly the reference's arithmetic for a pair whose row maxima
+// never exceed RESCALE_THRESH.  They report the largest backward Y (Y >= W1
+// at every cell) and the largest forward W0/Y0, so the host can tell whether
+// the reference would have rescaled; such pairs are re-scored by the exact
+// row-rescaled path (dp_exact_wave.cuh), whose modes apply the reference's
+// rescale counts.
 //
 // Mid score.  The reference forms promote(W0)*promote(W1) in double and
 // rounds the mantissa to float (dummest-batch.hh:216-235); with both counts
@@ -626,91 +630,6 @@ __device__ __forceinline__ void backwardStep(BwdState<R, MODE> &b, const SweepAr
     ++b.u;
 }
 
-// ---------------------------------------------------------------------------
-// Interior blocks of the fast sweeps (kFilter, kMid).  A block of steps is
-// interior when every lane, at every step of the block (and, for the
-// forward's W1 staging, `ahead` steps further), is inside one stripe, past
-// its first column and before its column L: then no lane starts a stripe
-// (coefficient loads, history reset), idles or changes stripe, and a step
-// needs none of backwardStep's / forwardStep's bookkeeping.  The emission row
-// base, the ring writer and the W1 pointers are fixed for the block.  The
-// arithmetic is the same operations in the same order, so the results are
-// the same bits.  The test is warp-uniform (it depends on the block only):
-// lane 0 is the latest lane at the block's first step and lane 31 the
-// earliest at its last, or the reverse in the forward, which spans the same
-// local times.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool interiorBlock(const SweepArgs &a, int t0, int n, int total, int ahead) {
-    const int uLo = t0 - (kLanes - 1), uHi = t0 + n - 1 + ahead;
-    if (uLo < 0 || uHi >= total) return false;
-    const int k = uLo / a.P;
-    return uLo - k * a.P >= 1 && uHi - k * a.P <= a.L - 1;
-}
-
-// SH: the emission table is in shared memory, at the 32-bit shared address
-// eBaseS of the lane's rows (else at eBase, global memory through L1).
-template <int R, int MODE, int PH, bool SH>
-__device__ __forceinline__ void backwardInterior(BwdState<R, MODE> &b, const SweepArgs &a, Window &win, int lane,
-                                                 const float *eBase, unsigned eBaseS, bool ringWriter) {
-    static_assert(MODE == kFilter || MODE == kMid, "fast modes only");
-    constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
-    float inW = __shfl_down_sync(kFull, b.sendW, 1);
-    float inY = __shfl_down_sync(kFull, b.sendY, 1);
-    const int slot = b.u & (kWin - 1);
-    const float4 col = win.col[slot];
-    if (lane == kLanes - 1) {
-        const float4 r = win.ring[slot];
-        inW = r.x;
-        inY = r.y;
-    }
-    const float bgv = col.y, sufv = col.z, prev = col.w;
-    float e[R];
-    if (SH)
-        loadEmitS<R>(e, eBaseS + 4u * (unsigned)__float_as_int(col.x));
-    else
-        loadEmit<R>(e, eBase + __float_as_int(col.x));
-    float p[R];
-    p[R - 1] = (b.rb[I3] * e[R - 1]) * b.c.enter[R - 1];
-#pragma unroll
-    for (int k = 0; k < R - 1; ++k) p[k] = (b.h[I3][k + 1] * e[k]) * b.c.enter[k];
-    float bW1 = b.rb[I1], bW2 = b.rb[I2], bY = inY;
-    float wv[R], yv[R];
-#pragma unroll
-    for (int k = R - 1; k >= 0; --k) {
-        float acc = p[k];
-        acc = __fmaf_rn(bY, b.c.d0[k], acc);
-        acc = __fmaf_rn(bW2, b.c.d1[k], acc);
-        acc = __fmaf_rn(bW1, b.c.d2[k], acc);
-        const float zbg = b.z[I3][k] * bgv;
-        acc = __fmaf_rn(zbg, b.c.a0[k], acc);
-        acc = __fmaf_rn(b.h[I2][k], b.c.a2[k], acc);
-        acc = __fmaf_rn(b.h[I1][k], b.c.a1[k], acc);
-        const float W = __fmaf_rn(sufv, b.c.rs[k], acc);
-        const float Y = __fmaf_rn(b.c.eps[k], bY, W);
-        const float Z = __fmaf_rn(b.c.b0[k], zbg, W);
-        yv[k] = Y;
-        bW1 = b.h[I1][k];
-        bW2 = b.h[I2][k];
-        bY = Y;
-        wv[k] = W;
-        b.h[I3][k] = W;
-        b.z[I3][k] = Z;
-    }
-#pragma unroll
-    for (int k = 0; k < R; k += 2) b.maxY = (k + 1 < R) ? fmax3(b.maxY, yv[k], yv[k + 1]) : fmaxf(b.maxY, yv[k]);
-    b.filt = stepFilt<R>(b.filt, wv, prev);
-    b.rb[I3] = inW;
-    b.sendW = wv[0];
-    b.sendY = bY;
-    if (MODE == kMid) {
-        storeW1<R>(b.wp, wv);
-        b.wp += kLanes * R;
-    }
-    if (ringWriter) ringStore(a.ring, b.jj, b.sendW, b.sendY);
-    ++b.jj;
-    ++b.u;
-}
-
 // Window refills for a block of kBlock steps starting at t0: local times
 // [t0 + kBlock, t0 + 2 kBlock), one entry per lane and pass.
 template <bool BACKWARD, bool EXACT = false>
@@ -724,96 +643,6 @@ __device__ __forceinline__ void fillBlock(Window &win, const SweepArgs &a, int f
                 fillForward<EXACT>(win, a, first + o + lane);
         }
     }
-}
-
-template <int R, int MODE, bool SH = false>
-__device__ void backwardSweep(const SweepArgs &a, Window &win, int lane, float &filtOut, float &maxYOut,
-                              const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
-    BwdState<R, MODE> b;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-#pragma unroll
-        for (int k = 0; k < R; ++k) b.h[q][k] = b.z[q][k] = 0.0f;
-        b.rb[q] = 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        b.rmax[k] = 0.0f;
-        b.cOut[k] = 0;
-        b.fOut[k] = 1.0f;
-        b.rowBest[k] = 0.0;
-    }
-    b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
-    b.sendC = b.cnt = 0;
-    b.u = -(kLanes - 1 - lane);  // lane 31 leads
-    b.sp = b.jj = 0;
-    b.wp = a.w1;
-    const int total = a.nMine * a.P;
-    const int T = (total + (kLanes - 1) + 2) / 3 * 3;  // whole groups of three steps
-    __syncwarp();
-    fillBlock<true>(win, a, 0, lane);
-    for (int t0 = 0; t0 < T; t0 += kBlock) {
-        __syncwarp();
-        fillBlock<true>(win, a, t0 + kBlock, lane);
-        const int n = (t0 + kBlock < T ? kBlock : T - t0);
-        if (MODE == kFilter || MODE == kMid) {
-            // Groups of three steps from g: the interior ones (see interiorBlock)
-            // form at most two runs, one per stripe the block touches (a block
-            // and the lanes' skew span fewer steps than a stripe), so the runs'
-            // bounds are found once per block and the steps between them are
-            // the general ones.
-            constexpr int S = kLanes * R;
-            const int u0 = t0 - (kLanes - 1);  // lane 0's local time at the block's first step
-            const int k0 = u0 >= 0 ? u0 / a.P : -1;
-            int g = 0;
-#pragma unroll 1
-            for (int kk = 0; kk < 2; ++kk) {
-                const int kb = (k0 + kk) * a.P;  // the stripe's first local time
-                if (kb < 0) continue;
-                int gA = kb + kLanes - t0;       // lane 0 past its column 0
-                gA = gA < 0 ? 0 : (gA + 2) / 3 * 3;
-                int gB = min(kb + a.L - 3, total - 3) - t0;  // lane 31's group ends by column L-1
-                gB = min(gB, n - 3);
-                if (gB < gA) continue;
-                gB = gB / 3 * 3;
-#pragma unroll 1
-                for (; g < gA; g += 3) {
-                    backwardStep<R, MODE, 0, false, SH>(b, a, win, lane, total, x, exact);
-                    backwardStep<R, MODE, 1, false, SH>(b, a, win, lane, total, x, exact);
-                    backwardStep<R, MODE, 2, false, SH>(b, a, win, lane, total, x, exact);
-                }
-                const float *eBase = a.smE + (a.nS - 1 - b.sp) * S + lane * R;
-                const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
-                const bool ringWriter = lane == 0 && b.sp < a.nS - 1;
-#pragma unroll 1
-                for (; g <= gB; g += 3) {
-                    backwardInterior<R, MODE, 0, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
-                    backwardInterior<R, MODE, 1, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
-                    backwardInterior<R, MODE, 2, SH>(b, a, win, lane, eBase, eBaseS, ringWriter);
-                }
-                // a lane whose last step was its stripe's column L-1 = P-1 moves to the next stripe
-                if (b.jj == a.P) {
-                    b.jj = 0;
-                    ++b.sp;
-                }
-            }
-#pragma unroll 1
-            for (; g < n; g += 3) {
-                backwardStep<R, MODE, 0, false, SH>(b, a, win, lane, total, x, exact);
-                backwardStep<R, MODE, 1, false, SH>(b, a, win, lane, total, x, exact);
-                backwardStep<R, MODE, 2, false, SH>(b, a, win, lane, total, x, exact);
-            }
-            continue;
-        }
-#pragma unroll 1
-        for (int g = 0; g < n; g += 3) {
-            backwardStep<R, MODE, 0>(b, a, win, lane, total, x, exact);
-            backwardStep<R, MODE, 1>(b, a, win, lane, total, x, exact);
-            backwardStep<R, MODE, 2>(b, a, win, lane, total, x, exact);
-        }
-    }
-    filtOut = b.filt;
-    maxYOut = b.maxY;
 }
 
 // Asynchronous global-to-shared copies of W1 (cp.async: the copy bypasses the
@@ -1090,72 +919,6 @@ __device__ __forceinline__ void forwardStep(FwdState<R, MODE> &f, const SweepArg
     ++f.u;
 }
 
-// A forward step of an interior block (see interiorBlock) at position P6 of
-// a six-step group, with its W1 staging: the copy for the step kW1Ahead
-// later comes from w1src, which steps back one diagonal (32 R floats) per step.
-template <int R, int MODE, int P6, bool SH>
-__device__ __forceinline__ void forwardInterior(FwdState<R, MODE> &f, const SweepArgs &a, Window &win, int lane,
-                                                const float *eBase, unsigned eBaseS, bool ringWriter,
-                                                const float *&w1src) {
-    static_assert(MODE == kMid, "the fast forward");
-    constexpr int PH = P6 % 3;
-    constexpr int I1 = (3 - PH) % 3, I2 = (4 - PH) % 3, I3 = (5 - PH) % 3;
-    float q[R];
-    cpAsyncWait<kW1Ahead - 1>();
-    {
-        const float4 v = win.w1[P6][lane];
-        q[0] = v.x;
-        if constexpr (R > 1) q[1] = v.y;
-        if constexpr (R > 2) {
-            q[2] = v.z;
-            q[3] = v.w;
-        }
-    }
-    float inW = __shfl_up_sync(kFull, f.sendIn, 1);
-    float inY = __shfl_up_sync(kFull, f.sendY, 1);
-    const int slot = f.u & (kWin - 1);
-    const float4 col = win.col[slot];
-    if (lane == 0) {
-        const float4 r = win.ring[slot];
-        inW = r.x;
-        inY = r.y;
-    }
-    const float bgsC = col.y, prev = col.z;
-    float e[R];
-    if (SH)
-        loadEmitS<R>(e, eBaseS + 4u * (unsigned)__float_as_int(col.x));
-    else
-        loadEmit<R>(e, eBase + __float_as_int(col.x));
-    float win0 = inW, yab = inY;
-    float bv[R];
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const float w1 = f.w[I1][k], w2 = f.w[I2][k], w3 = f.w[I3][k];
-        const float X = (f.c.enter[k] * e[k]) * w3;
-        const float Z0 = bgsC * __fmaf_rn(f.c.b0[k], f.z[I3][k], f.c.a0[k] * w3);
-        const float zs = __fmaf_rn(f.c.a2[k], w2, __fmaf_rn(f.c.a1[k], w1, Z0));
-        const float W0 = win0 + __fadd_rn(zs, prev);
-        bv[k] = W0 * q[k];
-        const float Y0 = __fmaf_rn(f.c.eps[k], yab, f.c.d0[k] * W0);
-        f.mx = fmax3(f.mx, W0, Y0);
-        const float nin = __fmaf_rn(f.c.d2[k], w1, __fmaf_rn(f.c.d1[k], w2, X + Y0));
-        f.w[I3][k] = W0;
-        f.z[I3][k] = Z0;
-        win0 = nin;
-        yab = Y0;
-    }
-#pragma unroll
-    for (int k = 0; k < R; k += 2) f.best = (k + 1 < R) ? fmax3(f.best, bv[k], bv[k + 1]) : fmaxf(f.best, bv[k]);
-    f.sendIn = win0;
-    f.sendY = yab;
-    if (ringWriter) ringStore(a.ring, f.j, f.sendIn, f.sendY);
-    ++f.j;
-    ++f.u;
-    cpAsyncW1<R>(&win.w1[(P6 + kW1Ahead) % kW1Slots][lane], w1src);
-    cpAsyncCommit();
-    w1src -= kLanes * R;
-}
-
 // One forward step at position P6 of a six-step group: wait for this step's
 // W1 copy, read it from the staging ring, run the step, and stage the W1 of
 // the step kW1Ahead later into the slot this lane read one step ago.
@@ -1181,123 +944,6 @@ __device__ __forceinline__ void forwardStaged(FwdState<R, MODE> &f, const SweepA
     }
     forwardStep<R, MODE, P6 % 3, ANCH, PIPE, SH>(f, a, win, lane, total, q, x, exact);
     if (kReadW1) st.issue(a, win, (P6 + kW1Ahead) % kW1Slots, lane, total);
-}
-
-// ---------------------------------------------------------------------------
-// Forward sweep (reads W1 written by the backward sweep of the same mode).
-// Steps run in groups of six, so that both the history phase (t mod 3) and
-// the W1 staging slot (t mod 6) are compile-time constants.
-// ---------------------------------------------------------------------------
-template <int R, int MODE, bool SH = false>
-__device__ void forwardSweep(const SweepArgs &a, Window &win, int lane, float &bestOut, float &maxOut,
-                             const ExactRows *x = nullptr, ExactBest *exact = nullptr) {
-    static_assert(kW1Slots == 6 && kBlock % 6 == 0, "six-step groups");
-    FwdState<R, MODE> f;
-#pragma unroll
-    for (int h = 0; h < 3; ++h)
-#pragma unroll
-        for (int k = 0; k < R; ++k) f.w[h][k] = f.z[h][k] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        f.rmax[k] = 0.0f;
-        f.cIn[k] = f.cB[k] = 0;
-        f.fOut[k] = 1.0f;
-        f.rowBest[k] = 0.0;
-    }
-    f.sendIn = f.sendY = f.best = f.mx = 0.0f;
-    f.sendC = f.cnt = 0;
-    f.u = -lane;  // lane 0 leads
-    f.s = f.j = 0;
-    const int total = a.nMine * a.P;
-    const int T = (total + (kLanes - 1) + 5) / 6 * 6;  // whole groups of six steps
-    constexpr bool kReadW1 = MODE == kMid || MODE == kReplay;
-    W1Stage<R, MODE == kDiscover || MODE == kReplay> st{-lane, 0, 0};
-    if (kReadW1) {
-#pragma unroll
-        for (int k = 0; k < kW1Ahead; ++k) st.issue(a, win, k, lane, total);
-    }
-    __syncwarp();
-    fillBlock<false>(win, a, 0, lane);
-    for (int t0 = 0; t0 < T; t0 += kBlock) {
-        __syncwarp();
-        fillBlock<false>(win, a, t0 + kBlock, lane);
-        const int n = (t0 + kBlock < T ? kBlock : T - t0);
-        if (MODE == kMid) {
-            // Interior runs of six-step groups, found per block as in
-            // backwardSweep; an interior group also needs its W1 staging
-            // (kW1Ahead steps further) inside the stripe.
-            constexpr int S = kLanes * R;
-            const int u0 = t0 - (kLanes - 1);  // lane 31's local time at the block's first step
-            const int k0 = u0 >= 0 ? u0 / a.P : -1;
-            int g = 0;
-#pragma unroll 1
-            for (int kk = 0; kk < 2; ++kk) {
-                const int kb = (k0 + kk) * a.P;
-                if (kb < 0) continue;
-                int gA = kb + kLanes - t0;
-                gA = gA < 0 ? 0 : (gA + 5) / 6 * 6;
-                int gB = min(kb + a.L - 6 - kW1Ahead, total - 6 - kW1Ahead) - t0;
-                gB = min(gB, n - 6);
-                if (gB < gA) continue;
-                gB = gB / 6 * 6;
-#pragma unroll 1
-                for (; g < gA; g += 6) {
-                    forwardStaged<R, MODE, 0, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                    forwardStaged<R, MODE, 1, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                    forwardStaged<R, MODE, 2, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                    forwardStaged<R, MODE, 3, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                    forwardStaged<R, MODE, 4, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                    forwardStaged<R, MODE, 5, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                }
-                const float *eBase = a.smE + f.s * S + lane * R;
-                const unsigned eBaseS = SH ? (unsigned)__cvta_generic_to_shared(eBase) : 0u;
-                const bool ringWriter = lane == kLanes - 1 && f.s < a.nS - 1;
-                // the staging cursor is kW1Ahead steps ahead, in the same stripe
-                const float *w1src =
-                    a.w1 + (((size_t)f.s * a.D + (a.L - 1 - (f.j + kW1Ahead)) + (kLanes - 1 - lane)) * kLanes + lane) * R;
-#pragma unroll 1
-                for (; g <= gB; g += 6) {
-                    forwardInterior<R, MODE, 0, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                    forwardInterior<R, MODE, 1, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                    forwardInterior<R, MODE, 2, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                    forwardInterior<R, MODE, 3, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                    forwardInterior<R, MODE, 4, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                    forwardInterior<R, MODE, 5, SH>(f, a, win, lane, eBase, eBaseS, ringWriter, w1src);
-                }
-                // the staging cursor stays kW1Ahead steps ahead: in the same stripe
-                // (f ends at most at column L-5), or at the next stripe's start
-                st.u = f.u + kW1Ahead;
-                st.j = f.j + kW1Ahead;
-                st.s = f.s;
-                if (st.j == a.P) {
-                    st.j = 0;
-                    ++st.s;
-                }
-            }
-#pragma unroll 1
-            for (; g < n; g += 6) {
-                forwardStaged<R, MODE, 0, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                forwardStaged<R, MODE, 1, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                forwardStaged<R, MODE, 2, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                forwardStaged<R, MODE, 3, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                forwardStaged<R, MODE, 4, false, false, SH>(f, a, win, lane, total, st, x, exact);
-                forwardStaged<R, MODE, 5, false, false, SH>(f, a, win, lane, total, st, x, exact);
-            }
-            continue;
-        }
-#pragma unroll 1
-        for (int g = 0; g < n; g += 6) {
-            forwardStaged<R, MODE, 0>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 1>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 2>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 3>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 4>(f, a, win, lane, total, st, x, exact);
-            forwardStaged<R, MODE, 5>(f, a, win, lane, total, st, x, exact);
-        }
-    }
-    if (kReadW1) cpAsyncWait<0>();  // no copy outlives the sweep (the slot is reused)
-    bestOut = f.best;
-    maxOut = f.mx;
 }
 
 __device__ __forceinline__ float warpMax(float v) {
