@@ -209,6 +209,7 @@ SIGNATURES = [
     ("dmst_tuned_shape", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("dmst_set_wait_limit", C.c_int, [C.c_void_p, C.c_int]),
     ("dmst_tuned_rates", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("dmst_tuned_rates_ex", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int]),
     ("dmst_posterior_summary", C.c_int,
      [C.c_void_p, C.POINTER(Pair), C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
       C.POINTER(C.c_double)]),

@@ -374,14 +374,16 @@ const char *statusText(int s) {
 
 // Kernel shapes the autotuner chooses among: rows per lane (the stripe is
 // 32 R rows) and warps per CTA.
-constexpr int kShapeR[3] = {4, 2, 1};
+constexpr int kNumR = 4;
+constexpr int kShapeR[kNumR] = {4, 3, 2, 1};
 constexpr int kShapeWarps[3] = {kCtaWarps, kCtaWarpsNarrow, kCtaWarpsMid};
-inline int rIndex(int R) { return R == 4 ? 0 : (R == 2 ? 1 : 2); }
+inline int rIndex(int R) { return R == 4 ? 0 : (R == 3 ? 1 : (R == 2 ? 2 : 3)); }
 
 using DpKern = void (*)(DpArgs, int);
 template <bool MID, int W, bool GT>
 DpKern kernByR(int R) {
-    return R == 4 ? dpKernel<4, MID, W, GT> : (R == 2 ? dpKernel<2, MID, W, GT> : dpKernel<1, MID, W, GT>);
+    return R == 4 ? dpKernel<4, MID, W, GT>
+                  : (R == 3 ? dpKernel<3, MID, W, GT> : (R == 2 ? dpKernel<2, MID, W, GT> : dpKernel<1, MID, W, GT>));
 }
 template <bool GT>
 DpKern dpKernelShape(int R, bool mid, int warps) {
@@ -427,14 +429,14 @@ inline long long paddedRows(int M, int R) {
 // and its rate in computed (padded) cells per millisecond.
 struct Tuning {
     bool tuned = false;
-    int warps[3] = {kCtaWarps, kCtaWarps, kCtaWarps};
-    double rate[3] = {0, 0, 0};
-    double rates[3][3] = {};  // per R, per kShapeWarps: the measured rates (cells per ms), for dmst_tuned_rates
+    int warps[kNumR] = {kCtaWarps, kCtaWarps, kCtaWarps, kCtaWarps};
+    double rate[kNumR] = {0, 0, 0, 0};
+    double rates[kNumR][3] = {};  // per R, per kShapeWarps: the measured rates (cells per ms), for dmst_tuned_rates
     int forceR = 0, forceWarps = 0;  // set while the autotuner measures one shape
 };
 
 int rowsPerLane(int M, int forced, const Tuning &t) {
-    if (forced == 1 || forced == 2 || forced == 4) return forced;
+    if (forced >= 1 && forced <= 4) return forced;
     if (t.forceR) return t.forceR;
     // Untuned default, measured on B200 (synthetic profiles, M 50-800): the
     // per-step cost of a lane dominates, so four rows per lane is fastest per
@@ -443,7 +445,7 @@ int rowsPerLane(int M, int forced, const Tuning &t) {
     // Tuned: the shape with the least expected time for this profile length.
     int best = 4;
     double bestT = 1e300;
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < kNumR; ++q) {
         if (!(t.rate[q] > 0)) continue;
         const double time = (double)paddedRows(M, kShapeR[q]) / t.rate[q];
         if (time < bestT) {
@@ -815,7 +817,7 @@ static HostProfile makeHostProfile(const float *values, int width, int M, const 
                                    const float *bg) {
     HostProfile hp;
     hp.M = M;
-    hp.rowPad = (M + 1 + kRowAlign - 1) / kRowAlign * kRowAlign;
+    hp.rowPad = rowPadOf(M);
     hp.emit.assign((size_t)kNumCodes * hp.rowPad, 0.0f);
     for (int i = 0; i <= M; ++i)
         for (int c = 0; c < kNumCodes; ++c) hp.emit[(size_t)c * hp.rowPad + i] = values[(size_t)i * width + 4 + c];
@@ -1553,17 +1555,20 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // launch; its profiles join the largest group instead.
     std::vector<int> profR(ctx->profiles.size(), 0);
     {
-        long long groupPairs[3] = {0, 0, 0};
+        long long groupPairs[kNumR] = {0, 0, 0, 0};
         for (size_t i = 0; i < n; ++i) {
             int &r = profR[pairs[i].profile];
-            if (!r) r = rowsPerLane(ctx->profiles[pairs[i].profile].M, ctx->opts.rows_per_lane, ctx->tune);
+            if (!r) {
+                r = rowsPerLane(ctx->profiles[pairs[i].profile].M, ctx->opts.rows_per_lane, ctx->tune);
+                if (plainStriped && r == 3) r = 4;  // the plain schedule's stripes take R = 4, 2 or 1
+            }
             ++groupPairs[rIndex(r)];
         }
         if (ctx->tune.tuned && !ctx->tune.forceR && ctx->opts.rows_per_lane == 0 && !plain) {
             int big = 0;
-            for (int q = 1; q < 3; ++q)
+            for (int q = 1; q < kNumR; ++q)
                 if (groupPairs[q] > groupPairs[big]) big = q;
-            for (int q = 0; q < 3; ++q) {
+            for (int q = 0; q < kNumR; ++q) {
                 const long long fill = 2LL * ctx->smCount * 4 * ctx->tune.warps[q];
                 if (q != big && groupPairs[q] > 0 && groupPairs[q] < fill)
                     for (int &r : profR)
@@ -1603,8 +1608,8 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         int grid = 0;
         size_t chunkBase = 0;
     };
-    Group groups[3];
-    for (int q = 0; q < 3; ++q) {
+    Group groups[kNumR];
+    for (int q = 0; q < kNumR; ++q) {
         const int W = ctx->tune.forceWarps ? ctx->tune.forceWarps : ctx->tune.warps[q];
         groups[q].R = kShapeR[q];
         groups[q].kernWarps = W;
@@ -1616,7 +1621,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // (or keep their table in global memory), and long pairs of tall profiles
     // are capped by the device memory their W1 slots take.
     const size_t smemLimit = (size_t)ctx->maxSmemOptin - 1024;
-    long long groupPairs[3] = {0, 0, 0};
+    long long groupPairs[kNumR] = {0, 0, 0, 0};
     for (size_t k = 0; k < n && !nullOnly; ++k) {
         Group &G = groups[groupOf(dp[k].R)];
         G.maxRowPad = std::max(G.maxRowPad, ctx->profiles[dp[k].prof].rowPad);
@@ -1658,8 +1663,8 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (size_t)(0.6 * (double)(freeB + held));
         maxSlots = std::max<size_t>(1, budget / slotBytes);
     }
-    int chunkPairsOf[3] = {1, 1, 1};
-    for (int q = 0; q < 3; ++q) {
+    int chunkPairsOf[kNumR] = {1, 1, 1, 1};
+    for (int q = 0; q < kNumR; ++q) {
         Group &G = groups[q];
         if (!groupPairs[q]) continue;
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
@@ -1748,7 +1753,8 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             plainScratch = std::max(plainScratch, (size_t)plainScratchFloats(dp[k].M, dp[k].L, dp[k].R));
     CK(ctx->dW1.ensure(std::max<size_t>(std::max(slotsMax * w1Slot, plainScratch), 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
-    const size_t nCounters = std::max<size_t>(allChunks.size() + 3, 6);  // search: the second wave's at 3..5
+    // one counter per group (search: the second wave's after them; the one-warp plain schedule: one per chunk)
+    const size_t nCounters = std::max<size_t>(allChunks.size() + kNumR, 2 * kNumR);
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
 
     // Null-model jobs: up to 32 pairs of reads of one length per warp (the
@@ -1945,7 +1951,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(record(S.ev[1]), "event");
         if (search) {
             // the filter wave over every pair, then each chunk's survivors
-            for (int gi = 0; gi < 3; ++gi) {
+            for (int gi = 0; gi < kNumR; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
                 DpArgs gk = g;
@@ -1965,7 +1971,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             ++launches;
         }
         if (!forceExact && !nullOnly) {
-            for (int gi = 0; gi < 3; ++gi) {
+            for (int gi = 0; gi < kNumR; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
                 if (plainStriped) {
@@ -1983,7 +1989,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                         DpArgs gk = g;
                         gk.chunks = ctx->dChunks.p + G.chunkBase + k;
                         gk.nChunks = 1;
-                        gk.chunkCounter = ctx->dCounter.p + 3 + G.chunkBase + k;
+                        gk.chunkCounter = ctx->dCounter.p + kNumR + G.chunkBase + k;
                         G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                         ++launches;
                     }
@@ -1991,7 +1997,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                     DpArgs gk = g;
                     gk.chunks = (search ? ctx->dMidChunks.p : ctx->dChunks.p) + G.chunkBase;
                     gk.nChunks = (int)G.chunks.size();
-                    gk.chunkCounter = ctx->dCounter.p + (search ? 3 : 0) + gi;
+                    gk.chunkCounter = ctx->dCounter.p + (search ? kNumR : 0) + gi;
                     if (search) gk.pairIdx = ctx->dSurvivors.p;
                     G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                     ++launches;
@@ -2799,7 +2805,7 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
             return ctx->fail(DMST_EINVAL, "autotune sample pair %zu: unknown sequence or profile id", i);
     std::vector<dmst_result> res(n);
     Tuning t = ctx->tune;
-    for (int q = 0; q < 3; ++q) {
+    for (int q = 0; q < kNumR; ++q) {
         const int R = kShapeR[q];
         double padded = 0;
         for (size_t i = 0; i < n; ++i)
@@ -2820,7 +2826,7 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
                 return st;
             }
             const double rate = ms > 0 ? padded / ms : 0;  // padded cells per ms
-            if (gcups6 && w < 2) gcups6[q * 2 + w] = rate / 1e6;
+            if (gcups6 && w < 2 && R != 3) gcups6[(q == 0 ? 0 : q - 1) * 2 + w] = rate / 1e6;  // R = 4, 2, 1
             t.rates[q][w] = rate;
             if (rate > bestRate) {
                 bestRate = rate;
@@ -2837,8 +2843,15 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
 
 int dmst_tuned_rates(const dmst_ctx *ctx, double *gcups9) {
     if (!ctx || !gcups9) return DMST_EINVAL;
-    for (int q = 0; q < 3; ++q)
-        for (int w = 0; w < 3; ++w) gcups9[q * 3 + w] = ctx->tune.rates[q][w] / 1e6;
+    const int qs[3] = {rIndex(4), rIndex(2), rIndex(1)};
+    for (int i = 0; i < 3; ++i)
+        for (int w = 0; w < 3; ++w) gcups9[i * 3 + w] = ctx->tune.rates[qs[i]][w] / 1e6;
+    return DMST_OK;
+}
+
+int dmst_tuned_rates_ex(const dmst_ctx *ctx, double *gcups, int n) {
+    if (!ctx || !gcups || n < 0 || n > kNumR * 3) return DMST_EINVAL;
+    for (int i = 0; i < n; ++i) gcups[i] = ctx->tune.rates[i / 3][i % 3] / 1e6;
     return DMST_OK;
 }
 

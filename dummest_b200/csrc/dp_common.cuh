@@ -11,6 +11,15 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kNumCodes = 25;    // codon codes 0..24 (24 = zero pad, dummest-dp.hh:93)
 constexpr int kPad = 24;
 constexpr int kRowAlign = 128;   // emission-table row padding (32 lanes x 4 rows)
+// Rows of a profile's emission table and coefficient planes: M+1 rounded up
+// to whole 96-row stripes (32 lanes x 3 rows), then to kRowAlign, so that the
+// last stripe of every rows-per-lane shape (128, 96, 64 or 32 rows) lies in
+// the zero-filled padding.
+__host__ __device__ constexpr int rowPadOf(int M) {
+    const int r96 = (M + 1 + 95) / 96 * 96;
+    const int r = r96 > M + 1 ? r96 : M + 1;
+    return (r + kRowAlign - 1) / kRowAlign * kRowAlign;
+}
 constexpr int kParamFloats = 11; // Params (dummest-core.hh:233-239)
 // RESCALE_THRESH of the FP32 engine (dummest-score.hh:93).  The fast path is
 // exact with respect to the reference only while no row maximum exceeds it.

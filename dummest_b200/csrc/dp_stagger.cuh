@@ -278,6 +278,11 @@ __device__ __forceinline__ void bwdStepS(BwdS<R> &b, const SweepArgs &a, WindowS
         b.maxY = fmax3(b.maxY, nY[2], nY[3]);
         b.filt = fmax3(b.filt, nW[0] * pv[0], nW[1] * pv[1]);
         b.filt = fmax3(b.filt, nW[2] * pv[2], nW[3] * pv[3]);
+    } else if constexpr (R == 3) {
+        b.maxY = fmax3(b.maxY, nY[0], nY[1]);
+        b.maxY = fmaxf(b.maxY, nY[2]);
+        b.filt = fmax3(b.filt, nW[0] * pv[0], nW[1] * pv[1]);
+        b.filt = fmaxf(b.filt, nW[2] * pv[2]);
     } else if constexpr (R == 2) {
         b.maxY = fmax3(b.maxY, nY[0], nY[1]);
         b.filt = fmax3(b.filt, nW[0] * pv[0], nW[1] * pv[1]);
@@ -410,10 +415,15 @@ struct FwdS {
 template <int R>
 __device__ __forceinline__ void cpAsyncStage(float *dst, const float *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    if constexpr (R == 4)
+    if constexpr (R == 4) {
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-    else
+    } else if constexpr (R == 3) {  // 12 bytes: three 4-byte copies (4, 8 and 16 bytes are the copy sizes)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d + 4u * k), "l"(src + k) : "memory");
+    } else {
         asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(4 * R) : "memory");
+    }
 }
 
 template <int R, int PH, bool GEN, bool SH>
@@ -434,7 +444,8 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
         q[0] = v.x;
         q[1] = v.y;
     } else {
-        q[0] = win.w1[PH][lane];
+#pragma unroll
+        for (int k = 0; k < R; ++k) q[k] = win.w1[PH][lane * R + k];
     }
     float inW = __shfl_up_sync(kFull, f.sendIn, 1);
     float inY = __shfl_up_sync(kFull, f.sendY, 1);
@@ -493,6 +504,9 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
     if constexpr (R == 4) {
         f.best = fmax3(f.best, bv[0], bv[1]);
         f.best = fmax3(f.best, bv[2], bv[3]);
+    } else if constexpr (R == 3) {
+        f.best = fmax3(f.best, bv[0], bv[1]);
+        f.best = fmaxf(f.best, bv[2]);
     } else if constexpr (R == 2) {
         f.best = fmax3(f.best, bv[0], bv[1]);
     } else {
@@ -750,7 +764,8 @@ __global__ void __launch_bounds__(WARPS * kLanes, 1) dpKernel(DpArgs g, int tabl
 
 // Shared memory of one warp's staging (host side: launch sizes).
 inline size_t stagWindowBytes(int R) {
-    return R == 4 ? sizeof(WindowS<4>) : (R == 2 ? sizeof(WindowS<2>) : sizeof(WindowS<1>));
+    return R == 4 ? sizeof(WindowS<4>)
+                  : (R == 3 ? sizeof(WindowS<3>) : (R == 2 ? sizeof(WindowS<2>) : sizeof(WindowS<1>)));
 }
 
 }  // namespace dmst

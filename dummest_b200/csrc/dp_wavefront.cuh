@@ -123,8 +123,9 @@ __device__ __forceinline__ void loadRows(float (&v)[R], const float *p) {
     } else if constexpr (R == 2) {
         const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
         v[0] = t.x; v[1] = t.y;
-    } else {
-        v[0] = __ldg(p);
+    } else {  // R = 1 or 3 (rows not 8-byte aligned for R = 3)
+#pragma unroll
+        for (int k = 0; k < R; ++k) v[k] = __ldg(p + k);
     }
 }
 
@@ -184,7 +185,8 @@ __device__ __forceinline__ void loadEmit(float (&e)[R], const float *p) {
         float2 v = *reinterpret_cast<const float2 *>(p);
         e[0] = v.x; e[1] = v.y;
     } else {
-        e[0] = p[0];
+#pragma unroll
+        for (int k = 0; k < R; ++k) e[k] = p[k];
     }
 }
 
@@ -200,7 +202,8 @@ __device__ __forceinline__ void loadEmitS(float (&e)[R], unsigned addr) {
     } else if constexpr (R == 2) {
         asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(e[0]), "=f"(e[1]) : "r"(addr));
     } else {
-        asm("ld.shared.f32 %0, [%1];" : "=f"(e[0]) : "r"(addr));
+#pragma unroll
+        for (int k = 0; k < R; ++k) asm("ld.shared.f32 %0, [%1];" : "=f"(e[k]) : "r"(addr + 4u * k));
     }
 }
 
@@ -211,7 +214,8 @@ __device__ __forceinline__ void storeW1(float *p, const float (&w)[R]) {
     } else if constexpr (R == 2) {
         *reinterpret_cast<float2 *>(p) = make_float2(w[0], w[1]);
     } else {
-        p[0] = w[0];
+#pragma unroll
+        for (int k = 0; k < R; ++k) p[k] = w[k];
     }
 }
 

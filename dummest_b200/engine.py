@@ -476,9 +476,9 @@ class Context:
         for k, (s, p) in enumerate(zip(seq_ids, profile_ids)):
             pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, p, -2.0
         self._check(self.lib.dmst_autotune(self.h, pairs, n, None), "dmst_autotune")
-        out = (C.c_double * 9)()
-        self._check(self.lib.dmst_tuned_rates(self.h, out), "dmst_tuned_rates")
-        return {(r, w): out[i * 3 + j] for i, r in enumerate((4, 2, 1)) for j, w in enumerate((16, 8, 12))}
+        out = (C.c_double * 12)()
+        self._check(self.lib.dmst_tuned_rates_ex(self.h, out, 12), "dmst_tuned_rates_ex")
+        return {(r, w): out[i * 3 + j] for i, r in enumerate((4, 3, 2, 1)) for j, w in enumerate((16, 8, 12))}
 
     def set_wait_limit(self, iterations: int = 0) -> None:
         """The exact path's wait budget in 64 ns sleeps (dmst_set_wait_limit; 0: the default)."""

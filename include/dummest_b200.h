@@ -103,7 +103,7 @@ typedef struct dmst_opts {
     double stop_codon_prob;                    /* STOP_CODON_PROB */
     double bg_stop_codon_prob;                 /* BG_STOP_CODON_PROB */
     int device;                                /* CUDA device ordinal */
-    int rows_per_lane;                         /* 0 = autotuned, else 1, 2 or 4 */
+    int rows_per_lane;                         /* 0 = autotuned, else 1, 2, 3 or 4 */
     size_t device_budget_bytes;                /* 0 = 60% of free device memory */
     double tantan_threshold;                   /* TANTAN_MASK_THRESHOLD (OPT_tantan, 0.5) for DMST_HMM_MASK */
 } dmst_opts;
@@ -451,18 +451,20 @@ int dmst_last_timing(const dmst_ctx *ctx, double *total_ms, double *dp_ms, doubl
 int dmst_last_timing_ex(const dmst_ctx *ctx, double *out, int n);
 
 /* ---- autotuning ------------------------------------------------------
- * Kernel shapes: R rows of the profile per lane (a stripe of 32 R rows: 4, 2
- * or 1) and 16, 8 or 12 warps per CTA.  dmst_autotune times the DP kernel of
+ * Kernel shapes: R rows of the profile per lane (a stripe of 32 R rows: 4, 3,
+ * 2 or 1) and 16, 8 or 12 warps per CTA.  dmst_autotune times the DP kernel of
  * every shape on the caller's sample of pairs (mode MID, each shape run twice,
  * the second timed) and keeps, per R, the fastest CTA shape and its rate in
  * computed cells per second.  Later calls with rows_per_lane == 0 then pick,
  * per profile, the R with the least expected time (computed rows / rate).
  * gcups6 (may be NULL) receives the rates in GCUPS of computed cells, for
- * R = 4, 2, 1 x 16, 8 warps; dmst_tuned_rates gives all nine (R = 4, 2, 1 x
- * 16, 8, 12 warps).  No counterpart in the reference (its SIMD width is fixed
- * at compile time). */
+ * R = 4, 2, 1 x 16, 8 warps; dmst_tuned_rates gives nine (R = 4, 2, 1 x 16, 8,
+ * 12 warps) and dmst_tuned_rates_ex the first n <= 12 of all twelve
+ * (R = 4, 3, 2, 1 x 16, 8, 12 warps).  No counterpart in the reference (its
+ * SIMD width is fixed at compile time). */
 int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcups6);
 int dmst_tuned_rates(const dmst_ctx *ctx, double *gcups9);
+int dmst_tuned_rates_ex(const dmst_ctx *ctx, double *gcups, int n);
 /* The shape a call would use for a profile of length M. */
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta);
 

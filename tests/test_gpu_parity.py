@@ -65,7 +65,7 @@ def test_null_model_bit_exact(gpu_ctx, ref32, tmp_path):
             assert np.array_equal(suf, rsuf), (L, np.argwhere(suf != rsuf)[:5])
 
 
-@pytest.mark.parametrize("rows_per_lane", [0, 1, 2, 4])
+@pytest.mark.parametrize("rows_per_lane", [0, 1, 2, 3, 4])
 def test_mid_and_filter_match_fp32_reference(ref32, ref64, tmp_path, rows_per_lane):
     Ms = [2, 31, 32, 33, 63, 95, 127, 128, 200, 257]
     rng, profs, txt = _setup_profiles(tmp_path, ref32, Ms, seed=5 + rows_per_lane)
@@ -99,17 +99,19 @@ def test_mid_and_filter_match_fp32_reference(ref32, ref64, tmp_path, rows_per_la
         print(f"R={rows_per_lane}: max |d bits| vs FP32 ref {worst:.3e}, vs FP64 ref {worst64:.3e}, exact-path pairs {n_exact}")
 
 
-def test_mid_and_filter_bit_identical_to_oracle(ref32, tmp_path):
-    """The batched kernel, the plain C oracle and the FP32 reference give the
-    same ExpScores, mantissa and exponent, for every pair: the float
-    recurrences use the reference's operations in its order (including the
-    multiply-adds its compiler forms) and the scores are exact products."""
+@pytest.mark.parametrize("rows_per_lane", [0, 1, 2, 3, 4])
+def test_mid_and_filter_bit_identical_to_oracle(ref32, tmp_path, rows_per_lane):
+    """The batched kernel (every rows-per-lane shape), the plain C oracle and
+    the FP32 reference give the same ExpScores, mantissa and exponent, for
+    every pair: the float recurrences use the reference's operations in its
+    order (including the multiply-adds its compiler forms) and the scores are
+    exact products."""
     from oracle import port
-    Ms = [2, 31, 33, 128, 257]
+    Ms = [2, 31, 33, 95, 96, 128, 191, 257]
     rng, profs, txt = _setup_profiles(tmp_path, ref32, Ms, seed=41)
-    reads = _mk_reads(rng, profs, [3, 4, 7, 33, 150, 640, 1000])
+    reads = _mk_reads(rng, profs, [3, 4, 7, 33, 150, 188, 640, 1000])
     codes = [ref32.decode(ref32.encode(s)) for s in reads]
-    with d.Context(device=0) as ctx:
+    with d.Context(device=0, rows_per_lane=rows_per_lane) as ctx:
         pids = ctx.load_hmm(txt)
         sids = ctx.add_decoded(codes)
         for p, pid in enumerate(pids):

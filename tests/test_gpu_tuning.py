@@ -43,11 +43,11 @@ def test_autotune_measures_every_shape_and_keeps_results(ref32, tmp_path):
         sids = ctx.add_decoded(codes)
         before = _got(ctx, sids, pids, d.MODE_MID)
         rates = ctx.autotune([s for _ in pids for s in sids], [p for p in pids for _ in sids])
-        assert set(rates) == {(r, w) for r in (4, 2, 1) for w in (16, 8, 12)}
+        assert set(rates) == {(r, w) for r in (4, 3, 2, 1) for w in (16, 8, 12)}
         assert all(v > 0 for v in rates.values()), rates
         for M in Ms:
             r, w = ctx.tuned_shape(M)
-            assert r in (1, 2, 4) and w in (8, 12, 16)
+            assert r in (1, 2, 3, 4) and w in (8, 12, 16)
         after = _got(ctx, sids, pids, d.MODE_MID)
     assert before == want
     assert after == want
