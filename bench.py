@@ -1275,8 +1275,10 @@ def run_ours(args, rank, world, local):
         for M in Ms:
             key = "R%d/W%d" % ctx.tuned_shape(int(M))
             shapes[key] = shapes.get(key, 0) + 1
+        short = ctx.tuned_rates("short")
         tuning = {"gcups_computed_cells": {f"R{r}/W{w}": round(v, 2) for (r, w), v in rates.items()},
-                  "profiles_per_shape": shapes, "sample_pairs": len(samp) * len(pids)}
+                  "gcups_computed_cells_short_reads": {f"R{r}/W{w}": round(v, 2) for (r, w), v in short.items()},
+                  "profiles_per_shape_long_reads": shapes, "sample_pairs": len(samp) * len(pids)}
     MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
     for w in range(args.warmup):
         finish(ctx.score_pairs_raw(set_pairs[step_set[w]], MODE), step_set[w])

@@ -425,35 +425,51 @@ inline long long paddedRows(int M, int R) {
     return (M + 1 + S - 1) / S * S;
 }
 
-// What the autotuner measured: per rows-per-lane value, the faster CTA shape
-// and its rate in computed (padded) cells per millisecond.
+// Kernel shapes: (R, W) pairs, index rIndex(R) * 3 + wIndex(W).
+constexpr int kNumShapes = kNumR * 3;
+inline int wIndex(int W) { return W == kShapeWarps[0] ? 0 : (W == kShapeWarps[1] ? 1 : 2); }
+// Reads shorter than this form the short length class: the autotuner times
+// every shape on each class of its sample, and a pair takes the shape with
+// the least expected time for its class (16-warp CTAs of three rows per lane
+// are fastest on short reads, 8- or 12-warp CTAs of four rows on long ones).
+constexpr int kShortRead = 700;
+inline int lengthClass(int L) { return L < kShortRead ? 1 : 0; }
+
+// What the autotuner measured: per length class (0: long, 1: short) and
+// rows-per-lane value, the faster CTA shape and its rate in computed (padded)
+// cells per millisecond.
 struct Tuning {
     bool tuned = false;
-    int warps[kNumR] = {kCtaWarps, kCtaWarps, kCtaWarps, kCtaWarps};
-    double rate[kNumR] = {0, 0, 0, 0};
-    double rates[kNumR][3] = {};  // per R, per kShapeWarps: the measured rates (cells per ms), for dmst_tuned_rates
+    int warps[2][kNumR] = {{kCtaWarps, kCtaWarps, kCtaWarps, kCtaWarps}, {kCtaWarps, kCtaWarps, kCtaWarps, kCtaWarps}};
+    double rate[2][kNumR] = {};
+    double rates[2][kNumR][3] = {};  // per class, R, kShapeWarps: the measured rates (cells per ms)
     int forceR = 0, forceWarps = 0;  // set while the autotuner measures one shape
 };
 
-int rowsPerLane(int M, int forced, const Tuning &t) {
-    if (forced >= 1 && forced <= 4) return forced;
-    if (t.forceR) return t.forceR;
-    // Untuned default, measured on B200 (synthetic profiles, M 50-800): the
-    // per-step cost of a lane dominates, so four rows per lane is fastest per
-    // real cell even where most of the 128-row stripe is padding.
-    if (!t.tuned) return 4;
-    // Tuned: the shape with the least expected time for this profile length.
-    int best = 4;
-    double bestT = 1e300;
-    for (int q = 0; q < kNumR; ++q) {
-        if (!(t.rate[q] > 0)) continue;
-        const double time = (double)paddedRows(M, kShapeR[q]) / t.rate[q];
-        if (time < bestT) {
-            bestT = time;
-            best = kShapeR[q];
+// The kernel shape of a pair of a profile of length M and a read of length L.
+void shapeOf(int M, int L, int forced, const Tuning &t, int &R, int &W) {
+    const int c = lengthClass(L);
+    if (forced >= 1 && forced <= 4) {
+        R = forced;
+    } else if (t.forceR) {
+        R = t.forceR;
+    } else if (!t.tuned) {
+        // Untuned default: four rows per lane.
+        R = 4;
+    } else {
+        // Tuned: the R with the least expected time (computed rows / rate).
+        R = 4;
+        double bestT = 1e300;
+        for (int q = 0; q < kNumR; ++q) {
+            if (!(t.rate[c][q] > 0)) continue;
+            const double time = (double)paddedRows(M, kShapeR[q]) / t.rate[c][q];
+            if (time < bestT) {
+                bestT = time;
+                R = kShapeR[q];
+            }
         }
     }
-    return best;
+    W = t.forceWarps ? t.forceWarps : t.warps[c][rIndex(R)];
 }
 
 }  // namespace
@@ -1550,29 +1566,30 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             for (size_t i = 0; i < n; ++i) order[i] = keys[i].second;
         }
     }
-    // Rows per lane per profile.  With tuned shapes, a rows-per-lane group too
-    // small to give every CTA two chunks would run as its own underfilled
-    // launch; its profiles join the largest group instead.
-    std::vector<int> profR(ctx->profiles.size(), 0);
+    // The kernel shape of every pair (rows per lane and warps per CTA, from
+    // the profile's length and the read's length class).  With tuned shapes,
+    // a shape group too small to give every CTA two chunks would run as its
+    // own underfilled launch; its pairs join the largest group instead.
+    std::vector<int> pairShape(n);
     {
-        long long groupPairs[kNumR] = {0, 0, 0, 0};
+        long long groupPairs[kNumShapes] = {};
         for (size_t i = 0; i < n; ++i) {
-            int &r = profR[pairs[i].profile];
-            if (!r) {
-                r = rowsPerLane(ctx->profiles[pairs[i].profile].M, ctx->opts.rows_per_lane, ctx->tune);
-                if (plainStriped && r == 3) r = 4;  // the plain schedule's stripes take R = 4, 2 or 1
-            }
-            ++groupPairs[rIndex(r)];
+            int R, W;
+            shapeOf(ctx->profiles[pairs[i].profile].M, ctx->seqLen[pairs[i].seq], ctx->opts.rows_per_lane, ctx->tune,
+                    R, W);
+            if (plainStriped && R == 3) R = 4;  // the plain schedule's stripes take R = 4, 2 or 1
+            pairShape[i] = rIndex(R) * 3 + wIndex(W);
+            ++groupPairs[pairShape[i]];
         }
         if (ctx->tune.tuned && !ctx->tune.forceR && ctx->opts.rows_per_lane == 0 && !plain) {
             int big = 0;
-            for (int q = 1; q < kNumR; ++q)
+            for (int q = 1; q < kNumShapes; ++q)
                 if (groupPairs[q] > groupPairs[big]) big = q;
-            for (int q = 0; q < kNumR; ++q) {
-                const long long fill = 2LL * ctx->smCount * 4 * ctx->tune.warps[q];
+            for (int q = 0; q < kNumShapes; ++q) {
+                const long long fill = 2LL * ctx->smCount * 4 * kShapeWarps[q % 3];
                 if (q != big && groupPairs[q] > 0 && groupPairs[q] < fill)
-                    for (int &r : profR)
-                        if (r == kShapeR[q]) r = kShapeR[big];
+                    for (int &sh : pairShape)
+                        if (sh == q) sh = big;
             }
         }
     }
@@ -1586,15 +1603,15 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         d.L = ctx->seqLen[q.seq];
         d.M = ctx->profiles[q.profile].M;
         d.prof = q.profile;
-        d.R = profR[q.profile];
+        d.R = kShapeR[pairShape[order[k]] / 3];
         d.seedOff = seedFloats;
         seedFloats += 2LL * d.L;
         // the staggered kernel's W1 groups (one per step) and its ring (W, Y per column)
         if (mid) w1Max = std::max(w1Max, (size_t)stagSlotFloats(d.M, d.L, d.R));
         ringMax = std::max(ringMax, 2 * (size_t)stagPeriod(d.L, d.R));
     }
-    // Kernel groups by rows per lane (fixed per profile).  Chunks: runs of up to
-    // 2 x warps pairs of one profile, costliest first within each group.
+    // Kernel groups by shape.  Chunks: runs of pairs of one profile and shape,
+    // costliest first within each group.
     struct Group {
         int R, warps;     // warps launched per CTA (<= kernWarps when shared memory is short)
         int kernWarps;    // the kernel's CTA shape (warp slots per CTA)
@@ -1608,24 +1625,24 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         int grid = 0;
         size_t chunkBase = 0;
     };
-    Group groups[kNumR];
-    for (int q = 0; q < kNumR; ++q) {
-        const int W = ctx->tune.forceWarps ? ctx->tune.forceWarps : ctx->tune.warps[q];
-        groups[q].R = kShapeR[q];
+    Group groups[kNumShapes];
+    for (int q = 0; q < kNumShapes; ++q) {
+        const int W = kShapeWarps[q % 3];
+        groups[q].R = kShapeR[q / 3];
         groups[q].kernWarps = W;
         groups[q].warps = W;
-        groups[q].kern = dpKernelFor(kShapeR[q], mid, W, false);
+        groups[q].kern = dpKernelFor(groups[q].R, mid, W, false);
     }
-    auto groupOf = [](int R) { return rIndex(R); };
+    auto groupOf = [&](size_t k) { return pairShape[order[k]]; };  // the group of sorted position k
     // Warps per CTA: tall profiles leave less shared memory for the windows
     // (or keep their table in global memory), and long pairs of tall profiles
     // are capped by the device memory their W1 slots take.
     const size_t smemLimit = (size_t)ctx->maxSmemOptin - 1024;
-    long long groupPairs[kNumR] = {0, 0, 0, 0};
+    long long groupPairs[kNumShapes] = {};
     for (size_t k = 0; k < n && !nullOnly; ++k) {
-        Group &G = groups[groupOf(dp[k].R)];
+        Group &G = groups[groupOf(k)];
         G.maxRowPad = std::max(G.maxRowPad, ctx->profiles[dp[k].prof].rowPad);
-        ++groupPairs[groupOf(dp[k].R)];
+        ++groupPairs[groupOf(k)];
     }
     // Slot sizes rounded up to one of eight levels per power of two (at most
     // 12.5% larger), so that calls of similar shape keep the same slot layout
@@ -1663,8 +1680,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             ctx->opts.device_budget_bytes ? ctx->opts.device_budget_bytes : (size_t)(0.6 * (double)(freeB + held));
         maxSlots = std::max<size_t>(1, budget / slotBytes);
     }
-    int chunkPairsOf[kNumR] = {1, 1, 1, 1};
-    for (int q = 0; q < kNumR; ++q) {
+    int chunkPairsOf[kNumShapes];
+    for (int q = 0; q < kNumShapes; ++q) {
+        chunkPairsOf[q] = 1;
         Group &G = groups[q];
         if (!groupPairs[q]) continue;
         const size_t table = (size_t)kNumCodes * G.maxRowPad * sizeof(float);
@@ -1687,11 +1705,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             plain ? 1 : (int)std::max<long long>(1, std::min<long long>(4LL * G.warps, std::max(floorPairs, perCta)));
     }
     for (size_t k = 0; k < n && !nullOnly;) {
-        Group &G = groups[groupOf(dp[k].R)];
+        Group &G = groups[groupOf(k)];
         size_t e = k;
         double cost = 0;
-        const int chunkPairs = chunkPairsOf[groupOf(dp[k].R)];
-        while (e < n && dp[e].prof == dp[k].prof && (int)(e - k) < chunkPairs) {
+        const int chunkPairs = chunkPairsOf[groupOf(k)];
+        while (e < n && dp[e].prof == dp[k].prof && groupOf(e) == groupOf(k) && (int)(e - k) < chunkPairs) {
             cost += (double)(dp[e].M + 1) * dp[e].L;
             ++e;
         }
@@ -1754,7 +1772,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     CK(ctx->dW1.ensure(std::max<size_t>(std::max(slotsMax * w1Slot, plainScratch), 1)), "alloc W1 slots");
     CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
     // one counter per group (search: the second wave's after them; the one-warp plain schedule: one per chunk)
-    const size_t nCounters = std::max<size_t>(allChunks.size() + kNumR, 2 * kNumR);
+    const size_t nCounters = std::max<size_t>(allChunks.size() + kNumShapes, 2 * kNumShapes);
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
 
     // Null-model jobs: up to 32 pairs of reads of one length per warp (the
@@ -1951,7 +1969,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         CK(record(S.ev[1]), "event");
         if (search) {
             // the filter wave over every pair, then each chunk's survivors
-            for (int gi = 0; gi < kNumR; ++gi) {
+            for (int gi = 0; gi < kNumShapes; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
                 DpArgs gk = g;
@@ -1971,7 +1989,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
             ++launches;
         }
         if (!forceExact && !nullOnly) {
-            for (int gi = 0; gi < kNumR; ++gi) {
+            for (int gi = 0; gi < kNumShapes; ++gi) {
                 Group &G = groups[gi];
                 if (G.chunks.empty()) continue;
                 if (plainStriped) {
@@ -1989,7 +2007,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                         DpArgs gk = g;
                         gk.chunks = ctx->dChunks.p + G.chunkBase + k;
                         gk.nChunks = 1;
-                        gk.chunkCounter = ctx->dCounter.p + kNumR + G.chunkBase + k;
+                        gk.chunkCounter = ctx->dCounter.p + kNumShapes + G.chunkBase + k;
                         G.kern<<<1, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                         ++launches;
                     }
@@ -1997,7 +2015,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                     DpArgs gk = g;
                     gk.chunks = (search ? ctx->dMidChunks.p : ctx->dChunks.p) + G.chunkBase;
                     gk.nChunks = (int)G.chunks.size();
-                    gk.chunkCounter = ctx->dCounter.p + (search ? kNumR : 0) + gi;
+                    gk.chunkCounter = ctx->dCounter.p + (search ? kNumShapes : 0) + gi;
                     if (search) gk.pairIdx = ctx->dSurvivors.p;
                     G.kern<<<G.grid, G.warps * kLanes, G.smem, ctx->stream>>>(gk, G.gt ? 0 : kNumCodes * G.maxRowPad);
                     ++launches;
@@ -2803,37 +2821,55 @@ int dmst_autotune(dmst_ctx *ctx, const dmst_pair *sample, size_t n, double *gcup
         if (sample[i].seq < 0 || sample[i].seq >= (int)ctx->seqLen.size() || sample[i].profile < 0 ||
             sample[i].profile >= (int)ctx->profiles.size())
             return ctx->fail(DMST_EINVAL, "autotune sample pair %zu: unknown sequence or profile id", i);
-    std::vector<dmst_result> res(n);
+    // The sample's pairs by read length class; every shape is timed on each.
+    std::vector<dmst_pair> cls[2];
+    for (size_t i = 0; i < n; ++i) cls[lengthClass(ctx->seqLen[sample[i].seq])].push_back(sample[i]);
     Tuning t = ctx->tune;
-    for (int q = 0; q < kNumR; ++q) {
-        const int R = kShapeR[q];
-        double padded = 0;
-        for (size_t i = 0; i < n; ++i)
-            padded += (double)paddedRows(ctx->profiles[sample[i].profile].M, R) * ctx->seqLen[sample[i].seq];
-        double bestRate = 0;
-        for (int w = 0; w < 3; ++w) {
-            ctx->tune.forceR = R;
-            ctx->tune.forceWarps = kShapeWarps[w];
-            double ms = 0;
-            int st = DMST_OK;
-            for (int rep = 0; rep < 2 && st == DMST_OK; ++rep) {  // the first run warms up
-                st = dmst_score_pairs(ctx, sample, n, DMST_MODE_MID, res.data());
-                ms = ctx->lastDpMs;
+    for (int c = 0; c < 2; ++c) {
+        const std::vector<dmst_pair> &sub = cls[c];
+        if (sub.empty()) continue;
+        std::vector<dmst_result> res(sub.size());
+        for (int q = 0; q < kNumR; ++q) {
+            const int R = kShapeR[q];
+            double padded = 0;
+            for (const dmst_pair &pp : sub)
+                padded += (double)paddedRows(ctx->profiles[pp.profile].M, R) * ctx->seqLen[pp.seq];
+            double bestRate = 0;
+            for (int w = 0; w < 3; ++w) {
+                ctx->tune.forceR = R;
+                ctx->tune.forceWarps = kShapeWarps[w];
+                double ms = 0;
+                int st = DMST_OK;
+                for (int rep = 0; rep < 2 && st == DMST_OK; ++rep) {  // the first run warms up
+                    st = dmst_score_pairs(ctx, sub.data(), sub.size(), DMST_MODE_MID, res.data());
+                    ms = ctx->lastDpMs;
+                }
+                ctx->tune.forceR = ctx->tune.forceWarps = 0;
+                if (st) {
+                    ctx->tune = t;
+                    return st;
+                }
+                const double rate = ms > 0 ? padded / ms : 0;  // padded cells per ms
+                t.rates[c][q][w] = rate;
+                if (rate > bestRate) {
+                    bestRate = rate;
+                    t.warps[c][q] = kShapeWarps[w];
+                }
             }
-            ctx->tune.forceR = ctx->tune.forceWarps = 0;
-            if (st) {
-                ctx->tune = t;
-                return st;
-            }
-            const double rate = ms > 0 ? padded / ms : 0;  // padded cells per ms
-            if (gcups6 && w < 2 && R != 3) gcups6[(q == 0 ? 0 : q - 1) * 2 + w] = rate / 1e6;  // R = 4, 2, 1
-            t.rates[q][w] = rate;
-            if (rate > bestRate) {
-                bestRate = rate;
-                t.warps[q] = kShapeWarps[w];
-            }
+            t.rate[c][q] = bestRate;
         }
-        t.rate[q] = bestRate;
+    }
+    // a class the sample does not have takes the other's shapes
+    for (int c = 0; c < 2; ++c)
+        if (cls[c].empty()) {
+            std::memcpy(t.warps[c], t.warps[1 - c], sizeof t.warps[c]);
+            std::memcpy(t.rate[c], t.rate[1 - c], sizeof t.rate[c]);
+            std::memcpy(t.rates[c], t.rates[1 - c], sizeof t.rates[c]);
+        }
+    if (gcups6) {
+        const int qs[3] = {rIndex(4), rIndex(2), rIndex(1)};
+        for (int i = 0; i < 3; ++i)
+            for (int w = 0; w < 2; ++w) gcups6[i * 2 + w] = t.rates[0][qs[i]][w] / 1e6;
     }
     t.tuned = true;
     t.forceR = t.forceWarps = 0;
@@ -2845,13 +2881,16 @@ int dmst_tuned_rates(const dmst_ctx *ctx, double *gcups9) {
     if (!ctx || !gcups9) return DMST_EINVAL;
     const int qs[3] = {rIndex(4), rIndex(2), rIndex(1)};
     for (int i = 0; i < 3; ++i)
-        for (int w = 0; w < 3; ++w) gcups9[i * 3 + w] = ctx->tune.rates[qs[i]][w] / 1e6;
+        for (int w = 0; w < 3; ++w) gcups9[i * 3 + w] = ctx->tune.rates[0][qs[i]][w] / 1e6;
     return DMST_OK;
 }
 
 int dmst_tuned_rates_ex(const dmst_ctx *ctx, double *gcups, int n) {
-    if (!ctx || !gcups || n < 0 || n > kNumR * 3) return DMST_EINVAL;
-    for (int i = 0; i < n; ++i) gcups[i] = ctx->tune.rates[i / 3][i % 3] / 1e6;
+    if (!ctx || !gcups || n < 0 || n > 2 * kNumShapes) return DMST_EINVAL;
+    for (int i = 0; i < n; ++i) {
+        const int c = i / kNumShapes, k = i % kNumShapes;
+        gcups[i] = ctx->tune.rates[c][k / 3][k % 3] / 1e6;
+    }
     return DMST_OK;
 }
 
@@ -3054,9 +3093,10 @@ int dmst_posterior_summary(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, doub
 
 int dmst_tuned_shape(const dmst_ctx *ctx, int M, int *rows_per_lane, int *warps_per_cta) {
     if (!ctx || M < 1) return DMST_EINVAL;
-    const int R = rowsPerLane(M, ctx->opts.rows_per_lane, ctx->tune);
+    int R, W;
+    shapeOf(M, kShortRead, ctx->opts.rows_per_lane, ctx->tune, R, W);  // reads of the long class
     if (rows_per_lane) *rows_per_lane = R;
-    if (warps_per_cta) *warps_per_cta = ctx->tune.warps[rIndex(R)];
+    if (warps_per_cta) *warps_per_cta = W;
     return DMST_OK;
 }
 

@@ -468,17 +468,24 @@ class Context:
         return logt, out
 
     def autotune(self, seq_ids: Sequence[int], profile_ids: Sequence[int]) -> dict:
-        """Time every kernel shape on these pairs (dmst_autotune); returns the
-        rates in GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)
-        (dmst_tuned_rates)."""
+        """Time every kernel shape on these pairs (dmst_autotune), on their
+        short and long reads separately; returns the long class's rates in
+        GCUPS of computed cells keyed by (rows_per_lane, warps_per_cta)."""
         n = len(seq_ids)
         pairs = (F.Pair * n)()
         for k, (s, p) in enumerate(zip(seq_ids, profile_ids)):
             pairs[k].seq, pairs[k].profile, pairs[k].min_prob_ratio = s, p, -2.0
         self._check(self.lib.dmst_autotune(self.h, pairs, n, None), "dmst_autotune")
-        out = (C.c_double * 12)()
-        self._check(self.lib.dmst_tuned_rates_ex(self.h, out, 12), "dmst_tuned_rates_ex")
-        return {(r, w): out[i * 3 + j] for i, r in enumerate((4, 3, 2, 1)) for j, w in enumerate((16, 8, 12))}
+        return self.tuned_rates("long")
+
+    def tuned_rates(self, length_class: str = "long") -> dict:
+        """The autotuner's rates (GCUPS of computed cells) keyed by
+        (rows_per_lane, warps_per_cta) for the reads of one length class:
+        "long" (700 nt and more) or "short" (dmst_tuned_rates_ex)."""
+        out = (C.c_double * 24)()
+        self._check(self.lib.dmst_tuned_rates_ex(self.h, out, 24), "dmst_tuned_rates_ex")
+        base = 0 if length_class == "long" else 12
+        return {(r, w): out[base + i * 3 + j] for i, r in enumerate((4, 3, 2, 1)) for j, w in enumerate((16, 8, 12))}
 
     def set_wait_limit(self, iterations: int = 0) -> None:
         """The exact path's wait budget in 64 ns sleeps (dmst_set_wait_limit; 0: the default)."""

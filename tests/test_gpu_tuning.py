@@ -45,6 +45,8 @@ def test_autotune_measures_every_shape_and_keeps_results(ref32, tmp_path):
         rates = ctx.autotune([s for _ in pids for s in sids], [p for p in pids for _ in sids])
         assert set(rates) == {(r, w) for r in (4, 3, 2, 1) for w in (16, 8, 12)}
         assert all(v > 0 for v in rates.values()), rates
+        short = ctx.tuned_rates("short")  # the sample has reads on both sides of 700 nt
+        assert set(short) == set(rates) and all(v > 0 for v in short.values()), short
         for M in Ms:
             r, w = ctx.tuned_shape(M)
             assert r in (1, 2, 3, 4) and w in (8, 12, 16)
