@@ -3269,9 +3269,6 @@ __global__ void naHeaderKernel(NaHeader h, NaHeader *dst) {
     if (threadIdx.x == 0) *dst = h;
 }
 
-constexpr int kNaMaxDevices = 64;
-std::mutex gNaMutex;
-void *gNaScratch[kNaMaxDevices];  // per-device address of gNullScratch, set on first use
 
 }  // namespace
 
@@ -3288,24 +3285,13 @@ extern "C" int dmst_null_model_noalloc(const uint8_t *codes, int length, const f
     // An error left pending by the caller's earlier CUDA work is reported as
     // it is and left in place for the caller to read (not cleared here).
     if (cudaPeekAtLastError() != cudaSuccess) return DMST_EDEVICE;
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) {
+    // The scratch's address on the current device, asked for on every call
+    // (it allocates nothing once the module is loaded, and stays right after
+    // a device reset, which gives module globals new addresses).
+    void *base = nullptr;
+    if (cudaGetSymbolAddress(&base, gNullScratch) != cudaSuccess || !base) {
         cudaGetLastError();
         return DMST_EDEVICE;
-    }
-    void *base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(gNaMutex);
-        if (!gNaScratch[dev]) {
-            // Set-up, once per device, with that device current.
-            void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, gNullScratch) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return DMST_EDEVICE;
-            }
-            gNaScratch[dev] = p;
-        }
-        base = gNaScratch[dev];
     }
     NaHeader *hdr = reinterpret_cast<NaHeader *>(base);
     XS *tmp = reinterpret_cast<XS *>(static_cast<unsigned char *>(base) + kNaHeaderBytes);
