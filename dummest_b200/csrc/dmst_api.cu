@@ -538,6 +538,7 @@ struct dmst_ctx {
     int device = 0;
     int smCount = 0;
     int maxSmemOptin = 0;
+    int nullBlocksPerSm = 0;  // resident null-model blocks per SM (queried on first use)
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;  // the exact path and result copies of scoring calls
     PinnedBuf<char> hSeqStage[2];    // dmst_seqs_add_packed: host staging blocks, in turn
@@ -1777,11 +1778,13 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
 
     // Null-model jobs: up to 32 pairs of reads of one length per warp (the
     // lanes run in lock step over the columns), the pairs of one read
-    // side by side.
+    // side by side, the longest reads first: the kernel's warps take the jobs
+    // round-robin, so that each warp ends on short jobs and the kernel has no
+    // tail of long reads started last.
     std::vector<int> jobPairs(n);
     {
         // A counting sort of the (profile-major) pair slots by read, with the
-        // call's reads taken in (length, id) order.
+        // call's reads taken in (length descending, id) order.
         const size_t nSeq = ctx->seqLen.size();
         std::vector<int> start(nSeq, 0);  // pairs of each read, then where they start
         for (size_t k = 0; k < n; ++k) ++start[pairs[order[k]].seq];
@@ -1789,7 +1792,7 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
         for (size_t q = 0; q < nSeq; ++q)
             if (start[q]) used.push_back((int)q);
         std::sort(used.begin(), used.end(), [&](int x, int y) {
-            return ctx->seqLen[x] != ctx->seqLen[y] ? ctx->seqLen[x] < ctx->seqLen[y] : x < y;
+            return ctx->seqLen[x] != ctx->seqLen[y] ? ctx->seqLen[x] > ctx->seqLen[y] : x < y;
         });
         int at = 0;
         for (int q : used) {
@@ -1930,7 +1933,15 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     nr.single = (double)(ctx->rates.insert1 + ctx->rates.delete2);
     nr.dbl = (double)(ctx->rates.insert2 + ctx->rates.delete1);
     const int nj = (int)nullJobs.size();
-    const int nullBlocks = std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * 16));
+    // One wave of null-model blocks: as many as fit on the GPU at once.
+    if (!ctx->nullBlocksPerSm) {
+        int perSm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, nullModelKernel, kNullWarps * 32, 0),
+           "null-model occupancy");
+        ctx->nullBlocksPerSm = std::max(1, perSm);
+    }
+    const int nullBlocks =
+        std::max(1, std::min((nj + kNullWarps - 1) / kNullWarps, ctx->smCount * ctx->nullBlocksPerSm));
     DpArgs g;
     g.pairs = S.dPairs.p;
     g.profiles = ctx->dProfiles.p;
