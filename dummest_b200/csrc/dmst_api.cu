@@ -2041,6 +2041,9 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
                                                                         search ? S.dMask.p : nullptr);
             CK(cudaGetLastError(), "flag kernel");
             ++launches;
+            queueSortKernel<<<1, 1024, 0, ctx->stream>>>(S.dQueue.p, S.dQueueCount.p, S.dPairs.p);
+            CK(cudaGetLastError(), "queue sort kernel");
+            ++launches;
         }
         return DMST_OK;
     };

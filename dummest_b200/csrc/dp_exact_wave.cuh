@@ -297,6 +297,48 @@ __global__ void flagKernel(const PairOut *po, int n, int force, int *queue, int 
     if (!ok) queue[atomicAdd(queueCount, 1)] = k;
 }
 
+// Orders the exact-path queue costliest pair first ((M + 1) L cells, ties by
+// pair position), so that the persistent CTAs that take pairs in queue order
+// end on the cheapest ones, and the order no longer depends on the flag
+// kernel's atomics.  One CTA of 1024 threads, a bitonic sort of up to
+// kQueueSortMax entries in shared memory; a longer queue keeps its order.
+constexpr int kQueueSortMax = 4096;
+__global__ void __launch_bounds__(1024) queueSortKernel(int *queue, const int *queueCount, const DevPair *pairs) {
+    __shared__ unsigned long long key[kQueueSortMax];
+    const int cnt = *queueCount;
+    if (cnt < 2 || cnt > kQueueSortMax) return;
+    int n = 2;
+    while (n < cnt) n *= 2;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        unsigned long long v = 0;  // padding sorts last
+        if (i < cnt) {
+            const int k = queue[i];
+            const DevPair p = pairs[k];
+            const long long cells = (long long)(p.M + 1) * p.L;
+            const unsigned long long c = cells < 0xffffffffLL ? (unsigned long long)cells : 0xffffffffULL;
+            // descending cost, then ascending position (complemented)
+            v = (c << 32) | (unsigned long long)(0x7fffffffu - (unsigned)k);
+        }
+        key[i] = v;
+    }
+    __syncthreads();
+    for (int size = 2; size <= n; size *= 2) {
+        for (int stride = size / 2; stride > 0; stride /= 2) {
+            for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool desc = (lo & size) == 0;  // the final merge (size == n) is descending
+                const unsigned long long a = key[lo], b = key[hi];
+                if (desc ? a < b : a > b) {
+                    key[lo] = b;
+                    key[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) queue[i] = (int)(0x7fffffffu - (unsigned)(key[i] & 0xffffffffULL));
+}
+
 // Persistent CTAs of kPipeWarps warps take the queued pairs one at a time
 // (queueCount[1] is the next queue position) and score each with its stripes
 // spread over the CTA's warps; CTA b uses scratch slot b (slotFloats floats).
