@@ -1573,25 +1573,34 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     // own underfilled launch; its pairs join the largest group instead.
     std::vector<int> pairShape(n);
     {
+        // the shape depends on the profile and the read's length class only
+        const size_t nProf = ctx->profiles.size();
+        std::vector<int> shapeTab(2 * nProf);
+        for (size_t q = 0; q < nProf; ++q)
+            for (int c = 0; c < 2; ++c) {
+                int R, W;
+                shapeOf(ctx->profiles[q].M, c ? 0 : kShortRead, ctx->opts.rows_per_lane, ctx->tune, R, W);
+                if (plainStriped && R == 3) R = 4;  // the plain schedule's stripes take R = 4, 2 or 1
+                shapeTab[2 * q + c] = rIndex(R) * 3 + wIndex(W);
+            }
         long long groupPairs[kNumShapes] = {};
         for (size_t i = 0; i < n; ++i) {
-            int R, W;
-            shapeOf(ctx->profiles[pairs[i].profile].M, ctx->seqLen[pairs[i].seq], ctx->opts.rows_per_lane, ctx->tune,
-                    R, W);
-            if (plainStriped && R == 3) R = 4;  // the plain schedule's stripes take R = 4, 2 or 1
-            pairShape[i] = rIndex(R) * 3 + wIndex(W);
+            pairShape[i] = shapeTab[2 * (size_t)pairs[i].profile + lengthClass(ctx->seqLen[pairs[i].seq])];
             ++groupPairs[pairShape[i]];
         }
         if (ctx->tune.tuned && !ctx->tune.forceR && ctx->opts.rows_per_lane == 0 && !plain) {
             int big = 0;
             for (int q = 1; q < kNumShapes; ++q)
                 if (groupPairs[q] > groupPairs[big]) big = q;
+            int remap[kNumShapes];
+            bool any = false;
             for (int q = 0; q < kNumShapes; ++q) {
                 const long long fill = 2LL * ctx->smCount * 4 * kShapeWarps[q % 3];
-                if (q != big && groupPairs[q] > 0 && groupPairs[q] < fill)
-                    for (int &sh : pairShape)
-                        if (sh == q) sh = big;
+                remap[q] = (q != big && groupPairs[q] > 0 && groupPairs[q] < fill) ? big : q;
+                any |= remap[q] != q;
             }
+            if (any)
+                for (int &sh : pairShape) sh = remap[sh];
         }
     }
     std::vector<DevPair> dp(n);
