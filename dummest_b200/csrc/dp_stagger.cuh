@@ -34,7 +34,9 @@
 // W1 is stored by warp step: the backward's step t writes the lane's R values
 // (its rows, each at its own column) to group t of the warp's slot, and the
 // forward's step t' = (nS-1) P + L + S - 2 - t needs exactly those cells, so a
-// step's store and load are each one contiguous 32*R*4-byte access.
+// step's store and load are each one contiguous access of 32 lanes x R floats
+// (at R = 3 each lane's three values take a 16-byte entry, so that the store,
+// the forward's staging copy and its shared load are one instruction each).
 //
 // The recurrences are the reference's, term for term and in the same
 // association order:
@@ -67,10 +69,13 @@ __host__ __device__ inline long long stagSteps(int M, int L, int R) {
     const long long nS = (M + 1 + S - 1) / S;
     return (nS - 1) * stagPeriod(L, R) + L - 1 + S;
 }
-// W1 slot of one pair: one group of S floats per step, steps rounded up to the
-// forward's eight-step groups.
+// Floats per lane in a W1 group: R, and 4 at R = 3, so that a lane's values
+// are one 16-byte store, copy and load (the fourth float is padding).
+__host__ __device__ constexpr int stagLaneStride(int R) { return R == 3 ? 4 : R; }
+// W1 slot of one pair: one group of 32 stagLaneStride(R) floats per step,
+// steps rounded up to the forward's eight-step groups.
 __host__ __device__ inline long long stagSlotFloats(int M, int L, int R) {
-    return (stagSteps(M, L, R) + kSW1Slots - 1) / kSW1Slots * kSW1Slots * (long long)(kLanes * R);
+    return (stagSteps(M, L, R) + kSW1Slots - 1) / kSW1Slots * kSW1Slots * (long long)(kLanes * stagLaneStride(R));
 }
 
 // Per-warp staging: the column operands by lane-local time, the ring values
@@ -83,7 +88,7 @@ template <int R>
 struct WindowS {
     float4 col[kSWin + kSBlock];  // backward {code*rowPad, bg, suf, pre}; forward {code*rowPad, bg*sC, pre, 0}
     float2 ring[kSRingWin + kSBlock];
-    float w1[kSW1Slots][kLanes * R];
+    float w1[kSW1Slots][kLanes * stagLaneStride(R)];
     PairCold cold;
 };
 
@@ -130,6 +135,15 @@ __device__ __forceinline__ void fillStoreS(WindowS<R> &w, const SweepArgs &a, co
     if (e < kSBlock) w.col[e + kSWin] = c;
     w.ring[e2] = r;
     if (e2 < kSBlock) w.ring[e2 + kSRingWin] = r;
+}
+
+// A lane's R values of one W1 group (R = 3: one 16-byte store, padding last).
+template <int R>
+__device__ __forceinline__ void storeW1S(float *p, const float (&w)[R]) {
+    if constexpr (R == 3)
+        *reinterpret_cast<float4 *>(p) = make_float4(w[0], w[1], w[2], 0.0f);
+    else
+        storeW1<R>(p, w);
 }
 
 __device__ __forceinline__ void ringStoreS(float *ring, int col, float w, float y) {
@@ -204,6 +218,7 @@ template <int R, bool MID, int PH, bool GEN, bool SH>
 __device__ __forceinline__ void bwdStepS(BwdS<R> &b, const SweepArgs &a, WindowS<R> &win, int lane,
                                          bool ringWriter, const RunPtrs &ip) {
     constexpr int S = kLanes * R;
+    constexpr int SW = kLanes * stagLaneStride(R);  // floats per W1 group
     float inW = __shfl_down_sync(kFull, b.sendW, 1);
     float inY = __shfl_down_sync(kFull, b.sendY, 1);
     if (GEN && b.u >= 0 && b.jj == 0 && b.sp < a.nS) {
@@ -300,8 +315,8 @@ __device__ __forceinline__ void bwdStepS(BwdS<R> &b, const SweepArgs &a, WindowS
     b.sendY = nY[0];
     // the stripe's lowest row (lane 0, row 0) hands its row to the next stripe
     if (GEN) {
-        if (MID) storeW1<R>(b.wp, nW);
-        b.wp += S;
+        if (MID) storeW1S<R>(b.wp, nW);
+        b.wp += SW;
         if (lane == 0 && b.u >= 0 && b.sp < a.nS - 1 && b.jj >= R - 1 && b.jj < a.L + R - 1)
             ringStoreS(a.ring, b.jj - (R - 1), nW[0], nY[0]);
         if (b.u >= 0 && ++b.jj == a.P) {
@@ -310,7 +325,7 @@ __device__ __forceinline__ void bwdStepS(BwdS<R> &b, const SweepArgs &a, WindowS
         }
         ++b.u;
     } else {  // the run advances u, jj and the W1 pointer
-        if (MID) storeW1<R>(ip.w1 + PH * S, nW);
+        if (MID) storeW1S<R>(ip.w1 + PH * SW, nW);
         if (ringWriter) __stcg(ip.ringOut + PH, make_float2(nW[0], nY[0]));
     }
 }
@@ -318,6 +333,7 @@ __device__ __forceinline__ void bwdStepS(BwdS<R> &b, const SweepArgs &a, WindowS
 template <int R, bool MID, bool SH>
 __device__ void backwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, float &filtOut, float &maxYOut) {
     constexpr int S = kLanes * R;
+    constexpr int SW = kLanes * stagLaneStride(R);  // floats per W1 group
     BwdS<R> b;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -334,7 +350,7 @@ __device__ void backwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, fl
     b.sendW = b.sendY = b.filt = b.maxY = 0.0f;
     b.u = -(kLanes - 1 - lane) * R;  // lane 31's leading row leads
     b.jj = b.sp = 0;
-    b.wp = a.w1 + lane * R;
+    b.wp = a.w1 + lane * stagLaneStride(R);
     {
         const int rowBase = (a.nS - 1) * S + lane * R;  // in bounds before the lane's first stripe
         b.eS = SH ? (unsigned)__cvta_generic_to_shared(a.smE + rowBase) : 0u;
@@ -374,12 +390,12 @@ __device__ void backwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, fl
                 bwdStepS<R, MID, 3, false, SH>(b, a, win, lane, ringWriter, ip);
                 ip.col += 4;
                 ip.ring += 4;
-                ip.w1 += 4 * S;
+                ip.w1 += 4 * SW;
                 ip.ringOut += 4;
             }
             b.u += gB - gA;
             b.jj += gB - gA;
-            b.wp += (gB - gA) * S;
+            b.wp += (gB - gA) * SW;
         }
 #pragma unroll 1
         for (; g < n; g += 4) {
@@ -415,12 +431,8 @@ struct FwdS {
 template <int R>
 __device__ __forceinline__ void cpAsyncStage(float *dst, const float *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    if constexpr (R == 4) {
+    if constexpr (R == 4 || R == 3) {  // R = 3: the lane's 16-byte group entry, padding included
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-    } else if constexpr (R == 3) {  // 12 bytes: three 4-byte copies (4, 8 and 16 bytes are the copy sizes)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d + 4u * k), "l"(src + k) : "memory");
     } else {
         asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(4 * R) : "memory");
     }
@@ -430,6 +442,7 @@ template <int R, int PH, bool GEN, bool SH>
 __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS<R> &win, int lane,
                                          bool ringWriter, const RunPtrs &ip) {
     constexpr int S = kLanes * R;
+    constexpr int SW = kLanes * stagLaneStride(R);  // floats per W1 group
     constexpr int H = PH & 3;
     float q[R];
     cpAsyncWait<kSW1Ahead - 1>();
@@ -439,6 +452,11 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
         q[1] = v.y;
         q[2] = v.z;
         q[3] = v.w;
+    } else if constexpr (R == 3) {
+        const float4 v = *reinterpret_cast<const float4 *>(&win.w1[PH][lane * 4]);
+        q[0] = v.x;
+        q[1] = v.y;
+        q[2] = v.z;
     } else if constexpr (R == 2) {
         const float2 v = *reinterpret_cast<const float2 *>(&win.w1[PH][lane * 2]);
         q[0] = v.x;
@@ -525,9 +543,9 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
     if (GEN) {
         if (lane == kLanes - 1 && f.u >= 0 && f.sp < a.nS - 1 && f.jj >= R - 1 && f.jj < a.L + R - 1)
             ringStoreS(a.ring, f.jj - (R - 1), nN[R - 1], nY[R - 1]);
-        if (f.gAhead >= 0) cpAsyncStage<R>(&win.w1[(PH + kSW1Ahead) % kSW1Slots][lane * R], f.w1src);
+        if (f.gAhead >= 0) cpAsyncStage<R>(&win.w1[(PH + kSW1Ahead) % kSW1Slots][lane * stagLaneStride(R)], f.w1src);
         cpAsyncCommit();
-        f.w1src -= S;
+        f.w1src -= SW;
         --f.gAhead;
         if (f.u >= 0 && ++f.jj == a.P) {
             f.jj = 0;
@@ -536,7 +554,7 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
         ++f.u;
     } else {  // the run advances u, jj and the staging cursor
         if (ringWriter) __stcg(ip.ringOut + PH, make_float2(nN[R - 1], nY[R - 1]));
-        cpAsyncStage<R>(&win.w1[(PH + kSW1Ahead) % kSW1Slots][lane * R], ip.w1 - PH * S);
+        cpAsyncStage<R>(&win.w1[(PH + kSW1Ahead) % kSW1Slots][lane * stagLaneStride(R)], ip.w1 - PH * SW);
         cpAsyncCommit();
     }
 }
@@ -544,6 +562,7 @@ __device__ __forceinline__ void fwdStepS(FwdS<R> &f, const SweepArgs &a, WindowS
 template <int R, bool SH>
 __device__ void forwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, float &bestOut, float &maxOut) {
     constexpr int S = kLanes * R;
+    constexpr int SW = kLanes * stagLaneStride(R);  // floats per W1 group
     FwdS<R> f;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -569,12 +588,12 @@ __device__ void forwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, flo
     const int T = (steps + kSW1Slots - 1) / kSW1Slots * kSW1Slots;
     // step t reads the backward's group steps - 1 - t
     {
-        const float *src = a.w1 + (size_t)(steps - 1) * S + lane * R;
+        const float *src = a.w1 + (size_t)(steps - 1) * SW + lane * stagLaneStride(R);
 #pragma unroll
         for (int k = 0; k < kSW1Ahead; ++k) {
-            cpAsyncStage<R>(&win.w1[k][lane * R], src);
+            cpAsyncStage<R>(&win.w1[k][lane * stagLaneStride(R)], src);
             cpAsyncCommit();
-            src -= S;
+            src -= SW;
         }
         f.w1src = src;
         f.gAhead = steps - 1 - kSW1Ahead;
@@ -619,12 +638,12 @@ __device__ void forwardSweepS(const SweepArgs &a, WindowS<R> &win, int lane, flo
                 fwdStepS<R, 7, false, SH>(f, a, win, lane, ringWriter, ip);
                 ip.col += 8;
                 ip.ring += 8;
-                ip.w1 -= 8 * S;
+                ip.w1 -= 8 * SW;
                 ip.ringOut += 8;
             }
             f.u += gB - gA;
             f.jj += gB - gA;
-            f.w1src -= (gB - gA) * S;
+            f.w1src -= (gB - gA) * SW;
             f.gAhead -= gB - gA;
         }
 #pragma unroll 1
