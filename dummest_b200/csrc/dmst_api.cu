@@ -191,7 +191,12 @@ windowDecodeKernel(const uint32_t *words, const uint32_t *mask, const WinSeg *se
 // make the host wait for every queued call (with calls submitted one ahead of
 // their completion, a whole call's device time).  The old buffer is kept here
 // instead and freed when its context has no call in flight (drainCalls,
-// dmst_ctx_destroy), or at once when the kept bytes pass kGraveLimit.
+// dmst_ctx_destroy), or at once when the kept bytes pass graveLimit(): 40% of
+// the device's memory, at least 16 GB.  The W1 slots of the default batch
+// take 20-30 GB, so a lower limit made every growth of them (a call whose
+// longest pairs need longer slots) wait for the call in flight and leave the
+// device idle while the host finished preparing.  An allocation that fails
+// for want of memory frees the kept buffers and tries again (devAlloc).
 // ---------------------------------------------------------------------------
 struct Grave {
     void *p;
@@ -202,7 +207,17 @@ struct Grave {
 std::mutex gGraveMutex;
 std::vector<Grave> gGraves;
 size_t gGraveBytes = 0;
-constexpr size_t kGraveLimit = (size_t)16 << 30;
+size_t graveLimit() {
+    static const size_t limit = [] {
+        size_t v = (size_t)16 << 30, freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) == cudaSuccess)
+            v = std::max(v, (size_t)(0.4 * (double)totalB));
+        else
+            cudaGetLastError();
+        return v;
+    }();
+    return limit;
+}
 
 void reapGraves() {
     std::vector<Grave> g;
@@ -228,12 +243,13 @@ void reapGraves() {
 void bury(void *p, bool host, size_t bytes) {
     int dev = 0;
     cudaGetDevice(&dev);
+    const size_t limit = graveLimit();
     bool full;
     {
         std::lock_guard<std::mutex> lock(gGraveMutex);
         gGraves.push_back(Grave{p, host, dev, bytes});
         gGraveBytes += bytes;
-        full = gGraveBytes > kGraveLimit;
+        full = gGraveBytes > limit;
     }
     if (full) reapGraves();  // frees synchronise the device, as before the graveyard
 }
@@ -1779,8 +1795,11 @@ static int submitCall(dmst_ctx *ctx, const dmst_pair *pairs, size_t n, int mode,
     if (plainStriped)
         for (size_t k = 0; k < n; ++k)
             plainScratch = std::max(plainScratch, (size_t)plainScratchFloats(dp[k].M, dp[k].L, dp[k].R));
-    CK(ctx->dW1.ensure(std::max<size_t>(std::max(slotsMax * w1Slot, plainScratch), 1)), "alloc W1 slots");
-    CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1)), "alloc ring slots");
+    // 25% headroom: the slot size follows the call's longest pairs and their
+    // kernel shapes, so calls of one workload vary, and a grown W1 buffer
+    // (tens of GB) costs the host a long allocation
+    CK(ctx->dW1.ensure(std::max<size_t>(std::max(slotsMax * w1Slot, plainScratch), 1), 0.25), "alloc W1 slots");
+    CK(ctx->dRing.ensure(std::max<size_t>(slotsMax * ringSlot, 1), 0.25), "alloc ring slots");
     // one counter per group (search: the second wave's after them; the one-warp plain schedule: one per chunk)
     const size_t nCounters = std::max<size_t>(allChunks.size() + kNumShapes, 2 * kNumShapes);
     CK(ctx->dCounter.ensure(nCounters), "alloc counters");
