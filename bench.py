@@ -990,8 +990,13 @@ def run_calibration(args, rank, world, local):
         rates = ctx.autotune([sids[k] for k in samp], [pids[k // T] for k in samp])
         tuning = {"gcups_computed_cells": {f"R{r}/W{w}": round(v, 2) for (r, w), v in rates.items()}}
     MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
-    for _ in range(args.warmup):
-        ctx.score_pairs_raw(pairs, MODE)
+    # warm-up steps in the timed steps' pattern (both call slots in use)
+    for w in range(args.warmup):
+        ctx.submit_raw(pairs, MODE)
+        if w > 0:
+            ctx.complete()
+    if args.warmup:
+        ctx.complete()
     barrier(world)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -1280,8 +1285,18 @@ def run_ours(args, rank, world, local):
                   "gcups_computed_cells_short_reads": {f"R{r}/W{w}": round(v, 2) for (r, w), v in short.items()},
                   "profiles_per_shape_long_reads": shapes, "sample_pairs": len(samp) * len(pids)}
     MODE = d.MODE_MID | (0 if args.no_graph else d.MODE_GRAPH)
+    # Warm-up steps in the timed steps' pattern (each call submitted before the
+    # previous one completes), so that both of the context's call slots hold
+    # their buffers and launch graphs before the timed region.
     for w in range(args.warmup):
-        finish(ctx.score_pairs_raw(set_pairs[step_set[w]], MODE), step_set[w])
+        if args.no_async:
+            finish(ctx.score_pairs_raw(set_pairs[step_set[w]], MODE), step_set[w])
+            continue
+        ctx.submit_raw(set_pairs[step_set[w]], MODE)
+        if w > 0:
+            finish(ctx.complete(), step_set[w - 1])
+    if args.warmup and not args.no_async:
+        finish(ctx.complete(), step_set[args.warmup - 1])
     barrier(world)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -1369,10 +1384,17 @@ def run_ours(args, rank, world, local):
         e2e_pairs.append(rank_pairs(list(range(base, base + len(sets[si]))), set_shares[si]))
         base += len(sets[si])
     h2d = d2h = 0
-    for w in range(args.warmup):
+    for w in range(args.warmup):  # in the timed steps' pattern, as above
         words, mask, lens = packed[step_set[w]]
         ctx.add_packed(words, lens, mask)
-        finish(ctx.score_pairs_raw(e2e_pairs[w], MODE), step_set[w])
+        if args.no_async:
+            finish(ctx.score_pairs_raw(e2e_pairs[w], MODE), step_set[w])
+            continue
+        ctx.submit_raw(e2e_pairs[w], MODE)
+        if w > 0:
+            finish(ctx.complete(), step_set[w - 1])
+    if args.warmup and not args.no_async:
+        finish(ctx.complete(), step_set[args.warmup - 1])
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
